@@ -1,0 +1,326 @@
+#!/usr/bin/env python
+"""Benchmark of the D3Q27 cumulant level step on B200.
+
+Workload (one GPU): the 256 x 128 x 128 sphere channel (D = 24 cells at x = 64, inlet u = 0.05,
+Re = 1000, zero-gradient outlet, lateral mirrors, half-way bounce-back with the FP64
+momentum-exchange drag collected every step), FP32 arithmetic, populations stored as FP16
+deviations from the lattice weights. A step is one fused pull-stream-collide launch over all
+8,192 blocks plus the deterministic FP64 drag reduction.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--storage f16|f32|bf16|f64]
+
+MLUPS counts every cell of the level, like the reference (src/main.jl:1265,1698-1712). With N > 1
+each rank runs an independent replica (the step is not domain-decomposed here), so per-GPU work
+is fixed and ``value`` is the aggregate over ranks (weak scaling).
+
+``--impl reference`` times the reference's algorithm on the host cores: the CPU restatement of
+the reference's Julia kernel (the reference itself is Julia and cannot run on this image), FP32,
+OpenMP over every host thread, on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "MLUPS & % of HBM roofline; batched/served vs plain cases/s; p50/p99 latency"
+STORAGE_BYTES = {"f16": 2, "bf16": 2, "f32": 4, "f64": 8}
+
+
+def _env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_record(storage):
+    """Per-launch DRAM bytes of the step kernel from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "cumulant_d3q27_traffic.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text())
+    rec = d.get(storage)
+    return None if rec is None else rec.get("dram_bytes_per_launch")
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.file is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.file.flush()
+        rows = [r.split(",") for r in Path(self.file.name).read_text().strip().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        loaded = [s for s in sm if smax and s > 0.5 * smax] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": smax,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU arm (the reference's algorithm on the host cores)
+# ---------------------------------------------------------------------------------------------
+def cpu_sample_case():
+    """Bounded sample of the workload: a 256 x 128 x 16 slab of the channel (same inlet, outlet,
+    mirror faces and sphere centre line, sphere cut by the slab), 524,288 cells."""
+    from openaerolab_alpha_01_b200.cases import sphere_channel_case
+    return sphere_channel_case(256, 128, 16, diameter=24.0, centre_x=64.0)
+
+
+def run_cpu_arm(steps, warmup, target_s=None):
+    """Time the FP32 oracle on every host thread; returns (MLUPS, cores, steps_done, seconds)."""
+    import oracle
+    cores = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(cores)
+    case = cpu_sample_case()
+    d = case.dom
+    O = oracle.OracleLevel(d.coords, d.neighbor_table, d.shape, obstacle=d.obstacle, dtype=np.float32)
+    O.init_equilibrium(case.rho, case.vel)
+    p = case.params
+    for _ in range(warmup):
+        O.step(p)
+    t0 = time.perf_counter()
+    done = 0
+    while True:
+        O.step(p)
+        done += 1
+        el = time.perf_counter() - t0
+        if target_s is None and done >= steps:
+            break
+        if target_s is not None and (el >= target_s or done >= steps):
+            break
+    el = time.perf_counter() - t0
+    cells = d.n_blocks * 512
+    return cells * done / el / 1e6, cores, done, el, cells
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    mlups, cores, done, el, cells = run_cpu_arm(args.steps, args.warmup)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(mlups, 3), "unit": "MLUPS", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * el / done, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(args.storage),
+        "cpu_baseline": {"value": round(mlups, 3), "unit": "MLUPS", "cores": cores, "kind": "port",
+                         "sample": f"{cells} cells/step: 256x128x16 slab of the channel, FP32 C++ restatement of "
+                                   "kernel_cumulant.jl (Julia reference not runnable here)"},
+        "e2e": {"value": round(mlups, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(storage):
+    return {"workload": "sphere_channel_256x128x128_D24_Re1000", "cells": 256 * 128 * 128, "blocks": 8192,
+            "operator": "cumulant_d3q27", "storage": f"{storage}_dev" if storage in ("f16", "bf16") else storage,
+            "c_wale": 0.2, "solid_bc": "halfway", "forces": "FP64 momentum exchange every step",
+            "l2": "inputs larger than L2 (populations 2 x %d MB)" % (256 * 128 * 128 * 27 * STORAGE_BYTES[storage] // 2**20),
+            "parallelism": "replicas"}
+
+
+# ---------------------------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--storage", default="f16", choices=["f16", "bf16", "f32", "f64"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU-baseline leg")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = _env_int("RANK", 0)
+    world = _env_int("WORLD_SIZE", 1)
+    local = _env_int("LOCAL_RANK", 0)
+
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+
+    # CPU leg first (before any CUDA call), rank 0 at N = 1 only
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        mlups, cores, done, el, cells = run_cpu_arm(10**6, 1, target_s=args.cpu_seconds)
+        cpu = {"value": round(mlups, 3), "unit": "MLUPS", "cores": cores, "kind": "port",
+               "sample": f"{done} steps of {cells} cells (256x128x16 slab of the channel), FP32 C++ restatement "
+                         f"of kernel_cumulant.jl, OpenMP {cores} threads, {el:.1f} s"}
+
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.cuda.current_device()
+
+    from openaerolab_alpha_01_b200 import _capi as capi
+    from openaerolab_alpha_01_b200.cases import sphere_channel_case
+    from openaerolab_alpha_01_b200.solver import Geometry, Level
+
+    case = sphere_channel_case(256, 128, 128, diameter=24.0, centre_x=64.0)
+    geom = Geometry(case.dom, device=dev)
+    level = Level(geom, storage=args.storage)
+    level.init_equilibrium(case.rho, case.vel)
+    p = case.params
+    cells = case.dom.n_blocks * 512
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    with torch.cuda.stream(stream):
+        for i in range(args.warmup):
+            p.time_step_seed = i
+            level.perform_timestep(p, sh)
+    torch.cuda.synchronize()
+
+    # ---- device-timed region: K steps, a CUDA-event pair around every step on its stream ----
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t_begin, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clocks:
+        with torch.cuda.stream(stream):
+            t_begin.record(stream)
+            for i in range(args.steps):
+                p.time_step_seed = args.warmup + i
+                ev[i][0].record(stream)
+                level.perform_timestep(p, sh)
+                ev[i][1].record(stream)
+            t_end.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    total_ms = t_begin.elapsed_time(t_end)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    force = level.forces()
+
+    # ---- end-to-end through the public API: per step the step parameters go from pinned host
+    # memory into the launch and the FP64 drag comes back to pinned host memory ----
+    pinned_force = torch.zeros(3, dtype=torch.float64).pin_memory()
+    e2e_steps = args.steps
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    with torch.cuda.stream(stream):
+        for i in range(e2e_steps):
+            p.time_step_seed = args.warmup + args.steps + i
+            level.perform_timestep(p, sh)
+            level.forces_async(pinned_force.data_ptr(), sh)
+            stream.synchronize()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_s = float(te.item())
+
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        sb = STORAGE_BYTES[args.storage]
+        alg_bytes = cells * 27 * sb * 2
+        avg_ms = statistics.mean(step_ms)
+        achieved = alg_bytes / (avg_ms * 1e-3) / 1e9
+        value = world * cells * args.steps / (total_ms * 1e-3) / 1e6
+        e2e_val = world * cells * e2e_steps / e2e_s / 1e6
+        cs = clocks.summary()
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(args.storage),
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                         "frac_of_8000": round(achieved / 8000.0, 4),
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "timed_span": "per-step CUDA events around the cumulant launch and the 1-CTA FP64 drag reduction",
+                         "traffic": traffic_record(args.storage)},
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(e2e_val, 2), "unit": "MLUPS",
+                    "h2d_bytes_per_step": C.sizeof(capi.StepParams), "d2h_bytes_per_step": 24},
+            "gpu_launches": 2 * args.steps,
+            "clocks": cs,
+            "drag_fx_lattice": force[0],
+            "cd": force[0] * case.meta["drag_scale"],
+        }
+        print(json.dumps(line), flush=True)
+
+    level.close()
+    geom.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

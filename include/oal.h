@@ -1,0 +1,246 @@
+/*
+ * oal.h — C ABI of liboal, the B200 (sm_100a) lattice-Boltzmann step library.
+ *
+ * The entry points below are what a Julia `ccall` shim binds in place of the reference's
+ * solver-step and collision-operator API (OpenAeroLab, Julia + KernelAbstractions):
+ *
+ *   reference                                              replaced by
+ *   -----------------------------------------------------  ------------------------------------
+ *   get_collision_kernel(op, backend, is_l1)               oal_lookup_operator
+ *     src/collision/physics_kernels.jl:50-75
+ *   scalar kernel args `_kargs` + isbits param packs       oal_step_params / oal_default_step_params
+ *     src/collision/timestep.jl:1238-1478,
+ *     src/collision/kernel_param_packs.jl:45-76,
+ *     defaults src/io/config_loader.jl:1305-1380
+ *   build_neighbor_table(active_coords, bx,by,bz)          oal_build_box_blocks
+ *     src/geometry/domain_topology.jl:919-953
+ *   apply_analytic_sphere_obstacle!                        oal_build_sphere_obstacle
+ *     src/geometry/domain_generation.jl:111-154
+ *   BlockLevel arrays (f, f_temp, rho, vel, obstacle ...)  oal_geometry_* + oal_level_*
+ *     src/geometry/blocks.jl:14-364
+ *   stream_collide_cumulant!(f_out, f_in, ..., ndrange)    oal_stream_collide (caller-owned arrays)
+ *     src/collision/kernel_cumulant.jl:29-912              oal_level_step   (library-owned arrays)
+ *   perform_timestep_v2!(level, ...) launch + ping-pong    oal_level_step / oal_level_advance
+ *     src/collision/timestep.jl:946-1559,
+ *     src/solver/solver_control.jl:85-119
+ *   init kernels (equilibrium start)                       oal_level_init_equilibrium
+ *     src/main.jl:546-600
+ *   total mass / momentum (Float64)                        oal_level_mass_momentum
+ *     src/octree_q19/src/state.jl:614-637
+ *   momentum-exchange force (Float64 per cut link)         oal_level_get_forces
+ *     src/octree_q19/src/stream.jl:248-256,382-389
+ *
+ * Conventions
+ *   - Every function returns OAL_OK (0) or a negative oal_status; oal_last_error() gives the
+ *     text of the last failure on the calling host thread.
+ *   - Arrays named "host" are plain host memory; arrays named "device" are CUDA device pointers.
+ *   - Array layouts follow the reference (Julia, column-major, 1-based indices):
+ *       populations  f(8,8,8,n_blocks,Q)       element (x,y,z,b,k) at x + 8y + 64z + 512b + 512*n_blocks*k
+ *       density      rho(8,8,8,n_blocks)
+ *       velocity     vel(8,8,8,n_blocks,3)
+ *       obstacle     obstacle(8,8,8,n_blocks)   (Bool / uint8, nonzero = solid)
+ *       neighbours   neighbor_table(n_blocks,27) 1-based block index, 0 = none,
+ *                    direction (dx,dy,dz) at (dx+1) + 3(dy+1) + 9(dz+1)   (0-based column)
+ *       block coords active_coords (bx,by,bz) 1-based, stored as n_blocks rows of 3
+ *   - Streams are passed as `void*` (a cudaStream_t; NULL = the legacy default stream).
+ *   - A context object (geometry, level, batch, server) is not thread-safe: one host thread
+ *     drives it at a time. Different objects may be driven from different threads.
+ */
+#ifndef OAL_H
+#define OAL_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OAL_ABI_VERSION 1
+
+typedef int32_t oal_status;
+enum {
+  OAL_OK = 0,
+  OAL_E_INVALID_ARG = -1,
+  OAL_E_UNKNOWN_OPERATOR = -2, /* physics_kernels.jl:71-74 error() */
+  OAL_E_CUDA = -3,
+  OAL_E_OUT_OF_MEMORY = -4,
+  OAL_E_UNSUPPORTED = -5,
+  OAL_E_ABI_MISMATCH = -6,
+  OAL_E_ADMISSION = -7, /* request does not fit the HBM budget */
+  OAL_E_TOO_LARGE = -8,
+  OAL_E_NOT_FOUND = -9,
+  OAL_E_TIMEOUT = -10,
+  OAL_E_NO_DEVICE = -11
+};
+
+/* Collision operators (reference symbols :cumulant, :entropic, octree :hrr). */
+enum {
+  OAL_OP_CUMULANT_D3Q27 = 1,
+  OAL_OP_ENTROPIC_D3Q39 = 2,
+  OAL_OP_HRR_D3Q19 = 3
+};
+
+/* Population storage codecs. DEV = deviation (f/w_k - 1) from the lattice weight. */
+enum {
+  OAL_STORE_F32 = 0,
+  OAL_STORE_F16_DEV = 1,
+  OAL_STORE_BF16_DEV = 2,
+  OAL_STORE_F64 = 3
+};
+
+/* Cumulant limiter codes (config_loader.jl:1378-1383, timestep.jl:1158-1163). */
+enum { OAL_LIMITER_NONE = 0, OAL_LIMITER_FACTORED = 1, OAL_LIMITER_POSITIVITY = 2 };
+
+/* Treatment of solid (obstacle) cells.
+ *   FULLWAY: the reference's "simple bounce-back" inside obstacle cells
+ *            (kernel_cumulant.jl:402-417); fluid cells pull from solid cells unchanged.
+ *   HALFWAY: half-way bounce-back on every fluid->solid link with the momentum-exchange
+ *            force of the octree solver (octree_q19/src/stream.jl:229-256) on D3Q27 links;
+ *            solid cells hold the rest equilibrium. */
+enum { OAL_SOLID_FULLWAY = 0, OAL_SOLID_HALFWAY = 1 };
+
+/* Scalar step parameters: the scalars of `_kargs` (timestep.jl:1238-1478) that the
+ * D3Q27 level-1 path reads. Field meaning and units are the reference's (lattice units). */
+typedef struct oal_step_params {
+  uint32_t abi_version;          /* must be OAL_ABI_VERSION */
+  int32_t operator_id;           /* OAL_OP_* */
+  float tau;                     /* tau_molecular */
+  float tau_parent;              /* parent level tau (refined levels) */
+  float c_wale;                  /* WALE constant (config default 0.20) */
+  float nu_sgs_background;       /* background eddy viscosity (default 0) */
+  float amr_sgs_scale;           /* SGS scale of the level (timestep.jl:1127: 1.0) */
+  float omega_bulk;              /* default 1 */
+  float omega3;                  /* default 1 */
+  float omega4;                  /* default 1 */
+  int32_t adaptive_omega4;       /* default 1 */
+  float lambda_param;            /* default 1/6 */
+  int32_t limiter_type;          /* OAL_LIMITER_*, default FACTORED */
+  int32_t compressible_corr;     /* 1 = O(u^4) Hermite equilibrium, default 0 */
+  float u_inlet;                 /* inlet velocity (x) */
+  float inlet_turbulence;        /* inlet noise amplitude (fraction of u_inlet) */
+  int32_t time_step_seed;        /* noise seed (the step counter) */
+  int32_t ymin_wall_bc;          /* 1 = bounce-back ground at y_min */
+  int32_t zwall_bc;              /* 0 legacy mirror, 1 slip, 2 no-slip */
+  int32_t wall_model_active;     /* Werner-Wengle / log-law wall model */
+  float wall_model_max_distance; /* cells */
+  int32_t sponge_blend_distributions;
+  int32_t transverse_freestream;
+  float transverse_freestream_blend;
+  int32_t solid_bc;              /* OAL_SOLID_* */
+  int32_t collect_forces;        /* accumulate the FP64 momentum-exchange force this step */
+  int32_t store_post_collision;  /* also write f_post_collision */
+  float temporal_weight;         /* refined levels (reserved) */
+  int32_t use_temporal_interp;   /* refined levels (reserved) */
+  int32_t level_visc_physical;   /* refined levels (reserved) */
+  int32_t reserved[8];
+} oal_step_params;
+
+/* ---- library ---------------------------------------------------------------------------- */
+int32_t oal_abi_version(void);
+const char* oal_status_string(oal_status s);
+const char* oal_last_error(void);
+/* Number of CUDA devices visible (0 when none). */
+int32_t oal_device_count(void);
+
+/* Operator registry: "cumulant" -> OAL_OP_CUMULANT_D3Q27, "entropic" -> OAL_OP_ENTROPIC_D3Q39,
+ * "hrr"/"octree_q19" -> OAL_OP_HRR_D3Q19; anything else -> OAL_E_UNKNOWN_OPERATOR.
+ * Replaces get_collision_kernel (src/collision/physics_kernels.jl:50-75). */
+oal_status oal_lookup_operator(const char* name, int32_t* out_operator_id);
+
+/* Fill `p` with the reference's configuration defaults (src/io/config_loader.jl:1305-1380). */
+void oal_default_step_params(oal_step_params* p);
+
+/* ---- host-side domain builders ------------------------------------------------------------ */
+/* Active blocks of a full bx_max x by_max x bz_max box in the reference's sorted order
+ * (tuples sorted lexicographically, src/geometry/domain.jl:785) and their 27-entry
+ * neighbour table (domain_topology.jl:919-953). periodic_mask bit 0/1/2 wraps x/y/z.
+ * coords_out: host int32[n*3] (n = bx_max*by_max*bz_max); nbr_out: host int32[n*27],
+ * Julia column-major (n,27). */
+oal_status oal_build_box_blocks(int32_t bx_max, int32_t by_max, int32_t bz_max,
+                                int32_t periodic_mask, int32_t* coords_out, int32_t* nbr_out);
+
+/* Analytic sphere mask (domain_generation.jl:132-150): cell (lx,ly,lz) of block (bx,by,bz) is
+ * solid when its centre ((b-1)*8 + l - 0.5, cell units) lies within `radius` of `centre`.
+ * obstacle_out: host uint8[512*n_blocks]. Returns the solid count in *n_solid (may be NULL). */
+oal_status oal_build_sphere_obstacle(int32_t n_blocks, const int32_t* coords,
+                                     double cx, double cy, double cz, double radius,
+                                     uint8_t* obstacle_out, int64_t* n_solid);
+
+/* ---- geometry (device-resident topology of one level) -------------------------------------- */
+typedef struct oal_geometry_desc {
+  int32_t n_blocks;
+  int32_t nx_global, ny_global, nz_global; /* domain size in cells (boundary classification) */
+  const int32_t* active_coords;            /* host int32[n_blocks*3] */
+  const int32_t* neighbor_table;           /* host int32[n_blocks*27], Julia layout */
+  const uint8_t* obstacle;                 /* host uint8[512*n_blocks] or NULL (all fluid) */
+  const float* sponge;                     /* host float[512*n_blocks] or NULL */
+  const float* wall_dist;                  /* host float[512*n_blocks] or NULL */
+} oal_geometry_desc;
+
+typedef struct oal_geometry oal_geometry;
+oal_status oal_geometry_create(const oal_geometry_desc* desc, int32_t device, oal_geometry** out);
+void oal_geometry_destroy(oal_geometry* g);
+/* Counts: out[0]=n_blocks, out[1]=fluid cells, out[2]=solid cells, out[3]=boundary blocks,
+ * out[4]=blocks needing per-cell solid masks. */
+oal_status oal_geometry_info(const oal_geometry* g, int64_t out[5]);
+
+/* ---- caller-owned arrays: drop-in for stream_collide_cumulant! ------------------------------ */
+/* Device pointers of one level step, in the reference layout by default. Element strides let
+ * the caller pass the library's block-major layout too. */
+typedef struct oal_level_fields {
+  const void* f_in;        /* device, storage type */
+  void* f_out;             /* device, storage type */
+  void* f_post_collision;  /* device or NULL */
+  void* rho_out;           /* device float (double for OAL_STORE_F64) */
+  void* vel_out;           /* device float/double */
+  const void* vel_in;      /* device float/double (previous step's velocity) */
+  int32_t storage;         /* OAL_STORE_* */
+  int32_t reserved0;
+  int64_t f_block_stride;  /* elements between blocks   (reference: 512) */
+  int64_t f_dir_stride;    /* elements between directions (reference: 512*n_blocks) */
+  int64_t vel_comp_stride; /* elements between velocity components (reference: 512*n_blocks) */
+  double* force_out;       /* device double[3] receiving the momentum-exchange force, or NULL */
+} oal_level_fields;
+
+/* One fused pull-stream-collide step of a level-1 (no parent) D3Q27 cumulant level.
+ * Stream-ordered, asynchronous; force_out (when collect_forces) is written by a second
+ * stream-ordered reduction. Replaces stream_collide_cumulant! (kernel_cumulant.jl:29-912). */
+oal_status oal_stream_collide(const oal_geometry* g, const oal_level_fields* fields,
+                              const oal_step_params* p, void* stream);
+
+/* ---- library-owned level state ---------------------------------------------------------- */
+typedef struct oal_level oal_level;
+oal_status oal_level_create(const oal_geometry* g, int32_t operator_id, int32_t storage,
+                            oal_level** out);
+void oal_level_destroy(oal_level* L);
+/* Equilibrium start from host rho(8,8,8,nb) and vel(8,8,8,nb,3) in double precision:
+ * f_k = feq(rho,u) (physics_utils.jl:30-35), vel_in = u. */
+oal_status oal_level_init_equilibrium(oal_level* L, const double* rho_host, const double* vel_host,
+                                      int32_t compressible_corr);
+/* Overwrite the state from host arrays (reference layout, double precision). vel/rho may be NULL. */
+oal_status oal_level_set_state(oal_level* L, const double* f_host, const double* rho_host,
+                               const double* vel_host);
+/* Read the current state (after the last step) into host arrays (reference layout, double).
+ * Any pointer may be NULL. Synchronises the level's stream. */
+oal_status oal_level_get_state(oal_level* L, double* f_host, double* rho_host, double* vel_host);
+/* One step (ping-pong by parity, solver_control.jl:85-91). */
+oal_status oal_level_step(oal_level* L, const oal_step_params* p, void* stream);
+/* n steps as one captured CUDA graph (re-captured when n or p change); time_step_seed advances
+ * by one per step inside the graph. */
+oal_status oal_level_advance(oal_level* L, const oal_step_params* p, int32_t n_steps, void* stream);
+/* Momentum-exchange force of the last step that collected it (lattice units, FP64).
+ * Synchronises the level's stream. */
+oal_status oal_level_get_forces(oal_level* L, double out[3]);
+/* Non-blocking variant: enqueue the copy of the force into a host buffer (pinned for overlap). */
+oal_status oal_level_get_forces_async(oal_level* L, double* host_out3, void* stream);
+/* FP64 on-device reduction of the current state: out = {mass, px, py, pz} over fluid cells. */
+oal_status oal_level_mass_momentum(oal_level* L, double out[4]);
+/* Device pointers of the current state (for zero-copy interop): f, rho, vel. */
+oal_status oal_level_device_state(oal_level* L, void** f, void** rho, void** vel);
+/* Bytes of device memory this level holds. */
+int64_t oal_level_device_bytes(const oal_level* L);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OAL_H */

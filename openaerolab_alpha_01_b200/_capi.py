@@ -1,0 +1,193 @@
+"""ctypes bindings of liboal.so (declarations of include/oal.h).
+
+The library is loaded from the package directory; a missing library raises immediately (there is
+no CPU fallback on the product path).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "liboal.so"
+
+OAL_ABI_VERSION = 1
+
+# status codes
+OAL_OK = 0
+OAL_E_INVALID_ARG = -1
+OAL_E_UNKNOWN_OPERATOR = -2
+OAL_E_CUDA = -3
+OAL_E_OUT_OF_MEMORY = -4
+OAL_E_UNSUPPORTED = -5
+OAL_E_ABI_MISMATCH = -6
+OAL_E_ADMISSION = -7
+OAL_E_TOO_LARGE = -8
+OAL_E_NOT_FOUND = -9
+OAL_E_TIMEOUT = -10
+OAL_E_NO_DEVICE = -11
+
+OAL_OP_CUMULANT_D3Q27 = 1
+OAL_OP_ENTROPIC_D3Q39 = 2
+OAL_OP_HRR_D3Q19 = 3
+
+OAL_STORE_F32 = 0
+OAL_STORE_F16_DEV = 1
+OAL_STORE_BF16_DEV = 2
+OAL_STORE_F64 = 3
+
+OAL_LIMITER_NONE = 0
+OAL_LIMITER_FACTORED = 1
+OAL_LIMITER_POSITIVITY = 2
+
+OAL_SOLID_FULLWAY = 0
+OAL_SOLID_HALFWAY = 1
+
+STORAGE_NAMES = {"f32": OAL_STORE_F32, "f16": OAL_STORE_F16_DEV, "bf16": OAL_STORE_BF16_DEV, "f64": OAL_STORE_F64}
+
+
+class StepParams(C.Structure):
+    """oal_step_params: scalar arguments of one level step (timestep.jl:1238-1478)."""
+
+    _fields_ = [
+        ("abi_version", C.c_uint32),
+        ("operator_id", C.c_int32),
+        ("tau", C.c_float),
+        ("tau_parent", C.c_float),
+        ("c_wale", C.c_float),
+        ("nu_sgs_background", C.c_float),
+        ("amr_sgs_scale", C.c_float),
+        ("omega_bulk", C.c_float),
+        ("omega3", C.c_float),
+        ("omega4", C.c_float),
+        ("adaptive_omega4", C.c_int32),
+        ("lambda_param", C.c_float),
+        ("limiter_type", C.c_int32),
+        ("compressible_corr", C.c_int32),
+        ("u_inlet", C.c_float),
+        ("inlet_turbulence", C.c_float),
+        ("time_step_seed", C.c_int32),
+        ("ymin_wall_bc", C.c_int32),
+        ("zwall_bc", C.c_int32),
+        ("wall_model_active", C.c_int32),
+        ("wall_model_max_distance", C.c_float),
+        ("sponge_blend_distributions", C.c_int32),
+        ("transverse_freestream", C.c_int32),
+        ("transverse_freestream_blend", C.c_float),
+        ("solid_bc", C.c_int32),
+        ("collect_forces", C.c_int32),
+        ("store_post_collision", C.c_int32),
+        ("temporal_weight", C.c_float),
+        ("use_temporal_interp", C.c_int32),
+        ("level_visc_physical", C.c_int32),
+        ("reserved", C.c_int32 * 8),
+    ]
+
+
+class GeometryDesc(C.Structure):
+    _fields_ = [
+        ("n_blocks", C.c_int32),
+        ("nx_global", C.c_int32),
+        ("ny_global", C.c_int32),
+        ("nz_global", C.c_int32),
+        ("active_coords", C.POINTER(C.c_int32)),
+        ("neighbor_table", C.POINTER(C.c_int32)),
+        ("obstacle", C.POINTER(C.c_uint8)),
+        ("sponge", C.POINTER(C.c_float)),
+        ("wall_dist", C.POINTER(C.c_float)),
+    ]
+
+
+class LevelFields(C.Structure):
+    _fields_ = [
+        ("f_in", C.c_void_p),
+        ("f_out", C.c_void_p),
+        ("f_post_collision", C.c_void_p),
+        ("rho_out", C.c_void_p),
+        ("vel_out", C.c_void_p),
+        ("vel_in", C.c_void_p),
+        ("storage", C.c_int32),
+        ("reserved0", C.c_int32),
+        ("f_block_stride", C.c_int64),
+        ("f_dir_stride", C.c_int64),
+        ("vel_comp_stride", C.c_int64),
+        ("force_out", C.c_void_p),
+    ]
+
+
+class OALError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"oal status {status}: {msg}")
+        self.status = status
+
+
+# Every symbol declared in include/oal.h, with its ctypes signature.
+_SIGNATURES = {
+    "oal_abi_version": (C.c_int32, []),
+    "oal_status_string": (C.c_char_p, [C.c_int32]),
+    "oal_last_error": (C.c_char_p, []),
+    "oal_device_count": (C.c_int32, []),
+    "oal_lookup_operator": (C.c_int32, [C.c_char_p, C.POINTER(C.c_int32)]),
+    "oal_default_step_params": (None, [C.POINTER(StepParams)]),
+    "oal_build_box_blocks": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32),
+                                         C.POINTER(C.c_int32)]),
+    "oal_build_sphere_obstacle": (C.c_int32, [C.c_int32, C.POINTER(C.c_int32), C.c_double, C.c_double, C.c_double,
+                                              C.c_double, C.POINTER(C.c_uint8), C.POINTER(C.c_int64)]),
+    "oal_geometry_create": (C.c_int32, [C.POINTER(GeometryDesc), C.c_int32, C.POINTER(C.c_void_p)]),
+    "oal_geometry_destroy": (None, [C.c_void_p]),
+    "oal_geometry_info": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "oal_stream_collide": (C.c_int32, [C.c_void_p, C.POINTER(LevelFields), C.POINTER(StepParams), C.c_void_p]),
+    "oal_level_create": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
+    "oal_level_destroy": (None, [C.c_void_p]),
+    "oal_level_init_equilibrium": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]),
+    "oal_level_set_state": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "oal_level_get_state": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "oal_level_step": (C.c_int32, [C.c_void_p, C.POINTER(StepParams), C.c_void_p]),
+    "oal_level_advance": (C.c_int32, [C.c_void_p, C.POINTER(StepParams), C.c_int32, C.c_void_p]),
+    "oal_level_get_forces": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double)]),
+    "oal_level_get_forces_async": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "oal_level_mass_momentum": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double)]),
+    "oal_level_device_state": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                           C.POINTER(C.c_void_p)]),
+    "oal_level_device_bytes": (C.c_int64, [C.c_void_p]),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load liboal.so once (raises when it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m openaerolab_alpha_01_b200.build`")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in _SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        if L.oal_abi_version() != OAL_ABI_VERSION:
+            raise RuntimeError("liboal ABI version mismatch")
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != OAL_OK:
+        msg = lib().oal_last_error().decode(errors="replace")
+        raise OALError(status, msg)
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGNATURES)
+
+
+def default_params(**overrides) -> StepParams:
+    p = StepParams()
+    lib().oal_default_step_params(C.byref(p))
+    for k, v in overrides.items():
+        if not hasattr(p, k):
+            raise AttributeError(k)
+        setattr(p, k, v)
+    return p

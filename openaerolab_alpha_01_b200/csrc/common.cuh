@@ -1,0 +1,117 @@
+// common.cuh — shared device definitions of liboal: the D3Q27 velocity set as compile-time
+// constants, the population storage codecs and the argument blocks of the step kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+namespace oal {
+
+constexpr int kQ27 = 27;
+constexpr int kBS = 8;           // block edge (src/geometry/blocks.jl:14)
+constexpr int kCells = 512;      // cells per block
+
+// D3Q27 ordering of the reference (src/collision/lattice.jl:16, z outer, x inner):
+// k = (cx+1) + 3(cy+1) + 9(cz+1), 0-based here. The chimera passes rely on this order.
+__host__ __device__ constexpr int q27_cx(int k) { return k % 3 - 1; }
+__host__ __device__ constexpr int q27_cy(int k) { return (k / 3) % 3 - 1; }
+__host__ __device__ constexpr int q27_cz(int k) { return k / 9 - 1; }
+__host__ __device__ constexpr int q27_opp(int k) { return 26 - k; }
+__host__ __device__ constexpr int q27_mir_y(int k) { return (k % 3) + 3 * (2 - (k / 3) % 3) + 9 * (k / 9); }
+__host__ __device__ constexpr int q27_mir_z(int k) { return (k % 9) + 9 * (2 - k / 9); }
+__host__ __device__ constexpr int q27_d2(int k) {
+  return q27_cx(k) * q27_cx(k) + q27_cy(k) * q27_cy(k) + q27_cz(k) * q27_cz(k);
+}
+// weights 8/27, 2/27, 1/54, 1/216 by |c|^2 (lattice.jl:22-31)
+__host__ __device__ constexpr double q27_w(int k) {
+  return q27_d2(k) == 0 ? 8.0 / 27.0 : q27_d2(k) == 1 ? 2.0 / 27.0 : q27_d2(k) == 2 ? 1.0 / 54.0 : 1.0 / 216.0;
+}
+// direction index of a neighbour-block offset (ox,oy,oz) in {-1,0,1}^3 (domain_topology.jl:940)
+__host__ __device__ constexpr int nbr_dir(int ox, int oy, int oz) { return (ox + 1) + 3 * (oy + 1) + 9 * (oz + 1); }
+
+// ---- population storage codecs --------------------------------------------------------------
+// F32/F64: the population itself. F16/BF16 "deviation": d = f/w_k - 1, so that every direction
+// stores an O(Ma) number and the half-precision relative rounding applies to the deviation only.
+template <class S> struct Codec;
+template <> struct Codec<float> {
+  template <class R> __device__ static __forceinline__ R dec(float v, R, R) { return R(v); }
+  template <class R> __device__ static __forceinline__ float enc(R f, R, R) { return float(f); }
+};
+template <> struct Codec<double> {
+  template <class R> __device__ static __forceinline__ R dec(double v, R, R) { return R(v); }
+  template <class R> __device__ static __forceinline__ double enc(R f, R, R) { return double(f); }
+};
+template <> struct Codec<__half> {
+  __device__ static __forceinline__ float dec(__half v, float w, float) { return fmaf(w, __half2float(v), w); }
+  __device__ static __forceinline__ __half enc(float f, float, float inv_w) { return __float2half_rn(fmaf(f, inv_w, -1.0f)); }
+};
+template <> struct Codec<__nv_bfloat16> {
+  __device__ static __forceinline__ float dec(__nv_bfloat16 v, float w, float) { return fmaf(w, __bfloat162float(v), w); }
+  __device__ static __forceinline__ __nv_bfloat16 enc(float f, float, float inv_w) { return __float2bfloat16_rn(fmaf(f, inv_w, -1.0f)); }
+};
+
+// ---- per-case scalar parameters (resolved from oal_step_params on the host) -----------------
+enum CaseFlags : uint32_t {
+  CF_ADAPTIVE_OMEGA4 = 1u << 0,
+  CF_LIMITER_FACTORED = 1u << 1,
+  CF_LIMITER_POSITIVITY = 1u << 2,
+  CF_COMPRESSIBLE = 1u << 3,
+  CF_YMIN_WALL = 1u << 4,
+  CF_ZWALL_SLIP = 1u << 5,
+  CF_ZWALL_NOSLIP = 1u << 6,
+  CF_WALL_MODEL = 1u << 7,
+  CF_SPONGE_BLEND = 1u << 8,
+  CF_TRANSVERSE_FS = 1u << 9,
+  CF_HALFWAY = 1u << 10,
+  CF_COLLECT = 1u << 11,
+  CF_STORE_POST = 1u << 12,
+  CF_GRADIENTS = 1u << 13,  // c_wale != 0: the WALE velocity-gradient stencil is needed
+  CF_INLET_NOISE = 1u << 14
+};
+
+struct CaseParams {
+  float tau, c_wale, nu_sgs_bg, amr_sgs_scale;
+  float omega_bulk, omega3, omega4, lambda_param;
+  float u_inlet, inlet_turbulence, wall_model_max_distance, transverse_blend;
+  int32_t time_step_seed;
+  uint32_t flags;
+  int32_t nx, ny, nz;
+  int32_t pad[3];
+};
+static_assert(sizeof(CaseParams) == 80, "CaseParams layout");
+
+// per-block geometry flags
+enum BlockFlags : uint32_t {
+  BF_INTERIOR = 1u << 0,    // all 26 neighbour blocks exist: no domain-face pulls
+  BF_NEAR_SOLID = 1u << 1,  // per-cell solid masks apply (own or a pull source is solid)
+};
+
+// Kernel argument block of one launch. Element strides address either the reference layout
+// (block stride 512, direction stride 512*n_blocks) or the block-major layout of library-owned
+// state (block stride 512*Q, direction stride 512).
+struct StepArgs {
+  const void* f_in;
+  void* f_out;
+  void* f_post;
+  void* rho_out;
+  void* vel_out;
+  const void* vel_in;
+  int64_t f_bstride, f_kstride;
+  int64_t v_bstride, v_cstride;   // velocity/density: block stride, component stride
+  const int32_t* nbr;             // [nb*27], 0-based block index, -1 = none
+  const int4* binfo;              // [nb] (bx, by, bz, case) 1-based coords
+  const uint32_t* bflags;         // [nb]
+  const int32_t* mslot;           // [nb] mask slot or -1
+  const uint32_t* cmask;          // [slots*512] bit k: source of direction k is solid (13: own)
+  const float* sponge;            // [nb*512] or null
+  const float* wall_dist;         // [nb*512] or null
+  const CaseParams* cases;        // [n_cases] or null (use p0)
+  double* force_part;             // [n_ctas*3] momentum-exchange partials or null
+  int32_t n_blocks;
+  int32_t block_base;             // first block of this launch (per-case launches)
+  CaseParams p0;
+};
+
+}  // namespace oal

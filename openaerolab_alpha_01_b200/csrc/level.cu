@@ -1,0 +1,873 @@
+// level.cu — host runtime of liboal: geometry upload, library-owned level state (ping-pong
+// buffers, parity), FP64 reductions, state conversion, CUDA-graph capture of multi-step runs and
+// the C-ABI entry points of include/oal.h.
+#include <cuda_runtime.h>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <cmath>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+#include "common.cuh"
+#include "../../include/oal.h"
+
+namespace oal {
+template <class S, class R>
+cudaError_t launch_cumulant(const StepArgs& a, int n_blocks, cudaStream_t st);
+}
+using namespace oal;
+
+// ------------------------------------------------------------------------------------------------
+// error reporting
+// ------------------------------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+
+static oal_status set_error(oal_status s, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return s;
+}
+
+#define OAL_CUDA_TRY(expr)                                                                           \
+  do {                                                                                               \
+    cudaError_t _e = (expr);                                                                         \
+    if (_e != cudaSuccess)                                                                           \
+      return set_error(_e == cudaErrorMemoryAllocation ? OAL_E_OUT_OF_MEMORY : OAL_E_CUDA, "%s: %s (%s:%d)", \
+                       #expr, cudaGetErrorString(_e), __FILE__, __LINE__);                           \
+  } while (0)
+
+// ------------------------------------------------------------------------------------------------
+// device helper kernels
+// ------------------------------------------------------------------------------------------------
+namespace {
+
+// Deterministic FP64 sum of n triples (fixed strided order per thread, fixed tree).
+__global__ void k_reduce3(const double* __restrict__ part, int64_t n, double* __restrict__ out) {
+  __shared__ double s[3][256];
+  const int t = threadIdx.x;
+  double a0 = 0, a1 = 0, a2 = 0;
+  for (int64_t i = t; i < n; i += 256) {
+    a0 += part[3 * i]; a1 += part[3 * i + 1]; a2 += part[3 * i + 2];
+  }
+  s[0][t] = a0; s[1][t] = a1; s[2][t] = a2;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (t < w) { s[0][t] += s[0][t + w]; s[1][t] += s[1][t + w]; s[2][t] += s[2][t + w]; }
+    __syncthreads();
+  }
+  if (t == 0) { out[0] = s[0][0]; out[1] = s[1][0]; out[2] = s[2][0]; }
+}
+
+// Deterministic FP64 sum of n quadruples.
+__global__ void k_reduce4(const double* __restrict__ part, int64_t n, double* __restrict__ out) {
+  __shared__ double s[4][256];
+  const int t = threadIdx.x;
+  double a[4] = {0, 0, 0, 0};
+  for (int64_t i = t; i < n; i += 256)
+    for (int c = 0; c < 4; ++c) a[c] += part[4 * i + c];
+  for (int c = 0; c < 4; ++c) s[c][t] = a[c];
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (t < w)
+      for (int c = 0; c < 4; ++c) s[c][t] += s[c][t + w];
+    __syncthreads();
+  }
+  if (t == 0)
+    for (int c = 0; c < 4; ++c) out[c] = s[c][0];
+}
+
+// Per-block FP64 mass and momentum of the fluid cells (state.jl:614-637): one CTA per block.
+template <class S, class R>
+__global__ void k_mass_momentum(const S* __restrict__ f, int64_t bst, int64_t kst, const uint32_t* __restrict__ bflags,
+                                const int32_t* __restrict__ mslot, const uint32_t* __restrict__ cmask,
+                                double* __restrict__ part) {
+  __shared__ double s[4][16];
+  const int b = blockIdx.x, t = threadIdx.x;
+  double m = 0, px = 0, py = 0, pz = 0;
+  const bool ns = (bflags[b] & BF_NEAR_SOLID) != 0;
+  for (int cell = t; cell < kCells; cell += blockDim.x) {
+    if (ns && ((cmask[(int64_t)mslot[b] * kCells + cell] >> 13) & 1u)) continue;
+#pragma unroll
+    for (int k = 0; k < kQ27; ++k) {
+      const double v = (double)Codec<S>::dec(f[(int64_t)b * bst + k * kst + cell], R(q27_w(k)), R(1.0 / q27_w(k)));
+      m += v; px += v * q27_cx(k); py += v * q27_cy(k); pz += v * q27_cz(k);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    m += __shfl_down_sync(0xffffffffu, m, o);
+    px += __shfl_down_sync(0xffffffffu, px, o);
+    py += __shfl_down_sync(0xffffffffu, py, o);
+    pz += __shfl_down_sync(0xffffffffu, pz, o);
+  }
+  if ((t & 31) == 0) { s[0][t >> 5] = m; s[1][t >> 5] = px; s[2][t >> 5] = py; s[3][t >> 5] = pz; }
+  __syncthreads();
+  if (t < 4) {
+    double acc = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) acc += s[t][w];
+    part[4 * (int64_t)b + t] = acc;
+  }
+}
+
+// Equilibrium start (physics_utils.jl:30-35 / 65-95) from reference-layout double rho / vel.
+template <class S, class R>
+__global__ void k_init_feq(const double* __restrict__ rho, const double* __restrict__ vel, int64_t ncell, int comp,
+                           S* __restrict__ f, int64_t bst, int64_t kst, R* __restrict__ rho_out, R* __restrict__ vel_out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= ncell) return;
+  const int64_t b = i >> 9, cell = i & 511;
+  const R r = R(rho[i]), ux = R(vel[i]), uy = R(vel[i + ncell]), uz = R(vel[i + 2 * ncell]);
+  const R usq = ux * ux + uy * uy + uz * uz;
+#pragma unroll
+  for (int k = 0; k < kQ27; ++k) {
+    const R w = R(q27_w(k));
+    const R cu = R(q27_cx(k)) * ux + R(q27_cy(k)) * uy + R(q27_cz(k)) * uz;
+    R val = R(1) + R(3) * cu + R(4.5) * cu * cu - R(1.5) * usq;
+    if (comp) {
+      const R cu2 = cu * cu;
+      val += (R(4.5) * cu2 * cu - R(4.5) * cu * usq) + (R(3.375) * cu2 * cu2 - R(6.75) * cu2 * usq + R(1.125) * usq * usq);
+    }
+    f[b * bst + k * kst + cell] = Codec<S>::enc(r * w * val, w, R(1.0 / q27_w(k)));
+  }
+  rho_out[i] = r;
+  vel_out[i] = ux; vel_out[i + ncell] = uy; vel_out[i + 2 * ncell] = uz;
+}
+
+// Reference-layout double -> storage layout.
+template <class S, class R>
+__global__ void k_import_f(const double* __restrict__ src, int64_t ncell, S* __restrict__ f, int64_t bst, int64_t kst) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= ncell) return;
+  const int64_t b = i >> 9, cell = i & 511;
+#pragma unroll
+  for (int k = 0; k < kQ27; ++k)
+    f[b * bst + k * kst + cell] = Codec<S>::enc(R(src[i + ncell * k]), R(q27_w(k)), R(1.0 / q27_w(k)));
+}
+// Storage layout -> reference-layout double.
+template <class S, class R>
+__global__ void k_export_f(const S* __restrict__ f, int64_t bst, int64_t kst, int64_t ncell, double* __restrict__ dst) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= ncell) return;
+  const int64_t b = i >> 9, cell = i & 511;
+#pragma unroll
+  for (int k = 0; k < kQ27; ++k)
+    dst[i + ncell * k] = (double)Codec<S>::dec(f[b * bst + k * kst + cell], R(q27_w(k)), R(1.0 / q27_w(k)));
+}
+template <class R>
+__global__ void k_to_double(const R* __restrict__ src, int64_t n, double* __restrict__ dst) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = (double)src[i];
+}
+template <class R>
+__global__ void k_from_double(const double* __restrict__ src, int64_t n, R* __restrict__ dst) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = R(src[i]);
+}
+
+inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+size_t storage_bytes(int32_t storage) {
+  switch (storage) {
+    case OAL_STORE_F32: return 4;
+    case OAL_STORE_F16_DEV: return 2;
+    case OAL_STORE_BF16_DEV: return 2;
+    case OAL_STORE_F64: return 8;
+  }
+  return 0;
+}
+size_t macro_bytes(int32_t storage) { return storage == OAL_STORE_F64 ? 8 : 4; }
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------------
+// objects
+// ------------------------------------------------------------------------------------------------
+struct oal_geometry {
+  int device = 0;
+  int32_t nb = 0, nx = 0, ny = 0, nz = 0;
+  int32_t* d_nbr = nullptr;
+  int4* d_binfo = nullptr;
+  uint32_t* d_bflags = nullptr;
+  int32_t* d_mslot = nullptr;
+  uint32_t* d_cmask = nullptr;
+  float* d_sponge = nullptr;
+  float* d_wdist = nullptr;
+  double* d_force_part = nullptr;  // scratch of oal_stream_collide
+  double* d_force = nullptr;
+  int64_t n_fluid = 0, n_solid = 0, n_boundary = 0, n_slots = 0;
+};
+
+struct GraphCache {
+  cudaGraphExec_t exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  int32_t n = 0;
+  int parity = -1;
+  oal_step_params p{};
+};
+
+struct oal_level {
+  const oal_geometry* g = nullptr;
+  int32_t op = 0, storage = 0;
+  void* f[2] = {nullptr, nullptr};
+  void* vel[2] = {nullptr, nullptr};
+  void* rho = nullptr;
+  double* d_force_part = nullptr;
+  double* d_force = nullptr;
+  double* d_mm_part = nullptr;
+  double* d_mm = nullptr;
+  int parity = 0;
+  int64_t bytes = 0;
+  cudaStream_t cap = nullptr;
+  GraphCache gc;
+  bool forces_valid = false;
+};
+
+// ------------------------------------------------------------------------------------------------
+// parameter resolution
+// ------------------------------------------------------------------------------------------------
+static oal_status resolve_params(const oal_step_params* p, const oal_geometry* g, CaseParams* cp) {
+  if (!p) return set_error(OAL_E_INVALID_ARG, "null step params");
+  if (p->abi_version != OAL_ABI_VERSION)
+    return set_error(OAL_E_ABI_MISMATCH, "oal_step_params.abi_version %u != %d", p->abi_version, OAL_ABI_VERSION);
+  if (p->operator_id != OAL_OP_CUMULANT_D3Q27)
+    return set_error(OAL_E_UNSUPPORTED, "operator %d has no level-step kernel in this build", p->operator_id);
+  if (!(p->tau > 0.5f) || !std::isfinite(p->tau)) return set_error(OAL_E_INVALID_ARG, "tau must be > 0.5 (got %g)", p->tau);
+  if (p->limiter_type < 0 || p->limiter_type > 2) return set_error(OAL_E_INVALID_ARG, "limiter_type %d", p->limiter_type);
+  if (p->zwall_bc < 0 || p->zwall_bc > 2) return set_error(OAL_E_INVALID_ARG, "zwall_bc %d", p->zwall_bc);
+  if (p->solid_bc != OAL_SOLID_FULLWAY && p->solid_bc != OAL_SOLID_HALFWAY)
+    return set_error(OAL_E_INVALID_ARG, "solid_bc %d", p->solid_bc);
+  std::memset(cp, 0, sizeof *cp);
+  cp->tau = p->tau;
+  cp->c_wale = p->c_wale;
+  cp->nu_sgs_bg = p->nu_sgs_background;
+  cp->amr_sgs_scale = p->amr_sgs_scale;
+  cp->omega_bulk = p->omega_bulk;
+  cp->omega3 = p->omega3;
+  cp->omega4 = p->omega4;
+  cp->lambda_param = p->lambda_param;
+  cp->u_inlet = p->u_inlet;
+  cp->inlet_turbulence = p->inlet_turbulence;
+  cp->wall_model_max_distance = p->wall_model_max_distance;
+  cp->transverse_blend = p->transverse_freestream_blend;
+  cp->time_step_seed = p->time_step_seed;
+  cp->nx = g->nx; cp->ny = g->ny; cp->nz = g->nz;
+  uint32_t f = 0;
+  if (p->adaptive_omega4 == 1) f |= CF_ADAPTIVE_OMEGA4;
+  if (p->limiter_type == OAL_LIMITER_FACTORED) f |= CF_LIMITER_FACTORED;
+  if (p->limiter_type == OAL_LIMITER_POSITIVITY) f |= CF_LIMITER_POSITIVITY;
+  if (p->compressible_corr == 1) f |= CF_COMPRESSIBLE;
+  if (p->ymin_wall_bc == 1) f |= CF_YMIN_WALL;
+  if (p->zwall_bc == 1) f |= CF_ZWALL_SLIP;
+  if (p->zwall_bc == 2) f |= CF_ZWALL_NOSLIP;
+  if (p->wall_model_active == 1) f |= CF_WALL_MODEL;
+  if (p->sponge_blend_distributions == 1) f |= CF_SPONGE_BLEND;
+  if (p->transverse_freestream == 1) f |= CF_TRANSVERSE_FS;
+  if (p->solid_bc == OAL_SOLID_HALFWAY) f |= CF_HALFWAY;
+  if (p->collect_forces) f |= CF_COLLECT;
+  if (p->store_post_collision == 1) f |= CF_STORE_POST;
+  if (p->c_wale != 0.0f) f |= CF_GRADIENTS;
+  if (p->inlet_turbulence > 0.0f) f |= CF_INLET_NOISE;
+  cp->flags = f;
+  return OAL_OK;
+}
+
+static cudaError_t launch_by_storage(int32_t storage, const StepArgs& a, int nb, cudaStream_t st) {
+  switch (storage) {
+    case OAL_STORE_F32: return launch_cumulant<float, float>(a, nb, st);
+    case OAL_STORE_F16_DEV: return launch_cumulant<__half, float>(a, nb, st);
+    case OAL_STORE_BF16_DEV: return launch_cumulant<__nv_bfloat16, float>(a, nb, st);
+    case OAL_STORE_F64: return launch_cumulant<double, double>(a, nb, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+static void fill_geometry_args(const oal_geometry* g, StepArgs* a) {
+  a->nbr = g->d_nbr;
+  a->binfo = g->d_binfo;
+  a->bflags = g->d_bflags;
+  a->mslot = g->d_mslot;
+  a->cmask = g->d_cmask;
+  a->sponge = g->d_sponge;
+  a->wall_dist = g->d_wdist;
+  a->n_blocks = g->nb;
+  a->block_base = 0;
+  a->cases = nullptr;
+}
+
+static void level_layout(const oal_level* L, int64_t* bst, int64_t* kst) {
+  *bst = 27 * 512;  // block-major: f[b][k][cell]
+  *kst = 512;
+}
+
+template <class S, class R>
+static cudaError_t init_feq_t(oal_level* L, const double* d_rho, const double* d_vel, int comp) {
+  int64_t bst, kst;
+  level_layout(L, &bst, &kst);
+  const int64_t ncell = (int64_t)L->g->nb * 512;
+  k_init_feq<S, R><<<nblk(ncell, 256), 256>>>(d_rho, d_vel, ncell, comp, static_cast<S*>(L->f[0]), bst, kst,
+                                              static_cast<R*>(L->rho), static_cast<R*>(L->vel[0]));
+  return cudaGetLastError();
+}
+
+template <class S, class R>
+static cudaError_t import_t(oal_level* L, const double* d_f, const double* d_rho, const double* d_vel) {
+  int64_t bst, kst;
+  level_layout(L, &bst, &kst);
+  const int64_t ncell = (int64_t)L->g->nb * 512;
+  k_import_f<S, R><<<nblk(ncell, 256), 256>>>(d_f, ncell, static_cast<S*>(L->f[L->parity]), bst, kst);
+  if (d_rho) k_from_double<R><<<nblk(ncell, 256), 256>>>(d_rho, ncell, static_cast<R*>(L->rho));
+  if (d_vel) k_from_double<R><<<nblk(3 * ncell, 256), 256>>>(d_vel, 3 * ncell, static_cast<R*>(L->vel[L->parity]));
+  return cudaGetLastError();
+}
+template <class S, class R>
+static cudaError_t export_t(oal_level* L, double* d_f, double* d_rho, double* d_vel) {
+  int64_t bst, kst;
+  level_layout(L, &bst, &kst);
+  const int64_t ncell = (int64_t)L->g->nb * 512;
+  if (d_f) k_export_f<S, R><<<nblk(ncell, 256), 256>>>(static_cast<const S*>(L->f[L->parity]), bst, kst, ncell, d_f);
+  if (d_rho) k_to_double<R><<<nblk(ncell, 256), 256>>>(static_cast<const R*>(L->rho), ncell, d_rho);
+  if (d_vel) k_to_double<R><<<nblk(3 * ncell, 256), 256>>>(static_cast<const R*>(L->vel[L->parity]), 3 * ncell, d_vel);
+  return cudaGetLastError();
+}
+
+template <class S, class R>
+static cudaError_t mm_t(oal_level* L) {
+  int64_t bst, kst;
+  level_layout(L, &bst, &kst);
+  const oal_geometry* g = L->g;
+  k_mass_momentum<S, R><<<g->nb, 128>>>(static_cast<const S*>(L->f[L->parity]), bst, kst, g->d_bflags, g->d_mslot,
+                                        g->d_cmask, L->d_mm_part);
+  k_reduce4<<<1, 256>>>(L->d_mm_part, g->nb, L->d_mm);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------------------------
+extern "C" {
+
+int32_t oal_abi_version(void) { return OAL_ABI_VERSION; }
+
+const char* oal_status_string(oal_status s) {
+  switch (s) {
+    case OAL_OK: return "ok";
+    case OAL_E_INVALID_ARG: return "invalid argument";
+    case OAL_E_UNKNOWN_OPERATOR: return "unknown collision operator";
+    case OAL_E_CUDA: return "CUDA error";
+    case OAL_E_OUT_OF_MEMORY: return "out of device memory";
+    case OAL_E_UNSUPPORTED: return "unsupported";
+    case OAL_E_ABI_MISMATCH: return "ABI version mismatch";
+    case OAL_E_ADMISSION: return "request exceeds the memory budget";
+    case OAL_E_TOO_LARGE: return "size exceeds the supported maximum";
+    case OAL_E_NOT_FOUND: return "not found";
+    case OAL_E_TIMEOUT: return "timeout";
+    case OAL_E_NO_DEVICE: return "no CUDA device";
+  }
+  return "unknown status";
+}
+
+const char* oal_last_error(void) { return g_last_error.c_str(); }
+
+int32_t oal_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) { cudaGetLastError(); return 0; }
+  return n;
+}
+
+oal_status oal_lookup_operator(const char* name, int32_t* out) {
+  if (!name || !out) return set_error(OAL_E_INVALID_ARG, "null argument");
+  std::string s(name);
+  if (!s.empty() && s[0] == ':') s = s.substr(1);
+  if (s == "cumulant") { *out = OAL_OP_CUMULANT_D3Q27; return OAL_OK; }
+  if (s == "entropic") { *out = OAL_OP_ENTROPIC_D3Q39; return OAL_OK; }
+  if (s == "hrr" || s == "octree_q19") { *out = OAL_OP_HRR_D3Q19; return OAL_OK; }
+  return set_error(OAL_E_UNKNOWN_OPERATOR,
+                   "Unknown or retired operator: :%s. Valid options: :cumulant (D3Q27), :entropic (D3Q39), :hrr (D3Q19 octree).",
+                   s.c_str());
+}
+
+void oal_default_step_params(oal_step_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof *p);
+  p->abi_version = OAL_ABI_VERSION;
+  p->operator_id = OAL_OP_CUMULANT_D3Q27;
+  p->tau = 0.6f;
+  p->tau_parent = 0.6f;
+  p->c_wale = 0.20f;              // config_loader.jl:1305
+  p->nu_sgs_background = 0.0f;    // :1310
+  p->amr_sgs_scale = 1.0f;        // timestep.jl:1127
+  p->omega_bulk = 1.0f;           // :1373
+  p->omega3 = 1.0f;               // :1374
+  p->omega4 = 1.0f;               // :1375
+  p->adaptive_omega4 = 1;         // :1376
+  p->lambda_param = 1.0f / 6.0f;  // :1377
+  p->limiter_type = OAL_LIMITER_FACTORED;  // :1379
+  p->compressible_corr = 0;
+  p->u_inlet = 0.05f;
+  p->inlet_turbulence = 0.0f;
+  p->time_step_seed = 0;
+  p->ymin_wall_bc = 0;
+  p->zwall_bc = 0;
+  p->wall_model_active = 0;       // :1870
+  p->wall_model_max_distance = 10.0f;  // :1873
+  p->sponge_blend_distributions = 0;
+  p->transverse_freestream = 0;
+  p->transverse_freestream_blend = 1.0f;
+  p->solid_bc = OAL_SOLID_FULLWAY;
+  p->collect_forces = 0;
+  p->store_post_collision = 0;
+  p->temporal_weight = 1.0f;
+  p->use_temporal_interp = 0;
+  p->level_visc_physical = 0;
+}
+
+oal_status oal_build_box_blocks(int32_t bxm, int32_t bym, int32_t bzm, int32_t periodic_mask, int32_t* coords,
+                                int32_t* nbr) {
+  if (bxm <= 0 || bym <= 0 || bzm <= 0 || !coords || !nbr) return set_error(OAL_E_INVALID_ARG, "bad box");
+  const int64_t n = (int64_t)bxm * bym * bzm;
+  // sorted tuples (bx, by, bz): bx most significant (domain.jl:785)
+  auto index_of = [&](int bx, int by, int bz) -> int64_t { return ((int64_t)(bx - 1) * bym + (by - 1)) * bzm + (bz - 1); };
+  for (int bx = 1; bx <= bxm; ++bx)
+    for (int by = 1; by <= bym; ++by)
+      for (int bz = 1; bz <= bzm; ++bz) {
+        const int64_t i = index_of(bx, by, bz);
+        coords[3 * i] = bx; coords[3 * i + 1] = by; coords[3 * i + 2] = bz;
+      }
+  const bool px = periodic_mask & 1, py = periodic_mask & 2, pz = periodic_mask & 4;
+  for (int64_t i = 0; i < n; ++i) {
+    const int bx = coords[3 * i], by = coords[3 * i + 1], bz = coords[3 * i + 2];
+    for (int d = 0; d < 27; ++d) {
+      int nx = bx + d % 3 - 1, ny = by + (d / 3) % 3 - 1, nz = bz + d / 9 - 1;
+      if (px) nx = nx < 1 ? bxm : (nx > bxm ? 1 : nx);
+      if (py) ny = ny < 1 ? bym : (ny > bym ? 1 : ny);
+      if (pz) nz = nz < 1 ? bzm : (nz > bzm ? 1 : nz);
+      const bool in = nx >= 1 && nx <= bxm && ny >= 1 && ny <= bym && nz >= 1 && nz <= bzm;
+      nbr[i + n * d] = in ? (int32_t)(index_of(nx, ny, nz) + 1) : 0;
+    }
+  }
+  return OAL_OK;
+}
+
+oal_status oal_build_sphere_obstacle(int32_t nb, const int32_t* coords, double cx, double cy, double cz, double radius,
+                                     uint8_t* obst, int64_t* n_solid) {
+  if (nb <= 0 || !coords || !obst) return set_error(OAL_E_INVALID_ARG, "bad sphere arguments");
+  const double r2 = radius * radius;
+  int64_t count = 0;
+  for (int64_t b = 0; b < nb; ++b)
+    for (int lz = 1; lz <= 8; ++lz)
+      for (int ly = 1; ly <= 8; ++ly)
+        for (int lx = 1; lx <= 8; ++lx) {
+          const double px = (coords[3 * b] - 1) * 8 + lx - 0.5;
+          const double py = (coords[3 * b + 1] - 1) * 8 + ly - 0.5;
+          const double pz = (coords[3 * b + 2] - 1) * 8 + lz - 0.5;
+          const double d = (px - cx) * (px - cx) + (py - cy) * (py - cy) + (pz - cz) * (pz - cz);
+          const uint8_t s = d <= r2;
+          obst[(lx - 1) + 8 * (ly - 1) + 64 * (lz - 1) + 512 * b] = s;
+          count += s;
+        }
+  if (n_solid) *n_solid = count;
+  return OAL_OK;
+}
+
+oal_status oal_geometry_create(const oal_geometry_desc* d, int32_t device, oal_geometry** out) {
+  if (!d || !out) return set_error(OAL_E_INVALID_ARG, "null argument");
+  *out = nullptr;
+  if (d->n_blocks <= 0 || !d->active_coords || !d->neighbor_table)
+    return set_error(OAL_E_INVALID_ARG, "geometry needs n_blocks > 0, active_coords and neighbor_table");
+  if (d->nx_global <= 0 || d->ny_global <= 0 || d->nz_global <= 0)
+    return set_error(OAL_E_INVALID_ARG, "global sizes must be positive");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return set_error(OAL_E_NO_DEVICE, "no CUDA device visible");
+  }
+  if (device < 0 || device >= ndev) return set_error(OAL_E_INVALID_ARG, "device %d out of range", device);
+  OAL_CUDA_TRY(cudaSetDevice(device));
+
+  const int64_t nb = d->n_blocks;
+  std::vector<int32_t> nbr0((size_t)nb * 27);
+  std::vector<int4> binfo((size_t)nb);
+  std::vector<uint32_t> bflags((size_t)nb, 0);
+  for (int64_t b = 0; b < nb; ++b) {
+    bool interior = true;
+    for (int dir = 0; dir < 27; ++dir) {
+      const int32_t v = d->neighbor_table[b + nb * dir];
+      if (v < 0 || v > nb) return set_error(OAL_E_INVALID_ARG, "neighbor_table[%lld,%d] = %d out of range", (long long)b, dir, v);
+      nbr0[(size_t)b * 27 + dir] = v - 1;
+      if (v == 0) interior = false;
+    }
+    if (nbr0[(size_t)b * 27 + 13] != b)
+      return set_error(OAL_E_INVALID_ARG, "neighbor_table[%lld, self] must be the block itself", (long long)b);
+    binfo[(size_t)b] = make_int4(d->active_coords[3 * b], d->active_coords[3 * b + 1], d->active_coords[3 * b + 2], 0);
+    if (interior) bflags[(size_t)b] |= BF_INTERIOR;
+  }
+  auto* g = new oal_geometry();
+  g->device = device;
+  g->nb = d->n_blocks; g->nx = d->nx_global; g->ny = d->ny_global; g->nz = d->nz_global;
+
+  // per-cell solid masks: bit k = source cell x - c_k is solid, bit 13 = own cell solid
+  std::vector<int32_t> mslot((size_t)nb, -1);
+  std::vector<uint32_t> cmask;
+  int64_t n_solid = 0;
+  if (d->obstacle) {
+    std::vector<uint32_t> m(512);
+    for (int64_t b = 0; b < nb; ++b) {
+      bool any = false;
+      for (int cell = 0; cell < 512; ++cell) {
+        const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
+        uint32_t bits = 0;
+        for (int k = 0; k < 27; ++k) {
+          const int sx = x - q27_cx(k), sy = y - q27_cy(k), sz = z - q27_cz(k);
+          const int dir = nbr_dir(sx >> 3, sy >> 3, sz >> 3);
+          const int32_t sb = nbr0[(size_t)b * 27 + dir];
+          if (sb < 0) continue;
+          const int sc = (sx & 7) | ((sy & 7) << 3) | ((sz & 7) << 6);
+          if (d->obstacle[(int64_t)sb * 512 + sc]) bits |= 1u << k;
+        }
+        m[cell] = bits;
+        if (bits) any = true;
+        if (bits & (1u << 13)) ++n_solid;
+      }
+      if (any) {
+        mslot[(size_t)b] = (int32_t)(cmask.size() / 512);
+        cmask.insert(cmask.end(), m.begin(), m.end());
+        bflags[(size_t)b] |= BF_NEAR_SOLID;
+      }
+    }
+  }
+  g->n_solid = n_solid;
+  g->n_fluid = nb * 512 - n_solid;
+  g->n_slots = (int64_t)cmask.size() / 512;
+  for (int64_t b = 0; b < nb; ++b)
+    if (!(bflags[(size_t)b] & BF_INTERIOR)) ++g->n_boundary;
+
+  auto fail = [&](oal_status s) { oal_geometry_destroy(g); return s; };
+#define GTRY(expr)                                                                         \
+  do {                                                                                     \
+    cudaError_t _e = (expr);                                                               \
+    if (_e != cudaSuccess)                                                                 \
+      return fail(set_error(_e == cudaErrorMemoryAllocation ? OAL_E_OUT_OF_MEMORY : OAL_E_CUDA, "%s: %s", #expr, \
+                            cudaGetErrorString(_e)));                                      \
+  } while (0)
+  GTRY(cudaMalloc(&g->d_nbr, nbr0.size() * sizeof(int32_t)));
+  GTRY(cudaMemcpy(g->d_nbr, nbr0.data(), nbr0.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  GTRY(cudaMalloc(&g->d_binfo, binfo.size() * sizeof(int4)));
+  GTRY(cudaMemcpy(g->d_binfo, binfo.data(), binfo.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  GTRY(cudaMalloc(&g->d_bflags, bflags.size() * sizeof(uint32_t)));
+  GTRY(cudaMemcpy(g->d_bflags, bflags.data(), bflags.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  GTRY(cudaMalloc(&g->d_mslot, mslot.size() * sizeof(int32_t)));
+  GTRY(cudaMemcpy(g->d_mslot, mslot.data(), mslot.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  if (!cmask.empty()) {
+    GTRY(cudaMalloc(&g->d_cmask, cmask.size() * sizeof(uint32_t)));
+    GTRY(cudaMemcpy(g->d_cmask, cmask.data(), cmask.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  }
+  if (d->sponge) {
+    GTRY(cudaMalloc(&g->d_sponge, (size_t)nb * 512 * sizeof(float)));
+    GTRY(cudaMemcpy(g->d_sponge, d->sponge, (size_t)nb * 512 * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  if (d->wall_dist) {
+    GTRY(cudaMalloc(&g->d_wdist, (size_t)nb * 512 * sizeof(float)));
+    GTRY(cudaMemcpy(g->d_wdist, d->wall_dist, (size_t)nb * 512 * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  GTRY(cudaMalloc(&g->d_force_part, (size_t)nb * 4 * 3 * sizeof(double)));
+  GTRY(cudaMalloc(&g->d_force, 3 * sizeof(double)));
+  GTRY(cudaMemset(g->d_force, 0, 3 * sizeof(double)));
+#undef GTRY
+  *out = g;
+  return OAL_OK;
+}
+
+void oal_geometry_destroy(oal_geometry* g) {
+  if (!g) return;
+  cudaSetDevice(g->device);
+  cudaFree(g->d_nbr); cudaFree(g->d_binfo); cudaFree(g->d_bflags); cudaFree(g->d_mslot);
+  cudaFree(g->d_cmask); cudaFree(g->d_sponge); cudaFree(g->d_wdist);
+  cudaFree(g->d_force_part); cudaFree(g->d_force);
+  delete g;
+}
+
+oal_status oal_geometry_info(const oal_geometry* g, int64_t out[5]) {
+  if (!g || !out) return set_error(OAL_E_INVALID_ARG, "null argument");
+  out[0] = g->nb; out[1] = g->n_fluid; out[2] = g->n_solid; out[3] = g->n_boundary; out[4] = g->n_slots;
+  return OAL_OK;
+}
+
+oal_status oal_stream_collide(const oal_geometry* g, const oal_level_fields* fl, const oal_step_params* p, void* stream) {
+  if (!g || !fl) return set_error(OAL_E_INVALID_ARG, "null argument");
+  CaseParams cp;
+  oal_status s = resolve_params(p, g, &cp);
+  if (s != OAL_OK) return s;
+  if (!fl->f_in || !fl->f_out || !fl->rho_out || !fl->vel_out || !fl->vel_in)
+    return set_error(OAL_E_INVALID_ARG, "f_in, f_out, rho_out, vel_out and vel_in are required");
+  if (fl->f_in == fl->f_out) return set_error(OAL_E_INVALID_ARG, "f_in and f_out must differ (pull scheme)");
+  if (fl->storage < OAL_STORE_F32 || fl->storage > OAL_STORE_F64) return set_error(OAL_E_INVALID_ARG, "storage %d", fl->storage);
+  if (fl->f_block_stride < 512 || fl->f_dir_stride < 512) return set_error(OAL_E_INVALID_ARG, "bad population strides");
+  OAL_CUDA_TRY(cudaSetDevice(g->device));
+  StepArgs a{};
+  fill_geometry_args(g, &a);
+  a.f_in = fl->f_in; a.f_out = fl->f_out; a.f_post = fl->f_post_collision;
+  a.rho_out = fl->rho_out; a.vel_out = fl->vel_out; a.vel_in = fl->vel_in;
+  a.f_bstride = fl->f_block_stride; a.f_kstride = fl->f_dir_stride;
+  a.v_bstride = 512; a.v_cstride = fl->vel_comp_stride > 0 ? fl->vel_comp_stride : 512 * (int64_t)g->nb;
+  a.force_part = g->d_force_part;
+  a.p0 = cp;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  OAL_CUDA_TRY(launch_by_storage(fl->storage, a, g->nb, st));
+  if ((cp.flags & CF_COLLECT) && fl->force_out) {
+    k_reduce3<<<1, 256, 0, st>>>(g->d_force_part, (int64_t)g->nb * 4, fl->force_out);
+    OAL_CUDA_TRY(cudaGetLastError());
+  }
+  return OAL_OK;
+}
+
+// ---- levels ----
+oal_status oal_level_create(const oal_geometry* g, int32_t op, int32_t storage, oal_level** out) {
+  if (!g || !out) return set_error(OAL_E_INVALID_ARG, "null argument");
+  *out = nullptr;
+  if (op != OAL_OP_CUMULANT_D3Q27) return set_error(OAL_E_UNSUPPORTED, "operator %d has no level state in this build", op);
+  if (storage < OAL_STORE_F32 || storage > OAL_STORE_F64) return set_error(OAL_E_INVALID_ARG, "storage %d", storage);
+  OAL_CUDA_TRY(cudaSetDevice(g->device));
+  auto* L = new oal_level();
+  L->g = g; L->op = op; L->storage = storage;
+  const int64_t ncell = (int64_t)g->nb * 512;
+  const size_t fbytes = (size_t)ncell * 27 * storage_bytes(storage);
+  const size_t mb = macro_bytes(storage);
+  auto fail = [&](cudaError_t e) {
+    oal_level_destroy(L);
+    return set_error(e == cudaErrorMemoryAllocation ? OAL_E_OUT_OF_MEMORY : OAL_E_CUDA, "level allocation: %s",
+                     cudaGetErrorString(e));
+  };
+  cudaError_t e;
+  for (int i = 0; i < 2; ++i) {
+    if ((e = cudaMalloc(&L->f[i], fbytes)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&L->vel[i], (size_t)ncell * 3 * mb)) != cudaSuccess) return fail(e);
+    if ((e = cudaMemset(L->vel[i], 0, (size_t)ncell * 3 * mb)) != cudaSuccess) return fail(e);
+  }
+  if ((e = cudaMalloc(&L->rho, (size_t)ncell * mb)) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&L->d_force_part, (size_t)g->nb * 4 * 3 * sizeof(double))) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&L->d_force, 3 * sizeof(double))) != cudaSuccess) return fail(e);
+  if ((e = cudaMemset(L->d_force, 0, 3 * sizeof(double))) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&L->d_mm_part, (size_t)g->nb * 4 * sizeof(double))) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&L->d_mm, 4 * sizeof(double))) != cudaSuccess) return fail(e);
+  if ((e = cudaStreamCreateWithFlags(&L->cap, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+  L->bytes = (int64_t)(2 * fbytes + ncell * 7 * mb + g->nb * 16 * 8 + 56);
+  *out = L;
+  return OAL_OK;
+}
+
+static void release_graph(oal_level* L) {
+  if (L->gc.exec) cudaGraphExecDestroy(L->gc.exec);
+  if (L->gc.graph) cudaGraphDestroy(L->gc.graph);
+  L->gc = GraphCache{};
+}
+
+void oal_level_destroy(oal_level* L) {
+  if (!L) return;
+  cudaSetDevice(L->g->device);
+  release_graph(L);
+  for (int i = 0; i < 2; ++i) { cudaFree(L->f[i]); cudaFree(L->vel[i]); }
+  cudaFree(L->rho); cudaFree(L->d_force_part); cudaFree(L->d_force); cudaFree(L->d_mm_part); cudaFree(L->d_mm);
+  if (L->cap) cudaStreamDestroy(L->cap);
+  delete L;
+}
+
+oal_status oal_level_init_equilibrium(oal_level* L, const double* rho, const double* vel, int32_t comp) {
+  if (!L || !rho || !vel) return set_error(OAL_E_INVALID_ARG, "null argument");
+  OAL_CUDA_TRY(cudaSetDevice(L->g->device));
+  const int64_t ncell = (int64_t)L->g->nb * 512;
+  double *d_rho = nullptr, *d_vel = nullptr;
+  OAL_CUDA_TRY(cudaMalloc(&d_rho, ncell * sizeof(double)));
+  cudaError_t e = cudaMalloc(&d_vel, 3 * ncell * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpy(d_rho, rho, ncell * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_vel, vel, 3 * ncell * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    switch (L->storage) {
+      case OAL_STORE_F32: e = init_feq_t<float, float>(L, d_rho, d_vel, comp); break;
+      case OAL_STORE_F16_DEV: e = init_feq_t<__half, float>(L, d_rho, d_vel, comp); break;
+      case OAL_STORE_BF16_DEV: e = init_feq_t<__nv_bfloat16, float>(L, d_rho, d_vel, comp); break;
+      case OAL_STORE_F64: e = init_feq_t<double, double>(L, d_rho, d_vel, comp); break;
+    }
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  cudaFree(d_rho); cudaFree(d_vel);
+  if (e != cudaSuccess) return set_error(OAL_E_CUDA, "init_equilibrium: %s", cudaGetErrorString(e));
+  L->parity = 0;
+  L->forces_valid = false;
+  release_graph(L);
+  return OAL_OK;
+}
+
+oal_status oal_level_set_state(oal_level* L, const double* f, const double* rho, const double* vel) {
+  if (!L || !f) return set_error(OAL_E_INVALID_ARG, "null argument");
+  OAL_CUDA_TRY(cudaSetDevice(L->g->device));
+  const int64_t ncell = (int64_t)L->g->nb * 512;
+  double *d_f = nullptr, *d_r = nullptr, *d_v = nullptr;
+  cudaError_t e = cudaMalloc(&d_f, 27 * ncell * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpy(d_f, f, 27 * ncell * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && rho) {
+    e = cudaMalloc(&d_r, ncell * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpy(d_r, rho, ncell * sizeof(double), cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess && vel) {
+    e = cudaMalloc(&d_v, 3 * ncell * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpy(d_v, vel, 3 * ncell * sizeof(double), cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess) {
+    switch (L->storage) {
+      case OAL_STORE_F32: e = import_t<float, float>(L, d_f, d_r, d_v); break;
+      case OAL_STORE_F16_DEV: e = import_t<__half, float>(L, d_f, d_r, d_v); break;
+      case OAL_STORE_BF16_DEV: e = import_t<__nv_bfloat16, float>(L, d_f, d_r, d_v); break;
+      case OAL_STORE_F64: e = import_t<double, double>(L, d_f, d_r, d_v); break;
+    }
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  cudaFree(d_f); cudaFree(d_r); cudaFree(d_v);
+  if (e != cudaSuccess) return set_error(OAL_E_CUDA, "set_state: %s", cudaGetErrorString(e));
+  release_graph(L);
+  return OAL_OK;
+}
+
+oal_status oal_level_get_state(oal_level* L, double* f, double* rho, double* vel) {
+  if (!L) return set_error(OAL_E_INVALID_ARG, "null argument");
+  OAL_CUDA_TRY(cudaSetDevice(L->g->device));
+  OAL_CUDA_TRY(cudaDeviceSynchronize());
+  const int64_t ncell = (int64_t)L->g->nb * 512;
+  double *d_f = nullptr, *d_r = nullptr, *d_v = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (f) e = cudaMalloc(&d_f, 27 * ncell * sizeof(double));
+  if (e == cudaSuccess && rho) e = cudaMalloc(&d_r, ncell * sizeof(double));
+  if (e == cudaSuccess && vel) e = cudaMalloc(&d_v, 3 * ncell * sizeof(double));
+  if (e == cudaSuccess) {
+    switch (L->storage) {
+      case OAL_STORE_F32: e = export_t<float, float>(L, d_f, d_r, d_v); break;
+      case OAL_STORE_F16_DEV: e = export_t<__half, float>(L, d_f, d_r, d_v); break;
+      case OAL_STORE_BF16_DEV: e = export_t<__nv_bfloat16, float>(L, d_f, d_r, d_v); break;
+      case OAL_STORE_F64: e = export_t<double, double>(L, d_f, d_r, d_v); break;
+    }
+  }
+  if (e == cudaSuccess && f) e = cudaMemcpy(f, d_f, 27 * ncell * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && rho) e = cudaMemcpy(rho, d_r, ncell * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && vel) e = cudaMemcpy(vel, d_v, 3 * ncell * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(d_f); cudaFree(d_r); cudaFree(d_v);
+  if (e != cudaSuccess) return set_error(OAL_E_CUDA, "get_state: %s", cudaGetErrorString(e));
+  return OAL_OK;
+}
+
+// Enqueue one step of L on st (no host synchronisation).
+static oal_status enqueue_step(oal_level* L, const CaseParams& cp, cudaStream_t st) {
+  const oal_geometry* g = L->g;
+  StepArgs a{};
+  fill_geometry_args(g, &a);
+  int64_t bst, kst;
+  level_layout(L, &bst, &kst);
+  const int p = L->parity;
+  a.f_in = L->f[p]; a.f_out = L->f[p ^ 1]; a.f_post = nullptr;
+  a.rho_out = L->rho; a.vel_out = L->vel[p ^ 1]; a.vel_in = L->vel[p];
+  a.f_bstride = bst; a.f_kstride = kst;
+  a.v_bstride = 512; a.v_cstride = 512 * (int64_t)g->nb;
+  a.force_part = L->d_force_part;
+  a.p0 = cp;
+  OAL_CUDA_TRY(launch_by_storage(L->storage, a, g->nb, st));
+  if (cp.flags & CF_COLLECT) {
+    k_reduce3<<<1, 256, 0, st>>>(L->d_force_part, (int64_t)g->nb * 4, L->d_force);
+    OAL_CUDA_TRY(cudaGetLastError());
+    L->forces_valid = true;
+  }
+  L->parity ^= 1;
+  return OAL_OK;
+}
+
+oal_status oal_level_step(oal_level* L, const oal_step_params* p, void* stream) {
+  if (!L) return set_error(OAL_E_INVALID_ARG, "null level");
+  CaseParams cp;
+  oal_status s = resolve_params(p, L->g, &cp);
+  if (s != OAL_OK) return s;
+  if (cp.flags & CF_STORE_POST) return set_error(OAL_E_UNSUPPORTED, "store_post_collision needs caller-owned arrays (oal_stream_collide)");
+  OAL_CUDA_TRY(cudaSetDevice(L->g->device));
+  return enqueue_step(L, cp, static_cast<cudaStream_t>(stream));
+}
+
+oal_status oal_level_advance(oal_level* L, const oal_step_params* p, int32_t n, void* stream) {
+  if (!L) return set_error(OAL_E_INVALID_ARG, "null level");
+  if (n <= 0) return set_error(OAL_E_INVALID_ARG, "n_steps must be positive");
+  CaseParams cp;
+  oal_status s = resolve_params(p, L->g, &cp);
+  if (s != OAL_OK) return s;
+  if (cp.flags & CF_STORE_POST) return set_error(OAL_E_UNSUPPORTED, "store_post_collision needs caller-owned arrays");
+  OAL_CUDA_TRY(cudaSetDevice(L->g->device));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  oal_step_params key = *p;
+  if (!(cp.flags & CF_INLET_NOISE)) key.time_step_seed = 0;  // the seed only matters with inlet noise
+  const bool hit = L->gc.exec && L->gc.n == n && L->gc.parity == L->parity && std::memcmp(&L->gc.p, &key, sizeof key) == 0;
+  if (!hit) {
+    release_graph(L);
+    const int start_parity = L->parity;
+    OAL_CUDA_TRY(cudaStreamBeginCapture(L->cap, cudaStreamCaptureModeThreadLocal));
+    oal_status es = OAL_OK;
+    for (int i = 0; i < n && es == OAL_OK; ++i) {
+      CaseParams ci = cp;
+      ci.time_step_seed = p->time_step_seed + i;
+      es = enqueue_step(L, ci, L->cap);
+    }
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(L->cap, &graph);
+    L->parity = start_parity;
+    if (es != OAL_OK) { if (graph) cudaGraphDestroy(graph); return es; }
+    if (e != cudaSuccess) return set_error(OAL_E_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) { cudaGraphDestroy(graph); return set_error(OAL_E_CUDA, "graph instantiate: %s", cudaGetErrorString(e)); }
+    L->gc.exec = exec; L->gc.graph = graph; L->gc.n = n; L->gc.parity = start_parity; L->gc.p = key;
+  }
+  OAL_CUDA_TRY(cudaGraphLaunch(L->gc.exec, st));
+  if (n & 1) L->parity ^= 1;
+  if (cp.flags & CF_COLLECT) L->forces_valid = true;
+  return OAL_OK;
+}
+
+oal_status oal_level_get_forces(oal_level* L, double out[3]) {
+  if (!L || !out) return set_error(OAL_E_INVALID_ARG, "null argument");
+  OAL_CUDA_TRY(cudaSetDevice(L->g->device));
+  if (!L->forces_valid) { out[0] = out[1] = out[2] = 0.0; return OAL_OK; }
+  OAL_CUDA_TRY(cudaMemcpy(out, L->d_force, 3 * sizeof(double), cudaMemcpyDeviceToHost));
+  return OAL_OK;
+}
+
+oal_status oal_level_get_forces_async(oal_level* L, double* host_out3, void* stream) {
+  if (!L || !host_out3) return set_error(OAL_E_INVALID_ARG, "null argument");
+  OAL_CUDA_TRY(cudaMemcpyAsync(host_out3, L->d_force, 3 * sizeof(double), cudaMemcpyDeviceToHost,
+                               static_cast<cudaStream_t>(stream)));
+  return OAL_OK;
+}
+
+oal_status oal_level_mass_momentum(oal_level* L, double out[4]) {
+  if (!L || !out) return set_error(OAL_E_INVALID_ARG, "null argument");
+  OAL_CUDA_TRY(cudaSetDevice(L->g->device));
+  cudaError_t e = cudaSuccess;
+  switch (L->storage) {
+    case OAL_STORE_F32: e = mm_t<float, float>(L); break;
+    case OAL_STORE_F16_DEV: e = mm_t<__half, float>(L); break;
+    case OAL_STORE_BF16_DEV: e = mm_t<__nv_bfloat16, float>(L); break;
+    case OAL_STORE_F64: e = mm_t<double, double>(L); break;
+  }
+  if (e != cudaSuccess) return set_error(OAL_E_CUDA, "mass_momentum: %s", cudaGetErrorString(e));
+  OAL_CUDA_TRY(cudaMemcpy(out, L->d_mm, 4 * sizeof(double), cudaMemcpyDeviceToHost));
+  return OAL_OK;
+}
+
+oal_status oal_level_device_state(oal_level* L, void** f, void** rho, void** vel) {
+  if (!L) return set_error(OAL_E_INVALID_ARG, "null level");
+  if (f) *f = L->f[L->parity];
+  if (rho) *rho = L->rho;
+  if (vel) *vel = L->vel[L->parity];
+  return OAL_OK;
+}
+
+int64_t oal_level_device_bytes(const oal_level* L) { return L ? L->bytes : 0; }
+
+}  // extern "C"

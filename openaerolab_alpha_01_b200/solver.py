@@ -1,0 +1,245 @@
+"""Host-side mirror of the reference's solver-step and collision-operator interface.
+
+Names follow the reference (OpenAeroLab, Julia):
+
+* ``get_collision_kernel(operator)``  — operator registry (src/collision/physics_kernels.jl:50-75);
+  unknown names raise like the reference's ``error()``.
+* ``BlockDomain`` + ``build_box`` / ``apply_analytic_sphere_obstacle`` — the block topology of
+  ``build_neighbor_table`` (src/geometry/domain_topology.jl:919-953) and the analytic sphere mask
+  (src/geometry/domain_generation.jl:132-150).
+* ``Level.perform_timestep`` — ``perform_timestep_v2!`` for a level without a parent
+  (src/collision/timestep.jl:946-1559): one fused ``stream_collide_cumulant!`` launch, buffers
+  swapped by parity (src/solver/solver_control.jl:85-91).
+* ``Level.execute_timestep_batch`` — ``execute_timestep_batch!`` (src/solver/solver_control.jl:796-828):
+  n steps as one captured CUDA graph.
+
+Arrays use the reference layout flattened to C order: populations ``(Q, n_blocks, 512)``,
+density ``(n_blocks, 512)``, velocity ``(3, n_blocks, 512)``; the cell index inside a block is
+``x + 8y + 64z``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import _capi as capi
+from ._capi import check, lib
+
+_i32p = C.POINTER(C.c_int32)
+_u8p = C.POINTER(C.c_uint8)
+_f32p = C.POINTER(C.c_float)
+_f64p = C.POINTER(C.c_double)
+
+
+def _ptr(a: Optional[np.ndarray], ty):
+    if a is None:
+        return C.cast(None, ty)
+    return a.ctypes.data_as(ty)
+
+
+def _stream_handle(stream) -> Optional[int]:
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    h = getattr(stream, "cuda_stream", None)
+    if h is None:
+        raise TypeError("stream must be None, an int handle or a torch.cuda.Stream")
+    return int(h)
+
+
+def get_collision_kernel(operator: str) -> int:
+    """Operator id for a reference operator symbol (``"cumulant"``, ``"entropic"``, ``"hrr"``)."""
+    out = C.c_int32()
+    check(lib().oal_lookup_operator(operator.encode(), C.byref(out)))
+    return out.value
+
+
+def default_step_params(**overrides) -> capi.StepParams:
+    """The reference's configuration defaults (src/io/config_loader.jl:1305-1380) with overrides."""
+    return capi.default_params(**overrides)
+
+
+@dataclass
+class BlockDomain:
+    """Block topology and cell fields of one level (host arrays, reference semantics)."""
+
+    bx_max: int
+    by_max: int
+    bz_max: int
+    coords: np.ndarray  # (n, 3) int32, 1-based
+    neighbor_table: np.ndarray  # (27, n) int32 C order == Julia (n, 27) column-major, 1-based, 0 = none
+    obstacle: Optional[np.ndarray] = None  # (n, 512) uint8
+    sponge: Optional[np.ndarray] = None  # (n, 512) float32
+    wall_dist: Optional[np.ndarray] = None  # (n, 512) float32
+    periodic_mask: int = 0
+
+    @property
+    def n_blocks(self) -> int:
+        return int(self.coords.shape[0])
+
+    @property
+    def shape(self) -> tuple[int, int, int]:
+        return (8 * self.bx_max, 8 * self.by_max, 8 * self.bz_max)
+
+    def cell_positions(self) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """1-based global cell indices (gx, gy, gz), each (n, 512)."""
+        cell = np.arange(512)
+        lx, ly, lz = cell & 7, (cell >> 3) & 7, cell >> 6
+        gx = (self.coords[:, 0:1] - 1) * 8 + lx[None, :] + 1
+        gy = (self.coords[:, 1:2] - 1) * 8 + ly[None, :] + 1
+        gz = (self.coords[:, 2:3] - 1) * 8 + lz[None, :] + 1
+        return gx, gy, gz
+
+
+def build_box(bx_max: int, by_max: int, bz_max: int, periodic: tuple[bool, bool, bool] = (False, False, False)) -> BlockDomain:
+    """All blocks of a box, sorted like the reference, with their 27-entry neighbour table."""
+    n = bx_max * by_max * bz_max
+    coords = np.zeros((n, 3), dtype=np.int32)
+    nbr = np.zeros((27, n), dtype=np.int32)
+    mask = (1 if periodic[0] else 0) | (2 if periodic[1] else 0) | (4 if periodic[2] else 0)
+    check(lib().oal_build_box_blocks(bx_max, by_max, bz_max, mask, _ptr(coords, _i32p), _ptr(nbr, _i32p)))
+    return BlockDomain(bx_max, by_max, bz_max, coords, nbr, periodic_mask=mask)
+
+
+def apply_analytic_sphere_obstacle(dom: BlockDomain, centre: tuple[float, float, float], radius: float) -> int:
+    """Solid mask of a sphere (cell units, cell centres at index - 0.5); returns the solid count."""
+    obst = np.zeros((dom.n_blocks, 512), dtype=np.uint8)
+    n = C.c_int64()
+    check(lib().oal_build_sphere_obstacle(dom.n_blocks, _ptr(dom.coords, _i32p), float(centre[0]), float(centre[1]),
+                                          float(centre[2]), float(radius), _ptr(obst, _u8p), C.byref(n)))
+    dom.obstacle = obst
+    return int(n.value)
+
+
+def taylor_green_fields(dom: BlockDomain, u0: float, phase: tuple[float, float] = (0.0, 0.0)):
+    """2-D Taylor-Green vortex (uniform in z) on a periodic box with the consistent pressure field
+    rho = 1 + 3 (u0^2/4)(cos 2kx + cos 2ky), k = 2 pi / nx (tools/tests/q19_octree_step.jl:94)."""
+    gx, gy, _ = dom.cell_positions()
+    nx = 8 * dom.bx_max
+    k = 2.0 * np.pi / nx
+    x = gx - 0.5 + phase[0]
+    y = gy - 0.5 + phase[1]
+    rho = 1.0 + 3.0 * (u0 * u0 / 4.0) * (np.cos(2 * k * x) + np.cos(2 * k * y))
+    vel = np.zeros((3,) + rho.shape)
+    vel[0] = u0 * np.sin(k * x) * np.cos(k * y)
+    vel[1] = -u0 * np.cos(k * x) * np.sin(k * y)
+    return np.ascontiguousarray(rho, dtype=np.float64), np.ascontiguousarray(vel, dtype=np.float64)
+
+
+class Geometry:
+    """Device-resident topology of one level (oal_geometry)."""
+
+    def __init__(self, dom: BlockDomain, device: int = 0):
+        self.dom = dom
+        self._coords = np.ascontiguousarray(dom.coords, dtype=np.int32)
+        self._nbr = np.ascontiguousarray(dom.neighbor_table, dtype=np.int32)
+        self._obst = None if dom.obstacle is None else np.ascontiguousarray(dom.obstacle, dtype=np.uint8)
+        self._sponge = None if dom.sponge is None else np.ascontiguousarray(dom.sponge, dtype=np.float32)
+        self._wd = None if dom.wall_dist is None else np.ascontiguousarray(dom.wall_dist, dtype=np.float32)
+        nx, ny, nz = dom.shape
+        desc = capi.GeometryDesc(dom.n_blocks, nx, ny, nz, _ptr(self._coords, _i32p), _ptr(self._nbr, _i32p),
+                                 _ptr(self._obst, _u8p), _ptr(self._sponge, _f32p), _ptr(self._wd, _f32p))
+        h = C.c_void_p()
+        check(lib().oal_geometry_create(C.byref(desc), device, C.byref(h)))
+        self.handle = h
+
+    def info(self) -> dict:
+        out = (C.c_int64 * 5)()
+        check(lib().oal_geometry_info(self.handle, out))
+        return dict(n_blocks=out[0], fluid_cells=out[1], solid_cells=out[2], boundary_blocks=out[3], mask_blocks=out[4])
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().oal_geometry_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Level:
+    """Library-owned state of one level: ping-pong populations, density, velocity."""
+
+    def __init__(self, geom: Geometry, operator: str = "cumulant", storage: str = "f32"):
+        self.geom = geom
+        self.storage = capi.STORAGE_NAMES[storage]
+        self.operator = get_collision_kernel(operator)
+        h = C.c_void_p()
+        check(lib().oal_level_create(geom.handle, self.operator, self.storage, C.byref(h)))
+        self.handle = h
+        self.n_blocks = geom.dom.n_blocks
+
+    # -- state ---------------------------------------------------------------------------
+    def init_equilibrium(self, rho: np.ndarray, vel: np.ndarray, compressible_corr: int = 0) -> None:
+        rho = np.ascontiguousarray(rho, dtype=np.float64)
+        vel = np.ascontiguousarray(vel, dtype=np.float64)
+        assert rho.size == self.n_blocks * 512 and vel.size == 3 * rho.size
+        check(lib().oal_level_init_equilibrium(self.handle, rho.ctypes.data, vel.ctypes.data, compressible_corr))
+
+    def set_state(self, f: np.ndarray, rho: Optional[np.ndarray] = None, vel: Optional[np.ndarray] = None) -> None:
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        r = None if rho is None else np.ascontiguousarray(rho, dtype=np.float64)
+        v = None if vel is None else np.ascontiguousarray(vel, dtype=np.float64)
+        check(lib().oal_level_set_state(self.handle, f.ctypes.data, None if r is None else r.ctypes.data,
+                                        None if v is None else v.ctypes.data))
+
+    def state(self):
+        nb = self.n_blocks
+        f = np.empty((27, nb, 512))
+        rho = np.empty((nb, 512))
+        vel = np.empty((3, nb, 512))
+        check(lib().oal_level_get_state(self.handle, f.ctypes.data, rho.ctypes.data, vel.ctypes.data))
+        return f, rho, vel
+
+    # -- stepping ------------------------------------------------------------------------
+    def perform_timestep(self, params: capi.StepParams, stream=None) -> None:
+        check(lib().oal_level_step(self.handle, C.byref(params), _stream_handle(stream)))
+
+    step = perform_timestep
+
+    def execute_timestep_batch(self, params: capi.StepParams, n_steps: int, stream=None) -> None:
+        check(lib().oal_level_advance(self.handle, C.byref(params), int(n_steps), _stream_handle(stream)))
+
+    advance = execute_timestep_batch
+
+    def forces(self) -> np.ndarray:
+        out = (C.c_double * 3)()
+        check(lib().oal_level_get_forces(self.handle, out))
+        return np.array(out[:])
+
+    def forces_async(self, host_buf_ptr: int, stream=None) -> None:
+        check(lib().oal_level_get_forces_async(self.handle, host_buf_ptr, _stream_handle(stream)))
+
+    def mass_momentum(self) -> np.ndarray:
+        out = (C.c_double * 4)()
+        check(lib().oal_level_mass_momentum(self.handle, out))
+        return np.array(out[:])
+
+    def device_bytes(self) -> int:
+        return int(lib().oal_level_device_bytes(self.handle))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().oal_level_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def kinetic_energy(rho: np.ndarray, vel: np.ndarray, obstacle: Optional[np.ndarray] = None) -> float:
+    """Sum of rho |u|^2 / 2 over fluid cells (tools/tests/q19_octree_step.jl:17-24)."""
+    ke = 0.5 * rho * (vel[0] ** 2 + vel[1] ** 2 + vel[2] ** 2)
+    if obstacle is not None:
+        ke = np.where(obstacle != 0, 0.0, ke)
+    return float(ke.sum())

@@ -1,0 +1,127 @@
+"""CPU ORACLE — test infrastructure only.
+
+A C++ restatement of the reference's D3Q27 cumulant level step (see oal_oracle.cpp for the
+file:line map into the reference). Only tests/, the smoke check and the CPU-baseline leg of
+bench.py use it; the product path never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboal_oracle.so"
+
+_lib = None
+
+
+def build(force: bool = False) -> Path:
+    src = HERE / "oal_oracle.cpp"
+    hdr = HERE.parent / "include" / "oal.h"
+    if force or not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < max(src.stat().st_mtime, hdr.stat().st_mtime):
+        subprocess.run(["make", "-s", "-C", str(HERE), "-B" if force else "liboal_oracle.so"], check=True)
+    return LIB_PATH
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        L = C.CDLL(str(LIB_PATH))
+        vp = C.c_void_p
+        i32 = C.c_int32
+        L.ora_d3q27_tables.argtypes = [vp] * 7
+        L.ora_build_box.argtypes = [i32, i32, i32, i32, vp, vp]
+        L.ora_sphere.argtypes = [i32, vp, C.c_double, C.c_double, C.c_double, C.c_double, vp]
+        L.ora_sphere.restype = C.c_int64
+        L.ora_init_feq_f64.argtypes = [i32, vp, vp, i32, vp]
+        for n in ("ora_step_d3q27_f64", "ora_step_d3q27_f32"):
+            getattr(L, n).argtypes = [i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+            getattr(L, n).restype = C.c_int
+        L.ora_mass_momentum_f64.argtypes = [i32, vp, vp, vp]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def d3q27_tables():
+    cx, cy, cz, opp, my, mz = (np.zeros(27, np.int32) for _ in range(6))
+    w = np.zeros(27)
+    lib().ora_d3q27_tables(_p(cx), _p(cy), _p(cz), _p(w), _p(opp), _p(my), _p(mz))
+    return dict(cx=cx, cy=cy, cz=cz, w=w, opp=opp, mirror_y=my, mirror_z=mz)
+
+
+def build_box(bx, by, bz, periodic_mask):
+    n = bx * by * bz
+    coords = np.zeros((n, 3), np.int32)
+    nbr = np.zeros((27, n), np.int32)
+    lib().ora_build_box(bx, by, bz, periodic_mask, _p(coords), _p(nbr))
+    return coords, nbr
+
+
+def sphere(coords, centre, radius):
+    nb = coords.shape[0]
+    obst = np.zeros((nb, 512), np.uint8)
+    n = lib().ora_sphere(nb, _p(np.ascontiguousarray(coords, np.int32)), *map(float, centre), float(radius), _p(obst))
+    return obst, int(n)
+
+
+def init_feq(rho, vel, compressible=0):
+    nb = rho.shape[0]
+    f = np.zeros((27, nb, 512))
+    lib().ora_init_feq_f64(nb, _p(np.ascontiguousarray(rho, np.float64)), _p(np.ascontiguousarray(vel, np.float64)),
+                           compressible, _p(f))
+    return f
+
+
+class OracleLevel:
+    """Reference-layout state stepped by the CPU restatement (double or float)."""
+
+    def __init__(self, coords, nbr, shape, obstacle=None, sponge=None, wall_dist=None, dtype=np.float64):
+        self.coords = np.ascontiguousarray(coords, np.int32)
+        self.nbr = np.ascontiguousarray(nbr, np.int32)
+        self.nb = self.coords.shape[0]
+        self.shape = tuple(int(s) for s in shape)
+        self.obstacle = None if obstacle is None else np.ascontiguousarray(obstacle, np.uint8)
+        self.sponge = None if sponge is None else np.ascontiguousarray(sponge, np.float32)
+        self.wall_dist = None if wall_dist is None else np.ascontiguousarray(wall_dist, np.float32)
+        self.dtype = np.dtype(dtype)
+        nb = self.nb
+        self.f = np.zeros((27, nb, 512), self.dtype)
+        self.g = np.zeros_like(self.f)
+        self.rho = np.ones((nb, 512), self.dtype)
+        self.vel = np.zeros((3, nb, 512), self.dtype)
+        self.vel_new = np.zeros_like(self.vel)
+        self.force = np.zeros(3)
+
+    def init_equilibrium(self, rho, vel, compressible=0):
+        self.f[...] = init_feq(rho, vel, compressible).astype(self.dtype)
+        self.rho[...] = rho
+        self.vel[...] = vel
+
+    def step(self, params):
+        fn = lib().ora_step_d3q27_f64 if self.dtype == np.float64 else lib().ora_step_d3q27_f32
+        force = np.zeros(3)
+        rc = fn(self.nb, *self.shape, _p(self.coords), _p(self.nbr), _p(self.obstacle), _p(self.sponge),
+                _p(self.wall_dist), C.addressof(params), _p(self.f), _p(self.g), None, _p(self.rho),
+                _p(self.vel_new), _p(self.vel), _p(force))
+        assert rc == 0
+        self.f, self.g = self.g, self.f
+        self.vel, self.vel_new = self.vel_new, self.vel
+        if params.collect_forces:
+            self.force = force
+        return self
+
+    def mass_momentum(self):
+        out = np.zeros(4)
+        f = np.ascontiguousarray(self.f, np.float64)
+        lib().ora_mass_momentum_f64(self.nb, _p(self.obstacle), _p(f), _p(out))
+        return out

@@ -1,0 +1,708 @@
+// oal_oracle.cpp — CPU ORACLE (test infrastructure only; never linked into the product).
+//
+// A plain C++ restatement of the reference's D3Q27 cumulant lattice-Boltzmann level step
+// (OpenAeroLab, Julia), templated on the arithmetic type: instantiated in double it is the
+// FP64 oracle; in float it mirrors the reference's Float32 kernel and is the timed CPU
+// baseline. Parallelised over blocks with OpenMP. Built with -ffp-contract=off so the float
+// instantiation rounds like the reference (no fused multiply-add contraction).
+//
+// Followed line by line (paths inside the reference project):
+//   D3Q27 tables ............ src/collision/lattice.jl:10-60, src/collision/timestep.jl:2005-2023
+//   block order ............. src/geometry/domain.jl:785 (sorted active block tuples)
+//   neighbour table ......... src/geometry/domain_topology.jl:919-953 (+ periodic wrap per axis)
+//   analytic sphere ......... src/geometry/domain_generation.jl:132-150
+//   equilibria .............. src/collision/physics_utils.jl:30-109
+//   inlet noise hash ........ src/collision/physics_utils.jl:5-17
+//   pull + face BCs ......... src/collision/kernel_cumulant.jl:173-400
+//   obstacle (full-way) ..... src/collision/kernel_cumulant.jl:402-417
+//   macros/sponge/wall model  src/collision/kernel_cumulant.jl:420-491
+//   WALE + gradients ........ src/collision/kernel_cumulant.jl:496-595,
+//                             src/collision/physics_utils.jl:1981-2035,2217-2233
+//   cumulant collision ...... src/collision/kernel_cumulant.jl:1-26,597-844
+//   positivity limiter ...... src/collision/kernel_cumulant.jl:849-884
+//   Guo forcing + store ..... src/collision/kernel_cumulant.jl:889-908
+//   half-way BB + MEM ....... src/octree_q19/src/stream.jl:229-256 (link rule, generalised to the
+//                             27 D3Q27 links; the reference's GPU path has no D3Q27 analogue)
+//   mass / momentum ......... src/octree_q19/src/state.jl:614-637 (Float64 sums)
+//
+// Parity status: the reference is Julia and cannot run in this environment, so this restatement
+// is pinned by the reference's analytic gates (Taylor-Green decay, conservation, rest state) and
+// by the reference's own identities for the tables, not by reference-produced vectors.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+#include <array>
+#include <tuple>
+
+#include "../include/oal.h"
+
+namespace {
+
+constexpr int Q = 27;
+constexpr int BS = 8;
+
+struct Tables {
+  int cx[Q], cy[Q], cz[Q], opp[Q], mir_y[Q], mir_z[Q];
+  double w[Q];
+};
+
+// lattice.jl:10-60 — z outer, y middle, x inner; k = 1 + (cx+1) + 3(cy+1) + 9(cz+1)
+Tables make_tables() {
+  Tables t{};
+  int n = 0;
+  for (int z = -1; z <= 1; ++z)
+    for (int y = -1; y <= 1; ++y)
+      for (int x = -1; x <= 1; ++x) {
+        t.cx[n] = x; t.cy[n] = y; t.cz[n] = z;
+        int d2 = x * x + y * y + z * z;
+        t.w[n] = d2 == 0 ? 8.0 / 27.0 : d2 == 1 ? 2.0 / 27.0 : d2 == 2 ? 1.0 / 54.0 : 1.0 / 216.0;
+        ++n;
+      }
+  for (int i = 0; i < Q; ++i)
+    for (int j = 0; j < Q; ++j) {
+      if (t.cx[j] == -t.cx[i] && t.cy[j] == -t.cy[i] && t.cz[j] == -t.cz[i]) t.opp[i] = j;
+      if (t.cx[j] == t.cx[i] && t.cy[j] == -t.cy[i] && t.cz[j] == t.cz[i]) t.mir_y[i] = j;
+      if (t.cx[j] == t.cx[i] && t.cy[j] == t.cy[i] && t.cz[j] == -t.cz[i]) t.mir_z[i] = j;
+    }
+  return t;
+}
+const Tables TB = make_tables();
+
+// physics_utils.jl:5-17 (Int32 wrap-around arithmetic done in uint32)
+uint32_t gpu_hash(int32_t x) {
+  uint32_t h = (uint32_t)x;
+  h = (h ^ (h >> 16)) * 0x85ebca6bu;
+  h = (h ^ (h >> 13)) * 0xc2b2ae35u;
+  return h ^ (h >> 16);
+}
+float gradient_noise(int32_t gx, int32_t gy, int32_t gz, int32_t seed) {
+  uint32_t combined = (uint32_t)gx * 374761393u + (uint32_t)gy * 668265263u +
+                      (uint32_t)gz * 1274126177u + (uint32_t)seed;
+  uint32_t h = gpu_hash((int32_t)combined);
+  return ((float)(h & 0xFFFFu) / 32768.0f) - 1.0f;
+}
+
+// physics_utils.jl:30-35
+template <class T>
+T feq2(T rho, T ux, T uy, T uz, T w, T cx, T cy, T cz) {
+  T cu = cx * ux + cy * uy + cz * uz;
+  T usq = ux * ux + uy * uy + uz * uz;
+  return rho * w * (T(1) + T(3) * cu + T(4.5) * cu * cu - T(1.5) * usq);
+}
+// physics_utils.jl:65-95 (limiter gate off: the default build)
+template <class T>
+T feq4(T rho, T ux, T uy, T uz, T w, T cx, T cy, T cz) {
+  T cu = cx * ux + cy * uy + cz * uz;
+  T usq = ux * ux + uy * uy + uz * uz;
+  T cu2 = cu * cu, cu3 = cu2 * cu, cu4 = cu2 * cu2, usq2 = usq * usq;
+  T val = T(1) + T(3) * cu + T(4.5) * cu2 - T(1.5) * usq;
+  T ho = (T(4.5) * cu3 - T(4.5) * cu * usq) + (T(3.375) * cu4 - T(6.75) * cu2 * usq + T(1.125) * usq2);
+  val += ho;
+  return rho * w * val;
+}
+// physics_utils.jl:97-109
+template <class T>
+T feq_auto(T rho, T ux, T uy, T uz, T w, T cx, T cy, T cz, int comp) {
+  return comp == 1 ? feq4(rho, ux, uy, uz, w, cx, cy, cz) : feq2(rho, ux, uy, uz, w, cx, cy, cz);
+}
+
+// kernel_cumulant.jl:4-26
+template <class T>
+void chimera_forward(T& a, T& b, T& c, T u) {
+  T m0 = a + b + c, m1 = c - a, m2 = a + c;
+  a = m0;
+  b = m1 - u * m0;
+  c = m2 - T(2) * u * m1 + u * u * m0;
+}
+template <class T>
+void chimera_backward(T& a, T& b, T& c, T u) {
+  T kc0 = a, kc1 = b, kc2 = c;
+  T m0 = kc0;
+  T m1 = kc1 + u * kc0;
+  T m2 = kc2 + T(2) * u * kc1 + u * u * kc0;
+  T fp = (m2 + m1) * T(0.5);
+  T fm = (m2 - m1) * T(0.5);
+  T f0 = m0 - m2;
+  a = fm; b = f0; c = fp;
+}
+
+struct Level {
+  int32_t nb, nx, ny, nz;
+  const int32_t* coords;   // n*3 1-based
+  const int32_t* nbr;      // Julia (n,27): nbr[b + n*dir], 1-based, 0 none
+  const uint8_t* obstacle; // 512*n or null
+  const float* sponge;
+  const float* wall_dist;
+};
+
+inline int64_t cidx(int x, int y, int z) { return (int64_t)x + 8 * y + 64 * z; }  // 0-based
+
+template <class T>
+struct Arr {
+  // Reference layout accessors; x,y,z 0-based, b 0-based, k 0-based.
+  int64_t nb;
+  int64_t f(int x, int y, int z, int b, int k) const { return cidx(x, y, z) + 512 * (int64_t)b + 512 * nb * k; }
+  int64_t s(int x, int y, int z, int b) const { return cidx(x, y, z) + 512 * (int64_t)b; }
+};
+
+// physics_utils.jl:2001-2035 get_velocity_neighbor_fluid (sym_y_plane = 0)
+template <class T>
+void vel_nb_fluid(const Level& L, const T* vel_in, int x, int y, int z, int b, int dx, int dy, int dz,
+                  T& ux, T& uy, T& uz) {
+  Arr<T> A{L.nb};
+  const int64_t cs = 512 * (int64_t)L.nb;
+  int64_t own = A.s(x, y, z, b);
+  T ux0 = vel_in[own], uy0 = vel_in[own + cs], uz0 = vel_in[own + 2 * cs];
+  int nx = x + dx, ny = y + dy, nz = z + dz;
+  if (nx >= 0 && nx < BS && ny >= 0 && ny < BS && nz >= 0 && nz < BS) {
+    int64_t i = A.s(nx, ny, nz, b);
+    if (L.obstacle && L.obstacle[i]) { ux = ux0; uy = uy0; uz = uz0; return; }
+    ux = vel_in[i]; uy = vel_in[i + cs]; uz = vel_in[i + 2 * cs];
+    return;
+  }
+  int ox = nx < 0 ? -1 : (nx >= BS ? 1 : 0);
+  int oy = ny < 0 ? -1 : (ny >= BS ? 1 : 0);
+  int oz = nz < 0 ? -1 : (nz >= BS ? 1 : 0);
+  int dir = (ox + 1) + (oy + 1) * 3 + (oz + 1) * 9;
+  int nbi = L.nbr[b + (int64_t)L.nb * dir];
+  if (nbi > 0) {
+    int nnx = nx < 0 ? nx + BS : (nx >= BS ? nx - BS : nx);
+    int nny = ny < 0 ? ny + BS : (ny >= BS ? ny - BS : ny);
+    int nnz = nz < 0 ? nz + BS : (nz >= BS ? nz - BS : nz);
+    int64_t i = A.s(nnx, nny, nnz, nbi - 1);
+    if (L.obstacle && L.obstacle[i]) { ux = ux0; uy = uy0; uz = uz0; return; }
+    ux = vel_in[i]; uy = vel_in[i + cs]; uz = vel_in[i + 2 * cs];
+    return;
+  }
+  ux = ux0; uy = uy0; uz = uz0;
+}
+
+// Source cell of the pull x - c_k: block index (0-based, -1 = none) and local coordinates.
+inline int src_block(const Level& L, int b, int sx, int sy, int sz, int& lx, int& ly, int& lz) {
+  if (sx >= 0 && sx < BS && sy >= 0 && sy < BS && sz >= 0 && sz < BS) { lx = sx; ly = sy; lz = sz; return b; }
+  int ox = sx < 0 ? -1 : (sx >= BS ? 1 : 0);
+  int oy = sy < 0 ? -1 : (sy >= BS ? 1 : 0);
+  int oz = sz < 0 ? -1 : (sz >= BS ? 1 : 0);
+  int dir = (ox + 1) + (oy + 1) * 3 + (oz + 1) * 9;
+  int nbi = L.nbr[b + (int64_t)L.nb * dir];
+  if (nbi <= 0) return -1;
+  lx = sx - BS * ox; ly = sy - BS * oy; lz = sz - BS * oz;
+  return nbi - 1;
+}
+
+template <class T>
+void step_cell(const Level& L, const oal_step_params& P, const T* f_in, T* f_out, T* f_post, T* rho_out,
+               T* vel_out, const T* vel_in, int b, int x, int y, int z, double* force_acc) {
+  Arr<T> A{L.nb};
+  const int64_t cs = 512 * (int64_t)L.nb;
+  const int bx = L.coords[3 * b], by = L.coords[3 * b + 1], bz = L.coords[3 * b + 2];
+  // 1-based global coordinates (kernel_cumulant.jl:181-183)
+  const int gx = (bx - 1) * BS + x + 1, gy = (by - 1) * BS + y + 1, gz = (bz - 1) * BS + z + 1;
+  const int64_t own = A.s(x, y, z, b);
+  const bool is_obs = L.obstacle && L.obstacle[own];
+  const bool halfway = P.solid_bc == OAL_SOLID_HALFWAY;
+  const int comp = P.compressible_corr;
+  const T u_inlet = T(P.u_inlet);
+  const bool store_post = P.store_post_collision == 1 && f_post != nullptr;
+
+  if (halfway && is_obs) {
+    // Half-way mode: a solid cell holds the rest equilibrium; no fluid cell reads it.
+    vel_out[own] = T(0); vel_out[own + cs] = T(0); vel_out[own + 2 * cs] = T(0);
+    rho_out[own] = T(1);
+    for (int k = 0; k < Q; ++k) {
+      f_out[A.f(x, y, z, b, k)] = T(TB.w[k]);
+      if (store_post) f_post[A.f(x, y, z, b, k)] = T(TB.w[k]);
+    }
+    return;
+  }
+
+  // STEP 1: pull streaming (kernel_cumulant.jl:190-400)
+  T rho = T(0), jx = T(0), jy = T(0), jz = T(0);
+  T fs[Q];
+  double mx = 0, my = 0, mz = 0;
+  for (int k = 0; k < Q; ++k) {
+    const int cx = TB.cx[k], cy = TB.cy[k], cz = TB.cz[k];
+    const int sx = x - cx, sy = y - cy, sz = z - cz;
+    T val = T(0);
+    int lx, ly, lz;
+    int sb = src_block(L, b, sx, sy, sz, lx, ly, lz);
+    if (sb >= 0) {
+      const bool src_solid = L.obstacle && L.obstacle[A.s(lx, ly, lz, sb)];
+      if (halfway && src_solid) {
+        // link opp(k) of this cell is cut: the population this cell sent toward the wall
+        // returns (octree_q19/src/stream.jl:229-233, half-way rule, wall at rest)
+        const int i = TB.opp[k];
+        val = f_in[A.f(x, y, z, b, i)];
+        if (P.collect_forces) {
+          // momentum exchange (f_i* + f_j(t+1)) c_i with j = k, i toward the wall
+          // (stream.jl:248-256), accumulated in Float64
+          const double mom = (double)f_in[A.f(x, y, z, b, i)] + (double)val;
+          mx += mom * TB.cx[i]; my += mom * TB.cy[i]; mz += mom * TB.cz[i];
+        }
+      } else {
+        val = f_in[A.f(lx, ly, lz, sb, k)];
+      }
+    } else {
+      const int src_gx = gx - cx;
+      const int src_gy = gy - cy;  // _pwrap_y: identity (periodic-Y AMR gate off)
+      const int src_gz = gz - cz;
+      const bool is_inlet = src_gx < 1, is_outlet = src_gx > L.nx;
+      const bool is_y_min = src_gy < 1, is_y_max = src_gy > L.ny;
+      const bool is_z_min = src_gz < 1, is_z_max = src_gz > L.nz;
+      if (is_inlet) {
+        float noise = P.inlet_turbulence > 0.0f
+                          ? gradient_noise(gy, gz, P.time_step_seed, 1234) * P.inlet_turbulence * P.u_inlet
+                          : 0.0f;
+        T u_inst = u_inlet + T(noise);
+        val = feq_auto<T>(T(1), u_inst, T(0), T(0), T(TB.w[k]), T(cx), T(cy), T(cz), comp);
+      } else if (is_outlet) {
+        val = f_in[A.f(x, y, z, b, k)];
+      } else if (P.zwall_bc != 0 && (is_z_min || is_z_max)) {
+        if (P.zwall_bc == 2) {
+          val = f_in[A.f(x, y, z, b, TB.opp[k])];
+        } else {
+          const int zw_k = TB.mir_z[k];
+          const int zw_ix = x - cx, zw_iy = y - cy;
+          if (zw_ix >= 0 && zw_ix < BS && zw_iy >= 0 && zw_iy < BS) {
+            val = f_in[A.f(zw_ix, zw_iy, z, b, zw_k)];
+          } else {
+            const int zw_ox = zw_ix < 0 ? -1 : (zw_ix >= BS ? 1 : 0);
+            const int zw_oy = zw_iy < 0 ? -1 : (zw_iy >= BS ? 1 : 0);
+            const int dir = (zw_ox + 1) + (zw_oy + 1) * 3 + 9;
+            const int zw_nb = L.nbr[b + (int64_t)L.nb * dir];
+            if (zw_nb > 0) {
+              const int zw_lx = zw_ix < 0 ? zw_ix + BS : (zw_ix >= BS ? zw_ix - BS : zw_ix);
+              const int zw_ly = zw_iy < 0 ? zw_iy + BS : (zw_iy >= BS ? zw_iy - BS : zw_iy);
+              val = f_in[A.f(zw_lx, zw_ly, z, zw_nb - 1, zw_k)];
+            } else {
+              // level 1: no parent image; the cell's own mirror_z population
+              val = f_in[A.f(x, y, z, b, zw_k)];
+            }
+          }
+        }
+      } else if (P.transverse_freestream == 1 && (is_y_min || is_y_max || is_z_min || is_z_max)) {
+        const T beta_t = T(P.transverse_freestream_blend);
+        const T donor = f_in[A.f(x, y, z, b, k)];
+        const T feq_fs = feq_auto<T>(T(1), u_inlet, T(0), T(0), T(TB.w[k]), T(cx), T(cy), T(cz), comp);
+        val = (T(1) - beta_t) * donor + beta_t * feq_fs;
+      } else if (is_y_min && P.ymin_wall_bc == 1) {
+        val = f_in[A.f(x, y, z, b, TB.opp[k])];
+      } else if (is_y_min || is_y_max) {
+        val = f_in[A.f(x, y, z, b, TB.mir_y[k])];
+      } else if (is_z_min || is_z_max) {
+        val = f_in[A.f(x, y, z, b, TB.mir_z[k])];
+      } else {
+        // level 1 (no parent): lattice weight (kernel_cumulant.jl:389-391)
+        val = T(TB.w[k]);
+      }
+    }
+    fs[k] = val;
+    rho += val;
+    jx += val * T(cx);
+    jy += val * T(cy);
+    jz += val * T(cz);
+  }
+  if (P.collect_forces && (mx != 0 || my != 0 || mz != 0)) {
+    force_acc[0] += mx; force_acc[1] += my; force_acc[2] += mz;
+  }
+
+  // Obstacle: simple bounce-back (kernel_cumulant.jl:402-417)
+  if (is_obs) {
+    vel_out[own] = T(0); vel_out[own + cs] = T(0); vel_out[own + 2 * cs] = T(0);
+    rho_out[own] = T(1);
+    for (int k = 0; k < Q; ++k) {
+      T fc = fs[TB.opp[k]];
+      f_out[A.f(x, y, z, b, k)] = fc;
+      if (store_post) f_post[A.f(x, y, z, b, k)] = fc;
+    }
+    return;
+  }
+
+  // STEP 2: macros + sponge + wall model (kernel_cumulant.jl:420-491)
+  rho = std::max(rho, T(0.01));
+  T inv_rho = T(1) / rho;
+  T ux = jx * inv_rho, uy = jy * inv_rho, uz = jz * inv_rho;
+  const T sp = L.sponge ? T(L.sponge[own]) : T(0);
+  if (sp > T(0)) {
+    const T rho_target = T(1), ux_target = u_inlet;
+    rho = rho * (T(1) - sp) + rho_target * sp;
+    ux = ux * (T(1) - sp) + ux_target * sp;
+    uy = uy * (T(1) - sp);
+    uz = uz * (T(1) - sp);
+    if (P.sponge_blend_distributions == 1) {
+      for (int k = 0; k < Q; ++k) {
+        T fe = feq_auto<T>(rho_target, ux_target, T(0), T(0), T(TB.w[k]), T(TB.cx[k]), T(TB.cy[k]), T(TB.cz[k]), comp);
+        fs[k] = fs[k] * (T(1) - sp) + fe * sp;
+      }
+    }
+  }
+  T Fx = T(0), Fy = T(0), Fz = T(0);
+  if (P.wall_model_active == 1 && L.wall_dist) {
+    const T dist_wall = T(L.wall_dist[own]);
+    if (dist_wall > T(0) && dist_wall < T(P.wall_model_max_distance)) {
+      T u_mag = std::sqrt(ux * ux + uy * uy + uz * uz);
+      T nu_visc = (T(P.tau) - T(0.5)) / T(3);
+      if (u_mag > T(1e-6) && nu_visc > T(1e-10)) {
+        T u_tau = u_mag * std::pow(nu_visc / (dist_wall * u_mag + T(1e-10)), T(1) / T(7)) *
+                  std::pow(T(2) * T(8.3), -T(1) / T(7));
+        u_tau = std::max(u_tau, T(1e-6));
+        T y_p = u_tau * dist_wall / nu_visc;
+        if (y_p > T(11.81)) {
+          T u_plus_law = (T(1) / T(0.41)) * std::log(y_p) + T(5.2);
+          if (u_plus_law > T(0.1)) {
+            u_tau = u_tau * ((u_mag / u_tau) / u_plus_law);
+            u_tau = std::max(u_tau, T(1e-6));
+          }
+        }
+        T tau_wall = rho * u_tau * u_tau;
+        T tau_res = rho * nu_visc * (u_mag / dist_wall);
+        if (tau_wall > tau_res) {
+          T force_mag = (tau_wall - tau_res) / dist_wall;
+          Fx = -force_mag * ux / u_mag;
+          Fy = -force_mag * uy / u_mag;
+          Fz = -force_mag * uz / u_mag;
+        }
+      }
+    }
+  }
+  const T ux_eq = ux + T(0.5) * Fx * inv_rho;
+  const T uy_eq = uy + T(0.5) * Fy * inv_rho;
+  const T uz_eq = uz + T(0.5) * Fz * inv_rho;
+  vel_out[own] = ux; vel_out[own + cs] = uy; vel_out[own + 2 * cs] = uz;
+  rho_out[own] = rho;
+
+  // STEP 3: WALE (kernel_cumulant.jl:496-595), background path (variable_nu_sgs off)
+  T uE[3], uW[3], uN[3], uS[3], uT[3], uB[3];
+  vel_nb_fluid(L, vel_in, x, y, z, b, 1, 0, 0, uE[0], uE[1], uE[2]);
+  vel_nb_fluid(L, vel_in, x, y, z, b, -1, 0, 0, uW[0], uW[1], uW[2]);
+  vel_nb_fluid(L, vel_in, x, y, z, b, 0, 1, 0, uN[0], uN[1], uN[2]);
+  vel_nb_fluid(L, vel_in, x, y, z, b, 0, -1, 0, uS[0], uS[1], uS[2]);
+  vel_nb_fluid(L, vel_in, x, y, z, b, 0, 0, 1, uT[0], uT[1], uT[2]);
+  vel_nb_fluid(L, vel_in, x, y, z, b, 0, 0, -1, uB[0], uB[1], uB[2]);
+  const T h = T(0.5);
+  const T g11 = h * (uE[0] - uW[0]), g12 = h * (uN[0] - uS[0]), g13 = h * (uT[0] - uB[0]);
+  const T g21 = h * (uE[1] - uW[1]), g22 = h * (uN[1] - uS[1]), g23 = h * (uT[1] - uB[1]);
+  const T g31 = h * (uE[2] - uW[2]), g32 = h * (uN[2] - uS[2]), g33 = h * (uT[2] - uB[2]);
+  const T gsq11 = g11 * g11 + g12 * g21 + g13 * g31;
+  const T gsq12 = g11 * g12 + g12 * g22 + g13 * g32;
+  const T gsq13 = g11 * g13 + g12 * g23 + g13 * g33;
+  const T gsq21 = g21 * g11 + g22 * g21 + g23 * g31;
+  const T gsq22 = g21 * g12 + g22 * g22 + g23 * g32;
+  const T gsq23 = g21 * g13 + g22 * g23 + g23 * g33;
+  const T gsq31 = g31 * g11 + g32 * g21 + g33 * g31;
+  const T gsq32 = g31 * g12 + g32 * g22 + g33 * g32;
+  const T gsq33 = g31 * g13 + g32 * g23 + g33 * g33;
+  const T tr_term = (gsq11 + gsq22 + gsq33) / T(3);
+  const T Sd11 = gsq11 - tr_term, Sd22 = gsq22 - tr_term, Sd33 = gsq33 - tr_term;
+  const T Sd12 = T(0.5) * (gsq12 + gsq21), Sd13 = T(0.5) * (gsq13 + gsq31), Sd23 = T(0.5) * (gsq23 + gsq32);
+  const T S12 = T(0.5) * (g12 + g21), S13 = T(0.5) * (g13 + g31), S23 = T(0.5) * (g23 + g32);
+  const T OP1 = Sd11 * Sd11 + Sd22 * Sd22 + Sd33 * Sd33 + T(2) * (Sd12 * Sd12 + Sd13 * Sd13 + Sd23 * Sd23);
+  const T OP2 = g11 * g11 + g22 * g22 + g33 * g33 + T(2) * (S12 * S12 + S13 * S13 + S23 * S23);
+  T nu_eddy = T(0);
+  if (OP1 > T(1e-12)) {
+    T OP1_32 = OP1 * std::sqrt(OP1);
+    T OP2_52 = OP2 * OP2 * std::sqrt(std::max(OP2, T(1e-12)));
+    T denom = OP2_52 + OP1 * std::sqrt(std::sqrt(std::max(OP1, T(1e-12))));
+    if (denom > T(1e-12)) nu_eddy = (T(P.c_wale) * T(P.c_wale)) * OP1_32 / denom;
+  }
+  nu_eddy = nu_eddy * T(P.amr_sgs_scale);
+  nu_eddy = std::max(nu_eddy, T(P.nu_sgs_background) * T(P.amr_sgs_scale));
+  const T nu_mol = (T(P.tau) - T(0.5)) / T(3);
+  const T nu_eff = nu_mol + nu_eddy;
+  const T tau_eff = T(0.5) + T(3) * nu_eff;
+  const T omega1 = T(1) / std::max(tau_eff, T(0.500001));
+  const T omega_bulk = T(P.omega_bulk), omega3 = T(P.omega3), omega4 = T(P.omega4);
+  T omega4_diag = omega4;
+  if (P.adaptive_omega4 == 1) {
+    T om1_m2 = omega1 - T(2);
+    T denom_adaptive = T(P.lambda_param) * omega1 + T(1e-10);
+    T A_val = -(om1_m2 * om1_m2) / denom_adaptive;
+    omega4_diag = std::min(std::max(A_val, T(0.01)), T(2));
+  }
+
+  // STEP 4: chimera forward (kernel_cumulant.jl:612-656); A index = (cx+1)+3(cy+1)+9(cz+1)
+  T Am[Q];
+  for (int k = 0; k < Q; ++k) Am[k] = fs[k];
+  for (int iz = 0; iz < 3; ++iz)
+    for (int iy = 0; iy < 3; ++iy) {
+      int base = iy * 3 + iz * 9;
+      chimera_forward(Am[base], Am[base + 1], Am[base + 2], ux_eq);
+    }
+  for (int iz = 0; iz < 3; ++iz)
+    for (int ma = 0; ma < 3; ++ma)
+      chimera_forward(Am[ma + iz * 9], Am[ma + 3 + iz * 9], Am[ma + 6 + iz * 9], uy_eq);
+  for (int mb = 0; mb < 3; ++mb)
+    for (int ma = 0; ma < 3; ++ma)
+      chimera_forward(Am[ma + mb * 3], Am[ma + mb * 3 + 9], Am[ma + mb * 3 + 18], uz_eq);
+
+  // STEP 5: central moments -> cumulants (kernel_cumulant.jl:661-699); 1-based A[n] = Am[n-1]
+  const T k_000 = Am[0];
+  const T k_200 = Am[2], k_020 = Am[6], k_002 = Am[18];
+  const T k_110 = Am[4], k_101 = Am[10], k_011 = Am[12];
+  const T k_210 = Am[5], k_120 = Am[7], k_201 = Am[11];
+  const T k_021 = Am[15], k_102 = Am[19], k_012 = Am[21];
+  const T k_111 = Am[13];
+  const T k_220 = Am[8], k_202 = Am[20], k_022 = Am[24];
+  const T k_211 = Am[14], k_121 = Am[16], k_112 = Am[22];
+  const T inv_r = T(1) / std::max(k_000, T(0.01));
+  const T c200 = k_200 * inv_r, c020 = k_020 * inv_r, c002 = k_002 * inv_r;
+  const T c110 = k_110 * inv_r, c101 = k_101 * inv_r, c011 = k_011 * inv_r;
+  const T c210 = k_210 * inv_r, c120 = k_120 * inv_r, c201 = k_201 * inv_r;
+  const T c021 = k_021 * inv_r, c102 = k_102 * inv_r, c012 = k_012 * inv_r;
+  const T c111 = k_111 * inv_r;
+  const T c220n = k_220 * inv_r, c202n = k_202 * inv_r, c022n = k_022 * inv_r;
+  const T c211n = k_211 * inv_r, c121n = k_121 * inv_r, c112n = k_112 * inv_r;
+  const T C_220 = c220n - c200 * c020 - T(2) * c110 * c110;
+  const T C_202 = c202n - c200 * c002 - T(2) * c101 * c101;
+  const T C_022 = c022n - c020 * c002 - T(2) * c011 * c011;
+  const T C_211 = c211n - c200 * c011 - T(2) * c110 * c101;
+  const T C_121 = c121n - c020 * c101 - T(2) * c110 * c011;
+  const T C_112 = c112n - c002 * c110 - T(2) * c101 * c011;
+
+  // STEP 6: relaxation (kernel_cumulant.jl:705-754)
+  // the reference's literal 0.333333333f0 rounds to the float nearest 1/3; 1/3 keeps that value in
+  // float and is the intended constant in double
+  const T cs2 = T(1) / T(3);
+  const T D_trace = c200 + c020 + c002;
+  const T D_trace_eq = T(3) * cs2;
+  const T D_trace_s = (T(1) - omega_bulk) * D_trace + omega_bulk * D_trace_eq;
+  const T D1 = c200 - c020, D2 = c200 - c002;
+  const T D1_s = (T(1) - omega1) * D1, D2_s = (T(1) - omega1) * D2;
+  const T c200_s = (D_trace_s + D1_s + D2_s) / T(3);
+  const T c020_s = (D_trace_s - T(2) * D1_s + D2_s) / T(3);
+  const T c002_s = (D_trace_s + D1_s - T(2) * D2_s) / T(3);
+  T c110_s = (T(1) - omega1) * c110;
+  T c101_s = (T(1) - omega1) * c101;
+  T c011_s = (T(1) - omega1) * c011;
+  if (P.limiter_type == 1) {
+    T b110 = std::sqrt(std::max(c200_s * c020_s, T(0)));
+    T b101 = std::sqrt(std::max(c200_s * c002_s, T(0)));
+    T b011 = std::sqrt(std::max(c020_s * c002_s, T(0)));
+    c110_s = std::min(std::max(c110_s, -b110), b110);
+    c101_s = std::min(std::max(c101_s, -b101), b101);
+    c011_s = std::min(std::max(c011_s, -b011), b011);
+  }
+  const T c210_s = (T(1) - omega3) * c210, c120_s = (T(1) - omega3) * c120;
+  const T c201_s = (T(1) - omega3) * c201, c021_s = (T(1) - omega3) * c021;
+  const T c102_s = (T(1) - omega3) * c102, c012_s = (T(1) - omega3) * c012;
+  const T c111_s = (T(1) - omega3) * c111;
+  const T C_220_s = (T(1) - omega4_diag) * C_220;
+  const T C_202_s = (T(1) - omega4_diag) * C_202;
+  const T C_022_s = (T(1) - omega4_diag) * C_022;
+  const T C_211_s = (T(1) - omega4) * C_211;
+  const T C_121_s = (T(1) - omega4) * C_121;
+  const T C_112_s = (T(1) - omega4) * C_112;
+
+  // STEP 7: reconstruction (kernel_cumulant.jl:759-781)
+  const T c220_s = C_220_s + c200_s * c020_s + T(2) * c110_s * c110_s;
+  const T c202_s = C_202_s + c200_s * c002_s + T(2) * c101_s * c101_s;
+  const T c022_s = C_022_s + c020_s * c002_s + T(2) * c011_s * c011_s;
+  const T c211_s = C_211_s + c200_s * c011_s + T(2) * c110_s * c101_s;
+  const T c121_s = C_121_s + c020_s * c101_s + T(2) * c110_s * c011_s;
+  const T c112_s = C_112_s + c002_s * c110_s + T(2) * c101_s * c011_s;
+  const T c221_s = c200_s * c021_s + c020_s * c201_s + T(4) * c110_s * c111_s + T(2) * c101_s * c120_s +
+                   T(2) * c011_s * c210_s;
+  const T c212_s = c200_s * c012_s + c002_s * c210_s + T(2) * c110_s * c102_s + T(4) * c101_s * c111_s +
+                   T(2) * c011_s * c201_s;
+  const T c122_s = c020_s * c102_s + c002_s * c120_s + T(2) * c110_s * c012_s + T(4) * c011_s * c111_s +
+                   T(2) * c101_s * c021_s;
+  T c222_s = c200_s * C_022_s + c020_s * C_202_s + c002_s * C_220_s +
+             T(4) * (c110_s * C_112_s + c101_s * C_121_s + c011_s * C_211_s);
+  c222_s += T(2) * (c210_s * c012_s + c201_s * c021_s + c120_s * c102_s) + T(4) * c111_s * c111_s;
+  c222_s += c200_s * c020_s * c002_s +
+            T(2) * (c200_s * c011_s * c011_s + c020_s * c101_s * c101_s + c002_s * c110_s * c110_s) +
+            T(8) * c110_s * c101_s * c011_s;
+
+  // STEP 8: write back (kernel_cumulant.jl:786-804)
+  const T r = k_000;
+  Am[0] = r;
+  Am[1] = T(0); Am[3] = T(0); Am[9] = T(0);
+  Am[2] = r * c200_s; Am[6] = r * c020_s; Am[18] = r * c002_s;
+  Am[4] = r * c110_s; Am[10] = r * c101_s; Am[12] = r * c011_s;
+  Am[5] = r * c210_s; Am[7] = r * c120_s; Am[11] = r * c201_s;
+  Am[15] = r * c021_s; Am[19] = r * c102_s; Am[21] = r * c012_s;
+  Am[13] = r * c111_s;
+  Am[8] = r * c220_s; Am[20] = r * c202_s; Am[24] = r * c022_s;
+  Am[14] = r * c211_s; Am[16] = r * c121_s; Am[22] = r * c112_s;
+  Am[17] = r * c221_s; Am[23] = r * c212_s; Am[25] = r * c122_s;
+  Am[26] = r * c222_s;
+
+  // STEP 9: chimera backward z, y, x (kernel_cumulant.jl:810-844)
+  for (int mb = 0; mb < 3; ++mb)
+    for (int ma = 0; ma < 3; ++ma)
+      chimera_backward(Am[ma + mb * 3], Am[ma + mb * 3 + 9], Am[ma + mb * 3 + 18], uz_eq);
+  for (int iz = 0; iz < 3; ++iz)
+    for (int ma = 0; ma < 3; ++ma)
+      chimera_backward(Am[ma + iz * 9], Am[ma + 3 + iz * 9], Am[ma + 6 + iz * 9], uy_eq);
+  for (int iz = 0; iz < 3; ++iz)
+    for (int iy = 0; iy < 3; ++iy) {
+      int base = iy * 3 + iz * 9;
+      chimera_backward(Am[base], Am[base + 1], Am[base + 2], ux_eq);
+    }
+
+  // positivity limiter (kernel_cumulant.jl:849-884)
+  if (P.limiter_type == 2) {
+    T fmin = Am[0];
+    for (int k = 1; k < Q; ++k) fmin = std::min(fmin, Am[k]);
+    if (fmin < T(0)) {
+      T alpha = T(1);
+      for (int k = 0; k < Q; ++k) {
+        T fe = feq_auto<T>(rho, ux_eq, uy_eq, uz_eq, T(TB.w[k]), T(TB.cx[k]), T(TB.cy[k]), T(TB.cz[k]), comp);
+        T fneq = Am[k] - fe;
+        if (fneq < T(0) && fe > T(1e-15)) alpha = std::min(alpha, fe / (fe - fneq + T(1e-15)));
+      }
+      alpha = std::max(alpha, T(0));
+      for (int k = 0; k < Q; ++k) {
+        T fe = feq_auto<T>(rho, ux_eq, uy_eq, uz_eq, T(TB.w[k]), T(TB.cx[k]), T(TB.cy[k]), T(TB.cz[k]), comp);
+        Am[k] = fe + alpha * (Am[k] - fe);
+      }
+    }
+  }
+
+  // STEP 10: Guo forcing + store (kernel_cumulant.jl:889-908)
+  for (int k = 0; k < Q; ++k) {
+    const T cxf = T(TB.cx[k]), cyf = T(TB.cy[k]), czf = T(TB.cz[k]);
+    const T cu = cxf * ux_eq + cyf * uy_eq + czf * uz_eq;
+    const T force_term = T(TB.w[k]) * T(3) *
+                         ((cxf - ux + T(3) * cu * cxf) * Fx + (cyf - uy + T(3) * cu * cyf) * Fy +
+                          (czf - uz + T(3) * cu * czf) * Fz);
+    const T fc = Am[k] + (T(1) - T(0.5) * omega1) * force_term;
+    if (store_post) f_post[A.f(x, y, z, b, k)] = fc;
+    f_out[A.f(x, y, z, b, k)] = fc;
+  }
+}
+
+template <class T>
+int step_level(const Level& L, const oal_step_params& P, const T* f_in, T* f_out, T* f_post, T* rho_out,
+               T* vel_out, const T* vel_in, double* force_out) {
+  std::vector<double> part((size_t)L.nb * 3, 0.0);
+#pragma omp parallel for schedule(static)
+  for (int b = 0; b < L.nb; ++b) {
+    double acc[3] = {0, 0, 0};
+    for (int z = 0; z < BS; ++z)
+      for (int y = 0; y < BS; ++y)
+        for (int x = 0; x < BS; ++x)
+          step_cell<T>(L, P, f_in, f_out, f_post, rho_out, vel_out, vel_in, b, x, y, z, acc);
+    part[3 * b] = acc[0]; part[3 * b + 1] = acc[1]; part[3 * b + 2] = acc[2];
+  }
+  if (force_out && P.collect_forces) {
+    double s[3] = {0, 0, 0};
+    for (int b = 0; b < L.nb; ++b) { s[0] += part[3 * b]; s[1] += part[3 * b + 1]; s[2] += part[3 * b + 2]; }
+    force_out[0] = s[0]; force_out[1] = s[1]; force_out[2] = s[2];
+  }
+  return 0;
+}
+
+Level make_level(int32_t nb, int32_t nx, int32_t ny, int32_t nz, const int32_t* coords, const int32_t* nbr,
+                 const uint8_t* obstacle, const float* sponge, const float* wall_dist) {
+  return Level{nb, nx, ny, nz, coords, nbr, obstacle, sponge, wall_dist};
+}
+
+}  // namespace
+
+extern "C" {
+
+// D3Q27 tables in the reference order (0-based indices for opp/mirrors).
+void ora_d3q27_tables(int32_t* cx, int32_t* cy, int32_t* cz, double* w, int32_t* opp, int32_t* mir_y,
+                      int32_t* mir_z) {
+  for (int k = 0; k < Q; ++k) {
+    cx[k] = TB.cx[k]; cy[k] = TB.cy[k]; cz[k] = TB.cz[k]; w[k] = TB.w[k];
+    opp[k] = TB.opp[k]; mir_y[k] = TB.mir_y[k]; mir_z[k] = TB.mir_z[k];
+  }
+}
+
+// domain.jl:785 sorted tuples (bx most significant) + domain_topology.jl:919-953 with a wrap
+// on each axis whose bit is set in periodic_mask (the reference wraps y only; a full wrap makes
+// the same kernel a periodic box).
+int ora_build_box(int32_t bxm, int32_t bym, int32_t bzm, int32_t periodic_mask, int32_t* coords, int32_t* nbr) {
+  const int64_t n = (int64_t)bxm * bym * bzm;
+  std::vector<int32_t> ptr((size_t)n, 0);
+  int64_t i = 0;
+  for (int bx = 1; bx <= bxm; ++bx)
+    for (int by = 1; by <= bym; ++by)
+      for (int bz = 1; bz <= bzm; ++bz) {
+        coords[3 * i] = bx; coords[3 * i + 1] = by; coords[3 * i + 2] = bz;
+        ptr[((size_t)(bx - 1) * bym + (by - 1)) * bzm + (bz - 1)] = (int32_t)(i + 1);
+        ++i;
+      }
+  auto wrap = [](int v, int m, bool p) { return p ? (v < 1 ? m : (v > m ? 1 : v)) : v; };
+  for (int64_t b = 0; b < n; ++b) {
+    int bx = coords[3 * b], by = coords[3 * b + 1], bz = coords[3 * b + 2];
+    for (int dz = -1; dz <= 1; ++dz)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          int dir = (dx + 1) + (dy + 1) * 3 + (dz + 1) * 9;
+          int nx = wrap(bx + dx, bxm, periodic_mask & 1);
+          int ny = wrap(by + dy, bym, periodic_mask & 2);
+          int nz = wrap(bz + dz, bzm, periodic_mask & 4);
+          int32_t v = 0;
+          if (nx >= 1 && nx <= bxm && ny >= 1 && ny <= bym && nz >= 1 && nz <= bzm)
+            v = ptr[((size_t)(nx - 1) * bym + (ny - 1)) * bzm + (nz - 1)];
+          nbr[b + n * dir] = v;
+        }
+  }
+  return 0;
+}
+
+// domain_generation.jl:140-150 with dx = 1 (cell units)
+int64_t ora_sphere(int32_t nb, const int32_t* coords, double cx, double cy, double cz, double radius,
+                   uint8_t* obstacle) {
+  const double r2 = radius * radius;
+  int64_t count = 0;
+  for (int b = 0; b < nb; ++b) {
+    int bx = coords[3 * b], by = coords[3 * b + 1], bz = coords[3 * b + 2];
+    for (int lz = 1; lz <= BS; ++lz)
+      for (int ly = 1; ly <= BS; ++ly)
+        for (int lx = 1; lx <= BS; ++lx) {
+          double px = ((bx - 1) * BS + lx - 0.5), py = ((by - 1) * BS + ly - 0.5), pz = ((bz - 1) * BS + lz - 0.5);
+          double d = (px - cx) * (px - cx) + (py - cy) * (py - cy) + (pz - cz) * (pz - cz);
+          uint8_t s = d <= r2 ? 1 : 0;
+          obstacle[(lx - 1) + 8 * (ly - 1) + 64 * (lz - 1) + 512 * (int64_t)b] = s;
+          count += s;
+        }
+  }
+  return count;
+}
+
+// Equilibrium start f = feq(rho, u) (physics_utils.jl:30-35 / :65-95).
+void ora_init_feq_f64(int32_t nb, const double* rho, const double* vel, int32_t comp, double* f) {
+  const int64_t n = 512 * (int64_t)nb;
+  for (int64_t i = 0; i < n; ++i)
+    for (int k = 0; k < Q; ++k)
+      f[i + n * k] = feq_auto<double>(rho[i], vel[i], vel[i + n], vel[i + 2 * n], TB.w[k], TB.cx[k], TB.cy[k],
+                                       TB.cz[k], comp);
+}
+
+int ora_step_d3q27_f64(int32_t nb, int32_t nx, int32_t ny, int32_t nz, const int32_t* coords, const int32_t* nbr,
+                       const uint8_t* obstacle, const float* sponge, const float* wall_dist,
+                       const oal_step_params* P, const double* f_in, double* f_out, double* f_post,
+                       double* rho_out, double* vel_out, const double* vel_in, double* force_out) {
+  Level L = make_level(nb, nx, ny, nz, coords, nbr, obstacle, sponge, wall_dist);
+  return step_level<double>(L, *P, f_in, f_out, f_post, rho_out, vel_out, vel_in, force_out);
+}
+
+int ora_step_d3q27_f32(int32_t nb, int32_t nx, int32_t ny, int32_t nz, const int32_t* coords, const int32_t* nbr,
+                       const uint8_t* obstacle, const float* sponge, const float* wall_dist,
+                       const oal_step_params* P, const float* f_in, float* f_out, float* f_post,
+                       float* rho_out, float* vel_out, const float* vel_in, double* force_out) {
+  Level L = make_level(nb, nx, ny, nz, coords, nbr, obstacle, sponge, wall_dist);
+  return step_level<float>(L, *P, f_in, f_out, f_post, rho_out, vel_out, vel_in, force_out);
+}
+
+// Float64 totals over fluid cells (state.jl:614-637): out = {mass, px, py, pz} from f.
+void ora_mass_momentum_f64(int32_t nb, const uint8_t* obstacle, const double* f, double* out) {
+  const int64_t n = 512 * (int64_t)nb;
+  double m = 0, px = 0, py = 0, pz = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    if (obstacle && obstacle[i]) continue;
+    for (int k = 0; k < Q; ++k) {
+      double v = f[i + n * k];
+      m += v; px += v * TB.cx[k]; py += v * TB.cy[k]; pz += v * TB.cz[k];
+    }
+  }
+  out[0] = m; out[1] = px; out[2] = py; out[3] = pz;
+}
+
+}  // extern "C"
