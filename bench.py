@@ -173,11 +173,11 @@ def reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def workload_config(storage):
-    return {"workload": "sphere_channel_256x128x128_D24_Re1000", "cells": 256 * 128 * 128, "blocks": 8192,
+def workload_config(storage, nz=128):
+    return {"workload": f"sphere_channel_256x128x{nz}_D24_Re1000", "cells": 256 * 128 * nz, "blocks": 32 * 16 * (nz // 8),
             "operator": "cumulant_d3q27", "storage": f"{storage}_dev" if storage in ("f16", "bf16") else storage,
             "c_wale": 0.2, "solid_bc": "halfway", "forces": "FP64 momentum exchange every step",
-            "l2": "inputs larger than L2 (populations 2 x %d MB)" % (256 * 128 * 128 * 27 * STORAGE_BYTES[storage] // 2**20),
+            "l2": "inputs larger than L2 (populations 2 x %d MB)" % (256 * 128 * nz * 27 * STORAGE_BYTES[storage] // 2**20),
             "parallelism": "replicas"}
 
 
@@ -193,6 +193,7 @@ def main():
     ap.add_argument("--storage", default="f16", choices=["f16", "bf16", "f32", "f64"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU-baseline leg")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--nz", type=int, default=128, help="channel depth (smaller values for profiling captures)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -223,7 +224,7 @@ def main():
     from openaerolab_alpha_01_b200.cases import sphere_channel_case
     from openaerolab_alpha_01_b200.solver import Geometry, Level
 
-    case = sphere_channel_case(256, 128, 128, diameter=24.0, centre_x=64.0)
+    case = sphere_channel_case(256, 128, args.nz, diameter=24.0, centre_x=64.0)
     geom = Geometry(case.dom, device=dev)
     level = Level(geom, storage=args.storage)
     level.init_equilibrium(case.rho, case.vel)
@@ -299,7 +300,7 @@ def main():
             "metric": METRIC, "value": round(value, 2), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": workload_config(args.storage),
+            "config": workload_config(args.storage, args.nz),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                          "frac_of_8000": round(achieved / 8000.0, 4),

@@ -18,8 +18,10 @@ INCLUDE = PKG.parent / "include"
 LIB = PKG / "liboal.so"
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# -fmad=false: every fused multiply-add in the kernels is written explicitly, so the one-cell and
+# two-cell (packed f32x2) forms of the collision round identically.
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
-              "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
+              "--expt-relaxed-constexpr", "-fmad=false", "-Xptxas", "-warn-spills"]
 
 
 def nvcc() -> str:

@@ -15,7 +15,11 @@
 
 namespace oal {
 template <class S, class R>
-cudaError_t launch_cumulant(const StepArgs& a, int n_blocks, cudaStream_t st);
+cudaError_t launch_fill_ghosts(const StepArgs& a, const uint2* entries, int64_t n, cudaStream_t st);
+template <class S, class R>
+cudaError_t launch_fast(const StepArgs& a, const int32_t* work, int n_work, cudaStream_t st);
+template <class S, class R>
+cudaError_t launch_general(const StepArgs& a, const int32_t* work, int n_work, cudaStream_t st);
 }
 using namespace oal;
 
@@ -190,7 +194,14 @@ size_t macro_bytes(int32_t storage) { return storage == OAL_STORE_F64 ? 8 : 4; }
 struct oal_geometry {
   int device = 0;
   int32_t nb = 0, nx = 0, ny = 0, nz = 0;
-  int32_t* d_nbr = nullptr;
+  int32_t n_ghost = 0;             // ghost blocks appended after the real ones (library-owned levels)
+  int32_t* d_nbr = nullptr;        // [nb*27] 0-based, -1 = none (caller-owned arrays)
+  int32_t* d_nbr_ghost = nullptr;  // [nb*27] missing neighbours point at ghost blocks
+  uint2* d_gentries = nullptr;     // ghost fill entries (block, cell | k << 9)
+  int64_t n_gentries = 0;
+  int32_t* d_fast = nullptr;       // blocks for the uniform kernel
+  int32_t* d_general = nullptr;    // blocks for the general kernel
+  int32_t n_fast = 0, n_general = 0;
   int4* d_binfo = nullptr;
   uint32_t* d_bflags = nullptr;
   int32_t* d_mslot = nullptr;
@@ -276,12 +287,25 @@ static oal_status resolve_params(const oal_step_params* p, const oal_geometry* g
   return OAL_OK;
 }
 
-static cudaError_t launch_by_storage(int32_t storage, const StepArgs& a, int nb, cudaStream_t st) {
+// Which kernels one step launches.
+enum StepPath { PATH_PLAIN = 0, PATH_GHOSTED = 1 };
+
+template <class S, class R>
+static cudaError_t launch_step_t(const oal_geometry* g, const StepArgs& a, StepPath path, cudaStream_t st) {
+  cudaError_t e;
+  if (path == PATH_PLAIN) return launch_general<S, R>(a, nullptr, g->nb, st);
+  if ((e = launch_fill_ghosts<S, R>(a, g->d_gentries, g->n_gentries, st)) != cudaSuccess) return e;
+  if ((e = launch_fast<S, R>(a, g->d_fast, g->n_fast, st)) != cudaSuccess) return e;
+  return launch_general<S, R>(a, g->d_general, g->n_general, st);
+}
+
+static cudaError_t launch_by_storage(int32_t storage, const oal_geometry* g, const StepArgs& a, StepPath path,
+                                     cudaStream_t st) {
   switch (storage) {
-    case OAL_STORE_F32: return launch_cumulant<float, float>(a, nb, st);
-    case OAL_STORE_F16_DEV: return launch_cumulant<__half, float>(a, nb, st);
-    case OAL_STORE_BF16_DEV: return launch_cumulant<__nv_bfloat16, float>(a, nb, st);
-    case OAL_STORE_F64: return launch_cumulant<double, double>(a, nb, st);
+    case OAL_STORE_F32: return launch_step_t<float, float>(g, a, path, st);
+    case OAL_STORE_F16_DEV: return launch_step_t<__half, float>(g, a, path, st);
+    case OAL_STORE_BF16_DEV: return launch_step_t<__nv_bfloat16, float>(g, a, path, st);
+    case OAL_STORE_F64: return launch_step_t<double, double>(g, a, path, st);
   }
   return cudaErrorInvalidValue;
 }
@@ -546,6 +570,58 @@ oal_status oal_geometry_create(const oal_geometry_desc* d, int32_t device, oal_g
   for (int64_t b = 0; b < nb; ++b)
     if (!(bflags[(size_t)b] & BF_INTERIOR)) ++g->n_boundary;
 
+  // Ghost blocks: every missing neighbour position gets a block appended after the real ones; the
+  // fill kernel writes into it, before each step, exactly the populations that real cells pull
+  // from it, so the step kernels pull uniformly. A ghost slot (cell g, direction k) feeds the
+  // single destination g + c_k, so no two entries write the same slot.
+  std::vector<int32_t> nbrg(nbr0);
+  std::vector<uint2> gentries;
+  {
+    std::vector<int64_t> keys;  // packed ghost block coordinates, index = ghost id
+    auto pack = [](int64_t bx, int64_t by, int64_t bz) { return ((bx + 4) << 42) | ((by + 4) << 21) | (bz + 4); };
+    std::vector<std::pair<int64_t, int32_t>> lookup;
+    for (int64_t b = 0; b < nb; ++b)
+      for (int dir = 0; dir < 27; ++dir) {
+        if (nbr0[(size_t)b * 27 + dir] >= 0) continue;
+        const int64_t key = pack(binfo[b].x + dir % 3 - 1, binfo[b].y + (dir / 3) % 3 - 1, binfo[b].z + dir / 9 - 1);
+        keys.push_back(key);
+      }
+    std::sort(keys.begin(), keys.end());
+    keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+    g->n_ghost = (int32_t)keys.size();
+    for (int64_t b = 0; b < nb; ++b)
+      for (int dir = 0; dir < 27; ++dir) {
+        if (nbr0[(size_t)b * 27 + dir] >= 0) continue;
+        const int64_t key = pack(binfo[b].x + dir % 3 - 1, binfo[b].y + (dir / 3) % 3 - 1, binfo[b].z + dir / 9 - 1);
+        const int64_t gi = std::lower_bound(keys.begin(), keys.end(), key) - keys.begin();
+        nbrg[(size_t)b * 27 + dir] = (int32_t)(nb + gi);
+      }
+    for (int64_t b = 0; b < nb; ++b) {
+      if (bflags[(size_t)b] & BF_INTERIOR) continue;
+      for (int cell = 0; cell < 512; ++cell) {
+        const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
+        for (int k = 0; k < 27; ++k) {
+          const int sx = x - q27_cx(k), sy = y - q27_cy(k), sz = z - q27_cz(k);
+          if (nbr0[(size_t)b * 27 + nbr_dir(sx >> 3, sy >> 3, sz >> 3)] < 0)
+            gentries.push_back(make_uint2((uint32_t)b, (uint32_t)cell | ((uint32_t)k << 9)));
+        }
+      }
+    }
+  }
+  g->n_gentries = (int64_t)gentries.size();
+  // Work lists: blocks near solids, with sponge cells or with wall distances take the general kernel.
+  std::vector<int32_t> fast, general;
+  for (int64_t b = 0; b < nb; ++b) {
+    bool gen = (bflags[(size_t)b] & BF_NEAR_SOLID) != 0;
+    for (int c = 0; c < 512 && !gen; ++c) {
+      if (d->sponge && d->sponge[b * 512 + c] > 0.0f) gen = true;
+      if (d->wall_dist && d->wall_dist[b * 512 + c] > 0.0f) gen = true;
+    }
+    (gen ? general : fast).push_back((int32_t)b);
+  }
+  g->n_fast = (int32_t)fast.size();
+  g->n_general = (int32_t)general.size();
+
   auto fail = [&](oal_status s) { oal_geometry_destroy(g); return s; };
 #define GTRY(expr)                                                                         \
   do {                                                                                     \
@@ -574,6 +650,20 @@ oal_status oal_geometry_create(const oal_geometry_desc* d, int32_t device, oal_g
     GTRY(cudaMalloc(&g->d_wdist, (size_t)nb * 512 * sizeof(float)));
     GTRY(cudaMemcpy(g->d_wdist, d->wall_dist, (size_t)nb * 512 * sizeof(float), cudaMemcpyHostToDevice));
   }
+  GTRY(cudaMalloc(&g->d_nbr_ghost, nbrg.size() * sizeof(int32_t)));
+  GTRY(cudaMemcpy(g->d_nbr_ghost, nbrg.data(), nbrg.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  if (!gentries.empty()) {
+    GTRY(cudaMalloc(&g->d_gentries, gentries.size() * sizeof(uint2)));
+    GTRY(cudaMemcpy(g->d_gentries, gentries.data(), gentries.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+  }
+  if (!fast.empty()) {
+    GTRY(cudaMalloc(&g->d_fast, fast.size() * sizeof(int32_t)));
+    GTRY(cudaMemcpy(g->d_fast, fast.data(), fast.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  }
+  if (!general.empty()) {
+    GTRY(cudaMalloc(&g->d_general, general.size() * sizeof(int32_t)));
+    GTRY(cudaMemcpy(g->d_general, general.data(), general.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  }
   GTRY(cudaMalloc(&g->d_force_part, (size_t)nb * 4 * 3 * sizeof(double)));
   GTRY(cudaMalloc(&g->d_force, 3 * sizeof(double)));
   GTRY(cudaMemset(g->d_force, 0, 3 * sizeof(double)));
@@ -585,6 +675,7 @@ oal_status oal_geometry_create(const oal_geometry_desc* d, int32_t device, oal_g
 void oal_geometry_destroy(oal_geometry* g) {
   if (!g) return;
   cudaSetDevice(g->device);
+  cudaFree(g->d_nbr_ghost); cudaFree(g->d_gentries); cudaFree(g->d_fast); cudaFree(g->d_general);
   cudaFree(g->d_nbr); cudaFree(g->d_binfo); cudaFree(g->d_bflags); cudaFree(g->d_mslot);
   cudaFree(g->d_cmask); cudaFree(g->d_sponge); cudaFree(g->d_wdist);
   cudaFree(g->d_force_part); cudaFree(g->d_force);
@@ -617,7 +708,7 @@ oal_status oal_stream_collide(const oal_geometry* g, const oal_level_fields* fl,
   a.force_part = g->d_force_part;
   a.p0 = cp;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  OAL_CUDA_TRY(launch_by_storage(fl->storage, a, g->nb, st));
+  OAL_CUDA_TRY(launch_by_storage(fl->storage, g, a, PATH_PLAIN, st));
   if ((cp.flags & CF_COLLECT) && fl->force_out) {
     k_reduce3<<<1, 256, 0, st>>>(g->d_force_part, (int64_t)g->nb * 4, fl->force_out);
     OAL_CUDA_TRY(cudaGetLastError());
@@ -635,7 +726,8 @@ oal_status oal_level_create(const oal_geometry* g, int32_t op, int32_t storage, 
   auto* L = new oal_level();
   L->g = g; L->op = op; L->storage = storage;
   const int64_t ncell = (int64_t)g->nb * 512;
-  const size_t fbytes = (size_t)ncell * 27 * storage_bytes(storage);
+  // populations of the real blocks followed by the ghost blocks
+  const size_t fbytes = (size_t)(g->nb + g->n_ghost) * 512 * 27 * storage_bytes(storage);
   const size_t mb = macro_bytes(storage);
   auto fail = [&](cudaError_t e) {
     oal_level_destroy(L);
@@ -645,6 +737,7 @@ oal_status oal_level_create(const oal_geometry* g, int32_t op, int32_t storage, 
   cudaError_t e;
   for (int i = 0; i < 2; ++i) {
     if ((e = cudaMalloc(&L->f[i], fbytes)) != cudaSuccess) return fail(e);
+    if ((e = cudaMemset(L->f[i], 0, fbytes)) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&L->vel[i], (size_t)ncell * 3 * mb)) != cudaSuccess) return fail(e);
     if ((e = cudaMemset(L->vel[i], 0, (size_t)ncell * 3 * mb)) != cudaSuccess) return fail(e);
   }
@@ -766,16 +859,22 @@ static oal_status enqueue_step(oal_level* L, const CaseParams& cp, cudaStream_t 
   int64_t bst, kst;
   level_layout(L, &bst, &kst);
   const int p = L->parity;
+  a.nbr = g->d_nbr_ghost;
   a.f_in = L->f[p]; a.f_out = L->f[p ^ 1]; a.f_post = nullptr;
   a.rho_out = L->rho; a.vel_out = L->vel[p ^ 1]; a.vel_in = L->vel[p];
   a.f_bstride = bst; a.f_kstride = kst;
   a.v_bstride = 512; a.v_cstride = 512 * (int64_t)g->nb;
   a.force_part = L->d_force_part;
   a.p0 = cp;
-  OAL_CUDA_TRY(launch_by_storage(L->storage, a, g->nb, st));
+  OAL_CUDA_TRY(launch_by_storage(L->storage, g, a, PATH_GHOSTED, st));
   if (cp.flags & CF_COLLECT) {
-    k_reduce3<<<1, 256, 0, st>>>(L->d_force_part, (int64_t)g->nb * 4, L->d_force);
-    OAL_CUDA_TRY(cudaGetLastError());
+    // the momentum exchange lives on the general kernel's CTAs (blocks near solids)
+    if (g->n_general > 0) {
+      k_reduce3<<<1, 256, 0, st>>>(L->d_force_part, (int64_t)g->n_general * 4, L->d_force);
+      OAL_CUDA_TRY(cudaGetLastError());
+    } else {
+      OAL_CUDA_TRY(cudaMemsetAsync(L->d_force, 0, 3 * sizeof(double), st));
+    }
     L->forces_valid = true;
   }
   L->parity ^= 1;

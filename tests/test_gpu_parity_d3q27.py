@@ -71,15 +71,19 @@ def channel():
     return sphere_channel_case(32, 16, 16, diameter=6.0, centre_x=10.0, u_inlet=0.05, re=100.0)
 
 
-@pytest.mark.parametrize("storage,dtype,tol,ftol", [("f64", np.float64, 1e-11, 1e-10), ("f32", np.float32, 2e-5, 1e-4),
-                                                    ("f16", np.float64, 2e-3, 5e-3), ("bf16", np.float64, 2e-2, 5e-2)])
-def test_sphere_channel_halfway_drag(oal, oracle_lib, channel, storage, dtype, tol, ftol):
+@pytest.mark.parametrize("storage,dtype,tol,ftol,sym", [("f64", np.float64, 1e-11, 1e-10, 1e-9),
+                                                        ("f32", np.float32, 2e-5, 1e-4, 1e-4),
+                                                        ("f16", np.float64, 2e-3, 5e-3, 1e-3),
+                                                        ("bf16", np.float64, 2e-2, 5e-2, 1e-2)])
+def test_sphere_channel_halfway_drag(oal, oracle_lib, channel, storage, dtype, tol, ftol, sym):
     steps = 30
     f, rho, vel, force, _ = run_gpu(channel, storage, steps)
     O = run_oracle(oracle_lib, channel, steps, dtype)
     assert rel(f, O.f) < tol
     assert abs(force[0] - O.force[0]) / abs(O.force[0]) < ftol
-    assert abs(force[1]) < 1e-3 * abs(force[0]) + 1e-12
+    # the sphere is centred in y and z: the side forces vanish up to storage rounding
+    assert abs(force[1]) < sym * abs(force[0]) + 1e-12
+    assert abs(force[2]) < sym * abs(force[0]) + 1e-12
 
 
 VARIANTS = {
