@@ -38,10 +38,15 @@ static oal_status set_error(oal_status s, const char* fmt, ...) {
   return s;
 }
 
+// error hook for the other translation units of the library
+oal_status oal_internal_set_error(oal_status s, const char* msg) { return set_error(s, "%s", msg); }
+
+// On failure the runtime's (non-sticky) last error is consumed, so it is not reported again by a
+// later call's launch check.
 #define OAL_CUDA_TRY(expr)                                                                           \
   do {                                                                                               \
     cudaError_t _e = (expr);                                                                         \
-    if (_e != cudaSuccess)                                                                           \
+    if (_e != cudaSuccess && (cudaGetLastError(), true))                                             \
       return set_error(_e == cudaErrorMemoryAllocation ? OAL_E_OUT_OF_MEMORY : OAL_E_CUDA, "%s: %s (%s:%d)", \
                        #expr, cudaGetErrorString(_e), __FILE__, __LINE__);                           \
   } while (0)
@@ -211,6 +216,10 @@ struct oal_geometry {
   double* d_force_part = nullptr;  // scratch of oal_stream_collide
   double* d_force = nullptr;
   int64_t n_fluid = 0, n_solid = 0, n_boundary = 0, n_slots = 0;
+  // levels built on this geometry; destroying the geometry while levels live defers the release
+  // to the last level's destroy
+  int32_t n_levels = 0;
+  bool destroy_requested = false;
 };
 
 struct GraphCache {
@@ -223,6 +232,7 @@ struct GraphCache {
 
 struct oal_level {
   const oal_geometry* g = nullptr;
+  int device = 0;
   int32_t op = 0, storage = 0;
   void* f[2] = {nullptr, nullptr};
   void* vel[2] = {nullptr, nullptr};
@@ -672,14 +682,20 @@ oal_status oal_geometry_create(const oal_geometry_desc* d, int32_t device, oal_g
   return OAL_OK;
 }
 
-void oal_geometry_destroy(oal_geometry* g) {
-  if (!g) return;
+static void geometry_release(oal_geometry* g) {
   cudaSetDevice(g->device);
   cudaFree(g->d_nbr_ghost); cudaFree(g->d_gentries); cudaFree(g->d_fast); cudaFree(g->d_general);
   cudaFree(g->d_nbr); cudaFree(g->d_binfo); cudaFree(g->d_bflags); cudaFree(g->d_mslot);
   cudaFree(g->d_cmask); cudaFree(g->d_sponge); cudaFree(g->d_wdist);
   cudaFree(g->d_force_part); cudaFree(g->d_force);
+  cudaGetLastError();
   delete g;
+}
+
+void oal_geometry_destroy(oal_geometry* g) {
+  if (!g) return;
+  if (g->n_levels > 0) { g->destroy_requested = true; return; }
+  geometry_release(g);
 }
 
 oal_status oal_geometry_info(const oal_geometry* g, int64_t out[5]) {
@@ -724,7 +740,8 @@ oal_status oal_level_create(const oal_geometry* g, int32_t op, int32_t storage, 
   if (storage < OAL_STORE_F32 || storage > OAL_STORE_F64) return set_error(OAL_E_INVALID_ARG, "storage %d", storage);
   OAL_CUDA_TRY(cudaSetDevice(g->device));
   auto* L = new oal_level();
-  L->g = g; L->op = op; L->storage = storage;
+  L->g = g; L->device = g->device; L->op = op; L->storage = storage;
+  ++const_cast<oal_geometry*>(g)->n_levels;
   const int64_t ncell = (int64_t)g->nb * 512;
   // populations of the real blocks followed by the ghost blocks
   const size_t fbytes = (size_t)(g->nb + g->n_ghost) * 512 * 27 * storage_bytes(storage);
@@ -761,12 +778,15 @@ static void release_graph(oal_level* L) {
 
 void oal_level_destroy(oal_level* L) {
   if (!L) return;
-  cudaSetDevice(L->g->device);
+  cudaSetDevice(L->device);
   release_graph(L);
   for (int i = 0; i < 2; ++i) { cudaFree(L->f[i]); cudaFree(L->vel[i]); }
   cudaFree(L->rho); cudaFree(L->d_force_part); cudaFree(L->d_force); cudaFree(L->d_mm_part); cudaFree(L->d_mm);
   if (L->cap) cudaStreamDestroy(L->cap);
+  cudaGetLastError();  // teardown leaves no error behind for the next call
+  auto* g = const_cast<oal_geometry*>(L->g);
   delete L;
+  if (g && --g->n_levels == 0 && g->destroy_requested) geometry_release(g);
 }
 
 oal_status oal_level_init_equilibrium(oal_level* L, const double* rho, const double* vel, int32_t comp) {

@@ -153,6 +153,7 @@ class Geometry:
         return dict(n_blocks=out[0], fluid_cells=out[1], solid_cells=out[2], boundary_blocks=out[3], mask_blocks=out[4])
 
     def close(self):
+        # the library defers the release while levels built on this geometry are alive
         if getattr(self, "handle", None):
             lib().oal_geometry_destroy(self.handle)
             self.handle = None
