@@ -240,6 +240,21 @@ oal_status oal_level_device_state(oal_level* L, void** f, void** rho, void** vel
 /* Bytes of device memory this level holds. */
 int64_t oal_level_device_bytes(const oal_level* L);
 
+/* ---- no-allocation entry point -------------------------------------------------------------- */
+/* No counterpart in the reference. For callers that cannot call cudaMalloc when they need the
+ * totals (a step recorded into a CUDA graph, a stream-ordered pool that forbids stray
+ * allocations, a host runtime that must not grow device memory between steps): FP64 {mass, px,
+ * py, pz} of the fluid cells of caller-owned populations, with the per-block partial sums kept in
+ * a fixed file-scope device array of OAL_NOALLOC_MAX_BLOCKS blocks (2 MiB, held by every GPU that
+ * loads the library until the process exits). f: device populations (storage type, element
+ * strides as in oal_level_fields); obstacle: device uint8[512*n_blocks] or NULL; out: device
+ * double[4]. n_blocks above the maximum returns OAL_E_TOO_LARGE. The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress) and should come before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race and must be serialised. */
+#define OAL_NOALLOC_MAX_BLOCKS 65536
+oal_status oal_mass_momentum_noalloc(const void* f, int32_t storage, int64_t f_block_stride, int64_t f_dir_stride,
+                                     const uint8_t* obstacle, int32_t n_blocks, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -151,7 +151,11 @@ _SIGNATURES = {
     "oal_level_device_state": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                            C.POINTER(C.c_void_p)]),
     "oal_level_device_bytes": (C.c_int64, [C.c_void_p]),
+    "oal_mass_momentum_noalloc": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int64, C.c_int64, C.c_void_p, C.c_int32,
+                                              C.c_void_p, C.c_void_p]),
 }
+
+OAL_NOALLOC_MAX_BLOCKS = 65536
 
 _lib = None
 
