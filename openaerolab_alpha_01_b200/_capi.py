@@ -10,7 +10,8 @@ import os
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
-LIB_PATH = PKG / "liboal.so"
+# OAL_LIBRARY selects another build of the library (for instance a tuning variant)
+LIB_PATH = Path(os.environ.get("OAL_LIBRARY", str(PKG / "liboal.so")))
 
 OAL_ABI_VERSION = 1
 

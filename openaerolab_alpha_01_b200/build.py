@@ -42,12 +42,15 @@ def _stale(target: Path, deps: list[Path]) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
-def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> Path:
-    """Compile the CUDA sources into liboal.so (objects under csrc/_build/)."""
+def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None,
+          out: Path | None = None, objdir: Path | None = None) -> Path:
+    """Compile the CUDA sources into liboal.so (objects under csrc/_build/), or into `out` with
+    extra nvcc flags (tuning variants)."""
     srcs = sources()
     headers = list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
-    objdir = CSRC / "_build"
-    objdir.mkdir(exist_ok=True)
+    lib = Path(out) if out else LIB
+    objdir = Path(objdir) if objdir else CSRC / "_build"
+    objdir.mkdir(parents=True, exist_ok=True)
     objs = []
     procs = []
     for s in srcs:
@@ -64,12 +67,12 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
             sys.stdout.write(out)
         if p.returncode != 0:
             raise RuntimeError(f"nvcc failed on {s.name}:\n{out}")
-    if force or _stale(LIB, objs):
-        cmd = [nvcc(), *ARCH_FLAGS, "-shared", "-o", str(LIB), *map(str, objs)]
+    if force or _stale(lib, objs):
+        cmd = [nvcc(), *ARCH_FLAGS, "-shared", "-o", str(lib), *map(str, objs)]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}{r.stderr}")
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":

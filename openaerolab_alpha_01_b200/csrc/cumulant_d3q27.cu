@@ -25,6 +25,15 @@
 #include "vmath.cuh"
 #include "cumulant_math.cuh"
 
+// Tuning knobs of the uniform kernel (compile time): resident CTAs per SM the register budget
+// is sized for, and cells per thread (2 = packed f32x2 pairs, 1 = scalar float).
+#ifndef OAL_FAST_MIN_CTAS
+#define OAL_FAST_MIN_CTAS 3
+#endif
+#ifndef OAL_FAST_CELLS
+#define OAL_FAST_CELLS 2
+#endif
+
 namespace oal {
 
 // physics_utils.jl:5-17
@@ -43,11 +52,11 @@ __device__ __forceinline__ R dec_k(const S* __restrict__ f, int64_t i, int k) {
 
 // Population arriving at cell (x,y,z) of block b in direction k from outside every block
 // (kernel_cumulant.jl:221-391), level without parent. `nbr` is the block's 27-entry row; entries
-// >= n_real are ghost blocks, which count as missing here.
+// >= n_real are ghost blocks, which count as missing here. k may be a run-time value.
 template <class S, class R>
-__device__ __noinline__ R face_population(const S* __restrict__ fin, int64_t bbase, int cell, int64_t kst,
-                                           const int32_t* nbr, int n_real, int64_t bst, int k, int x, int y, int z,
-                                           int gx, int gy, int gz, const CaseParams& cp) {
+__device__ __forceinline__ R face_population_impl(const S* __restrict__ fin, int64_t bbase, int cell, int64_t kst,
+                                                  const int32_t* nbr, int n_real, int64_t bst, int k, int x, int y,
+                                                  int z, int gx, int gy, int gz, const CaseParams& cp) {
   const int64_t own = bbase + cell;
   const int cx = q27_cx(k), cy = q27_cy(k), cz = q27_cz(k);
   const int src_gx = gx - cx, src_gy = gy - cy, src_gz = gz - cz;
@@ -62,28 +71,50 @@ __device__ __noinline__ R face_population(const S* __restrict__ fin, int64_t bba
     const R u_inst = R(cp.u_inlet) + R(noise);
     return feq_k<R>(k, R(1), u_inst, R(0), R(0), comp);
   }
-  if (is_outlet) return dec_k<S, R>(fin, own + k * kst, k);
-  if ((cp.flags & (CF_ZWALL_SLIP | CF_ZWALL_NOSLIP)) && (is_z_min || is_z_max)) {
-    if (cp.flags & CF_ZWALL_NOSLIP) return dec_k<S, R>(fin, own + q27_opp(k) * kst, q27_opp(k));
-    const int zw_k = q27_mir_z(k);
-    const int zw_ix = x - cx, zw_iy = y - cy;
-    if (zw_ix >= 0 && zw_ix < kBS && zw_iy >= 0 && zw_iy < kBS)
-      return dec_k<S, R>(fin, bbase + (zw_ix + 8 * zw_iy + 64 * z) + zw_k * kst, zw_k);
-    const int zw_nb = nbr[nbr_dir(zw_ix >> 3, zw_iy >> 3, 0)];
-    if (zw_nb >= 0 && zw_nb < n_real)
-      return dec_k<S, R>(fin, (int64_t)zw_nb * bst + zw_k * kst + ((zw_ix & 7) + 8 * (zw_iy & 7) + 64 * z), zw_k);
-    return dec_k<S, R>(fin, own + zw_k * kst, zw_k);
+  int j = k;             // own-cell direction that supplies the value, or
+  int64_t src = -1;      // another cell's element (z-wall slip image)
+  bool blend = false;    // transverse freestream
+  if (is_outlet) {
+    j = k;
+  } else if ((cp.flags & (CF_ZWALL_SLIP | CF_ZWALL_NOSLIP)) && (is_z_min || is_z_max)) {
+    if (cp.flags & CF_ZWALL_NOSLIP) {
+      j = q27_opp(k);
+    } else {
+      j = q27_mir_z(k);
+      const int zw_ix = x - cx, zw_iy = y - cy;
+      if (zw_ix >= 0 && zw_ix < kBS && zw_iy >= 0 && zw_iy < kBS) {
+        src = bbase + (zw_ix + 8 * zw_iy + 64 * z) + j * kst;
+      } else {
+        const int zw_nb = nbr[nbr_dir(zw_ix >> 3, zw_iy >> 3, 0)];
+        if (zw_nb >= 0 && zw_nb < n_real) src = (int64_t)zw_nb * bst + j * kst + ((zw_ix & 7) + 8 * (zw_iy & 7) + 64 * z);
+      }
+    }
+  } else if ((cp.flags & CF_TRANSVERSE_FS) && (is_y_min || is_y_max || is_z_min || is_z_max)) {
+    j = k;
+    blend = true;
+  } else if (is_y_min && (cp.flags & CF_YMIN_WALL)) {
+    j = q27_opp(k);
+  } else if (is_y_min || is_y_max) {
+    j = q27_mir_y(k);
+  } else if (is_z_min || is_z_max) {
+    j = q27_mir_z(k);
+  } else {
+    return R(q27_w(k));  // kernel_cumulant.jl:389-391
   }
-  if ((cp.flags & CF_TRANSVERSE_FS) && (is_y_min || is_y_max || is_z_min || is_z_max)) {
-    const R beta = R(cp.transverse_blend);
-    const R donor = dec_k<S, R>(fin, own + k * kst, k);
-    const R fe = feq_k<R>(k, R(1), R(cp.u_inlet), R(0), R(0), comp);
-    return vfma(R(1) - beta, donor, beta * fe);
-  }
-  if (is_y_min && (cp.flags & CF_YMIN_WALL)) return dec_k<S, R>(fin, own + q27_opp(k) * kst, q27_opp(k));
-  if (is_y_min || is_y_max) return dec_k<S, R>(fin, own + q27_mir_y(k) * kst, q27_mir_y(k));
-  if (is_z_min || is_z_max) return dec_k<S, R>(fin, own + q27_mir_z(k) * kst, q27_mir_z(k));
-  return R(q27_w(k));  // kernel_cumulant.jl:389-391
+  const R v = dec_k<S, R>(fin, src >= 0 ? src : own + j * kst, j);
+  if (!blend) return v;
+  const R beta = R(cp.transverse_blend);
+  const R fe = feq_k<R>(k, R(1), R(cp.u_inlet), R(0), R(0), comp);
+  return vfma(R(1) - beta, v, beta * fe);
+}
+
+// The general kernel calls the face logic from 27 unrolled sites; one out-of-line copy keeps
+// its code small.
+template <class S, class R>
+__device__ __noinline__ R face_population(const S* __restrict__ fin, int64_t bbase, int cell, int64_t kst,
+                                           const int32_t* nbr, int n_real, int64_t bst, int k, int x, int y, int z,
+                                           int gx, int gy, int gz, const CaseParams& cp) {
+  return face_population_impl<S, R>(fin, bbase, cell, kst, nbr, n_real, bst, k, x, y, z, gx, gy, gz, cp);
 }
 
 __device__ __forceinline__ const CaseParams& case_of(const StepArgs& a, int case_id) {
@@ -107,25 +138,12 @@ __global__ void __launch_bounds__(256) k_fill_ghosts(const StepArgs a, const uin
   const int32_t* nbr = a.nbr + (int64_t)b * 27;
   const int64_t bst = a.f_bstride, kst = a.f_kstride;
   const int gx = (bi.x - 1) * kBS + x + 1, gy = (bi.y - 1) * kBS + y + 1, gz = (bi.z - 1) * kBS + z + 1;
-  switch (k) {
-#define OAL_FILL_CASE(K)                                                                                       \
-  case K: {                                                                                                    \
-    const R val = face_population<S, R>(f, (int64_t)b * bst, cell, kst, nbr, a.n_blocks, bst, K, x, y, z, gx, gy, \
-                                        gz, cp);                                                               \
-    const int sx = x - q27_cx(K), sy = y - q27_cy(K), sz = z - q27_cz(K);                                      \
-    const int g = nbr[nbr_dir(sx >> 3, sy >> 3, sz >> 3)];                                                     \
-    f[(int64_t)g * bst + K * kst + ((sx & 7) | ((sy & 7) << 3) | ((sz & 7) << 6))] =                           \
-        Codec<S>::enc(val, R(q27_w(K)), R(1.0 / q27_w(K)));                                                    \
-    break;                                                                                                     \
-  }
-    OAL_FILL_CASE(0) OAL_FILL_CASE(1) OAL_FILL_CASE(2) OAL_FILL_CASE(3) OAL_FILL_CASE(4) OAL_FILL_CASE(5)
-    OAL_FILL_CASE(6) OAL_FILL_CASE(7) OAL_FILL_CASE(8) OAL_FILL_CASE(9) OAL_FILL_CASE(10) OAL_FILL_CASE(11)
-    OAL_FILL_CASE(12) OAL_FILL_CASE(14) OAL_FILL_CASE(15) OAL_FILL_CASE(16) OAL_FILL_CASE(17)
-    OAL_FILL_CASE(18) OAL_FILL_CASE(19) OAL_FILL_CASE(20) OAL_FILL_CASE(21) OAL_FILL_CASE(22) OAL_FILL_CASE(23)
-    OAL_FILL_CASE(24) OAL_FILL_CASE(25) OAL_FILL_CASE(26)
-#undef OAL_FILL_CASE
-    default: break;
-  }
+  const R val = face_population_impl<S, R>(f, (int64_t)b * bst, cell, kst, nbr, a.n_blocks, bst, k, x, y, z, gx, gy,
+                                           gz, cp);
+  const int sx = x - q27_cx(k), sy = y - q27_cy(k), sz = z - q27_cz(k);
+  const int g = nbr[nbr_dir(sx >> 3, sy >> 3, sz >> 3)];
+  f[(int64_t)g * bst + k * kst + ((sx & 7) | ((sy & 7) << 3) | ((sz & 7) << 6))] =
+      Codec<S>::enc(val, R(q27_w(k)), R(1.0 / q27_w(k)));
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -160,7 +178,7 @@ __device__ __forceinline__ void store2(S* __restrict__ f, int64_t i0, int64_t i1
 }
 
 template <class S, class V>
-__global__ void __launch_bounds__(128) k_cumulant_fast(const StepArgs a, const int32_t* __restrict__ work) {
+__global__ void __launch_bounds__(128, OAL_FAST_MIN_CTAS) k_cumulant_fast(const StepArgs a, const int32_t* __restrict__ work) {
   constexpr int NL = Lane<V>::N;  // cells per thread
   constexpr int CPB = 4 / NL;     // CTAs per block
   using T = SC<V>;
@@ -504,6 +522,8 @@ cudaError_t launch_fast(const StepArgs& a, const int32_t* work, int n_work, cuda
   if (n_work <= 0) return cudaSuccess;
   if constexpr (sizeof(R) == 8) {
     k_cumulant_fast<S, double><<<(unsigned)n_work * 4u, 128, 0, st>>>(a, work);
+  } else if constexpr (OAL_FAST_CELLS == 1) {
+    k_cumulant_fast<S, float><<<(unsigned)n_work * 4u, 128, 0, st>>>(a, work);
   } else {
     k_cumulant_fast<S, F2><<<(unsigned)n_work * 2u, 128, 0, st>>>(a, work);
   }

@@ -222,6 +222,13 @@ struct oal_geometry {
   bool destroy_requested = false;
 };
 
+// Stream resources of an overlapped step: the general kernel (blocks at solids, sponge, wall
+// model) runs on `side` while the uniform kernel runs on the caller's stream.
+struct Overlap {
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+
 struct GraphCache {
   cudaGraphExec_t exec = nullptr;
   cudaGraph_t graph = nullptr;
@@ -244,6 +251,7 @@ struct oal_level {
   int parity = 0;
   int64_t bytes = 0;
   cudaStream_t cap = nullptr;
+  Overlap ov;
   GraphCache gc;
   bool forces_valid = false;
 };
@@ -301,21 +309,31 @@ static oal_status resolve_params(const oal_step_params* p, const oal_geometry* g
 enum StepPath { PATH_PLAIN = 0, PATH_GHOSTED = 1 };
 
 template <class S, class R>
-static cudaError_t launch_step_t(const oal_geometry* g, const StepArgs& a, StepPath path, cudaStream_t st) {
+static cudaError_t launch_step_t(const oal_geometry* g, const StepArgs& a, StepPath path, cudaStream_t st,
+                                 const Overlap* ov) {
   cudaError_t e;
   if (path == PATH_PLAIN) return launch_general<S, R>(a, nullptr, g->nb, st);
   if ((e = launch_fill_ghosts<S, R>(a, g->d_gentries, g->n_gentries, st)) != cudaSuccess) return e;
+  const bool fork = ov && ov->side && g->n_general > 0 && g->n_fast > 0;
+  if (fork) {
+    if ((e = cudaEventRecord(ov->fork, st)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(ov->side, ov->fork, 0)) != cudaSuccess) return e;
+    if ((e = launch_general<S, R>(a, g->d_general, g->n_general, ov->side)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(ov->join, ov->side)) != cudaSuccess) return e;
+    if ((e = launch_fast<S, R>(a, g->d_fast, g->n_fast, st)) != cudaSuccess) return e;
+    return cudaStreamWaitEvent(st, ov->join, 0);
+  }
   if ((e = launch_fast<S, R>(a, g->d_fast, g->n_fast, st)) != cudaSuccess) return e;
   return launch_general<S, R>(a, g->d_general, g->n_general, st);
 }
 
 static cudaError_t launch_by_storage(int32_t storage, const oal_geometry* g, const StepArgs& a, StepPath path,
-                                     cudaStream_t st) {
+                                     cudaStream_t st, const Overlap* ov = nullptr) {
   switch (storage) {
-    case OAL_STORE_F32: return launch_step_t<float, float>(g, a, path, st);
-    case OAL_STORE_F16_DEV: return launch_step_t<__half, float>(g, a, path, st);
-    case OAL_STORE_BF16_DEV: return launch_step_t<__nv_bfloat16, float>(g, a, path, st);
-    case OAL_STORE_F64: return launch_step_t<double, double>(g, a, path, st);
+    case OAL_STORE_F32: return launch_step_t<float, float>(g, a, path, st, ov);
+    case OAL_STORE_F16_DEV: return launch_step_t<__half, float>(g, a, path, st, ov);
+    case OAL_STORE_BF16_DEV: return launch_step_t<__nv_bfloat16, float>(g, a, path, st, ov);
+    case OAL_STORE_F64: return launch_step_t<double, double>(g, a, path, st, ov);
   }
   return cudaErrorInvalidValue;
 }
@@ -765,6 +783,9 @@ oal_status oal_level_create(const oal_geometry* g, int32_t op, int32_t storage, 
   if ((e = cudaMalloc(&L->d_mm_part, (size_t)g->nb * 4 * sizeof(double))) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&L->d_mm, 4 * sizeof(double))) != cudaSuccess) return fail(e);
   if ((e = cudaStreamCreateWithFlags(&L->cap, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+  if ((e = cudaStreamCreateWithFlags(&L->ov.side, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+  if ((e = cudaEventCreateWithFlags(&L->ov.fork, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
+  if ((e = cudaEventCreateWithFlags(&L->ov.join, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
   L->bytes = (int64_t)(2 * fbytes + ncell * 7 * mb + g->nb * 16 * 8 + 56);
   *out = L;
   return OAL_OK;
@@ -783,6 +804,9 @@ void oal_level_destroy(oal_level* L) {
   for (int i = 0; i < 2; ++i) { cudaFree(L->f[i]); cudaFree(L->vel[i]); }
   cudaFree(L->rho); cudaFree(L->d_force_part); cudaFree(L->d_force); cudaFree(L->d_mm_part); cudaFree(L->d_mm);
   if (L->cap) cudaStreamDestroy(L->cap);
+  if (L->ov.side) cudaStreamDestroy(L->ov.side);
+  if (L->ov.fork) cudaEventDestroy(L->ov.fork);
+  if (L->ov.join) cudaEventDestroy(L->ov.join);
   cudaGetLastError();  // teardown leaves no error behind for the next call
   auto* g = const_cast<oal_geometry*>(L->g);
   delete L;
@@ -886,7 +910,7 @@ static oal_status enqueue_step(oal_level* L, const CaseParams& cp, cudaStream_t 
   a.v_bstride = 512; a.v_cstride = 512 * (int64_t)g->nb;
   a.force_part = L->d_force_part;
   a.p0 = cp;
-  OAL_CUDA_TRY(launch_by_storage(L->storage, g, a, PATH_GHOSTED, st));
+  OAL_CUDA_TRY(launch_by_storage(L->storage, g, a, PATH_GHOSTED, st, &L->ov));
   if (cp.flags & CF_COLLECT) {
     // the momentum exchange lives on the general kernel's CTAs (blocks near solids)
     if (g->n_general > 0) {
