@@ -194,6 +194,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="budget of the CPU-baseline leg")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--nz", type=int, default=128, help="channel depth (smaller values for profiling captures)")
+    ap.add_argument("--layout", default="block", choices=["block", "dense"], help="population layout of the level")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -226,7 +227,7 @@ def main():
 
     case = sphere_channel_case(256, 128, args.nz, diameter=24.0, centre_x=64.0)
     geom = Geometry(case.dom, device=dev)
-    level = Level(geom, storage=args.storage)
+    level = Level(geom, storage=args.storage, layout=args.layout)
     level.init_equilibrium(case.rho, case.vel)
     p = case.params
     cells = case.dom.n_blocks * 512

@@ -213,6 +213,11 @@ typedef struct oal_level oal_level;
 oal_status oal_level_create(const oal_geometry* g, int32_t operator_id, int32_t storage,
                             oal_level** out);
 void oal_level_destroy(oal_level* L);
+/* Level creation options (bits of `flags`). */
+enum { OAL_LEVEL_DENSE = 1 /* box levels in FP32/FP16/BF16: dense padded population grid */ };
+/* oal_level_create with options; flags = 0 is oal_level_create. */
+oal_status oal_level_create_ex(const oal_geometry* g, int32_t operator_id, int32_t storage, uint32_t flags,
+                               oal_level** out);
 /* Equilibrium start from host rho(8,8,8,nb) and vel(8,8,8,nb,3) in double precision:
  * f_k = feq(rho,u) (physics_utils.jl:30-35), vel_in = u. */
 oal_status oal_level_init_equilibrium(oal_level* L, const double* rho_host, const double* vel_host,
@@ -239,6 +244,11 @@ oal_status oal_level_mass_momentum(oal_level* L, double out[4]);
 oal_status oal_level_device_state(oal_level* L, void** f, void** rho, void** vel);
 /* Bytes of device memory this level holds. */
 int64_t oal_level_device_bytes(const oal_level* L);
+/* Population layout of the level's device state (what oal_level_device_state points at):
+ * out = {dense, PX, PY, PZ, block_stride, dir_stride}. dense = 1: box levels in FP32/FP16/BF16
+ * keep f[k][Z][Y][X] on a padded PX x PY x PZ grid (interior cell (i,j,l) at X = i+8, Y = j+1,
+ * Z = l+1); dense = 0: block-major f[b][k][cell], element b*block_stride + k*dir_stride + cell. */
+oal_status oal_level_layout(const oal_level* L, int64_t out[6]);
 
 /* ---- no-allocation entry point -------------------------------------------------------------- */
 /* No counterpart in the reference. For callers that cannot call cudaMalloc when they need the

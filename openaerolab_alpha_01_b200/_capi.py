@@ -42,6 +42,8 @@ OAL_LIMITER_NONE = 0
 OAL_LIMITER_FACTORED = 1
 OAL_LIMITER_POSITIVITY = 2
 
+OAL_LEVEL_DENSE = 1
+
 OAL_SOLID_FULLWAY = 0
 OAL_SOLID_HALFWAY = 1
 
@@ -141,6 +143,7 @@ _SIGNATURES = {
     "oal_stream_collide": (C.c_int32, [C.c_void_p, C.POINTER(LevelFields), C.POINTER(StepParams), C.c_void_p]),
     "oal_level_create": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
     "oal_level_destroy": (None, [C.c_void_p]),
+    "oal_level_create_ex": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.c_uint32, C.POINTER(C.c_void_p)]),
     "oal_level_init_equilibrium": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]),
     "oal_level_set_state": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "oal_level_get_state": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -152,6 +155,7 @@ _SIGNATURES = {
     "oal_level_device_state": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                            C.POINTER(C.c_void_p)]),
     "oal_level_device_bytes": (C.c_int64, [C.c_void_p]),
+    "oal_level_layout": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
     "oal_mass_momentum_noalloc": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int64, C.c_int64, C.c_void_p, C.c_int32,
                                               C.c_void_p, C.c_void_p]),
 }

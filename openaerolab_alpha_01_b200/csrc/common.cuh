@@ -68,7 +68,10 @@ enum CaseFlags : uint32_t {
   CF_COLLECT = 1u << 11,
   CF_STORE_POST = 1u << 12,
   CF_GRADIENTS = 1u << 13,  // c_wale != 0: the WALE velocity-gradient stencil is needed
-  CF_INLET_NOISE = 1u << 14
+  CF_INLET_NOISE = 1u << 14,
+  CF_PERIODIC_X = 1u << 15,  // periodic axes of a dense (box) level
+  CF_PERIODIC_Y = 1u << 16,
+  CF_PERIODIC_Z = 1u << 17
 };
 
 struct CaseParams {
@@ -111,7 +114,18 @@ struct StepArgs {
   double* force_part;             // [n_ctas*3] momentum-exchange partials or null
   int32_t n_blocks;
   int32_t block_base;             // first block of this launch (per-case launches)
+  int32_t n_total_blocks;         // real + ghost blocks of the population buffers
+  // dense (box) population layout: f[k][Z][Y][X] over a padded grid PX x PY x PZ with the
+  // interior cell (i,j,l) at X = i + 8, Y = j + 1, Z = l + 1; f_kstride = PX*PY*PZ
+  int32_t dense;
+  int32_t PX, PY, PZ;
+  uint32_t* err;                  // device error word (bounded waits that gave up), or null
   CaseParams p0;
 };
+
+// Element index of cell (X, Y, Z) of the dense padded population grid (direction 0).
+__host__ __device__ __forceinline__ int64_t dense_idx(const StepArgs& a, int X, int Y, int Z) {
+  return ((int64_t)Z * a.PY + Y) * a.PX + X;
+}
 
 }  // namespace oal

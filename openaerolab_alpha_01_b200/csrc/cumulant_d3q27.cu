@@ -28,7 +28,7 @@
 // Tuning knobs of the uniform kernel (compile time): resident CTAs per SM the register budget
 // is sized for, and cells per thread (2 = packed f32x2 pairs, 1 = scalar float).
 #ifndef OAL_FAST_MIN_CTAS
-#define OAL_FAST_MIN_CTAS 3
+#define OAL_FAST_MIN_CTAS 4
 #endif
 #ifndef OAL_FAST_CELLS
 #define OAL_FAST_CELLS 2
@@ -53,10 +53,12 @@ __device__ __forceinline__ R dec_k(const S* __restrict__ f, int64_t i, int k) {
 // Population arriving at cell (x,y,z) of block b in direction k from outside every block
 // (kernel_cumulant.jl:221-391), level without parent. `nbr` is the block's 27-entry row; entries
 // >= n_real are ghost blocks, which count as missing here. k may be a run-time value.
-template <class S, class R>
+template <class S, class R, bool DENSE = false>
 __device__ __forceinline__ R face_population_impl(const S* __restrict__ fin, int64_t bbase, int cell, int64_t kst,
                                                   const int32_t* nbr, int n_real, int64_t bst, int k, int x, int y,
-                                                  int z, int gx, int gy, int gz, const CaseParams& cp) {
+                                                  int z, int gx, int gy, int gz, const CaseParams& cp,
+                                                  const StepArgs* da = nullptr) {
+  // block layouts: own = bbase + cell; dense layout: bbase is the cell's own element, cell = 0
   const int64_t own = bbase + cell;
   const int cx = q27_cx(k), cy = q27_cy(k), cz = q27_cz(k);
   const int src_gx = gx - cx, src_gy = gy - cy, src_gz = gz - cz;
@@ -81,12 +83,20 @@ __device__ __forceinline__ R face_population_impl(const S* __restrict__ fin, int
       j = q27_opp(k);
     } else {
       j = q27_mir_z(k);
-      const int zw_ix = x - cx, zw_iy = y - cy;
-      if (zw_ix >= 0 && zw_ix < kBS && zw_iy >= 0 && zw_iy < kBS) {
-        src = bbase + (zw_ix + 8 * zw_iy + 64 * z) + j * kst;
+      if constexpr (DENSE) {
+        // the image cell (x - cx, y - cy, z) of the box, wrapped on periodic axes
+        int ix = gx - cx, iy = gy - cy;
+        if (cp.flags & CF_PERIODIC_X) ix = ix < 1 ? ix + cp.nx : (ix > cp.nx ? ix - cp.nx : ix);
+        if (cp.flags & CF_PERIODIC_Y) iy = iy < 1 ? iy + cp.ny : (iy > cp.ny ? iy - cp.ny : iy);
+        if (ix >= 1 && ix <= cp.nx && iy >= 1 && iy <= cp.ny) src = dense_idx(*da, ix + 7, iy, gz) + j * kst;
       } else {
-        const int zw_nb = nbr[nbr_dir(zw_ix >> 3, zw_iy >> 3, 0)];
-        if (zw_nb >= 0 && zw_nb < n_real) src = (int64_t)zw_nb * bst + j * kst + ((zw_ix & 7) + 8 * (zw_iy & 7) + 64 * z);
+        const int zw_ix = x - cx, zw_iy = y - cy;
+        if (zw_ix >= 0 && zw_ix < kBS && zw_iy >= 0 && zw_iy < kBS) {
+          src = bbase + (zw_ix + 8 * zw_iy + 64 * z) + j * kst;
+        } else {
+          const int zw_nb = nbr[nbr_dir(zw_ix >> 3, zw_iy >> 3, 0)];
+          if (zw_nb >= 0 && zw_nb < n_real) src = (int64_t)zw_nb * bst + j * kst + ((zw_ix & 7) + 8 * (zw_iy & 7) + 64 * z);
+        }
       }
     }
   } else if ((cp.flags & CF_TRANSVERSE_FS) && (is_y_min || is_y_max || is_z_min || is_z_max)) {
@@ -124,13 +134,14 @@ __device__ __forceinline__ const CaseParams& case_of(const StepArgs& a, int case
 // ------------------------------------------------------------------------------------------------
 // ghost fill: one thread per (destination cell, direction) whose pull source is a ghost cell
 // ------------------------------------------------------------------------------------------------
-template <class S, class R>
+template <class S, class R, bool DENSE>
 __global__ void __launch_bounds__(256) k_fill_ghosts(const StepArgs a, const uint2* __restrict__ entries, int64_t n) {
   const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (e >= n) return;
   const uint2 en = entries[e];
   const int b = (int)en.x;
-  const int cell = (int)(en.y & 511u), k = (int)(en.y >> 9);
+  const int cell = (int)(en.y & 511u), k = (int)((en.y >> 9) & 31u);
+  const bool wrap = (en.y >> 31) != 0;  // dense periodic crossing: a copy of the wrapped interior cell
   const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
   const int4 bi = a.binfo[b];
   const CaseParams& cp = case_of(a, a.cases ? bi.w : 0);
@@ -138,12 +149,29 @@ __global__ void __launch_bounds__(256) k_fill_ghosts(const StepArgs a, const uin
   const int32_t* nbr = a.nbr + (int64_t)b * 27;
   const int64_t bst = a.f_bstride, kst = a.f_kstride;
   const int gx = (bi.x - 1) * kBS + x + 1, gy = (bi.y - 1) * kBS + y + 1, gz = (bi.z - 1) * kBS + z + 1;
-  const R val = face_population_impl<S, R>(f, (int64_t)b * bst, cell, kst, nbr, a.n_blocks, bst, k, x, y, z, gx, gy,
-                                           gz, cp);
-  const int sx = x - q27_cx(k), sy = y - q27_cy(k), sz = z - q27_cz(k);
-  const int g = nbr[nbr_dir(sx >> 3, sy >> 3, sz >> 3)];
-  f[(int64_t)g * bst + k * kst + ((sx & 7) | ((sy & 7) << 3) | ((sz & 7) << 6))] =
-      Codec<S>::enc(val, R(q27_w(k)), R(1.0 / q27_w(k)));
+  const int cx = q27_cx(k), cy = q27_cy(k), cz = q27_cz(k);
+  if constexpr (DENSE) {
+    // ghost slot: the padded position of the source cell (1-based global g - c_k)
+    const int64_t slot = dense_idx(a, gx - cx + 7, gy - cy, gz - cz) + k * kst;
+    if (wrap) {
+      int sx = gx - cx, sy = gy - cy, sz = gz - cz;
+      sx = sx < 1 ? sx + cp.nx : (sx > cp.nx ? sx - cp.nx : sx);
+      sy = sy < 1 ? sy + cp.ny : (sy > cp.ny ? sy - cp.ny : sy);
+      sz = sz < 1 ? sz + cp.nz : (sz > cp.nz ? sz - cp.nz : sz);
+      f[slot] = f[dense_idx(a, sx + 7, sy, sz) + k * kst];
+      return;
+    }
+    const int64_t own = dense_idx(a, gx + 7, gy, gz);
+    const R val = face_population_impl<S, R, true>(f, own, 0, kst, nbr, a.n_blocks, bst, k, x, y, z, gx, gy, gz, cp, &a);
+    f[slot] = Codec<S>::enc(val, R(q27_w(k)), R(1.0 / q27_w(k)));
+  } else {
+    const R val = face_population_impl<S, R>(f, (int64_t)b * bst, cell, kst, nbr, a.n_blocks, bst, k, x, y, z, gx, gy,
+                                             gz, cp);
+    const int sx = x - cx, sy = y - cy, sz = z - cz;
+    const int g = nbr[nbr_dir(sx >> 3, sy >> 3, sz >> 3)];
+    f[(int64_t)g * bst + k * kst + ((sx & 7) | ((sy & 7) << 3) | ((sz & 7) << 6))] =
+        Codec<S>::enc(val, R(q27_w(k)), R(1.0 / q27_w(k)));
+  }
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -177,7 +205,9 @@ __device__ __forceinline__ void store2(S* __restrict__ f, int64_t i0, int64_t i1
   }
 }
 
-template <class S, class V>
+// Library-owned block-major layout: block stride 27*512, direction stride 512 (compile time).
+// IDX = uint32_t when the buffer (real + ghost blocks) has fewer than 2^32 elements.
+template <class S, class V, class IDX>
 __global__ void __launch_bounds__(128, OAL_FAST_MIN_CTAS) k_cumulant_fast(const StepArgs a, const int32_t* __restrict__ work) {
   constexpr int NL = Lane<V>::N;  // cells per thread
   constexpr int CPB = 4 / NL;     // CTAs per block
@@ -200,7 +230,8 @@ __global__ void __launch_bounds__(128, OAL_FAST_MIN_CTAS) k_cumulant_fast(const 
   T* __restrict__ rho_out = static_cast<T*>(a.rho_out);
   T* __restrict__ vel_out = static_cast<T*>(a.vel_out);
   const T* __restrict__ vel_in = static_cast<const T*>(a.vel_in);
-  const int64_t bst = a.f_bstride, kst = a.f_kstride, vcs = a.v_cstride;
+  constexpr IDX bst = 27 * kCells, kst = kCells;
+  const IDX vcs = (IDX)a.v_cstride;
   const int n_real = a.n_blocks;
 
   const int x = tid & 7, y = (tid >> 3) & 7;
@@ -213,12 +244,12 @@ __global__ void __launch_bounds__(128, OAL_FAST_MIN_CTAS) k_cumulant_fast(const 
 #pragma unroll
   for (int k = 0; k < kQ27; ++k) {
     const int sx = x - q27_cx(k), sy = y - q27_cy(k);
-    int64_t idx[NL];
+    IDX idx[NL];
 #pragma unroll
     for (int l = 0; l < NL; ++l) {
       const int sz = z[l] - q27_cz(k);
       const int nb = s_nbr[nbr_dir(sx >> 3, sy >> 3, sz >> 3)];
-      idx[l] = (int64_t)nb * bst + k * kst + ((sx & 7) | ((sy & 7) << 3) | ((sz & 7) << 6));
+      idx[l] = (IDX)nb * bst + (IDX)(k * kst) + (IDX)((sx & 7) | ((sy & 7) << 3) | ((sz & 7) << 6));
     }
     if constexpr (NL == 2) A[k] = load2<S>(fin, idx[0], idx[1], k);
     else A[k] = dec_k<S, T>(fin, idx[0], k);
@@ -238,9 +269,9 @@ __global__ void __launch_bounds__(128, OAL_FAST_MIN_CTAS) k_cumulant_fast(const 
   rho = vmaxc(rho, T(0.01));
   const V inv_rho = vrcp(rho);
   const V ux = jx * inv_rho, uy = jy * inv_rho, uz = jz * inv_rho;
-  int64_t vown[NL];
+  IDX vown[NL];
 #pragma unroll
-  for (int l = 0; l < NL; ++l) vown[l] = (int64_t)b * kCells + (x | (y << 3) | (z[l] << 6));
+  for (int l = 0; l < NL; ++l) vown[l] = (IDX)b * kCells + (IDX)(x | (y << 3) | (z[l] << 6));
   if constexpr (NL == 2) {
     float r0, r1, a0, a1;
     f2split(rho, r0, r1); rho_out[vown[0]] = r0; rho_out[vown[1]] = r1;
@@ -262,8 +293,8 @@ __global__ void __launch_bounds__(128, OAL_FAST_MIN_CTAS) k_cumulant_fast(const 
       for (int l = 0; l < NL; ++l) {
         const int nx = x + dx, ny = y + dy, nz = z[l] + dz;
         const int nb = s_nbr[nbr_dir(nx >> 3, ny >> 3, nz >> 3)];
-        const int64_t i = nb < n_real ? (int64_t)nb * kCells + ((nx & 7) | ((ny & 7) << 3) | ((nz & 7) << 6)) : vown[l];
-        v[l] = vel_in[i + c * vcs];
+        const IDX i = nb < n_real ? (IDX)nb * kCells + (IDX)((nx & 7) | ((ny & 7) << 3) | ((nz & 7) << 6)) : vown[l];
+        v[l] = vel_in[i + (IDX)c * vcs];
       }
       if constexpr (NL == 2) return f2(v[0], v[1]);
       else return v[0];
@@ -287,9 +318,9 @@ __global__ void __launch_bounds__(128, OAL_FAST_MIN_CTAS) k_cumulant_fast(const 
   // ---- store (kernel_cumulant.jl:889-908 with zero force) ----
 #pragma unroll
   for (int k = 0; k < kQ27; ++k) {
-    int64_t o[NL];
+    IDX o[NL];
 #pragma unroll
-    for (int l = 0; l < NL; ++l) o[l] = (int64_t)b * bst + k * kst + (x | (y << 3) | (z[l] << 6));
+    for (int l = 0; l < NL; ++l) o[l] = (IDX)b * bst + (IDX)(k * kst) + (IDX)(x | (y << 3) | (z[l] << 6));
     if constexpr (NL == 2) store2<S>(fout, o[0], o[1], A[k], k);
     else fout[o[0]] = Codec<S>::enc(A[k], T(q27_w(k)), T(1.0 / q27_w(k)));
   }
@@ -298,7 +329,7 @@ __global__ void __launch_bounds__(128, OAL_FAST_MIN_CTAS) k_cumulant_fast(const 
 // ------------------------------------------------------------------------------------------------
 // general kernel: one cell per thread, every option
 // ------------------------------------------------------------------------------------------------
-template <class S, class R>
+template <class S, class R, bool DENSE>
 __global__ void __launch_bounds__(128) k_cumulant_gen(const StepArgs a, const int32_t* __restrict__ work) {
   __shared__ int32_t s_nbr[28];
   __shared__ CaseParams s_cp;
@@ -327,9 +358,10 @@ __global__ void __launch_bounds__(128) k_cumulant_gen(const StepArgs a, const in
 
   const int x = tid & 7, y = (tid >> 3) & 7, z = 2 * part + (tid >> 6);
   const int cell = x | (y << 3) | (z << 6);
-  const int64_t own = (int64_t)b * bst + cell;
-  const int64_t vown = (int64_t)b * kCells + cell;
   const int gx = (bi.x - 1) * kBS + x + 1, gy = (bi.y - 1) * kBS + y + 1, gz = (bi.z - 1) * kBS + z + 1;
+  // own element of direction 0: block layouts b*bst + cell; dense layout the padded grid position
+  const int64_t own = DENSE ? dense_idx(a, gx + 7, gy, gz) : (int64_t)b * bst + cell;
+  const int64_t vown = (int64_t)b * kCells + cell;
   const bool store_post = (flags & CF_STORE_POST) && fpost;
 
   uint32_t mask = 0;
@@ -355,9 +387,9 @@ __global__ void __launch_bounds__(128) k_cumulant_gen(const StepArgs a, const in
     for (int k = 0; k < kQ27; ++k) {
       const int cx = q27_cx(k), cy = q27_cy(k), cz = q27_cz(k);
       const int sx = x - cx, sy = y - cy, sz = z - cz;
-      const int nb = s_nbr[nbr_dir(sx >> 3, sy >> 3, sz >> 3)];
+      const int nb = DENSE ? 0 : s_nbr[nbr_dir(sx >> 3, sy >> 3, sz >> 3)];
       R val;
-      if (nb >= 0) {
+      if (DENSE || nb >= 0) {
         if (halfway && ((mask >> k) & 1u)) {
           // the link opp(k) of this cell is cut: its own post-collision population returns
           const int i = q27_opp(k);
@@ -367,6 +399,9 @@ __global__ void __launch_bounds__(128) k_cumulant_gen(const StepArgs a, const in
             const double mom = 2.0 * (double)fi;  // (f_i* + f_k(t+1)) c_i with c_i = -c_k
             mx -= mom * cx; my -= mom * cy; mz -= mom * cz;
           }
+        } else if (DENSE) {
+          // the padded grid holds every source, ghost frame included
+          val = dec_k<S, R>(fin, own - cx - (int64_t)cy * a.PX - (int64_t)cz * a.PX * a.PY + k * kst, k);
         } else {
           val = dec_k<S, R>(fin, (int64_t)nb * bst + k * kst + ((sx & 7) | ((sy & 7) << 3) | ((sz & 7) << 6)), k);
         }
@@ -513,19 +548,25 @@ __global__ void __launch_bounds__(128) k_cumulant_gen(const StepArgs a, const in
 template <class S, class R>
 cudaError_t launch_fill_ghosts(const StepArgs& a, const uint2* entries, int64_t n, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  k_fill_ghosts<S, R><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, entries, n);
+  if (a.dense) k_fill_ghosts<S, R, true><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, entries, n);
+  else k_fill_ghosts<S, R, false><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, entries, n);
   return cudaGetLastError();
 }
 
 template <class S, class R>
 cudaError_t launch_fast(const StepArgs& a, const int32_t* work, int n_work, cudaStream_t st) {
   if (n_work <= 0) return cudaSuccess;
+  // element count of the buffer (real + ghost blocks) decides the index width
+  const bool idx32 = (uint64_t)a.n_total_blocks * 27u * kCells < (1ull << 32);
   if constexpr (sizeof(R) == 8) {
-    k_cumulant_fast<S, double><<<(unsigned)n_work * 4u, 128, 0, st>>>(a, work);
+    if (idx32) k_cumulant_fast<S, double, uint32_t><<<(unsigned)n_work * 4u, 128, 0, st>>>(a, work);
+    else k_cumulant_fast<S, double, int64_t><<<(unsigned)n_work * 4u, 128, 0, st>>>(a, work);
   } else if constexpr (OAL_FAST_CELLS == 1) {
-    k_cumulant_fast<S, float><<<(unsigned)n_work * 4u, 128, 0, st>>>(a, work);
+    if (idx32) k_cumulant_fast<S, float, uint32_t><<<(unsigned)n_work * 4u, 128, 0, st>>>(a, work);
+    else k_cumulant_fast<S, float, int64_t><<<(unsigned)n_work * 4u, 128, 0, st>>>(a, work);
   } else {
-    k_cumulant_fast<S, F2><<<(unsigned)n_work * 2u, 128, 0, st>>>(a, work);
+    if (idx32) k_cumulant_fast<S, F2, uint32_t><<<(unsigned)n_work * 2u, 128, 0, st>>>(a, work);
+    else k_cumulant_fast<S, F2, int64_t><<<(unsigned)n_work * 2u, 128, 0, st>>>(a, work);
   }
   return cudaGetLastError();
 }
@@ -533,7 +574,8 @@ cudaError_t launch_fast(const StepArgs& a, const int32_t* work, int n_work, cuda
 template <class S, class R>
 cudaError_t launch_general(const StepArgs& a, const int32_t* work, int n_work, cudaStream_t st) {
   if (n_work <= 0) return cudaSuccess;
-  k_cumulant_gen<S, R><<<(unsigned)n_work * 4u, 128, 0, st>>>(a, work);
+  if (a.dense) k_cumulant_gen<S, R, true><<<(unsigned)n_work * 4u, 128, 0, st>>>(a, work);
+  else k_cumulant_gen<S, R, false><<<(unsigned)n_work * 4u, 128, 0, st>>>(a, work);
   return cudaGetLastError();
 }
 

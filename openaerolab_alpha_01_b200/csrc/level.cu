@@ -20,6 +20,10 @@ template <class S, class R>
 cudaError_t launch_fast(const StepArgs& a, const int32_t* work, int n_work, cudaStream_t st);
 template <class S, class R>
 cudaError_t launch_general(const StepArgs& a, const int32_t* work, int n_work, cudaStream_t st);
+template <class S>
+cudaError_t launch_dense_fast(const StepArgs& a, const int32_t* work, int n_work, int grid, cudaStream_t st);
+template <class S>
+int dense_ctas_per_sm();
 }
 using namespace oal;
 
@@ -91,9 +95,26 @@ __global__ void k_reduce4(const double* __restrict__ part, int64_t n, double* __
     for (int c = 0; c < 4; ++c) out[c] = s[c][0];
 }
 
+// Element of (block b, cell, direction k) in either population layout of a library-owned level.
+struct PopIndex {
+  const int4* binfo;
+  int dense;
+  int PX, PY;
+  int64_t bst, kst;
+  __device__ __forceinline__ int64_t operator()(int64_t b, int cell, int k) const {
+    if (dense) {
+      const int4 bi = binfo[b];
+      const int X = (bi.x - 1) * kBS + (cell & 7) + 8, Y = (bi.y - 1) * kBS + ((cell >> 3) & 7) + 1,
+                Z = (bi.z - 1) * kBS + (cell >> 6) + 1;
+      return ((int64_t)Z * PY + Y) * PX + X + k * kst;
+    }
+    return b * bst + k * kst + cell;
+  }
+};
+
 // Per-block FP64 mass and momentum of the fluid cells (state.jl:614-637): one CTA per block.
 template <class S, class R>
-__global__ void k_mass_momentum(const S* __restrict__ f, int64_t bst, int64_t kst, const uint32_t* __restrict__ bflags,
+__global__ void k_mass_momentum(const S* __restrict__ f, PopIndex pi, const uint32_t* __restrict__ bflags,
                                 const int32_t* __restrict__ mslot, const uint32_t* __restrict__ cmask,
                                 double* __restrict__ part) {
   __shared__ double s[4][16];
@@ -104,7 +125,7 @@ __global__ void k_mass_momentum(const S* __restrict__ f, int64_t bst, int64_t ks
     if (ns && ((cmask[(int64_t)mslot[b] * kCells + cell] >> 13) & 1u)) continue;
 #pragma unroll
     for (int k = 0; k < kQ27; ++k) {
-      const double v = (double)Codec<S>::dec(f[(int64_t)b * bst + k * kst + cell], R(q27_w(k)), R(1.0 / q27_w(k)));
+      const double v = (double)Codec<S>::dec(f[pi(b, cell, k)], R(q27_w(k)), R(1.0 / q27_w(k)));
       m += v; px += v * q27_cx(k); py += v * q27_cy(k); pz += v * q27_cz(k);
     }
   }
@@ -126,7 +147,7 @@ __global__ void k_mass_momentum(const S* __restrict__ f, int64_t bst, int64_t ks
 // Equilibrium start (physics_utils.jl:30-35 / 65-95) from reference-layout double rho / vel.
 template <class S, class R>
 __global__ void k_init_feq(const double* __restrict__ rho, const double* __restrict__ vel, int64_t ncell, int comp,
-                           S* __restrict__ f, int64_t bst, int64_t kst, R* __restrict__ rho_out, R* __restrict__ vel_out) {
+                           S* __restrict__ f, PopIndex pi, R* __restrict__ rho_out, R* __restrict__ vel_out) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= ncell) return;
   const int64_t b = i >> 9, cell = i & 511;
@@ -141,7 +162,7 @@ __global__ void k_init_feq(const double* __restrict__ rho, const double* __restr
       const R cu2 = cu * cu;
       val += (R(4.5) * cu2 * cu - R(4.5) * cu * usq) + (R(3.375) * cu2 * cu2 - R(6.75) * cu2 * usq + R(1.125) * usq * usq);
     }
-    f[b * bst + k * kst + cell] = Codec<S>::enc(r * w * val, w, R(1.0 / q27_w(k)));
+    f[pi(b, (int)cell, k)] = Codec<S>::enc(r * w * val, w, R(1.0 / q27_w(k)));
   }
   rho_out[i] = r;
   vel_out[i] = ux; vel_out[i + ncell] = uy; vel_out[i + 2 * ncell] = uz;
@@ -149,23 +170,23 @@ __global__ void k_init_feq(const double* __restrict__ rho, const double* __restr
 
 // Reference-layout double -> storage layout.
 template <class S, class R>
-__global__ void k_import_f(const double* __restrict__ src, int64_t ncell, S* __restrict__ f, int64_t bst, int64_t kst) {
+__global__ void k_import_f(const double* __restrict__ src, int64_t ncell, S* __restrict__ f, PopIndex pi) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= ncell) return;
   const int64_t b = i >> 9, cell = i & 511;
 #pragma unroll
   for (int k = 0; k < kQ27; ++k)
-    f[b * bst + k * kst + cell] = Codec<S>::enc(R(src[i + ncell * k]), R(q27_w(k)), R(1.0 / q27_w(k)));
+    f[pi(b, (int)cell, k)] = Codec<S>::enc(R(src[i + ncell * k]), R(q27_w(k)), R(1.0 / q27_w(k)));
 }
 // Storage layout -> reference-layout double.
 template <class S, class R>
-__global__ void k_export_f(const S* __restrict__ f, int64_t bst, int64_t kst, int64_t ncell, double* __restrict__ dst) {
+__global__ void k_export_f(const S* __restrict__ f, PopIndex pi, int64_t ncell, double* __restrict__ dst) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= ncell) return;
   const int64_t b = i >> 9, cell = i & 511;
 #pragma unroll
   for (int k = 0; k < kQ27; ++k)
-    dst[i + ncell * k] = (double)Codec<S>::dec(f[b * bst + k * kst + cell], R(q27_w(k)), R(1.0 / q27_w(k)));
+    dst[i + ncell * k] = (double)Codec<S>::dec(f[pi(b, (int)cell, k)], R(q27_w(k)), R(1.0 / q27_w(k)));
 }
 template <class R>
 __global__ void k_to_double(const R* __restrict__ src, int64_t n, double* __restrict__ dst) {
@@ -216,6 +237,13 @@ struct oal_geometry {
   double* d_force_part = nullptr;  // scratch of oal_stream_collide
   double* d_force = nullptr;
   int64_t n_fluid = 0, n_solid = 0, n_boundary = 0, n_slots = 0;
+  // box levels (every block of a bx x by x bz box): dense padded population layout
+  bool box = false;
+  int32_t bdim[3] = {0, 0, 0};
+  uint32_t pmask = 0;              // CF_PERIODIC_* bits
+  uint2* d_dense_gentries = nullptr;  // (block, cell | k << 9 | wrap << 31)
+  int64_t n_dense_gentries = 0;
+  int32_t* d_dense_fast = nullptr;    // uniform blocks, x fastest
   // levels built on this geometry; destroying the geometry while levels live defers the release
   // to the last level's destroy
   int32_t n_levels = 0;
@@ -241,6 +269,11 @@ struct oal_level {
   const oal_geometry* g = nullptr;
   int device = 0;
   int32_t op = 0, storage = 0;
+  // dense padded layout (box levels, FP32/FP16/BF16)
+  bool dense = false;
+  int32_t PX = 0, PY = 0, PZ = 0;
+  int32_t dense_grid = 0;
+  uint32_t* d_err = nullptr;
   void* f[2] = {nullptr, nullptr};
   void* vel[2] = {nullptr, nullptr};
   void* rho = nullptr;
@@ -352,36 +385,45 @@ static void fill_geometry_args(const oal_geometry* g, StepArgs* a) {
 }
 
 static void level_layout(const oal_level* L, int64_t* bst, int64_t* kst) {
-  *bst = 27 * 512;  // block-major: f[b][k][cell]
-  *kst = 512;
+  if (L->dense) {
+    *bst = 0;
+    *kst = (int64_t)L->PX * L->PY * L->PZ;  // dense: f[k][Z][Y][X]
+  } else {
+    *bst = 27 * 512;  // block-major: f[b][k][cell]
+    *kst = 512;
+  }
+}
+
+static PopIndex pop_index(const oal_level* L) {
+  PopIndex pi{};
+  pi.binfo = L->g->d_binfo;
+  pi.dense = L->dense ? 1 : 0;
+  pi.PX = L->PX;
+  pi.PY = L->PY;
+  level_layout(L, &pi.bst, &pi.kst);
+  return pi;
 }
 
 template <class S, class R>
 static cudaError_t init_feq_t(oal_level* L, const double* d_rho, const double* d_vel, int comp) {
-  int64_t bst, kst;
-  level_layout(L, &bst, &kst);
   const int64_t ncell = (int64_t)L->g->nb * 512;
-  k_init_feq<S, R><<<nblk(ncell, 256), 256>>>(d_rho, d_vel, ncell, comp, static_cast<S*>(L->f[0]), bst, kst,
+  k_init_feq<S, R><<<nblk(ncell, 256), 256>>>(d_rho, d_vel, ncell, comp, static_cast<S*>(L->f[0]), pop_index(L),
                                               static_cast<R*>(L->rho), static_cast<R*>(L->vel[0]));
   return cudaGetLastError();
 }
 
 template <class S, class R>
 static cudaError_t import_t(oal_level* L, const double* d_f, const double* d_rho, const double* d_vel) {
-  int64_t bst, kst;
-  level_layout(L, &bst, &kst);
   const int64_t ncell = (int64_t)L->g->nb * 512;
-  k_import_f<S, R><<<nblk(ncell, 256), 256>>>(d_f, ncell, static_cast<S*>(L->f[L->parity]), bst, kst);
+  k_import_f<S, R><<<nblk(ncell, 256), 256>>>(d_f, ncell, static_cast<S*>(L->f[L->parity]), pop_index(L));
   if (d_rho) k_from_double<R><<<nblk(ncell, 256), 256>>>(d_rho, ncell, static_cast<R*>(L->rho));
   if (d_vel) k_from_double<R><<<nblk(3 * ncell, 256), 256>>>(d_vel, 3 * ncell, static_cast<R*>(L->vel[L->parity]));
   return cudaGetLastError();
 }
 template <class S, class R>
 static cudaError_t export_t(oal_level* L, double* d_f, double* d_rho, double* d_vel) {
-  int64_t bst, kst;
-  level_layout(L, &bst, &kst);
   const int64_t ncell = (int64_t)L->g->nb * 512;
-  if (d_f) k_export_f<S, R><<<nblk(ncell, 256), 256>>>(static_cast<const S*>(L->f[L->parity]), bst, kst, ncell, d_f);
+  if (d_f) k_export_f<S, R><<<nblk(ncell, 256), 256>>>(static_cast<const S*>(L->f[L->parity]), pop_index(L), ncell, d_f);
   if (d_rho) k_to_double<R><<<nblk(ncell, 256), 256>>>(static_cast<const R*>(L->rho), ncell, d_rho);
   if (d_vel) k_to_double<R><<<nblk(3 * ncell, 256), 256>>>(static_cast<const R*>(L->vel[L->parity]), 3 * ncell, d_vel);
   return cudaGetLastError();
@@ -389,13 +431,37 @@ static cudaError_t export_t(oal_level* L, double* d_f, double* d_rho, double* d_
 
 template <class S, class R>
 static cudaError_t mm_t(oal_level* L) {
-  int64_t bst, kst;
-  level_layout(L, &bst, &kst);
   const oal_geometry* g = L->g;
-  k_mass_momentum<S, R><<<g->nb, 128>>>(static_cast<const S*>(L->f[L->parity]), bst, kst, g->d_bflags, g->d_mslot,
+  k_mass_momentum<S, R><<<g->nb, 128>>>(static_cast<const S*>(L->f[L->parity]), pop_index(L), g->d_bflags, g->d_mslot,
                                         g->d_cmask, L->d_mm_part);
   k_reduce4<<<1, 256>>>(L->d_mm_part, g->nb, L->d_mm);
   return cudaGetLastError();
+}
+
+template <class S, class R>
+static cudaError_t dense_step_t(oal_level* L, const StepArgs& a, cudaStream_t st) {
+  const oal_geometry* g = L->g;
+  cudaError_t e;
+  if ((e = launch_fill_ghosts<S, R>(a, g->d_dense_gentries, g->n_dense_gentries, st)) != cudaSuccess) return e;
+  const int n_fast = (int)(g->nb - g->n_general);
+  if (g->n_general > 0) {
+    if ((e = cudaEventRecord(L->ov.fork, st)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(L->ov.side, L->ov.fork, 0)) != cudaSuccess) return e;
+    if ((e = launch_general<S, R>(a, g->d_general, g->n_general, L->ov.side)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(L->ov.join, L->ov.side)) != cudaSuccess) return e;
+  }
+  if ((e = launch_dense_fast<S>(a, g->d_dense_fast, n_fast, L->dense_grid, st)) != cudaSuccess) return e;
+  if (g->n_general > 0) return cudaStreamWaitEvent(st, L->ov.join, 0);
+  return cudaSuccess;
+}
+
+// Reads (and clears) the level's device error word after a synchronisation.
+static oal_status check_level_error(oal_level* L) {
+  uint32_t w = 0;
+  OAL_CUDA_TRY(cudaMemcpy(&w, L->d_err, sizeof w, cudaMemcpyDeviceToHost));
+  if (w == 0) return OAL_OK;
+  OAL_CUDA_TRY(cudaMemset(L->d_err, 0, sizeof w));
+  return set_error(OAL_E_TIMEOUT, "a bounded device wait gave up (code 0x%x); the step's results are invalid", w);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -650,6 +716,68 @@ oal_status oal_geometry_create(const oal_geometry_desc* d, int32_t device, oal_g
   g->n_fast = (int32_t)fast.size();
   g->n_general = (int32_t)general.size();
 
+  // Box levels: every block of the bx x by x bz box present -> dense padded population layout.
+  // Periodic axes are read from the neighbour table (a first block that has a neighbour across the
+  // low face of an axis wraps on that axis).
+  std::vector<uint2> dentries;
+  std::vector<int32_t> dfast;
+  {
+    int bxm = 0, bym = 0, bzm = 0;
+    bool ok = true;
+    for (int64_t b = 0; b < nb; ++b) {
+      if (binfo[b].x < 1 || binfo[b].y < 1 || binfo[b].z < 1) ok = false;
+      bxm = std::max(bxm, binfo[b].x); bym = std::max(bym, binfo[b].y); bzm = std::max(bzm, binfo[b].z);
+    }
+    ok = ok && (int64_t)bxm * bym * bzm == nb && d->nx_global == 8 * bxm && d->ny_global == 8 * bym &&
+         d->nz_global == 8 * bzm;
+    if (ok) {
+      std::vector<int32_t> at((size_t)nb, -1);
+      for (int64_t b = 0; b < nb && ok; ++b) {
+        const int64_t key = ((int64_t)(binfo[b].x - 1) * bym + (binfo[b].y - 1)) * bzm + (binfo[b].z - 1);
+        if (at[(size_t)key] >= 0) ok = false; else at[(size_t)key] = (int32_t)b;
+      }
+      if (ok) {
+        g->box = true;
+        g->bdim[0] = bxm; g->bdim[1] = bym; g->bdim[2] = bzm;
+        const int64_t first = at[0];  // block (1,1,1)
+        if (nbr0[(size_t)first * 27 + nbr_dir(-1, 0, 0)] >= 0) g->pmask |= CF_PERIODIC_X;
+        if (nbr0[(size_t)first * 27 + nbr_dir(0, -1, 0)] >= 0) g->pmask |= CF_PERIODIC_Y;
+        if (nbr0[(size_t)first * 27 + nbr_dir(0, 0, -1)] >= 0) g->pmask |= CF_PERIODIC_Z;
+        const int N[3] = {8 * bxm, 8 * bym, 8 * bzm};
+        const bool per[3] = {(g->pmask & CF_PERIODIC_X) != 0, (g->pmask & CF_PERIODIC_Y) != 0, (g->pmask & CF_PERIODIC_Z) != 0};
+        // ghost-frame slots: every (cell, k) whose source leaves the box; a crossing of periodic
+        // axes only is a copy of the wrapped interior cell, any other goes through the face rules
+        for (int64_t b = 0; b < nb; ++b) {
+          const int g0[3] = {(binfo[b].x - 1) * 8, (binfo[b].y - 1) * 8, (binfo[b].z - 1) * 8};
+          const bool edge = g0[0] == 0 || g0[1] == 0 || g0[2] == 0 || g0[0] + 8 == N[0] || g0[1] + 8 == N[1] ||
+                            g0[2] + 8 == N[2];
+          if (!edge) continue;
+          for (int cell = 0; cell < 512; ++cell) {
+            const int c3[3] = {g0[0] + (cell & 7), g0[1] + ((cell >> 3) & 7), g0[2] + (cell >> 6)};
+            for (int k = 0; k < 27; ++k) {
+              const int ck[3] = {q27_cx(k), q27_cy(k), q27_cz(k)};
+              bool out = false, face = false;
+              for (int ax = 0; ax < 3; ++ax) {
+                const int sc = c3[ax] - ck[ax];
+                if (sc < 0 || sc >= N[ax]) { out = true; if (!per[ax]) face = true; }
+              }
+              if (out)
+                dentries.push_back(make_uint2((uint32_t)b, (uint32_t)cell | ((uint32_t)k << 9) | (face ? 0u : (1u << 31))));
+            }
+          }
+        }
+        // uniform blocks ordered x fastest, so CTAs running together write neighbouring rows
+        for (int bz = 1; bz <= bzm; ++bz)
+          for (int by = 1; by <= bym; ++by)
+            for (int bx = 1; bx <= bxm; ++bx) {
+              const int32_t b = at[((size_t)(bx - 1) * bym + (by - 1)) * bzm + (bz - 1)];
+              if (std::find(general.begin(), general.end(), b) == general.end()) dfast.push_back(b);
+            }
+      }
+    }
+  }
+  g->n_dense_gentries = (int64_t)dentries.size();
+
   auto fail = [&](oal_status s) { oal_geometry_destroy(g); return s; };
 #define GTRY(expr)                                                                         \
   do {                                                                                     \
@@ -692,6 +820,14 @@ oal_status oal_geometry_create(const oal_geometry_desc* d, int32_t device, oal_g
     GTRY(cudaMalloc(&g->d_general, general.size() * sizeof(int32_t)));
     GTRY(cudaMemcpy(g->d_general, general.data(), general.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
   }
+  if (!dentries.empty()) {
+    GTRY(cudaMalloc(&g->d_dense_gentries, dentries.size() * sizeof(uint2)));
+    GTRY(cudaMemcpy(g->d_dense_gentries, dentries.data(), dentries.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+  }
+  if (!dfast.empty()) {
+    GTRY(cudaMalloc(&g->d_dense_fast, dfast.size() * sizeof(int32_t)));
+    GTRY(cudaMemcpy(g->d_dense_fast, dfast.data(), dfast.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  }
   GTRY(cudaMalloc(&g->d_force_part, (size_t)nb * 4 * 3 * sizeof(double)));
   GTRY(cudaMalloc(&g->d_force, 3 * sizeof(double)));
   GTRY(cudaMemset(g->d_force, 0, 3 * sizeof(double)));
@@ -703,6 +839,7 @@ oal_status oal_geometry_create(const oal_geometry_desc* d, int32_t device, oal_g
 static void geometry_release(oal_geometry* g) {
   cudaSetDevice(g->device);
   cudaFree(g->d_nbr_ghost); cudaFree(g->d_gentries); cudaFree(g->d_fast); cudaFree(g->d_general);
+  cudaFree(g->d_dense_gentries); cudaFree(g->d_dense_fast);
   cudaFree(g->d_nbr); cudaFree(g->d_binfo); cudaFree(g->d_bflags); cudaFree(g->d_mslot);
   cudaFree(g->d_cmask); cudaFree(g->d_sponge); cudaFree(g->d_wdist);
   cudaFree(g->d_force_part); cudaFree(g->d_force);
@@ -752,6 +889,10 @@ oal_status oal_stream_collide(const oal_geometry* g, const oal_level_fields* fl,
 
 // ---- levels ----
 oal_status oal_level_create(const oal_geometry* g, int32_t op, int32_t storage, oal_level** out) {
+  return oal_level_create_ex(g, op, storage, 0u, out);
+}
+
+oal_status oal_level_create_ex(const oal_geometry* g, int32_t op, int32_t storage, uint32_t flags, oal_level** out) {
   if (!g || !out) return set_error(OAL_E_INVALID_ARG, "null argument");
   *out = nullptr;
   if (op != OAL_OP_CUMULANT_D3Q27) return set_error(OAL_E_UNSUPPORTED, "operator %d has no level state in this build", op);
@@ -761,8 +902,16 @@ oal_status oal_level_create(const oal_geometry* g, int32_t op, int32_t storage, 
   L->g = g; L->device = g->device; L->op = op; L->storage = storage;
   ++const_cast<oal_geometry*>(g)->n_levels;
   const int64_t ncell = (int64_t)g->nb * 512;
-  // populations of the real blocks followed by the ghost blocks
-  const size_t fbytes = (size_t)(g->nb + g->n_ghost) * 512 * 27 * storage_bytes(storage);
+  // box levels in FP32/FP16/BF16: dense padded grid; otherwise the real blocks followed by the
+  // ghost blocks
+  L->dense = (flags & OAL_LEVEL_DENSE) && g->box && storage != OAL_STORE_F64;
+  if (L->dense) {
+    L->PX = 8 * g->bdim[0] + 16;
+    L->PY = 8 * g->bdim[1] + 2;
+    L->PZ = 8 * g->bdim[2] + 2;
+  }
+  const size_t fbytes = L->dense ? (size_t)27 * L->PX * L->PY * L->PZ * storage_bytes(storage)
+                                 : (size_t)(g->nb + g->n_ghost) * 512 * 27 * storage_bytes(storage);
   const size_t mb = macro_bytes(storage);
   auto fail = [&](cudaError_t e) {
     oal_level_destroy(L);
@@ -786,7 +935,18 @@ oal_status oal_level_create(const oal_geometry* g, int32_t op, int32_t storage, 
   if ((e = cudaStreamCreateWithFlags(&L->ov.side, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
   if ((e = cudaEventCreateWithFlags(&L->ov.fork, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
   if ((e = cudaEventCreateWithFlags(&L->ov.join, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
-  L->bytes = (int64_t)(2 * fbytes + ncell * 7 * mb + g->nb * 16 * 8 + 56);
+  if ((e = cudaMalloc(&L->d_err, sizeof(uint32_t))) != cudaSuccess) return fail(e);
+  if ((e = cudaMemset(L->d_err, 0, sizeof(uint32_t))) != cudaSuccess) return fail(e);
+  if (L->dense) {
+    int sms = 0;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device)) != cudaSuccess) return fail(e);
+    int per = 1;
+    if (storage == OAL_STORE_F32) per = dense_ctas_per_sm<float>();
+    else if (storage == OAL_STORE_F16_DEV) per = dense_ctas_per_sm<__half>();
+    else per = dense_ctas_per_sm<__nv_bfloat16>();
+    L->dense_grid = sms * per;
+  }
+  L->bytes = (int64_t)(2 * fbytes + ncell * 7 * mb + g->nb * 16 * 8 + 60);
   *out = L;
   return OAL_OK;
 }
@@ -807,6 +967,7 @@ void oal_level_destroy(oal_level* L) {
   if (L->ov.side) cudaStreamDestroy(L->ov.side);
   if (L->ov.fork) cudaEventDestroy(L->ov.fork);
   if (L->ov.join) cudaEventDestroy(L->ov.join);
+  cudaFree(L->d_err);
   cudaGetLastError();  // teardown leaves no error behind for the next call
   auto* g = const_cast<oal_geometry*>(L->g);
   delete L;
@@ -892,7 +1053,7 @@ oal_status oal_level_get_state(oal_level* L, double* f, double* rho, double* vel
   if (e == cudaSuccess && vel) e = cudaMemcpy(vel, d_v, 3 * ncell * sizeof(double), cudaMemcpyDeviceToHost);
   cudaFree(d_f); cudaFree(d_r); cudaFree(d_v);
   if (e != cudaSuccess) return set_error(OAL_E_CUDA, "get_state: %s", cudaGetErrorString(e));
-  return OAL_OK;
+  return check_level_error(L);
 }
 
 // Enqueue one step of L on st (no host synchronisation).
@@ -904,13 +1065,29 @@ static oal_status enqueue_step(oal_level* L, const CaseParams& cp, cudaStream_t 
   level_layout(L, &bst, &kst);
   const int p = L->parity;
   a.nbr = g->d_nbr_ghost;
+  a.n_total_blocks = g->nb + g->n_ghost;
   a.f_in = L->f[p]; a.f_out = L->f[p ^ 1]; a.f_post = nullptr;
   a.rho_out = L->rho; a.vel_out = L->vel[p ^ 1]; a.vel_in = L->vel[p];
   a.f_bstride = bst; a.f_kstride = kst;
   a.v_bstride = 512; a.v_cstride = 512 * (int64_t)g->nb;
   a.force_part = L->d_force_part;
+  a.err = L->d_err;
   a.p0 = cp;
-  OAL_CUDA_TRY(launch_by_storage(L->storage, g, a, PATH_GHOSTED, st, &L->ov));
+  if (L->dense) {
+    a.dense = 1;
+    a.PX = L->PX; a.PY = L->PY; a.PZ = L->PZ;
+    a.f_bstride = 0;
+    a.p0.flags |= g->pmask;
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (L->storage) {
+      case OAL_STORE_F32: e = dense_step_t<float, float>(L, a, st); break;
+      case OAL_STORE_F16_DEV: e = dense_step_t<__half, float>(L, a, st); break;
+      case OAL_STORE_BF16_DEV: e = dense_step_t<__nv_bfloat16, float>(L, a, st); break;
+    }
+    OAL_CUDA_TRY(e);
+  } else {
+    OAL_CUDA_TRY(launch_by_storage(L->storage, g, a, PATH_GHOSTED, st, &L->ov));
+  }
   if (cp.flags & CF_COLLECT) {
     // the momentum exchange lives on the general kernel's CTAs (blocks near solids)
     if (g->n_general > 0) {
@@ -976,9 +1153,9 @@ oal_status oal_level_advance(oal_level* L, const oal_step_params* p, int32_t n, 
 oal_status oal_level_get_forces(oal_level* L, double out[3]) {
   if (!L || !out) return set_error(OAL_E_INVALID_ARG, "null argument");
   OAL_CUDA_TRY(cudaSetDevice(L->g->device));
-  if (!L->forces_valid) { out[0] = out[1] = out[2] = 0.0; return OAL_OK; }
+  if (!L->forces_valid) { out[0] = out[1] = out[2] = 0.0; return check_level_error(L); }
   OAL_CUDA_TRY(cudaMemcpy(out, L->d_force, 3 * sizeof(double), cudaMemcpyDeviceToHost));
-  return OAL_OK;
+  return check_level_error(L);
 }
 
 oal_status oal_level_get_forces_async(oal_level* L, double* host_out3, void* stream) {
@@ -1000,7 +1177,7 @@ oal_status oal_level_mass_momentum(oal_level* L, double out[4]) {
   }
   if (e != cudaSuccess) return set_error(OAL_E_CUDA, "mass_momentum: %s", cudaGetErrorString(e));
   OAL_CUDA_TRY(cudaMemcpy(out, L->d_mm, 4 * sizeof(double), cudaMemcpyDeviceToHost));
-  return OAL_OK;
+  return check_level_error(L);
 }
 
 oal_status oal_level_device_state(oal_level* L, void** f, void** rho, void** vel) {
@@ -1012,5 +1189,13 @@ oal_status oal_level_device_state(oal_level* L, void** f, void** rho, void** vel
 }
 
 int64_t oal_level_device_bytes(const oal_level* L) { return L ? L->bytes : 0; }
+
+oal_status oal_level_layout(const oal_level* L, int64_t out[6]) {
+  if (!L || !out) return set_error(OAL_E_INVALID_ARG, "null argument");
+  int64_t bst, kst;
+  level_layout(L, &bst, &kst);
+  out[0] = L->dense ? 1 : 0; out[1] = L->PX; out[2] = L->PY; out[3] = L->PZ; out[4] = bst; out[5] = kst;
+  return OAL_OK;
+}
 
 }  // extern "C"

@@ -168,12 +168,15 @@ class Geometry:
 class Level:
     """Library-owned state of one level: ping-pong populations, density, velocity."""
 
-    def __init__(self, geom: Geometry, operator: str = "cumulant", storage: str = "f32"):
+    def __init__(self, geom: Geometry, operator: str = "cumulant", storage: str = "f32", layout: str = "block"):
+        """layout "block": block-major populations with ghost blocks (default); "dense": the
+        padded grid with shared-memory-staged streaming (box levels in FP32/FP16/BF16)."""
         self.geom = geom
         self.storage = capi.STORAGE_NAMES[storage]
         self.operator = get_collision_kernel(operator)
+        flags = capi.OAL_LEVEL_DENSE if layout == "dense" else 0
         h = C.c_void_p()
-        check(lib().oal_level_create(geom.handle, self.operator, self.storage, C.byref(h)))
+        check(lib().oal_level_create_ex(geom.handle, self.operator, self.storage, flags, C.byref(h)))
         self.handle = h
         self.n_blocks = geom.dom.n_blocks
 
@@ -222,6 +225,11 @@ class Level:
         out = (C.c_double * 4)()
         check(lib().oal_level_mass_momentum(self.handle, out))
         return np.array(out[:])
+
+    def layout(self) -> dict:
+        out = (C.c_int64 * 6)()
+        check(lib().oal_level_layout(self.handle, out))
+        return dict(dense=bool(out[0]), PX=out[1], PY=out[2], PZ=out[3], block_stride=out[4], dir_stride=out[5])
 
     def device_bytes(self) -> int:
         return int(lib().oal_level_device_bytes(self.handle))

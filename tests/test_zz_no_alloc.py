@@ -22,11 +22,16 @@ RTOL = 1e-12  # both are FP64 sums of the same values in the same order
 
 
 def _noalloc(L, obstacle_dev, out_dev, n_blocks):
-    f = C.c_void_p()
-    capi.check(capi.lib().oal_level_device_state(L.handle, C.byref(f), None, None))
-    capi.check(capi.lib().oal_mass_momentum_noalloc(f, L.storage, 27 * 512, 512,
+    """The caller's own copy of the level's populations, in the reference layout (8,8,8,nb,27),
+    FP32 (exactly the decoded values the level sums), reduced without allocation."""
+    import torch
+    f, _, _ = L.state()
+    fd = torch.tensor(f, dtype=torch.float32, device="cuda").contiguous()
+    capi.check(capi.lib().oal_mass_momentum_noalloc(fd.data_ptr(), capi.OAL_STORE_F32, 512, 512 * n_blocks,
                                                     None if obstacle_dev is None else obstacle_dev.data_ptr(),
                                                     n_blocks, out_dev.data_ptr(), None))
+    torch.cuda.synchronize()
+    del fd
 
 
 @pytest.mark.parametrize("storage", ["f32", "f16"])
