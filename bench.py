@@ -195,6 +195,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--nz", type=int, default=128, help="channel depth (smaller values for profiling captures)")
     ap.add_argument("--layout", default="block", choices=["block", "dense"], help="population layout of the level")
+    ap.add_argument("--batch-steps", type=int, default=200,
+                    help="steps of the batched-vs-plain-loop comparison (64-case config 4); 0 skips it")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -316,6 +318,9 @@ def main():
             "drag_fx_lattice": force[0],
             "cd": force[0] * case.meta["drag_scale"],
         }
+        if args.batch_steps > 0:
+            from openaerolab_alpha_01_b200.workloads import config4
+            line["batched"] = config4(steps=args.batch_steps, storage=args.storage)
         print(json.dumps(line), flush=True)
 
     level.close()

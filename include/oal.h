@@ -250,6 +250,35 @@ int64_t oal_level_device_bytes(const oal_level* L);
  * Z = l+1); dense = 0: block-major f[b][k][cell], element b*block_stride + k*dir_stride + cell. */
 oal_status oal_level_layout(const oal_level* L, int64_t out[6]);
 
+/* ---- batches: many cases stepped by one launch per kernel ------------------------------------ */
+/* A batch owns a block pool (populations in `storage`, macros, masks) and steps every member case
+ * with one launch per kernel per step; n steps are one CUDA graph. Members are added and removed
+ * between advances without moving other members' state; each result is independent of the batch
+ * composition (per-case parameters, per-case fixed-order FP64 reductions). The reference runs
+ * cases one after another (src/main.jl:2184-2238); this is the batched form of
+ * execute_timestep_batch! (src/solver/solver_control.jl:796-828). */
+typedef struct oal_batch oal_batch;
+oal_status oal_batch_create(int32_t device, int32_t storage, int32_t max_real_blocks, int32_t max_ghost_blocks,
+                            int32_t max_mask_blocks, int32_t max_members, oal_batch** out);
+void oal_batch_destroy(oal_batch* B);
+/* Admit a case (block-layout geometry on the batch's device, its step parameters, equilibrium start
+ * from host rho(8,8,8,nb) / vel(8,8,8,nb,3) in double). OAL_E_ADMISSION when the pool has no room. */
+oal_status oal_batch_add(oal_batch* B, const oal_geometry* g, const oal_step_params* p, const double* rho_host,
+                         const double* vel_host, int32_t* member_out);
+oal_status oal_batch_remove(oal_batch* B, int32_t member);
+oal_status oal_batch_set_params(oal_batch* B, int32_t member, const oal_step_params* p);
+oal_status oal_batch_advance(oal_batch* B, int32_t n_steps, void* stream);
+/* Member state in the reference layout (double); synchronises. Any pointer may be NULL. */
+oal_status oal_batch_get_state(oal_batch* B, int32_t member, double* f, double* rho, double* vel);
+/* Momentum-exchange force of the member's last collecting step (FP64, lattice units); synchronises. */
+oal_status oal_batch_get_forces(oal_batch* B, int32_t member, double out[3]);
+oal_status oal_batch_mass_momentum(oal_batch* B, int32_t member, double out[4]);
+/* Pool usage: out = {members, real blocks used, ghost blocks used, mask blocks used,
+ * real capacity, ghost capacity, mask capacity, device bytes}. */
+oal_status oal_batch_info(const oal_batch* B, int64_t out[8]);
+/* Blocks one member of this geometry occupies: out = {real, ghost, mask}. */
+oal_status oal_geometry_blocks(const oal_geometry* g, int64_t out[3]);
+
 /* ---- no-allocation entry point -------------------------------------------------------------- */
 /* No counterpart in the reference. For callers that cannot call cudaMalloc when they need the
  * totals (a step recorded into a CUDA graph, a stream-ordered pool that forbids stray

@@ -5,6 +5,7 @@ its ctypes bindings and the host-side mirror of the reference's operator and ste
 """
 from ._capi import OALError, lib, default_params, StepParams  # noqa: F401
 from .solver import (  # noqa: F401
+    Batch,
     BlockDomain,
     Geometry,
     Level,
@@ -17,7 +18,7 @@ from .solver import (  # noqa: F401
 )
 
 __all__ = [
-    "OALError", "lib", "default_params", "StepParams", "BlockDomain", "Geometry", "Level",
+    "OALError", "lib", "default_params", "StepParams", "Batch", "BlockDomain", "Geometry", "Level",
     "apply_analytic_sphere_obstacle", "build_box", "default_step_params", "get_collision_kernel",
     "kinetic_energy", "taylor_green_fields",
 ]

@@ -156,6 +156,19 @@ _SIGNATURES = {
                                            C.POINTER(C.c_void_p)]),
     "oal_level_device_bytes": (C.c_int64, [C.c_void_p]),
     "oal_level_layout": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "oal_batch_create": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                     C.POINTER(C.c_void_p)]),
+    "oal_batch_destroy": (None, [C.c_void_p]),
+    "oal_batch_add": (C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(StepParams), C.c_void_p, C.c_void_p,
+                                  C.POINTER(C.c_int32)]),
+    "oal_batch_remove": (C.c_int32, [C.c_void_p, C.c_int32]),
+    "oal_batch_set_params": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(StepParams)]),
+    "oal_batch_advance": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p]),
+    "oal_batch_get_state": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "oal_batch_get_forces": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),
+    "oal_batch_mass_momentum": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),
+    "oal_batch_info": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "oal_geometry_blocks": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
     "oal_mass_momentum_noalloc": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int64, C.c_int64, C.c_void_p, C.c_int32,
                                               C.c_void_p, C.c_void_p]),
 }

@@ -244,6 +244,15 @@ struct oal_geometry {
   uint2* d_dense_gentries = nullptr;  // (block, cell | k << 9 | wrap << 31)
   int64_t n_dense_gentries = 0;
   int32_t* d_dense_fast = nullptr;    // uniform blocks, x fastest
+  // host copies of the block-layout tables (batches remap them into a shared block pool)
+  std::vector<int32_t> h_nbrg;       // [nb*27], ghost-indexed
+  std::vector<int4> h_binfo;
+  std::vector<uint32_t> h_bflags;
+  std::vector<int32_t> h_mslot;
+  std::vector<uint32_t> h_cmask;
+  std::vector<uint2> h_gentries;
+  std::vector<int32_t> h_fast, h_general;
+  std::vector<float> h_sponge, h_wdist;
   // levels built on this geometry; destroying the geometry while levels live defers the release
   // to the last level's destroy
   int32_t n_levels = 0;
@@ -778,6 +787,17 @@ oal_status oal_geometry_create(const oal_geometry_desc* d, int32_t device, oal_g
   }
   g->n_dense_gentries = (int64_t)dentries.size();
 
+  g->h_nbrg = nbrg;
+  g->h_binfo = binfo;
+  g->h_bflags = bflags;
+  g->h_mslot = mslot;
+  g->h_cmask = cmask;
+  g->h_gentries = gentries;
+  g->h_fast = fast;
+  g->h_general = general;
+  if (d->sponge) g->h_sponge.assign(d->sponge, d->sponge + nb * 512);
+  if (d->wall_dist) g->h_wdist.assign(d->wall_dist, d->wall_dist + nb * 512);
+
   auto fail = [&](oal_status s) { oal_geometry_destroy(g); return s; };
 #define GTRY(expr)                                                                         \
   do {                                                                                     \
@@ -1195,6 +1215,561 @@ oal_status oal_level_layout(const oal_level* L, int64_t out[6]) {
   int64_t bst, kst;
   level_layout(L, &bst, &kst);
   out[0] = L->dense ? 1 : 0; out[1] = L->PX; out[2] = L->PY; out[3] = L->PZ; out[4] = bst; out[5] = kst;
+  return OAL_OK;
+}
+
+}  // extern "C"
+
+// ================================================================================================
+// Batches: a block pool shared by many cases
+// ================================================================================================
+namespace {
+
+// first-fit allocator of index ranges
+struct RangeAlloc {
+  int64_t cap = 0;
+  std::vector<std::pair<int64_t, int64_t>> free_;  // (begin, length), sorted by begin
+  void init(int64_t c) { cap = c; free_.clear(); if (c > 0) free_.push_back({0, c}); }
+  int64_t alloc(int64_t n) {
+    if (n == 0) return 0;
+    for (size_t i = 0; i < free_.size(); ++i)
+      if (free_[i].second >= n) {
+        const int64_t b = free_[i].first;
+        free_[i].first += n; free_[i].second -= n;
+        if (free_[i].second == 0) free_.erase(free_.begin() + (long)i);
+        return b;
+      }
+    return -1;
+  }
+  void release(int64_t b, int64_t n) {
+    if (n == 0) return;
+    auto it = std::lower_bound(free_.begin(), free_.end(), std::make_pair(b, (int64_t)0));
+    it = free_.insert(it, {b, n});
+    // coalesce with neighbours
+    size_t i = (size_t)(it - free_.begin());
+    if (i + 1 < free_.size() && free_[i].first + free_[i].second == free_[i + 1].first) {
+      free_[i].second += free_[i + 1].second; free_.erase(free_.begin() + (long)i + 1);
+    }
+    if (i > 0 && free_[i - 1].first + free_[i - 1].second == free_[i].first) {
+      free_[i - 1].second += free_[i].second; free_.erase(free_.begin() + (long)i);
+    }
+  }
+  int64_t used() const { int64_t f = 0; for (auto& r : free_) f += r.second; return cap - f; }
+};
+
+// Equilibrium start of one member's real blocks inside the pool.
+template <class S, class R>
+__global__ void k_pool_init(const double* __restrict__ rho, const double* __restrict__ vel, int64_t ncell, int comp,
+                            S* __restrict__ f, R* __restrict__ rho_out, R* __restrict__ vel_out, int64_t vcs) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= ncell) return;
+  const int64_t b = i >> 9, cell = i & 511;
+  const R r = R(rho[i]), ux = R(vel[i]), uy = R(vel[i + ncell]), uz = R(vel[i + 2 * ncell]);
+  const R usq = ux * ux + uy * uy + uz * uz;
+#pragma unroll
+  for (int k = 0; k < kQ27; ++k) {
+    const R w = R(q27_w(k));
+    const R cu = R(q27_cx(k)) * ux + R(q27_cy(k)) * uy + R(q27_cz(k)) * uz;
+    R val = R(1) + R(3) * cu + R(4.5) * cu * cu - R(1.5) * usq;
+    if (comp) {
+      const R cu2 = cu * cu;
+      val += (R(4.5) * cu2 * cu - R(4.5) * cu * usq) + (R(3.375) * cu2 * cu2 - R(6.75) * cu2 * usq + R(1.125) * usq * usq);
+    }
+    f[b * 27 * kCells + k * kCells + cell] = Codec<S>::enc(r * w * val, w, R(1.0 / q27_w(k)));
+  }
+  rho_out[i] = r;
+  vel_out[i] = ux; vel_out[i + vcs] = uy; vel_out[i + 2 * vcs] = uz;
+}
+
+// One member's state out of the pool, reference layout (double).
+template <class S, class R>
+__global__ void k_pool_export(const S* __restrict__ f, const R* __restrict__ rho, const R* __restrict__ vel, int64_t vcs,
+                              int64_t ncell, double* __restrict__ fo, double* __restrict__ ro, double* __restrict__ vo) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= ncell) return;
+  const int64_t b = i >> 9, cell = i & 511;
+  if (fo)
+#pragma unroll
+    for (int k = 0; k < kQ27; ++k)
+      fo[i + ncell * k] = (double)Codec<S>::dec(f[b * 27 * kCells + k * kCells + cell], R(q27_w(k)), R(1.0 / q27_w(k)));
+  if (ro) ro[i] = (double)rho[i];
+  if (vo) { vo[i] = (double)vel[i]; vo[i + ncell] = (double)vel[i + vcs]; vo[i + 2 * ncell] = (double)vel[i + 2 * vcs]; }
+}
+
+// Per-member FP64 sums of consecutive CTA partial triples: member m owns [seg[m], seg[m+1]).
+__global__ void k_reduce3_segments(const double* __restrict__ part, const int32_t* __restrict__ seg, double* __restrict__ out) {
+  __shared__ double s[3][256];
+  const int m = blockIdx.x, t = threadIdx.x;
+  const int64_t b0 = seg[m], b1 = seg[m + 1];
+  double a0 = 0, a1 = 0, a2 = 0;
+  for (int64_t i = b0 + t; i < b1; i += 256) { a0 += part[3 * i]; a1 += part[3 * i + 1]; a2 += part[3 * i + 2]; }
+  s[0][t] = a0; s[1][t] = a1; s[2][t] = a2;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (t < w) { s[0][t] += s[0][t + w]; s[1][t] += s[1][t + w]; s[2][t] += s[2][t + w]; }
+    __syncthreads();
+  }
+  if (t == 0) { out[3 * m] = s[0][0]; out[3 * m + 1] = s[1][0]; out[3 * m + 2] = s[2][0]; }
+}
+
+}  // namespace
+
+struct BatchMember {
+  bool active = false;
+  const oal_geometry* g = nullptr;
+  oal_step_params p{};
+  CaseParams cp{};
+  int64_t rb = 0, gb = 0, mb = 0;  // pool bases: real blocks, ghost blocks, mask slots
+  int64_t nb = 0, ng = 0, nm = 0;
+  bool forces_valid = false;
+};
+
+struct oal_batch {
+  int device = 0;
+  int32_t storage = 0;
+  int64_t R = 0, G = 0, M = 0;  // capacities: real blocks, ghost blocks, mask slots
+  int32_t max_members = 0;
+  RangeAlloc ar, ag, am;
+  std::vector<BatchMember> mem;
+  void* f[2] = {nullptr, nullptr};
+  void* vel[2] = {nullptr, nullptr};
+  void* rho = nullptr;
+  int32_t* d_nbr = nullptr;      // [R*27] pool indices (ghosts at R + g)
+  int4* d_binfo = nullptr;       // [R] coords + member id
+  uint32_t* d_bflags = nullptr;  // [R]
+  int32_t* d_mslot = nullptr;    // [R]
+  uint32_t* d_cmask = nullptr;   // [M*512]
+  float* d_sponge = nullptr;     // [R*512] (allocated when a member brings one)
+  float* d_wdist = nullptr;
+  CaseParams* d_cases = nullptr;  // [max_members]
+  // work lists, rebuilt when membership changes
+  uint2* d_gentries = nullptr; int64_t n_gentries = 0, cap_gentries = 0;
+  int32_t* d_fast = nullptr; int64_t n_fast = 0;
+  int32_t* d_general = nullptr; int64_t n_general = 0;
+  int32_t* d_seg = nullptr;       // [max_members + 1] general-CTA segments per member
+  double* d_part = nullptr;       // [R*4*3]
+  double* d_forces = nullptr;     // [max_members*3]
+  double* d_mm_part = nullptr;    // [R*4]
+  double* d_mm = nullptr;         // [4]
+  int parity = 0;
+  bool dirty = true;
+  cudaStream_t cap = nullptr;
+  Overlap ov;
+  cudaGraphExec_t exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  int32_t graph_n = 0;
+  int graph_parity = -1;
+  int64_t bytes = 0;
+};
+
+static void batch_release_graph(oal_batch* B) {
+  if (B->exec) cudaGraphExecDestroy(B->exec);
+  if (B->graph) cudaGraphDestroy(B->graph);
+  B->exec = nullptr; B->graph = nullptr; B->graph_n = 0; B->graph_parity = -1;
+}
+
+// Combined work lists over the active members (host concatenation, then upload).
+static oal_status batch_rebuild(oal_batch* B) {
+  std::vector<uint2> ge;
+  std::vector<int32_t> fast, general, seg(1, 0);
+  std::vector<CaseParams> cases((size_t)B->max_members);
+  for (int32_t m = 0; m < B->max_members; ++m) {
+    const BatchMember& M = B->mem[(size_t)m];
+    if (M.active) {
+      const oal_geometry* g = M.g;
+      for (const uint2& e : g->h_gentries) ge.push_back(make_uint2((uint32_t)(M.rb + e.x), e.y));
+      for (int32_t b : g->h_fast) fast.push_back((int32_t)(M.rb + b));
+      for (int32_t b : g->h_general) general.push_back((int32_t)(M.rb + b));
+      cases[(size_t)m] = M.cp;
+    }
+    seg.push_back((int32_t)(general.size() * 4));
+  }
+  auto upload = [&](auto*& dptr, const auto& vec, int64_t& n) -> cudaError_t {
+    using Tv = typename std::remove_reference<decltype(vec)>::type::value_type;
+    cudaFree(dptr); dptr = nullptr; n = (int64_t)vec.size();
+    if (vec.empty()) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&dptr, vec.size() * sizeof(Tv));
+    if (e == cudaSuccess) e = cudaMemcpy(dptr, vec.data(), vec.size() * sizeof(Tv), cudaMemcpyHostToDevice);
+    return e;
+  };
+  OAL_CUDA_TRY(upload(B->d_gentries, ge, B->n_gentries));
+  OAL_CUDA_TRY(upload(B->d_fast, fast, B->n_fast));
+  OAL_CUDA_TRY(upload(B->d_general, general, B->n_general));
+  OAL_CUDA_TRY(cudaMemcpy(B->d_seg, seg.data(), seg.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  OAL_CUDA_TRY(cudaMemcpy(B->d_cases, cases.data(), cases.size() * sizeof(CaseParams), cudaMemcpyHostToDevice));
+  B->dirty = false;
+  batch_release_graph(B);
+  return OAL_OK;
+}
+
+template <class S, class R>
+static cudaError_t batch_step_t(oal_batch* B, const StepArgs& a, cudaStream_t st) {
+  cudaError_t e;
+  if ((e = launch_fill_ghosts<S, R>(a, B->d_gentries, B->n_gentries, st)) != cudaSuccess) return e;
+  const bool fork = B->n_general > 0 && B->n_fast > 0;
+  if (fork) {
+    if ((e = cudaEventRecord(B->ov.fork, st)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(B->ov.side, B->ov.fork, 0)) != cudaSuccess) return e;
+    if ((e = launch_general<S, R>(a, B->d_general, (int)B->n_general, B->ov.side)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(B->ov.join, B->ov.side)) != cudaSuccess) return e;
+    if ((e = launch_fast<S, R>(a, B->d_fast, (int)B->n_fast, st)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(st, B->ov.join, 0)) != cudaSuccess) return e;
+  } else {
+    if ((e = launch_fast<S, R>(a, B->d_fast, (int)B->n_fast, st)) != cudaSuccess) return e;
+    if ((e = launch_general<S, R>(a, B->d_general, (int)B->n_general, st)) != cudaSuccess) return e;
+  }
+  if (B->n_general > 0) {
+    k_reduce3_segments<<<B->max_members, 256, 0, st>>>(B->d_part, B->d_seg, B->d_forces);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+static oal_status batch_enqueue_step(oal_batch* B, int step_offset, cudaStream_t st) {
+  StepArgs a{};
+  a.nbr = B->d_nbr;
+  a.binfo = B->d_binfo;
+  a.bflags = B->d_bflags;
+  a.mslot = B->d_mslot;
+  a.cmask = B->d_cmask;
+  a.sponge = B->d_sponge;
+  a.wall_dist = B->d_wdist;
+  a.cases = B->d_cases;
+  a.n_blocks = (int32_t)B->R;
+  a.n_total_blocks = (int32_t)(B->R + B->G);
+  a.block_base = 0;
+  const int p = B->parity;
+  a.f_in = B->f[p]; a.f_out = B->f[p ^ 1]; a.f_post = nullptr;
+  a.rho_out = B->rho; a.vel_out = B->vel[p ^ 1]; a.vel_in = B->vel[p];
+  a.f_bstride = 27 * 512; a.f_kstride = 512;
+  a.v_bstride = 512; a.v_cstride = 512 * B->R;
+  a.force_part = B->d_part;
+  (void)step_offset;
+  cudaError_t e = cudaErrorInvalidValue;
+  switch (B->storage) {
+    case OAL_STORE_F32: e = batch_step_t<float, float>(B, a, st); break;
+    case OAL_STORE_F16_DEV: e = batch_step_t<__half, float>(B, a, st); break;
+    case OAL_STORE_BF16_DEV: e = batch_step_t<__nv_bfloat16, float>(B, a, st); break;
+    case OAL_STORE_F64: e = batch_step_t<double, double>(B, a, st); break;
+  }
+  OAL_CUDA_TRY(e);
+  B->parity ^= 1;
+  return OAL_OK;
+}
+
+template <class S, class R>
+static cudaError_t pool_init_t(oal_batch* B, const BatchMember& M, const double* d_rho, const double* d_vel, int comp) {
+  const int64_t ncell = M.nb * 512;
+  k_pool_init<S, R><<<nblk(ncell, 256), 256>>>(d_rho, d_vel, ncell, comp,
+                                              static_cast<S*>(B->f[B->parity]) + M.rb * 27 * 512,
+                                              static_cast<R*>(B->rho) + M.rb * 512,
+                                              static_cast<R*>(B->vel[B->parity]) + M.rb * 512, 512 * B->R);
+  return cudaGetLastError();
+}
+
+template <class S, class R>
+static cudaError_t pool_export_t(oal_batch* B, const BatchMember& M, double* fo, double* ro, double* vo) {
+  const int64_t ncell = M.nb * 512;
+  k_pool_export<S, R><<<nblk(ncell, 256), 256>>>(static_cast<const S*>(B->f[B->parity]) + M.rb * 27 * 512,
+                                                static_cast<const R*>(B->rho) + M.rb * 512,
+                                                static_cast<const R*>(B->vel[B->parity]) + M.rb * 512, 512 * B->R,
+                                                ncell, fo, ro, vo);
+  return cudaGetLastError();
+}
+
+template <class S, class R>
+static cudaError_t pool_mm_t(oal_batch* B, const BatchMember& M) {
+  PopIndex pi{};
+  pi.binfo = B->d_binfo + M.rb; pi.dense = 0; pi.bst = 27 * 512; pi.kst = 512;
+  k_mass_momentum<S, R><<<(unsigned)M.nb, 128>>>(static_cast<const S*>(B->f[B->parity]) + M.rb * 27 * 512, pi,
+                                                B->d_bflags + M.rb, B->d_mslot + M.rb, B->d_cmask, B->d_mm_part);
+  k_reduce4<<<1, 256>>>(B->d_mm_part, M.nb, B->d_mm);
+  return cudaGetLastError();
+}
+
+extern "C" {
+
+oal_status oal_geometry_blocks(const oal_geometry* g, int64_t out[3]) {
+  if (!g || !out) return set_error(OAL_E_INVALID_ARG, "null argument");
+  out[0] = g->nb; out[1] = g->n_ghost; out[2] = g->n_slots;
+  return OAL_OK;
+}
+
+void oal_batch_destroy(oal_batch* B) {
+  if (!B) return;
+  cudaSetDevice(B->device);
+  batch_release_graph(B);
+  for (int i = 0; i < 2; ++i) { cudaFree(B->f[i]); cudaFree(B->vel[i]); }
+  cudaFree(B->rho); cudaFree(B->d_nbr); cudaFree(B->d_binfo); cudaFree(B->d_bflags); cudaFree(B->d_mslot);
+  cudaFree(B->d_cmask); cudaFree(B->d_sponge); cudaFree(B->d_wdist); cudaFree(B->d_cases);
+  cudaFree(B->d_gentries); cudaFree(B->d_fast); cudaFree(B->d_general); cudaFree(B->d_seg);
+  cudaFree(B->d_part); cudaFree(B->d_forces); cudaFree(B->d_mm_part); cudaFree(B->d_mm);
+  if (B->cap) cudaStreamDestroy(B->cap);
+  if (B->ov.side) cudaStreamDestroy(B->ov.side);
+  if (B->ov.fork) cudaEventDestroy(B->ov.fork);
+  if (B->ov.join) cudaEventDestroy(B->ov.join);
+  for (auto& M : B->mem)
+    if (M.active && M.g) {
+      auto* g = const_cast<oal_geometry*>(M.g);
+      if (--g->n_levels == 0 && g->destroy_requested) geometry_release(g);
+    }
+  cudaGetLastError();
+  delete B;
+}
+
+oal_status oal_batch_create(int32_t device, int32_t storage, int32_t max_real, int32_t max_ghost, int32_t max_mask,
+                            int32_t max_members, oal_batch** out) {
+  if (!out) return set_error(OAL_E_INVALID_ARG, "null argument");
+  *out = nullptr;
+  if (storage < OAL_STORE_F32 || storage > OAL_STORE_F64) return set_error(OAL_E_INVALID_ARG, "storage %d", storage);
+  if (max_real <= 0 || max_ghost < 0 || max_mask < 0 || max_members <= 0 || max_members > 4096)
+    return set_error(OAL_E_INVALID_ARG, "bad batch capacities");
+  if ((int64_t)(max_real + max_ghost) * 27 * 512 >= (1ll << 32))
+    return set_error(OAL_E_TOO_LARGE, "a batch pool holds fewer than 2^32 population elements");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return set_error(OAL_E_NO_DEVICE, "no CUDA device visible"); }
+  OAL_CUDA_TRY(cudaSetDevice(device));
+  auto* B = new oal_batch();
+  B->device = device; B->storage = storage;
+  B->R = max_real; B->G = max_ghost; B->M = max_mask; B->max_members = max_members;
+  B->ar.init(B->R); B->ag.init(B->G); B->am.init(B->M);
+  B->mem.resize((size_t)max_members);
+  const size_t fbytes = (size_t)(B->R + B->G) * 27 * 512 * storage_bytes(storage);
+  const size_t mb = macro_bytes(storage);
+  const size_t ncell = (size_t)B->R * 512;
+  cudaError_t e = cudaSuccess;
+  auto A = [&](void** p, size_t n) { if (e == cudaSuccess && n) e = cudaMalloc(p, n); };
+  for (int i = 0; i < 2; ++i) { A(&B->f[i], fbytes); A(&B->vel[i], ncell * 3 * mb); }
+  A(&B->rho, ncell * mb);
+  A((void**)&B->d_nbr, (size_t)B->R * 27 * sizeof(int32_t));
+  A((void**)&B->d_binfo, (size_t)B->R * sizeof(int4));
+  A((void**)&B->d_bflags, (size_t)B->R * sizeof(uint32_t));
+  A((void**)&B->d_mslot, (size_t)B->R * sizeof(int32_t));
+  A((void**)&B->d_cmask, (size_t)B->M * 512 * sizeof(uint32_t));
+  A((void**)&B->d_cases, (size_t)max_members * sizeof(CaseParams));
+  A((void**)&B->d_seg, (size_t)(max_members + 1) * sizeof(int32_t));
+  A((void**)&B->d_part, (size_t)B->R * 4 * 3 * sizeof(double));
+  A((void**)&B->d_forces, (size_t)max_members * 3 * sizeof(double));
+  A((void**)&B->d_mm_part, (size_t)B->R * 4 * sizeof(double));
+  A((void**)&B->d_mm, 4 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemset(B->f[0], 0, fbytes);
+  if (e == cudaSuccess) e = cudaMemset(B->f[1], 0, fbytes);
+  if (e == cudaSuccess) e = cudaMemset(B->d_forces, 0, (size_t)max_members * 3 * sizeof(double));
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&B->ov.side, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&B->ov.fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&B->ov.join, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    oal_batch_destroy(B);
+    return set_error(e == cudaErrorMemoryAllocation ? OAL_E_OUT_OF_MEMORY : OAL_E_CUDA, "batch allocation: %s",
+                     cudaGetErrorString(e));
+  }
+  B->bytes = (int64_t)(2 * fbytes + ncell * 7 * mb + (size_t)B->R * (27 * 4 + 16 + 4 + 4 + 96 + 32) +
+                       (size_t)B->M * 2048 + (size_t)max_members * 112);
+  *out = B;
+  return OAL_OK;
+}
+
+
+oal_status oal_batch_add(oal_batch* B, const oal_geometry* g, const oal_step_params* p, const double* rho,
+                         const double* vel, int32_t* member_out) {
+  if (!B || !g || !p || !rho || !vel || !member_out) return set_error(OAL_E_INVALID_ARG, "null argument");
+  if (g->device != B->device) return set_error(OAL_E_INVALID_ARG, "geometry and batch on different devices");
+  CaseParams cp;
+  oal_status s = resolve_params(p, g, &cp);
+  if (s != OAL_OK) return s;
+  if (cp.flags & CF_STORE_POST) return set_error(OAL_E_UNSUPPORTED, "store_post_collision needs caller-owned arrays");
+  int32_t m = -1;
+  for (int32_t i = 0; i < B->max_members; ++i)
+    if (!B->mem[(size_t)i].active) { m = i; break; }
+  if (m < 0) return set_error(OAL_E_ADMISSION, "no free member slot (max_members %d)", B->max_members);
+  const int64_t rb = B->ar.alloc(g->nb);
+  const int64_t gb = rb >= 0 ? B->ag.alloc(g->n_ghost) : -1;
+  const int64_t mbase = gb >= 0 ? B->am.alloc(g->n_slots) : -1;
+  if (rb < 0 || gb < 0 || mbase < 0) {
+    if (gb >= 0) B->ag.release(gb, g->n_ghost);
+    if (rb >= 0) B->ar.release(rb, g->nb);
+    return set_error(OAL_E_ADMISSION, "the block pool has no room for %lld real / %lld ghost / %lld mask blocks",
+                     (long long)g->nb, (long long)g->n_ghost, (long long)g->n_slots);
+  }
+  OAL_CUDA_TRY(cudaSetDevice(B->device));
+  BatchMember& M = B->mem[(size_t)m];
+  M = BatchMember();
+  M.active = true; M.g = g; M.p = *p; M.cp = cp;
+  M.rb = rb; M.gb = gb; M.mb = mbase; M.nb = g->nb; M.ng = g->n_ghost; M.nm = g->n_slots;
+  ++const_cast<oal_geometry*>(g)->n_levels;
+  // static tables of the member, remapped into the pool
+  const int64_t nb = g->nb;
+  std::vector<int32_t> nbr((size_t)nb * 27);
+  for (size_t i = 0; i < nbr.size(); ++i) {
+    const int32_t v = g->h_nbrg[i];
+    nbr[i] = v < 0 ? -1 : (v < g->nb ? (int32_t)(rb + v) : (int32_t)(B->R + gb + (v - g->nb)));
+  }
+  std::vector<int4> bi(g->h_binfo);
+  for (auto& x : bi) x.w = m;
+  std::vector<int32_t> ms(g->h_mslot);
+  for (auto& x : ms) if (x >= 0) x = (int32_t)(mbase + x);
+  cudaError_t e = cudaMemcpy(B->d_nbr + rb * 27, nbr.data(), nbr.size() * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(B->d_binfo + rb, bi.data(), bi.size() * sizeof(int4), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(B->d_bflags + rb, g->h_bflags.data(), (size_t)nb * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(B->d_mslot + rb, ms.data(), (size_t)nb * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !g->h_cmask.empty())
+    e = cudaMemcpy(B->d_cmask + mbase * 512, g->h_cmask.data(), g->h_cmask.size() * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !g->h_sponge.empty()) {
+    if (!B->d_sponge) {
+      e = cudaMalloc(&B->d_sponge, (size_t)B->R * 512 * sizeof(float));
+      if (e == cudaSuccess) e = cudaMemset(B->d_sponge, 0, (size_t)B->R * 512 * sizeof(float));
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(B->d_sponge + rb * 512, g->h_sponge.data(), g->h_sponge.size() * 4, cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess && !g->h_wdist.empty()) {
+    if (!B->d_wdist) {
+      e = cudaMalloc(&B->d_wdist, (size_t)B->R * 512 * sizeof(float));
+      if (e == cudaSuccess) e = cudaMemset(B->d_wdist, 0, (size_t)B->R * 512 * sizeof(float));
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(B->d_wdist + rb * 512, g->h_wdist.data(), g->h_wdist.size() * 4, cudaMemcpyHostToDevice);
+  }
+  // equilibrium start into the current input buffer
+  double *d_rho = nullptr, *d_vel = nullptr;
+  const int64_t ncell = nb * 512;
+  if (e == cudaSuccess) e = cudaMalloc(&d_rho, ncell * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&d_vel, 3 * ncell * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpy(d_rho, rho, ncell * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_vel, vel, 3 * ncell * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    switch (B->storage) {
+      case OAL_STORE_F32: e = pool_init_t<float, float>(B, M, d_rho, d_vel, p->compressible_corr); break;
+      case OAL_STORE_F16_DEV: e = pool_init_t<__half, float>(B, M, d_rho, d_vel, p->compressible_corr); break;
+      case OAL_STORE_BF16_DEV: e = pool_init_t<__nv_bfloat16, float>(B, M, d_rho, d_vel, p->compressible_corr); break;
+      case OAL_STORE_F64: e = pool_init_t<double, double>(B, M, d_rho, d_vel, p->compressible_corr); break;
+    }
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  cudaFree(d_rho); cudaFree(d_vel);
+  if (e != cudaSuccess) {
+    oal_batch_remove(B, m);
+    return set_error(OAL_E_CUDA, "batch_add: %s", cudaGetErrorString(e));
+  }
+  B->dirty = true;
+  *member_out = m;
+  return OAL_OK;
+}
+
+oal_status oal_batch_remove(oal_batch* B, int32_t m) {
+  if (!B || m < 0 || m >= B->max_members || !B->mem[(size_t)m].active) return set_error(OAL_E_INVALID_ARG, "no such member");
+  BatchMember& M = B->mem[(size_t)m];
+  B->ar.release(M.rb, M.nb); B->ag.release(M.gb, M.ng); B->am.release(M.mb, M.nm);
+  auto* g = const_cast<oal_geometry*>(M.g);
+  M = BatchMember();
+  if (--g->n_levels == 0 && g->destroy_requested) geometry_release(g);
+  B->dirty = true;
+  return OAL_OK;
+}
+
+oal_status oal_batch_set_params(oal_batch* B, int32_t m, const oal_step_params* p) {
+  if (!B || m < 0 || m >= B->max_members || !B->mem[(size_t)m].active) return set_error(OAL_E_INVALID_ARG, "no such member");
+  CaseParams cp;
+  oal_status s = resolve_params(p, B->mem[(size_t)m].g, &cp);
+  if (s != OAL_OK) return s;
+  B->mem[(size_t)m].p = *p; B->mem[(size_t)m].cp = cp;
+  B->dirty = true;
+  return OAL_OK;
+}
+
+oal_status oal_batch_advance(oal_batch* B, int32_t n, void* stream) {
+  if (!B) return set_error(OAL_E_INVALID_ARG, "null batch");
+  if (n <= 0) return set_error(OAL_E_INVALID_ARG, "n_steps must be positive");
+  OAL_CUDA_TRY(cudaSetDevice(B->device));
+  if (B->dirty) {
+    // a rebuild must not race with steps still in flight on the caller's stream
+    OAL_CUDA_TRY(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    oal_status s = batch_rebuild(B);
+    if (s != OAL_OK) return s;
+  }
+  if (B->n_fast + B->n_general == 0) return OAL_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (!(B->exec && B->graph_n == n && B->graph_parity == B->parity)) {
+    batch_release_graph(B);
+    const int start = B->parity;
+    OAL_CUDA_TRY(cudaStreamBeginCapture(B->cap, cudaStreamCaptureModeThreadLocal));
+    oal_status es = OAL_OK;
+    for (int i = 0; i < n && es == OAL_OK; ++i) es = batch_enqueue_step(B, i, B->cap);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(B->cap, &graph);
+    B->parity = start;
+    if (es != OAL_OK) { if (graph) cudaGraphDestroy(graph); return es; }
+    if (e != cudaSuccess) return set_error(OAL_E_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) { cudaGraphDestroy(graph); return set_error(OAL_E_CUDA, "graph instantiate: %s", cudaGetErrorString(e)); }
+    B->exec = exec; B->graph = graph; B->graph_n = n; B->graph_parity = start;
+  }
+  OAL_CUDA_TRY(cudaGraphLaunch(B->exec, st));
+  if (n & 1) B->parity ^= 1;
+  for (auto& M : B->mem)
+    if (M.active && (M.cp.flags & CF_COLLECT)) M.forces_valid = true;
+  return OAL_OK;
+}
+
+
+oal_status oal_batch_get_state(oal_batch* B, int32_t m, double* f, double* rho, double* vel) {
+  if (!B || m < 0 || m >= B->max_members || !B->mem[(size_t)m].active) return set_error(OAL_E_INVALID_ARG, "no such member");
+  OAL_CUDA_TRY(cudaSetDevice(B->device));
+  OAL_CUDA_TRY(cudaDeviceSynchronize());
+  const BatchMember& M = B->mem[(size_t)m];
+  const int64_t ncell = M.nb * 512;
+  double *df = nullptr, *dr = nullptr, *dv = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (f) e = cudaMalloc(&df, 27 * ncell * sizeof(double));
+  if (e == cudaSuccess && rho) e = cudaMalloc(&dr, ncell * sizeof(double));
+  if (e == cudaSuccess && vel) e = cudaMalloc(&dv, 3 * ncell * sizeof(double));
+  if (e == cudaSuccess) {
+    switch (B->storage) {
+      case OAL_STORE_F32: e = pool_export_t<float, float>(B, M, df, dr, dv); break;
+      case OAL_STORE_F16_DEV: e = pool_export_t<__half, float>(B, M, df, dr, dv); break;
+      case OAL_STORE_BF16_DEV: e = pool_export_t<__nv_bfloat16, float>(B, M, df, dr, dv); break;
+      case OAL_STORE_F64: e = pool_export_t<double, double>(B, M, df, dr, dv); break;
+    }
+  }
+  if (e == cudaSuccess && f) e = cudaMemcpy(f, df, 27 * ncell * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && rho) e = cudaMemcpy(rho, dr, ncell * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && vel) e = cudaMemcpy(vel, dv, 3 * ncell * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(df); cudaFree(dr); cudaFree(dv);
+  if (e != cudaSuccess) return set_error(OAL_E_CUDA, "batch_get_state: %s", cudaGetErrorString(e));
+  return OAL_OK;
+}
+
+oal_status oal_batch_get_forces(oal_batch* B, int32_t m, double out[3]) {
+  if (!B || !out || m < 0 || m >= B->max_members || !B->mem[(size_t)m].active) return set_error(OAL_E_INVALID_ARG, "no such member");
+  OAL_CUDA_TRY(cudaSetDevice(B->device));
+  if (!B->mem[(size_t)m].forces_valid || B->n_general == 0) { out[0] = out[1] = out[2] = 0.0; return OAL_OK; }
+  OAL_CUDA_TRY(cudaMemcpy(out, B->d_forces + 3 * m, 3 * sizeof(double), cudaMemcpyDeviceToHost));
+  return OAL_OK;
+}
+
+
+oal_status oal_batch_mass_momentum(oal_batch* B, int32_t m, double out[4]) {
+  if (!B || !out || m < 0 || m >= B->max_members || !B->mem[(size_t)m].active) return set_error(OAL_E_INVALID_ARG, "no such member");
+  OAL_CUDA_TRY(cudaSetDevice(B->device));
+  const BatchMember& M = B->mem[(size_t)m];
+  cudaError_t e = cudaErrorInvalidValue;
+  switch (B->storage) {
+    case OAL_STORE_F32: e = pool_mm_t<float, float>(B, M); break;
+    case OAL_STORE_F16_DEV: e = pool_mm_t<__half, float>(B, M); break;
+    case OAL_STORE_BF16_DEV: e = pool_mm_t<__nv_bfloat16, float>(B, M); break;
+    case OAL_STORE_F64: e = pool_mm_t<double, double>(B, M); break;
+  }
+  OAL_CUDA_TRY(e);
+  OAL_CUDA_TRY(cudaMemcpy(out, B->d_mm, 4 * sizeof(double), cudaMemcpyDeviceToHost));
+  return OAL_OK;
+}
+
+oal_status oal_batch_info(const oal_batch* B, int64_t out[8]) {
+  if (!B || !out) return set_error(OAL_E_INVALID_ARG, "null argument");
+  int64_t n = 0;
+  for (auto& M : B->mem) n += M.active ? 1 : 0;
+  out[0] = n; out[1] = B->ar.used(); out[2] = B->ag.used(); out[3] = B->am.used();
+  out[4] = B->R; out[5] = B->G; out[6] = B->M; out[7] = B->bytes;
   return OAL_OK;
 }
 

@@ -147,6 +147,12 @@ class Geometry:
         check(lib().oal_geometry_create(C.byref(desc), device, C.byref(h)))
         self.handle = h
 
+    def blocks(self) -> tuple[int, int, int]:
+        """(real, ghost, mask) blocks one member of this geometry occupies in a batch pool."""
+        out = (C.c_int64 * 3)()
+        check(lib().oal_geometry_blocks(self.handle, out))
+        return int(out[0]), int(out[1]), int(out[2])
+
     def info(self) -> dict:
         out = (C.c_int64 * 5)()
         check(lib().oal_geometry_info(self.handle, out))
@@ -237,6 +243,81 @@ class Level:
     def close(self):
         if getattr(self, "handle", None):
             lib().oal_level_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many cases stepped together: one block pool, one launch per kernel per step for all members,
+    n steps per CUDA graph (oal_batch_*). Members join and leave between advances."""
+
+    def __init__(self, storage: str = "f16", max_real_blocks: int = 65536, max_ghost_blocks: int = 16384,
+                 max_mask_blocks: int = 4096, max_members: int = 256, device: int = 0):
+        self.storage = capi.STORAGE_NAMES[storage]
+        h = C.c_void_p()
+        check(lib().oal_batch_create(device, self.storage, max_real_blocks, max_ghost_blocks, max_mask_blocks,
+                                     max_members, C.byref(h)))
+        self.handle = h
+        self._geoms = {}
+
+    def add(self, geom: Geometry, params: capi.StepParams, rho: np.ndarray, vel: np.ndarray) -> int:
+        rho = np.ascontiguousarray(rho, dtype=np.float64)
+        vel = np.ascontiguousarray(vel, dtype=np.float64)
+        m = C.c_int32()
+        check(lib().oal_batch_add(self.handle, geom.handle, C.byref(params), rho.ctypes.data, vel.ctypes.data,
+                                  C.byref(m)))
+        self._geoms[m.value] = geom
+        return m.value
+
+    def try_add(self, geom: Geometry, params: capi.StepParams, rho: np.ndarray, vel: np.ndarray) -> Optional[int]:
+        """add(), or None when the pool has no room (OAL_E_ADMISSION)."""
+        try:
+            return self.add(geom, params, rho, vel)
+        except capi.OALError as e:
+            if e.status == capi.OAL_E_ADMISSION:
+                return None
+            raise
+
+    def remove(self, member: int) -> None:
+        check(lib().oal_batch_remove(self.handle, member))
+        self._geoms.pop(member, None)
+
+    def set_params(self, member: int, params: capi.StepParams) -> None:
+        check(lib().oal_batch_set_params(self.handle, member, C.byref(params)))
+
+    def advance(self, n_steps: int, stream=None) -> None:
+        check(lib().oal_batch_advance(self.handle, int(n_steps), _stream_handle(stream)))
+
+    def state(self, member: int):
+        nb = self._geoms[member].dom.n_blocks
+        f = np.empty((27, nb, 512)); rho = np.empty((nb, 512)); vel = np.empty((3, nb, 512))
+        check(lib().oal_batch_get_state(self.handle, member, f.ctypes.data, rho.ctypes.data, vel.ctypes.data))
+        return f, rho, vel
+
+    def forces(self, member: int) -> np.ndarray:
+        out = (C.c_double * 3)()
+        check(lib().oal_batch_get_forces(self.handle, member, out))
+        return np.array(out[:])
+
+    def mass_momentum(self, member: int) -> np.ndarray:
+        out = (C.c_double * 4)()
+        check(lib().oal_batch_mass_momentum(self.handle, member, out))
+        return np.array(out[:])
+
+    def info(self) -> dict:
+        out = (C.c_int64 * 8)()
+        check(lib().oal_batch_info(self.handle, out))
+        keys = ["members", "real_used", "ghost_used", "mask_used", "real_cap", "ghost_cap", "mask_cap", "bytes"]
+        return dict(zip(keys, [int(v) for v in out]))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().oal_batch_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -1,0 +1,81 @@
+"""Batched stepping (oal_batch_*): every member's result is bit-identical to the same case run
+alone, across storages, mixed case kinds, membership changes and pool admission."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+from openaerolab_alpha_01_b200 import _capi as capi
+from openaerolab_alpha_01_b200.cases import sphere_channel_case, taylor_green_case
+from openaerolab_alpha_01_b200.solver import Batch, Geometry, Level
+
+
+def mixed_cases():
+    return [taylor_green_case(16, u0=0.05, re=100.0, c_wale=0.2),
+            sphere_channel_case(32, 16, 16, diameter=6.0, centre_x=10.0, u_inlet=0.05, re=100.0),
+            taylor_green_case(24, u0=0.03, re=400.0, c_wale=0.0, phase=(1.5, 2.5)),
+            sphere_channel_case(24, 16, 16, diameter=5.0, centre_x=8.0, u_inlet=0.04, re=80.0,
+                                solid_bc=capi.OAL_SOLID_FULLWAY)]
+
+
+def alone(case, storage, steps):
+    g = Geometry(case.dom)
+    L = Level(g, storage=storage)
+    L.init_equilibrium(case.rho, case.vel)
+    L.execute_timestep_batch(case.params, steps)
+    f, rho, vel = L.state()
+    out = (f, rho, vel, L.forces(), L.mass_momentum())
+    L.close(); g.close()
+    return out
+
+
+@pytest.mark.parametrize("storage", ["f16", "f32", "f64"])
+def test_members_match_alone_bitwise(oal, storage):
+    cases = mixed_cases()
+    steps = 9
+    B = Batch(storage=storage, max_real_blocks=256, max_ghost_blocks=256, max_mask_blocks=64, max_members=8)
+    geoms = [Geometry(c.dom) for c in cases]
+    ids = [B.add(g, c.params, c.rho, c.vel) for g, c in zip(geoms, cases)]
+    B.advance(4)
+    B.advance(5)
+    for c, m in zip(cases, ids):
+        f, rho, vel, force, mm = alone(c, storage, steps)
+        fb, rb, vb = B.state(m)
+        assert np.array_equal(fb, f) and np.array_equal(vb, vel) and np.array_equal(rb, rho), c.name
+        assert np.array_equal(B.forces(m), force), c.name
+        assert np.array_equal(B.mass_momentum(m), mm), c.name
+    B.close()
+
+
+def test_membership_changes_leave_others_untouched(oal):
+    cases = mixed_cases()
+    B = Batch(storage="f32", max_real_blocks=256, max_ghost_blocks=256, max_mask_blocks=64, max_members=8)
+    geoms = [Geometry(c.dom) for c in cases]
+    a = B.add(geoms[0], cases[0].params, cases[0].rho, cases[0].vel)
+    b = B.add(geoms[1], cases[1].params, cases[1].rho, cases[1].vel)
+    B.advance(3)
+    c = B.add(geoms[2], cases[2].params, cases[2].rho, cases[2].vel)   # joins mid-run
+    B.remove(b)                                                         # leaves mid-run
+    d = B.add(geoms[3], cases[3].params, cases[3].rho, cases[3].vel)   # reuses the freed blocks
+    B.advance(4)
+    fa = alone(cases[0], "f32", 7)[0]
+    fc = alone(cases[2], "f32", 4)[0]
+    fd = alone(cases[3], "f32", 4)[0]
+    assert np.array_equal(B.state(a)[0], fa)
+    assert np.array_equal(B.state(c)[0], fc)
+    assert np.array_equal(B.state(d)[0], fd)
+    assert B.info()["members"] == 3
+    B.close()
+
+
+def test_admission_by_pool_capacity(oal):
+    case = taylor_green_case(32)  # 64 blocks
+    g = Geometry(case.dom)
+    B = Batch(storage="f16", max_real_blocks=130, max_ghost_blocks=0, max_mask_blocks=0, max_members=4)
+    assert B.try_add(g, case.params, case.rho, case.vel) is not None
+    m2 = B.try_add(g, case.params, case.rho, case.vel)
+    assert m2 is not None
+    assert B.try_add(g, case.params, case.rho, case.vel) is None   # 3 x 64 > 130
+    B.remove(m2)
+    assert B.try_add(g, case.params, case.rho, case.vel) is not None
+    B.close()
