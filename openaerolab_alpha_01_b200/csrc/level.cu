@@ -253,6 +253,8 @@ struct oal_geometry {
   std::vector<uint2> h_gentries;
   std::vector<int32_t> h_fast, h_general;
   std::vector<float> h_sponge, h_wdist;
+  std::vector<int32_t> h_box_at;     // box levels: block index at ((bx-1)*by + by-1)*bz + bz-1
+  bool dense_tables = false;
   // levels built on this geometry; destroying the geometry while levels live defers the release
   // to the last level's destroy
   int32_t n_levels = 0;
@@ -473,6 +475,58 @@ static oal_status check_level_error(oal_level* L) {
   return set_error(OAL_E_TIMEOUT, "a bounded device wait gave up (code 0x%x); the step's results are invalid", w);
 }
 
+// Dense ghost-frame slots and the x-fastest uniform work order of a box geometry (first dense level).
+static oal_status build_dense_tables(oal_geometry* g) {
+  if (g->dense_tables) return OAL_OK;
+  const int64_t nb = g->nb;
+  const int bxm = g->bdim[0], bym = g->bdim[1], bzm = g->bdim[2];
+  const int N[3] = {8 * bxm, 8 * bym, 8 * bzm};
+  const bool per[3] = {(g->pmask & CF_PERIODIC_X) != 0, (g->pmask & CF_PERIODIC_Y) != 0, (g->pmask & CF_PERIODIC_Z) != 0};
+  std::vector<uint2> dentries;
+  // every (cell, k) whose source leaves the box; a crossing of periodic axes only is a copy of the
+  // wrapped interior cell, any other goes through the face rules
+  for (int64_t b = 0; b < nb; ++b) {
+    const int4 bi = g->h_binfo[(size_t)b];
+    const int g0[3] = {(bi.x - 1) * 8, (bi.y - 1) * 8, (bi.z - 1) * 8};
+    const bool edge = g0[0] == 0 || g0[1] == 0 || g0[2] == 0 || g0[0] + 8 == N[0] || g0[1] + 8 == N[1] || g0[2] + 8 == N[2];
+    if (!edge) continue;
+    for (int cell = 0; cell < 512; ++cell) {
+      const int c3[3] = {g0[0] + (cell & 7), g0[1] + ((cell >> 3) & 7), g0[2] + (cell >> 6)};
+      for (int k = 0; k < 27; ++k) {
+        const int ck[3] = {q27_cx(k), q27_cy(k), q27_cz(k)};
+        bool out = false, face = false;
+        for (int ax = 0; ax < 3; ++ax) {
+          const int sc = c3[ax] - ck[ax];
+          if (sc < 0 || sc >= N[ax]) { out = true; if (!per[ax]) face = true; }
+        }
+        if (out) dentries.push_back(make_uint2((uint32_t)b, (uint32_t)cell | ((uint32_t)k << 9) | (face ? 0u : (1u << 31))));
+      }
+    }
+  }
+  std::vector<uint8_t> gen((size_t)nb, 0);
+  for (int32_t b : g->h_general) gen[(size_t)b] = 1;
+  std::vector<int32_t> dfast;
+  // uniform blocks ordered x fastest, so CTAs running together write neighbouring rows
+  for (int bz = 1; bz <= bzm; ++bz)
+    for (int by = 1; by <= bym; ++by)
+      for (int bx = 1; bx <= bxm; ++bx) {
+        const int32_t b = g->h_box_at[((size_t)(bx - 1) * bym + (by - 1)) * bzm + (bz - 1)];
+        if (!gen[(size_t)b]) dfast.push_back(b);
+      }
+  OAL_CUDA_TRY(cudaSetDevice(g->device));
+  if (!dentries.empty()) {
+    OAL_CUDA_TRY(cudaMalloc(&g->d_dense_gentries, dentries.size() * sizeof(uint2)));
+    OAL_CUDA_TRY(cudaMemcpy(g->d_dense_gentries, dentries.data(), dentries.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+  }
+  if (!dfast.empty()) {
+    OAL_CUDA_TRY(cudaMalloc(&g->d_dense_fast, dfast.size() * sizeof(int32_t)));
+    OAL_CUDA_TRY(cudaMemcpy(g->d_dense_fast, dfast.data(), dfast.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  }
+  g->n_dense_gentries = (int64_t)dentries.size();
+  g->dense_tables = true;
+  return OAL_OK;
+}
+
 // ------------------------------------------------------------------------------------------------
 // C ABI
 // ------------------------------------------------------------------------------------------------
@@ -642,8 +696,18 @@ oal_status oal_geometry_create(const oal_geometry_desc* d, int32_t device, oal_g
   std::vector<uint32_t> cmask;
   int64_t n_solid = 0;
   if (d->obstacle) {
+    // only blocks with a solid cell in their 27-block neighbourhood can carry mask bits
+    std::vector<uint8_t> has_solid((size_t)nb, 0);
+    for (int64_t b = 0; b < nb; ++b)
+      for (int c = 0; c < 512 && !has_solid[(size_t)b]; ++c) has_solid[(size_t)b] = d->obstacle[b * 512 + c] != 0;
     std::vector<uint32_t> m(512);
     for (int64_t b = 0; b < nb; ++b) {
+      bool near = false;
+      for (int dir = 0; dir < 27 && !near; ++dir) {
+        const int32_t sb = nbr0[(size_t)b * 27 + dir];
+        near = sb >= 0 && has_solid[(size_t)sb];
+      }
+      if (!near) continue;
       bool any = false;
       for (int cell = 0; cell < 512; ++cell) {
         const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
@@ -725,11 +789,10 @@ oal_status oal_geometry_create(const oal_geometry_desc* d, int32_t device, oal_g
   g->n_fast = (int32_t)fast.size();
   g->n_general = (int32_t)general.size();
 
-  // Box levels: every block of the bx x by x bz box present -> dense padded population layout.
-  // Periodic axes are read from the neighbour table (a first block that has a neighbour across the
-  // low face of an axis wraps on that axis).
-  std::vector<uint2> dentries;
-  std::vector<int32_t> dfast;
+  // Box levels: every block of the bx x by x bz box present -> a dense padded population layout
+  // is available. Periodic axes are read from the neighbour table (a first block that has a
+  // neighbour across the low face of an axis wraps on that axis). The dense ghost-frame entries
+  // and work order are built by the first dense level (build_dense_tables).
   {
     int bxm = 0, bym = 0, bzm = 0;
     bool ok = true;
@@ -752,40 +815,10 @@ oal_status oal_geometry_create(const oal_geometry_desc* d, int32_t device, oal_g
         if (nbr0[(size_t)first * 27 + nbr_dir(-1, 0, 0)] >= 0) g->pmask |= CF_PERIODIC_X;
         if (nbr0[(size_t)first * 27 + nbr_dir(0, -1, 0)] >= 0) g->pmask |= CF_PERIODIC_Y;
         if (nbr0[(size_t)first * 27 + nbr_dir(0, 0, -1)] >= 0) g->pmask |= CF_PERIODIC_Z;
-        const int N[3] = {8 * bxm, 8 * bym, 8 * bzm};
-        const bool per[3] = {(g->pmask & CF_PERIODIC_X) != 0, (g->pmask & CF_PERIODIC_Y) != 0, (g->pmask & CF_PERIODIC_Z) != 0};
-        // ghost-frame slots: every (cell, k) whose source leaves the box; a crossing of periodic
-        // axes only is a copy of the wrapped interior cell, any other goes through the face rules
-        for (int64_t b = 0; b < nb; ++b) {
-          const int g0[3] = {(binfo[b].x - 1) * 8, (binfo[b].y - 1) * 8, (binfo[b].z - 1) * 8};
-          const bool edge = g0[0] == 0 || g0[1] == 0 || g0[2] == 0 || g0[0] + 8 == N[0] || g0[1] + 8 == N[1] ||
-                            g0[2] + 8 == N[2];
-          if (!edge) continue;
-          for (int cell = 0; cell < 512; ++cell) {
-            const int c3[3] = {g0[0] + (cell & 7), g0[1] + ((cell >> 3) & 7), g0[2] + (cell >> 6)};
-            for (int k = 0; k < 27; ++k) {
-              const int ck[3] = {q27_cx(k), q27_cy(k), q27_cz(k)};
-              bool out = false, face = false;
-              for (int ax = 0; ax < 3; ++ax) {
-                const int sc = c3[ax] - ck[ax];
-                if (sc < 0 || sc >= N[ax]) { out = true; if (!per[ax]) face = true; }
-              }
-              if (out)
-                dentries.push_back(make_uint2((uint32_t)b, (uint32_t)cell | ((uint32_t)k << 9) | (face ? 0u : (1u << 31))));
-            }
-          }
-        }
-        // uniform blocks ordered x fastest, so CTAs running together write neighbouring rows
-        for (int bz = 1; bz <= bzm; ++bz)
-          for (int by = 1; by <= bym; ++by)
-            for (int bx = 1; bx <= bxm; ++bx) {
-              const int32_t b = at[((size_t)(bx - 1) * bym + (by - 1)) * bzm + (bz - 1)];
-              if (std::find(general.begin(), general.end(), b) == general.end()) dfast.push_back(b);
-            }
+        g->h_box_at = at;
       }
     }
   }
-  g->n_dense_gentries = (int64_t)dentries.size();
 
   g->h_nbrg = nbrg;
   g->h_binfo = binfo;
@@ -839,14 +872,6 @@ oal_status oal_geometry_create(const oal_geometry_desc* d, int32_t device, oal_g
   if (!general.empty()) {
     GTRY(cudaMalloc(&g->d_general, general.size() * sizeof(int32_t)));
     GTRY(cudaMemcpy(g->d_general, general.data(), general.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
-  }
-  if (!dentries.empty()) {
-    GTRY(cudaMalloc(&g->d_dense_gentries, dentries.size() * sizeof(uint2)));
-    GTRY(cudaMemcpy(g->d_dense_gentries, dentries.data(), dentries.size() * sizeof(uint2), cudaMemcpyHostToDevice));
-  }
-  if (!dfast.empty()) {
-    GTRY(cudaMalloc(&g->d_dense_fast, dfast.size() * sizeof(int32_t)));
-    GTRY(cudaMemcpy(g->d_dense_fast, dfast.data(), dfast.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
   }
   GTRY(cudaMalloc(&g->d_force_part, (size_t)nb * 4 * 3 * sizeof(double)));
   GTRY(cudaMalloc(&g->d_force, 3 * sizeof(double)));
@@ -925,6 +950,10 @@ oal_status oal_level_create_ex(const oal_geometry* g, int32_t op, int32_t storag
   // box levels in FP32/FP16/BF16: dense padded grid; otherwise the real blocks followed by the
   // ghost blocks
   L->dense = (flags & OAL_LEVEL_DENSE) && g->box && storage != OAL_STORE_F64;
+  if (L->dense) {
+    oal_status ds = build_dense_tables(const_cast<oal_geometry*>(g));
+    if (ds != OAL_OK) { delete L; return ds; }
+  }
   if (L->dense) {
     L->PX = 8 * g->bdim[0] + 16;
     L->PY = 8 * g->bdim[1] + 2;
@@ -1688,12 +1717,14 @@ oal_status oal_batch_advance(oal_batch* B, int32_t n, void* stream) {
   }
   if (B->n_fast + B->n_general == 0) return OAL_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (!(B->exec && B->graph_n == n && B->graph_parity == B->parity)) {
+  // One graph of two steps (both parities) launched n/2 times, plus one single step when n is odd:
+  // membership changes then cost one small capture instead of an n-step graph.
+  if (!(B->exec && B->graph_parity == B->parity)) {
     batch_release_graph(B);
     const int start = B->parity;
     OAL_CUDA_TRY(cudaStreamBeginCapture(B->cap, cudaStreamCaptureModeThreadLocal));
     oal_status es = OAL_OK;
-    for (int i = 0; i < n && es == OAL_OK; ++i) es = batch_enqueue_step(B, i, B->cap);
+    for (int i = 0; i < 2 && es == OAL_OK; ++i) es = batch_enqueue_step(B, i, B->cap);
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamEndCapture(B->cap, &graph);
     B->parity = start;
@@ -1702,10 +1733,13 @@ oal_status oal_batch_advance(oal_batch* B, int32_t n, void* stream) {
     cudaGraphExec_t exec = nullptr;
     e = cudaGraphInstantiate(&exec, graph, 0);
     if (e != cudaSuccess) { cudaGraphDestroy(graph); return set_error(OAL_E_CUDA, "graph instantiate: %s", cudaGetErrorString(e)); }
-    B->exec = exec; B->graph = graph; B->graph_n = n; B->graph_parity = start;
+    B->exec = exec; B->graph = graph; B->graph_n = 2; B->graph_parity = start;
   }
-  OAL_CUDA_TRY(cudaGraphLaunch(B->exec, st));
-  if (n & 1) B->parity ^= 1;
+  for (int i = 0; i + 1 < n; i += 2) OAL_CUDA_TRY(cudaGraphLaunch(B->exec, st));
+  if (n & 1) {
+    oal_status es = batch_enqueue_step(B, n - 1, st);  // flips the parity; the graph is re-made next time
+    if (es != OAL_OK) return es;
+  }
   for (auto& M : B->mem)
     if (M.active && (M.cp.flags & CF_COLLECT)) M.forces_valid = true;
   return OAL_OK;

@@ -1,0 +1,45 @@
+"""Serving: request generation (CPU) and continuous batching (GPU): every served result equals the
+same request solved alone, while requests join and leave the resident mix."""
+import math
+
+import numpy as np
+import pytest
+
+from openaerolab_alpha_01_b200 import server
+
+
+def test_request_stream_is_seeded_and_in_range():
+    a = server.make_requests(200, rate=20.0, steps=100, seed=3)
+    b = server.make_requests(200, rate=20.0, steps=100, seed=3)
+    assert [(r.arrival, r.n, r.kind, r.re) for r in a] == [(r.arrival, r.n, r.kind, r.re) for r in b]
+    assert all(32 <= r.n <= 192 and r.n % 8 == 0 for r in a)
+    assert all(100 <= r.re <= 5000 for r in a)
+    gaps = np.diff([0.0] + [r.arrival for r in a])
+    assert abs(gaps.mean() - 1 / 20.0) < 0.02          # Poisson rate
+    assert 0.3 < np.mean([r.kind == "channel" for r in a]) < 0.7
+
+
+def test_pool_block_costs():
+    rb, gb = server.block_bytes("f16")
+    assert rb > gb > 27 * 512 * 2
+
+
+@pytest.mark.gpu
+def test_served_results_equal_solving_alone(oal):
+    reqs = server.make_requests(8, rate=200.0, steps=40, n_min=16, n_max=24, seed=11)
+    served, states = server.serve(reqs, budget_bytes=30e6, storage="f32", tick_steps=15, keep_states=True)
+    assert served["completed"] == 8
+    assert all(r.done > r.admitted >= r.arrival for r in reqs)
+    reqs2 = server.make_requests(8, rate=200.0, steps=40, n_min=16, n_max=24, seed=11)
+    seq, alone = server.serve_sequential(reqs2, storage="f32", keep_states=True)
+    for r in reqs:
+        assert np.array_equal(states[r.rid], alone[r.rid]), r.rid
+    # the small budget forced queueing: not everything was admitted at its arrival
+    assert any(r.admitted - r.arrival > 1e-3 for r in reqs)
+
+
+@pytest.mark.gpu
+def test_request_larger_than_the_pool_is_rejected(oal):
+    reqs = server.make_requests(2, rate=200.0, steps=10, n_min=32, n_max=32, seed=2)
+    served, _ = server.serve(reqs, budget_bytes=2e6, storage="f32", tick_steps=5)
+    assert served["rejected"] == 2 and served["completed"] == 0
