@@ -294,6 +294,66 @@ oal_status oal_geometry_blocks(const oal_geometry* g, int64_t out[3]);
 oal_status oal_mass_momentum_noalloc(const void* f, int32_t storage, int64_t f_block_stride, int64_t f_dir_stride,
                                      const uint8_t* obstacle, int32_t n_blocks, double* out, void* stream);
 
+/* ---- D3Q19 octree level (OpenAeroLab src/octree_q19) -----------------------------------------
+ *
+ *   reference                                              replaced by
+ *   -----------------------------------------------------  ------------------------------------
+ *   Numerics (nu per level, sgs, c_wale, c_smagorinsky,    oal_q19_params / oal_q19_default_params
+ *     hrr_sigma, body_force) config.jl:306-335,
+ *     state.jl:235-249
+ *   generate(Tri[], MeshSpec(periodic=(true,true,true),    oal_q19_periodic_box
+ *     levels=1)) generator.jl:270-350 (level 1 of a
+ *     periodic box: octs in Morton order, onbr)
+ *   State(mesh, cfg, T) level buffers f/g, u/v, rho/rhob   oal_q19_level_create / _destroy
+ *     state.jl:40-60,230-255
+ *   initialise!(st, init) / initialise_uniform!            oal_q19_level_initialise
+ *     state.jl:267-330 (host evaluates init; rebuild on the device)
+ *   advance!(st) = step_level! + swap_buffers!             oal_q19_level_advance
+ *     run.jl:6-11, stream.jl:280-380
+ *   total_mass / total_momentum (Float64)                  oal_q19_level_totals
+ *     state.jl:333-356
+ *   collide_rr(f, omega, sigma, pi_fd, F) per cell         oal_q19_collide_cells (test hook)
+ *     collision.jl:58-75, kernel.jl:92-134
+ *
+ * Layouts (Julia column-major, the reference's own): f(8,19,nocts) shifted populations f - w_i,
+ * u(8,3,nocts), rho(8,nocts), du(8,9,nocts) with du[k, 3a+b, o] = d u_b / d x_a over one cell,
+ * onbr(27,nocts) 1-based (0 = none), origin(3,nocts) 0-based level cells. `precision` is
+ * OAL_STORE_F32 or OAL_STORE_F64 (the solver's Float32 / Float64); host arrays have that type.
+ * Levels whose octs miss a neighbour (domain faces, AMR ghosts, bodies) are refused with
+ * OAL_E_UNSUPPORTED. */
+enum { OAL_Q19_SGS_NONE = 0, OAL_Q19_SGS_WALE = 1, OAL_Q19_SGS_SMAGORINSKY = 2, OAL_Q19_SGS_VREMAN = 3 };
+
+typedef struct oal_q19_params {
+  uint32_t abi_version;   /* OAL_ABI_VERSION */
+  int32_t sgs;            /* OAL_Q19_SGS_* */
+  double nu;              /* molecular viscosity, lattice units of the level */
+  double c_wale;          /* WALE constant (0.5) */
+  double c_smagorinsky;   /* Smagorinsky constant (0.1); Vreman uses 2.5 c^2 */
+  double hrr_sigma;       /* 1 = RR; < 1 blends the finite-difference stress (HRR) */
+  double body_force[3];   /* Guo body force, lattice units of the level */
+  double reserved[4];
+} oal_q19_params;
+
+typedef struct oal_q19_level oal_q19_level;
+
+oal_status oal_q19_default_params(oal_q19_params* out);
+oal_status oal_q19_periodic_box(int32_t n0, int32_t n1, int32_t n2, int32_t* origin, int32_t* onbr);
+oal_status oal_q19_level_create(int32_t device, int32_t precision, int32_t nocts, const int32_t* onbr,
+                                oal_q19_level** out);
+oal_status oal_q19_level_destroy(oal_q19_level* level);
+/* host rho, u and (nullable) du: with du the Chapman-Enskog non-equilibrium is rebuilt, else the equilibrium */
+oal_status oal_q19_level_initialise(oal_q19_level* level, const oal_q19_params* p, const void* rho, const void* u,
+                                    const void* du);
+oal_status oal_q19_level_advance(oal_q19_level* level, const oal_q19_params* p, int32_t n_steps, void* stream);
+oal_status oal_q19_level_get_state(oal_q19_level* level, void* f, void* u, void* rho);       /* host, nullable */
+oal_status oal_q19_level_set_state(oal_q19_level* level, const void* f, const void* u, const void* rho);
+oal_status oal_q19_level_device_state(oal_q19_level* level, void** f, void** u, void** rho, int64_t* steps);
+/* out[5] = {mass, px, py, pz, kinetic energy sum 0.5 rho |u|^2}, FP64, fixed reduction order */
+oal_status oal_q19_level_totals(oal_q19_level* level, double* out, void* stream);
+/* device arrays: f(n,19) omega(n) pfd(n,6) F(n,3) -> out(n,19) rho(n) u(n,3) */
+oal_status oal_q19_collide_cells(int32_t precision, int64_t n, const void* f, const void* omega, double sigma,
+                                 const void* pfd, const void* F, void* out, void* rho, void* u, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

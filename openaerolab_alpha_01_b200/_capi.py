@@ -119,6 +119,26 @@ class LevelFields(C.Structure):
     ]
 
 
+OAL_Q19_SGS_NONE = 0
+OAL_Q19_SGS_WALE = 1
+OAL_Q19_SGS_SMAGORINSKY = 2
+OAL_Q19_SGS_VREMAN = 3
+
+
+class Q19Params(C.Structure):
+    """oal_q19_params (include/oal.h): the octree level's numerics."""
+    _fields_ = [
+        ("abi_version", C.c_uint32),
+        ("sgs", C.c_int32),
+        ("nu", C.c_double),
+        ("c_wale", C.c_double),
+        ("c_smagorinsky", C.c_double),
+        ("hrr_sigma", C.c_double),
+        ("body_force", C.c_double * 3),
+        ("reserved", C.c_double * 4),
+    ]
+
+
 class OALError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"oal status {status}: {msg}")
@@ -171,6 +191,19 @@ _SIGNATURES = {
     "oal_geometry_blocks": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
     "oal_mass_momentum_noalloc": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int64, C.c_int64, C.c_void_p, C.c_int32,
                                               C.c_void_p, C.c_void_p]),
+    "oal_q19_default_params": (C.c_int32, [C.POINTER(Q19Params)]),
+    "oal_q19_periodic_box": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p]),
+    "oal_q19_level_create": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "oal_q19_level_destroy": (C.c_int32, [C.c_void_p]),
+    "oal_q19_level_initialise": (C.c_int32, [C.c_void_p, C.POINTER(Q19Params), C.c_void_p, C.c_void_p, C.c_void_p]),
+    "oal_q19_level_advance": (C.c_int32, [C.c_void_p, C.POINTER(Q19Params), C.c_int32, C.c_void_p]),
+    "oal_q19_level_get_state": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "oal_q19_level_set_state": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "oal_q19_level_device_state": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                               C.POINTER(C.c_void_p), C.POINTER(C.c_int64)]),
+    "oal_q19_level_totals": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double), C.c_void_p]),
+    "oal_q19_collide_cells": (C.c_int32, [C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 OAL_NOALLOC_MAX_BLOCKS = 65536

@@ -1,0 +1,811 @@
+// q19.cu — the D3Q19 octree level step: recursive-regularised (RR/HRR) collision in closed form,
+// pull streaming over 2x2x2 octs in Morton order, subgrid viscosity from the previous step's
+// velocity, Guo body force and the positivity safeguard; FP32 or FP64.
+//
+// Reference (OpenAeroLab src/octree_q19, Julia, CPU):
+//   velocity set and weights ........ src/octree_q19/src/lattice.jl:8-31
+//   moments / Pi_neq / populations .. src/octree_q19/src/kernel.jl:26-91
+//   collide_q19, below_floor ........ src/octree_q19/src/kernel.jl:92-134, :93-102
+//   positivity safeguard ............ src/octree_q19/src/collision.jl:18-75
+//   WALE / Smagorinsky / Vreman ..... src/octree_q19/src/collision.jl:77-127
+//   level step (plain fluid slots) .. src/octree_q19/src/stream.jl:280-370, gradient :13-30
+//   pull tables, neighbour slots .... src/octree_q19/src/octree.jl:139-159
+//   rebuild (initial state) ......... src/octree_q19/src/coupling.jl:26-30, state.jl:267-305
+//
+// Data layout (the reference's own, so state moves in and out by plain copies):
+//   f  (8, 19, nocts)  slot k of oct o, direction i at k + 8 i + 152 o (shifted populations f - w_i)
+//   u  (8, 3, nocts)   k + 8 a + 24 o;   rho (8, nocts)  k + 8 o
+//   onbr (27, nocts)   1-based neighbour oct of offset (dx,dy,dz) at (dx+1)+3(dy+1)+9(dz+1)
+// One thread per slot, one CTA per 32 octs; the CTA stages its octs' neighbour rows in shared
+// memory. The arithmetic is IEEE (no contraction: the library builds with -fmad=false; division
+// and square root are the correctly rounded ones) in the reference's operation order, so a level
+// steps to the same bits as the reference's scalar form.
+#include <cuda_runtime.h>
+#include <cstdarg>
+#include <cstdio>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+#include "../../include/oal.h"
+
+oal_status oal_internal_set_error(oal_status s, const char* msg);
+
+namespace {
+
+constexpr int Q = 19;
+constexpr int kOctsPerCta = 32;
+constexpr int kThreads = 8 * kOctsPerCta;
+
+// lattice.jl:8-11 (0-based)
+__host__ __device__ constexpr int cx(int i) {
+  return (i == 1 || i == 7 || i == 9 || i == 11 || i == 13) ? 1 : (i == 2 || i == 8 || i == 10 || i == 12 || i == 14) ? -1 : 0;
+}
+__host__ __device__ constexpr int cy(int i) {
+  return (i == 3 || i == 7 || i == 10 || i == 15 || i == 17) ? 1 : (i == 4 || i == 8 || i == 9 || i == 16 || i == 18) ? -1 : 0;
+}
+__host__ __device__ constexpr int cz(int i) {
+  return (i == 5 || i == 11 || i == 14 || i == 15 || i == 18) ? 1 : (i == 6 || i == 12 || i == 13 || i == 16 || i == 17) ? -1 : 0;
+}
+__host__ __device__ constexpr double wt(int i) { return i == 0 ? 1.0 / 3 : i < 7 ? 1.0 / 18 : 1.0 / 36; }
+
+// ---- the cell arithmetic ---------------------------------------------------------------------
+
+template <class T>
+__device__ __forceinline__ void moments(const T* f, T& drho, T& mx, T& my, T& mz, T* P) {
+  const T sx = f[1] + f[2], dx = f[1] - f[2];
+  const T sy = f[3] + f[4], dy = f[3] - f[4];
+  const T sz = f[5] + f[6], dz = f[5] - f[6];
+  const T sxy = f[7] + f[8], dxy = f[7] - f[8];
+  const T sxY = f[9] + f[10], dxY = f[9] - f[10];
+  const T sxz = f[11] + f[12], dxz = f[11] - f[12];
+  const T sxZ = f[13] + f[14], dxZ = f[13] - f[14];
+  const T syz = f[15] + f[16], dyz = f[15] - f[16];
+  const T syZ = f[17] + f[18], dyZ = f[17] - f[18];
+  const T exy = sxy + sxY, exz = sxz + sxZ, eyz = syz + syZ;
+  drho = (f[0] + ((sx + sy) + sz)) + ((exy + exz) + eyz);
+  mx = dx + ((dxy + dxY) + (dxz + dxZ));
+  my = dy + ((dxy - dxY) + (dyz + dyZ));
+  mz = dz + ((dxz - dxZ) + (dyz - dyZ));
+  P[0] = sx + (exy + exz);
+  P[1] = sy + (exy + eyz);
+  P[2] = sz + (exz + eyz);
+  P[3] = sxy - sxY;
+  P[4] = sxz - sxZ;
+  P[5] = syz - syZ;
+}
+
+// populations of (1 + drho, u) with second-order non-equilibrium a2 scaled by `keep`
+template <class T>
+__device__ __forceinline__ void populations(T drho, T rho, T ux, T uy, T uz, const T* a2, T keep, T* out) {
+  const T pxx = a2[0], pyy = a2[1], pzz = a2[2], pxy = a2[3], pxz = a2[4], pyz = a2[5];
+  const T A = drho - T(1.5) * rho * (ux * ux + uy * uy + uz * uz);
+  const T k2 = T(4.5) * keep, k3 = T(13.5) * keep;
+  const T r3 = T(3) * rho, r45 = T(4.5) * rho;
+  const T t = (pxx + pyy + pzz) * T(1.0 / 3.0);
+  const T two = T(2), t3 = T(1.0 / 3.0), t23 = T(2.0 / 3.0);
+  const T axxy = two * ux * pxy + uy * pxx, axxz = two * ux * pxz + uz * pxx;
+  const T ayyx = two * uy * pxy + ux * pyy, ayyz = two * uy * pyz + uz * pyy;
+  const T azzx = two * uz * pxz + ux * pzz, azzy = two * uz * pyz + uy * pzz;
+  const T w1 = T(1.0 / 18.0), w2 = T(1.0 / 36.0);
+  auto pair = [&](T w, T cu, T h2, T h3, T& a, T& b) {
+    const T e = A + r45 * cu * cu + k2 * h2;
+    const T o = r3 * cu + k3 * h3;
+    a = w * (e + o);
+    b = w * (e - o);
+  };
+  out[0] = T(1.0 / 3.0) * (A - k2 * t);
+  pair(w1, ux, pxx - t, -(ayyx + azzx) * t3, out[1], out[2]);
+  pair(w1, uy, pyy - t, -(axxy + azzy) * t3, out[3], out[4]);
+  pair(w1, uz, pzz - t, -(axxz + ayyz) * t3, out[5], out[6]);
+  const T hxy = pxx + pyy - t, hxz = pxx + pzz - t, hyz = pyy + pzz - t;
+  pair(w2, ux + uy, hxy + two * pxy, t23 * (axxy + ayyx) - t3 * (azzx + azzy), out[7], out[8]);
+  pair(w2, ux - uy, hxy - two * pxy, t23 * (ayyx - axxy) - t3 * (azzx - azzy), out[9], out[10]);
+  pair(w2, ux + uz, hxz + two * pxz, t23 * (axxz + azzx) - t3 * (ayyx + ayyz), out[11], out[12]);
+  pair(w2, ux - uz, hxz - two * pxz, t23 * (azzx - axxz) - t3 * (ayyx - ayyz), out[13], out[14]);
+  pair(w2, uy + uz, hyz + two * pyz, t23 * (ayyz + azzy) - t3 * (axxy + axxz), out[15], out[16]);
+  pair(w2, uy - uz, hyz - two * pyz, t23 * (azzy - ayyz) - t3 * (axxy - axxz), out[17], out[18]);
+}
+
+template <class T>
+__device__ __forceinline__ bool below_floor(const T* out) {
+  const T l0 = T(-(1 - 1e-6) / 3), l1 = T(-(1 - 1e-6) / 18), l2 = T(-(1 - 1e-6) / 36);
+  bool bad = out[0] < l0;
+#pragma unroll
+  for (int i = 1; i < 7; ++i) bad = bad | (out[i] < l1);
+#pragma unroll
+  for (int i = 7; i < Q; ++i) bad = bad | (out[i] < l2);
+  return bad;
+}
+
+template <class T>
+__device__ __forceinline__ T feq_shifted(int i, T rho, T ux, T uy, T uz, T usq) {
+  const T cu = T(cx(i)) * ux + T(cy(i)) * uy + T(cz(i)) * uz;
+  return T(wt(i)) * rho * (T(1) + T(3) * cu + T(4.5) * cu * cu - T(1.5) * usq) - T(wt(i));
+}
+
+// blend toward `eq` until every population clears 1e-6 of its weight (collision.jl:23-40)
+template <class T>
+__device__ __noinline__ void positive_shifted(T* out, const T* eq) {
+  T alpha = T(1);
+  for (int i = 0; i < Q; ++i) {
+    const T w = T(wt(i)), fl = T(1e-6) * w;
+    const T actual = out[i] + w;
+    if (actual < fl) {
+      const T equilibrium = eq[i] + w;
+      if (!(isfinite(equilibrium) && equilibrium > fl)) return;
+      const T candidate = (equilibrium - fl) / (equilibrium - actual);
+      alpha = candidate < alpha ? candidate : alpha;
+    }
+  }
+  if (alpha < T(1)) {
+    const T a99 = T(0.99) * alpha;
+    const T safe_alpha = a99 > T(0) ? a99 : T(0);
+    for (int i = 0; i < Q; ++i) out[i] = eq[i] + safe_alpha * (out[i] - eq[i]);
+  }
+}
+
+// the safeguard of a forced collision: equilibrium of the post-force moments (collision.jl:45-56)
+template <class T>
+__device__ __noinline__ void limit_forced(T* out) {
+  bool needs = false;
+  for (int i = 0; i < Q; ++i) {
+    const T w = T(wt(i));
+    needs = needs | (out[i] + w < T(1e-6) * w);
+  }
+  if (!needs) return;
+  T rho = T(1), mx = T(0), my = T(0), mz = T(0);
+  for (int i = 0; i < Q; ++i) {
+    rho += out[i];
+    mx += T(cx(i)) * out[i];
+    my += T(cy(i)) * out[i];
+    mz += T(cz(i)) * out[i];
+  }
+  const T inv = T(1) / rho;
+  const T ux = mx * inv, uy = my * inv, uz = mz * inv;
+  const T usq = ux * ux + uy * uy + uz * uz;
+  T eq[Q];
+  for (int i = 0; i < Q; ++i) eq[i] = feq_shifted<T>(i, rho, ux, uy, uz, usq);
+  positive_shifted<T>(out, eq);
+}
+
+template <class T>
+__device__ __noinline__ void limit_unforced(T* out, T drho, T rho, T ux, T uy, T uz) {
+  const T z[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+  T eq[Q];
+  populations<T>(drho, rho, ux, uy, uz, z, T(0), eq);
+  positive_shifted<T>(out, eq);
+}
+
+// collide_q19 + limit_positive: `out` from the arriving `f`; returns rho, u
+template <class T>
+__device__ __forceinline__ void collide(const T* f, T omega, T sigma, const T* pfd, const T F0, const T F1, const T F2,
+                                        bool forced, T* out, T& rho, T& ux, T& uy, T& uz) {
+  T drho, mx, my, mz, P[6];
+  moments<T>(f, drho, mx, my, mz, P);
+  rho = drho + T(1);
+  const T inv = T(1) / rho;
+  const T hF = forced ? T(0.5) : T(0);
+  ux = (mx + hF * F0) * inv;
+  uy = (my + hF * F1) * inv;
+  uz = (mz + hF * F2) * inv;
+  T p[6];
+  {
+    const T d3 = drho * T(1.0 / 3.0);
+    const T rx = rho * ux, ry = rho * uy, rz = rho * uz;
+    p[0] = P[0] - d3 - rx * ux;
+    p[1] = P[1] - d3 - ry * uy;
+    p[2] = P[2] - d3 - rz * uz;
+    p[3] = P[3] - rx * uy;
+    p[4] = P[4] - rx * uz;
+    p[5] = P[5] - ry * uz;
+  }
+  if (sigma != T(1)) {
+    const T s1 = T(1) - sigma;
+#pragma unroll
+    for (int n = 0; n < 6; ++n) p[n] = sigma * p[n] + s1 * pfd[n];
+  }
+  populations<T>(drho, rho, ux, uy, uz, p, T(1) - omega, out);
+  if (forced) {
+    const T pre = T(1) - T(0.5) * omega;
+    const T uF = ux * F0 + uy * F1 + uz * F2;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+      const T ci = T(cx(i)), cj = T(cy(i)), ck = T(cz(i));
+      const T cu = ci * ux + cj * uy + ck * uz, cF = ci * F0 + cj * F1 + ck * F2;
+      out[i] = out[i] + T(wt(i)) * (T(1.5) * cF + pre * (T(9) * cu * cF - T(3) * uF));
+    }
+  }
+  if (below_floor<T>(out)) {
+    if (forced) limit_forced<T>(out);
+    else limit_unforced<T>(out, drho, rho, ux, uy, uz);
+  }
+}
+
+template <class T>
+__device__ __forceinline__ T nu_wale(const T* g, T cw) {
+  const T g11 = g[0], g12 = g[1], g13 = g[2], g21 = g[3], g22 = g[4], g23 = g[5], g31 = g[6], g32 = g[7], g33 = g[8];
+  const T s11 = g11, s22 = g22, s33 = g33;
+  const T s12 = T(0.5) * (g12 + g21), s13 = T(0.5) * (g13 + g31), s23 = T(0.5) * (g23 + g32);
+  const T q11 = g11 * g11 + g12 * g21 + g13 * g31, q12 = g11 * g12 + g12 * g22 + g13 * g32, q13 = g11 * g13 + g12 * g23 + g13 * g33;
+  const T q21 = g21 * g11 + g22 * g21 + g23 * g31, q22 = g21 * g12 + g22 * g22 + g23 * g32, q23 = g21 * g13 + g22 * g23 + g23 * g33;
+  const T q31 = g31 * g11 + g32 * g21 + g33 * g31, q32 = g31 * g12 + g32 * g22 + g33 * g32, q33 = g31 * g13 + g32 * g23 + g33 * g33;
+  const T tr = (q11 + q22 + q33) / T(3);
+  const T d11 = q11 - tr, d22 = q22 - tr, d33 = q33 - tr;
+  const T d12 = T(0.5) * (q12 + q21), d13 = T(0.5) * (q13 + q31), d23 = T(0.5) * (q23 + q32);
+  const T ss = s11 * s11 + s22 * s22 + s33 * s33 + T(2) * (s12 * s12 + s13 * s13 + s23 * s23);
+  const T dd = d11 * d11 + d22 * d22 + d33 * d33 + T(2) * (d12 * d12 + d13 * d13 + d23 * d23);
+  const T den = ss * ss * sqrt(ss) + dd * sqrt(sqrt(dd)) + T(1e-20);
+  return cw * cw * dd * sqrt(dd) / den;
+}
+template <class T>
+__device__ __forceinline__ T nu_smagorinsky(const T* g, T cs) {
+  const T s12 = T(0.5) * (g[1] + g[3]), s13 = T(0.5) * (g[2] + g[6]), s23 = T(0.5) * (g[5] + g[7]);
+  const T ss = g[0] * g[0] + g[4] * g[4] + g[8] * g[8] + T(2) * (s12 * s12 + s13 * s13 + s23 * s23);
+  return cs * cs * sqrt(T(2) * ss);
+}
+template <class T>
+__device__ __forceinline__ T nu_vreman(const T* g, T c) {
+  const T g11 = g[0], g12 = g[1], g13 = g[2], g21 = g[3], g22 = g[4], g23 = g[5], g31 = g[6], g32 = g[7], g33 = g[8];
+  const T b11 = g11 * g11 + g21 * g21 + g31 * g31, b22 = g12 * g12 + g22 * g22 + g32 * g32, b33 = g13 * g13 + g23 * g23 + g33 * g33;
+  const T b12 = g11 * g12 + g21 * g22 + g31 * g32, b13 = g11 * g13 + g21 * g23 + g31 * g33, b23 = g12 * g13 + g22 * g23 + g32 * g33;
+  const T bb = b11 * b22 - b12 * b12 + b11 * b33 - b13 * b13 + b22 * b33 - b23 * b23;
+  const T aa = b11 + b22 + b33;
+  const bool off = (aa <= T(1e-20)) | (bb <= T(0));
+  return off ? T(0) : c * sqrt(bb / aa);
+}
+
+__device__ __forceinline__ int nbr_slot_index(int dx, int dy, int dz) { return (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1); }
+
+// ---- kernels -----------------------------------------------------------------------------------
+
+template <class T>
+struct LevelArgs {
+  const T* fin;
+  T* fout;
+  const T* uin;
+  T* uout;
+  const T* rhoin;
+  T* rhoout;
+  const int32_t* onbr;  // (27, nocts) 1-based
+  int32_t nocts;
+  T nu, omega0, cw, cs, cv, sigma;
+  T F0, F1, F2;
+};
+
+// SGS: 0 none, 1 WALE, 2 Smagorinsky, 3 Vreman; GRAD: the velocity gradient is needed (SGS or HRR)
+template <class T, int SGS, bool GRAD, bool FORCED>
+__global__ void __launch_bounds__(kThreads) k_q19_step(const LevelArgs<T> a) {
+  __shared__ int32_t s_nb[kOctsPerCta * 27];
+  const int64_t o0 = (int64_t)blockIdx.x * kOctsPerCta;
+  const int64_t left = (int64_t)a.nocts - o0;
+  const int n_here = left < kOctsPerCta ? (int)left : kOctsPerCta;
+  for (int t = threadIdx.x; t < n_here * 27; t += kThreads) s_nb[t] = a.onbr[o0 * 27 + t] - 1;
+  __syncthreads();
+  const int lo = threadIdx.x >> 3, k = threadIdx.x & 7;
+  if (lo >= n_here) return;
+  const int64_t o = o0 + lo;
+  const int32_t* nb = s_nb + 27 * lo;
+  const int x = k & 1, y = (k >> 1) & 1, z = (k >> 2) & 1;
+
+  // pull: slot k takes direction i from slot (x,y,z) - c_i, in this oct or a neighbour (octree.jl:139-150)
+  T f[Q];
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    const int px = x - cx(i), py = y - cy(i), pz = z - cz(i);
+    const int ox = px < 0 ? -1 : (px > 1 ? 1 : 0), oy = py < 0 ? -1 : (py > 1 ? 1 : 0), oz = pz < 0 ? -1 : (pz > 1 ? 1 : 0);
+    const int src = nb[nbr_slot_index(ox, oy, oz)];
+    const int child = (px - 2 * ox) + 2 * (py - 2 * oy) + 4 * (pz - 2 * oz);
+    f[i] = __ldg(a.fin + (int64_t)src * (8 * Q) + 8 * i + child);
+  }
+
+  T omega = a.omega0;
+  T pfd[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+  if (GRAD) {
+    // central differences of the previous step's velocity over the 6 face neighbours (stream.jl:13-30)
+    T g[9];
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+      T vp[3], vm[3];
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        const int d = s == 0 ? 1 : -1;
+        const int nx = x + (ax == 0 ? d : 0), ny = y + (ax == 1 ? d : 0), nz = z + (ax == 2 ? d : 0);
+        const int ox = nx < 0 ? -1 : (nx > 1 ? 1 : 0), oy = ny < 0 ? -1 : (ny > 1 ? 1 : 0), oz = nz < 0 ? -1 : (nz > 1 ? 1 : 0);
+        const int no = nb[nbr_slot_index(ox, oy, oz)];
+        const int nk = (nx - 2 * ox) + 2 * (ny - 2 * oy) + 4 * (nz - 2 * oz);
+        T* v = s == 0 ? vp : vm;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) v[c] = __ldg(a.uin + (int64_t)no * 24 + 8 * c + nk);
+      }
+      const T h = T(0.5);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) g[3 * ax + c] = h * (vp[c] - vm[c]);
+    }
+    T nut = T(0);
+    if (SGS == 1) nut = nu_wale<T>(g, a.cw);
+    if (SGS == 2) nut = nu_smagorinsky<T>(g, a.cs);
+    if (SGS == 3) nut = nu_vreman<T>(g, a.cv);
+    omega = T(1) / (T(3) * (a.nu + nut) + T(0.5));
+    if (a.sigma != T(1)) {
+      const T rho_prev = a.rhoin[o * 8 + k];
+      const T tau = T(1) / omega;
+      const T c = -rho_prev * tau / T(3);
+      pfd[0] = c * T(2) * g[0];
+      pfd[1] = c * T(2) * g[4];
+      pfd[2] = c * T(2) * g[8];
+      pfd[3] = c * (g[1] + g[3]);
+      pfd[4] = c * (g[2] + g[6]);
+      pfd[5] = c * (g[5] + g[7]);
+    }
+  }
+  T out[Q], rho, ux, uy, uz;
+  collide<T>(f, omega, a.sigma, pfd, a.F0, a.F1, a.F2, FORCED, out, rho, ux, uy, uz);
+  T* fo = a.fout + o * (8 * Q) + k;
+#pragma unroll
+  for (int i = 0; i < Q; ++i) fo[8 * i] = out[i];
+  T* uo = a.uout + o * 24 + k;
+  uo[0] = ux;
+  uo[8] = uy;
+  uo[16] = uz;
+  a.rhoout[o * 8 + k] = rho;
+}
+
+// initial state from (rho, u[, du]) per slot: `rebuild` with the Chapman-Enskog non-equilibrium,
+// or the equilibrium when du is null (state.jl:267-305, coupling.jl:26-30)
+template <class T>
+__global__ void k_q19_initialise(int64_t nslots, const T* __restrict__ rho_in, const T* __restrict__ u_in,
+                                 const T* __restrict__ du, T nu, T* __restrict__ fa, T* __restrict__ fb,
+                                 T* __restrict__ ua, T* __restrict__ ub, T* __restrict__ ra, T* __restrict__ rb) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nslots) return;
+  const int64_t o = s >> 3;
+  const int k = (int)(s & 7);
+  const T rho = rho_in[s];
+  const T ux = u_in[o * 24 + k], uy = u_in[o * 24 + 8 + k], uz = u_in[o * 24 + 16 + k];
+  T out[Q];
+  const T drho = rho - T(1);
+  const T omega = T(1) / (T(3) * nu + T(0.5));
+  if (du) {
+    T d[9];
+#pragma unroll
+    for (int n = 0; n < 9; ++n) d[n] = du[o * 72 + 8 * n + k];
+    const T tau = T(1) / omega;
+    const T c = -rho * tau / T(3);
+    const T pn[6] = {c * T(2) * d[0], c * T(2) * d[4], c * T(2) * d[8], c * (d[1] + d[3]), c * (d[2] + d[6]), c * (d[5] + d[7])};
+    populations<T>(drho, rho, ux, uy, uz, pn, T(1) - omega, out);
+    if (below_floor<T>(out)) limit_unforced<T>(out, drho, rho, ux, uy, uz);
+  } else {
+    const T zz[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+    populations<T>(drho, rho, ux, uy, uz, zz, T(0), out);
+  }
+#pragma unroll
+  for (int i = 0; i < Q; ++i) {
+    fa[o * (8 * Q) + 8 * i + k] = out[i];
+    fb[o * (8 * Q) + 8 * i + k] = out[i];
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const T v = c == 0 ? ux : c == 1 ? uy : uz;
+    ua[o * 24 + 8 * c + k] = v;
+    ub[o * 24 + 8 * c + k] = v;
+  }
+  ra[s] = rho;
+  rb[s] = rho;
+}
+
+// the collision alone over n cells in (n, 19) rows (a test hook of the known-answer checks)
+template <class T>
+__global__ void k_q19_collide_cells(int64_t n, const T* __restrict__ f, const T* __restrict__ omega, T sigma,
+                                    const T* __restrict__ pfd, const T* __restrict__ F, T* __restrict__ out,
+                                    T* __restrict__ rho, T* __restrict__ u) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  T fl[Q], o[Q], pf[6];
+  for (int i = 0; i < Q; ++i) fl[i] = f[c * Q + i];
+  for (int i = 0; i < 6; ++i) pf[i] = pfd[c * 6 + i];
+  const T F0 = F[3 * c], F1 = F[3 * c + 1], F2 = F[3 * c + 2];
+  const bool forced = !(F0 == T(0) && F1 == T(0) && F2 == T(0));
+  T r, ux, uy, uz;
+  collide<T>(fl, omega[c], sigma, pf, F0, F1, F2, forced, o, r, ux, uy, uz);
+  for (int i = 0; i < Q; ++i) out[c * Q + i] = o[i];
+  rho[c] = r;
+  u[3 * c] = ux;
+  u[3 * c + 1] = uy;
+  u[3 * c + 2] = uz;
+}
+
+// FP64 totals per CTA: mass, momentum, kinetic energy over the slots (state.jl:333-356)
+template <class T>
+__global__ void k_q19_totals(int64_t nslots, const T* __restrict__ rho, const T* __restrict__ u, double* __restrict__ part) {
+  __shared__ double s[5][8];
+  double a[5] = {0, 0, 0, 0, 0};
+  for (int64_t sl = (int64_t)blockIdx.x * 256 + threadIdx.x; sl < nslots; sl += (int64_t)gridDim.x * 256) {
+    const int64_t o = sl >> 3;
+    const int k = (int)(sl & 7);
+    const double r = (double)rho[sl];
+    const double ux = (double)u[o * 24 + k], uy = (double)u[o * 24 + 8 + k], uz = (double)u[o * 24 + 16 + k];
+    a[0] += r;
+    a[1] += r * ux;
+    a[2] += r * uy;
+    a[3] += r * uz;
+    a[4] += 0.5 * r * (ux * ux + uy * uy + uz * uz);
+  }
+#pragma unroll
+  for (int c = 0; c < 5; ++c)
+    for (int off = 16; off > 0; off >>= 1) a[c] += __shfl_down_sync(0xffffffffu, a[c], off);
+  if ((threadIdx.x & 31) == 0)
+    for (int c = 0; c < 5; ++c) s[c][threadIdx.x >> 5] = a[c];
+  __syncthreads();
+  if (threadIdx.x < 5) {
+    double v = 0;
+    for (int w = 0; w < 8; ++w) v += s[threadIdx.x][w];
+    part[5 * (int64_t)blockIdx.x + threadIdx.x] = v;
+  }
+}
+
+__global__ void k_q19_totals_final(const double* __restrict__ part, int n, double* __restrict__ out) {
+  if (threadIdx.x < 5) {
+    double v = 0;
+    for (int b = 0; b < n; ++b) v += part[5 * b + threadIdx.x];
+    out[threadIdx.x] = v;
+  }
+}
+
+constexpr int kTotalsCtas = 592;  // 4 per SM on 148 SMs
+
+oal_status fail(oal_status s, const char* fmt, ...) {
+  char buf[400];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  return oal_internal_set_error(s, buf);
+}
+
+#define Q19_TRY(expr)                                                                                 \
+  do {                                                                                                \
+    cudaError_t _e = (expr);                                                                          \
+    if (_e != cudaSuccess) {                                                                          \
+      cudaGetLastError();                                                                             \
+      return fail(_e == cudaErrorMemoryAllocation ? OAL_E_OUT_OF_MEMORY : OAL_E_CUDA, "%s: %s", #expr, \
+                  cudaGetErrorString(_e));                                                            \
+    }                                                                                                 \
+  } while (0)
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+// Morton key of an oct origin in oct units (octree.jl:35-48)
+uint64_t spread3(uint64_t v) {
+  v &= 0x1fffff;
+  v = (v | (v << 32)) & 0x1f00000000ffffULL;
+  v = (v | (v << 16)) & 0x1f0000ff0000ffULL;
+  v = (v | (v << 8)) & 0x100f00f00f00f00fULL;
+  v = (v | (v << 4)) & 0x10c30c30c30c30c3ULL;
+  v = (v | (v << 2)) & 0x1249249249249249ULL;
+  return v;
+}
+uint64_t morton3(uint64_t ix, uint64_t iy, uint64_t iz) { return spread3(ix) | (spread3(iy) << 1) | (spread3(iz) << 2); }
+
+}  // namespace
+
+struct oal_q19_level {
+  int device = 0;
+  int precision = OAL_STORE_F32;
+  int32_t nocts = 0;
+  size_t es = 4;
+  int32_t* onbr = nullptr;
+  void* f[2] = {nullptr, nullptr};
+  void* u[2] = {nullptr, nullptr};
+  void* rho[2] = {nullptr, nullptr};
+  double* part = nullptr;  // kTotalsCtas * 5 + 5
+  int cur = 0;             // buffer holding the current state
+  int64_t steps = 0;
+};
+
+namespace {
+
+oal_status check_params(const oal_q19_params* p) {
+  if (!p) return fail(OAL_E_INVALID_ARG, "null oal_q19_params");
+  if (p->abi_version != OAL_ABI_VERSION)
+    return fail(OAL_E_ABI_MISMATCH, "oal_q19_params.abi_version %u != %d", p->abi_version, OAL_ABI_VERSION);
+  if (!(p->nu > 0) || !std::isfinite(p->nu)) return fail(OAL_E_INVALID_ARG, "nu must be positive (got %g)", p->nu);
+  if (p->sgs < OAL_Q19_SGS_NONE || p->sgs > OAL_Q19_SGS_VREMAN) return fail(OAL_E_INVALID_ARG, "sgs model %d", p->sgs);
+  if (!(p->hrr_sigma >= 0 && p->hrr_sigma <= 1)) return fail(OAL_E_INVALID_ARG, "hrr_sigma must lie in [0, 1]");
+  for (int a = 0; a < 3; ++a)
+    if (!std::isfinite(p->body_force[a])) return fail(OAL_E_INVALID_ARG, "body_force must be finite");
+  return OAL_OK;
+}
+
+template <class T>
+LevelArgs<T> level_args(oal_q19_level* L, const oal_q19_params* p) {
+  LevelArgs<T> a;
+  const int src = L->cur, dst = 1 - L->cur;
+  a.fin = static_cast<const T*>(L->f[src]);
+  a.fout = static_cast<T*>(L->f[dst]);
+  a.uin = static_cast<const T*>(L->u[src]);
+  a.uout = static_cast<T*>(L->u[dst]);
+  a.rhoin = static_cast<const T*>(L->rho[src]);
+  a.rhoout = static_cast<T*>(L->rho[dst]);
+  a.onbr = L->onbr;
+  a.nocts = L->nocts;
+  a.nu = T(p->nu);
+  a.omega0 = T(1) / (T(3) * a.nu + T(0.5));
+  a.cw = T(p->c_wale);
+  a.cs = T(p->c_smagorinsky);
+  a.cv = T(2.5 * p->c_smagorinsky * p->c_smagorinsky);
+  a.sigma = T(p->hrr_sigma);
+  a.F0 = T(p->body_force[0]);
+  a.F1 = T(p->body_force[1]);
+  a.F2 = T(p->body_force[2]);
+  return a;
+}
+
+template <class T, int SGS, bool GRAD>
+cudaError_t launch_step3(const LevelArgs<T>& a, bool forced, cudaStream_t st) {
+  const unsigned grid = (unsigned)((a.nocts + kOctsPerCta - 1) / kOctsPerCta);
+  if (forced) k_q19_step<T, SGS, GRAD, true><<<grid, kThreads, 0, st>>>(a);
+  else k_q19_step<T, SGS, GRAD, false><<<grid, kThreads, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t launch_step(const LevelArgs<T>& a, int sgs, bool forced, cudaStream_t st) {
+  const bool hrr = a.sigma != T(1);
+  switch (sgs) {
+    case OAL_Q19_SGS_WALE: return launch_step3<T, 1, true>(a, forced, st);
+    case OAL_Q19_SGS_SMAGORINSKY: return launch_step3<T, 2, true>(a, forced, st);
+    case OAL_Q19_SGS_VREMAN: return launch_step3<T, 3, true>(a, forced, st);
+    default: return hrr ? launch_step3<T, 0, true>(a, forced, st) : launch_step3<T, 0, false>(a, forced, st);
+  }
+}
+
+template <class T>
+oal_status advance_t(oal_q19_level* L, const oal_q19_params* p, int32_t n, cudaStream_t st) {
+  const bool forced = !(T(p->body_force[0]) == T(0) && T(p->body_force[1]) == T(0) && T(p->body_force[2]) == T(0));
+  for (int32_t s = 0; s < n; ++s) {
+    const LevelArgs<T> a = level_args<T>(L, p);
+    Q19_TRY(launch_step<T>(a, p->sgs, forced, st));
+    L->cur = 1 - L->cur;
+    ++L->steps;
+  }
+  return OAL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+oal_status oal_q19_default_params(oal_q19_params* p) {
+  if (!p) return fail(OAL_E_INVALID_ARG, "null argument");
+  std::memset(p, 0, sizeof *p);
+  p->abi_version = OAL_ABI_VERSION;
+  p->sgs = OAL_Q19_SGS_NONE;
+  p->nu = 0.01;
+  p->c_wale = 0.5;          // config.jl Numerics defaults
+  p->c_smagorinsky = 0.1;
+  p->hrr_sigma = 1.0;
+  return OAL_OK;
+}
+
+oal_status oal_q19_periodic_box(int32_t n0, int32_t n1, int32_t n2, int32_t* origin, int32_t* onbr) {
+  if (n0 < 2 || n1 < 2 || n2 < 2 || (n0 | n1 | n2) & 1)
+    return fail(OAL_E_INVALID_ARG, "a periodic box needs even cell counts >= 2 per axis (got %d %d %d)", n0, n1, n2);
+  if (!origin || !onbr) return fail(OAL_E_INVALID_ARG, "null output");
+  const int m0 = n0 / 2, m1 = n1 / 2, m2 = n2 / 2;
+  if ((int64_t)m0 * m1 * m2 > INT32_MAX / 27) return fail(OAL_E_TOO_LARGE, "too many octs");
+  const int64_t no = (int64_t)m0 * m1 * m2;
+  std::vector<std::pair<uint64_t, int64_t>> keys((size_t)no);
+  for (int i = 0; i < m0; ++i)
+    for (int j = 0; j < m1; ++j)
+      for (int k = 0; k < m2; ++k) {
+        const int64_t lin = ((int64_t)i * m1 + j) * m2 + k;
+        keys[(size_t)lin] = {morton3(i + 1, j + 1, k + 1), lin};
+      }
+  std::sort(keys.begin(), keys.end());
+  std::vector<int32_t> index((size_t)no);
+  for (int64_t o = 0; o < no; ++o) index[(size_t)keys[(size_t)o].second] = (int32_t)o;
+  for (int64_t o = 0; o < no; ++o) {
+    const int64_t lin = keys[(size_t)o].second;
+    const int i = (int)(lin / ((int64_t)m1 * m2)), j = (int)((lin / m2) % m1), k = (int)(lin % m2);
+    origin[3 * o] = 2 * i;
+    origin[3 * o + 1] = 2 * j;
+    origin[3 * o + 2] = 2 * k;
+    for (int dz = -1; dz <= 1; ++dz)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int a = (i + dx + m0) % m0, b = (j + dy + m1) % m1, c = (k + dz + m2) % m2;
+          onbr[27 * o + (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1)] = index[((size_t)a * m1 + b) * m2 + c] + 1;
+        }
+  }
+  return OAL_OK;
+}
+
+oal_status oal_q19_level_create(int32_t device, int32_t precision, int32_t nocts, const int32_t* onbr, oal_q19_level** out) {
+  if (!out || !onbr) return fail(OAL_E_INVALID_ARG, "null argument");
+  *out = nullptr;
+  if (precision != OAL_STORE_F32 && precision != OAL_STORE_F64)
+    return fail(OAL_E_INVALID_ARG, "the octree level stores FP32 or FP64 populations (got storage %d)", precision);
+  if (nocts <= 0 || (int64_t)nocts * 27 > INT32_MAX) return fail(OAL_E_INVALID_ARG, "bad oct count %d", nocts);
+  for (int64_t t = 0; t < (int64_t)nocts * 27; ++t) {
+    if (onbr[t] < 0 || onbr[t] > nocts) return fail(OAL_E_INVALID_ARG, "onbr entry %lld out of range", (long long)t);
+    if (onbr[t] == 0)
+      return fail(OAL_E_UNSUPPORTED,
+                  "oct %lld has no neighbour at offset %d: levels with boundary, ghost or solid slots have no "
+                  "kernel in this build (periodic single levels only)", (long long)(t / 27) + 1, (int)(t % 27));
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(OAL_E_NO_DEVICE, "no CUDA device");
+  }
+  if (device < 0 || device >= ndev) return fail(OAL_E_INVALID_ARG, "device %d of %d", device, ndev);
+  DeviceGuard g(device);
+  oal_q19_level* L = new oal_q19_level();
+  L->device = device;
+  L->precision = precision;
+  L->nocts = nocts;
+  L->es = precision == OAL_STORE_F64 ? 8 : 4;
+  const size_t ns = (size_t)nocts * 8;
+  auto cleanup = [&](oal_status s) {
+    oal_q19_level_destroy(L);
+    return s;
+  };
+  cudaError_t e = cudaMalloc(&L->onbr, sizeof(int32_t) * 27 * (size_t)nocts);
+  for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
+    e = cudaMalloc(&L->f[b], L->es * ns * Q);
+    if (e == cudaSuccess) e = cudaMalloc(&L->u[b], L->es * ns * 3);
+    if (e == cudaSuccess) e = cudaMalloc(&L->rho[b], L->es * ns);
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&L->part, sizeof(double) * (kTotalsCtas * 5 + 5));
+  if (e == cudaSuccess) e = cudaMemcpy(L->onbr, onbr, sizeof(int32_t) * 27 * (size_t)nocts, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return cleanup(fail(e == cudaErrorMemoryAllocation ? OAL_E_OUT_OF_MEMORY : OAL_E_CUDA, "level allocation: %s",
+                        cudaGetErrorString(e)));
+  }
+  *out = L;
+  return OAL_OK;
+}
+
+oal_status oal_q19_level_destroy(oal_q19_level* L) {
+  if (!L) return OAL_OK;
+  {
+    DeviceGuard g(L->device);
+    cudaFree(L->onbr);
+    for (int b = 0; b < 2; ++b) {
+      cudaFree(L->f[b]);
+      cudaFree(L->u[b]);
+      cudaFree(L->rho[b]);
+    }
+    cudaFree(L->part);
+  }
+  delete L;
+  return OAL_OK;
+}
+
+oal_status oal_q19_level_initialise(oal_q19_level* L, const oal_q19_params* p, const void* rho, const void* u, const void* du) {
+  if (!L || !rho || !u) return fail(OAL_E_INVALID_ARG, "null argument");
+  if (oal_status s = check_params(p)) return s;
+  DeviceGuard g(L->device);
+  const size_t ns = (size_t)L->nocts * 8;
+  void *d_rho = nullptr, *d_u = nullptr, *d_du = nullptr;
+  cudaError_t e = cudaMalloc(&d_rho, L->es * ns);
+  if (e == cudaSuccess) e = cudaMalloc(&d_u, L->es * ns * 3);
+  if (e == cudaSuccess && du) e = cudaMalloc(&d_du, L->es * ns * 9);
+  if (e == cudaSuccess) e = cudaMemcpy(d_rho, rho, L->es * ns, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_u, u, L->es * ns * 3, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && du) e = cudaMemcpy(d_du, du, L->es * ns * 9, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    const unsigned grid = (unsigned)((ns + 255) / 256);
+    if (L->precision == OAL_STORE_F64) {
+      k_q19_initialise<double><<<grid, 256>>>((int64_t)ns, (const double*)d_rho, (const double*)d_u, (const double*)d_du,
+                                              p->nu, (double*)L->f[0], (double*)L->f[1], (double*)L->u[0],
+                                              (double*)L->u[1], (double*)L->rho[0], (double*)L->rho[1]);
+    } else {
+      k_q19_initialise<float><<<grid, 256>>>((int64_t)ns, (const float*)d_rho, (const float*)d_u, (const float*)d_du,
+                                             (float)p->nu, (float*)L->f[0], (float*)L->f[1], (float*)L->u[0], (float*)L->u[1],
+                                             (float*)L->rho[0], (float*)L->rho[1]);
+    }
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  }
+  cudaFree(d_rho);
+  cudaFree(d_u);
+  cudaFree(d_du);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(OAL_E_CUDA, "q19 initialise: %s", cudaGetErrorString(e));
+  }
+  L->cur = 0;
+  L->steps = 0;
+  return OAL_OK;
+}
+
+oal_status oal_q19_level_advance(oal_q19_level* L, const oal_q19_params* p, int32_t n_steps, void* stream) {
+  if (!L) return fail(OAL_E_INVALID_ARG, "null level");
+  if (oal_status s = check_params(p)) return s;
+  if (n_steps < 0) return fail(OAL_E_INVALID_ARG, "n_steps < 0");
+  DeviceGuard g(L->device);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  return L->precision == OAL_STORE_F64 ? advance_t<double>(L, p, n_steps, st) : advance_t<float>(L, p, n_steps, st);
+}
+
+oal_status oal_q19_level_get_state(oal_q19_level* L, void* f, void* u, void* rho) {
+  if (!L) return fail(OAL_E_INVALID_ARG, "null level");
+  DeviceGuard g(L->device);
+  const size_t ns = (size_t)L->nocts * 8;
+  Q19_TRY(cudaDeviceSynchronize());
+  if (f) Q19_TRY(cudaMemcpy(f, L->f[L->cur], L->es * ns * Q, cudaMemcpyDeviceToHost));
+  if (u) Q19_TRY(cudaMemcpy(u, L->u[L->cur], L->es * ns * 3, cudaMemcpyDeviceToHost));
+  if (rho) Q19_TRY(cudaMemcpy(rho, L->rho[L->cur], L->es * ns, cudaMemcpyDeviceToHost));
+  return OAL_OK;
+}
+
+oal_status oal_q19_level_set_state(oal_q19_level* L, const void* f, const void* u, const void* rho) {
+  if (!L || !f || !u || !rho) return fail(OAL_E_INVALID_ARG, "null argument");
+  DeviceGuard g(L->device);
+  const size_t ns = (size_t)L->nocts * 8;
+  Q19_TRY(cudaDeviceSynchronize());
+  Q19_TRY(cudaMemcpy(L->f[L->cur], f, L->es * ns * Q, cudaMemcpyHostToDevice));
+  Q19_TRY(cudaMemcpy(L->u[L->cur], u, L->es * ns * 3, cudaMemcpyHostToDevice));
+  Q19_TRY(cudaMemcpy(L->rho[L->cur], rho, L->es * ns, cudaMemcpyHostToDevice));
+  return OAL_OK;
+}
+
+oal_status oal_q19_level_device_state(oal_q19_level* L, void** f, void** u, void** rho, int64_t* steps) {
+  if (!L) return fail(OAL_E_INVALID_ARG, "null level");
+  if (f) *f = L->f[L->cur];
+  if (u) *u = L->u[L->cur];
+  if (rho) *rho = L->rho[L->cur];
+  if (steps) *steps = L->steps;
+  return OAL_OK;
+}
+
+oal_status oal_q19_level_totals(oal_q19_level* L, double* out, void* stream) {
+  if (!L || !out) return fail(OAL_E_INVALID_ARG, "null argument");
+  DeviceGuard g(L->device);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int64_t ns = (int64_t)L->nocts * 8;
+  const int grid = (int)std::min<int64_t>(kTotalsCtas, (ns + 255) / 256);
+  if (L->precision == OAL_STORE_F64)
+    k_q19_totals<double><<<grid, 256, 0, st>>>(ns, (const double*)L->rho[L->cur], (const double*)L->u[L->cur], L->part);
+  else
+    k_q19_totals<float><<<grid, 256, 0, st>>>(ns, (const float*)L->rho[L->cur], (const float*)L->u[L->cur], L->part);
+  k_q19_totals_final<<<1, 32, 0, st>>>(L->part, grid, L->part + 5 * kTotalsCtas);
+  Q19_TRY(cudaGetLastError());
+  Q19_TRY(cudaMemcpyAsync(out, L->part + 5 * kTotalsCtas, 5 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  Q19_TRY(cudaStreamSynchronize(st));
+  return OAL_OK;
+}
+
+oal_status oal_q19_collide_cells(int32_t precision, int64_t n, const void* f, const void* omega, double sigma,
+                                 const void* pfd, const void* F, void* out, void* rho, void* u, void* stream) {
+  if (n < 0 || (n > 0 && (!f || !omega || !pfd || !F || !out || !rho || !u)))
+    return fail(OAL_E_INVALID_ARG, "bad arguments");
+  if (precision != OAL_STORE_F32 && precision != OAL_STORE_F64) return fail(OAL_E_INVALID_ARG, "precision %d", precision);
+  if (n == 0) return OAL_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const unsigned grid = (unsigned)((n + 127) / 128);
+  if (precision == OAL_STORE_F64)
+    k_q19_collide_cells<double><<<grid, 128, 0, st>>>(n, (const double*)f, (const double*)omega, sigma, (const double*)pfd,
+                                                      (const double*)F, (double*)out, (double*)rho, (double*)u);
+  else
+    k_q19_collide_cells<float><<<grid, 128, 0, st>>>(n, (const float*)f, (const float*)omega, (float)sigma, (const float*)pfd,
+                                                     (const float*)F, (float*)out, (float*)rho, (float*)u);
+  Q19_TRY(cudaGetLastError());
+  return OAL_OK;
+}
+
+}  // extern "C"

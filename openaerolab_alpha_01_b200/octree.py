@@ -1,0 +1,240 @@
+"""D3Q19 octree solver on the GPU: a single periodic level behind the reference's OctreeQ19 API.
+
+Mirrors (OpenAeroLab src/octree_q19, Julia):
+    MeshSpec(domain, periodic=(true,)*3, levels=1) + generate(Tri[], spec)   -> PeriodicBox
+        generator.jl:270-350 (octs of level 1 in Morton order, onbr with periodic wrap)
+    test_case_config(spec; nu_lattice, u_lattice, velocity, hrr_sigma, sgs, precision, body_force)
+        config.jl:306-335, lattice scaling config.jl:328-335           -> test_case_config / CaseConfig
+    State(mesh, cfg, T)                                                  -> State
+    initialise!(st, init; nonequilibrium) / initialise_uniform!          -> State.initialise / initialise_uniform
+        state.jl:267-330
+    advance!(st)                                                         -> State.advance
+        run.jl:6-11, stream.jl:280-380
+    total_mass / total_momentum                                          -> State.total_mass / total_momentum
+        state.jl:333-356
+
+The step runs in liboal (include/oal.h, oal_q19_*); `init` is evaluated on the host as in the
+reference. `init(x, y, z)` takes arrays of slot centres (metres) and returns (rho, ux, uy, uz)
+arrays (numpy broadcasting: the reference's per-point function written with numpy functions).
+Levels with domain faces, bodies or refinement are refused by the library (OAL_E_UNSUPPORTED).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _capi as capi
+from ._capi import check, lib
+
+SGS_CODES = {"none": capi.OAL_Q19_SGS_NONE, "wale": capi.OAL_Q19_SGS_WALE,
+             "smagorinsky": capi.OAL_Q19_SGS_SMAGORINSKY, "vreman": capi.OAL_Q19_SGS_VREMAN}
+_PRECISION = {np.dtype(np.float32): capi.OAL_STORE_F32, np.dtype(np.float64): capi.OAL_STORE_F64}
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class PeriodicBox:
+    """Level 1 of a periodic box of n0 x n1 x n2 cells (even counts) with cell size dx."""
+
+    def __init__(self, n0: int, n1: int | None = None, n2: int | None = None, dx: float = 1.0):
+        n1 = n0 if n1 is None else n1
+        n2 = n0 if n2 is None else n2
+        self.n = (int(n0), int(n1), int(n2))
+        self.dx = float(dx)
+        self.nocts = (n0 // 2) * (n1 // 2) * (n2 // 2)
+        self.origin = np.zeros((self.nocts, 3), np.int32)   # reference (3, nocts)
+        self.onbr = np.zeros((self.nocts, 27), np.int32)    # reference (27, nocts), 1-based
+        check(lib().oal_q19_periodic_box(n0, n1, n2, _ptr(self.origin), _ptr(self.onbr)))
+        self.counts = {"fluid_total": n0 * n1 * n2, "octs": self.nocts}
+
+    def slot_cells(self) -> np.ndarray:
+        """(nocts, 3, 8) integer cell of every slot (octree.jl slot_offset: k-1 = x + 2y + 4z)."""
+        k = np.arange(8)
+        off = np.stack([k & 1, (k >> 1) & 1, (k >> 2) & 1])  # (3, 8)
+        return self.origin[:, :, None] + off[None]
+
+    def slot_centres(self) -> np.ndarray:
+        """(nocts, 3, 8) slot centres in metres (octree.jl:113-116)."""
+        return (self.slot_cells() + 0.5) * self.dx
+
+
+@dataclass
+class CaseConfig:
+    nu_lattice: float = 0.01
+    u_lattice: float = 0.08
+    velocity: float = 1.0
+    hrr_sigma: float = 1.0
+    sgs: str = "none"
+    c_wale: float = 0.5
+    c_smagorinsky: float = 0.1
+    body_force: tuple = (0.0, 0.0, 0.0)
+    precision: type = np.float32
+    dx: float = 1.0
+    extra: dict = field(default_factory=dict)
+
+    def level_nu(self) -> float:
+        """Lattice viscosity of the single level (config.jl:309, 328-335 with L = 1)."""
+        nu_phys = self.nu_lattice * self.velocity * self.dx / self.u_lattice
+        vs = self.velocity / self.u_lattice
+        dtf = self.dx / vs
+        return nu_phys * dtf / (self.dx * self.dx)
+
+    def params(self) -> capi.Q19Params:
+        if self.sgs not in SGS_CODES:
+            raise ValueError(f"unknown sgs model {self.sgs!r}")
+        p = capi.Q19Params()
+        check(lib().oal_q19_default_params(C.byref(p)))
+        p.nu = self.level_nu()
+        p.sgs = SGS_CODES[self.sgs]
+        p.c_wale = self.c_wale
+        p.c_smagorinsky = self.c_smagorinsky
+        p.hrr_sigma = self.hrr_sigma
+        for a in range(3):
+            p.body_force[a] = float(self.body_force[a])
+        return p
+
+
+def test_case_config(box: PeriodicBox, nu_lattice: float = 0.01, u_lattice: float = 0.08, velocity: float = 1.0,
+                     hrr_sigma: float = 1.0, sgs: str = "none", precision=np.float32,
+                     body_force=(0.0, 0.0, 0.0)) -> CaseConfig:
+    return CaseConfig(nu_lattice=nu_lattice, u_lattice=u_lattice, velocity=velocity, hrr_sigma=hrr_sigma, sgs=sgs,
+                      body_force=tuple(body_force), precision=precision, dx=box.dx)
+
+
+test_case_config.__test__ = False  # a configuration factory, not a pytest test
+
+
+class State:
+    """The level's populations, velocity and density on the GPU (two buffers, swapped per step)."""
+
+    def __init__(self, mesh: PeriodicBox, cfg: CaseConfig, precision=None, device: int = 0):
+        self.mesh = mesh
+        self.cfg = cfg
+        self.dtype = np.dtype(precision or cfg.precision)
+        if self.dtype not in _PRECISION:
+            raise ValueError("precision must be float32 or float64")
+        self.params = cfg.params()
+        self.step = 0
+        self.mass0 = float("nan")
+        h = C.c_void_p()
+        check(lib().oal_q19_level_create(device, _PRECISION[self.dtype], mesh.nocts, _ptr(mesh.onbr), C.byref(h)))
+        self._h = h
+
+    # -- lifetime
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().oal_q19_level_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- initial state
+    def _upload(self, rho, u, du):
+        rho = np.ascontiguousarray(rho, self.dtype)
+        u = np.ascontiguousarray(u, self.dtype)
+        du = None if du is None else np.ascontiguousarray(du, self.dtype)
+        check(lib().oal_q19_level_initialise(self._h, C.byref(self.params), _ptr(rho), _ptr(u), _ptr(du)))
+        self.step = 0
+        self.mass0 = self.total_mass()
+
+    def initial_fields(self, init, nonequilibrium: bool = True):
+        """(rho (nocts,8), u (nocts,3,8), du (nocts,9,8) or None) of `init` at the slot centres, in the
+        level's precision, as state.jl:267-305 forms them (du over one cell, evaluated in Float64)."""
+        p = self.mesh.slot_centres()
+        x, y, z = p[:, 0], p[:, 1], p[:, 2]
+        rho, ux, uy, uz = (np.broadcast_to(np.asarray(v, np.float64), x.shape) for v in init(x, y, z))
+        u = np.stack([ux, uy, uz], 1)
+        du = None
+        if nonequilibrium:
+            h = self.mesh.dx / 2
+            du = np.zeros((self.mesh.nocts, 9, 8), np.float64)
+            for a in range(3):
+                e = [0.0, 0.0, 0.0]
+                e[a] = h
+                up = init(x + e[0], y + e[1], z + e[2])
+                um = init(x - e[0], y - e[1], z - e[2])
+                for b in range(3):
+                    du[:, 3 * a + b] = np.asarray(up[b + 1], np.float64) - np.asarray(um[b + 1], np.float64)
+            du = du.astype(self.dtype)
+        return rho.astype(self.dtype), u.astype(self.dtype), du
+
+    def initialise(self, init, nonequilibrium: bool = True):
+        self._upload(*self.initial_fields(init, nonequilibrium))
+        return self
+
+    def initialise_uniform(self, rho0: float, ux0: float, uy0: float, uz0: float):
+        no = self.mesh.nocts
+        rho = np.full((no, 8), rho0, self.dtype)
+        u = np.empty((no, 3, 8), self.dtype)
+        u[:, 0], u[:, 1], u[:, 2] = self.dtype.type(ux0), self.dtype.type(uy0), self.dtype.type(uz0)
+        self._upload(rho, u, None)
+        return self
+
+    # -- stepping
+    def advance(self, n: int = 1, stream=None):
+        st = None if stream is None else C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else stream)
+        check(lib().oal_q19_level_advance(self._h, C.byref(self.params), int(n), st))
+        self.step += n
+        return self
+
+    # -- read-out
+    def state(self):
+        no = self.mesh.nocts
+        f = np.empty((no, 19, 8), self.dtype)
+        u = np.empty((no, 3, 8), self.dtype)
+        rho = np.empty((no, 8), self.dtype)
+        check(lib().oal_q19_level_get_state(self._h, _ptr(f), _ptr(u), _ptr(rho)))
+        return f, u, rho
+
+    def set_state(self, f, u, rho):
+        f = np.ascontiguousarray(f, self.dtype)
+        u = np.ascontiguousarray(u, self.dtype)
+        rho = np.ascontiguousarray(rho, self.dtype)
+        check(lib().oal_q19_level_set_state(self._h, _ptr(f), _ptr(u), _ptr(rho)))
+
+    def totals(self) -> np.ndarray:
+        out = (C.c_double * 5)()
+        check(lib().oal_q19_level_totals(self._h, out, None))
+        return np.array(out[:])
+
+    def total_mass(self) -> float:
+        return float(self.totals()[0])
+
+    def total_momentum(self) -> np.ndarray:
+        return self.totals()[1:4]
+
+    def kinetic_energy(self) -> float:
+        return float(self.totals()[4])
+
+    def device_state(self):
+        f, u, rho = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        steps = C.c_int64()
+        check(lib().oal_q19_level_device_state(self._h, C.byref(f), C.byref(u), C.byref(rho), C.byref(steps)))
+        return f.value, u.value, rho.value, steps.value
+
+
+def collide_cells(f, omega, sigma, pfd, F):
+    """The collision alone on the GPU over n cells (torch CUDA tensors: f (n,19), omega (n), pfd (n,6),
+    F (n,3)); returns (out, rho, u). A test hook of the known-answer checks."""
+    import torch
+    dt = f.dtype
+    prec = capi.OAL_STORE_F64 if dt == torch.float64 else capi.OAL_STORE_F32
+    n = f.shape[0]
+    out = torch.empty_like(f)
+    rho = torch.empty(n, dtype=dt, device=f.device)
+    u = torch.empty(n, 3, dtype=dt, device=f.device)
+    args = [t.contiguous() for t in (f, omega, pfd, F)]
+    stream = torch.cuda.current_stream(f.device).cuda_stream
+    check(lib().oal_q19_collide_cells(prec, n, args[0].data_ptr(), args[1].data_ptr(), float(sigma),
+                                      args[2].data_ptr(), args[3].data_ptr(), out.data_ptr(), rho.data_ptr(),
+                                      u.data_ptr(), C.c_void_p(stream)))
+    torch.cuda.current_stream(f.device).synchronize()
+    return out, rho, u

@@ -1,8 +1,9 @@
 """CPU ORACLE — test infrastructure only.
 
-A C++ restatement of the reference's D3Q27 cumulant level step (see oal_oracle.cpp for the
-file:line map into the reference). Only tests/, the smoke check and the CPU-baseline leg of
-bench.py use it; the product path never imports it.
+C++ restatements of the reference's D3Q27 cumulant level step (oal_oracle.cpp) and of its D3Q19
+octree level step (oal_oracle_q19.cpp); each source holds the file:line map into the reference.
+Only tests/, the smoke check and the CPU-baseline leg of bench.py use it; the product path never
+imports it.
 """
 from __future__ import annotations
 
@@ -20,9 +21,8 @@ _lib = None
 
 
 def build(force: bool = False) -> Path:
-    src = HERE / "oal_oracle.cpp"
-    hdr = HERE.parent / "include" / "oal.h"
-    if force or not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < max(src.stat().st_mtime, hdr.stat().st_mtime):
+    deps = [HERE / "oal_oracle.cpp", HERE / "oal_oracle_q19.cpp", HERE.parent / "include" / "oal.h"]
+    if force or not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < max(d.stat().st_mtime for d in deps):
         subprocess.run(["make", "-s", "-C", str(HERE), "-B" if force else "liboal_oracle.so"], check=True)
     return LIB_PATH
 
@@ -44,6 +44,17 @@ def lib() -> C.CDLL:
             getattr(L, n).argtypes = [i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
             getattr(L, n).restype = C.c_int
         L.ora_mass_momentum_f64.argtypes = [i32, vp, vp, vp]
+        L.ora_q19_tables.argtypes = [vp] * 6
+        L.ora_q19_periodic_box.argtypes = [i32, i32, i32, vp, vp]
+        L.ora_q19_periodic_box.restype = C.c_int
+        i64 = C.c_int64
+        L.ora_q19_collide_f32.argtypes = [i64, vp, vp, C.c_float, vp, vp, vp, vp, vp]
+        L.ora_q19_collide_f64.argtypes = [i64, vp, vp, C.c_double, vp, vp, vp, vp, vp]
+        L.ora_q19_reference_collide_f32.argtypes = [i64, vp, vp, C.c_float, vp, vp, vp]
+        L.ora_q19_reference_collide_f64.argtypes = [i64, vp, vp, C.c_double, vp, vp, vp]
+        for suf in ("f32", "f64"):
+            getattr(L, f"ora_q19_step_{suf}").argtypes = [i32, vp, vp, vp, vp, vp, vp, vp, vp]
+            getattr(L, f"ora_q19_initialise_{suf}").argtypes = [i64, vp, vp, vp, C.c_double, vp]
         _lib = L
     return _lib
 
@@ -125,3 +136,88 @@ class OracleLevel:
         f = np.ascontiguousarray(self.f, np.float64)
         lib().ora_mass_momentum_f64(self.nb, _p(self.obstacle), _p(f), _p(out))
         return out
+
+
+# ---- D3Q19 octree (oal_oracle_q19.cpp) ---------------------------------------------------------
+
+def _suffix(dtype):
+    return "f64" if np.dtype(dtype) == np.float64 else "f32"
+
+
+def q19_tables():
+    cx, cy, cz = (np.zeros(19, np.int32) for _ in range(3))
+    w = np.zeros(19)
+    off, child = np.zeros((8, 19), np.int32), np.zeros((8, 19), np.int32)
+    lib().ora_q19_tables(_p(cx), _p(cy), _p(cz), _p(w), _p(off), _p(child))
+    return dict(cx=cx, cy=cy, cz=cz, w=w, src_off=off, src_child=child)
+
+
+def q19_periodic_box(n0, n1, n2):
+    """(origin (nocts, 3), onbr (nocts, 27) 1-based): level 1 of a periodic box, Morton order."""
+    no = (n0 // 2) * (n1 // 2) * (n2 // 2)
+    origin = np.zeros((no, 3), np.int32)
+    onbr = np.zeros((no, 27), np.int32)
+    assert lib().ora_q19_periodic_box(n0, n1, n2, _p(origin), _p(onbr)) == 0
+    return origin, onbr
+
+
+def q19_collide(f, omega, sigma, pfd, F, reference=False):
+    """Closed-form collision (or, with reference=True, the per-direction form) of n cells."""
+    dt = np.dtype(f.dtype)
+    f = np.ascontiguousarray(f)
+    n = f.shape[0]
+    omega = np.ascontiguousarray(omega, dt)
+    pfd = np.ascontiguousarray(pfd, dt)
+    F = np.ascontiguousarray(F, dt)
+    out = np.zeros((n, 19), dt)
+    if reference:
+        getattr(lib(), f"ora_q19_reference_collide_{_suffix(dt)}")(n, _p(f), _p(omega), sigma, _p(pfd), _p(F), _p(out))
+        return out
+    rho, u = np.zeros(n, dt), np.zeros((n, 3), dt)
+    getattr(lib(), f"ora_q19_collide_{_suffix(dt)}")(n, _p(f), _p(omega), sigma, _p(pfd), _p(F), _p(out), _p(rho), _p(u))
+    return out, rho, u
+
+
+class OracleQ19Level:
+    """One periodic octree level stepped by the CPU restatement; arrays in the reference's layout
+    (numpy C-order shapes: f (nocts, 19, 8), u (nocts, 3, 8), rho (nocts, 8))."""
+
+    def __init__(self, onbr, dtype=np.float32):
+        self.onbr = np.ascontiguousarray(onbr, np.int32)
+        self.nocts = self.onbr.shape[0]
+        self.dtype = np.dtype(dtype)
+        no = self.nocts
+        self.f = np.zeros((no, 19, 8), self.dtype)
+        self.g = np.zeros_like(self.f)
+        self.u = np.zeros((no, 3, 8), self.dtype)
+        self.v = np.zeros_like(self.u)
+        self.rho = np.ones((no, 8), self.dtype)
+        self.rhob = np.ones_like(self.rho)
+
+    def initialise(self, params, rho, u, du=None):
+        rho = np.ascontiguousarray(rho, self.dtype)
+        u = np.ascontiguousarray(u, self.dtype)
+        du = None if du is None else np.ascontiguousarray(du, self.dtype)
+        getattr(lib(), f"ora_q19_initialise_{_suffix(self.dtype)}")(self.nocts * 8, _p(rho), _p(u), _p(du),
+                                                                    float(params.nu), _p(self.f))
+        self.g[...] = self.f
+        self.u[...] = u
+        self.v[...] = u
+        self.rho[...] = rho
+        self.rhob[...] = rho
+
+    def step(self, params, n=1):
+        fn = getattr(lib(), f"ora_q19_step_{_suffix(self.dtype)}")
+        for _ in range(n):
+            fn(self.nocts, _p(self.onbr), C.addressof(params), _p(self.f), _p(self.g), _p(self.u), _p(self.v),
+               _p(self.rho), _p(self.rhob))
+            self.f, self.g = self.g, self.f
+            self.u, self.v = self.v, self.u
+            self.rho, self.rhob = self.rhob, self.rho
+        return self
+
+    def totals(self):
+        r = self.rho.astype(np.float64)
+        u = self.u.astype(np.float64)
+        return np.array([r.sum(), (r * u[:, 0]).sum(), (r * u[:, 1]).sum(), (r * u[:, 2]).sum(),
+                         0.5 * (r * (u ** 2).sum(1)).sum()])

@@ -1,0 +1,231 @@
+"""The D3Q19 octree level on the GPU: bit-for-bit parity with the oracle, and the reference's gates.
+
+Parity: every population, velocity and density after each configuration's steps has the oracle's
+bits (the kernel and the oracle evaluate the reference's closed form in the same IEEE operation
+order, without contraction). Gates (tools/tests/q19_octree_step.jl): G0.3 rest state, G0.4
+conservation, G1.1 shear-wave viscosity, G1.2 Taylor-Green convergence order, with the reference's
+sizes, step counts and thresholds.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from .test_oracle_q19 import SEED, _fields, _params, collide_each, g04_init, kat_inputs, random_states
+
+pytestmark = pytest.mark.gpu
+
+
+def same_bits(a, b):
+    a = np.ascontiguousarray(a)
+    b = np.ascontiguousarray(b)
+    v = np.uint64 if a.dtype == np.float64 else np.uint32
+    return a.shape == b.shape and np.array_equal(a.view(v), b.view(v))
+
+
+@pytest.fixture(scope="module")
+def env(oal, oracle_lib):
+    import torch
+    from openaerolab_alpha_01_b200 import octree
+    return oracle_lib, oracle_lib.q19_tables(), octree, torch
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+@pytest.mark.parametrize("noise", [1e-3, 0.6])
+def test_collide_cells_bitwise(env, dt, noise):
+    """The collision alone (2000 known-answer inputs; noise 0.6 drives many cells into the positivity
+    safeguard) equals the oracle bit for bit, and the per-direction form within the reference's bound."""
+    oracle, t, octree, torch = env
+    f, omega, sigma, pfd, F = kat_inputs(t, dt)
+    if noise != 1e-3:
+        f = random_states(t, f.shape[0], dt, np.random.default_rng(SEED + 7), noise=noise)
+    ref_out, ref_rho, ref_u = collide_each(oracle, f, omega, sigma, pfd, F)
+    dev = torch.device("cuda", 0)
+    out = np.zeros_like(f)
+    rho = np.zeros(f.shape[0], dt)
+    u = np.zeros((f.shape[0], 3), dt)
+    for s in np.unique(sigma):
+        m = sigma == s
+        tt = [torch.from_numpy(np.ascontiguousarray(a[m])).to(dev) for a in (f, omega, pfd, F)]
+        o, r, uu = octree.collide_cells(tt[0], tt[1], float(s), tt[2], tt[3])
+        out[m], rho[m], u[m] = o.cpu().numpy(), r.cpu().numpy(), uu.cpu().numpy()
+    assert same_bits(out, ref_out) and same_bits(rho, ref_rho) and same_bits(u, ref_u)
+    if noise == 1e-3:
+        per_dir = collide_each(oracle, f, omega, sigma, pfd, F, reference=True)
+        tol = 2e-15 if dt == np.float64 else 1e-6
+        assert np.abs(out.astype(np.float64) - per_dir).max() < tol
+
+
+def _pair(env, n, dt, p, init, nonequilibrium=True):
+    oracle, _, octree, _ = env
+    box = octree.PeriodicBox(*n)
+    cfg = octree.test_case_config(box, precision=dt)
+    st = octree.State(box, cfg)
+    st.params = p
+    rho, u, du = st.initial_fields(init, nonequilibrium)
+    st._upload(rho, u, du)
+    L = oracle.OracleQ19Level(box.onbr, dt)
+    L.initialise(p, rho, u, du)
+    return st, L
+
+
+def _check_same(st, L):
+    f, u, rho = st.state()
+    assert same_bits(f, L.f), np.abs(f.astype(float) - L.f).max()
+    assert same_bits(u, L.u) and same_bits(rho, L.rho)
+
+
+def shear_layer(n, amp=0.08):
+    tp = 2 * math.pi
+    return lambda x, y, z: (1.0 + 0.02 * np.sin(tp * x / n[0]) * np.cos(tp * y / n[1]),
+                            amp * np.sin(tp * z / n[2]) + 0.02 * np.cos(tp * y / n[1]),
+                            0.03 * np.sin(tp * x / n[0] + 1.0) * np.cos(tp * z / n[2]),
+                            0.02 * np.cos(tp * (x / n[0] + y / n[1])))
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+def test_initialise_bitwise(env, dt):
+    st, L = _pair(env, (16, 8, 12), dt, _params(nu=0.004), shear_layer((16, 8, 12)))
+    _check_same(st, L)
+    st.close()
+
+
+VARIANTS = [
+    # (sgs, sigma, body force)
+    (0, 1.0, (0.0, 0.0, 0.0)),
+    (0, 0.98, (0.0, 0.0, 0.0)),
+    (1, 0.98, (0.0, 0.0, 0.0)),
+    (1, 1.0, (1e-5, -2e-5, 3e-6)),
+    (2, 0.98, (0.0, 0.0, 0.0)),
+    (3, 1.0, (0.0, 0.0, 0.0)),
+    (3, 0.98, (2e-5, 0.0, 0.0)),
+    (0, 1.0, (1e-5, 0.0, -1e-5)),
+]
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+@pytest.mark.parametrize("sgs,sigma,F", VARIANTS)
+def test_level_step_bitwise(env, dt, sgs, sigma, F):
+    """20 steps of a non-cubic periodic level with a strong shear layer: GPU == oracle, bit for bit."""
+    n = (16, 8, 24)
+    p = _params(nu=0.002, sgs=sgs, sigma=sigma, F=F)
+    st, L = _pair(env, n, dt, p, shear_layer(n))
+    for _ in range(4):
+        st.advance(5)
+        L.step(p, 5)
+        _check_same(st, L)
+    st.close()
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+def test_level_step_limiter_bitwise(env, dt):
+    """A state far from equilibrium (random populations around a rest state) exercises the positivity
+    safeguard inside the level step; GPU == oracle, bit for bit."""
+    oracle, t, octree, _ = env
+    n = (8, 8, 8)
+    p = _params(nu=0.0005, sgs=1, sigma=0.98)
+    st, L = _pair(env, n, dt, p, shear_layer(n, 0.1))
+    rng = np.random.default_rng(SEED + 11)
+    f = (t["w"][None, :, None] * 0.5 * rng.standard_normal((st.mesh.nocts, 19, 8))).astype(dt)
+    _, u, rho = st.state()
+    st.set_state(f, u, rho)
+    L.f[...] = f
+    for _ in range(3):
+        st.advance(1)
+        L.step(p, 1)
+        _check_same(st, L)
+    st.close()
+
+
+def test_g03_rest_state(env):
+    """q19_octree_step.jl:30-41 on the GPU."""
+    _, _, octree, _ = env
+    box = octree.PeriodicBox(16)
+    assert box.counts["fluid_total"] == 16 ** 3
+    st = octree.State(box, octree.test_case_config(box))
+    st.initialise(lambda x, y, z: (1.0, 0.0 * x, 0.0 * x, 0.0 * x))
+    st.advance(50)
+    f, u, rho = st.state()
+    assert (f == 0).all() and (u == 0).all()
+    assert st.total_mass() == 16 ** 3
+    st.close()
+
+
+@pytest.mark.parametrize("dt,tol", [(np.float32, 2e-6), (np.float64, 1e-12)])
+@pytest.mark.parametrize("sigma", [1.0, 0.98])
+def test_g04_conservation(env, dt, tol, sigma):
+    """q19_octree_step.jl:43-54 on the GPU."""
+    _, _, octree, _ = env
+    box = octree.PeriodicBox(16)
+    st = octree.State(box, octree.test_case_config(box, precision=dt, hrr_sigma=sigma))
+    st.initialise(g04_init(16))
+    m0, p0 = st.total_mass(), st.total_momentum()
+    st.advance(100)
+    assert abs(st.total_mass() - m0) / m0 < tol
+    assert np.abs(st.total_momentum() - p0).max() / (16 ** 3 * 0.03) < tol
+    assert np.isfinite(st.state()[0]).all()
+    st.close()
+
+
+def _measured_nu(octree, n, nu, dt, steps):
+    U0 = 0.01
+    box = octree.PeriodicBox(n)
+    st = octree.State(box, octree.test_case_config(box, nu_lattice=nu, precision=dt))
+    st.initialise(lambda x, y, z: (1.0, U0 * np.sin(2 * np.pi * z / n), 0.0 * x, 0.0 * x))
+    s1 = steps // 5
+    st.advance(s1)
+    ke1 = st.kinetic_energy()
+    st.advance(steps - s1)
+    ke2 = st.kinetic_energy()
+    st.close()
+    k = 2 * np.pi / n
+    return -math.log(ke2 / ke1) / (2 * k * k * (steps - s1))
+
+
+@pytest.mark.parametrize("nu,steps64", [(0.02 / 3, 1500), (0.005 / 3, 6000)])
+def test_g11_shear_wave_viscosity(env, nu, steps64):
+    """q19_octree_step.jl:56-83: viscosity error < 1 % (FP32) / 0.5 % (FP64) at 64^3, second order."""
+    _, _, octree, _ = env
+    e32 = abs(_measured_nu(octree, 32, nu, np.float64, steps64 // 4) - nu) / nu
+    for dt, tol in ((np.float32, 0.01), (np.float64, 0.005)):
+        e64 = abs(_measured_nu(octree, 64, nu, dt, steps64) - nu) / nu
+        assert e64 < tol, (dt, e64)
+        if dt == np.float64:
+            assert e32 / e64 > 3.0, (e32, e64)
+
+
+def test_g12_taylor_green_order(env):
+    """q19_octree_step.jl:85-107: KE decay error < 1 % at 64^3 and convergence order >= 1.8."""
+    _, _, octree, _ = env
+    nu, U0 = 0.01, 0.002
+    errors = []
+    for n in (16, 32, 64):
+        k = 2 * np.pi / n
+        box = octree.PeriodicBox(n)
+        st = octree.State(box, octree.test_case_config(box, nu_lattice=nu, precision=np.float64))
+        st.initialise(lambda x, y, z: (1.0 + 3 * (U0 ** 2 / 4) * (np.cos(2 * k * x) + np.cos(2 * k * y)),
+                                       U0 * np.sin(k * x) * np.cos(k * y), -U0 * np.cos(k * x) * np.sin(k * y), 0.0 * x))
+        steps = 125 * (n // 16) ** 2
+        s1 = steps // 5
+        st.advance(s1)
+        ke1 = st.kinetic_energy()
+        st.advance(steps - s1)
+        ke2 = st.kinetic_energy()
+        st.close()
+        expected = math.exp(-4 * nu * k * k * (steps - s1))
+        errors.append(abs(ke2 / ke1 - expected) / expected)
+    order = math.log(errors[0] / errors[1]) / math.log(2)
+    order2 = math.log(errors[1] / errors[2]) / math.log(2)
+    assert errors[2] < 0.01, errors
+    assert min(order, order2) >= 1.8, (errors, order, order2)
+
+
+def test_unsupported_levels_are_refused(env):
+    """An oct without a neighbour (a domain face, a ghost or a body) has no kernel here: refused loudly."""
+    _, _, octree, _ = env
+    from openaerolab_alpha_01_b200 import _capi as capi
+    box = octree.PeriodicBox(4)
+    box.onbr[0, 4] = 0
+    with pytest.raises(capi.OALError) as e:
+        octree.State(box, octree.test_case_config(box))
+    assert e.value.status == capi.OAL_E_UNSUPPORTED
