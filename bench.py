@@ -195,6 +195,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--nz", type=int, default=128, help="channel depth (smaller values for profiling captures)")
     ap.add_argument("--layout", default="block", choices=["block", "dense"], help="population layout of the level")
+    ap.add_argument("--q19-steps", type=int, default=100,
+                    help="steps of the D3Q19 octree periodic-box measurement (256^3, FP32 and FP64); 0 skips it")
     ap.add_argument("--batch-steps", type=int, default=200,
                     help="steps of the batched-vs-plain-loop comparison (64-case config 4); 0 skips it")
     args = ap.parse_args()
@@ -313,11 +315,18 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_val, 2), "unit": "MLUPS",
                     "h2d_bytes_per_step": C.sizeof(capi.StepParams), "d2h_bytes_per_step": 24},
-            "gpu_launches": 2 * args.steps,
+            # per step: ghost fill, fast kernel, general kernel (blocks at the sphere), FP64 drag reduction
+            "gpu_launches": 4 * args.steps,
             "clocks": cs,
             "drag_fx_lattice": force[0],
             "cd": force[0] * case.meta["drag_scale"],
         }
+        if args.q19_steps > 0:
+            from openaerolab_alpha_01_b200.octree import benchmark_periodic_box
+            q = [benchmark_periodic_box(256, args.q19_steps, precision=dt) for dt in (np.float32, np.float64)]
+            for r in q:
+                r["roofline_frac"] = round(r["achieved_gbs"] / peak, 4)
+            line["octree_q19"] = q
         if args.batch_steps > 0:
             from openaerolab_alpha_01_b200.workloads import config4
             line["batched"] = config4(steps=args.batch_steps, storage=args.storage)

@@ -312,6 +312,10 @@ oal_status oal_mass_momentum_noalloc(const void* f, int32_t storage, int64_t f_b
  *     run.jl:6-11, stream.jl:280-380
  *   total_mass / total_momentum (Float64)                  oal_q19_level_totals
  *     state.jl:333-356
+ *   generate(tri, MeshSpec(levels=1)) generator.jl:106-837 oal_q19_mesh_generate / _counts / _level_desc
+ *   State(mesh, cfg, T) on a mesh with a body              oal_q19_level_create_desc
+ *   st.forces after advance!(st; collect=true)             oal_q19_level_forces
+ *     stream.jl:248-256, run.jl reduce_forces!
  *   collide_rr(f, omega, sigma, pi_fd, F) per cell         oal_q19_collide_cells (test hook)
  *     collision.jl:58-75, kernel.jl:92-134
  *
@@ -319,8 +323,9 @@ oal_status oal_mass_momentum_noalloc(const void* f, int32_t storage, int64_t f_b
  * u(8,3,nocts), rho(8,nocts), du(8,9,nocts) with du[k, 3a+b, o] = d u_b / d x_a over one cell,
  * onbr(27,nocts) 1-based (0 = none), origin(3,nocts) 0-based level cells. `precision` is
  * OAL_STORE_F32 or OAL_STORE_F64 (the solver's Float32 / Float64); host arrays have that type.
- * Levels whose octs miss a neighbour (domain faces, AMR ghosts, bodies) are refused with
- * OAL_E_UNSUPPORTED. */
+ * Octs of a periodic level made by oal_q19_level_create must have all 26 neighbours; levels with
+ * domain faces and bodies come through oal_q19_level_create_desc. Refinement (ghost / covered
+ * slots, several levels) is refused with OAL_E_UNSUPPORTED. */
 enum { OAL_Q19_SGS_NONE = 0, OAL_Q19_SGS_WALE = 1, OAL_Q19_SGS_SMAGORINSKY = 2, OAL_Q19_SGS_VREMAN = 3 };
 
 typedef struct oal_q19_params {
@@ -331,20 +336,80 @@ typedef struct oal_q19_params {
   double c_smagorinsky;   /* Smagorinsky constant (0.1); Vreman uses 2.5 c^2 */
   double hrr_sigma;       /* 1 = RR; < 1 blends the finite-difference stress (HRR) */
   double body_force[3];   /* Guo body force, lattice units of the level */
-  double reserved[4];
+  double u_inlet[3];      /* inlet / freestream velocity of the open faces, lattice units (stream.jl:291) */
+  double force_scale;     /* momentum-exchange scale of the level, 8^(1-l) (1 on a single level) */
 } oal_q19_params;
+
+/* Slot kinds (octree.jl:5-11) and domain-face conditions (MeshSpec.faces, generator.jl:29). */
+enum { OAL_Q19_K_NONE = 0, OAL_Q19_K_FLUID = 1, OAL_Q19_K_SOLID = 2, OAL_Q19_K_COVERED = 3, OAL_Q19_K_GHOST = 4,
+       OAL_Q19_K_BOUNDARY = 5 };
+enum { OAL_Q19_FACE_PERIODIC = 0, OAL_Q19_FACE_INLET = 1, OAL_Q19_FACE_OUTLET = 2, OAL_Q19_FACE_SLIP = 3,
+       OAL_Q19_FACE_SYMMETRY = 4, OAL_Q19_FACE_NOSLIP = 5, OAL_Q19_FACE_GROUND = 6, OAL_Q19_FACE_FREESTREAM = 7 };
+
+/* One level of an octree mesh, the reference's OctLevel arrays (octree.jl:50-71), all host memory,
+ * 1-based indices as in the reference. Nullable: real (all real), kind (all fluid), face, special
+ * and cutidx (none), the cut arrays when ncut = 0. */
+typedef struct oal_q19_level_desc {
+  int32_t nocts;
+  const int32_t* origin;       /* (3, nocts) level cells */
+  const uint8_t* real;         /* (nocts) stepped octs */
+  const int32_t* onbr;         /* (27, nocts) */
+  const uint8_t* kind;         /* (8, nocts) OAL_Q19_K_* */
+  const uint8_t* face;         /* (8, nocts) faces a boundary slot lies beyond, bit f = face f (-x +x -y +y -z +z) */
+  const uint32_t* special;     /* (8, nocts) bit j-1: direction j arrives by a face condition or a cut link */
+  const int32_t* cutidx;       /* (8, nocts) cut cell of a fluid slot, 0 none */
+  int32_t ncut;                /* cut cells */
+  const int32_t* cut_slot;     /* (ncut) slot id k + 8 (o - 1) */
+  const int32_t* cut_off;      /* (ncut + 1) CSR into the links */
+  int32_t nlinks;
+  const uint8_t* cut_dir;      /* (nlinks) direction 2..19 toward the wall */
+  const float* cut_q;          /* (nlinks) Bouzidi q in (0, 1] */
+  const int32_t* cut_tri;      /* (nlinks) triangle, 0 none */
+  const uint8_t* cut_partner;  /* (nlinks) the Bouzidi partner x - c_i is a plain fluid slot */
+  int32_t ntri;                /* triangles (force bins) */
+  int32_t faces[6];            /* OAL_Q19_FACE_* of -x +x -y +y -z +z */
+} oal_q19_level_desc;
+
+/* Mesh generator of one level from placed triangles (MeshSpec with levels = 1). */
+typedef struct oal_q19_mesh_spec {
+  double domain[3];            /* metres; periodic axes an even number of cells */
+  double dx;                   /* cell size, metres */
+  int32_t periodic[3];
+  int32_t faces[6];            /* OAL_Q19_FACE_*, PERIODIC exactly on periodic axes */
+  int32_t band_fine;           /* refinement band of the surface level, cells (8); sets the periodic replication margin */
+  int32_t reserved[5];
+} oal_q19_mesh_spec;
+typedef struct oal_q19_mesh oal_q19_mesh;
 
 typedef struct oal_q19_level oal_q19_level;
 
 oal_status oal_q19_default_params(oal_q19_params* out);
 oal_status oal_q19_periodic_box(int32_t n0, int32_t n1, int32_t n2, int32_t* origin, int32_t* onbr);
+oal_status oal_q19_default_mesh_spec(oal_q19_mesh_spec* out);
+/* tri: (ntri, 3 vertices, 3 coordinates) metres; ntri = 0 meshes an empty box */
+oal_status oal_q19_mesh_generate(const double* tri, int32_t ntri, const oal_q19_mesh_spec* spec, oal_q19_mesh** out);
+oal_status oal_q19_mesh_destroy(oal_q19_mesh* mesh);
+/* out[16] = {nocts, n0, n1, n2, fluid, solid, boundary, cut cells, cut links, leak cells,
+ *            links without a Bouzidi partner, unreached triangles, special slots, real octs, triangles with periodic copies, 0} */
+oal_status oal_q19_mesh_counts(const oal_q19_mesh* mesh, int64_t* out);
+/* the mesh's arrays as a level descriptor (pointers valid while the mesh lives) */
+oal_status oal_q19_mesh_level_desc(const oal_q19_mesh* mesh, oal_q19_level_desc* out);
+
 oal_status oal_q19_level_create(int32_t device, int32_t precision, int32_t nocts, const int32_t* onbr,
                                 oal_q19_level** out);
+oal_status oal_q19_level_create_desc(int32_t device, int32_t precision, const oal_q19_level_desc* desc,
+                                     oal_q19_level** out);
 oal_status oal_q19_level_destroy(oal_q19_level* level);
 /* host rho, u and (nullable) du: with du the Chapman-Enskog non-equilibrium is rebuilt, else the equilibrium */
 oal_status oal_q19_level_initialise(oal_q19_level* level, const oal_q19_params* p, const void* rho, const void* u,
                                     const void* du);
-oal_status oal_q19_level_advance(oal_q19_level* level, const oal_q19_params* p, int32_t n_steps, void* stream);
+/* n steps; with collect_forces the last step accumulates the momentum exchange of the cut links
+ * (stream.jl:248-256), read by oal_q19_level_forces */
+oal_status oal_q19_level_advance(oal_q19_level* level, const oal_q19_params* p, int32_t n_steps,
+                                 int32_t collect_forces, void* stream);
+/* FP64 force on the walls of the last collecting step: total[3], and per triangle (ntri, 3) if not null
+ * (links without a triangle count to triangle 1, as run.jl's accumulator does) */
+oal_status oal_q19_level_forces(oal_q19_level* level, double* total, double* per_triangle);
 oal_status oal_q19_level_get_state(oal_q19_level* level, void* f, void* u, void* rho);       /* host, nullable */
 oal_status oal_q19_level_set_state(oal_q19_level* level, const void* f, const void* u, const void* rho);
 oal_status oal_q19_level_device_state(oal_q19_level* level, void** f, void** u, void** rho, int64_t* steps);

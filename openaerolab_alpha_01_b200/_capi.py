@@ -135,7 +135,51 @@ class Q19Params(C.Structure):
         ("c_smagorinsky", C.c_double),
         ("hrr_sigma", C.c_double),
         ("body_force", C.c_double * 3),
-        ("reserved", C.c_double * 4),
+        ("u_inlet", C.c_double * 3),
+        ("force_scale", C.c_double),
+    ]
+
+
+OAL_Q19_K_NONE, OAL_Q19_K_FLUID, OAL_Q19_K_SOLID, OAL_Q19_K_COVERED, OAL_Q19_K_GHOST, OAL_Q19_K_BOUNDARY = range(6)
+(OAL_Q19_FACE_PERIODIC, OAL_Q19_FACE_INLET, OAL_Q19_FACE_OUTLET, OAL_Q19_FACE_SLIP, OAL_Q19_FACE_SYMMETRY,
+ OAL_Q19_FACE_NOSLIP, OAL_Q19_FACE_GROUND, OAL_Q19_FACE_FREESTREAM) = range(8)
+Q19_FACE_NAMES = {"periodic": 0, "inlet": 1, "outlet": 2, "slip": 3, "symmetry": 4, "noslip": 5, "ground": 6,
+                  "freestream": 7}
+
+
+class Q19LevelDesc(C.Structure):
+    """oal_q19_level_desc (include/oal.h): one octree level's arrays (the reference's OctLevel)."""
+    _fields_ = [
+        ("nocts", C.c_int32),
+        ("origin", C.c_void_p),
+        ("real", C.c_void_p),
+        ("onbr", C.c_void_p),
+        ("kind", C.c_void_p),
+        ("face", C.c_void_p),
+        ("special", C.c_void_p),
+        ("cutidx", C.c_void_p),
+        ("ncut", C.c_int32),
+        ("cut_slot", C.c_void_p),
+        ("cut_off", C.c_void_p),
+        ("nlinks", C.c_int32),
+        ("cut_dir", C.c_void_p),
+        ("cut_q", C.c_void_p),
+        ("cut_tri", C.c_void_p),
+        ("cut_partner", C.c_void_p),
+        ("ntri", C.c_int32),
+        ("faces", C.c_int32 * 6),
+    ]
+
+
+class Q19MeshSpec(C.Structure):
+    """oal_q19_mesh_spec (include/oal.h): MeshSpec of a single-level mesh."""
+    _fields_ = [
+        ("domain", C.c_double * 3),
+        ("dx", C.c_double),
+        ("periodic", C.c_int32 * 3),
+        ("faces", C.c_int32 * 6),
+        ("band_fine", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 
@@ -196,7 +240,14 @@ _SIGNATURES = {
     "oal_q19_level_create": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.POINTER(C.c_void_p)]),
     "oal_q19_level_destroy": (C.c_int32, [C.c_void_p]),
     "oal_q19_level_initialise": (C.c_int32, [C.c_void_p, C.POINTER(Q19Params), C.c_void_p, C.c_void_p, C.c_void_p]),
-    "oal_q19_level_advance": (C.c_int32, [C.c_void_p, C.POINTER(Q19Params), C.c_int32, C.c_void_p]),
+    "oal_q19_level_advance": (C.c_int32, [C.c_void_p, C.POINTER(Q19Params), C.c_int32, C.c_int32, C.c_void_p]),
+    "oal_q19_level_forces": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "oal_q19_level_create_desc": (C.c_int32, [C.c_int32, C.c_int32, C.POINTER(Q19LevelDesc), C.POINTER(C.c_void_p)]),
+    "oal_q19_default_mesh_spec": (C.c_int32, [C.POINTER(Q19MeshSpec)]),
+    "oal_q19_mesh_generate": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(Q19MeshSpec), C.POINTER(C.c_void_p)]),
+    "oal_q19_mesh_destroy": (C.c_int32, [C.c_void_p]),
+    "oal_q19_mesh_counts": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "oal_q19_mesh_level_desc": (C.c_int32, [C.c_void_p, C.POINTER(Q19LevelDesc)]),
     "oal_q19_level_get_state": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "oal_q19_level_set_state": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "oal_q19_level_device_state": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),

@@ -1,6 +1,6 @@
 """Build liboal.so (the sm_100a CUDA library) in-tree with nvcc.
 
-``python -m openaerolab_alpha_01_b200.build`` compiles every ``csrc/*.cu`` into
+``python -m openaerolab_alpha_01_b200.build`` compiles every ``csrc/*.cu`` and ``csrc/*.cpp`` into
 ``openaerolab_alpha_01_b200/liboal.so``. The library links the CUDA runtime statically, so the
 built file is self-contained and travels with the source tree.
 """
@@ -32,7 +32,8 @@ def nvcc() -> str:
 
 
 def sources() -> list[Path]:
-    return sorted(CSRC.glob("*.cu"))
+    """CUDA sources and the host-only C++ sources (the mesh generator), all compiled by nvcc."""
+    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
 
 
 def _stale(target: Path, deps: list[Path]) -> bool:
@@ -54,7 +55,7 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
     objs = []
     procs = []
     for s in srcs:
-        o = objdir / (s.stem + ".o")
+        o = objdir / (s.name.replace(".", "_") + ".o")
         objs.append(o)
         if force or _stale(o, [s] + headers):
             cmd = [nvcc(), *ARCH_FLAGS, *NVCC_FLAGS, *(extra or []), "-I", str(INCLUDE), "-c", str(s), "-o", str(o)]

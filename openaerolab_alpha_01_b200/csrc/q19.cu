@@ -259,6 +259,24 @@ __device__ __forceinline__ T nu_vreman(const T* g, T c) {
 
 __device__ __forceinline__ int nbr_slot_index(int dx, int dy, int dz) { return (dx + 1) + 3 * (dy + 1) + 9 * (dz + 1); }
 
+
+// direction of velocity (x, y, z), 0-based (lattice.jl:15-25)
+__host__ __device__ constexpr int dir_of(int x, int y, int z) {
+  return (x == 0 && y == 0 && z == 0) ? 0
+         : (x == 1 && y == 0 && z == 0) ? 1 : (x == -1 && y == 0 && z == 0) ? 2
+         : (x == 0 && y == 1 && z == 0) ? 3 : (x == 0 && y == -1 && z == 0) ? 4
+         : (x == 0 && y == 0 && z == 1) ? 5 : (x == 0 && y == 0 && z == -1) ? 6
+         : (x == 1 && y == 1 && z == 0) ? 7 : (x == -1 && y == -1 && z == 0) ? 8
+         : (x == 1 && y == -1 && z == 0) ? 9 : (x == -1 && y == 1 && z == 0) ? 10
+         : (x == 1 && y == 0 && z == 1) ? 11 : (x == -1 && y == 0 && z == -1) ? 12
+         : (x == 1 && y == 0 && z == -1) ? 13 : (x == -1 && y == 0 && z == 1) ? 14
+         : (x == 0 && y == 1 && z == 1) ? 15 : (x == 0 && y == -1 && z == -1) ? 16
+         : (x == 0 && y == 1 && z == -1) ? 17 : (x == 0 && y == -1 && z == 1) ? 18 : -1;
+}
+__host__ __device__ constexpr int opp(int i) { return dir_of(-cx(i), -cy(i), -cz(i)); }
+
+enum : uint8_t { K_NONE = 0, K_FLUID = 1, K_SOLID = 2, K_COVERED = 3, K_GHOST = 4, K_BOUNDARY = 5 };
+
 // ---- kernels -----------------------------------------------------------------------------------
 
 template <class T>
@@ -270,23 +288,124 @@ struct LevelArgs {
   const T* rhoin;
   T* rhoout;
   const int32_t* onbr;  // (27, nocts) 1-based
+  const int32_t* work;  // octs to step (null: octs 0 .. n_work-1)
+  int32_t n_work;
   int32_t nocts;
   T nu, omega0, cw, cs, cv, sigma;
   T F0, F1, F2;
 };
 
+// the per-slot tables of a level with domain faces and cut links
+template <class T>
+struct WallArgs {
+  const uint8_t* kind;      // (8, nocts)
+  const uint8_t* face;      // (8, nocts)
+  const uint32_t* special;  // (8, nocts)
+  const int32_t* cutidx;    // (8, nocts) 1-based
+  const float* qdir;        // (19, ncut)
+  const uint8_t* okdir;     // (19, ncut)
+  const int32_t* cut_off;   // (ncut + 1) 1-based
+  const uint8_t* cut_dir;   // (nlinks) 1-based direction
+  double* mom;              // (nlinks) momentum exchanged per link, or null
+  double scale;
+  int faces[6];
+  T uin0, uin1, uin2;
+};
+
+// staged neighbour rows of the CTA's octs; returns the number of octs of this CTA
+template <class T>
+__device__ __forceinline__ int stage_octs(const LevelArgs<T>& a, int32_t* s_nb, int64_t* s_o) {
+  const int64_t w0 = (int64_t)blockIdx.x * kOctsPerCta;
+  const int64_t total = a.n_work;
+  const int64_t left = total - w0;
+  const int n_here = left < kOctsPerCta ? (int)left : kOctsPerCta;
+  if (threadIdx.x < n_here) s_o[threadIdx.x] = a.work ? (int64_t)a.work[w0 + threadIdx.x] : w0 + threadIdx.x;
+  __syncthreads();
+  for (int t = threadIdx.x; t < n_here * 27; t += kThreads) s_nb[t] = a.onbr[s_o[t / 27] * 27 + t % 27] - 1;
+  __syncthreads();
+  return n_here;
+}
+
+// central differences of the previous step's velocity over the 6 face neighbours (stream.jl:13-30);
+// WALLS: a missing or domain-boundary neighbour contributes the slot's own velocity
+template <class T, bool WALLS>
+__device__ __forceinline__ void velocity_gradient(const LevelArgs<T>& a, const uint8_t* kind, const int32_t* nb, int64_t o,
+                                                  int k, T* g) {
+  const int x = k & 1, y = (k >> 1) & 1, z = (k >> 2) & 1;
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax) {
+    T vp[3], vm[3];
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      const int d = s == 0 ? 1 : -1;
+      const int nx = x + (ax == 0 ? d : 0), ny = y + (ax == 1 ? d : 0), nz = z + (ax == 2 ? d : 0);
+      const int ox = nx < 0 ? -1 : (nx > 1 ? 1 : 0), oy = ny < 0 ? -1 : (ny > 1 ? 1 : 0), oz = nz < 0 ? -1 : (nz > 1 ? 1 : 0);
+      int64_t no = nb[nbr_slot_index(ox, oy, oz)];
+      int nk = (nx - 2 * ox) + 2 * (ny - 2 * oy) + 4 * (nz - 2 * oz);
+      if (WALLS && (no < 0 || kind[no * 8 + nk] == K_BOUNDARY)) {
+        no = o;
+        nk = k;
+      }
+      T* v = s == 0 ? vp : vm;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) v[c] = __ldg(a.uin + no * 24 + 8 * c + nk);
+    }
+    const T h = T(0.5);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) g[3 * ax + c] = h * (vp[c] - vm[c]);
+  }
+}
+
+// subgrid viscosity, omega and the HRR stress of slot (k, o) (stream.jl:357-360)
+template <class T, int SGS, bool GRAD, bool WALLS>
+__device__ __forceinline__ T relaxation(const LevelArgs<T>& a, const uint8_t* kind, const int32_t* nb, int64_t o, int k,
+                                        T* pfd) {
+#pragma unroll
+  for (int n = 0; n < 6; ++n) pfd[n] = T(0);
+  if (!GRAD) return a.omega0;
+  T g[9];
+  velocity_gradient<T, WALLS>(a, kind, nb, o, k, g);
+  T nut = T(0);
+  if (SGS == 1) nut = nu_wale<T>(g, a.cw);
+  if (SGS == 2) nut = nu_smagorinsky<T>(g, a.cs);
+  if (SGS == 3) nut = nu_vreman<T>(g, a.cv);
+  const T omega = T(1) / (T(3) * (a.nu + nut) + T(0.5));
+  if (a.sigma != T(1)) {
+    const T rho_prev = a.rhoin[o * 8 + k];
+    const T tau = T(1) / omega;
+    const T c = -rho_prev * tau / T(3);
+    pfd[0] = c * T(2) * g[0];
+    pfd[1] = c * T(2) * g[4];
+    pfd[2] = c * T(2) * g[8];
+    pfd[3] = c * (g[1] + g[3]);
+    pfd[4] = c * (g[2] + g[6]);
+    pfd[5] = c * (g[5] + g[7]);
+  }
+  return omega;
+}
+
+template <class T>
+__device__ __forceinline__ void store_cell(const LevelArgs<T>& a, int64_t o, int k, const T* out, T rho, T ux, T uy, T uz) {
+  T* fo = a.fout + o * (8 * Q) + k;
+#pragma unroll
+  for (int i = 0; i < Q; ++i) fo[8 * i] = out[i];
+  T* uo = a.uout + o * 24 + k;
+  uo[0] = ux;
+  uo[8] = uy;
+  uo[16] = uz;
+  a.rhoout[o * 8 + k] = rho;
+}
+
+// octs whose eight slots are plain fluid cells (every pull source is a fluid slot)
 // SGS: 0 none, 1 WALE, 2 Smagorinsky, 3 Vreman; GRAD: the velocity gradient is needed (SGS or HRR)
 template <class T, int SGS, bool GRAD, bool FORCED>
 __global__ void __launch_bounds__(kThreads) k_q19_step(const LevelArgs<T> a) {
   __shared__ int32_t s_nb[kOctsPerCta * 27];
-  const int64_t o0 = (int64_t)blockIdx.x * kOctsPerCta;
-  const int64_t left = (int64_t)a.nocts - o0;
-  const int n_here = left < kOctsPerCta ? (int)left : kOctsPerCta;
-  for (int t = threadIdx.x; t < n_here * 27; t += kThreads) s_nb[t] = a.onbr[o0 * 27 + t] - 1;
-  __syncthreads();
+  __shared__ int64_t s_o[kOctsPerCta];
+  const int n_here = stage_octs<T>(a, s_nb, s_o);
   const int lo = threadIdx.x >> 3, k = threadIdx.x & 7;
   if (lo >= n_here) return;
-  const int64_t o = o0 + lo;
+  const int64_t o = s_o[lo];
   const int32_t* nb = s_nb + 27 * lo;
   const int x = k & 1, y = (k >> 1) & 1, z = (k >> 2) & 1;
 
@@ -300,86 +419,213 @@ __global__ void __launch_bounds__(kThreads) k_q19_step(const LevelArgs<T> a) {
     const int child = (px - 2 * ox) + 2 * (py - 2 * oy) + 4 * (pz - 2 * oz);
     f[i] = __ldg(a.fin + (int64_t)src * (8 * Q) + 8 * i + child);
   }
-
-  T omega = a.omega0;
-  T pfd[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
-  if (GRAD) {
-    // central differences of the previous step's velocity over the 6 face neighbours (stream.jl:13-30)
-    T g[9];
-#pragma unroll
-    for (int ax = 0; ax < 3; ++ax) {
-      T vp[3], vm[3];
-#pragma unroll
-      for (int s = 0; s < 2; ++s) {
-        const int d = s == 0 ? 1 : -1;
-        const int nx = x + (ax == 0 ? d : 0), ny = y + (ax == 1 ? d : 0), nz = z + (ax == 2 ? d : 0);
-        const int ox = nx < 0 ? -1 : (nx > 1 ? 1 : 0), oy = ny < 0 ? -1 : (ny > 1 ? 1 : 0), oz = nz < 0 ? -1 : (nz > 1 ? 1 : 0);
-        const int no = nb[nbr_slot_index(ox, oy, oz)];
-        const int nk = (nx - 2 * ox) + 2 * (ny - 2 * oy) + 4 * (nz - 2 * oz);
-        T* v = s == 0 ? vp : vm;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) v[c] = __ldg(a.uin + (int64_t)no * 24 + 8 * c + nk);
-      }
-      const T h = T(0.5);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) g[3 * ax + c] = h * (vp[c] - vm[c]);
-    }
-    T nut = T(0);
-    if (SGS == 1) nut = nu_wale<T>(g, a.cw);
-    if (SGS == 2) nut = nu_smagorinsky<T>(g, a.cs);
-    if (SGS == 3) nut = nu_vreman<T>(g, a.cv);
-    omega = T(1) / (T(3) * (a.nu + nut) + T(0.5));
-    if (a.sigma != T(1)) {
-      const T rho_prev = a.rhoin[o * 8 + k];
-      const T tau = T(1) / omega;
-      const T c = -rho_prev * tau / T(3);
-      pfd[0] = c * T(2) * g[0];
-      pfd[1] = c * T(2) * g[4];
-      pfd[2] = c * T(2) * g[8];
-      pfd[3] = c * (g[1] + g[3]);
-      pfd[4] = c * (g[2] + g[6]);
-      pfd[5] = c * (g[5] + g[7]);
-    }
-  }
+  T pfd[6];
+  const T omega = relaxation<T, SGS, GRAD, false>(a, nullptr, nb, o, k, pfd);
   T out[Q], rho, ux, uy, uz;
   collide<T>(f, omega, a.sigma, pfd, a.F0, a.F1, a.F2, FORCED, out, rho, ux, uy, uz);
-  T* fo = a.fout + o * (8 * Q) + k;
-#pragma unroll
-  for (int i = 0; i < Q; ++i) fo[8 * i] = out[i];
-  T* uo = a.uout + o * 24 + k;
-  uo[0] = ux;
-  uo[8] = uy;
-  uo[16] = uz;
-  a.rhoout[o * 8 + k] = rho;
+  store_cell<T>(a, o, k, out, rho, ux, uy, uz);
 }
 
-// initial state from (rho, u[, du]) per slot: `rebuild` with the Chapman-Enskog non-equilibrium,
-// or the equilibrium when du is null (state.jl:267-305, coupling.jl:26-30)
+// the population j arriving from a domain-boundary slot with face mask `mask` (stream.jl:32-78)
 template <class T>
-__global__ void k_q19_initialise(int64_t nslots, const T* __restrict__ rho_in, const T* __restrict__ u_in,
-                                 const T* __restrict__ du, T nu, T* __restrict__ fa, T* __restrict__ fb,
-                                 T* __restrict__ ua, T* __restrict__ ub, T* __restrict__ ra, T* __restrict__ rb) {
+__device__ T face_population(const WallArgs<T>& w, uint32_t mask, int j, const T* fo, T rho, T ux, T uy, T uz) {
+  const int i = opp(j);
+  auto feq_s = [](int d, T r, T vx, T vy, T vz, T vsq) { return feq_shifted<T>(d, r, vx, vy, vz, vsq); };
+  auto dirichlet = [&](int cond) {
+    const T usq = ux * ux + uy * uy + uz * uz;
+    const T own = fo[i] - feq_s(i, rho, ux, uy, uz, usq);
+    if (cond == OAL_Q19_FACE_INLET) {
+      const T vsq = w.uin0 * w.uin0 + w.uin1 * w.uin1 + w.uin2 * w.uin2;
+      return feq_s(j, rho, w.uin0, w.uin1, w.uin2, vsq) + own;
+    }
+    if (cond == OAL_Q19_FACE_OUTLET) return feq_s(j, T(1), ux, uy, uz, usq) + own;
+    const T vsq = w.uin0 * w.uin0 + w.uin1 * w.uin1 + w.uin2 * w.uin2;
+    return feq_s(j, T(1), w.uin0, w.uin1, w.uin2, vsq) + own;
+  };
+  auto mirror = [&](int d, int axis) {
+    return dir_of(axis == 0 ? -cx(d) : cx(d), axis == 1 ? -cy(d) : cy(d), axis == 2 ? -cz(d) : cz(d));
+  };
+  if (__popc(mask) == 1) {
+    const int f = __ffs(mask) - 1;
+    const int cond = w.faces[f];
+    if (cond == OAL_Q19_FACE_NOSLIP || cond == OAL_Q19_FACE_GROUND) return fo[i];
+    if (cond == OAL_Q19_FACE_SLIP || cond == OAL_Q19_FACE_SYMMETRY) return fo[mirror(j, f >> 1)];
+    return dirichlet(cond);
+  }
+  bool wall = false, open = false;
+  for (int f = 0; f < 6; ++f) {
+    if (!((mask >> f) & 1u)) continue;
+    const int c = w.faces[f];
+    wall = wall || c == OAL_Q19_FACE_NOSLIP || c == OAL_Q19_FACE_GROUND;
+    open = open || c == OAL_Q19_FACE_INLET || c == OAL_Q19_FACE_OUTLET || c == OAL_Q19_FACE_FREESTREAM;
+  }
+  if (wall) return fo[i];
+  if (open) return dirichlet(OAL_Q19_FACE_FREESTREAM);
+  int m = j;
+  if (mask & 0x03u) m = mirror(m, 0);
+  if (mask & 0x0cu) m = mirror(m, 1);
+  if (mask & 0x30u) m = mirror(m, 2);
+  return fo[m];
+}
+
+// octs with a non-fluid slot or a special direction: fluid slots step with the face conditions, the
+// Bouzidi rule on cut links and the momentum exchange (stream.jl:205-257)
+template <class T, int SGS, bool GRAD, bool FORCED>
+__global__ void __launch_bounds__(kThreads) k_q19_walls(const LevelArgs<T> a, const WallArgs<T> w) {
+  __shared__ int32_t s_nb[kOctsPerCta * 27];
+  __shared__ int64_t s_o[kOctsPerCta];
+  const int n_here = stage_octs<T>(a, s_nb, s_o);
+  const int lo = threadIdx.x >> 3, k = threadIdx.x & 7;
+  if (lo >= n_here) return;
+  const int64_t o = s_o[lo];
+  const int64_t s = o * 8 + k;
+  if (w.kind[s] != K_FLUID) return;
+  const int32_t* nb = s_nb + 27 * lo;
+  const int x = k & 1, y = (k >> 1) & 1, z = (k >> 2) & 1;
+  const uint32_t sp = w.special[s];
+  T f[Q];
+  auto pull = [&](int i, int& src, int& child) {
+    const int px = x - cx(i), py = y - cy(i), pz = z - cz(i);
+    const int ox = px < 0 ? -1 : (px > 1 ? 1 : 0), oy = py < 0 ? -1 : (py > 1 ? 1 : 0), oz = pz < 0 ? -1 : (pz > 1 ? 1 : 0);
+    src = nb[nbr_slot_index(ox, oy, oz)];
+    child = (px - 2 * ox) + 2 * (py - 2 * oy) + 4 * (pz - 2 * oz);
+  };
+  if (sp == 0) {
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+      int src, child;
+      pull(i, src, child);
+      f[i] = __ldg(a.fin + (int64_t)src * (8 * Q) + 8 * i + child);
+    }
+  } else {
+    T fo[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) fo[i] = a.fin[o * (8 * Q) + 8 * i + k];
+    const T rho0 = a.rhoin[s], ux0 = a.uin[o * 24 + k], uy0 = a.uin[o * 24 + 8 + k], uz0 = a.uin[o * 24 + 16 + k];
+    const int ci = w.cutidx[s] - 1;
+    for (int j = 0; j < Q; ++j) {
+      int src, child;
+      pull(j, src, child);
+      if (!((sp >> j) & 1u)) {
+        f[j] = __ldg(a.fin + (int64_t)src * (8 * Q) + 8 * j + child);
+      } else if (src >= 0 && w.kind[(int64_t)src * 8 + child] == K_BOUNDARY) {
+        f[j] = face_population<T>(w, w.face[(int64_t)src * 8 + child], j, fo, rho0, ux0, uy0, uz0);
+      } else {
+        // the link opposite to j is cut: Bouzidi from the own populations and the partner x - c_i
+        const int i = opp(j);
+        const T q = T(w.qdir[(int64_t)ci * Q + i]);
+        if (!w.okdir[(int64_t)ci * Q + i]) {
+          f[j] = fo[i];
+        } else if (q < T(0.5)) {
+          int po, pk;
+          {
+            const int px = x - cx(i), py = y - cy(i), pz = z - cz(i);
+            const int ox = px < 0 ? -1 : (px > 1 ? 1 : 0), oy = py < 0 ? -1 : (py > 1 ? 1 : 0), oz = pz < 0 ? -1 : (pz > 1 ? 1 : 0);
+            po = nb[nbr_slot_index(ox, oy, oz)];
+            pk = (px - 2 * ox) + 2 * (py - 2 * oy) + 4 * (pz - 2 * oz);
+          }
+          f[j] = T(2) * q * fo[i] + (T(1) - T(2) * q) * a.fin[(int64_t)po * (8 * Q) + 8 * i + pk];
+        } else {
+          const T inv2q = T(1) / (T(2) * q);
+          f[j] = inv2q * fo[i] + (T(1) - inv2q) * fo[j];
+        }
+      }
+    }
+    if (w.mom && ci >= 0) {
+      // momentum exchange on the cut links: (f_i* + f_j(t+1)) c_i per link, i toward the wall
+      for (int li = w.cut_off[ci] - 1; li < w.cut_off[ci + 1] - 1; ++li) {
+        const int i = w.cut_dir[li] - 1;
+        w.mom[li] = w.scale * (double)(fo[i] + f[opp(i)]);
+      }
+    }
+  }
+  T pfd[6];
+  const T omega = relaxation<T, SGS, GRAD, true>(a, w.kind, nb, o, k, pfd);
+  T out[Q], rho, ux, uy, uz;
+  collide<T>(f, omega, a.sigma, pfd, a.F0, a.F1, a.F2, FORCED, out, rho, ux, uy, uz);
+  store_cell<T>(a, o, k, out, rho, ux, uy, uz);
+}
+
+// per-triangle force: the triangle's links in ascending order (the reference's accumulator bins)
+__global__ void k_q19_tri_forces(int32_t ntri, const int32_t* __restrict__ tri_off, const int32_t* __restrict__ tri_links,
+                                 const uint8_t* __restrict__ cut_dir, const double* __restrict__ mom,
+                                 double* __restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ntri) return;
+  double fx = 0, fy = 0, fz = 0;
+  for (int n = tri_off[t]; n < tri_off[t + 1]; ++n) {
+    const int li = tri_links[n];
+    const int i = cut_dir[li] - 1;
+    const double m = mom[li];
+    fx += m * cx(i);
+    fy += m * cy(i);
+    fz += m * cz(i);
+  }
+  out[3 * (int64_t)t] = fx;
+  out[3 * (int64_t)t + 1] = fy;
+  out[3 * (int64_t)t + 2] = fz;
+}
+
+// fixed-order sum of the per-triangle forces: strided per thread, then a fixed tree
+__global__ void k_q19_force_total(int32_t ntri, const double* __restrict__ per_tri, double* __restrict__ total) {
+  __shared__ double s[3][256];
+  const int t = threadIdx.x;
+  double a0 = 0, a1 = 0, a2 = 0;
+  for (int i = t; i < ntri; i += 256) {
+    a0 += per_tri[3 * (int64_t)i];
+    a1 += per_tri[3 * (int64_t)i + 1];
+    a2 += per_tri[3 * (int64_t)i + 2];
+  }
+  s[0][t] = a0;
+  s[1][t] = a1;
+  s[2][t] = a2;
+  __syncthreads();
+  for (int h = 128; h > 0; h >>= 1) {
+    if (t < h)
+      for (int c = 0; c < 3; ++c) s[c][t] += s[c][t + h];
+    __syncthreads();
+  }
+  if (t < 3) total[t] = s[t][0];
+}
+
+// initial state of the fluid slots from (rho, u[, du]): `rebuild` with the Chapman-Enskog
+// non-equilibrium, or the equilibrium when du is null (state.jl:267-305, coupling.jl:26-30);
+// the other slots keep the allocation state (f = 0, u = 0, rho = 1)
+template <class T>
+__global__ void k_q19_initialise(int64_t nslots, const uint8_t* __restrict__ kind, const T* __restrict__ rho_in,
+                                 const T* __restrict__ u_in, const T* __restrict__ du, T nu, T* __restrict__ fa,
+                                 T* __restrict__ fb, T* __restrict__ ua, T* __restrict__ ub, T* __restrict__ ra,
+                                 T* __restrict__ rb) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nslots) return;
   const int64_t o = s >> 3;
   const int k = (int)(s & 7);
-  const T rho = rho_in[s];
-  const T ux = u_in[o * 24 + k], uy = u_in[o * 24 + 8 + k], uz = u_in[o * 24 + 16 + k];
+  const bool fluid = !kind || kind[s] == K_FLUID;
   T out[Q];
-  const T drho = rho - T(1);
-  const T omega = T(1) / (T(3) * nu + T(0.5));
-  if (du) {
-    T d[9];
+  T rho = T(1), ux = T(0), uy = T(0), uz = T(0);
+  if (fluid) {
+    rho = rho_in[s];
+    ux = u_in[o * 24 + k];
+    uy = u_in[o * 24 + 8 + k];
+    uz = u_in[o * 24 + 16 + k];
+    const T drho = rho - T(1);
+    const T omega = T(1) / (T(3) * nu + T(0.5));
+    if (du) {
+      T d[9];
 #pragma unroll
-    for (int n = 0; n < 9; ++n) d[n] = du[o * 72 + 8 * n + k];
-    const T tau = T(1) / omega;
-    const T c = -rho * tau / T(3);
-    const T pn[6] = {c * T(2) * d[0], c * T(2) * d[4], c * T(2) * d[8], c * (d[1] + d[3]), c * (d[2] + d[6]), c * (d[5] + d[7])};
-    populations<T>(drho, rho, ux, uy, uz, pn, T(1) - omega, out);
-    if (below_floor<T>(out)) limit_unforced<T>(out, drho, rho, ux, uy, uz);
+      for (int n = 0; n < 9; ++n) d[n] = du[o * 72 + 8 * n + k];
+      const T tau = T(1) / omega;
+      const T c = -rho * tau / T(3);
+      const T pn[6] = {c * T(2) * d[0], c * T(2) * d[4], c * T(2) * d[8], c * (d[1] + d[3]), c * (d[2] + d[6]), c * (d[5] + d[7])};
+      populations<T>(drho, rho, ux, uy, uz, pn, T(1) - omega, out);
+      if (below_floor<T>(out)) limit_unforced<T>(out, drho, rho, ux, uy, uz);
+    } else {
+      const T zz[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+      populations<T>(drho, rho, ux, uy, uz, zz, T(0), out);
+    }
   } else {
-    const T zz[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
-    populations<T>(drho, rho, ux, uy, uz, zz, T(0), out);
+#pragma unroll
+    for (int i = 0; i < Q; ++i) out[i] = T(0);
   }
 #pragma unroll
   for (int i = 0; i < Q; ++i) {
@@ -417,12 +663,14 @@ __global__ void k_q19_collide_cells(int64_t n, const T* __restrict__ f, const T*
   u[3 * c + 2] = uz;
 }
 
-// FP64 totals per CTA: mass, momentum, kinetic energy over the slots (state.jl:333-356)
+// FP64 totals per CTA over the fluid slots: mass, momentum, kinetic energy (state.jl:333-356)
 template <class T>
-__global__ void k_q19_totals(int64_t nslots, const T* __restrict__ rho, const T* __restrict__ u, double* __restrict__ part) {
+__global__ void k_q19_totals(int64_t nslots, const uint8_t* __restrict__ kind, const T* __restrict__ rho,
+                             const T* __restrict__ u, double* __restrict__ part) {
   __shared__ double s[5][8];
   double a[5] = {0, 0, 0, 0, 0};
   for (int64_t sl = (int64_t)blockIdx.x * 256 + threadIdx.x; sl < nslots; sl += (int64_t)gridDim.x * 256) {
+    if (kind && kind[sl] != K_FLUID) continue;
     const int64_t o = sl >> 3;
     const int k = (int)(sl & 7);
     const double r = (double)rho[sl];
@@ -452,6 +700,12 @@ __global__ void k_q19_totals_final(const double* __restrict__ part, int n, doubl
     for (int b = 0; b < n; ++b) v += part[5 * b + threadIdx.x];
     out[threadIdx.x] = v;
   }
+}
+
+template <class T>
+__global__ void k_fill(T* p, int64_t n, T v) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
 }
 
 constexpr int kTotalsCtas = 592;  // 4 per SM on 148 SMs
@@ -498,6 +752,14 @@ uint64_t spread3(uint64_t v) {
 }
 uint64_t morton3(uint64_t ix, uint64_t iy, uint64_t iz) { return spread3(ix) | (spread3(iy) << 1) | (spread3(iz) << 2); }
 
+template <class X>
+cudaError_t upload(X** dst, const X* src, size_t n) {
+  if (n == 0) return cudaSuccess;
+  cudaError_t e = cudaMalloc(dst, sizeof(X) * n);
+  if (e == cudaSuccess) e = cudaMemcpy(*dst, src, sizeof(X) * n, cudaMemcpyHostToDevice);
+  return e;
+}
+
 }  // namespace
 
 struct oal_q19_level {
@@ -512,6 +774,25 @@ struct oal_q19_level {
   double* part = nullptr;  // kTotalsCtas * 5 + 5
   int cur = 0;             // buffer holding the current state
   int64_t steps = 0;
+  // levels with faces / cut links
+  bool walls = false;
+  uint8_t* kind = nullptr;
+  uint8_t* face = nullptr;
+  uint32_t* special = nullptr;
+  int32_t* cutidx = nullptr;
+  float* qdir = nullptr;
+  uint8_t* okdir = nullptr;
+  int32_t* cut_off = nullptr;
+  uint8_t* cut_dir = nullptr;
+  double* mom = nullptr;
+  int32_t* tri_off = nullptr;
+  int32_t* tri_links = nullptr;
+  double* tri_force = nullptr;  // (ntri, 3) then the total (3)
+  int32_t* work_plain = nullptr;
+  int32_t* work_walls = nullptr;
+  int32_t n_plain = 0, n_walls = 0, ncut = 0, nlinks = 0, ntri = 0;
+  int faces[6] = {0, 0, 0, 0, 0, 0};
+  bool forces_valid = false;
 };
 
 namespace {
@@ -524,7 +805,9 @@ oal_status check_params(const oal_q19_params* p) {
   if (p->sgs < OAL_Q19_SGS_NONE || p->sgs > OAL_Q19_SGS_VREMAN) return fail(OAL_E_INVALID_ARG, "sgs model %d", p->sgs);
   if (!(p->hrr_sigma >= 0 && p->hrr_sigma <= 1)) return fail(OAL_E_INVALID_ARG, "hrr_sigma must lie in [0, 1]");
   for (int a = 0; a < 3; ++a)
-    if (!std::isfinite(p->body_force[a])) return fail(OAL_E_INVALID_ARG, "body_force must be finite");
+    if (!std::isfinite(p->body_force[a]) || !std::isfinite(p->u_inlet[a]))
+      return fail(OAL_E_INVALID_ARG, "body_force and u_inlet must be finite");
+  if (!std::isfinite(p->force_scale)) return fail(OAL_E_INVALID_ARG, "force_scale must be finite");
   return OAL_OK;
 }
 
@@ -539,6 +822,8 @@ LevelArgs<T> level_args(oal_q19_level* L, const oal_q19_params* p) {
   a.rhoin = static_cast<const T*>(L->rho[src]);
   a.rhoout = static_cast<T*>(L->rho[dst]);
   a.onbr = L->onbr;
+  a.work = L->walls ? L->work_plain : nullptr;
+  a.n_work = L->walls ? L->n_plain : L->nocts;
   a.nocts = L->nocts;
   a.nu = T(p->nu);
   a.omega0 = T(1) / (T(3) * a.nu + T(0.5));
@@ -553,10 +838,23 @@ LevelArgs<T> level_args(oal_q19_level* L, const oal_q19_params* p) {
 }
 
 template <class T, int SGS, bool GRAD>
-cudaError_t launch_step3(const LevelArgs<T>& a, bool forced, cudaStream_t st) {
-  const unsigned grid = (unsigned)((a.nocts + kOctsPerCta - 1) / kOctsPerCta);
-  if (forced) k_q19_step<T, SGS, GRAD, true><<<grid, kThreads, 0, st>>>(a);
-  else k_q19_step<T, SGS, GRAD, false><<<grid, kThreads, 0, st>>>(a);
+cudaError_t launch3(const LevelArgs<T>& a, const WallArgs<T>* w, bool forced, cudaStream_t st) {
+  const int64_t n = a.n_work;
+  if (n > 0) {
+    const unsigned grid = (unsigned)((n + kOctsPerCta - 1) / kOctsPerCta);
+    if (forced) k_q19_step<T, SGS, GRAD, true><<<grid, kThreads, 0, st>>>(a);
+    else k_q19_step<T, SGS, GRAD, false><<<grid, kThreads, 0, st>>>(a);
+  }
+  (void)w;
+  return cudaGetLastError();
+}
+
+template <class T, int SGS, bool GRAD>
+cudaError_t launch_walls3(const LevelArgs<T>& a, const WallArgs<T>& w, bool forced, cudaStream_t st) {
+  if (a.n_work <= 0) return cudaSuccess;
+  const unsigned grid = (unsigned)((a.n_work + kOctsPerCta - 1) / kOctsPerCta);
+  if (forced) k_q19_walls<T, SGS, GRAD, true><<<grid, kThreads, 0, st>>>(a, w);
+  else k_q19_walls<T, SGS, GRAD, false><<<grid, kThreads, 0, st>>>(a, w);
   return cudaGetLastError();
 }
 
@@ -564,22 +862,99 @@ template <class T>
 cudaError_t launch_step(const LevelArgs<T>& a, int sgs, bool forced, cudaStream_t st) {
   const bool hrr = a.sigma != T(1);
   switch (sgs) {
-    case OAL_Q19_SGS_WALE: return launch_step3<T, 1, true>(a, forced, st);
-    case OAL_Q19_SGS_SMAGORINSKY: return launch_step3<T, 2, true>(a, forced, st);
-    case OAL_Q19_SGS_VREMAN: return launch_step3<T, 3, true>(a, forced, st);
-    default: return hrr ? launch_step3<T, 0, true>(a, forced, st) : launch_step3<T, 0, false>(a, forced, st);
+    case OAL_Q19_SGS_WALE: return launch3<T, 1, true>(a, nullptr, forced, st);
+    case OAL_Q19_SGS_SMAGORINSKY: return launch3<T, 2, true>(a, nullptr, forced, st);
+    case OAL_Q19_SGS_VREMAN: return launch3<T, 3, true>(a, nullptr, forced, st);
+    default: return hrr ? launch3<T, 0, true>(a, nullptr, forced, st) : launch3<T, 0, false>(a, nullptr, forced, st);
   }
 }
 
 template <class T>
-oal_status advance_t(oal_q19_level* L, const oal_q19_params* p, int32_t n, cudaStream_t st) {
+cudaError_t launch_walls(const LevelArgs<T>& a, const WallArgs<T>& w, int sgs, bool forced, cudaStream_t st) {
+  const bool hrr = a.sigma != T(1);
+  switch (sgs) {
+    case OAL_Q19_SGS_WALE: return launch_walls3<T, 1, true>(a, w, forced, st);
+    case OAL_Q19_SGS_SMAGORINSKY: return launch_walls3<T, 2, true>(a, w, forced, st);
+    case OAL_Q19_SGS_VREMAN: return launch_walls3<T, 3, true>(a, w, forced, st);
+    default: return hrr ? launch_walls3<T, 0, true>(a, w, forced, st) : launch_walls3<T, 0, false>(a, w, forced, st);
+  }
+}
+
+template <class T>
+oal_status advance_t(oal_q19_level* L, const oal_q19_params* p, int32_t n, bool collect, cudaStream_t st) {
   const bool forced = !(T(p->body_force[0]) == T(0) && T(p->body_force[1]) == T(0) && T(p->body_force[2]) == T(0));
   for (int32_t s = 0; s < n; ++s) {
     const LevelArgs<T> a = level_args<T>(L, p);
     Q19_TRY(launch_step<T>(a, p->sgs, forced, st));
+    if (L->walls) {
+      LevelArgs<T> b = a;
+      b.work = L->work_walls;
+      b.n_work = L->n_walls;
+      WallArgs<T> w;
+      w.kind = L->kind;
+      w.face = L->face;
+      w.special = L->special;
+      w.cutidx = L->cutidx;
+      w.qdir = L->qdir;
+      w.okdir = L->okdir;
+      w.cut_off = L->cut_off;
+      w.cut_dir = L->cut_dir;
+      const bool last = s == n - 1;
+      w.mom = (collect && last && L->nlinks > 0) ? L->mom : nullptr;
+      w.scale = p->force_scale;
+      for (int f = 0; f < 6; ++f) w.faces[f] = L->faces[f];
+      w.uin0 = T(p->u_inlet[0]);
+      w.uin1 = T(p->u_inlet[1]);
+      w.uin2 = T(p->u_inlet[2]);
+      Q19_TRY(launch_walls<T>(b, w, p->sgs, forced, st));
+      if (w.mom) {
+        k_q19_tri_forces<<<(L->ntri + 127) / 128, 128, 0, st>>>(L->ntri, L->tri_off, L->tri_links, L->cut_dir, L->mom,
+                                                               L->tri_force);
+        k_q19_force_total<<<1, 256, 0, st>>>(L->ntri, L->tri_force, L->tri_force + 3 * (int64_t)L->ntri);
+        Q19_TRY(cudaGetLastError());
+        L->forces_valid = true;
+      }
+    }
     L->cur = 1 - L->cur;
     ++L->steps;
   }
+  return OAL_OK;
+}
+
+oal_status alloc_state(oal_q19_level* L) {
+  const size_t ns = (size_t)L->nocts * 8;
+  cudaError_t e = cudaSuccess;
+  for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
+    e = cudaMalloc(&L->f[b], L->es * ns * Q);
+    if (e == cudaSuccess) e = cudaMalloc(&L->u[b], L->es * ns * 3);
+    if (e == cudaSuccess) e = cudaMalloc(&L->rho[b], L->es * ns);
+    // the allocation state of the reference: f = 0, u = 0, rho = 1 (state.jl:217-232)
+    if (e == cudaSuccess) e = cudaMemset(L->f[b], 0, L->es * ns * Q);
+    if (e == cudaSuccess) e = cudaMemset(L->u[b], 0, L->es * ns * 3);
+    if (e == cudaSuccess) {
+      const unsigned grid = (unsigned)((ns + 255) / 256);
+      if (L->precision == OAL_STORE_F64) k_fill<double><<<grid, 256>>>((double*)L->rho[b], (int64_t)ns, 1.0);
+      else k_fill<float><<<grid, 256>>>((float*)L->rho[b], (int64_t)ns, 1.0f);
+      e = cudaGetLastError();
+    }
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&L->part, sizeof(double) * (kTotalsCtas * 5 + 5));
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? OAL_E_OUT_OF_MEMORY : OAL_E_CUDA, "level allocation: %s",
+                cudaGetErrorString(e));
+  }
+  return OAL_OK;
+}
+
+oal_status check_device(int32_t device) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(OAL_E_NO_DEVICE, "no CUDA device");
+  }
+  if (device < 0 || device >= ndev) return fail(OAL_E_INVALID_ARG, "device %d of %d", device, ndev);
   return OAL_OK;
 }
 
@@ -596,6 +971,7 @@ oal_status oal_q19_default_params(oal_q19_params* p) {
   p->c_wale = 0.5;          // config.jl Numerics defaults
   p->c_smagorinsky = 0.1;
   p->hrr_sigma = 1.0;
+  p->force_scale = 1.0;
   return OAL_OK;
 }
 
@@ -642,38 +1018,183 @@ oal_status oal_q19_level_create(int32_t device, int32_t precision, int32_t nocts
     if (onbr[t] < 0 || onbr[t] > nocts) return fail(OAL_E_INVALID_ARG, "onbr entry %lld out of range", (long long)t);
     if (onbr[t] == 0)
       return fail(OAL_E_UNSUPPORTED,
-                  "oct %lld has no neighbour at offset %d: levels with boundary, ghost or solid slots have no "
-                  "kernel in this build (periodic single levels only)", (long long)(t / 27) + 1, (int)(t % 27));
+                  "oct %lld has no neighbour at offset %d: a level with domain faces or bodies needs its slot "
+                  "tables (oal_q19_level_create_desc)", (long long)(t / 27) + 1, (int)(t % 27));
   }
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
-    cudaGetLastError();
-    return fail(OAL_E_NO_DEVICE, "no CUDA device");
-  }
-  if (device < 0 || device >= ndev) return fail(OAL_E_INVALID_ARG, "device %d of %d", device, ndev);
+  if (oal_status s = check_device(device)) return s;
   DeviceGuard g(device);
   oal_q19_level* L = new oal_q19_level();
   L->device = device;
   L->precision = precision;
   L->nocts = nocts;
   L->es = precision == OAL_STORE_F64 ? 8 : 4;
-  const size_t ns = (size_t)nocts * 8;
-  auto cleanup = [&](oal_status s) {
+  oal_status s = alloc_state(L);
+  if (s == OAL_OK) {
+    const cudaError_t e = upload(&L->onbr, onbr, (size_t)27 * nocts);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      s = fail(OAL_E_OUT_OF_MEMORY, "level tables: %s", cudaGetErrorString(e));
+    }
+  }
+  if (s != OAL_OK) {
     oal_q19_level_destroy(L);
     return s;
-  };
-  cudaError_t e = cudaMalloc(&L->onbr, sizeof(int32_t) * 27 * (size_t)nocts);
-  for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
-    e = cudaMalloc(&L->f[b], L->es * ns * Q);
-    if (e == cudaSuccess) e = cudaMalloc(&L->u[b], L->es * ns * 3);
-    if (e == cudaSuccess) e = cudaMalloc(&L->rho[b], L->es * ns);
   }
-  if (e == cudaSuccess) e = cudaMalloc(&L->part, sizeof(double) * (kTotalsCtas * 5 + 5));
-  if (e == cudaSuccess) e = cudaMemcpy(L->onbr, onbr, sizeof(int32_t) * 27 * (size_t)nocts, cudaMemcpyHostToDevice);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    return cleanup(fail(e == cudaErrorMemoryAllocation ? OAL_E_OUT_OF_MEMORY : OAL_E_CUDA, "level allocation: %s",
-                        cudaGetErrorString(e)));
+  *out = L;
+  return OAL_OK;
+}
+
+oal_status oal_q19_level_create_desc(int32_t device, int32_t precision, const oal_q19_level_desc* d, oal_q19_level** out) {
+  if (!out || !d || !d->onbr) return fail(OAL_E_INVALID_ARG, "null argument");
+  *out = nullptr;
+  if (precision != OAL_STORE_F32 && precision != OAL_STORE_F64)
+    return fail(OAL_E_INVALID_ARG, "the octree level stores FP32 or FP64 populations (got storage %d)", precision);
+  const int32_t nocts = d->nocts;
+  if (nocts <= 0 || (int64_t)nocts * 27 > INT32_MAX) return fail(OAL_E_INVALID_ARG, "bad oct count %d", nocts);
+  if (d->ncut < 0 || d->nlinks < 0 || d->ntri < 0) return fail(OAL_E_INVALID_ARG, "negative counts");
+  if (d->ncut > 0 && (!d->cutidx || !d->cut_off || !d->cut_dir || !d->cut_q || !d->cut_partner))
+    return fail(OAL_E_INVALID_ARG, "cut cells need cutidx, cut_off, cut_dir, cut_q and cut_partner");
+  for (int f = 0; f < 6; ++f)
+    if (d->faces[f] < OAL_Q19_FACE_PERIODIC || d->faces[f] > OAL_Q19_FACE_FREESTREAM)
+      return fail(OAL_E_INVALID_ARG, "face %d: unknown condition %d", f, d->faces[f]);
+  const size_t ns = (size_t)nocts * 8;
+  // host-side validation of every index the kernels follow
+  std::vector<uint8_t> kind(ns, OAL_Q19_K_FLUID);
+  if (d->kind) std::memcpy(kind.data(), d->kind, ns);
+  for (size_t s = 0; s < ns; ++s) {
+    if (kind[s] > OAL_Q19_K_BOUNDARY) return fail(OAL_E_INVALID_ARG, "slot %zu: unknown kind %d", s, kind[s]);
+    if (kind[s] == OAL_Q19_K_GHOST || kind[s] == OAL_Q19_K_COVERED)
+      return fail(OAL_E_UNSUPPORTED, "ghost and covered slots (refined levels) have no kernel in this build");
+  }
+  for (int64_t t = 0; t < (int64_t)nocts * 27; ++t)
+    if (d->onbr[t] < 0 || d->onbr[t] > nocts) return fail(OAL_E_INVALID_ARG, "onbr entry %lld out of range", (long long)t);
+  std::vector<uint32_t> special(ns, 0);
+  if (d->special) std::memcpy(special.data(), d->special, ns * 4);
+  std::vector<int32_t> cutidx(ns, 0);
+  if (d->cutidx) std::memcpy(cutidx.data(), d->cutidx, ns * 4);
+  if (d->ncut > 0) {
+    if (d->cut_off[0] != 1 || d->cut_off[d->ncut] != d->nlinks + 1)
+      return fail(OAL_E_INVALID_ARG, "cut_off must run from 1 to nlinks + 1");
+    for (int c = 0; c < d->ncut; ++c)
+      if (d->cut_off[c + 1] < d->cut_off[c]) return fail(OAL_E_INVALID_ARG, "cut_off must not decrease");
+    for (int li = 0; li < d->nlinks; ++li) {
+      if (d->cut_dir[li] < 2 || d->cut_dir[li] > 19) return fail(OAL_E_INVALID_ARG, "cut_dir %d", d->cut_dir[li]);
+      if (!(d->cut_q[li] > 0 && d->cut_q[li] <= 1)) return fail(OAL_E_INVALID_ARG, "cut_q must lie in (0, 1]");
+      if (d->cut_tri && (d->cut_tri[li] < 0 || d->cut_tri[li] > d->ntri)) return fail(OAL_E_INVALID_ARG, "cut_tri out of range");
+    }
+  }
+  std::vector<int32_t> plain, walls;
+  for (int32_t o = 0; o < nocts; ++o) {
+    if (d->real && !d->real[o]) continue;
+    bool any_fluid = false, all_plain = true;
+    for (int k = 0; k < 8; ++k) {
+      const size_t s = (size_t)o * 8 + k;
+      const bool fluid = kind[s] == OAL_Q19_K_FLUID;
+      any_fluid |= fluid;
+      if (!fluid || special[s] != 0) all_plain = false;
+      if (cutidx[s] < 0 || cutidx[s] > d->ncut) return fail(OAL_E_INVALID_ARG, "cutidx out of range");
+      if (!fluid) continue;
+      if (special[s] & 1u) return fail(OAL_E_INVALID_ARG, "the rest direction cannot be special");
+      // every pull source of a fluid slot must exist unless its direction is special; a special
+      // direction whose source is not a boundary slot needs the slot's cut cell
+      const int x = k & 1, y = (k >> 1) & 1, z = (k >> 2) & 1;
+      for (int j = 0; j < Q; ++j) {
+        const int px = x - cx(j), py = y - cy(j), pz = z - cz(j);
+        const int ox = px < 0 ? -1 : (px > 1 ? 1 : 0), oy = py < 0 ? -1 : (py > 1 ? 1 : 0), oz = pz < 0 ? -1 : (pz > 1 ? 1 : 0);
+        const int so = d->onbr[(int64_t)o * 27 + (ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)] - 1;
+        const int child = (px - 2 * ox) + 2 * (py - 2 * oy) + 4 * (pz - 2 * oz);
+        const bool boundary_src = so >= 0 && kind[(size_t)so * 8 + child] == OAL_Q19_K_BOUNDARY;
+        if (!((special[s] >> j) & 1u)) {
+          if (so < 0) return fail(OAL_E_INVALID_ARG, "slot %zu pulls direction %d from a missing oct", s, j + 1);
+          continue;
+        }
+        if (boundary_src) continue;
+        const int ci = cutidx[s] - 1;
+        if (ci < 0) return fail(OAL_E_INVALID_ARG, "slot %zu: special direction %d without a cut cell", s, j + 1);
+        // the Bouzidi q < 1/2 branch reads the partner x - c_i (i = opp j) when the link has one
+        const int i = opp(j);
+        bool found = false, ok = false;
+        for (int li = d->cut_off[ci] - 1; li < d->cut_off[ci + 1] - 1; ++li)
+          if (d->cut_dir[li] - 1 == i) {
+            found = true;
+            ok = d->cut_partner[li] != 0;
+          }
+        if (!found) return fail(OAL_E_INVALID_ARG, "slot %zu: special direction %d without its cut link", s, j + 1);
+        if (ok) {
+          const int qx = x - cx(i), qy = y - cy(i), qz = z - cz(i);
+          const int px2 = qx < 0 ? -1 : (qx > 1 ? 1 : 0), py2 = qy < 0 ? -1 : (qy > 1 ? 1 : 0), pz2 = qz < 0 ? -1 : (qz > 1 ? 1 : 0);
+          if (d->onbr[(int64_t)o * 27 + (px2 + 1) + 3 * (py2 + 1) + 9 * (pz2 + 1)] == 0)
+            return fail(OAL_E_INVALID_ARG, "slot %zu: a Bouzidi partner in a missing oct", s);
+        }
+      }
+      // the velocity gradient falls back to the own velocity for missing neighbours (no read)
+    }
+    if (!any_fluid) continue;
+    (all_plain ? plain : walls).push_back(o);
+  }
+  if (oal_status s = check_device(device)) return s;
+  DeviceGuard g(device);
+  oal_q19_level* L = new oal_q19_level();
+  L->device = device;
+  L->precision = precision;
+  L->nocts = nocts;
+  L->es = precision == OAL_STORE_F64 ? 8 : 4;
+  L->walls = true;
+  L->ncut = d->ncut;
+  L->nlinks = d->nlinks;
+  L->ntri = std::max(d->ntri, 1);
+  for (int f = 0; f < 6; ++f) L->faces[f] = d->faces[f];
+  L->n_plain = (int32_t)plain.size();
+  L->n_walls = (int32_t)walls.size();
+  std::vector<uint8_t> face(ns, 0);
+  if (d->face) std::memcpy(face.data(), d->face, ns);
+  std::vector<float> qdir((size_t)std::max(d->ncut, 1) * Q, 0.5f);
+  std::vector<uint8_t> okdir((size_t)std::max(d->ncut, 1) * Q, 0);
+  std::vector<int32_t> tri_off(L->ntri + 1, 0), tri_links;
+  if (d->ncut > 0) {
+    for (int c = 0; c < d->ncut; ++c)
+      for (int li = d->cut_off[c] - 1; li < d->cut_off[c + 1] - 1; ++li) {
+        qdir[(size_t)c * Q + d->cut_dir[li] - 1] = d->cut_q[li];
+        okdir[(size_t)c * Q + d->cut_dir[li] - 1] = d->cut_partner[li] != 0;
+      }
+    // links by triangle bin (no triangle -> bin 1), ascending link order within a bin
+    std::vector<int32_t> bin(d->nlinks);
+    for (int li = 0; li < d->nlinks; ++li) {
+      const int t = d->cut_tri ? d->cut_tri[li] : 0;
+      bin[li] = (t > 0 ? t : 1) - 1;
+      ++tri_off[bin[li] + 1];
+    }
+    for (int t = 0; t < L->ntri; ++t) tri_off[t + 1] += tri_off[t];
+    tri_links.resize(d->nlinks);
+    std::vector<int32_t> fillp(tri_off.begin(), tri_off.end() - 1);
+    for (int li = 0; li < d->nlinks; ++li) tri_links[fillp[bin[li]]++] = li;
+  }
+  oal_status s = alloc_state(L);
+  if (s == OAL_OK) {
+    cudaError_t e = upload(&L->onbr, d->onbr, (size_t)27 * nocts);
+    if (e == cudaSuccess) e = upload(&L->kind, kind.data(), ns);
+    if (e == cudaSuccess) e = upload(&L->face, face.data(), ns);
+    if (e == cudaSuccess) e = upload(&L->special, special.data(), ns);
+    if (e == cudaSuccess) e = upload(&L->cutidx, cutidx.data(), ns);
+    if (e == cudaSuccess) e = upload(&L->qdir, qdir.data(), qdir.size());
+    if (e == cudaSuccess) e = upload(&L->okdir, okdir.data(), okdir.size());
+    if (e == cudaSuccess && d->ncut > 0) e = upload(&L->cut_off, d->cut_off, (size_t)d->ncut + 1);
+    if (e == cudaSuccess && d->nlinks > 0) e = upload(&L->cut_dir, d->cut_dir, (size_t)d->nlinks);
+    if (e == cudaSuccess && d->nlinks > 0) e = cudaMalloc(&L->mom, sizeof(double) * d->nlinks);
+    if (e == cudaSuccess) e = upload(&L->tri_off, tri_off.data(), tri_off.size());
+    if (e == cudaSuccess && !tri_links.empty()) e = upload(&L->tri_links, tri_links.data(), tri_links.size());
+    if (e == cudaSuccess) e = cudaMalloc(&L->tri_force, sizeof(double) * (3 * (size_t)L->ntri + 3));
+    if (e == cudaSuccess) e = cudaMemset(L->tri_force, 0, sizeof(double) * (3 * (size_t)L->ntri + 3));
+    if (e == cudaSuccess) e = upload(&L->work_plain, plain.data(), plain.size());
+    if (e == cudaSuccess) e = upload(&L->work_walls, walls.data(), walls.size());
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      s = fail(e == cudaErrorMemoryAllocation ? OAL_E_OUT_OF_MEMORY : OAL_E_CUDA, "level tables: %s", cudaGetErrorString(e));
+    }
+  }
+  if (s != OAL_OK) {
+    oal_q19_level_destroy(L);
+    return s;
   }
   *out = L;
   return OAL_OK;
@@ -690,6 +1211,9 @@ oal_status oal_q19_level_destroy(oal_q19_level* L) {
       cudaFree(L->rho[b]);
     }
     cudaFree(L->part);
+    void* tabs[] = {L->kind, L->face, L->special, L->cutidx, L->qdir, L->okdir, L->cut_off, L->cut_dir, L->mom,
+                    L->tri_off, L->tri_links, L->tri_force, L->work_plain, L->work_walls};
+    for (void* t : tabs) cudaFree(t);
   }
   delete L;
   return OAL_OK;
@@ -710,13 +1234,13 @@ oal_status oal_q19_level_initialise(oal_q19_level* L, const oal_q19_params* p, c
   if (e == cudaSuccess) {
     const unsigned grid = (unsigned)((ns + 255) / 256);
     if (L->precision == OAL_STORE_F64) {
-      k_q19_initialise<double><<<grid, 256>>>((int64_t)ns, (const double*)d_rho, (const double*)d_u, (const double*)d_du,
-                                              p->nu, (double*)L->f[0], (double*)L->f[1], (double*)L->u[0],
-                                              (double*)L->u[1], (double*)L->rho[0], (double*)L->rho[1]);
+      k_q19_initialise<double><<<grid, 256>>>((int64_t)ns, L->kind, (const double*)d_rho, (const double*)d_u,
+                                              (const double*)d_du, p->nu, (double*)L->f[0], (double*)L->f[1],
+                                              (double*)L->u[0], (double*)L->u[1], (double*)L->rho[0], (double*)L->rho[1]);
     } else {
-      k_q19_initialise<float><<<grid, 256>>>((int64_t)ns, (const float*)d_rho, (const float*)d_u, (const float*)d_du,
-                                             (float)p->nu, (float*)L->f[0], (float*)L->f[1], (float*)L->u[0], (float*)L->u[1],
-                                             (float*)L->rho[0], (float*)L->rho[1]);
+      k_q19_initialise<float><<<grid, 256>>>((int64_t)ns, L->kind, (const float*)d_rho, (const float*)d_u,
+                                             (const float*)d_du, (float)p->nu, (float*)L->f[0], (float*)L->f[1],
+                                             (float*)L->u[0], (float*)L->u[1], (float*)L->rho[0], (float*)L->rho[1]);
     }
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
@@ -730,16 +1254,34 @@ oal_status oal_q19_level_initialise(oal_q19_level* L, const oal_q19_params* p, c
   }
   L->cur = 0;
   L->steps = 0;
+  L->forces_valid = false;
   return OAL_OK;
 }
 
-oal_status oal_q19_level_advance(oal_q19_level* L, const oal_q19_params* p, int32_t n_steps, void* stream) {
+oal_status oal_q19_level_advance(oal_q19_level* L, const oal_q19_params* p, int32_t n_steps, int32_t collect_forces,
+                                 void* stream) {
   if (!L) return fail(OAL_E_INVALID_ARG, "null level");
   if (oal_status s = check_params(p)) return s;
   if (n_steps < 0) return fail(OAL_E_INVALID_ARG, "n_steps < 0");
   DeviceGuard g(L->device);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  return L->precision == OAL_STORE_F64 ? advance_t<double>(L, p, n_steps, st) : advance_t<float>(L, p, n_steps, st);
+  const bool collect = collect_forces != 0;
+  return L->precision == OAL_STORE_F64 ? advance_t<double>(L, p, n_steps, collect, st)
+                                       : advance_t<float>(L, p, n_steps, collect, st);
+}
+
+oal_status oal_q19_level_forces(oal_q19_level* L, double* total, double* per_triangle) {
+  if (!L) return fail(OAL_E_INVALID_ARG, "null level");
+  DeviceGuard g(L->device);
+  if (!L->walls || !L->forces_valid) {
+    if (total) total[0] = total[1] = total[2] = 0;
+    if (per_triangle && L->walls) std::memset(per_triangle, 0, sizeof(double) * 3 * (size_t)L->ntri);
+    return OAL_OK;
+  }
+  Q19_TRY(cudaDeviceSynchronize());
+  if (total) Q19_TRY(cudaMemcpy(total, L->tri_force + 3 * (int64_t)L->ntri, 3 * sizeof(double), cudaMemcpyDeviceToHost));
+  if (per_triangle) Q19_TRY(cudaMemcpy(per_triangle, L->tri_force, 3 * sizeof(double) * L->ntri, cudaMemcpyDeviceToHost));
+  return OAL_OK;
 }
 
 oal_status oal_q19_level_get_state(oal_q19_level* L, void* f, void* u, void* rho) {
@@ -780,9 +1322,9 @@ oal_status oal_q19_level_totals(oal_q19_level* L, double* out, void* stream) {
   const int64_t ns = (int64_t)L->nocts * 8;
   const int grid = (int)std::min<int64_t>(kTotalsCtas, (ns + 255) / 256);
   if (L->precision == OAL_STORE_F64)
-    k_q19_totals<double><<<grid, 256, 0, st>>>(ns, (const double*)L->rho[L->cur], (const double*)L->u[L->cur], L->part);
+    k_q19_totals<double><<<grid, 256, 0, st>>>(ns, L->kind, (const double*)L->rho[L->cur], (const double*)L->u[L->cur], L->part);
   else
-    k_q19_totals<float><<<grid, 256, 0, st>>>(ns, (const float*)L->rho[L->cur], (const float*)L->u[L->cur], L->part);
+    k_q19_totals<float><<<grid, 256, 0, st>>>(ns, L->kind, (const float*)L->rho[L->cur], (const float*)L->u[L->cur], L->part);
   k_q19_totals_final<<<1, 32, 0, st>>>(L->part, grid, L->part + 5 * kTotalsCtas);
   Q19_TRY(cudaGetLastError());
   Q19_TRY(cudaMemcpyAsync(out, L->part + 5 * kTotalsCtas, 5 * sizeof(double), cudaMemcpyDeviceToHost, st));

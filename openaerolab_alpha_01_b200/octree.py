@@ -16,7 +16,8 @@ Mirrors (OpenAeroLab src/octree_q19, Julia):
 The step runs in liboal (include/oal.h, oal_q19_*); `init` is evaluated on the host as in the
 reference. `init(x, y, z)` takes arrays of slot centres (metres) and returns (rho, ux, uy, uz)
 arrays (numpy broadcasting: the reference's per-point function written with numpy functions).
-Levels with domain faces, bodies or refinement are refused by the library (OAL_E_UNSUPPORTED).
+A level with domain faces and a body comes from `generate(tri, MeshSpec(...))` (one level, the
+reference's generator restated natively); refined meshes are refused (OAL_E_UNSUPPORTED).
 """
 from __future__ import annotations
 
@@ -63,6 +64,126 @@ class PeriodicBox:
 
 
 @dataclass
+class MeshSpec:
+    """MeshSpec of the reference (generator.jl:21-36) for a single level: the domain in metres, the
+    periodic axes, the cell size and the condition of each domain face (-x +x -y +y -z +z)."""
+    domain: tuple
+    periodic: tuple = (False, False, False)
+    levels: int = 1
+    dx_finest: float = 1.0
+    band_fine: int = 8
+    faces: tuple = ("inlet", "outlet", "slip", "slip", "slip", "slip")
+
+    def native(self) -> capi.Q19MeshSpec:
+        if self.levels != 1:
+            raise capi.OALError(capi.OAL_E_UNSUPPORTED, "refined octree meshes (levels > 1) are not built")
+        s = capi.Q19MeshSpec()
+        check(lib().oal_q19_default_mesh_spec(C.byref(s)))
+        for a in range(3):
+            s.domain[a] = float(self.domain[a])
+            s.periodic[a] = int(bool(self.periodic[a]))
+        s.dx = float(self.dx_finest)
+        s.band_fine = int(self.band_fine)
+        for f in range(6):
+            s.faces[f] = capi.Q19_FACE_NAMES[self.faces[f]]
+        return s
+
+
+_DESC_ARRAYS = [("origin", np.int32, (3,)), ("real", np.uint8, ()), ("onbr", np.int32, (27,)),
+                ("kind", np.uint8, (8,)), ("face", np.uint8, (8,)), ("special", np.uint32, (8,)),
+                ("cutidx", np.int32, (8,))]
+_CUT_ARRAYS = [("cut_dir", np.uint8), ("cut_q", np.float32), ("cut_tri", np.int32), ("cut_partner", np.uint8)]
+COUNT_NAMES = ("octs", "n0", "n1", "n2", "fluid_total", "solid", "boundary", "wall_cells", "cut_links",
+               "leak_cells", "missing_partner_links", "unreached_triangles", "special_slots", "real_octs",
+               "triangles_with_periodic_copies")
+
+
+class Mesh:
+    """One octree level with domain faces and a body: the reference's OctLevel arrays as numpy arrays
+    in its memory order (C-order shapes: kind (nocts, 8) is Julia's (8, nocts))."""
+
+    def __init__(self, arrays: dict, n, dx, faces, ntri, counts=None):
+        self.__dict__.update(arrays)
+        self.nocts = int(self.onbr.shape[0])
+        self.n = tuple(int(v) for v in n)
+        self.dx = float(dx)
+        self.faces = tuple(int(f) for f in faces)
+        self.ntri = int(ntri)
+        self.counts = counts or {}
+
+    slot_cells = PeriodicBox.slot_cells
+    slot_centres = PeriodicBox.slot_centres
+
+    @classmethod
+    def from_native(cls, handle) -> "Mesh":
+        d = capi.Q19LevelDesc()
+        check(lib().oal_q19_mesh_level_desc(handle, C.byref(d)))
+        cnt = (C.c_int64 * 16)()
+        check(lib().oal_q19_mesh_counts(handle, cnt))
+        no = d.nocts
+        arrays = {}
+        for name, dt, shape in _DESC_ARRAYS:
+            n = no * int(np.prod(shape))
+            buf = (C.c_char * (n * np.dtype(dt).itemsize)).from_address(getattr(d, name))
+            arrays[name] = np.frombuffer(buf, dt).reshape((no,) + shape).copy()
+        def view(ptr, n, dt):
+            if not n or not ptr:
+                return np.zeros(n if ptr else 0, dt)
+            return np.frombuffer((C.c_char * (n * np.dtype(dt).itemsize)).from_address(ptr), dt).copy()
+
+        for name, dt in _CUT_ARRAYS:
+            arrays[name] = view(getattr(d, name), d.nlinks, dt)
+        arrays["cut_slot"] = view(d.cut_slot, d.ncut, np.int32)
+        arrays["cut_off"] = view(d.cut_off, d.ncut + 1, np.int32)
+        if arrays["cut_off"].size == 0:
+            arrays["cut_off"] = np.ones(1, np.int32)
+        counts = {k: int(v) for k, v in zip(COUNT_NAMES, cnt[:len(COUNT_NAMES)])}
+        return cls(arrays, (counts["n0"], counts["n1"], counts["n2"]), 0.0, list(d.faces), d.ntri, counts)
+
+    def desc(self) -> capi.Q19LevelDesc:
+        """A level descriptor pointing at this mesh's arrays (valid while the mesh lives)."""
+        d = capi.Q19LevelDesc()
+        d.nocts = self.nocts
+        for name, _, _ in _DESC_ARRAYS:
+            setattr(d, name, getattr(self, name).ctypes.data)
+        d.ncut = int(self.cut_slot.shape[0])
+        d.nlinks = int(self.cut_dir.shape[0])
+        for name in ("cut_slot", "cut_off", "cut_dir", "cut_q", "cut_tri", "cut_partner"):
+            a = getattr(self, name)
+            setattr(d, name, a.ctypes.data if a.size else None)
+        d.ntri = self.ntri
+        for f in range(6):
+            d.faces[f] = self.faces[f]
+        return d
+
+
+def generate(tri, spec: MeshSpec) -> Mesh:
+    """The reference's generate(tri, spec) for one level: triangles (ntri, 3, 3) in metres."""
+    t = np.ascontiguousarray(np.asarray(tri, np.float64).reshape(-1, 3, 3))
+    h = C.c_void_p()
+    check(lib().oal_q19_mesh_generate(t.ctypes.data_as(C.c_void_p) if t.size else None, t.shape[0],
+                                      C.byref(spec.native()), C.byref(h)))
+    try:
+        m = Mesh.from_native(h)
+    finally:
+        lib().oal_q19_mesh_destroy(h)
+    m.dx = float(spec.dx_finest)
+    m.domain = tuple(v * m.dx for v in m.n)
+    return m
+
+
+def box_triangles(lo, hi) -> np.ndarray:
+    """A closed box of 12 outward-facing triangles (the reference tests' box_tris)."""
+    v = np.array([(x, y, z) for z in (lo[2], hi[2]) for y in (lo[1], hi[1]) for x in (lo[0], hi[0])], np.float64)
+    faces = ((0, 2, 6, 4), (1, 5, 7, 3), (0, 4, 5, 1), (2, 3, 7, 6), (0, 1, 3, 2), (4, 6, 7, 5))
+    tri = []
+    for f in faces:
+        tri.append((v[f[0]], v[f[1]], v[f[2]]))
+        tri.append((v[f[0]], v[f[2]], v[f[3]]))
+    return np.array(tri)
+
+
+@dataclass
 class CaseConfig:
     nu_lattice: float = 0.01
     u_lattice: float = 0.08
@@ -89,6 +210,8 @@ class CaseConfig:
         p = capi.Q19Params()
         check(lib().oal_q19_default_params(C.byref(p)))
         p.nu = self.level_nu()
+        p.u_inlet[0] = self.u_lattice          # st.u_inlet * inlet_dir, inlet along +x (state.jl:255)
+        p.force_scale = 1.0
         p.sgs = SGS_CODES[self.sgs]
         p.c_wale = self.c_wale
         p.c_smagorinsky = self.c_smagorinsky
@@ -98,7 +221,7 @@ class CaseConfig:
         return p
 
 
-def test_case_config(box: PeriodicBox, nu_lattice: float = 0.01, u_lattice: float = 0.08, velocity: float = 1.0,
+def test_case_config(box, nu_lattice: float = 0.01, u_lattice: float = 0.08, velocity: float = 1.0,
                      hrr_sigma: float = 1.0, sgs: str = "none", precision=np.float32,
                      body_force=(0.0, 0.0, 0.0)) -> CaseConfig:
     return CaseConfig(nu_lattice=nu_lattice, u_lattice=u_lattice, velocity=velocity, hrr_sigma=hrr_sigma, sgs=sgs,
@@ -121,8 +244,13 @@ class State:
         self.step = 0
         self.mass0 = float("nan")
         h = C.c_void_p()
-        check(lib().oal_q19_level_create(device, _PRECISION[self.dtype], mesh.nocts, _ptr(mesh.onbr), C.byref(h)))
+        if isinstance(mesh, Mesh):
+            self._desc = mesh.desc()
+            check(lib().oal_q19_level_create_desc(device, _PRECISION[self.dtype], C.byref(self._desc), C.byref(h)))
+        else:
+            check(lib().oal_q19_level_create(device, _PRECISION[self.dtype], mesh.nocts, _ptr(mesh.onbr), C.byref(h)))
         self._h = h
+        self.forces = np.zeros(3)
 
     # -- lifetime
     def close(self):
@@ -179,11 +307,23 @@ class State:
         return self
 
     # -- stepping
-    def advance(self, n: int = 1, stream=None):
+    def advance(self, n: int = 1, stream=None, collect: bool = False):
+        """n steps (advance! n times); with `collect` the last step's momentum exchange is kept in
+        `forces` (lattice units, FP64)."""
         st = None if stream is None else C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else stream)
-        check(lib().oal_q19_level_advance(self._h, C.byref(self.params), int(n), st))
+        check(lib().oal_q19_level_advance(self._h, C.byref(self.params), int(n), int(bool(collect)), st))
         self.step += n
+        if collect and n > 0:
+            out = (C.c_double * 3)()
+            check(lib().oal_q19_level_forces(self._h, out, None))
+            self.forces = np.array(out[:])
         return self
+
+    def forces_per_triangle(self) -> np.ndarray:
+        ntri = max(getattr(self.mesh, "ntri", 0), 1)
+        out = np.zeros((ntri, 3))
+        check(lib().oal_q19_level_forces(self._h, None, out.ctypes.data_as(C.c_void_p)))
+        return out
 
     # -- read-out
     def state(self):
@@ -238,3 +378,61 @@ def collide_cells(f, omega, sigma, pfd, F):
                                       u.data_ptr(), C.c_void_p(stream)))
     torch.cuda.current_stream(f.device).synchronize()
     return out, rho, u
+
+
+def level_bytes_per_cell(dtype, sgs: str = "wale", hrr_sigma: float = 0.98) -> int:
+    """Algorithmic HBM bytes of one cell update: the 19 populations read and written, the velocity and
+    density written, and, when the velocity gradient is used (SGS or HRR), the previous velocity read
+    (and the previous density for HRR)."""
+    es = np.dtype(dtype).itemsize
+    grad = sgs != "none" or hrr_sigma != 1.0
+    return es * (2 * 19 + 3 + 1 + ((3 + (1 if hrr_sigma != 1.0 else 0)) if grad else 0))
+
+
+def benchmark_periodic_box(n: int = 256, steps: int = 100, warmup: int = 10, precision=np.float32,
+                           sgs: str = "wale", hrr_sigma: float = 0.98, nu_lattice: float = 0.001):
+    """Time `steps` level steps of an n^3 periodic box (a Taylor-Green start) with CUDA events on the
+    launching stream. Returns a dict (MLUPS, ms per step, algorithmic GB/s)."""
+    import math
+    import torch
+    box = PeriodicBox(n)
+    st = State(box, test_case_config(box, nu_lattice=nu_lattice, precision=precision, sgs=sgs, hrr_sigma=hrr_sigma))
+    k = 2 * math.pi / n
+    st.initialise(lambda x, y, z: (1.0, 0.05 * np.sin(k * x) * np.cos(k * y), -0.05 * np.cos(k * x) * np.sin(k * y),
+                                   0.0 * x))
+    s = torch.cuda.Stream()
+    st.advance(warmup, s)
+    s.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    st.advance(steps, s)
+    e1.record(s)
+    s.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    cells = n ** 3
+    ke = st.kinetic_energy()
+    st.close()
+    bpc = level_bytes_per_cell(precision, sgs, hrr_sigma)
+    return {"workload": f"q19_periodic_{n}^3_{np.dtype(precision).name}_{sgs}_sigma{hrr_sigma:g}", "cells": cells,
+            "steps": steps, "ms_per_step": round(ms, 4), "mlups": round(cells / ms / 1e3, 1),
+            "bytes_per_cell": bpc, "achieved_gbs": round(cells * bpc / ms / 1e6, 1), "kinetic_energy": ke,
+            "gpu_launches": steps}
+
+
+def main():
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="Time the D3Q19 octree step on an n^3 periodic box")
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
+    ap.add_argument("--sgs", default="wale", choices=list(SGS_CODES))
+    ap.add_argument("--sigma", type=float, default=0.98)
+    a = ap.parse_args()
+    dt = np.float32 if a.precision == "f32" else np.float64
+    print(json.dumps(benchmark_periodic_box(a.n, a.steps, a.warmup, dt, a.sgs, a.sigma)))
+
+
+if __name__ == "__main__":
+    main()

@@ -54,7 +54,9 @@ def lib() -> C.CDLL:
         L.ora_q19_reference_collide_f64.argtypes = [i64, vp, vp, C.c_double, vp, vp, vp]
         for suf in ("f32", "f64"):
             getattr(L, f"ora_q19_step_{suf}").argtypes = [i32, vp, vp, vp, vp, vp, vp, vp, vp]
-            getattr(L, f"ora_q19_initialise_{suf}").argtypes = [i64, vp, vp, vp, C.c_double, vp]
+            getattr(L, f"ora_q19_step_walls_{suf}").argtypes = [vp] * 9
+            getattr(L, f"ora_q19_initialise_{suf}").argtypes = [i64, vp, vp, vp, vp, C.c_double, vp, vp, vp]
+        L.ora_q19_forces.argtypes = [vp, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -179,13 +181,21 @@ def q19_collide(f, omega, sigma, pfd, F, reference=False):
 
 
 class OracleQ19Level:
-    """One periodic octree level stepped by the CPU restatement; arrays in the reference's layout
-    (numpy C-order shapes: f (nocts, 19, 8), u (nocts, 3, 8), rho (nocts, 8))."""
+    """One octree level stepped by the CPU restatement; arrays in the reference's layout (numpy
+    C-order shapes: f (nocts, 19, 8), u (nocts, 3, 8), rho (nocts, 8)). `desc` (a level descriptor
+    with its arrays kept alive by the caller) selects the step with domain faces and cut links."""
 
-    def __init__(self, onbr, dtype=np.float32):
+    def __init__(self, onbr, dtype=np.float32, desc=None):
         self.onbr = np.ascontiguousarray(onbr, np.int32)
         self.nocts = self.onbr.shape[0]
         self.dtype = np.dtype(dtype)
+        self.desc = desc
+        self.kind = None
+        if desc is not None and desc.kind:
+            self.kind = np.ctypeslib.as_array((C.c_uint8 * (8 * self.nocts)).from_address(desc.kind)).copy()
+        self.mom = np.zeros(max(desc.nlinks, 1) if desc is not None else 1)
+        self.forces = np.zeros(3)
+        self.per_tri = None
         no = self.nocts
         self.f = np.zeros((no, 19, 8), self.dtype)
         self.g = np.zeros_like(self.f)
@@ -198,19 +208,27 @@ class OracleQ19Level:
         rho = np.ascontiguousarray(rho, self.dtype)
         u = np.ascontiguousarray(u, self.dtype)
         du = None if du is None else np.ascontiguousarray(du, self.dtype)
-        getattr(lib(), f"ora_q19_initialise_{_suffix(self.dtype)}")(self.nocts * 8, _p(rho), _p(u), _p(du),
-                                                                    float(params.nu), _p(self.f))
+        getattr(lib(), f"ora_q19_initialise_{_suffix(self.dtype)}")(self.nocts * 8, _p(self.kind), _p(rho), _p(u),
+                                                                    _p(du), float(params.nu), _p(self.f), _p(self.u),
+                                                                    _p(self.rho))
         self.g[...] = self.f
-        self.u[...] = u
-        self.v[...] = u
-        self.rho[...] = rho
-        self.rhob[...] = rho
+        self.v[...] = self.u
+        self.rhob[...] = self.rho
 
-    def step(self, params, n=1):
-        fn = getattr(lib(), f"ora_q19_step_{_suffix(self.dtype)}")
-        for _ in range(n):
-            fn(self.nocts, _p(self.onbr), C.addressof(params), _p(self.f), _p(self.g), _p(self.u), _p(self.v),
-               _p(self.rho), _p(self.rhob))
+    def step(self, params, n=1, collect=False):
+        suf = _suffix(self.dtype)
+        for s in range(n):
+            if self.desc is None:
+                getattr(lib(), f"ora_q19_step_{suf}")(self.nocts, _p(self.onbr), C.addressof(params), _p(self.f),
+                                                      _p(self.g), _p(self.u), _p(self.v), _p(self.rho), _p(self.rhob))
+            else:
+                mom = self.mom if (collect and s == n - 1) else None
+                getattr(lib(), f"ora_q19_step_walls_{suf}")(C.addressof(self.desc), C.addressof(params), _p(self.f),
+                                                            _p(self.g), _p(self.u), _p(self.v), _p(self.rho),
+                                                            _p(self.rhob), _p(mom))
+                if mom is not None:
+                    self.per_tri = np.zeros((max(self.desc.ntri, 1), 3))
+                    lib().ora_q19_forces(C.addressof(self.desc), _p(self.mom), _p(self.per_tri), _p(self.forces))
             self.f, self.g = self.g, self.f
             self.u, self.v = self.v, self.u
             self.rho, self.rhob = self.rhob, self.rho
@@ -219,5 +237,9 @@ class OracleQ19Level:
     def totals(self):
         r = self.rho.astype(np.float64)
         u = self.u.astype(np.float64)
+        if self.kind is not None:
+            fl = (self.kind.reshape(self.nocts, 8) == 1)
+            r = r * fl
+            u = u * fl[:, None, :]
         return np.array([r.sum(), (r * u[:, 0]).sum(), (r * u[:, 1]).sum(), (r * u[:, 2]).sum(),
                          0.5 * (r * (u ** 2).sum(1)).sum()])

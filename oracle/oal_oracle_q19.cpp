@@ -18,6 +18,10 @@
 //   totals ......................... src/octree_q19/src/state.jl:333-356
 //   per-direction reference collision (the known-answer test's definition)
 //                                    tools/tests/q19_kernel.jl:20-44
+//   face conditions ................ src/octree_q19/src/stream.jl:32-78
+//   arriving populations, Bouzidi,
+//   momentum exchange .............. src/octree_q19/src/stream.jl:205-257
+//   cut-direction tables ........... src/octree_q19/src/state.jl:135-142
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -389,14 +393,24 @@ void rebuild(T rho, T ux, T uy, T uz, const T* p, T omega, T* out) {
 // (8, 9, nocts) with du[k, 3a+b, o] = d u_b / d x_a over one cell) rebuilt at the level's omega,
 // or the equilibrium (du null). rho (8, nocts), u (8, 3, nocts), f (8, 19, nocts).
 template <class T>
-void initialise(int64_t nslots, const T* rho_a, const T* u, const T* du, double nu_d, T* f) {
+void initialise(int64_t nslots, const uint8_t* kind, const T* rho_a, const T* u, const T* du, double nu_d, T* f,
+                T* u_out, T* rho_out) {
   const T nu = T(nu_d);
   const T omega = omega_of<T>(nu), tau = T(1) / omega;
 #pragma omp parallel for schedule(static)
   for (int64_t s = 0; s < nslots; ++s) {
     const int64_t o = s / 8;
     const int k = (int)(s % 8);
+    if (kind && kind[s] != 1) {
+      // slots without a state keep the allocation state (state.jl:217-232)
+      for (int i = 0; i < Q; ++i) f[k + 8 * i + 152 * o] = T(0);
+      for (int a = 0; a < 3; ++a) u_out[k + 8 * a + 24 * o] = T(0);
+      rho_out[s] = T(1);
+      continue;
+    }
     const T rho = rho_a[s], ux = u[k + 24 * o], uy = u[k + 8 + 24 * o], uz = u[k + 16 + 24 * o];
+    for (int a = 0; a < 3; ++a) u_out[k + 8 * a + 24 * o] = u[k + 8 * a + 24 * o];
+    rho_out[s] = rho;
     T out[Q];
     if (du) {
       T d[9];
@@ -411,9 +425,189 @@ void initialise(int64_t nslots, const T* rho_a, const T* u, const T* du, double 
   }
 }
 
+// ---- a level with domain faces and cut links (stream.jl:32-78, 205-257, 280-370) ----------------
+
+inline int dir_index(int x, int y, int z) {
+  for (int i = 0; i < Q; ++i)
+    if (CX[i] == x && CY[i] == y && CZ[i] == z) return i;
+  return -1;
+}
+inline int opp_of(int i) { return dir_index(-CX[i], -CY[i], -CZ[i]); }
+inline int mirror_of(int i, int axis) {
+  return dir_index(axis == 0 ? -CX[i] : CX[i], axis == 1 ? -CY[i] : CY[i], axis == 2 ? -CZ[i] : CZ[i]);
+}
+
+// stream.jl:32-47 (face conditions: OAL_Q19_FACE_*)
+template <class T>
+T face_dirichlet(int cond, int j, const T* fo, T rho, T ux, T uy, T uz, const T* uin) {
+  const int i = opp_of(j);
+  const T usq = ux * ux + uy * uy + uz * uz;
+  if (cond == OAL_Q19_FACE_INLET) {
+    const T vsq = uin[0] * uin[0] + uin[1] * uin[1] + uin[2] * uin[2];
+    return feq_shifted<T>(j, rho, uin[0], uin[1], uin[2], vsq) + (fo[i] - feq_shifted<T>(i, rho, ux, uy, uz, usq));
+  } else if (cond == OAL_Q19_FACE_OUTLET) {
+    return feq_shifted<T>(j, T(1), ux, uy, uz, usq) + (fo[i] - feq_shifted<T>(i, rho, ux, uy, uz, usq));
+  }
+  const T vsq = uin[0] * uin[0] + uin[1] * uin[1] + uin[2] * uin[2];
+  return feq_shifted<T>(j, T(1), uin[0], uin[1], uin[2], vsq) + (fo[i] - feq_shifted<T>(i, rho, ux, uy, uz, usq));
+}
+
+// stream.jl:49-78
+template <class T>
+T face_population(uint8_t mask, const int32_t* faces, int j, const T* fo, T rho, T ux, T uy, T uz, const T* uin) {
+  const int i = opp_of(j);
+  if (__builtin_popcount(mask) == 1) {
+    const int f = __builtin_ctz(mask);
+    const int cond = faces[f];
+    if (cond == OAL_Q19_FACE_NOSLIP || cond == OAL_Q19_FACE_GROUND) return fo[i];
+    if (cond == OAL_Q19_FACE_SLIP || cond == OAL_Q19_FACE_SYMMETRY) return fo[mirror_of(j, f <= 1 ? 0 : f <= 3 ? 1 : 2)];
+    return face_dirichlet<T>(cond, j, fo, rho, ux, uy, uz, uin);
+  }
+  bool wall = false, open = false;
+  for (int f = 0; f < 6; ++f) {
+    if (!((mask >> f) & 1)) continue;
+    const int c = faces[f];
+    if (c == OAL_Q19_FACE_NOSLIP || c == OAL_Q19_FACE_GROUND) wall = true;
+    if (c == OAL_Q19_FACE_INLET || c == OAL_Q19_FACE_OUTLET || c == OAL_Q19_FACE_FREESTREAM) open = true;
+  }
+  if (wall) return fo[i];
+  if (open) return face_dirichlet<T>(OAL_Q19_FACE_FREESTREAM, j, fo, rho, ux, uy, uz, uin);
+  int m = j;
+  if (mask & 0x03) m = mirror_of(m, 0);
+  if (mask & 0x0c) m = mirror_of(m, 1);
+  if (mask & 0x30) m = mirror_of(m, 2);
+  return fo[m];
+}
+
+template <class T>
+void step_level_walls(const oal_q19_level_desc& d, const oal_q19_params& P, const T* fin, T* fout, const T* uin,
+                      T* vout, const T* rho_a, T* rhob, double* mom) {
+  const T nu = T(P.nu), cw = T(P.c_wale), cs = T(P.c_smagorinsky), cv = T(2.5 * P.c_smagorinsky * P.c_smagorinsky);
+  const T sigma = T(P.hrr_sigma);
+  const T F[3] = {T(P.body_force[0]), T(P.body_force[1]), T(P.body_force[2])};
+  const T uinlet[3] = {T(P.u_inlet[0]), T(P.u_inlet[1]), T(P.u_inlet[2])};
+  const bool need_gradient = P.sgs != 0 || sigma != T(1);
+  const T omega0 = omega_of<T>(nu);
+  const int64_t nslots = (int64_t)d.nocts * 8;
+  // cut_direction_tables (state.jl:135-142): q per direction of each cut cell (0.5 elsewhere), partner flag
+  std::vector<float> qdir((size_t)std::max(d.ncut, 1) * Q, 0.5f);
+  std::vector<uint8_t> okdir((size_t)std::max(d.ncut, 1) * Q, 0);
+  for (int c = 0; c < d.ncut; ++c)
+    for (int li = d.cut_off[c] - 1; li < d.cut_off[c + 1] - 1; ++li) {
+      qdir[(size_t)c * Q + d.cut_dir[li] - 1] = d.cut_q[li];
+      okdir[(size_t)c * Q + d.cut_dir[li] - 1] = d.cut_partner[li];
+    }
+  auto kind = [&](int64_t s) -> uint8_t { return d.kind ? d.kind[s] : 1; };
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int o = 0; o < d.nocts; ++o) {
+    if (d.real && !d.real[o]) continue;
+    for (int k = 0; k < 8; ++k) {
+      const int64_t s = 8 * (int64_t)o + k;
+      if (kind(s) != 1) continue;
+      const uint32_t sp = d.special ? d.special[s] : 0u;
+      T f[Q];
+      if (sp == 0) {
+        for (int j = 0; j < Q; ++j) {
+          int off, child;
+          source(k, j, off, child);
+          f[j] = fin[child + 8 * j + 152 * (int64_t)(d.onbr[off + 27 * (int64_t)o] - 1)];
+        }
+      } else {
+        // stream.jl:205-246: the own post-collision populations and the previous macros
+        T fo[Q];
+        for (int j = 0; j < Q; ++j) fo[j] = fin[k + 8 * j + 152 * (int64_t)o];
+        const T rho0 = rho_a[s], ux0 = uin[k + 24 * (int64_t)o], uy0 = uin[k + 8 + 24 * (int64_t)o],
+                uz0 = uin[k + 16 + 24 * (int64_t)o];
+        const int ci = d.cutidx ? d.cutidx[s] : 0;
+        for (int j = 0; j < Q; ++j) {
+          int off, child;
+          source(k, j, off, child);
+          const int so = d.onbr[off + 27 * (int64_t)o];
+          if (!((sp >> j) & 1u)) {
+            f[j] = fin[child + 8 * j + 152 * (int64_t)(so - 1)];
+          } else if (so != 0 && kind(8 * (int64_t)(so - 1) + child) == 5) {
+            f[j] = face_population<T>(d.face[8 * (int64_t)(so - 1) + child], d.faces, j, fo, rho0, ux0, uy0, uz0, uinlet);
+          } else {
+            const int i = opp_of(j);
+            const T q = T(qdir[(size_t)(ci - 1) * Q + i]);
+            const bool ok = okdir[(size_t)(ci - 1) * Q + i] != 0;
+            if (!ok) {
+              f[j] = fo[i];
+            } else if (q < T(0.5)) {
+              int pi_, pk_;
+              neighbour_slot(k, -CX[i], -CY[i], -CZ[i], pi_, pk_);
+              const int po = d.onbr[pi_ + 27 * (int64_t)o];
+              f[j] = T(2) * q * fo[i] + (T(1) - T(2) * q) * fin[pk_ + 8 * i + 152 * (int64_t)(po - 1)];
+            } else {
+              const T inv2q = T(1) / (T(2) * q);
+              f[j] = inv2q * fo[i] + (T(1) - inv2q) * fo[j];
+            }
+          }
+        }
+        if (mom && ci != 0) {
+          // momentum exchange per cut link: scale (f_i* + f_j(t+1)), i toward the wall (stream.jl:248-256)
+          for (int li = d.cut_off[ci - 1] - 1; li < d.cut_off[ci] - 1; ++li) {
+            const int i = d.cut_dir[li] - 1, j = opp_of(i);
+            mom[li] = P.force_scale * (double)(fo[i] + f[j]);
+          }
+        }
+      }
+      // gradient of the previous velocity: missing or boundary neighbours give the own value (stream.jl:13-30)
+      T g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      if (need_gradient) {
+        auto at = [&](int ex, int ey, int ez, T* v) {
+          int ni, nk;
+          neighbour_slot(k, ex, ey, ez, ni, nk);
+          const int no = d.onbr[ni + 27 * (int64_t)o];
+          if (no == 0 || kind(8 * (int64_t)(no - 1) + nk) == 5) {
+            for (int a = 0; a < 3; ++a) v[a] = uin[k + 8 * a + 24 * (int64_t)o];
+            return;
+          }
+          for (int a = 0; a < 3; ++a) v[a] = uin[nk + 8 * a + 24 * (int64_t)(no - 1)];
+        };
+        T xp[3], xm[3], yp[3], ym[3], zp[3], zm[3];
+        at(1, 0, 0, xp); at(-1, 0, 0, xm); at(0, 1, 0, yp); at(0, -1, 0, ym); at(0, 0, 1, zp); at(0, 0, -1, zm);
+        const T h = T(0.5);
+        g[0] = h * (xp[0] - xm[0]); g[1] = h * (xp[1] - xm[1]); g[2] = h * (xp[2] - xm[2]);
+        g[3] = h * (yp[0] - ym[0]); g[4] = h * (yp[1] - ym[1]); g[5] = h * (yp[2] - ym[2]);
+        g[6] = h * (zp[0] - zm[0]); g[7] = h * (zp[1] - zm[1]); g[8] = h * (zp[2] - zm[2]);
+      }
+      const T nut = P.sgs == 1 ? nu_wale<T>(g, cw) : P.sgs == 2 ? nu_smagorinsky<T>(g, cs) : P.sgs == 3 ? nu_vreman<T>(g, cv) : T(0);
+      const T omega = need_gradient ? omega_of<T>(nu + nut) : omega0;
+      T pfd[6] = {0, 0, 0, 0, 0, 0};
+      if (sigma != T(1)) pi_fd_from_gradient<T>(g, rho_a[s], T(1) / omega, pfd);
+      T out[Q], rho, ux, uy, uz;
+      collide_rr<T>(f, omega, sigma, pfd, F, out, rho, ux, uy, uz);
+      for (int i = 0; i < Q; ++i) fout[k + 8 * i + 152 * (int64_t)o] = out[i];
+      vout[k + 24 * (int64_t)o] = ux;
+      vout[k + 8 + 24 * (int64_t)o] = uy;
+      vout[k + 16 + 24 * (int64_t)o] = uz;
+      rhob[s] = rho;
+    }
+  }
+  (void)nslots;
+}
+
 }  // namespace
 
 extern "C" {
+
+// per-triangle force in link order (no triangle -> bin 1) and the total as a plain sum over the bins
+void ora_q19_forces(const oal_q19_level_desc* d, const double* mom, double* per_tri, double* total) {
+  const int ntri = std::max(d->ntri, 1);
+  for (int t = 0; t < 3 * ntri; ++t) per_tri[t] = 0;
+  for (int li = 0; li < d->nlinks; ++li) {
+    const int t = (d->cut_tri && d->cut_tri[li] > 0 ? d->cut_tri[li] : 1) - 1;
+    const int i = d->cut_dir[li] - 1;
+    per_tri[3 * t] += mom[li] * CX[i];
+    per_tri[3 * t + 1] += mom[li] * CY[i];
+    per_tri[3 * t + 2] += mom[li] * CZ[i];
+  }
+  total[0] = total[1] = total[2] = 0;
+  for (int t = 0; t < ntri; ++t)
+    for (int a = 0; a < 3; ++a) total[a] += per_tri[3 * t + a];
+}
+
 
 void ora_q19_tables(int32_t* cx, int32_t* cy, int32_t* cz, double* w, int32_t* src_off, int32_t* src_child) {
   for (int i = 0; i < Q; ++i) { cx[i] = CX[i]; cy[i] = CY[i]; cz[i] = CZ[i]; w[i] = WT[i]; }
@@ -465,8 +659,13 @@ int ora_q19_periodic_box(int32_t n0, int32_t n1, int32_t n2, int32_t* origin, in
     Q19Level L{nocts, onbr};                                                                                     \
     step_level<T>(L, *P, fin, fout, uin, vout, rho_a, rhob);                                                     \
   }                                                                                                              \
-  void ora_q19_initialise_##SUF(int64_t nslots, const T* rho, const T* u, const T* du, double nu, T* f) {      \
-    initialise<T>(nslots, rho, u, du, nu, f);                                                                    \
+  void ora_q19_initialise_##SUF(int64_t nslots, const uint8_t* kind, const T* rho, const T* u, const T* du,     \
+                                double nu, T* f, T* u_out, T* rho_out) {                                         \
+    initialise<T>(nslots, kind, rho, u, du, nu, f, u_out, rho_out);                                              \
+  }                                                                                                              \
+  void ora_q19_step_walls_##SUF(const oal_q19_level_desc* d, const oal_q19_params* P, const T* fin, T* fout,      \
+                                const T* uin, T* vout, const T* rho_a, T* rhob, double* mom) {                   \
+    step_level_walls<T>(*d, *P, fin, fout, uin, vout, rho_a, rhob, mom);                                         \
   }
 ORA_Q19_COLLIDE(float, f32)
 ORA_Q19_COLLIDE(double, f64)

@@ -11,7 +11,8 @@ import math
 import numpy as np
 import pytest
 
-from .test_oracle_q19 import SEED, _fields, _params, collide_each, g04_init, kat_inputs, random_states
+from .test_oracle_q19 import (SEED, _fields, _params, channel, collide_each, g04_init, kat_inputs, obstacle_box_mesh,
+                              poiseuille, random_states)
 
 pytestmark = pytest.mark.gpu
 
@@ -229,3 +230,91 @@ def test_unsupported_levels_are_refused(env):
     with pytest.raises(capi.OALError) as e:
         octree.State(box, octree.test_case_config(box))
     assert e.value.status == capi.OAL_E_UNSUPPORTED
+
+
+# ---- one level with domain faces and a body ------------------------------------------------------
+
+def _wall_pair(env, m, dt, p, init, nonequilibrium=True):
+    oracle, _, octree, _ = env
+    st = octree.State(m, octree.test_case_config(m, precision=dt))
+    st.params = p
+    rho, u, du = st.initial_fields(init, nonequilibrium)
+    st._upload(rho, u, du)
+    desc = m.desc()
+    L = oracle.OracleQ19Level(m.onbr, dt, desc=desc)
+    L._keep = (m, desc)
+    L.initialise(p, rho, u, du)
+    return st, L
+
+
+def _check_walls(st, L):
+    _check_same(st, L)
+    per_tri = st.forces_per_triangle()
+    assert same_bits(per_tri, L.per_tri), np.abs(per_tri - L.per_tri).max()
+    assert np.allclose(st.forces, L.forces, rtol=1e-12, atol=1e-15), (st.forces, L.forces)
+
+
+WALL_VARIANTS = [(0, 1.0, (1e-5, 0.0, 0.0)), (1, 0.98, (0.0, 0.0, 0.0)), (3, 0.98, (2e-5, 1e-6, 0.0))]
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+@pytest.mark.parametrize("angle", [0.0, 30.0])
+@pytest.mark.parametrize("sgs,sigma,F", WALL_VARIANTS)
+def test_walls_channel_bitwise(env, dt, angle, sgs, sigma, F):
+    """The tilted channel (slip faces, Bouzidi links with and without partners, momentum exchange):
+    GPU == oracle bit for bit, per-triangle forces included."""
+    m, c, nrm = channel(18, 3.0, angle, int(angle) + 18)
+    p = _params(nu=0.02, sgs=sgs, sigma=sigma, F=F)
+    st, L = _wall_pair(env, m, dt, p, lambda x, y, z: (1.0 + 0.01 * np.sin(y / 3.0), 0.03 + 0.01 * np.cos(z / 2.0),
+                                                       0.005 * np.sin(x), 0.004 * np.cos(y / 4.0)))
+    for _ in range(3):
+        st.advance(4, collect=True)
+        L.step(p, 4, collect=True)
+        _check_walls(st, L)
+    assert np.abs(st.forces).max() > 0
+    st.close()
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+@pytest.mark.parametrize("sgs,sigma", [(0, 1.0), (1, 0.98)])
+def test_walls_face_conditions_bitwise(env, dt, sgs, sigma):
+    """A box in a domain whose faces are inlet, outlet, no-slip, freestream, symmetry and ground
+    (single faces, edges and corners of mixed conditions): GPU == oracle bit for bit."""
+    m = obstacle_box_mesh()
+    p = _params(nu=0.01, sgs=sgs, sigma=sigma, u_inlet=(0.05, 0.0, 0.0))
+    st, L = _wall_pair(env, m, dt, p, lambda x, y, z: (1.0 + 0.002 * np.sin(x), 0.05 + 0.0 * x, 0.01 * np.sin(z / 2.0),
+                                                       0.0 * x), nonequilibrium=False)
+    for _ in range(3):
+        st.advance(3, collect=True)
+        L.step(p, 3, collect=True)
+        _check_walls(st, L)
+    st.close()
+
+
+def test_g13_poiseuille_tilted_plates(env):
+    """tools/tests/q19_octree_poiseuille.jl:77-114 (gate G1.3): Poiseuille flow between STL plates
+    tilted by 0, 15, 30 and 45 degrees, n = 18, 36, 72 (H = 3, 6, 12), FP64, five diffusion times:
+    profile error < 20 % per case, profile order >= 1.8, wall position within 0.05 cells and the
+    momentum-exchange friction within 1 % of the body force at n = 72."""
+    _, _, octree, _ = env
+
+    def run(m, nu, Fx, steps):
+        st = octree.State(m, octree.test_case_config(m, nu_lattice=nu, precision=np.float64, body_force=(Fx, 0.0, 0.0)))
+        st.initialise(lambda x, y, z: (1.0, 0.0 * x, 0.0 * x, 0.0 * x))
+        st.advance(steps - 1)
+        st.advance(1, collect=True)
+        _, u, _ = st.state()
+        f = st.forces.copy()
+        st.close()
+        return u, f
+
+    sizes = (18, 36, 72)
+    for angle in (0.0, 15.0, 30.0, 45.0):
+        res = [poiseuille(run, n, angle) for n in sizes]
+        for prof, wall, fric in res:
+            assert np.isfinite(prof) and prof < 0.2, (angle, res)
+        e = [r[0] for r in res]
+        order = math.log(e[0] / e[2]) / math.log(4)
+        assert order >= 1.8, (angle, e, order)
+        assert abs(res[-1][1]) < 0.05, (angle, res[-1])
+        assert res[-1][2] < 0.01, (angle, res[-1])
