@@ -348,7 +348,7 @@ enum { OAL_Q19_FACE_PERIODIC = 0, OAL_Q19_FACE_INLET = 1, OAL_Q19_FACE_OUTLET = 
 
 /* One level of an octree mesh, the reference's OctLevel arrays (octree.jl:50-71), all host memory,
  * 1-based indices as in the reference. Nullable: real (all real), kind (all fluid), face, special
- * and cutidx (none), the cut arrays when ncut = 0. */
+ * and cutidx (none), the cut arrays when ncut = 0, the transfer lists when their count is 0. */
 typedef struct oal_q19_level_desc {
   int32_t nocts;
   const int32_t* origin;       /* (3, nocts) level cells */
@@ -368,16 +368,42 @@ typedef struct oal_q19_level_desc {
   const uint8_t* cut_partner;  /* (nlinks) the Bouzidi partner x - c_i is a plain fluid slot */
   int32_t ntri;                /* triangles (force bins) */
   int32_t faces[6];            /* OAL_Q19_FACE_* of -x +x -y +y -z +z */
+  /* transfers between levels (generator.jl:600-790): the ghost slots of this level filled from the
+   * coarser level (64 donor slots of level-1 with weights per ghost), and the covered slots of this
+   * level restricted from the finer one (64 source slots of level+1, cubic or inner-8 average) */
+  int32_t nghost;
+  const int32_t* ghost_slot;   /* (nghost) */
+  const int32_t* ghost_donor;  /* (64, nghost) slot ids of the coarser level, 0 unused */
+  const float* ghost_w;        /* (64, nghost) */
+  int32_t nrestrict;
+  const int32_t* restrict_slot;   /* (nrestrict) */
+  const int32_t* restrict_src;    /* (64, nrestrict) slot ids of the finer level, 0 unused */
+  const uint8_t* restrict_cubic;  /* (nrestrict) */
 } oal_q19_level_desc;
 
-/* Mesh generator of one level from placed triangles (MeshSpec with levels = 1). */
+/* A refinement region of the mesh spec (generator.jl:10-16). */
+typedef struct oal_q19_region {
+  int32_t kind;                /* 0 box (lo..hi), 1 sphere (centre, radius), 2 cylinder (axis lo -> hi, radius) */
+  int32_t level;               /* refined up to this level */
+  double lo[3], hi[3], centre[3], radius;
+} oal_q19_region;
+
+/* MeshSpec (generator.jl:21-36) without per-box surface levels. */
 typedef struct oal_q19_mesh_spec {
-  double domain[3];            /* metres; periodic axes an even number of cells */
-  double dx;                   /* cell size, metres */
+  double domain[3];            /* metres; periodic axes an even number of coarse cells */
+  double dx;                   /* finest cell size, metres */
   int32_t periodic[3];
   int32_t faces[6];            /* OAL_Q19_FACE_*, PERIODIC exactly on periodic axes */
-  int32_t band_fine;           /* refinement band of the surface level, cells (8); sets the periodic replication margin */
-  int32_t reserved[5];
+  int32_t levels;              /* L >= 1 */
+  int32_t surface_level;       /* level of the surface band (0 = L) */
+  int32_t band_fine;           /* band of the surface level, its cells (8) */
+  int32_t band;                /* band of each coarser level, its cells (6) */
+  int32_t wake_level_offset;   /* wake level = surface_level - offset (1) */
+  double wake_length;          /* body x extents; 0 disables */
+  double wake_margin;          /* body extents (0.1) */
+  int32_t nregions;
+  const oal_q19_region* regions;
+  int32_t reserved[4];
 } oal_q19_mesh_spec;
 typedef struct oal_q19_mesh oal_q19_mesh;
 
@@ -389,11 +415,14 @@ oal_status oal_q19_default_mesh_spec(oal_q19_mesh_spec* out);
 /* tri: (ntri, 3 vertices, 3 coordinates) metres; ntri = 0 meshes an empty box */
 oal_status oal_q19_mesh_generate(const double* tri, int32_t ntri, const oal_q19_mesh_spec* spec, oal_q19_mesh** out);
 oal_status oal_q19_mesh_destroy(oal_q19_mesh* mesh);
-/* out[16] = {nocts, n0, n1, n2, fluid, solid, boundary, cut cells, cut links, leak cells,
- *            links without a Bouzidi partner, unreached triangles, special slots, real octs, triangles with periodic copies, 0} */
-oal_status oal_q19_mesh_counts(const oal_q19_mesh* mesh, int64_t* out);
-/* the mesh's arrays as a level descriptor (pointers valid while the mesh lives) */
-oal_status oal_q19_mesh_level_desc(const oal_q19_mesh* mesh, oal_q19_level_desc* out);
+int32_t oal_q19_mesh_levels(const oal_q19_mesh* mesh);
+/* counts of level `level` (1..L): out[16] = {nocts, n0, n1, n2, fluid, solid, boundary, cut cells,
+ * cut links, leak cells, links without a Bouzidi partner, unreached triangles, special slots,
+ * real octs, listed ghosts, restricted slots}; level 0: the same summed over the levels (n0..n2
+ * of the finest level, the leak / unreached / triangle counts of the mesh) */
+oal_status oal_q19_mesh_counts(const oal_q19_mesh* mesh, int32_t level, int64_t* out);
+/* level `level` (1..L) as a descriptor (pointers valid while the mesh lives) */
+oal_status oal_q19_mesh_level_desc(const oal_q19_mesh* mesh, int32_t level, oal_q19_level_desc* out);
 
 oal_status oal_q19_level_create(int32_t device, int32_t precision, int32_t nocts, const int32_t* onbr,
                                 oal_q19_level** out);
@@ -416,6 +445,27 @@ oal_status oal_q19_level_device_state(oal_q19_level* level, void** f, void** u, 
 /* out[5] = {mass, px, py, pz, kinetic energy sum 0.5 rho |u|^2}, FP64, fixed reduction order */
 oal_status oal_q19_level_totals(oal_q19_level* level, double* out, void* stream);
 /* device arrays: f(n,19) omega(n) pfd(n,6) F(n,3) -> out(n,19) rho(n) u(n,3) */
+/* ---- several levels: the recursive step (run.jl:6-11, coupling.jl step_recursive!) ----------
+ * One coarse step = one step of level 1 and, recursively, two of each finer level, with the
+ * restriction into the covered slots and the ghost fill at the half and full time (coupling.jl).
+ * `params` holds one oal_q19_params per level (nu, body force and force scale of that level's
+ * lattice units). Level l's arrays are read through oal_q19_octree_level. */
+typedef struct oal_q19_octree oal_q19_octree;
+oal_status oal_q19_octree_create(int32_t device, int32_t precision, int32_t nlevels, const oal_q19_level_desc* levels,
+                                 oal_q19_octree** out);
+oal_status oal_q19_octree_destroy(oal_q19_octree* tree);
+oal_status oal_q19_octree_level(oal_q19_octree* tree, int32_t level, oal_q19_level** out);
+/* per level host arrays rho[l], u[l], du[l] (du[l] nullable) for the fluid, ghost and covered slots;
+ * then the coupling of the initial state (couple_initial!) */
+oal_status oal_q19_octree_initialise(oal_q19_octree* tree, const oal_q19_params* params, const void* const* rho,
+                                     const void* const* u, const void* const* du);
+oal_status oal_q19_octree_advance(oal_q19_octree* tree, const oal_q19_params* params, int32_t n_coarse_steps,
+                                  int32_t collect_forces, void* stream);
+/* force of the last collecting coarse step over all levels and sub-steps, coarse-lattice units */
+oal_status oal_q19_octree_forces(oal_q19_octree* tree, double* total, double* per_triangle);
+/* FP64 {mass, px, py, pz, kinetic energy} over the fluid leaves, each level weighted by 8^(L-l) */
+oal_status oal_q19_octree_totals(oal_q19_octree* tree, double* out);
+
 oal_status oal_q19_collide_cells(int32_t precision, int64_t n, const void* f, const void* omega, double sigma,
                                  const void* pfd, const void* F, void* out, void* rho, void* u, void* stream);
 

@@ -168,18 +168,46 @@ class Q19LevelDesc(C.Structure):
         ("cut_partner", C.c_void_p),
         ("ntri", C.c_int32),
         ("faces", C.c_int32 * 6),
+        ("nghost", C.c_int32),
+        ("ghost_slot", C.c_void_p),
+        ("ghost_donor", C.c_void_p),
+        ("ghost_w", C.c_void_p),
+        ("nrestrict", C.c_int32),
+        ("restrict_slot", C.c_void_p),
+        ("restrict_src", C.c_void_p),
+        ("restrict_cubic", C.c_void_p),
+    ]
+
+
+class Q19Region(C.Structure):
+    """oal_q19_region (include/oal.h): a refinement region (0 box, 1 sphere, 2 cylinder)."""
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("level", C.c_int32),
+        ("lo", C.c_double * 3),
+        ("hi", C.c_double * 3),
+        ("centre", C.c_double * 3),
+        ("radius", C.c_double),
     ]
 
 
 class Q19MeshSpec(C.Structure):
-    """oal_q19_mesh_spec (include/oal.h): MeshSpec of a single-level mesh."""
+    """oal_q19_mesh_spec (include/oal.h): the reference's MeshSpec."""
     _fields_ = [
         ("domain", C.c_double * 3),
         ("dx", C.c_double),
         ("periodic", C.c_int32 * 3),
         ("faces", C.c_int32 * 6),
+        ("levels", C.c_int32),
+        ("surface_level", C.c_int32),
         ("band_fine", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("band", C.c_int32),
+        ("wake_level_offset", C.c_int32),
+        ("wake_length", C.c_double),
+        ("wake_margin", C.c_double),
+        ("nregions", C.c_int32),
+        ("regions", C.c_void_p),
+        ("reserved", C.c_int32 * 4),
     ]
 
 
@@ -246,8 +274,16 @@ _SIGNATURES = {
     "oal_q19_default_mesh_spec": (C.c_int32, [C.POINTER(Q19MeshSpec)]),
     "oal_q19_mesh_generate": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(Q19MeshSpec), C.POINTER(C.c_void_p)]),
     "oal_q19_mesh_destroy": (C.c_int32, [C.c_void_p]),
-    "oal_q19_mesh_counts": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
-    "oal_q19_mesh_level_desc": (C.c_int32, [C.c_void_p, C.POINTER(Q19LevelDesc)]),
+    "oal_q19_mesh_counts": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64)]),
+    "oal_q19_mesh_level_desc": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(Q19LevelDesc)]),
+    "oal_q19_mesh_levels": (C.c_int32, [C.c_void_p]),
+    "oal_q19_octree_create": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "oal_q19_octree_destroy": (C.c_int32, [C.c_void_p]),
+    "oal_q19_octree_level": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)]),
+    "oal_q19_octree_initialise": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "oal_q19_octree_advance": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]),
+    "oal_q19_octree_forces": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "oal_q19_octree_totals": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double)]),
     "oal_q19_level_get_state": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "oal_q19_level_set_state": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "oal_q19_level_device_state": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),

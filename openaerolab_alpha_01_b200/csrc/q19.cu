@@ -28,6 +28,7 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <unordered_map>
 
 #include "../../include/oal.h"
 
@@ -535,7 +536,7 @@ __global__ void __launch_bounds__(kThreads) k_q19_walls(const LevelArgs<T> a, co
       // momentum exchange on the cut links: (f_i* + f_j(t+1)) c_i per link, i toward the wall
       for (int li = w.cut_off[ci] - 1; li < w.cut_off[ci + 1] - 1; ++li) {
         const int i = w.cut_dir[li] - 1;
-        w.mom[li] = w.scale * (double)(fo[i] + f[opp(i)]);
+        w.mom[li] += w.scale * (double)(fo[i] + f[opp(i)]);
       }
     }
   }
@@ -588,9 +589,9 @@ __global__ void k_q19_force_total(int32_t ntri, const double* __restrict__ per_t
   if (t < 3) total[t] = s[t][0];
 }
 
-// initial state of the fluid slots from (rho, u[, du]): `rebuild` with the Chapman-Enskog
-// non-equilibrium, or the equilibrium when du is null (state.jl:267-305, coupling.jl:26-30);
-// the other slots keep the allocation state (f = 0, u = 0, rho = 1)
+// initial state of the fluid, ghost and covered slots from (rho, u[, du]): `rebuild` with the
+// Chapman-Enskog non-equilibrium, or the equilibrium when du is null (state.jl:267-305,
+// coupling.jl:26-30); the other slots keep the allocation state (f = 0, u = 0, rho = 1)
 template <class T>
 __global__ void k_q19_initialise(int64_t nslots, const uint8_t* __restrict__ kind, const T* __restrict__ rho_in,
                                  const T* __restrict__ u_in, const T* __restrict__ du, T nu, T* __restrict__ fa,
@@ -600,7 +601,7 @@ __global__ void k_q19_initialise(int64_t nslots, const uint8_t* __restrict__ kin
   if (s >= nslots) return;
   const int64_t o = s >> 3;
   const int k = (int)(s & 7);
-  const bool fluid = !kind || kind[s] == K_FLUID;
+  const bool fluid = !kind || kind[s] == K_FLUID || kind[s] == K_GHOST || kind[s] == K_COVERED;
   T out[Q];
   T rho = T(1), ux = T(0), uy = T(0), uz = T(0);
   if (fluid) {
@@ -880,43 +881,60 @@ cudaError_t launch_walls(const LevelArgs<T>& a, const WallArgs<T>& w, int sgs, b
   }
 }
 
+// one step of a level (step_level! + swap_buffers!); with `collect` the momentum exchange of its
+// cut links is added to the per-link accumulator
+template <class T>
+cudaError_t step_level_t(oal_q19_level* L, const oal_q19_params* p, bool collect, cudaStream_t st) {
+  const bool forced = !(T(p->body_force[0]) == T(0) && T(p->body_force[1]) == T(0) && T(p->body_force[2]) == T(0));
+  const LevelArgs<T> a = level_args<T>(L, p);
+  cudaError_t e = launch_step<T>(a, p->sgs, forced, st);
+  if (e == cudaSuccess && L->walls) {
+    LevelArgs<T> b = a;
+    b.work = L->work_walls;
+    b.n_work = L->n_walls;
+    WallArgs<T> w;
+    w.kind = L->kind;
+    w.face = L->face;
+    w.special = L->special;
+    w.cutidx = L->cutidx;
+    w.qdir = L->qdir;
+    w.okdir = L->okdir;
+    w.cut_off = L->cut_off;
+    w.cut_dir = L->cut_dir;
+    w.mom = (collect && L->nlinks > 0) ? L->mom : nullptr;
+    w.scale = p->force_scale;
+    for (int f = 0; f < 6; ++f) w.faces[f] = L->faces[f];
+    w.uin0 = T(p->u_inlet[0]);
+    w.uin1 = T(p->u_inlet[1]);
+    w.uin2 = T(p->u_inlet[2]);
+    e = launch_walls<T>(b, w, p->sgs, forced, st);
+  }
+  L->cur = 1 - L->cur;
+  ++L->steps;
+  return e;
+}
+
+// per-triangle and total force of a level from its per-link accumulator
+cudaError_t level_forces(oal_q19_level* L, cudaStream_t st) {
+  if (!L->walls) return cudaSuccess;
+  if (L->nlinks > 0)
+    k_q19_tri_forces<<<(L->ntri + 127) / 128, 128, 0, st>>>(L->ntri, L->tri_off, L->tri_links, L->cut_dir, L->mom,
+                                                           L->tri_force);
+  else
+    cudaMemsetAsync(L->tri_force, 0, sizeof(double) * 3 * (size_t)L->ntri, st);
+  k_q19_force_total<<<1, 256, 0, st>>>(L->ntri, L->tri_force, L->tri_force + 3 * (int64_t)L->ntri);
+  L->forces_valid = true;
+  return cudaGetLastError();
+}
+
 template <class T>
 oal_status advance_t(oal_q19_level* L, const oal_q19_params* p, int32_t n, bool collect, cudaStream_t st) {
-  const bool forced = !(T(p->body_force[0]) == T(0) && T(p->body_force[1]) == T(0) && T(p->body_force[2]) == T(0));
   for (int32_t s = 0; s < n; ++s) {
-    const LevelArgs<T> a = level_args<T>(L, p);
-    Q19_TRY(launch_step<T>(a, p->sgs, forced, st));
-    if (L->walls) {
-      LevelArgs<T> b = a;
-      b.work = L->work_walls;
-      b.n_work = L->n_walls;
-      WallArgs<T> w;
-      w.kind = L->kind;
-      w.face = L->face;
-      w.special = L->special;
-      w.cutidx = L->cutidx;
-      w.qdir = L->qdir;
-      w.okdir = L->okdir;
-      w.cut_off = L->cut_off;
-      w.cut_dir = L->cut_dir;
-      const bool last = s == n - 1;
-      w.mom = (collect && last && L->nlinks > 0) ? L->mom : nullptr;
-      w.scale = p->force_scale;
-      for (int f = 0; f < 6; ++f) w.faces[f] = L->faces[f];
-      w.uin0 = T(p->u_inlet[0]);
-      w.uin1 = T(p->u_inlet[1]);
-      w.uin2 = T(p->u_inlet[2]);
-      Q19_TRY(launch_walls<T>(b, w, p->sgs, forced, st));
-      if (w.mom) {
-        k_q19_tri_forces<<<(L->ntri + 127) / 128, 128, 0, st>>>(L->ntri, L->tri_off, L->tri_links, L->cut_dir, L->mom,
-                                                               L->tri_force);
-        k_q19_force_total<<<1, 256, 0, st>>>(L->ntri, L->tri_force, L->tri_force + 3 * (int64_t)L->ntri);
-        Q19_TRY(cudaGetLastError());
-        L->forces_valid = true;
-      }
-    }
-    L->cur = 1 - L->cur;
-    ++L->steps;
+    const bool last = s == n - 1;
+    if (collect && last && L->walls && L->nlinks > 0)
+      Q19_TRY(cudaMemsetAsync(L->mom, 0, sizeof(double) * L->nlinks, st));
+    Q19_TRY(step_level_t<T>(L, p, collect && last, st));
+    if (collect && last) Q19_TRY(level_forces(L, st));
   }
   return OAL_OK;
 }
@@ -959,6 +977,9 @@ oal_status check_device(int32_t device) {
 }
 
 }  // namespace
+
+static oal_status create_desc_impl(int32_t device, int32_t precision, const oal_q19_level_desc* d, bool transfers,
+                                   oal_q19_level** out);
 
 extern "C" {
 
@@ -1045,6 +1066,13 @@ oal_status oal_q19_level_create(int32_t device, int32_t precision, int32_t nocts
 }
 
 oal_status oal_q19_level_create_desc(int32_t device, int32_t precision, const oal_q19_level_desc* d, oal_q19_level** out) {
+  return create_desc_impl(device, precision, d, false, out);
+}
+
+}  // extern "C"
+
+static oal_status create_desc_impl(int32_t device, int32_t precision, const oal_q19_level_desc* d, bool transfers,
+                                   oal_q19_level** out) {
   if (!out || !d || !d->onbr) return fail(OAL_E_INVALID_ARG, "null argument");
   *out = nullptr;
   if (precision != OAL_STORE_F32 && precision != OAL_STORE_F64)
@@ -1063,8 +1091,8 @@ oal_status oal_q19_level_create_desc(int32_t device, int32_t precision, const oa
   if (d->kind) std::memcpy(kind.data(), d->kind, ns);
   for (size_t s = 0; s < ns; ++s) {
     if (kind[s] > OAL_Q19_K_BOUNDARY) return fail(OAL_E_INVALID_ARG, "slot %zu: unknown kind %d", s, kind[s]);
-    if (kind[s] == OAL_Q19_K_GHOST || kind[s] == OAL_Q19_K_COVERED)
-      return fail(OAL_E_UNSUPPORTED, "ghost and covered slots (refined levels) have no kernel in this build");
+    if (!transfers && (kind[s] == OAL_Q19_K_GHOST || kind[s] == OAL_Q19_K_COVERED))
+      return fail(OAL_E_UNSUPPORTED, "ghost and covered slots belong to a refined mesh: create it with oal_q19_octree_create");
   }
   for (int64_t t = 0; t < (int64_t)nocts * 27; ++t)
     if (d->onbr[t] < 0 || d->onbr[t] > nocts) return fail(OAL_E_INVALID_ARG, "onbr entry %lld out of range", (long long)t);
@@ -1199,6 +1227,8 @@ oal_status oal_q19_level_create_desc(int32_t device, int32_t precision, const oa
   *out = L;
   return OAL_OK;
 }
+
+extern "C" {
 
 oal_status oal_q19_level_destroy(oal_q19_level* L) {
   if (!L) return OAL_OK;
@@ -1347,6 +1377,522 @@ oal_status oal_q19_collide_cells(int32_t precision, int64_t n, const void* f, co
     k_q19_collide_cells<float><<<grid, 128, 0, st>>>(n, (const float*)f, (const float*)omega, (float)sigma, (const float*)pfd,
                                                      (const float*)F, (float*)out, (float*)rho, (float*)u);
   Q19_TRY(cudaGetLastError());
+  return OAL_OK;
+}
+
+}  // extern "C"
+
+// ---- several levels: transfers and the recursive step (coupling.jl) ------------------------------
+
+namespace {
+
+// rho, u and Pi_neq of slot s of a population buffer (coupling.jl:16-23)
+template <class T>
+__device__ __forceinline__ void slot_moments(const T* __restrict__ f, int64_t s, T* m) {
+  const int64_t o = s >> 3;
+  const int k = (int)(s & 7);
+  T fl[Q];
+#pragma unroll
+  for (int i = 0; i < Q; ++i) fl[i] = f[o * (8 * Q) + 8 * i + k];
+  T drho, mx, my, mz, P[6];
+  moments<T>(fl, drho, mx, my, mz, P);
+  const T rho = drho + T(1), inv = T(1) / rho;
+  const T ux = mx * inv, uy = my * inv, uz = mz * inv;
+  const T d3 = drho * T(1.0 / 3.0);
+  const T rx = rho * ux, ry = rho * uy, rz = rho * uz;
+  m[0] = rho;
+  m[1] = ux;
+  m[2] = uy;
+  m[3] = uz;
+  m[4] = P[0] - d3 - rx * ux;
+  m[5] = P[1] - d3 - ry * uy;
+  m[6] = P[2] - d3 - rz * uz;
+  m[7] = P[3] - rx * uy;
+  m[8] = P[4] - rx * uz;
+  m[9] = P[5] - ry * uz;
+}
+
+// the ten moments of the donor cells at the requested time (fill_ghosts! stage 1): mode 0 the old
+// buffer, 1 the new one, 2 the blend w0 old + w1 new (covered donors unblended from the new buffer)
+template <class T>
+__global__ void k_q19_donor_moments(int32_t n, const int32_t* __restrict__ cells, const T* __restrict__ fnew,
+                                    const T* __restrict__ fold, int mode, T w0, T w1, const uint8_t* __restrict__ cov,
+                                    T* __restrict__ out) {
+  const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  T m[10];
+  if (mode == 0) {
+    slot_moments<T>(fold, cells[c], m);
+  } else if (mode == 1 || cov[c]) {
+    slot_moments<T>(fnew, cells[c], m);
+  } else {
+    T mo[10];
+    slot_moments<T>(fnew, cells[c], m);
+    slot_moments<T>(fold, cells[c], mo);
+#pragma unroll
+    for (int i = 0; i < 10; ++i) m[i] = w0 * mo[i] + w1 * m[i];
+  }
+#pragma unroll
+  for (int i = 0; i < 10; ++i) out[10 * (int64_t)c + i] = m[i];
+}
+
+// rebuild slot s from interpolated moments at `omega` (coupling.jl:26-30, rebuild_oct!)
+template <class T>
+__device__ __forceinline__ void rebuild_slot(const T* acc, T scale, T omega, int64_t s, T* f, T* u, T* rho) {
+  const T r = acc[0], ux = acc[1], uy = acc[2], uz = acc[3];
+  T p[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) p[i] = scale * acc[4 + i];
+  const T drho = r - T(1);
+  T out[Q];
+  populations<T>(drho, r, ux, uy, uz, p, T(1) - omega, out);
+  if (below_floor<T>(out)) limit_unforced<T>(out, drho, r, ux, uy, uz);
+  const int64_t o = s >> 3;
+  const int k = (int)(s & 7);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) f[o * (8 * Q) + 8 * i + k] = out[i];
+  u[o * 24 + k] = ux;
+  u[o * 24 + 8 + k] = uy;
+  u[o * 24 + 16 + k] = uz;
+  rho[s] = r;
+}
+
+// ghost fill (fill_ghosts! stage 2): weighted sums of the donor moments, rebuilt at the fine omega
+template <class T>
+__global__ void k_q19_fill(int32_t ng, const int32_t* __restrict__ ghost_slot, const int32_t* __restrict__ dix,
+                           const float* __restrict__ gw, const T* __restrict__ dm, T scale, T omega, T* f, T* u, T* rho) {
+  const int32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ng) return;
+  T acc[10];
+#pragma unroll
+  for (int i = 0; i < 10; ++i) acc[i] = T(0);
+  for (int n = 0; n < 64; ++n) {
+    const int32_t d = dix[64 * (int64_t)g + n];
+    if (!d) continue;
+    const T wn = T(gw[64 * (int64_t)g + n]);
+    const T* m = dm + 10 * (int64_t)(d - 1);
+#pragma unroll
+    for (int i = 0; i < 10; ++i) acc[i] += wn * m[i];
+  }
+  rebuild_slot<T>(acc, scale, omega, ghost_slot[g], f, u, rho);
+}
+
+// the ten moments of the restriction sources from the fine buffer (restrict! stage 1)
+template <class T>
+__global__ void k_q19_source_moments(int32_t n, const int32_t* __restrict__ cells, const T* __restrict__ f,
+                                     T* __restrict__ out) {
+  const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  T m[10];
+  slot_moments<T>(f, cells[c], m);
+#pragma unroll
+  for (int i = 0; i < 10; ++i) out[10 * (int64_t)c + i] = m[i];
+}
+
+__host__ __device__ constexpr double restrict_w1(int d) { return d == 0 || d == 3 ? -0.0625 : 0.5625; }  // cubic at 1/2
+__device__ __forceinline__ int stencil_inner_node(int m) {
+  return (1 + (m & 1)) + 4 * (1 + ((m >> 1) & 1)) + 16 * (1 + ((m >> 2) & 1));
+}
+
+// restriction (restrict! stage 2): cubic weights over 64 sources, or the admissible children averaged
+template <class T>
+__global__ void k_q19_restrict(int32_t nr, const int32_t* __restrict__ rslot, const int32_t* __restrict__ six,
+                               const uint8_t* __restrict__ cubic, const T* __restrict__ rm, T scale, T omega, T* f, T* u,
+                               T* rho) {
+  const int32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nr) return;
+  T acc[10];
+#pragma unroll
+  for (int i = 0; i < 10; ++i) acc[i] = T(0);
+  if (cubic[r]) {
+    for (int n = 0; n < 64; ++n) {
+      const T wn = T(restrict_w1(n & 3) * restrict_w1((n >> 2) & 3) * restrict_w1(n >> 4));
+      const T* m = rm + 10 * (int64_t)(six[64 * (int64_t)r + n] - 1);
+#pragma unroll
+      for (int i = 0; i < 10; ++i) acc[i] += wn * m[i];
+    }
+  } else {
+    int cnt = 0;
+    for (int mm = 0; mm < 8; ++mm) {
+      const int32_t d = six[64 * (int64_t)r + stencil_inner_node(mm)];
+      if (!d) continue;
+      const T* m = rm + 10 * (int64_t)(d - 1);
+#pragma unroll
+      for (int i = 0; i < 10; ++i) acc[i] += m[i];
+      ++cnt;
+    }
+    if (cnt == 0) return;
+    const T inv = T(1) / T(cnt);
+#pragma unroll
+    for (int i = 0; i < 10; ++i) acc[i] *= inv;
+  }
+  rebuild_slot<T>(acc, scale, omega, rslot[r], f, u, rho);
+}
+
+// copy slots (the last ghost fill) from the old buffers into the new ones (copy_ghosts!)
+template <class T>
+__global__ void k_q19_copy_slots(int32_t n, const int32_t* __restrict__ slots, const T* __restrict__ fs, T* fd,
+                                 const T* __restrict__ us, T* ud, const T* __restrict__ rs, T* rd) {
+  const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const int64_t s = slots[c], o = s >> 3;
+  const int k = (int)(s & 7);
+#pragma unroll
+  for (int i = 0; i < Q; ++i) fd[o * (8 * Q) + 8 * i + k] = fs[o * (8 * Q) + 8 * i + k];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) ud[o * 24 + 8 * a + k] = us[o * 24 + 8 * a + k];
+  rd[s] = rs[s];
+}
+
+__global__ void k_add3(int64_t n, const double* __restrict__ a, double* __restrict__ acc) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) acc[i] += a[i];
+}
+
+// distinct entries of a (64, n) 1-based slot table, in first-appearance order, and the table
+// re-indexed into them (state.jl:144-154 index_table)
+void index_table(const int32_t* tab, int32_t n, std::vector<int32_t>& cells, std::vector<int32_t>& ix) {
+  std::unordered_map<int32_t, int32_t> idx;
+  ix.assign(64 * (size_t)n, 0);
+  cells.clear();
+  for (int32_t j = 0; j < n; ++j)
+    for (int nn = 0; nn < 64; ++nn) {
+      const int32_t s = tab[64 * (size_t)j + nn];
+      if (!s) continue;
+      auto it = idx.find(s);
+      if (it == idx.end()) {
+        cells.push_back(s - 1);
+        it = idx.emplace(s, (int32_t)cells.size()).first;
+      }
+      ix[64 * (size_t)j + nn] = it->second;
+    }
+}
+
+struct Transfer {
+  // fill of this level from the coarser one
+  int32_t ng = 0, nd = 0;
+  int32_t* ghost_slot = nullptr;
+  int32_t* dix = nullptr;
+  float* gw = nullptr;
+  int32_t* dcells = nullptr;
+  uint8_t* dcov = nullptr;
+  void* dm = nullptr;
+  // restriction into this level from the finer one
+  int32_t nr = 0, ns = 0;
+  int32_t* rslot = nullptr;
+  int32_t* six = nullptr;
+  uint8_t* rcubic = nullptr;
+  int32_t* scells = nullptr;
+  void* rm = nullptr;
+};
+
+}  // namespace
+
+struct oal_q19_octree {
+  int device = 0;
+  int precision = OAL_STORE_F32;
+  int L = 0;
+  size_t es = 4;
+  std::vector<oal_q19_level*> lv;
+  std::vector<Transfer> tt;
+  int32_t ntri = 1;
+  double* tri_total = nullptr;  // (ntri, 3) then the total (3)
+  double* part = nullptr;       // per-level totals (5 L)
+  bool forces_valid = false;
+};
+
+namespace {
+
+template <class T>
+T omega_of_h(double nu) {
+  const T n = T(nu);
+  return T(1) / (T(3) * n + T(0.5));
+}
+template <class T>
+T pre_collision_factor_h(T omega) {
+  const T d = T(1) - omega;
+  return (d < T(0) ? -d : d) > T(0.05) ? T(1) / d : T(0);
+}
+
+template <class T>
+cudaError_t fill_ghosts_t(oal_q19_octree* tr, const oal_q19_params* p, int l, T weight, cudaStream_t st) {
+  const Transfer& t = tr->tt[l - 1];
+  if (t.ng == 0) return cudaSuccess;
+  oal_q19_level* Lc = tr->lv[l - 2];
+  oal_q19_level* Lf = tr->lv[l - 1];
+  const T omega_c = omega_of_h<T>(p[l - 2].nu), omega_f = omega_of_h<T>(p[l - 1].nu);
+  const T tau_c = T(1) / omega_c, tau_f = T(1) / omega_f;
+  const T scale = tau_f / (T(2) * tau_c) * pre_collision_factor_h<T>(omega_c);
+  const T w1 = weight, w0 = T(1) - weight;
+  const int mode = w1 == T(0) ? 0 : (w0 == T(0) ? 1 : 2);
+  k_q19_donor_moments<T><<<(t.nd + 127) / 128, 128, 0, st>>>(t.nd, t.dcells, (const T*)Lc->f[Lc->cur],
+                                                             (const T*)Lc->f[1 - Lc->cur], mode, w0, w1, t.dcov, (T*)t.dm);
+  k_q19_fill<T><<<(t.ng + 127) / 128, 128, 0, st>>>(t.ng, t.ghost_slot, t.dix, t.gw, (const T*)t.dm, scale, omega_f,
+                                                    (T*)Lf->f[Lf->cur], (T*)Lf->u[Lf->cur], (T*)Lf->rho[Lf->cur]);
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t restrict_t(oal_q19_octree* tr, const oal_q19_params* p, int l, cudaStream_t st) {
+  const Transfer& t = tr->tt[l - 1];
+  if (t.nr == 0) return cudaSuccess;
+  oal_q19_level* Lc = tr->lv[l - 1];
+  oal_q19_level* Lf = tr->lv[l];
+  const T omega_c = omega_of_h<T>(p[l - 1].nu), omega_f = omega_of_h<T>(p[l].nu);
+  const T tau_c = T(1) / omega_c, tau_f = T(1) / omega_f;
+  const T scale = T(2) * tau_c / tau_f * pre_collision_factor_h<T>(omega_f);
+  k_q19_source_moments<T><<<(t.ns + 127) / 128, 128, 0, st>>>(t.ns, t.scells, (const T*)Lf->f[Lf->cur], (T*)t.rm);
+  k_q19_restrict<T><<<(t.nr + 127) / 128, 128, 0, st>>>(t.nr, t.rslot, t.six, t.rcubic, (const T*)t.rm, scale, omega_c,
+                                                        (T*)Lc->f[Lc->cur], (T*)Lc->u[Lc->cur], (T*)Lc->rho[Lc->cur]);
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t copy_ghosts_t(oal_q19_octree* tr, int l, cudaStream_t st) {
+  const Transfer& t = tr->tt[l - 1];
+  if (l == tr->L || t.ng == 0) return cudaSuccess;
+  oal_q19_level* S = tr->lv[l - 1];
+  const int c = S->cur, o = 1 - S->cur;
+  k_q19_copy_slots<T><<<(t.ng + 127) / 128, 128, 0, st>>>(t.ng, t.ghost_slot, (const T*)S->f[o], (T*)S->f[c],
+                                                          (const T*)S->u[o], (T*)S->u[c], (const T*)S->rho[o], (T*)S->rho[c]);
+  return cudaGetLastError();
+}
+
+// step_recursive! (coupling.jl:240-254)
+template <class T>
+cudaError_t step_recursive_t(oal_q19_octree* tr, const oal_q19_params* p, int l, bool collect, cudaStream_t st) {
+  cudaError_t e = step_level_t<T>(tr->lv[l - 1], &p[l - 1], collect, st);
+  if (e == cudaSuccess) e = copy_ghosts_t<T>(tr, l, st);
+  if (e == cudaSuccess && l < tr->L) {
+    e = step_recursive_t<T>(tr, p, l + 1, collect, st);
+    if (e == cudaSuccess) e = restrict_t<T>(tr, p, l, st);
+    if (e == cudaSuccess) e = fill_ghosts_t<T>(tr, p, l + 1, T(0.5), st);
+    if (e == cudaSuccess) e = step_recursive_t<T>(tr, p, l + 1, collect, st);
+    if (e == cudaSuccess) e = restrict_t<T>(tr, p, l, st);
+    if (e == cudaSuccess) e = fill_ghosts_t<T>(tr, p, l + 1, T(1), st);
+  }
+  return e;
+}
+
+template <class T>
+oal_status octree_advance_t(oal_q19_octree* tr, const oal_q19_params* p, int32_t n, bool collect, cudaStream_t st) {
+  for (int32_t s = 0; s < n; ++s) {
+    const bool last = collect && s == n - 1;
+    if (last)
+      for (oal_q19_level* L : tr->lv)
+        if (L->walls && L->nlinks > 0) Q19_TRY(cudaMemsetAsync(L->mom, 0, sizeof(double) * L->nlinks, st));
+    Q19_TRY(step_recursive_t<T>(tr, p, 1, last, st));
+    if (last) {
+      Q19_TRY(cudaMemsetAsync(tr->tri_total, 0, sizeof(double) * 3 * (size_t)tr->ntri, st));
+      for (oal_q19_level* L : tr->lv) {
+        if (!L->walls) continue;
+        Q19_TRY(level_forces(L, st));
+        const int64_t nn = 3 * (int64_t)std::min(L->ntri, tr->ntri);
+        k_add3<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(nn, L->tri_force, tr->tri_total);
+      }
+      k_q19_force_total<<<1, 256, 0, st>>>(tr->ntri, tr->tri_total, tr->tri_total + 3 * (int64_t)tr->ntri);
+      Q19_TRY(cudaGetLastError());
+      tr->forces_valid = true;
+    }
+  }
+  return OAL_OK;
+}
+
+template <class T>
+oal_status couple_initial_t(oal_q19_octree* tr, const oal_q19_params* p) {
+  // couple_initial! (coupling.jl:257-268): restrict every level into its parent, then fill every
+  // level's ghosts; each level's old buffers mirror the new ones
+  auto mirror = [&](int l) -> cudaError_t {
+    oal_q19_level* S = tr->lv[l - 1];
+    const size_t ns = (size_t)S->nocts * 8;
+    cudaError_t e = cudaMemcpy(S->f[1 - S->cur], S->f[S->cur], S->es * ns * Q, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(S->u[1 - S->cur], S->u[S->cur], S->es * ns * 3, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(S->rho[1 - S->cur], S->rho[S->cur], S->es * ns, cudaMemcpyDeviceToDevice);
+    return e;
+  };
+  for (int l = tr->L - 1; l >= 1; --l) {
+    Q19_TRY(restrict_t<T>(tr, p, l, nullptr));
+    Q19_TRY(mirror(l));
+  }
+  for (int l = 2; l <= tr->L; ++l) {
+    Q19_TRY(fill_ghosts_t<T>(tr, p, l, T(1), nullptr));
+    Q19_TRY(mirror(l));
+  }
+  Q19_TRY(cudaDeviceSynchronize());
+  return OAL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+oal_status oal_q19_octree_destroy(oal_q19_octree* tr) {
+  if (!tr) return OAL_OK;
+  {
+    DeviceGuard g(tr->device);
+    for (Transfer& t : tr->tt) {
+      void* ptrs[] = {t.ghost_slot, t.dix, t.gw, t.dcells, t.dcov, t.dm, t.rslot, t.six, t.rcubic, t.scells, t.rm};
+      for (void* q : ptrs) cudaFree(q);
+    }
+    cudaFree(tr->tri_total);
+    cudaFree(tr->part);
+  }
+  for (oal_q19_level* L : tr->lv) oal_q19_level_destroy(L);
+  delete tr;
+  return OAL_OK;
+}
+
+oal_status oal_q19_octree_create(int32_t device, int32_t precision, int32_t nlevels, const oal_q19_level_desc* d,
+                                 oal_q19_octree** out) {
+  if (!out || !d) return fail(OAL_E_INVALID_ARG, "null argument");
+  *out = nullptr;
+  if (nlevels < 1 || nlevels > 12) return fail(OAL_E_INVALID_ARG, "nlevels %d", nlevels);
+  // host-side checks of the transfer tables: every slot they name exists and has the right kind
+  for (int l = 1; l <= nlevels; ++l) {
+    const oal_q19_level_desc& D = d[l - 1];
+    const int64_t ns = 8 * (int64_t)D.nocts;
+    auto kind_of = [&](const oal_q19_level_desc& X, int64_t s) { return X.kind ? X.kind[s] : (uint8_t)OAL_Q19_K_FLUID; };
+    if (D.nghost < 0 || D.nrestrict < 0) return fail(OAL_E_INVALID_ARG, "level %d: negative transfer counts", l);
+    if (D.nghost > 0 && (l == 1 || !D.ghost_slot || !D.ghost_donor || !D.ghost_w))
+      return fail(OAL_E_INVALID_ARG, "level %d: ghost lists need a coarser level and their arrays", l);
+    if (D.nrestrict > 0 && (l == nlevels || !D.restrict_slot || !D.restrict_src || !D.restrict_cubic))
+      return fail(OAL_E_INVALID_ARG, "level %d: restriction lists need a finer level and their arrays", l);
+    for (int32_t g = 0; g < D.nghost; ++g) {
+      const int64_t s = D.ghost_slot[g] - 1;
+      if (s < 0 || s >= ns || kind_of(D, s) != OAL_Q19_K_GHOST) return fail(OAL_E_INVALID_ARG, "level %d: ghost_slot %d", l, g);
+      const int64_t nsc = 8 * (int64_t)d[l - 2].nocts;
+      for (int n = 0; n < 64; ++n) {
+        const int64_t ds = D.ghost_donor[64 * (int64_t)g + n];
+        if (ds < 0 || ds > nsc) return fail(OAL_E_INVALID_ARG, "level %d: ghost donor out of range", l);
+      }
+    }
+    for (int32_t r = 0; r < D.nrestrict; ++r) {
+      const int64_t s = D.restrict_slot[r] - 1;
+      if (s < 0 || s >= ns || kind_of(D, s) != OAL_Q19_K_COVERED)
+        return fail(OAL_E_INVALID_ARG, "level %d: restrict_slot %d", l, r);
+      const int64_t nsf = 8 * (int64_t)d[l].nocts;
+      for (int n = 0; n < 64; ++n) {
+        const int64_t cs = D.restrict_src[64 * (int64_t)r + n];
+        if (cs < 0 || cs > nsf) return fail(OAL_E_INVALID_ARG, "level %d: restriction source out of range", l);
+        if (D.restrict_cubic[r] && cs == 0) return fail(OAL_E_INVALID_ARG, "level %d: incomplete cubic stencil", l);
+      }
+    }
+  }
+  if (oal_status s = check_device(device)) return s;
+  oal_q19_octree* tr = new oal_q19_octree();
+  tr->device = device;
+  tr->precision = precision;
+  tr->L = nlevels;
+  tr->es = precision == OAL_STORE_F64 ? 8 : 4;
+  tr->tt.resize(nlevels);
+  for (int l = 1; l <= nlevels; ++l) {
+    oal_q19_level* L = nullptr;
+    oal_status s = create_desc_impl(device, precision, &d[l - 1], true, &L);
+    if (s != OAL_OK) {
+      oal_q19_octree_destroy(tr);
+      return s;
+    }
+    tr->lv.push_back(L);
+    tr->ntri = std::max(tr->ntri, std::max(d[l - 1].ntri, 1));
+  }
+  DeviceGuard g(device);
+  cudaError_t e = cudaSuccess;
+  for (int l = 1; l <= nlevels && e == cudaSuccess; ++l) {
+    const oal_q19_level_desc& D = d[l - 1];
+    Transfer& t = tr->tt[l - 1];
+    if (D.nghost > 0) {
+      std::vector<int32_t> cells, ix, gs(D.nghost);
+      index_table(D.ghost_donor, D.nghost, cells, ix);
+      for (int32_t i = 0; i < D.nghost; ++i) gs[i] = D.ghost_slot[i] - 1;
+      std::vector<uint8_t> cov(cells.size());
+      const oal_q19_level_desc& P = d[l - 2];
+      for (size_t c = 0; c < cells.size(); ++c) cov[c] = P.kind && P.kind[cells[c]] == OAL_Q19_K_COVERED;
+      t.ng = D.nghost;
+      t.nd = (int32_t)cells.size();
+      e = upload(&t.ghost_slot, gs.data(), gs.size());
+      if (e == cudaSuccess) e = upload(&t.dix, ix.data(), ix.size());
+      if (e == cudaSuccess) e = upload(&t.gw, D.ghost_w, 64 * (size_t)D.nghost);
+      if (e == cudaSuccess) e = upload(&t.dcells, cells.data(), cells.size());
+      if (e == cudaSuccess) e = upload(&t.dcov, cov.data(), cov.size());
+      if (e == cudaSuccess) e = cudaMalloc(&t.dm, tr->es * 10 * std::max<size_t>(cells.size(), 1));
+    }
+    if (e == cudaSuccess && D.nrestrict > 0) {
+      std::vector<int32_t> cells, ix, rs(D.nrestrict);
+      index_table(D.restrict_src, D.nrestrict, cells, ix);
+      for (int32_t i = 0; i < D.nrestrict; ++i) rs[i] = D.restrict_slot[i] - 1;
+      t.nr = D.nrestrict;
+      t.ns = (int32_t)cells.size();
+      e = upload(&t.rslot, rs.data(), rs.size());
+      if (e == cudaSuccess) e = upload(&t.six, ix.data(), ix.size());
+      if (e == cudaSuccess) e = upload(&t.rcubic, D.restrict_cubic, (size_t)D.nrestrict);
+      if (e == cudaSuccess) e = upload(&t.scells, cells.data(), cells.size());
+      if (e == cudaSuccess) e = cudaMalloc(&t.rm, tr->es * 10 * std::max<size_t>(cells.size(), 1));
+    }
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&tr->tri_total, sizeof(double) * (3 * (size_t)tr->ntri + 3));
+  if (e == cudaSuccess) e = cudaMemset(tr->tri_total, 0, sizeof(double) * (3 * (size_t)tr->ntri + 3));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    oal_q19_octree_destroy(tr);
+    return fail(e == cudaErrorMemoryAllocation ? OAL_E_OUT_OF_MEMORY : OAL_E_CUDA, "octree tables: %s", cudaGetErrorString(e));
+  }
+  *out = tr;
+  return OAL_OK;
+}
+
+oal_status oal_q19_octree_level(oal_q19_octree* tr, int32_t level, oal_q19_level** out) {
+  if (!tr || !out || level < 1 || level > tr->L) return fail(OAL_E_INVALID_ARG, "bad level");
+  *out = tr->lv[level - 1];
+  return OAL_OK;
+}
+
+oal_status oal_q19_octree_initialise(oal_q19_octree* tr, const oal_q19_params* p, const void* const* rho,
+                                     const void* const* u, const void* const* du) {
+  if (!tr || !p || !rho || !u) return fail(OAL_E_INVALID_ARG, "null argument");
+  for (int l = 1; l <= tr->L; ++l) {
+    if (oal_status s = oal_q19_level_initialise(tr->lv[l - 1], &p[l - 1], rho[l - 1], u[l - 1], du ? du[l - 1] : nullptr))
+      return s;
+  }
+  DeviceGuard g(tr->device);
+  tr->forces_valid = false;
+  return tr->precision == OAL_STORE_F64 ? couple_initial_t<double>(tr, p) : couple_initial_t<float>(tr, p);
+}
+
+oal_status oal_q19_octree_advance(oal_q19_octree* tr, const oal_q19_params* p, int32_t n, int32_t collect_forces,
+                                  void* stream) {
+  if (!tr || !p) return fail(OAL_E_INVALID_ARG, "null argument");
+  for (int l = 0; l < tr->L; ++l)
+    if (oal_status s = check_params(&p[l])) return s;
+  if (n < 0) return fail(OAL_E_INVALID_ARG, "n_coarse_steps < 0");
+  DeviceGuard g(tr->device);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  return tr->precision == OAL_STORE_F64 ? octree_advance_t<double>(tr, p, n, collect_forces != 0, st)
+                                        : octree_advance_t<float>(tr, p, n, collect_forces != 0, st);
+}
+
+oal_status oal_q19_octree_forces(oal_q19_octree* tr, double* total, double* per_triangle) {
+  if (!tr) return fail(OAL_E_INVALID_ARG, "null argument");
+  DeviceGuard g(tr->device);
+  if (!tr->forces_valid) {
+    if (total) total[0] = total[1] = total[2] = 0;
+    if (per_triangle) std::memset(per_triangle, 0, sizeof(double) * 3 * (size_t)tr->ntri);
+    return OAL_OK;
+  }
+  Q19_TRY(cudaDeviceSynchronize());
+  if (total) Q19_TRY(cudaMemcpy(total, tr->tri_total + 3 * (int64_t)tr->ntri, 3 * sizeof(double), cudaMemcpyDeviceToHost));
+  if (per_triangle) Q19_TRY(cudaMemcpy(per_triangle, tr->tri_total, 3 * sizeof(double) * tr->ntri, cudaMemcpyDeviceToHost));
+  return OAL_OK;
+}
+
+oal_status oal_q19_octree_totals(oal_q19_octree* tr, double* out) {
+  if (!tr || !out) return fail(OAL_E_INVALID_ARG, "null argument");
+  for (int i = 0; i < 5; ++i) out[i] = 0;
+  for (int l = 1; l <= tr->L; ++l) {
+    double t[5];
+    if (oal_status s = oal_q19_level_totals(tr->lv[l - 1], t, nullptr)) return s;
+    const double w = std::ldexp(1.0, 3 * (tr->L - l));
+    for (int i = 0; i < 5; ++i) out[i] += w * t[i];
+  }
   return OAL_OK;
 }
 

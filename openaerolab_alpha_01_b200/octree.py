@@ -64,38 +64,73 @@ class PeriodicBox:
 
 
 @dataclass
+class Region:
+    """A refinement region (generator.jl:10-16): kind "box" (lo..hi), "sphere" (centre, radius) or
+    "cylinder" (axis lo -> hi, radius), refined up to `level`."""
+    kind: str
+    level: int
+    lo: tuple = (0.0, 0.0, 0.0)
+    hi: tuple = (0.0, 0.0, 0.0)
+    centre: tuple = (0.0, 0.0, 0.0)
+    radius: float = 0.0
+
+
+@dataclass
 class MeshSpec:
-    """MeshSpec of the reference (generator.jl:21-36) for a single level: the domain in metres, the
-    periodic axes, the cell size and the condition of each domain face (-x +x -y +y -z +z)."""
+    """MeshSpec of the reference (generator.jl:21-36): the domain in metres, the periodic axes, the
+    number of levels and the finest cell size, the surface bands, regions and the condition of each
+    domain face (-x +x -y +y -z +z). Per-box surface levels are not supported."""
     domain: tuple
     periodic: tuple = (False, False, False)
     levels: int = 1
     dx_finest: float = 1.0
+    surface_level: int = 0
     band_fine: int = 8
+    band: int = 6
+    wake_length: float = 0.0
+    wake_level_offset: int = 1
+    wake_margin: float = 0.1
+    regions: tuple = ()
     faces: tuple = ("inlet", "outlet", "slip", "slip", "slip", "slip")
 
-    def native(self) -> capi.Q19MeshSpec:
-        if self.levels != 1:
-            raise capi.OALError(capi.OAL_E_UNSUPPORTED, "refined octree meshes (levels > 1) are not built")
+    def native(self):
         s = capi.Q19MeshSpec()
         check(lib().oal_q19_default_mesh_spec(C.byref(s)))
         for a in range(3):
             s.domain[a] = float(self.domain[a])
             s.periodic[a] = int(bool(self.periodic[a]))
         s.dx = float(self.dx_finest)
+        s.levels = int(self.levels)
+        s.surface_level = int(self.surface_level)
         s.band_fine = int(self.band_fine)
+        s.band = int(self.band)
+        s.wake_length = float(self.wake_length)
+        s.wake_level_offset = int(self.wake_level_offset)
+        s.wake_margin = float(self.wake_margin)
         for f in range(6):
             s.faces[f] = capi.Q19_FACE_NAMES[self.faces[f]]
-        return s
+        regs = (capi.Q19Region * max(len(self.regions), 1))()
+        for i, r in enumerate(self.regions):
+            regs[i].kind = {"box": 0, "sphere": 1, "cylinder": 2}[r.kind]
+            regs[i].level = int(r.level)
+            for a in range(3):
+                regs[i].lo[a], regs[i].hi[a], regs[i].centre[a] = r.lo[a], r.hi[a], r.centre[a]
+            regs[i].radius = float(r.radius)
+        s.nregions = len(self.regions)
+        s.regions = C.cast(regs, C.c_void_p) if self.regions else None
+        return s, regs
 
 
 _DESC_ARRAYS = [("origin", np.int32, (3,)), ("real", np.uint8, ()), ("onbr", np.int32, (27,)),
                 ("kind", np.uint8, (8,)), ("face", np.uint8, (8,)), ("special", np.uint32, (8,)),
                 ("cutidx", np.int32, (8,))]
 _CUT_ARRAYS = [("cut_dir", np.uint8), ("cut_q", np.float32), ("cut_tri", np.int32), ("cut_partner", np.uint8)]
+_TRANSFER_ARRAYS = [("ghost_slot", "nghost", np.int32, ()), ("ghost_donor", "nghost", np.int32, (64,)),
+                    ("ghost_w", "nghost", np.float32, (64,)), ("restrict_slot", "nrestrict", np.int32, ()),
+                    ("restrict_src", "nrestrict", np.int32, (64,)), ("restrict_cubic", "nrestrict", np.uint8, ())]
 COUNT_NAMES = ("octs", "n0", "n1", "n2", "fluid_total", "solid", "boundary", "wall_cells", "cut_links",
                "leak_cells", "missing_partner_links", "unreached_triangles", "special_slots", "real_octs",
-               "triangles_with_periodic_copies")
+               "ghosts_listed", "restricted")
 
 
 class Mesh:
@@ -114,12 +149,18 @@ class Mesh:
     slot_cells = PeriodicBox.slot_cells
     slot_centres = PeriodicBox.slot_centres
 
+    def oct_index(self) -> dict:
+        """origin -> 0-based oct (built once)."""
+        if getattr(self, "_octidx", None) is None:
+            self._octidx = {tuple(int(v) for v in o): i for i, o in enumerate(self.origin)}
+        return self._octidx
+
     @classmethod
-    def from_native(cls, handle) -> "Mesh":
+    def from_native(cls, handle, level: int = 1) -> "Mesh":
         d = capi.Q19LevelDesc()
-        check(lib().oal_q19_mesh_level_desc(handle, C.byref(d)))
+        check(lib().oal_q19_mesh_level_desc(handle, level, C.byref(d)))
         cnt = (C.c_int64 * 16)()
-        check(lib().oal_q19_mesh_counts(handle, cnt))
+        check(lib().oal_q19_mesh_counts(handle, level, cnt))
         no = d.nocts
         arrays = {}
         for name, dt, shape in _DESC_ARRAYS:
@@ -133,6 +174,9 @@ class Mesh:
 
         for name, dt in _CUT_ARRAYS:
             arrays[name] = view(getattr(d, name), d.nlinks, dt)
+        for name, cname, dt, shape in _TRANSFER_ARRAYS:
+            cnt_ = getattr(d, cname)
+            arrays[name] = view(getattr(d, name), cnt_ * int(np.prod(shape)), dt).reshape((cnt_,) + shape)
         arrays["cut_slot"] = view(d.cut_slot, d.ncut, np.int32)
         arrays["cut_off"] = view(d.cut_off, d.ncut + 1, np.int32)
         if arrays["cut_off"].size == 0:
@@ -154,22 +198,70 @@ class Mesh:
         d.ntri = self.ntri
         for f in range(6):
             d.faces[f] = self.faces[f]
+        for name, cname, _, _ in _TRANSFER_ARRAYS:
+            a = getattr(self, name, None)
+            n = 0 if a is None else int(a.shape[0])
+            setattr(d, cname, n)
+            setattr(d, name, a.ctypes.data if n else None)
         return d
 
 
-def generate(tri, spec: MeshSpec) -> Mesh:
-    """The reference's generate(tri, spec) for one level: triangles (ntri, 3, 3) in metres."""
+class OctMesh:
+    """The levels of an octree mesh (the reference's OctMesh): `levels[l - 1]` is level l."""
+
+    def __init__(self, levels, counts, spec):
+        self.levels = levels
+        self.counts = counts
+        self.spec = spec
+
+    @property
+    def nlevels(self) -> int:
+        return len(self.levels)
+
+    def locate_leaf(self, p):
+        """(level, 0-based slot) of the real leaf (fluid, or solid) containing point p, or (0, -1)
+        (octree.jl:248-262)."""
+        for l in range(self.nlevels, 0, -1):
+            lv = self.levels[l - 1]
+            c = [int(np.floor(p[a] / lv.dx)) for a in range(3)]
+            if any(c[a] < 0 or c[a] >= lv.n[a] for a in range(3)):
+                return 0, -1
+            key = (c[0] & ~1, c[1] & ~1, c[2] & ~1)
+            o = lv.oct_index().get(key)
+            if o is None or not lv.real[o]:
+                continue
+            s = 8 * o + (c[0] & 1) + 2 * (c[1] & 1) + 4 * (c[2] & 1)
+            if lv.kind[o, s % 8] == capi.OAL_Q19_K_COVERED:
+                continue
+            return l, s
+        return 0, -1
+
+    def work_W(self) -> int:
+        """Fluid cell updates per coarse step, sum over levels of fluid_l 2^(l-1) (run.jl:99)."""
+        return sum(m.counts["fluid_total"] << l for l, m in enumerate(self.levels))
+
+
+def generate(tri, spec: MeshSpec) -> OctMesh:
+    """The reference's generate(tri, spec): triangles (ntri, 3, 3) in metres."""
     t = np.ascontiguousarray(np.asarray(tri, np.float64).reshape(-1, 3, 3))
     h = C.c_void_p()
+    native, _keep = spec.native()
     check(lib().oal_q19_mesh_generate(t.ctypes.data_as(C.c_void_p) if t.size else None, t.shape[0],
-                                      C.byref(spec.native()), C.byref(h)))
+                                      C.byref(native), C.byref(h)))
     try:
-        m = Mesh.from_native(h)
+        L = lib().oal_q19_mesh_levels(h)
+        levels = [Mesh.from_native(h, l) for l in range(1, L + 1)]
+        cnt = (C.c_int64 * 16)()
+        check(lib().oal_q19_mesh_counts(h, 0, cnt))
     finally:
         lib().oal_q19_mesh_destroy(h)
-    m.dx = float(spec.dx_finest)
-    m.domain = tuple(v * m.dx for v in m.n)
-    return m
+    for l, m in enumerate(levels, start=1):
+        m.level = l
+        m.dx = float(spec.dx_finest) * 2.0 ** (L - l)
+        m.domain = tuple(v * m.dx for v in m.n)
+    counts = {k: int(v) for k, v in zip(COUNT_NAMES, cnt[:len(COUNT_NAMES)])}
+    counts["per_level"] = [m.counts for m in levels]
+    return OctMesh(levels, counts, spec)
 
 
 def box_triangles(lo, hi) -> np.ndarray:
@@ -197,27 +289,32 @@ class CaseConfig:
     dx: float = 1.0
     extra: dict = field(default_factory=dict)
 
-    def level_nu(self) -> float:
-        """Lattice viscosity of the single level (config.jl:309, 328-335 with L = 1)."""
+    def level_nu(self, level: int = 1, levels: int = 1) -> float:
+        """Lattice viscosity of level `level` of `levels` (config.jl:309, 328-335): the physical
+        viscosity times dt_l / dx_l^2, both scaling with 2^(L - l) from the finest level."""
         nu_phys = self.nu_lattice * self.velocity * self.dx / self.u_lattice
         vs = self.velocity / self.u_lattice
         dtf = self.dx / vs
-        return nu_phys * dtf / (self.dx * self.dx)
+        s = 2.0 ** (levels - level)
+        return nu_phys * (dtf * s) / (self.dx * s) ** 2
 
-    def params(self) -> capi.Q19Params:
+    def params(self, level: int = 1, levels: int = 1) -> capi.Q19Params:
+        """The step parameters of level `level`: its viscosity, the body force in its lattice units
+        (x 2^(L - l), stream.jl:291-293) and the momentum-exchange scale 8^(1 - l) (coupling.jl:246)."""
         if self.sgs not in SGS_CODES:
             raise ValueError(f"unknown sgs model {self.sgs!r}")
         p = capi.Q19Params()
         check(lib().oal_q19_default_params(C.byref(p)))
-        p.nu = self.level_nu()
+        p.nu = self.level_nu(level, levels)
         p.u_inlet[0] = self.u_lattice          # st.u_inlet * inlet_dir, inlet along +x (state.jl:255)
-        p.force_scale = 1.0
+        p.force_scale = 8.0 ** (1 - level)
         p.sgs = SGS_CODES[self.sgs]
         p.c_wale = self.c_wale
         p.c_smagorinsky = self.c_smagorinsky
         p.hrr_sigma = self.hrr_sigma
+        fs = 2.0 ** (levels - level)
         for a in range(3):
-            p.body_force[a] = float(self.body_force[a])
+            p.body_force[a] = float(self.body_force[a] * fs)
         return p
 
 
@@ -234,29 +331,67 @@ test_case_config.__test__ = False  # a configuration factory, not a pytest test
 class State:
     """The level's populations, velocity and density on the GPU (two buffers, swapped per step)."""
 
-    def __init__(self, mesh: PeriodicBox, cfg: CaseConfig, precision=None, device: int = 0):
+    def __init__(self, mesh, cfg: CaseConfig, precision=None, device: int = 0):
+        """`mesh`: a PeriodicBox, one level (Mesh) or an OctMesh; an OctMesh of several levels is
+        stepped as the reference's step_recursive! (the coarse step of advance!)."""
+        if isinstance(mesh, OctMesh) and mesh.nlevels == 1:
+            mesh = mesh.levels[0]
         self.mesh = mesh
         self.cfg = cfg
         self.dtype = np.dtype(precision or cfg.precision)
         if self.dtype not in _PRECISION:
             raise ValueError("precision must be float32 or float64")
-        self.params = cfg.params()
         self.step = 0
         self.mass0 = float("nan")
-        h = C.c_void_p()
-        if isinstance(mesh, Mesh):
-            self._desc = mesh.desc()
-            check(lib().oal_q19_level_create_desc(device, _PRECISION[self.dtype], C.byref(self._desc), C.byref(h)))
-        else:
-            check(lib().oal_q19_level_create(device, _PRECISION[self.dtype], mesh.nocts, _ptr(mesh.onbr), C.byref(h)))
-        self._h = h
         self.forces = np.zeros(3)
+        self._tree = None
+        h = C.c_void_p()
+        if isinstance(mesh, OctMesh):
+            L = mesh.nlevels
+            self.level_meshes = mesh.levels
+            self.level_params = [cfg.params(l, L) for l in range(1, L + 1)]
+            self._descs = (capi.Q19LevelDesc * L)(*[m.desc() for m in mesh.levels])
+            check(lib().oal_q19_octree_create(device, _PRECISION[self.dtype], L, self._descs, C.byref(h)))
+            self._tree = h
+            self._h = None
+        else:
+            self.level_meshes = [mesh]
+            self.level_params = [cfg.params()]
+            if isinstance(mesh, Mesh):
+                self._desc = mesh.desc()
+                check(lib().oal_q19_level_create_desc(device, _PRECISION[self.dtype], C.byref(self._desc), C.byref(h)))
+            else:
+                check(lib().oal_q19_level_create(device, _PRECISION[self.dtype], mesh.nocts, _ptr(mesh.onbr), C.byref(h)))
+            self._h = h
+
+    @property
+    def params(self):
+        """The parameters of the single level (the finest level's of a refined mesh)."""
+        return self.level_params[-1]
+
+    @params.setter
+    def params(self, p):
+        self.level_params[-1] = p
+
+    @property
+    def nlevels(self) -> int:
+        return len(self.level_meshes)
+
+    def _level_handle(self, level: int):
+        if self._tree is None:
+            return self._h
+        h = C.c_void_p()
+        check(lib().oal_q19_octree_level(self._tree, level, C.byref(h)))
+        return h
 
     # -- lifetime
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
             lib().oal_q19_level_destroy(self._h)
             self._h = None
+        if getattr(self, "_tree", None) is not None and self._tree.value:
+            lib().oal_q19_octree_destroy(self._tree)
+            self._tree = None
 
     def __del__(self):
         try:
@@ -266,6 +401,8 @@ class State:
 
     # -- initial state
     def _upload(self, rho, u, du):
+        if self._tree is not None:
+            return self._upload_levels([(rho, u, du)] if not isinstance(rho, list) else list(zip(rho, u, du)))
         rho = np.ascontiguousarray(rho, self.dtype)
         u = np.ascontiguousarray(u, self.dtype)
         du = None if du is None else np.ascontiguousarray(du, self.dtype)
@@ -273,17 +410,31 @@ class State:
         self.step = 0
         self.mass0 = self.total_mass()
 
-    def initial_fields(self, init, nonequilibrium: bool = True):
+    def _upload_levels(self, fields):
+        keep = [tuple(None if a is None else np.ascontiguousarray(a, self.dtype) for a in f) for f in fields]
+        L = self.nlevels
+        P = (capi.Q19Params * L)(*self.level_params)
+        ptrs = [(C.c_void_p * L)(*[(k[i].ctypes.data if k[i] is not None else None) for k in keep]) for i in range(3)]
+        check(lib().oal_q19_octree_initialise(self._tree, P, ptrs[0], ptrs[1],
+                                              ptrs[2] if any(k[2] is not None for k in keep) else None))
+        self.step = 0
+        self.mass0 = self.total_mass()
+
+    def initial_fields(self, init, nonequilibrium: bool = True, level: int = None):
         """(rho (nocts,8), u (nocts,3,8), du (nocts,9,8) or None) of `init` at the slot centres, in the
-        level's precision, as state.jl:267-305 forms them (du over one cell, evaluated in Float64)."""
-        p = self.mesh.slot_centres()
+        level's precision, as state.jl:267-305 forms them (du over one cell, evaluated in Float64).
+        A refined mesh gives one such tuple per level (level=None) or that of `level`."""
+        if self._tree is not None and level is None:
+            return [self.initial_fields(init, nonequilibrium, l) for l in range(1, self.nlevels + 1)]
+        mesh = self.level_meshes[(level or 1) - 1]
+        p = mesh.slot_centres()
         x, y, z = p[:, 0], p[:, 1], p[:, 2]
         rho, ux, uy, uz = (np.broadcast_to(np.asarray(v, np.float64), x.shape) for v in init(x, y, z))
         u = np.stack([ux, uy, uz], 1)
         du = None
         if nonequilibrium:
-            h = self.mesh.dx / 2
-            du = np.zeros((self.mesh.nocts, 9, 8), np.float64)
+            h = mesh.dx / 2
+            du = np.zeros((mesh.nocts, 9, 8), np.float64)
             for a in range(3):
                 e = [0.0, 0.0, 0.0]
                 e[a] = h
@@ -295,54 +446,79 @@ class State:
         return rho.astype(self.dtype), u.astype(self.dtype), du
 
     def initialise(self, init, nonequilibrium: bool = True):
-        self._upload(*self.initial_fields(init, nonequilibrium))
+        f = self.initial_fields(init, nonequilibrium)
+        if self._tree is not None:
+            self._upload_levels(f)
+        else:
+            self._upload(*f)
         return self
 
     def initialise_uniform(self, rho0: float, ux0: float, uy0: float, uz0: float):
-        no = self.mesh.nocts
-        rho = np.full((no, 8), rho0, self.dtype)
-        u = np.empty((no, 3, 8), self.dtype)
-        u[:, 0], u[:, 1], u[:, 2] = self.dtype.type(ux0), self.dtype.type(uy0), self.dtype.type(uz0)
-        self._upload(rho, u, None)
+        fields = []
+        for m in self.level_meshes:
+            rho = np.full((m.nocts, 8), rho0, self.dtype)
+            u = np.empty((m.nocts, 3, 8), self.dtype)
+            u[:, 0], u[:, 1], u[:, 2] = self.dtype.type(ux0), self.dtype.type(uy0), self.dtype.type(uz0)
+            fields.append((rho, u, None))
+        if self._tree is not None:
+            self._upload_levels(fields)
+        else:
+            self._upload(*fields[0])
         return self
 
     # -- stepping
     def advance(self, n: int = 1, stream=None, collect: bool = False):
-        """n steps (advance! n times); with `collect` the last step's momentum exchange is kept in
-        `forces` (lattice units, FP64)."""
+        """n coarse steps (advance! n times); with `collect` the last coarse step's momentum exchange
+        (every level and sub-step) is kept in `forces` (coarse-lattice units, FP64)."""
         st = None if stream is None else C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else stream)
-        check(lib().oal_q19_level_advance(self._h, C.byref(self.params), int(n), int(bool(collect)), st))
+        if self._tree is not None:
+            P = (capi.Q19Params * self.nlevels)(*self.level_params)
+            check(lib().oal_q19_octree_advance(self._tree, P, int(n), int(bool(collect)), st))
+        else:
+            check(lib().oal_q19_level_advance(self._h, C.byref(self.params), int(n), int(bool(collect)), st))
         self.step += n
         if collect and n > 0:
             out = (C.c_double * 3)()
-            check(lib().oal_q19_level_forces(self._h, out, None))
+            if self._tree is not None:
+                check(lib().oal_q19_octree_forces(self._tree, out, None))
+            else:
+                check(lib().oal_q19_level_forces(self._h, out, None))
             self.forces = np.array(out[:])
         return self
 
     def forces_per_triangle(self) -> np.ndarray:
-        ntri = max(getattr(self.mesh, "ntri", 0), 1)
+        ntri = max(max(getattr(m, "ntri", 0) for m in self.level_meshes), 1)
         out = np.zeros((ntri, 3))
-        check(lib().oal_q19_level_forces(self._h, None, out.ctypes.data_as(C.c_void_p)))
+        if self._tree is not None:
+            check(lib().oal_q19_octree_forces(self._tree, None, out.ctypes.data_as(C.c_void_p)))
+        else:
+            check(lib().oal_q19_level_forces(self._h, None, out.ctypes.data_as(C.c_void_p)))
         return out
 
     # -- read-out
-    def state(self):
-        no = self.mesh.nocts
+    def state(self, level: int = 1):
+        """(f, u, rho) of `level` in the reference's layout (host copies)."""
+        no = self.level_meshes[level - 1].nocts
         f = np.empty((no, 19, 8), self.dtype)
         u = np.empty((no, 3, 8), self.dtype)
         rho = np.empty((no, 8), self.dtype)
-        check(lib().oal_q19_level_get_state(self._h, _ptr(f), _ptr(u), _ptr(rho)))
+        check(lib().oal_q19_level_get_state(self._level_handle(level), _ptr(f), _ptr(u), _ptr(rho)))
         return f, u, rho
 
-    def set_state(self, f, u, rho):
+    def set_state(self, f, u, rho, level: int = 1):
         f = np.ascontiguousarray(f, self.dtype)
         u = np.ascontiguousarray(u, self.dtype)
         rho = np.ascontiguousarray(rho, self.dtype)
-        check(lib().oal_q19_level_set_state(self._h, _ptr(f), _ptr(u), _ptr(rho)))
+        check(lib().oal_q19_level_set_state(self._level_handle(level), _ptr(f), _ptr(u), _ptr(rho)))
 
     def totals(self) -> np.ndarray:
+        """FP64 {mass, momentum, kinetic energy} over the fluid leaves, each level weighted by its
+        volume in finest cells, 8^(L - l) (state.jl:333-356)."""
         out = (C.c_double * 5)()
-        check(lib().oal_q19_level_totals(self._h, out, None))
+        if self._tree is not None:
+            check(lib().oal_q19_octree_totals(self._tree, out))
+        else:
+            check(lib().oal_q19_level_totals(self._h, out, None))
         return np.array(out[:])
 
     def total_mass(self) -> float:
@@ -354,10 +530,11 @@ class State:
     def kinetic_energy(self) -> float:
         return float(self.totals()[4])
 
-    def device_state(self):
+    def device_state(self, level: int = 1):
         f, u, rho = C.c_void_p(), C.c_void_p(), C.c_void_p()
         steps = C.c_int64()
-        check(lib().oal_q19_level_device_state(self._h, C.byref(f), C.byref(u), C.byref(rho), C.byref(steps)))
+        check(lib().oal_q19_level_device_state(self._level_handle(level), C.byref(f), C.byref(u), C.byref(rho),
+                                               C.byref(steps)))
         return f.value, u.value, rho.value, steps.value
 
 

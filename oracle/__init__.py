@@ -57,6 +57,9 @@ def lib() -> C.CDLL:
             getattr(L, f"ora_q19_step_walls_{suf}").argtypes = [vp] * 9
             getattr(L, f"ora_q19_initialise_{suf}").argtypes = [i64, vp, vp, vp, vp, C.c_double, vp, vp, vp]
         L.ora_q19_forces.argtypes = [vp, vp, vp, vp]
+        for suf in ("f32", "f64"):
+            getattr(L, f"ora_q19_fill_{suf}").argtypes = [vp, vp, vp, vp, C.c_double, C.c_double, C.c_double, vp, vp, vp]
+            getattr(L, f"ora_q19_restrict_{suf}").argtypes = [vp, vp, C.c_double, C.c_double, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -215,7 +218,9 @@ class OracleQ19Level:
         self.v[...] = self.u
         self.rhob[...] = self.rho
 
-    def step(self, params, n=1, collect=False):
+    def step(self, params, n=1, collect=False, accumulate=False):
+        """n steps; with `collect` the last step's momentum exchange is kept (added to the previous
+        collection when `accumulate`, as the sub-steps of a refined level add up)."""
         suf = _suffix(self.dtype)
         for s in range(n):
             if self.desc is None:
@@ -223,6 +228,8 @@ class OracleQ19Level:
                                                       _p(self.g), _p(self.u), _p(self.v), _p(self.rho), _p(self.rhob))
             else:
                 mom = self.mom if (collect and s == n - 1) else None
+                if mom is not None and not accumulate:
+                    mom[...] = 0.0
                 getattr(lib(), f"ora_q19_step_walls_{suf}")(C.addressof(self.desc), C.addressof(params), _p(self.f),
                                                             _p(self.g), _p(self.u), _p(self.v), _p(self.rho),
                                                             _p(self.rhob), _p(mom))
@@ -243,3 +250,92 @@ class OracleQ19Level:
             u = u * fl[:, None, :]
         return np.array([r.sum(), (r * u[:, 0]).sum(), (r * u[:, 1]).sum(), (r * u[:, 2]).sum(),
                          0.5 * (r * (u ** 2).sum(1)).sum()])
+
+
+class OracleQ19Octree:
+    """Several octree levels coupled by the oracle's transfers, stepped as the reference's
+    step_recursive! (coupling.jl:240-254); `descs` are the levels' descriptors (kept alive by the
+    caller), `params` one oal_q19_params per level."""
+
+    def __init__(self, descs, onbrs, dtype=np.float32):
+        self.dtype = np.dtype(dtype)
+        self.descs = descs
+        self.levels = [OracleQ19Level(o, dtype, desc=d) for o, d in zip(onbrs, descs)]
+        self.L = len(self.levels)
+        self.ghosts = [np.ctypeslib.as_array((C.c_int32 * d.nghost).from_address(d.ghost_slot)).copy() - 1
+                       if d.nghost else np.zeros(0, np.int64) for d in descs]
+        self.forces = np.zeros(3)
+        self.per_tri = None
+
+    def _fill(self, l, weight, params):
+        F, Cl = self.levels[l - 1], self.levels[l - 2]
+        getattr(lib(), f"ora_q19_fill_{_suffix(self.dtype)}")(
+            C.addressof(self.descs[l - 1]), _p(Cl.kind), _p(Cl.f), _p(Cl.g), float(weight), float(params[l - 2].nu),
+            float(params[l - 1].nu), _p(F.f), _p(F.u), _p(F.rho))
+
+    def _restrict(self, l, params):
+        Cl, F = self.levels[l - 1], self.levels[l]
+        getattr(lib(), f"ora_q19_restrict_{_suffix(self.dtype)}")(
+            C.addressof(self.descs[l - 1]), _p(F.f), float(params[l - 1].nu), float(params[l].nu), _p(Cl.f), _p(Cl.u),
+            _p(Cl.rho))
+
+    def _copy_ghosts(self, l):
+        if l == self.L or not len(self.ghosts[l - 1]):
+            return
+        S = self.levels[l - 1]
+        o, k = self.ghosts[l - 1] // 8, self.ghosts[l - 1] % 8
+        S.f[o, :, k] = S.g[o, :, k]
+        S.u[o, :, k] = S.v[o, :, k]
+        S.rho[o, k] = S.rhob[o, k]
+
+    @staticmethod
+    def _mirror(S):
+        S.g[...] = S.f
+        S.v[...] = S.u
+        S.rhob[...] = S.rho
+
+    def initialise(self, params, fields):
+        """fields[l] = (rho, u, du) of level l + 1; then couple_initial! (coupling.jl:257-268)."""
+        for S, p, (rho, u, du) in zip(self.levels, params, fields):
+            S.initialise(p, rho, u, du)
+        for l in range(self.L - 1, 0, -1):
+            self._restrict(l, params)
+            self._mirror(self.levels[l - 1])
+        for l in range(2, self.L + 1):
+            self._fill(l, 1.0, params)
+            self._mirror(self.levels[l - 1])
+
+    def _step_recursive(self, l, params, collect):
+        self.levels[l - 1].step(params[l - 1], 1, collect=collect, accumulate=True)
+        self._copy_ghosts(l)
+        if l < self.L:
+            self._step_recursive(l + 1, params, collect)
+            self._restrict(l, params)
+            self._fill(l + 1, 0.5, params)
+            self._step_recursive(l + 1, params, collect)
+            self._restrict(l, params)
+            self._fill(l + 1, 1.0, params)
+
+    def advance(self, params, n=1, collect=False):
+        for s in range(n):
+            last = collect and s == n - 1
+            if last:
+                for S in self.levels:
+                    S.mom[...] = 0.0
+            self._step_recursive(1, params, last)
+            if last:
+                ntri = max(max(d.ntri for d in self.descs), 1)
+                self.per_tri = np.zeros((ntri, 3))
+                for S, d in zip(self.levels, self.descs):
+                    pt = np.zeros((max(d.ntri, 1), 3))
+                    tot = np.zeros(3)
+                    if d.nlinks:
+                        lib().ora_q19_forces(C.addressof(d), _p(S.mom), _p(pt), _p(tot))
+                    self.per_tri[:pt.shape[0]] += pt
+                self.forces = self.per_tri.sum(0)
+
+    def totals(self):
+        out = np.zeros(5)
+        for l, S in enumerate(self.levels, start=1):
+            out += 8.0 ** (self.L - l) * S.totals()
+        return out

@@ -389,7 +389,7 @@ void rebuild(T rho, T ux, T uy, T uz, const T* p, T omega, T* out) {
   }
 }
 
-// state.jl:267-305: per slot, the Chapman-Enskog non-equilibrium of the initial field (du given,
+// state.jl:267-305: per fluid, ghost or covered slot, the Chapman-Enskog non-equilibrium of the initial field (du given,
 // (8, 9, nocts) with du[k, 3a+b, o] = d u_b / d x_a over one cell) rebuilt at the level's omega,
 // or the equilibrium (du null). rho (8, nocts), u (8, 3, nocts), f (8, 19, nocts).
 template <class T>
@@ -401,7 +401,7 @@ void initialise(int64_t nslots, const uint8_t* kind, const T* rho_a, const T* u,
   for (int64_t s = 0; s < nslots; ++s) {
     const int64_t o = s / 8;
     const int k = (int)(s % 8);
-    if (kind && kind[s] != 1) {
+    if (kind && kind[s] != 1 && kind[s] != 3 && kind[s] != 4) {
       // slots without a state keep the allocation state (state.jl:217-232)
       for (int i = 0; i < Q; ++i) f[k + 8 * i + 152 * o] = T(0);
       for (int a = 0; a < 3; ++a) u_out[k + 8 * a + 24 * o] = T(0);
@@ -545,10 +545,11 @@ void step_level_walls(const oal_q19_level_desc& d, const oal_q19_params& P, cons
           }
         }
         if (mom && ci != 0) {
-          // momentum exchange per cut link: scale (f_i* + f_j(t+1)), i toward the wall (stream.jl:248-256)
+          // momentum exchange per cut link, added up over the collecting steps: scale (f_i* + f_j(t+1)),
+          // i toward the wall (stream.jl:248-256)
           for (int li = d.cut_off[ci - 1] - 1; li < d.cut_off[ci] - 1; ++li) {
             const int i = d.cut_dir[li] - 1, j = opp_of(i);
-            mom[li] = P.force_scale * (double)(fo[i] + f[j]);
+            mom[li] += P.force_scale * (double)(fo[i] + f[j]);
           }
         }
       }
@@ -588,9 +589,131 @@ void step_level_walls(const oal_q19_level_desc& d, const oal_q19_params& P, cons
   (void)nslots;
 }
 
+// ---- transfers between levels (coupling.jl:16-238) -------------------------------------------
+
+template <class T>
+void slot_moments(const T* f, int64_t s, T* m) {  // coupling.jl:16-23
+  const int64_t o = s / 8;
+  const int k = (int)(s % 8);
+  T fs[Q];
+  for (int i = 0; i < Q; ++i) fs[i] = f[k + 8 * i + 152 * o];
+  T drho, mx, my, mz, P[6];
+  moments_q19<T>(fs, drho, mx, my, mz, P);
+  const T rho = drho + T(1), inv = T(1) / rho;
+  const T ux = mx * inv, uy = my * inv, uz = mz * inv;
+  T p[6];
+  pineq_q19<T>(drho, rho, ux, uy, uz, P, p);
+  m[0] = rho; m[1] = ux; m[2] = uy; m[3] = uz;
+  for (int i = 0; i < 6; ++i) m[4 + i] = p[i];
+}
+
+template <class T>
+T pre_collision_factor(T omega) {  // coupling.jl:32-35
+  return std::abs(T(1) - omega) > T(0.05) ? T(1) / (T(1) - omega) : T(0);
+}
+
+template <class T>
+void write_rebuilt(const T* acc, T scale, T omega, int64_t s, T* f, T* u, T* rho) {
+  const T p[6] = {scale * acc[4], scale * acc[5], scale * acc[6], scale * acc[7], scale * acc[8], scale * acc[9]};
+  T out[Q];
+  rebuild<T>(acc[0], acc[1], acc[2], acc[3], p, omega, out);
+  const int64_t o = s / 8;
+  const int k = (int)(s % 8);
+  for (int i = 0; i < Q; ++i) f[k + 8 * i + 152 * o] = out[i];
+  u[k + 24 * o] = acc[1]; u[k + 8 + 24 * o] = acc[2]; u[k + 16 + 24 * o] = acc[3];
+  rho[s] = acc[0];
+}
+
+// fill_ghosts! (coupling.jl:134-174): the ghosts of the fine level from the coarse buffers at `weight`
+template <class T>
+void fill_ghosts(const oal_q19_level_desc& F, const uint8_t* ckind, const T* cnew, const T* cold, T weight,
+                 double nu_c, double nu_f, T* ff, T* fu, T* fr) {
+  const T omega_c = omega_of<T>(T(nu_c)), omega_f = omega_of<T>(T(nu_f));
+  const T tau_c = T(1) / omega_c, tau_f = T(1) / omega_f;
+  const T scale = tau_f / (T(2) * tau_c) * pre_collision_factor<T>(omega_c);
+  const T w1 = weight, w0 = T(1) - weight;
+#pragma omp parallel for schedule(static)
+  for (int g = 0; g < F.nghost; ++g) {
+    T acc[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int n = 0; n < 64; ++n) {
+      const int d = F.ghost_donor[64 * (int64_t)g + n];
+      if (!d) continue;
+      const int64_t ds = d - 1;
+      T m[10];
+      if (w1 == T(0)) {
+        slot_moments<T>(cold, ds, m);
+      } else if (w0 == T(0) || (ckind && ckind[ds] == 3)) {
+        slot_moments<T>(cnew, ds, m);  // covered donors hold the fine average and enter unblended
+      } else {
+        T mn[10], mo[10];
+        slot_moments<T>(cnew, ds, mn);
+        slot_moments<T>(cold, ds, mo);
+        for (int i = 0; i < 10; ++i) m[i] = w0 * mo[i] + w1 * mn[i];
+      }
+      const T wn = T(F.ghost_w[64 * (int64_t)g + n]);
+      for (int i = 0; i < 10; ++i) acc[i] += wn * m[i];
+    }
+    write_rebuilt<T>(acc, scale, omega_f, F.ghost_slot[g] - 1, ff, fu, fr);
+  }
+}
+
+// restrict! (coupling.jl:176-207): the restricted slots of the coarse level from the fine buffer
+template <class T>
+void restrict_level(const oal_q19_level_desc& C, const T* ff, double nu_c, double nu_f, T* cf, T* cu, T* cr) {
+  const T omega_c = omega_of<T>(T(nu_c)), omega_f = omega_of<T>(T(nu_f));
+  const T tau_c = T(1) / omega_c, tau_f = T(1) / omega_f;
+  const T scale = T(2) * tau_c / tau_f * pre_collision_factor<T>(omega_f);
+  double w1d[4];
+  {
+    const double t = 0.5;  // cubic_weights(0.5) (octree.jl:84-86)
+    w1d[0] = -t * (1 - t) * (2 - t) / 6; w1d[1] = (1 + t) * (1 - t) * (2 - t) / 2;
+    w1d[2] = (1 + t) * t * (2 - t) / 2; w1d[3] = -(1 + t) * t * (1 - t) / 6;
+  }
+#pragma omp parallel for schedule(static)
+  for (int r = 0; r < C.nrestrict; ++r) {
+    T acc[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (C.restrict_cubic[r]) {
+      for (int n = 0; n < 64; ++n) {
+        const T wn = T(w1d[n & 3] * w1d[(n >> 2) & 3] * w1d[n >> 4]);
+        T m[10];
+        slot_moments<T>(ff, C.restrict_src[64 * (int64_t)r + n] - 1, m);
+        for (int i = 0; i < 10; ++i) acc[i] += wn * m[i];
+      }
+    } else {
+      int cnt = 0;
+      for (int mm = 0; mm < 8; ++mm) {  // STENCIL_INNER order (octree.jl:82)
+        const int nidx = (1 + (mm & 1)) + 4 * (1 + ((mm >> 1) & 1)) + 16 * (1 + ((mm >> 2) & 1));
+        const int d = C.restrict_src[64 * (int64_t)r + nidx];
+        if (!d) continue;
+        T m[10];
+        slot_moments<T>(ff, d - 1, m);
+        for (int i = 0; i < 10; ++i) acc[i] += m[i];
+        ++cnt;
+      }
+      if (cnt == 0) continue;
+      const T inv = T(1) / T(cnt);
+      for (int i = 0; i < 10; ++i) acc[i] *= inv;
+    }
+    write_rebuilt<T>(acc, scale, omega_c, C.restrict_slot[r] - 1, cf, cu, cr);
+  }
+}
+
 }  // namespace
 
 extern "C" {
+
+#define ORA_Q19_TRANSFER(T, SUF)                                                                              \
+  void ora_q19_fill_##SUF(const oal_q19_level_desc* F, const uint8_t* ckind, const T* cnew, const T* cold,     \
+                          double weight, double nu_c, double nu_f, T* ff, T* fu, T* fr) {                     \
+    fill_ghosts<T>(*F, ckind, cnew, cold, T(weight), nu_c, nu_f, ff, fu, fr);                                 \
+  }                                                                                                           \
+  void ora_q19_restrict_##SUF(const oal_q19_level_desc* C, const T* ff, double nu_c, double nu_f, T* cf, T* cu, \
+                              T* cr) {                                                                        \
+    restrict_level<T>(*C, ff, nu_c, nu_f, cf, cu, cr);                                                        \
+  }
+ORA_Q19_TRANSFER(float, f32)
+ORA_Q19_TRANSFER(double, f64)
+#undef ORA_Q19_TRANSFER
 
 // per-triangle force in link order (no triangle -> bin 1) and the total as a plain sum over the bins
 void ora_q19_forces(const oal_q19_level_desc* d, const double* mom, double* per_tri, double* total) {

@@ -266,7 +266,7 @@ def channel(n, H, angle_deg, seed):
         tris.append(rot(octree.box_triangles(lo, hi)) + c)
     spec = octree.MeshSpec(domain=(Lx, Ly, Lz), periodic=(True, False, False),
                            faces=("periodic", "periodic", "slip", "slip", "slip", "slip"))
-    return octree.generate(np.concatenate(tris), spec), c, np.array([0.0, -math.sin(a), math.cos(a)])
+    return octree.generate(np.concatenate(tris), spec).levels[0], c, np.array([0.0, -math.sin(a), math.cos(a)])
 
 
 def obstacle_box_mesh():
@@ -275,7 +275,7 @@ def obstacle_box_mesh():
     tri = octree.box_triangles((5.3, 4.6, 3.7), (9.1, 7.4, 8.2))
     spec = octree.MeshSpec(domain=(16.0, 12.0, 12.0), faces=("inlet", "outlet", "noslip", "freestream",
                                                                "symmetry", "ground"))
-    return octree.generate(tri, spec)
+    return octree.generate(tri, spec).levels[0]
 
 
 def mesh_invariants(m):
