@@ -327,6 +327,10 @@ def main():
             for r in q:
                 r["roofline_frac"] = round(r["achieved_gbs"] / peak, 4)
             line["octree_q19"] = q
+            from openaerolab_alpha_01_b200.octree import benchmark_naca
+            c3 = benchmark_naca(steps=args.q19_steps)
+            c3["roofline_frac"] = round(c3["achieved_gbs"] / peak, 4)
+            line["octree_config3"] = c3
         if args.batch_steps > 0:
             from openaerolab_alpha_01_b200.workloads import config4
             line["batched"] = config4(steps=args.batch_steps, storage=args.storage)

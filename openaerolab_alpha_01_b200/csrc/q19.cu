@@ -427,9 +427,19 @@ __global__ void __launch_bounds__(kThreads) k_q19_step(const LevelArgs<T> a) {
   store_cell<T>(a, o, k, out, rho, ux, uy, uz);
 }
 
+// fo[m] for a runtime m by selects (keeps the populations in registers)
+template <class T>
+__device__ __forceinline__ T select_dir(const T* fo, int m) {
+  T v = fo[0];
+#pragma unroll
+  for (int t = 1; t < Q; ++t) v = m == t ? fo[t] : v;
+  return v;
+}
+
 // the population j arriving from a domain-boundary slot with face mask `mask` (stream.jl:32-78)
 template <class T>
-__device__ T face_population(const WallArgs<T>& w, uint32_t mask, int j, const T* fo, T rho, T ux, T uy, T uz) {
+__device__ __forceinline__ T face_population(const WallArgs<T>& w, uint32_t mask, int j, const T* fo, T rho, T ux, T uy,
+                                             T uz) {
   const int i = opp(j);
   auto feq_s = [](int d, T r, T vx, T vy, T vz, T vsq) { return feq_shifted<T>(d, r, vx, vy, vz, vsq); };
   auto dirichlet = [&](int cond) {
@@ -450,7 +460,7 @@ __device__ T face_population(const WallArgs<T>& w, uint32_t mask, int j, const T
     const int f = __ffs(mask) - 1;
     const int cond = w.faces[f];
     if (cond == OAL_Q19_FACE_NOSLIP || cond == OAL_Q19_FACE_GROUND) return fo[i];
-    if (cond == OAL_Q19_FACE_SLIP || cond == OAL_Q19_FACE_SYMMETRY) return fo[mirror(j, f >> 1)];
+    if (cond == OAL_Q19_FACE_SLIP || cond == OAL_Q19_FACE_SYMMETRY) return select_dir<T>(fo, mirror(j, f >> 1));
     return dirichlet(cond);
   }
   bool wall = false, open = false;
@@ -466,7 +476,7 @@ __device__ T face_population(const WallArgs<T>& w, uint32_t mask, int j, const T
   if (mask & 0x03u) m = mirror(m, 0);
   if (mask & 0x0cu) m = mirror(m, 1);
   if (mask & 0x30u) m = mirror(m, 2);
-  return fo[m];
+  return select_dir<T>(fo, m);
 }
 
 // octs with a non-fluid slot or a special direction: fluid slots step with the face conditions, the
@@ -504,6 +514,7 @@ __global__ void __launch_bounds__(kThreads) k_q19_walls(const LevelArgs<T> a, co
     for (int i = 0; i < Q; ++i) fo[i] = a.fin[o * (8 * Q) + 8 * i + k];
     const T rho0 = a.rhoin[s], ux0 = a.uin[o * 24 + k], uy0 = a.uin[o * 24 + 8 + k], uz0 = a.uin[o * 24 + 16 + k];
     const int ci = w.cutidx[s] - 1;
+#pragma unroll
     for (int j = 0; j < Q; ++j) {
       int src, child;
       pull(j, src, child);
@@ -533,10 +544,16 @@ __global__ void __launch_bounds__(kThreads) k_q19_walls(const LevelArgs<T> a, co
       }
     }
     if (w.mom && ci >= 0) {
-      // momentum exchange on the cut links: (f_i* + f_j(t+1)) c_i per link, i toward the wall
-      for (int li = w.cut_off[ci] - 1; li < w.cut_off[ci + 1] - 1; ++li) {
-        const int i = w.cut_dir[li] - 1;
-        w.mom[li] += w.scale * (double)(fo[i] + f[opp(i)]);
+      // momentum exchange on the cut links: (f_i* + f_j(t+1)) c_i per link, i toward the wall; a cut
+      // cell's links are in direction order (checked at level creation)
+      int li = w.cut_off[ci] - 1;
+      const int end = w.cut_off[ci + 1] - 1;
+#pragma unroll
+      for (int i = 1; i < Q; ++i) {
+        if (li < end && w.cut_dir[li] - 1 == i) {
+          w.mom[li] += w.scale * (double)(fo[i] + f[opp(i)]);
+          ++li;
+        }
       }
     }
   }
@@ -1103,8 +1120,12 @@ static oal_status create_desc_impl(int32_t device, int32_t precision, const oal_
   if (d->ncut > 0) {
     if (d->cut_off[0] != 1 || d->cut_off[d->ncut] != d->nlinks + 1)
       return fail(OAL_E_INVALID_ARG, "cut_off must run from 1 to nlinks + 1");
-    for (int c = 0; c < d->ncut; ++c)
+    for (int c = 0; c < d->ncut; ++c) {
       if (d->cut_off[c + 1] < d->cut_off[c]) return fail(OAL_E_INVALID_ARG, "cut_off must not decrease");
+      for (int li = d->cut_off[c]; li < d->cut_off[c + 1] - 1; ++li)
+        if (d->cut_dir[li] <= d->cut_dir[li - 1])
+          return fail(OAL_E_INVALID_ARG, "the links of a cut cell must be in increasing direction order");
+    }
     for (int li = 0; li < d->nlinks; ++li) {
       if (d->cut_dir[li] < 2 || d->cut_dir[li] > 19) return fail(OAL_E_INVALID_ARG, "cut_dir %d", d->cut_dir[li]);
       if (!(d->cut_q[li] > 0 && d->cut_q[li] <= 1)) return fail(OAL_E_INVALID_ARG, "cut_q must lie in (0, 1]");
@@ -1457,24 +1478,32 @@ __device__ __forceinline__ void rebuild_slot(const T* acc, T scale, T omega, int
   rho[s] = r;
 }
 
-// ghost fill (fill_ghosts! stage 2): weighted sums of the donor moments, rebuilt at the fine omega
+// ghost fill (fill_ghosts! stage 2): weighted sums of the donor moments, rebuilt at the fine omega.
+// 16 lanes per ghost: lane q < 10 sums moment q over the 64 nodes in node order (the reference's
+// order per moment), lane 0 gathers the ten sums and rebuilds the slot.
 template <class T>
-__global__ void k_q19_fill(int32_t ng, const int32_t* __restrict__ ghost_slot, const int32_t* __restrict__ dix,
-                           const float* __restrict__ gw, const T* __restrict__ dm, T scale, T omega, T* f, T* u, T* rho) {
-  const int32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= ng) return;
-  T acc[10];
-#pragma unroll
-  for (int i = 0; i < 10; ++i) acc[i] = T(0);
-  for (int n = 0; n < 64; ++n) {
-    const int32_t d = dix[64 * (int64_t)g + n];
-    if (!d) continue;
-    const T wn = T(gw[64 * (int64_t)g + n]);
-    const T* m = dm + 10 * (int64_t)(d - 1);
-#pragma unroll
-    for (int i = 0; i < 10; ++i) acc[i] += wn * m[i];
+__global__ void __launch_bounds__(256) k_q19_fill(int32_t ng, const int32_t* __restrict__ ghost_slot,
+                                                  const int32_t* __restrict__ dix, const float* __restrict__ gw,
+                                                  const T* __restrict__ dm, T scale, T omega, T* f, T* u, T* rho) {
+  const int lane = threadIdx.x & 31, q = lane & 15;
+  const int64_t g = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
+  if (g >= ng) return;  // both lanes groups of a warp test their own g; a group leaves as a whole
+  const unsigned gmask = 0xffffu << (lane & 16);
+  T acc = T(0);
+  if (q < 10) {
+    const int32_t* dx = dix + 64 * g;
+    const float* w = gw + 64 * g;
+#pragma unroll 8
+    for (int n = 0; n < 64; ++n) {
+      const int32_t d = __ldg(dx + n);
+      if (!d) continue;
+      acc += T(__ldg(w + n)) * __ldg(dm + 10 * (int64_t)(d - 1) + q);
+    }
   }
-  rebuild_slot<T>(acc, scale, omega, ghost_slot[g], f, u, rho);
+  T m[10];
+#pragma unroll
+  for (int i = 0; i < 10; ++i) m[i] = __shfl_sync(gmask, acc, (lane & 16) + i);
+  if (q == 0) rebuild_slot<T>(m, scale, omega, ghost_slot[g], f, u, rho);
 }
 
 // the ten moments of the restriction sources from the fine buffer (restrict! stage 1)
@@ -1494,39 +1523,42 @@ __device__ __forceinline__ int stencil_inner_node(int m) {
   return (1 + (m & 1)) + 4 * (1 + ((m >> 1) & 1)) + 16 * (1 + ((m >> 2) & 1));
 }
 
-// restriction (restrict! stage 2): cubic weights over 64 sources, or the admissible children averaged
+// restriction (restrict! stage 2): cubic weights over 64 sources, or the admissible children
+// averaged; 16 lanes per restricted slot, lane q < 10 sums moment q in the reference's node order
 template <class T>
-__global__ void k_q19_restrict(int32_t nr, const int32_t* __restrict__ rslot, const int32_t* __restrict__ six,
-                               const uint8_t* __restrict__ cubic, const T* __restrict__ rm, T scale, T omega, T* f, T* u,
-                               T* rho) {
-  const int32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) k_q19_restrict(int32_t nr, const int32_t* __restrict__ rslot,
+                                                      const int32_t* __restrict__ six, const uint8_t* __restrict__ cubic,
+                                                      const T* __restrict__ rm, T scale, T omega, T* f, T* u, T* rho) {
+  const int lane = threadIdx.x & 31, q = lane & 15;
+  const int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
   if (r >= nr) return;
-  T acc[10];
-#pragma unroll
-  for (int i = 0; i < 10; ++i) acc[i] = T(0);
+  const unsigned gmask = 0xffffu << (lane & 16);
+  const int32_t* sx = six + 64 * r;
+  T acc = T(0);
+  int cnt = 0;
   if (cubic[r]) {
-    for (int n = 0; n < 64; ++n) {
-      const T wn = T(restrict_w1(n & 3) * restrict_w1((n >> 2) & 3) * restrict_w1(n >> 4));
-      const T* m = rm + 10 * (int64_t)(six[64 * (int64_t)r + n] - 1);
-#pragma unroll
-      for (int i = 0; i < 10; ++i) acc[i] += wn * m[i];
+    if (q < 10) {
+#pragma unroll 8
+      for (int n = 0; n < 64; ++n) {
+        const T wn = T(restrict_w1(n & 3) * restrict_w1((n >> 2) & 3) * restrict_w1(n >> 4));
+        acc += wn * __ldg(rm + 10 * (int64_t)(__ldg(sx + n) - 1) + q);
+      }
     }
   } else {
-    int cnt = 0;
-    for (int mm = 0; mm < 8; ++mm) {
-      const int32_t d = six[64 * (int64_t)r + stencil_inner_node(mm)];
-      if (!d) continue;
-      const T* m = rm + 10 * (int64_t)(d - 1);
 #pragma unroll
-      for (int i = 0; i < 10; ++i) acc[i] += m[i];
+    for (int mm = 0; mm < 8; ++mm) {
+      const int32_t d = __ldg(sx + stencil_inner_node(mm));
+      if (!d) continue;
+      if (q < 10) acc += __ldg(rm + 10 * (int64_t)(d - 1) + q);
       ++cnt;
     }
-    if (cnt == 0) return;
-    const T inv = T(1) / T(cnt);
-#pragma unroll
-    for (int i = 0; i < 10; ++i) acc[i] *= inv;
+    if (cnt == 0) return;  // uniform over the group: nothing to restrict
+    acc *= T(1) / T(cnt);
   }
-  rebuild_slot<T>(acc, scale, omega, rslot[r], f, u, rho);
+  T m[10];
+#pragma unroll
+  for (int i = 0; i < 10; ++i) m[i] = __shfl_sync(gmask, acc, (lane & 16) + i);
+  if (q == 0) rebuild_slot<T>(m, scale, omega, rslot[r], f, u, rho);
 }
 
 // copy slots (the last ghost fill) from the old buffers into the new ones (copy_ghosts!)
@@ -1588,6 +1620,15 @@ struct Transfer {
 
 }  // namespace
 
+// two coarse steps captured as one CUDA graph: after them every level is back on the buffers it
+// started from (level l steps 2^l times), so the graph replays as long as the parameters and the
+// coarsest level's starting buffer are those it was captured with
+struct CoarseGraph {
+  cudaGraphExec_t exec = nullptr;
+  std::vector<char> key;  // parameters of every level
+  int parity = -1;        // the coarsest level's current buffer at capture
+};
+
 struct oal_q19_octree {
   int device = 0;
   int precision = OAL_STORE_F32;
@@ -1599,6 +1640,8 @@ struct oal_q19_octree {
   double* tri_total = nullptr;  // (ntri, 3) then the total (3)
   double* part = nullptr;       // per-level totals (5 L)
   bool forces_valid = false;
+  cudaStream_t capture = nullptr;  // private stream the graphs are captured on
+  CoarseGraph graphs[2];           // one per starting parity of the coarsest level
 };
 
 namespace {
@@ -1627,7 +1670,7 @@ cudaError_t fill_ghosts_t(oal_q19_octree* tr, const oal_q19_params* p, int l, T 
   const int mode = w1 == T(0) ? 0 : (w0 == T(0) ? 1 : 2);
   k_q19_donor_moments<T><<<(t.nd + 127) / 128, 128, 0, st>>>(t.nd, t.dcells, (const T*)Lc->f[Lc->cur],
                                                              (const T*)Lc->f[1 - Lc->cur], mode, w0, w1, t.dcov, (T*)t.dm);
-  k_q19_fill<T><<<(t.ng + 127) / 128, 128, 0, st>>>(t.ng, t.ghost_slot, t.dix, t.gw, (const T*)t.dm, scale, omega_f,
+  k_q19_fill<T><<<(unsigned)((16 * (int64_t)t.ng + 255) / 256), 256, 0, st>>>(t.ng, t.ghost_slot, t.dix, t.gw, (const T*)t.dm, scale, omega_f,
                                                     (T*)Lf->f[Lf->cur], (T*)Lf->u[Lf->cur], (T*)Lf->rho[Lf->cur]);
   return cudaGetLastError();
 }
@@ -1642,7 +1685,7 @@ cudaError_t restrict_t(oal_q19_octree* tr, const oal_q19_params* p, int l, cudaS
   const T tau_c = T(1) / omega_c, tau_f = T(1) / omega_f;
   const T scale = T(2) * tau_c / tau_f * pre_collision_factor_h<T>(omega_f);
   k_q19_source_moments<T><<<(t.ns + 127) / 128, 128, 0, st>>>(t.ns, t.scells, (const T*)Lf->f[Lf->cur], (T*)t.rm);
-  k_q19_restrict<T><<<(t.nr + 127) / 128, 128, 0, st>>>(t.nr, t.rslot, t.six, t.rcubic, (const T*)t.rm, scale, omega_c,
+  k_q19_restrict<T><<<(unsigned)((16 * (int64_t)t.nr + 255) / 256), 256, 0, st>>>(t.nr, t.rslot, t.six, t.rcubic, (const T*)t.rm, scale, omega_c,
                                                         (T*)Lc->f[Lc->cur], (T*)Lc->u[Lc->cur], (T*)Lc->rho[Lc->cur]);
   return cudaGetLastError();
 }
@@ -1674,9 +1717,58 @@ cudaError_t step_recursive_t(oal_q19_octree* tr, const oal_q19_params* p, int l,
   return e;
 }
 
+// the graph of two non-collecting coarse steps for the current parity and parameters
+template <class T>
+cudaError_t coarse_graph(oal_q19_octree* tr, const oal_q19_params* p, cudaGraphExec_t* out) {
+  const int parity = tr->lv[0]->cur;
+  CoarseGraph& g = tr->graphs[parity];
+  const char* kp = reinterpret_cast<const char*>(p);
+  const size_t kn = sizeof(oal_q19_params) * (size_t)tr->L;
+  if (g.exec && g.parity == parity && g.key.size() == kn && std::memcmp(g.key.data(), kp, kn) == 0) {
+    *out = g.exec;
+    return cudaSuccess;
+  }
+  if (g.exec) {
+    cudaGraphExecDestroy(g.exec);
+    g.exec = nullptr;
+  }
+  cudaError_t e = cudaSuccess;
+  if (!tr->capture) e = cudaStreamCreateWithFlags(&tr->capture, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return e;
+  std::vector<int64_t> steps;
+  for (oal_q19_level* L : tr->lv) steps.push_back(L->steps);
+  cudaGraph_t graph = nullptr;
+  e = cudaStreamBeginCapture(tr->capture, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return e;
+  cudaError_t e1 = step_recursive_t<T>(tr, p, 1, false, tr->capture);
+  if (e1 == cudaSuccess) e1 = step_recursive_t<T>(tr, p, 1, false, tr->capture);
+  e = cudaStreamEndCapture(tr->capture, &graph);
+  for (size_t i = 0; i < tr->lv.size(); ++i) tr->lv[i]->steps = steps[i];  // captured, not run
+  if (e1 != cudaSuccess) e = e1;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&g.exec, graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    g.exec = nullptr;
+    return e;
+  }
+  g.key.assign(kp, kp + kn);
+  g.parity = parity;
+  *out = g.exec;
+  return cudaSuccess;
+}
+
 template <class T>
 oal_status octree_advance_t(oal_q19_octree* tr, const oal_q19_params* p, int32_t n, bool collect, cudaStream_t st) {
-  for (int32_t s = 0; s < n; ++s) {
+  // pairs of non-collecting coarse steps replay a captured graph; the rest runs launch by launch
+  int32_t s = 0;
+  while (n - s >= 2 && !(collect && n - s <= 2)) {
+    cudaGraphExec_t exec = nullptr;
+    Q19_TRY(coarse_graph<T>(tr, p, &exec));
+    Q19_TRY(cudaGraphLaunch(exec, st));
+    for (size_t l = 0; l < tr->lv.size(); ++l) tr->lv[l]->steps += (int64_t)2 << l;
+    s += 2;
+  }
+  for (; s < n; ++s) {
     const bool last = collect && s == n - 1;
     if (last)
       for (oal_q19_level* L : tr->lv)
@@ -1736,6 +1828,9 @@ oal_status oal_q19_octree_destroy(oal_q19_octree* tr) {
     }
     cudaFree(tr->tri_total);
     cudaFree(tr->part);
+    for (CoarseGraph& g : tr->graphs)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (tr->capture) cudaStreamDestroy(tr->capture);
   }
   for (oal_q19_level* L : tr->lv) oal_q19_level_destroy(L);
   delete tr;
