@@ -20,6 +20,9 @@
  *     src/geometry/blocks.jl:14-364
  *   stream_collide_cumulant!(f_out, f_in, ..., ndrange)    oal_stream_collide (caller-owned arrays)
  *     src/collision/kernel_cumulant.jl:29-912              oal_level_step   (library-owned arrays)
+ *   stream_collide_entropic_d3q39!(...) + lambda_cache     oal_level_step with OAL_OP_ENTROPIC_D3Q39
+ *     src/collision/kernel_entropic_d3q39.jl:529-3368,     oal_level_entropic_lambda
+ *     timestep.jl:1133-1143,1447-1450                      oal_default_entropic_params
  *   perform_timestep_v2!(level, ...) launch + ping-pong    oal_level_step / oal_level_advance
  *     src/collision/timestep.jl:946-1559,
  *     src/solver/solver_control.jl:85-119
@@ -132,7 +135,14 @@ typedef struct oal_step_params {
   float temporal_weight;         /* refined levels (reserved) */
   int32_t use_temporal_interp;   /* refined levels (reserved) */
   int32_t level_visc_physical;   /* refined levels (reserved) */
-  int32_t reserved[8];
+  /* D3Q39 entropic operator only (kernel_entropic_d3q39.jl arguments of the same names); for that
+   * operator `lambda_param` is the h-damping sigma (timestep.jl:1142) and `adaptive_omega4` the
+   * alpha solver: 0 bisection, 1 Newton, 2 approximate, 3 Taylor (timestep.jl:1139-1141). */
+  int32_t hrr_hybrid;            /* 1 = HRR-hybrid stress reconstruction (default 0) */
+  float hrr_sigma;               /* HRR blend, used when hrr_hybrid and < 0.999 (default 1) */
+  float nu_sgs_lattice_floor;    /* level-independent lattice-viscosity floor (default 0) */
+  float shock_nu_max;            /* Mach-pocket viscosity: max(5 shock_nu_max, 0.24) (default 0) */
+  int32_t reserved[4];
 } oal_step_params;
 
 /* ---- library ---------------------------------------------------------------------------- */
@@ -149,6 +159,9 @@ oal_status oal_lookup_operator(const char* name, int32_t* out_operator_id);
 
 /* Fill `p` with the reference's configuration defaults (src/io/config_loader.jl:1305-1380). */
 void oal_default_step_params(oal_step_params* p);
+/* The same with the D3Q39 entropic operator selected and its slots set as timestep.jl:1133-1143
+ * sets them: lambda_param = ENTROPIC_SIGMA (0), adaptive_omega4 = alpha solver (0, bisection). */
+void oal_default_entropic_params(oal_step_params* p);
 
 /* ---- host-side domain builders ------------------------------------------------------------ */
 /* Active blocks of a full bx_max x by_max x bz_max box in the reference's sorted order
@@ -210,6 +223,8 @@ oal_status oal_stream_collide(const oal_geometry* g, const oal_level_fields* fie
 
 /* ---- library-owned level state ---------------------------------------------------------- */
 typedef struct oal_level oal_level;
+/* operator_id OAL_OP_CUMULANT_D3Q27 (any storage) or OAL_OP_ENTROPIC_D3Q39 (OAL_STORE_F32; the
+ * level's population arrays then have Q = 39 and step with oal_default_entropic_params). */
 oal_status oal_level_create(const oal_geometry* g, int32_t operator_id, int32_t storage,
                             oal_level** out);
 void oal_level_destroy(oal_level* L);
@@ -244,6 +259,13 @@ oal_status oal_level_mass_momentum(oal_level* L, double out[4]);
 oal_status oal_level_device_state(oal_level* L, void** f, void** rho, void** vel);
 /* Bytes of device memory this level holds. */
 int64_t oal_level_device_bytes(const oal_level* L);
+/* D3Q39 entropic levels (operator OAL_OP_ENTROPIC_D3Q39, storage OAL_STORE_F32, a geometry whose
+ * blocks all have their 26 neighbours, no solid cell, no sponge, no wall within 16 cells): the
+ * 13-multiplier warm-start cache of the equilibrium solve (timestep.jl:1447-1450), host float in
+ * the reference layout lambda(8,8,8,n_blocks,13), NaN = no warm start. get_host receives the
+ * cache, set_host (after the get) replaces it; either may be NULL. Init and set_state reset it to
+ * NaN, as the reference allocates it. Synchronises. */
+oal_status oal_level_entropic_lambda(oal_level* L, float* get_host, const float* set_host);
 /* Population layout of the level's device state (what oal_level_device_state points at):
  * out = {dense, PX, PY, PZ, block_stride, dir_stride}. dense = 1: box levels in FP32/FP16/BF16
  * keep f[k][Z][Y][X] on a padded PX x PY x PZ grid (interior cell (i,j,l) at X = i+8, Y = j+1,

@@ -84,7 +84,11 @@ class StepParams(C.Structure):
         ("temporal_weight", C.c_float),
         ("use_temporal_interp", C.c_int32),
         ("level_visc_physical", C.c_int32),
-        ("reserved", C.c_int32 * 8),
+        ("hrr_hybrid", C.c_int32),
+        ("hrr_sigma", C.c_float),
+        ("nu_sgs_lattice_floor", C.c_float),
+        ("shock_nu_max", C.c_float),
+        ("reserved", C.c_int32 * 4),
     ]
 
 
@@ -225,6 +229,7 @@ _SIGNATURES = {
     "oal_device_count": (C.c_int32, []),
     "oal_lookup_operator": (C.c_int32, [C.c_char_p, C.POINTER(C.c_int32)]),
     "oal_default_step_params": (None, [C.POINTER(StepParams)]),
+    "oal_default_entropic_params": (None, [C.POINTER(StepParams)]),
     "oal_build_box_blocks": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32),
                                          C.POINTER(C.c_int32)]),
     "oal_build_sphere_obstacle": (C.c_int32, [C.c_int32, C.POINTER(C.c_int32), C.c_double, C.c_double, C.c_double,
@@ -248,6 +253,7 @@ _SIGNATURES = {
                                            C.POINTER(C.c_void_p)]),
     "oal_level_device_bytes": (C.c_int64, [C.c_void_p]),
     "oal_level_layout": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "oal_level_entropic_lambda": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "oal_batch_create": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                      C.POINTER(C.c_void_p)]),
     "oal_batch_destroy": (None, [C.c_void_p]),

@@ -3,6 +3,8 @@
 * ``taylor_green_case`` — uniform n^3 fully periodic box (every neighbour-table entry wraps, which
   turns the reference's level kernel into a periodic one), 2-D Taylor-Green vortex uniform in z,
   Re from u0 L / nu with L = n / (2 pi).
+* ``entropic_taylor_green_case`` — the same periodic box for the D3Q39 entropic KBC level
+  (cs^2 = 2/3, so tau = nu / cs^2 + 1/2), FP32.
 * ``sphere_channel_case`` — nx x ny x nz channel, velocity inlet at x_min
   (src/collision/kernel_cumulant.jl:235-239), zero-gradient outlet (:240-245), lateral mirrors
   (:342-345), analytic sphere (src/geometry/domain_generation.jl:132-150) with half-way
@@ -46,6 +48,20 @@ def taylor_green_case(n: int, u0: float = 0.05, re: float = 100.0, c_wale: float
     rho, vel = taylor_green_fields(dom, u0, phase)
     p = capi.default_params(tau=tau, c_wale=c_wale, u_inlet=0.0, **overrides)
     return Case(f"tgv{n}", dom, rho, vel, p, dict(u0=u0, re=re, nu=nu, tau=tau, k=2 * np.pi / n))
+
+
+def entropic_taylor_green_case(n: int, u0: float = 0.1, re: float = 1000.0, c_wale: float = 0.2,
+                               **overrides) -> Case:
+    if n % 8:
+        raise ValueError("box edge must be a multiple of 8")
+    from .solver import default_entropic_params
+    dom = build_box(n // 8, n // 8, n // 8, periodic=(True, True, True))
+    L = n / (2.0 * np.pi)
+    nu = u0 * L / re
+    tau = nu / (2.0 / 3.0) + 0.5
+    rho, vel = taylor_green_fields(dom, u0)
+    p = default_entropic_params(tau=tau, c_wale=c_wale, u_inlet=0.0, **overrides)
+    return Case(f"kbc_tgv{n}", dom, rho, vel, p, dict(u0=u0, re=re, nu=nu, tau=tau, k=2 * np.pi / n))
 
 
 def sphere_channel_case(nx: int = 256, ny: int = 128, nz: int = 128, diameter: float = 24.0,

@@ -1,0 +1,1187 @@
+// kbc_d3q39.cu — the D3Q39 entropic KBC level step on B200: the reference's
+// stream_collide_entropic_d3q39! (src/collision/kernel_entropic_d3q39.jl:529-3368) on a level whose
+// blocks all have their 26 neighbours (periodic boxes: no obstacle, sponge, wall model, AMR
+// parent, thermal coupling or lattice shift), with its lambda warm-start cache
+// (src/collision/timestep.jl:1447-1450) and the level ping-pong.
+//
+// One thread per cell, 128 threads per CTA (a quarter of an 8^3 block), 4 CTAs per SM. A thread
+// pulls its 39 populations through the block's 27-entry neighbour table (|c| <= 3 < 8, so at most
+// one block hop) and parks them in shared memory while the 13-moment Newton solve (warm-started
+// from the cached multipliers) runs in registers; f_eq is parked beside them for the rarely taken
+// post-collision paths. Then WALE from the 6 face neighbours' previous velocity, the Mach-pocket
+// viscosity, positivity clamp and realizability guard, the mirror split, the entropic alpha, the
+// KBC update and the post-collision guards. It writes 39 populations, rho, u and the 13
+// multipliers. The step is bound by FP32 issue (a Newton sweep is 117 exponentials, an entropy
+// evaluation 39 logarithms and divides), not by its 444 bytes of HBM traffic per cell.
+//
+// Every operation is the reference's, in its order, as single IEEE binary32 operations (the
+// library builds with -fmad=false); exp and log are kbc::exp / kbc::log, shared with the CPU
+// restatement, so the step is bit-identical to it. Terms whose coefficient is a compile-time
+// zero are left out of sums: adding +-0 to a value changes at most the sign of a zero sum, which no
+// later operation of the step can observe.
+//
+// Layout (library-owned): f[b][k][cell] and lambda[b][m][cell] block-major (FP32), rho and vel in
+// the reference layout rho(8,8,8,nb), vel(8,8,8,nb,3).
+#include <cstdarg>
+#include <cstdio>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <vector>
+
+#include "../../include/oal.h"
+#include "kbc_math.h"
+#include "kbc_d3q39.h"
+
+oal_status oal_internal_set_error(oal_status s, const char* msg);
+
+namespace {
+
+constexpr int Q = 39;
+constexpr int kThreads = 128;
+#ifndef KBC_MIN_BLOCKS
+#define KBC_MIN_BLOCKS 6  // CTAs per SM the register budget is cut for (33 KB of shared memory each)
+#endif
+
+// lattice.jl:177-262, 0-based
+__host__ __device__ constexpr int kcx(int k) {
+  constexpr int t[Q] = {0, -1, 1, 0, 0, 0, 0, -1, -1, -1, -1, 1, 1, 1, 1, -2, 2, 0, 0, 0,
+                        0, -2, -2, 2, 2, -2, -2, 2, 2, 0, 0, 0, 0, -3, 3, 0, 0, 0, 0};
+  return t[k];
+}
+__host__ __device__ constexpr int kcy(int k) {
+  constexpr int t[Q] = {0, 0, 0, -1, 1, 0, 0, -1, -1, 1, 1, -1, -1, 1, 1, 0, 0, -2, 2, 0,
+                        0, -2, 2, -2, 2, 0, 0, 0, 0, -2, -2, 2, 2, 0, 0, -3, 3, 0, 0};
+  return t[k];
+}
+__host__ __device__ constexpr int kcz(int k) {
+  constexpr int t[Q] = {0, 0, 0, 0, 0, -1, 1, -1, 1, -1, 1, -1, 1, -1, 1, 0, 0, 0, 0, -2,
+                        2, 0, 0, 0, 0, -2, 2, -2, 2, -2, 2, -2, 2, 0, 0, 0, 0, -3, 3};
+  return t[k];
+}
+__host__ __device__ constexpr int kopp(int k) {
+  constexpr int t[Q] = {0, 2, 1, 4, 3, 6, 5, 14, 13, 12, 11, 10, 9, 8, 7, 16, 15, 18, 17, 20,
+                        19, 24, 23, 22, 21, 28, 27, 26, 25, 32, 31, 30, 29, 34, 33, 36, 35, 38, 37};
+  return t[k];
+}
+__host__ __device__ constexpr float kw(int k) {
+  return k < 7 ? float(1.0 / 12) : k < 15 ? float(1.0 / 27) : k < 21 ? float(2.0 / 135) : k < 33 ? float(1.0 / 432)
+                                                                                             : float(1.0 / 1620);
+}
+
+constexpr float CS2 = float(2.0 / 3.0);
+constexpr float F_FLOOR = 1e-15f;
+
+// basis of the 13-moment solve without the constant: (cx, cy, cz, cx^2-cs2, cy^2-cs2, cz^2-cs2,
+// cxcy, cxcz, cycz, cx efl, cy efl, cz efl), efl = |c|^2 - 5 cs2 (physics_utils.jl:583-595)
+__host__ __device__ constexpr float kbasis(int m, int k) {
+  const float cx = float(kcx(k)) - 0.0f, cy = float(kcy(k)) - 0.0f, cz = float(kcz(k)) - 0.0f;
+  const float efl = (cx * cx + cy * cy + cz * cz) - 5.0f * CS2;
+  return m == 0 ? cx : m == 1 ? cy : m == 2 ? cz : m == 3 ? cx * cx - CS2 : m == 4 ? cy * cy - CS2
+       : m == 5 ? cz * cz - CS2 : m == 6 ? cx * cy : m == 7 ? cx * cz : m == 8 ? cy * cz
+       : m == 9 ? cx * efl : m == 10 ? cy * efl : cz * efl;
+}
+
+__device__ __forceinline__ float qnan() { return __int_as_float(0x7fc00000); }
+// Julia's min / max on floats: NaN in, NaN out
+__device__ __forceinline__ float jmax(float a, float b) { return (a != a || b != b) ? qnan() : (a < b ? b : a); }
+__device__ __forceinline__ float jmin(float a, float b) { return (a != a || b != b) ? qnan() : (a < b ? a : b); }
+__device__ __forceinline__ float jclamp(float v, float lo, float hi) { return v > hi ? hi : (v < lo ? lo : v); }
+__device__ __forceinline__ float smooth(float t) { return t * t * (3.0f - 2.0f * t); }
+__device__ __forceinline__ float safe_log(float x) { return x > 0.0f ? kbc::log(x) : -88.0f; }
+
+struct KbcArgs {
+  const float* fin;
+  float* fout;
+  const float* vin;
+  float* vout;
+  float* rho;
+  float* lam;
+  const int32_t* nbr;
+  int32_t nb;
+  int32_t solver;  // 0 bisection, 1 Newton, 2 approximate, 3 Taylor
+  int32_t hrr;     // HRR blend active (hrr_hybrid and hrr_sigma < 0.999)
+  float tau, c_wale, nu_bg, amr_sgs_scale, u_inlet, sigma0, hrr_sigma, nu_floor, shock_nu_max;
+  float feq_inlet[Q];
+};
+
+// pair index of direction k > 0 (k and opp(k) share it)
+__host__ __device__ constexpr int kpair(int k) {
+  constexpr int t[Q] = {-1, 0, 0, 1, 1, 2, 2, 3, 4, 5, 6, 6, 5, 4, 3, 7, 7, 8, 8, 9,
+                        9, 10, 11, 11, 10, 12, 13, 13, 12, 14, 15, 15, 14, 16, 16, 17, 17, 18, 18};
+  return t[k];
+}
+constexpr bool pairs_ok() {
+  for (int k = 1; k < Q; ++k) {
+    if (kpair(k) != kpair(kopp(k)) || kopp(k) == k || kpair(k) < 0 || kpair(k) >= 19) return false;
+    for (int j = 1; j < Q; ++j)
+      if (j != k && j != kopp(k) && kpair(j) == kpair(k)) return false;
+  }
+  return kopp(0) == 0;
+}
+static_assert(pairs_ok(), "pair table");
+
+// Julia's max(x, C) for a constant C that is not NaN: a NaN x stays NaN
+__device__ __forceinline__ float maxc(float x, float c) { return x < c ? c : x; }
+
+// Per-CTA tables, built at launch with runtime float arithmetic (the operations of the CPU
+// restatement): the 12 basis values of the 13-moment solve and the weight per direction, the pair
+// slot of h_k and its sign, and the direction itself.
+constexpr int NP = 19;     // direction pairs (k, opp k); slot NP holds the rest direction's h = 0
+constexpr int NSLOT = NP + 1;
+struct Tables {
+  float4 b[Q][4];  // [0..11] basis (cx, cy, cz, cx^2-cs2, cy^2-cs2, cz^2-cs2, cxcy, cxcz, cycz,
+                   // cx efl, cy efl, cz efl), [12] weight
+  int32_t ps[Q];   // h slot | 0x100 when h_k = -h_slot | 0x200 when k is the first of its pair
+  int32_t c[Q];    // (cx + 3) | (cy + 3) << 4 | (cz + 3) << 8 | opp(k) << 12
+};
+
+__device__ __forceinline__ void build_tables(Tables& T) {
+  for (int k = threadIdx.x; k < Q; k += blockDim.x) {
+    int cxi = 0, cyi = 0, czi = 0, opp = 0, pair = 0;
+    // lattice.jl:177-262 in order, 0-based
+#pragma unroll
+    for (int i = 0; i < Q; ++i)
+      if (i == k) { cxi = kcx(i); cyi = kcy(i); czi = kcz(i); opp = kopp(i); pair = kpair(i); }
+    const float cx = float(cxi) - 0.0f, cy = float(cyi) - 0.0f, cz = float(czi) - 0.0f;
+    const float efl = (cx * cx + cy * cy + cz * cz) - 5.0f * CS2;
+    float* r = reinterpret_cast<float*>(T.b[k]);
+    r[0] = cx; r[1] = cy; r[2] = cz;
+    r[3] = cx * cx - CS2; r[4] = cy * cy - CS2; r[5] = cz * cz - CS2;
+    r[6] = cx * cy; r[7] = cx * cz; r[8] = cy * cz;
+    r[9] = cx * efl; r[10] = cy * efl; r[11] = cz * efl;
+    r[12] = k < 7 ? float(1.0 / 12) : k < 15 ? float(1.0 / 27) : k < 21 ? float(2.0 / 135) : k < 33 ? float(1.0 / 432)
+                                                                                               : float(1.0 / 1620);
+    r[13] = r[14] = r[15] = 0.0f;
+    T.ps[k] = k == 0 ? (NP | 0x200) : (pair | (opp < k ? 0x100 : 0x200));
+    T.c[k] = (cxi + 3) | ((cyi + 3) << 4) | ((czi + 3) << 8) | (opp << 12);
+  }
+}
+
+// exp argument la0 + la1 b0 + ... + la12 b11 of one direction (physics_utils.jl:589-593), every
+// term written out in the reference's order
+__device__ __forceinline__ float lda_row(const float (&la)[13], const float4* row) {
+  const float4 r0 = row[0], r1 = row[1], r2 = row[2];
+  float l = la[0] + la[1] * r0.x;
+  l = l + la[2] * r0.y;
+  l = l + la[3] * r0.z;
+  l = l + la[4] * r0.w;
+  l = l + la[5] * r1.x;
+  l = l + la[6] * r1.y;
+  l = l + la[7] * r1.z;
+  l = l + la[8] * r1.w;
+  l = l + la[9] * r2.x;
+  l = l + la[10] * r2.y;
+  l = l + la[11] * r2.z;
+  l = l + la[12] * r2.w;
+  return l;
+}
+// max(rho w_k exp(clamp(lda)), 1e-15) (physics_utils.jl:594, 759-760)
+__device__ __forceinline__ float fi_row(float rho, const float (&la)[13], const float4* row) {
+  return maxc(rho * row[3].x * kbc::exp(jclamp(lda_row(la, row), -20.0f, 20.0f)), 1e-15f);
+}
+
+// physics_utils.jl:493-736: 13 multipliers by block-Jacobi Newton sweeps, warm-started from the
+// cached multipliers when they pass the staleness gate
+__device__ __forceinline__ void solve_lambdas(const Tables& T, float rho, float ux, float uy, float uz, float (&la)[13]) {
+  const float OMEGA = 1.5f, F_FLOOR_EQ = 1e-15f;
+  const float eps = 1.1920928955078125e-7f;
+  const float TOL_SQ = 507.0f * eps * eps * rho * rho * 1.0f;
+  const float eR = CS2;
+  const float usq = ux * ux + uy * uy + uz * uz;
+  const float dT = 1.0f - 1.0f;
+  const float ef = usq + 5.0f * eR * dT;
+  float mt[13];
+  mt[0] = rho; mt[1] = rho * ux; mt[2] = rho * uy; mt[3] = rho * uz;
+  mt[4] = rho * (ux * ux + eR * dT); mt[5] = rho * (uy * uy + eR * dT); mt[6] = rho * (uz * uz + eR * dT);
+  mt[7] = rho * ux * uy; mt[8] = rho * ux * uz; mt[9] = rho * uy * uz;
+  mt[10] = rho * ux * ef; mt[11] = rho * uy * ef; mt[12] = rho * uz * ef;
+  const float inv_cs2 = 1.0f / CS2, inv_cs4 = inv_cs2 * inv_cs2;
+  auto poly_start = [&]() {
+    la[0] = -0.5f * usq * inv_cs2; la[1] = ux * inv_cs2; la[2] = uy * inv_cs2; la[3] = uz * inv_cs2;
+    la[4] = 0.5f * inv_cs4 * ux * ux; la[5] = 0.5f * inv_cs4 * uy * uy; la[6] = 0.5f * inv_cs4 * uz * uz;
+    la[7] = inv_cs4 * ux * uy; la[8] = inv_cs4 * ux * uz; la[9] = inv_cs4 * uy * uz;
+    la[10] = 0.0f; la[11] = 0.0f; la[12] = 0.0f;
+  };
+  if (la[0] != la[0]) {
+    poly_start();
+  } else {
+    // staleness gate (physics_utils.jl:603-634)
+    float gd[13];
+#pragma unroll
+    for (int m = 0; m < 13; ++m) gd[m] = 0.0f;
+#pragma unroll 1
+    for (int k = 0; k < Q; ++k) {
+      const float4* row = T.b[k];
+      const float fi = fi_row(rho, la, row);
+      const float4 r0 = row[0], r1 = row[1], r2 = row[2];
+      gd[0] += fi;
+      gd[1] += fi * r0.x; gd[2] += fi * r0.y; gd[3] += fi * r0.z; gd[4] += fi * r0.w;
+      gd[5] += fi * r1.x; gd[6] += fi * r1.y; gd[7] += fi * r1.z; gd[8] += fi * r1.w;
+      gd[9] += fi * r2.x; gd[10] += fi * r2.y; gd[11] += fi * r2.z; gd[12] += fi * r2.w;
+    }
+    float gres = 0.0f;
+#pragma unroll
+    for (int m = 0; m < 13; ++m) gres += (mt[m] - gd[m]) * (mt[m] - gd[m]);
+    if (gres > 100.0f * TOL_SQ) poly_start();
+  }
+  auto upd = [&](int m, float d, float j) {
+    la[m] += j > F_FLOOR_EQ ? jclamp(OMEGA * (mt[m] - d) / j, -2.0f, 2.0f) : 0.0f;
+  };
+  for (int sweep = 0; sweep < 200; ++sweep) {
+    float d[13], j[13];
+#pragma unroll
+    for (int m = 0; m < 13; ++m) { d[m] = 0.0f; j[m] = 0.0f; }
+#pragma unroll 3
+    for (int k = 0; k < Q; ++k) {
+      const float4* row = T.b[k];
+      const float fi = fi_row(rho, la, row);
+      const float4 r0 = row[0];
+      d[0] += fi; j[0] += fi;
+      d[1] += fi * r0.x; j[1] += fi * r0.x * r0.x;
+      d[2] += fi * r0.y; j[2] += fi * r0.y * r0.y;
+      d[3] += fi * r0.z; j[3] += fi * r0.z * r0.z;
+    }
+#pragma unroll
+    for (int m = 0; m < 4; ++m) upd(m, d[m], j[m]);
+#pragma unroll 3
+    for (int k = 0; k < Q; ++k) {
+      const float4* row = T.b[k];
+      const float fi = fi_row(rho, la, row);
+      const float4 r0 = row[0], r1 = row[1], r2 = row[2];
+      d[4] += fi * r0.w; j[4] += fi * r0.w * r0.w;
+      d[5] += fi * r1.x; j[5] += fi * r1.x * r1.x;
+      d[6] += fi * r1.y; j[6] += fi * r1.y * r1.y;
+      d[7] += fi * r1.z; j[7] += fi * r1.z * r1.z;
+      d[8] += fi * r1.w; j[8] += fi * r1.w * r1.w;
+      d[9] += fi * r2.x; j[9] += fi * r2.x * r2.x;
+    }
+#pragma unroll
+    for (int m = 4; m < 10; ++m) upd(m, d[m], j[m]);
+#pragma unroll 3
+    for (int k = 0; k < Q; ++k) {
+      const float4* row = T.b[k];
+      const float fi = fi_row(rho, la, row);
+      const float4 r2 = row[2];
+      d[10] += fi * r2.y; j[10] += fi * r2.y * r2.y;
+      d[11] += fi * r2.z; j[11] += fi * r2.z * r2.z;
+      d[12] += fi * r2.w; j[12] += fi * r2.w * r2.w;
+    }
+#pragma unroll
+    for (int m = 10; m < 13; ++m) upd(m, d[m], j[m]);
+    float res = 0.0f;
+#pragma unroll
+    for (int m = 0; m < 13; ++m) res += (mt[m] - d[m]) * (mt[m] - d[m]);
+    if (res < TOL_SQ) break;
+  }
+}
+
+// The mass-corrected equilibrium, kept as its multipliers: f_eq_k = corr * fi_k
+// (physics_utils.jl:738-795, kernel_entropic_d3q39.jl:2365-2385)
+struct Eq {
+  float la[13];
+  float rho, corr;
+  __device__ __forceinline__ float operator()(const Tables& T, int k) const { return corr * fi_row(rho, la, T.b[k]); }
+};
+
+// HRR blend of the stress part (kernel_entropic_d3q39.jl:2991-3034); k and opp(k) give the same s_fd
+struct Hrr {
+  int on;
+  float sigma, oms, pxx, pyy, pzz, pxy, pxz, pyz;
+};
+__device__ __forceinline__ float hrr_s(const Tables& T, float s, int k, const Hrr& hr) {
+  if (!hr.on) return s;
+  const float4 r0 = T.b[k][0];
+  const float cx = r0.x, cy = r0.y, cz = r0.z;
+  const float Qxx = cx * cx - CS2, Qyy = cy * cy - CS2, Qzz = cz * cz - CS2;
+  const float Qxy = cx * cy, Qxz = cx * cz, Qyz = cy * cz;
+  const float contraction = Qxx * hr.pxx + Qyy * hr.pyy + Qzz * hr.pzz + 2.0f * (Qxy * hr.pxy + Qxz * hr.pxz + Qyz * hr.pyz);
+  const float s_fd = T.b[k][3].x * contraction * (0.5f / (CS2 * CS2));
+  return hr.sigma * s + hr.oms * s_fd;
+}
+
+// After the split the thread's population column holds a_k = f_eq_k + coeff_s s_k and its h column
+// one value per pair (h_opp(k) = -h_k, the rest direction's h in the last slot): the post-collision
+// population is a_k + coeff_h h_k, the intermediate the reference forms (:113-133, 3163-3176).
+__device__ __forceinline__ float h_at(const Tables& T, const float* sh, int k) {
+  const int ps = T.ps[k];
+  const float h = sh[(ps & 0xff) * kThreads];
+  return (ps & 0x100) ? -h : h;
+}
+
+// kernel_entropic_d3q39.jl:113-133
+__device__ __forceinline__ float entropy_ah(const Tables& T, const float* sa, const float* sh, float coeff_h) {
+  float H = 0.0f;
+#pragma unroll 3
+  for (int k = 0; k < Q; ++k) {
+    float fk = sa[k * kThreads] + coeff_h * h_at(T, sh, k);
+    fk = maxc(fk, F_FLOOR);
+    H += fk * safe_log(fk / T.b[k][3].x);
+  }
+  return H;
+}
+
+// kernel_entropic_d3q39.jl:417-442: the lower and upper brackets, then up to max_iter midpoints,
+// through one entropy evaluation site
+__device__ __forceinline__ float alpha_bisection(const Tables& T, const float* sa, const float* sh, float beta,
+                                                 float H_pre, int max_iter) {
+  const float inv_2beta = 0.5f / jmax(beta, 0.01f);
+  float lo = jmax(inv_2beta - 0.1f, 0.1f), hi = jmax(inv_2beta + 3.0f, 4.0f);
+  float H_lo = 0.0f;
+  for (int it = -2; it < max_iter; ++it) {
+    const float al = it == -2 ? lo : it == -1 ? hi : 0.5f * (lo + hi);
+    const float H = entropy_ah(T, sa, sh, 1.0f - 2.0f * beta * al);
+    if (it == -2) { H_lo = H; continue; }
+    if (it == -1) {
+      if (!((H_lo - H_pre) * (H - H_pre) < 0.0f)) return inv_2beta;
+      continue;
+    }
+    if ((H - H_pre) * (H_lo - H_pre) > 0.0f) { lo = al; H_lo = H; } else { hi = al; }
+    if ((hi - lo) < 0.005f * (inv_2beta + 1e-6f)) break;
+  }
+  return 0.5f * (lo + hi);
+}
+
+// kernel_entropic_d3q39.jl:444-462 with entropy_and_deriv_at_alpha_39_fused (:192-215)
+__device__ __forceinline__ float alpha_newton(const Tables& T, const float* sa, const float* sh, float beta, float H_pre) {
+  float alpha = 2.0f;
+  const float inv_2beta = 0.5f / jmax(beta, 0.01f);
+  for (int it = 0; it < 8; ++it) {
+    const float coeff_h = 1.0f - 2.0f * beta * alpha;
+    float H = 0.0f, dH = 0.0f;
+#pragma unroll 3
+    for (int k = 0; k < Q; ++k) {
+      const float hk = h_at(T, sh, k);
+      float fk = sa[k * kThreads] + coeff_h * hk;
+      fk = maxc(fk, F_FLOOR);
+      const float lr = safe_log(fk / T.b[k][3].x);
+      H += fk * lr;
+      dH += (-2.0f * beta * hk) * (1.0f + lr);
+    }
+    const float residual = H - H_pre;
+    if (fabsf(residual) < 1e-5f) break;
+    if (fabsf(dH) < 1e-12f) break;
+    const float delta = residual / dH;
+    alpha -= delta;
+    alpha = jclamp(alpha, jmax(inv_2beta - 0.1f, 0.1f), 6.0f);
+    if (fabsf(delta) < 1e-5f) break;
+  }
+  if (!(alpha > 0.0f)) alpha = inv_2beta;
+  return alpha;
+}
+
+// kernel_entropic_d3q39.jl:481-528 without its bisection fallback (false: the cell's deviation needs
+// the bisection); runs on the arriving populations before the split
+__device__ __forceinline__ bool alpha_taylor(const Tables& T, const float* sf, const Eq& eq, float h_scale, const Hrr& hr,
+                                             float beta, float& alpha) {
+  auto fneq_of = [&](int k, float& fe) {
+    const int kb = (T.c[k] >> 12) & 63;
+    fe = eq(T, k);
+    const float df = sf[k * kThreads] - fe, dfb = sf[kb * kThreads] - eq(T, kb);
+    const float s = hrr_s(T, 0.5f * (df + dfb), k, hr);
+    const float h = (0.5f * (df - dfb)) * h_scale;
+    return s + h;
+  };
+  float dev = 0.0f;
+#pragma unroll 1
+  for (int k = 0; k < Q; ++k) {
+    float fe;
+    const float fneq = fneq_of(k, fe);
+    const float fk = maxc(fe + fneq, F_FLOOR);
+    dev = jmax(dev, fabsf(fneq) / fk);
+    if (dev > 0.01f) break;
+  }
+  const float inv_2beta = 0.5f / jmax(beta, 0.01f);
+  if (dev < 1e-6f) { alpha = 2.0f; return true; }
+  if (!(dev < 0.01f)) return false;
+  float a1 = 0.0f, a2 = 0.0f, a3 = 0.0f, a4 = 0.0f;
+#pragma unroll 1
+  for (int k = 0; k < Q; ++k) {
+    float fe;
+    const float t = fneq_of(k, fe);
+    const float fk = maxc(fe + t, F_FLOOR);
+    const float inv = 1.0f / fk;
+    float p = t * t * inv; a1 += p;
+    p *= t * inv; a2 += p;
+    p *= t * inv; a3 += p;
+    p *= t * inv; a4 += p;
+  }
+  a1 *= 0.5f; a2 *= -1.0f / 6.0f; a3 *= 1.0f / 12.0f; a4 *= -0.05f;
+  if (fabsf(a1) > 1e-20f) {
+    const float i1 = 1.0f / a1;
+    const float al = 2.0f - 4.0f * a2 * i1 + 16.0f * a2 * a2 * i1 * i1 - 8.0f * a3 * i1 +
+                     80.0f * a2 * a3 * i1 * i1 - 80.0f * a2 * a2 * a2 * i1 * i1 * i1 - 16.0f * a4 * i1;
+    alpha = jclamp(al, inv_2beta, 6.0f);
+  } else {
+    alpha = 2.0f;
+  }
+  return true;
+}
+
+// One cell per thread (kernel_entropic_d3q39.jl:859-3368 on such a level). The thread's populations
+// live in its shared-memory column (the pulled f, then a_k, then the post-collision values) and the
+// per-direction loops run rolled over the CTA's tables, which keeps the step's code small enough to
+// stay in the instruction cache. f_eq is recomputed from its multipliers where a pass needs it.
+__global__ void __launch_bounds__(kThreads, KBC_MIN_BLOCKS) k_kbc_step(const KbcArgs a) {
+  __shared__ Tables T;
+  __shared__ int32_t s_nbr[27];
+  __shared__ float s_f[Q * kThreads];
+  __shared__ float s_h[NSLOT * kThreads];
+  const int tid = threadIdx.x;
+  const int b = blockIdx.x >> 2;
+  const int cell = ((blockIdx.x & 3) << 7) | tid;
+  build_tables(T);
+  if (tid < 27) s_nbr[tid] = a.nbr[(int64_t)b * 27 + tid];
+  __syncthreads();
+  float* sf = s_f + tid;
+  float* sh = s_h + tid;
+  const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
+  const int64_t N = (int64_t)a.nb * 512;
+  const int64_t ci = (int64_t)b * 512 + cell;
+
+  // STEP 1-2: pull, moments, density floor and NaN reset (:898-1290, 1616-1650)
+  float rho, ux, uy, uz, inv_rho;
+  {
+    float jx = 0.0f, jy = 0.0f, jz = 0.0f;
+    rho = 0.0f;
+#pragma unroll 13
+    for (int k = 0; k < Q; ++k) {
+      const int c = T.c[k];
+      const int cx = (c & 15) - 3, cy = ((c >> 4) & 15) - 3, cz = ((c >> 8) & 15) - 3;
+      const int sx = x - cx, sy = y - cy, sz = z - cz;
+      const int ox = sx < 0 ? -1 : (sx > 7 ? 1 : 0), oy = sy < 0 ? -1 : (sy > 7 ? 1 : 0), oz = sz < 0 ? -1 : (sz > 7 ? 1 : 0);
+      const int bo = s_nbr[(ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)];
+      const float f = a.fin[((int64_t)bo * Q + k) * 512 + ((sx & 7) | ((sy & 7) << 3) | ((sz & 7) << 6))];
+      sf[k * kThreads] = f;
+      rho += f;
+      jx += f * float(cx);
+      jy += f * float(cy);
+      jz += f * float(cz);
+    }
+    const float rho_raw = rho;
+    rho = jmax(rho_raw, 0.01f);
+    inv_rho = 1.0f / rho;
+    ux = jx * inv_rho; uy = jy * inv_rho; uz = jz * inv_rho;
+    const bool is_nan = !(rho_raw == rho_raw) || !(ux == ux) || !(uy == uy) || !(uz == uz);
+    if (is_nan || rho_raw < 0.01f) {
+      rho = 1.0f; ux = a.u_inlet; uy = 0.0f; uz = 0.0f; inv_rho = 1.0f;
+#pragma unroll 1
+      for (int k = 0; k < Q; ++k) sf[k * kThreads] = a.feq_inlet[k];
+    }
+  }
+  // macro realizability, far bulk (:2112-2229)
+  bool macro_limited = false;
+  {
+    const float u_trans = sqrtf(uy * uy + uz * uz);
+    const float uxr = ux - 0.0f;
+    float uyr = uy - 0.0f, uzr = uz - 0.0f;
+    float u_rel = sqrtf(uxr * uxr + uyr * uyr + uzr * uzr);
+    const float u_ref = jmax(jmax(a.u_inlet, 0.1f), 0.1f);
+    float u_cap = jmin(1.00f, jmax(0.80f, 1.35f * u_ref + 0.15f));
+    float u_trans_cap = jmin(0.92f, jmax(0.55f, 1.15f * u_ref + 0.12f));
+    u_cap = jmin(u_cap, jmin(0.78f, jmax(0.48f, 1.12f * u_ref + 0.08f)));
+    u_trans_cap = jmin(u_trans_cap, jmin(0.46f, jmax(0.18f, 0.68f * u_ref + 0.04f)));
+    const bool speed_path = u_rel > u_cap;
+    const bool trans_path = u_trans > u_trans_cap;
+    const float rho_floor = 0.42f, rho_ceil = 2.10f;
+    const bool density_path = rho < 0.30f || rho > 2.80f || (rho < rho_floor || rho > rho_ceil) ||
+                              ((rho < 0.45f || rho > 2.20f) && (speed_path || trans_path));
+    if (density_path) {
+      rho = jclamp(rho, rho_floor, rho_ceil);
+      inv_rho = 1.0f / jmax(rho, 0.01f);
+      macro_limited = true;
+    }
+    if (trans_path && u_trans > 1e-8f) {
+      const float ts = u_trans_cap / jmax(u_trans, 1e-8f);
+      uy *= ts;
+      uz *= ts;
+      uyr = uy - 0.0f; uzr = uz - 0.0f;
+      u_rel = sqrtf(uxr * uxr + uyr * uyr + uzr * uzr);
+      macro_limited = true;
+    }
+    if (speed_path && u_rel > 1e-8f) {
+      const float ss = u_cap / jmax(u_rel, 1e-8f);
+      ux = 0.0f + uxr * ss;
+      uy = 0.0f + uyr * ss;
+      uz = 0.0f + uzr * ss;
+      macro_limited = true;
+    }
+  }
+  // equilibrium velocity and its cap (:2262-2282)
+  float ux_rel = (ux + 0.5f * 0.0f * inv_rho) - 0.0f;
+  float uy_rel = (uy + 0.5f * 0.0f * inv_rho) - 0.0f;
+  float uz_rel = (uz + 0.5f * 0.0f * inv_rho) - 0.0f;
+  bool eq_limited = false;
+  {
+    const float m = sqrtf(ux_rel * ux_rel + uy_rel * uy_rel + uz_rel * uz_rel);
+    if (m > 0.82f) {
+      const float sc = 0.82f / jmax(m, 1e-6f);
+      ux_rel *= sc; uy_rel *= sc; uz_rel *= sc;
+      eq_limited = true;
+    }
+  }
+  a.rho[ci] = rho;
+  a.vout[ci] = ux;
+  a.vout[ci + N] = uy;
+  a.vout[ci + 2 * N] = uz;
+  // STEP 3a: multipliers (warm start from the cache) and the mass correction (:2330-2385)
+  Eq eq;
+  eq.rho = rho;
+  {
+    float* lam = a.lam + (int64_t)b * 13 * 512 + cell;
+#pragma unroll
+    for (int m = 0; m < 13; ++m) eq.la[m] = lam[m * 512];
+    solve_lambdas(T, rho, ux_rel, uy_rel, uz_rel, eq.la);
+#pragma unroll
+    for (int m = 0; m < 13; ++m) lam[m * 512] = eq.la[m];
+    float sum = 0.0f;
+#pragma unroll 3
+    for (int k = 0; k < Q; ++k) sum += fi_row(rho, eq.la, T.b[k]);
+    eq.corr = sum > 1e-15f ? rho / sum : 1.0f;
+  }
+  // STEP 3: WALE from the previous velocity (physics_utils.jl:2217-2233, :2588-2700)
+  float g11, g22, g33, S12, S13, S23;
+  float nu_eddy = 0.0f;
+  {
+    float g[9];
+    float up[3][3], um[3][3];
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        const int d = s == 0 ? 1 : -1;
+        const int px = x + (ax == 0 ? d : 0), py = y + (ax == 1 ? d : 0), pz = z + (ax == 2 ? d : 0);
+        const int ox = px < 0 ? -1 : (px > 7 ? 1 : 0), oy = py < 0 ? -1 : (py > 7 ? 1 : 0), oz = pz < 0 ? -1 : (pz > 7 ? 1 : 0);
+        const int bo = s_nbr[(ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)];
+        const int64_t c = ((px & 7) | ((py & 7) << 3) | ((pz & 7) << 6)) + 512 * (int64_t)bo;
+#pragma unroll
+        for (int comp = 0; comp < 3; ++comp) (s == 0 ? up : um)[ax][comp] = a.vin[c + N * comp];
+      }
+    }
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp)
+#pragma unroll
+      for (int ax = 0; ax < 3; ++ax) g[3 * comp + ax] = 0.5f * (up[ax][comp] - um[ax][comp]);
+    const float g12 = g[1], g13 = g[2], g21 = g[3], g23 = g[5], g31 = g[6], g32 = g[7];
+    g11 = g[0]; g22 = g[4]; g33 = g[8];
+    S12 = 0.5f * (g12 + g21); S13 = 0.5f * (g13 + g31); S23 = 0.5f * (g23 + g32);
+    const float q11 = g11 * g11 + g12 * g21 + g13 * g31, q12 = g11 * g12 + g12 * g22 + g13 * g32, q13 = g11 * g13 + g12 * g23 + g13 * g33;
+    const float q21 = g21 * g11 + g22 * g21 + g23 * g31, q22 = g21 * g12 + g22 * g22 + g23 * g32, q23 = g21 * g13 + g22 * g23 + g23 * g33;
+    const float q31 = g31 * g11 + g32 * g21 + g33 * g31, q32 = g31 * g12 + g32 * g22 + g33 * g32, q33 = g31 * g13 + g32 * g23 + g33 * g33;
+    const float tr = (q11 + q22 + q33) / 3.0f;
+    const float Sd11 = q11 - tr, Sd22 = q22 - tr, Sd33 = q33 - tr;
+    const float Sd12 = 0.5f * (q12 + q21), Sd13 = 0.5f * (q13 + q31), Sd23 = 0.5f * (q23 + q32);
+    const float OP1 = Sd11 * Sd11 + Sd22 * Sd22 + Sd33 * Sd33 + 2.0f * (Sd12 * Sd12 + Sd13 * Sd13 + Sd23 * Sd23);
+    const float OP2 = g11 * g11 + g22 * g22 + g33 * g33 + 2.0f * (S12 * S12 + S13 * S13 + S23 * S23);
+    if (OP1 > 1e-12f) {
+      const float OP1_32 = OP1 * sqrtf(OP1);
+      const float OP2_52 = OP2 * OP2 * sqrtf(jmax(OP2, 1e-12f));
+      const float denom = OP2_52 + OP1 * sqrtf(sqrtf(jmax(OP1, 1e-12f)));
+      if (denom > 1e-12f) nu_eddy = (a.c_wale * a.c_wale) * OP1_32 / denom;
+    }
+  }
+  nu_eddy = jmax(nu_eddy, a.nu_bg * a.amr_sgs_scale);
+  // Mach-pocket viscosity (:2777-2806), shock sensor off
+  float pocket;
+  {
+    const float cs_local = sqrtf(jmax(CS2 * jmax(1.0f, 0.2f), 1e-6f));
+    const float inv_cs = 1.0f / cs_local;
+    const float u_mag = sqrtf(ux * ux + uy * uy + uz * uz);
+    const float u_perp = sqrtf(uy * uy + uz * uz);
+    const float mach_boost = smooth(jclamp((u_mag * inv_cs - 0.50f) / 0.25f, 0.0f, 1.0f));
+    const float perp_boost = smooth(jclamp((u_perp * inv_cs - 0.32f) / 0.25f, 0.0f, 1.0f));
+    const float rho_lo = smooth(jclamp((0.90f - rho) / 0.26f, 0.0f, 1.0f));
+    const float rho_hi = smooth(jclamp((rho - 1.30f) / 0.70f, 0.0f, 1.0f));
+    const float rho_split = jmax(rho_lo, rho_hi);
+    pocket = jmax(jmax(perp_boost * jmax(rho_split, 0.0f), mach_boost * rho_split),
+                  jmax(0.0f * mach_boost, perp_boost * mach_boost));
+    if (pocket > 0.0f) nu_eddy = jmax(nu_eddy, pocket * jmax(5.00f * a.shock_nu_max, 0.24f) * a.amr_sgs_scale);
+  }
+  nu_eddy = jmax(nu_eddy, a.nu_floor);
+  const float tau_eff = 0.5f + ((a.tau - 0.5f) * CS2 + nu_eddy) / CS2;
+  const float omega = 1.0f / jmax(tau_eff, 0.500001f);
+  const float beta = 0.5f * omega;
+  float sigma = a.sigma0;
+  if (pocket > 0.0f) sigma = jmax(sigma, jmin(0.995f, 0.80f + 0.195f * pocket));
+  const float h_scale = sigma > 0.0f ? 1.0f - sigma : 1.0f;
+  Hrr hr;
+  hr.on = a.hrr;
+  hr.sigma = a.hrr_sigma;
+  hr.oms = 1.0f - a.hrr_sigma;
+  {
+    const float c = -2.0f * rho * CS2 * jmax(tau_eff - 0.5f, 0.0f);
+    hr.pxx = c * g11; hr.pyy = c * g22; hr.pzz = c * g33; hr.pxy = c * S12; hr.pxz = c * S13; hr.pyz = c * S23;
+  }
+  // STEP 4b: positivity of the arriving populations (:2885-2906)
+  {
+    bool any_negative = false;
+#pragma unroll 13
+    for (int k = 0; k < Q; ++k) any_negative = any_negative || sf[k * kThreads] < F_FLOOR;
+    if (any_negative) {
+      float worst = 1.0f;
+#pragma unroll 1
+      for (int k = 0; k < Q; ++k) {
+        const float fe = eq(T, k);
+        const float fneq = sf[k * kThreads] - fe;
+        if (fneq < 0.0f && fe > F_FLOOR) worst = jmin(worst, (fe - F_FLOOR) / (-fneq + F_FLOOR));
+      }
+      worst = jclamp(worst, 0.0f, 1.0f);
+#pragma unroll 1
+      for (int k = 0; k < Q; ++k) {
+        const float fe = eq(T, k);
+        sf[k * kThreads] = maxc(fe + worst * (sf[k * kThreads] - fe), F_FLOOR);
+      }
+    }
+  }
+  // realizability guard (:2907-2958)
+  float guard;
+  {
+    const float u_g = sqrtf(ux * ux + uy * uy + uz * uz);
+    const float cs_g = sqrtf(jmax(CS2 * jmax(1.0f, 0.2f), 1e-6f));
+    const float mach_gb = smooth(jclamp((u_g / cs_g - 0.62f) / 0.22f, 0.0f, 1.0f));
+    const float trans_gb = smooth(jclamp((sqrtf(uy * uy + uz * uz) / cs_g - 0.38f) / 0.22f, 0.0f, 1.0f));
+    const float rho_low_g = jclamp((0.88f - rho) / 0.28f, 0.0f, 1.0f);
+    const float rho_high_g = jclamp((rho - 1.35f) / 0.65f, 0.0f, 1.0f);
+    const float u_ref_g = jmax(jmax(a.u_inlet, 0.1f), 0.54f);
+    const float u_spike = jmax(jclamp((u_g - u_ref_g) / 0.24f, 0.0f, 1.0f), 0.85f * jmax(mach_gb, trans_gb));
+    const float neq_g = jclamp((0.0f - 0.12f) / 0.35f, 0.0f, 1.0f);
+    const float pocket_neq = jmax(jmax(0.0f, neq_g), jmax(mach_gb, trans_gb));
+    guard = jmax(jmax(0.0f * jmax(neq_g, mach_gb), rho_low_g * pocket_neq), jmax(rho_high_g, u_spike * pocket_neq));
+    guard = jmax(guard, pocket);
+    if (eq_limited || macro_limited) guard = jmax(guard, 1.0f);
+    if (guard > 0.0f) {
+      float sdf = 0.0f, sfe = 0.0f;
+#pragma unroll 1
+      for (int k = 0; k < Q; ++k) {
+        const float fe = eq(T, k);
+        sdf += fabsf(sf[k * kThreads] - fe);
+        sfe += fabsf(fe);
+      }
+      const float reps = sfe > 1e-10f ? sdf / sfe : 0.0f;
+      const float cap = jmax(0.025f, 0.18f - 0.155f * guard);
+      if (reps > cap) {
+        const float th = jclamp(cap / jmax(reps, 1e-12f), 0.0f, 1.0f);
+#pragma unroll 1
+        for (int k = 0; k < Q; ++k) {
+          const float fe = eq(T, k);
+          sf[k * kThreads] = maxc(fe + th * (sf[k * kThreads] - fe), F_FLOOR);
+        }
+      }
+    }
+  }
+  // entropy of the arriving populations (:55-62), formed whether or not the alpha search runs
+  float H_pre = 0.0f;
+#pragma unroll 3
+  for (int k = 0; k < Q; ++k) {
+    const float fk = maxc(sf[k * kThreads], F_FLOOR);
+    H_pre += fk * safe_log(fk / T.b[k][3].x);
+  }
+  const float inv_2beta = 0.5f / jmax(beta, 0.01f);
+  float alpha = 2.0f;
+  bool alpha_done = false;
+  if (a.solver == 3) alpha_done = alpha_taylor(T, sf, eq, h_scale, hr, beta, alpha);
+  // STEP 5: split per pair, a_k = f_eq_k + coeff_s s_k over f_k (:2962-3095)
+  const float coeff_s = 1.0f - 2.0f * beta;
+#pragma unroll 1
+  for (int k = 0; k < Q; ++k) {
+    const int ps = T.ps[k];
+    if (!(ps & 0x200)) continue;
+    const int kb = (T.c[k] >> 12) & 63;
+    const float fe = eq(T, k), feb = kb == k ? fe : eq(T, kb);
+    const float df = sf[k * kThreads] - fe, dfb = sf[kb * kThreads] - feb;
+    const float s = hrr_s(T, 0.5f * (df + dfb), k, hr);
+    sh[(ps & 0xff) * kThreads] = (0.5f * (df - dfb)) * h_scale;
+    sf[k * kThreads] = fe + coeff_s * s;
+    if (kb != k) sf[kb * kThreads] = feb + coeff_s * s;
+  }
+  float h_norm_sq = 0.0f;
+#pragma unroll 13
+  for (int k = 0; k < Q; ++k) {
+    const float hk = h_at(T, sh, k);
+    h_norm_sq += hk * hk;
+  }
+  // STEP 6: alpha (:3109-3150)
+  if (h_norm_sq > 1e-20f) {
+    if (a.solver == 1) { alpha = alpha_newton(T, sf, sh, beta, H_pre); alpha_done = true; }
+    else if (a.solver == 2) {
+      float fn = 0.0f;
+#pragma unroll 1
+      for (int k = 0; k < Q; ++k) {
+        const float fe = eq(T, k);
+        fn += fe * fe;
+      }
+      alpha = jclamp(2.0f - 0.5f * (h_norm_sq / jmax(fn, 1e-15f)), inv_2beta, 4.0f);
+      alpha_done = true;
+    }
+    if (!alpha_done) alpha = alpha_bisection(T, sf, sh, beta, H_pre, 10);
+    if (!(alpha > 0.0f)) alpha = inv_2beta;
+    alpha = jclamp(alpha, inv_2beta, 6.0f);
+  } else {
+    alpha = 2.0f;
+  }
+  // STEP 7-8: KBC, post-collision blend and guard, output (:3153-3368). The zero body force adds
+  // +-0 to a sum whose f_eq term is positive, which leaves it unchanged.
+  const float coeff_h = 1.0f - 2.0f * beta * alpha;
+  float fmin = 1.0f;
+#pragma unroll 13
+  for (int k = 0; k < Q; ++k) {
+    const float v = sf[k * kThreads] + coeff_h * h_at(T, sh, k);
+    sf[k * kThreads] = v;
+    fmin = jmin(fmin, v);
+  }
+  if (fmin < 0.0f) {
+    float blend = 1.0f;
+#pragma unroll 1
+    for (int k = 0; k < Q; ++k) {
+      const float fe = eq(T, k);
+      const float fneq = sf[k * kThreads] - fe;
+      if (fneq < 0.0f && fe > F_FLOOR) blend = jmin(blend, fe / (fe - fneq + F_FLOOR));
+    }
+    blend = jmax(blend, 0.0f);
+#pragma unroll 1
+    for (int k = 0; k < Q; ++k) {
+      const float fe = eq(T, k);
+      sf[k * kThreads] = fe + blend * (sf[k * kThreads] - fe);
+    }
+  }
+  if (guard > 0.0f) {
+    float sdf = 0.0f, sfe = 0.0f;
+#pragma unroll 1
+    for (int k = 0; k < Q; ++k) {
+      const float fe = eq(T, k);
+      sdf += fabsf(sf[k * kThreads] - fe);
+      sfe += fabsf(fe);
+    }
+    const float ep = sfe > 1e-10f ? sdf / sfe : 0.0f;
+    const float cap = jmax(0.025f, 0.22f - 0.195f * guard);
+    if (ep > cap) {
+      const float th = jclamp(cap / jmax(ep, 1e-12f), 0.0f, 1.0f);
+#pragma unroll 1
+      for (int k = 0; k < Q; ++k) {
+        const float fe = eq(T, k);
+        sf[k * kThreads] = maxc(fe + th * (sf[k * kThreads] - fe), F_FLOOR);
+      }
+    }
+  }
+  float* fo = a.fout + (int64_t)b * Q * 512 + cell;
+#pragma unroll 13
+  for (int k = 0; k < Q; ++k) {
+    float v = sf[k * kThreads];
+    if (!(v == v) || v > 1e3f) v = eq(T, k);
+    fo[k * 512] = v;
+  }
+}
+
+// equilibrium start from rho, u (device float, reference layout): f, vel, rho; lambda = NaN
+__global__ void __launch_bounds__(kThreads) k_kbc_init(const float* rho_in, const float* vel_in, float* f, float* vel,
+                                                       float* rho, float* lam, int32_t nb) {
+  __shared__ Tables T;
+  build_tables(T);
+  __syncthreads();
+  const int b = blockIdx.x >> 2;
+  const int cell = ((blockIdx.x & 3) << 7) | threadIdx.x;
+  const int64_t N = (int64_t)nb * 512, ci = (int64_t)b * 512 + cell;
+  const float r = rho_in[ci], ux = vel_in[ci], uy = vel_in[ci + N], uz = vel_in[ci + 2 * N];
+  Eq eq;
+  eq.rho = r;
+  eq.la[0] = qnan();
+  solve_lambdas(T, r, ux, uy, uz, eq.la);
+  float sum = 0.0f;
+  for (int k = 0; k < Q; ++k) sum += fi_row(r, eq.la, T.b[k]);
+  eq.corr = sum > 1e-15f ? r / sum : 1.0f;
+  for (int k = 0; k < Q; ++k) f[((int64_t)b * Q + k) * 512 + cell] = eq(T, k);
+#pragma unroll
+  for (int m = 0; m < 13; ++m) lam[((int64_t)b * 13 + m) * 512 + cell] = qnan();
+  rho[ci] = r;
+  vel[ci] = ux; vel[ci + N] = uy; vel[ci + 2 * N] = uz;
+}
+
+// FP64 mass and momentum: one CTA per block, per-block partials, then a fixed-order final sum
+__global__ void __launch_bounds__(kThreads) k_kbc_mm_part(const float* f, int32_t nb, double* part) {
+  const int b = blockIdx.x;
+  double m[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int c = threadIdx.x; c < 512; c += kThreads) {
+    const float* fc = f + (int64_t)b * Q * 512 + c;
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+      const double v = fc[k * 512];
+      m[0] += v; m[1] += v * kcx(k); m[2] += v * kcy(k); m[3] += v * kcz(k);
+    }
+  }
+  __shared__ double s[4][kThreads];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) s[i][threadIdx.x] = m[i];
+  __syncthreads();
+  for (int w = kThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) s[i][threadIdx.x] += s[i][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) part[(int64_t)b * 4 + threadIdx.x] = s[threadIdx.x][0];
+}
+
+__global__ void k_kbc_mm_final(const double* part, int32_t nb, double* out) {
+  if (threadIdx.x < 4) {
+    double acc = 0.0;
+    for (int32_t b = 0; b < nb; ++b) acc += part[(int64_t)b * 4 + threadIdx.x];
+    out[threadIdx.x] = acc;
+  }
+}
+
+oal_status fail(oal_status s, const char* fmt, ...) {
+  char buf[400];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  return oal_internal_set_error(s, buf);
+}
+
+#define KBC_TRY(expr)                                                                                 \
+  do {                                                                                                \
+    cudaError_t _e = (expr);                                                                          \
+    if (_e != cudaSuccess) {                                                                          \
+      cudaGetLastError();                                                                             \
+      return fail(_e == cudaErrorMemoryAllocation ? OAL_E_OUT_OF_MEMORY : OAL_E_CUDA, "%s: %s", #expr, \
+                  cudaGetErrorString(_e));                                                            \
+    }                                                                                                 \
+  } while (0)
+
+// Host restatement of the inlet equilibrium table (physics_utils.jl:280-460 at rho = 1,
+// u = (u_inlet, -0, -0), mass_correct_feq39!, floor 1e-10; timestep.jl:1169-1188): the populations
+// of a cell reset after a NaN or a density below 0.01.
+void inlet_equilibrium(float u_inlet, float* out) {
+  const float cs2 = CS2, rho = 1.0f, ux = u_inlet, uy = -0.0f, uz = -0.0f;
+  const float F_FLOOR_EQ = 1e-15f, OMEGA = 1.5f;
+  const float eps = std::numeric_limits<float>::epsilon();
+  const float TOL_SQ = 507.0f * eps * eps * rho * rho;
+  const float usq = ux * ux + uy * uy + uz * uz, dT = 1.0f - 1.0f, dplus2_cs2 = 5.0f * cs2;
+  const float ef = usq + 5.0f * cs2 * dT;
+  const float mt[13] = {rho, rho * ux, rho * uy, rho * uz, rho * (ux * ux + cs2 * dT), rho * (uy * uy + cs2 * dT),
+                        rho * (uz * uz + cs2 * dT), rho * ux * uy, rho * ux * uz, rho * uy * uz,
+                        rho * ux * ef, rho * uy * ef, rho * uz * ef};
+  const float inv_cs2 = 1.0f / cs2, inv_cs4 = inv_cs2 * inv_cs2;
+  float la[13] = {-0.5f * usq * inv_cs2, ux * inv_cs2, uy * inv_cs2, uz * inv_cs2, 0.5f * inv_cs4 * ux * ux,
+                  0.5f * inv_cs4 * uy * uy, 0.5f * inv_cs4 * uz * uz, inv_cs4 * ux * uy, inv_cs4 * ux * uz,
+                  inv_cs4 * uy * uz, 0.0f, 0.0f, 0.0f};
+  // f_i with the parenthesised products of this variant of the solve (la8*cx*cy = (la8*cx)*cy)
+  auto f_i = [&](int i) {
+    const float cx = float(kcx(i)) - 0.0f, cy = float(kcy(i)) - 0.0f, cz = float(kcz(i)) - 0.0f;
+    const float efl = (cx * cx + cy * cy + cz * cz) - dplus2_cs2;
+    const float lda = la[0] + la[1] * cx + la[2] * cy + la[3] * cz + la[4] * (cx * cx - cs2) +
+                      la[5] * (cy * cy - cs2) + la[6] * (cz * cz - cs2) + la[7] * cx * cy + la[8] * cx * cz +
+                      la[9] * cy * cz + la[10] * cx * efl + la[11] * cy * efl + la[12] * cz * efl;
+    const float v = rho * kw(i) * kbc::exp(std::min(std::max(lda, -20.0f), 20.0f));
+    return v < F_FLOOR_EQ ? F_FLOOR_EQ : v;
+  };
+  const int g0[4] = {0, 4, 10, 13};
+  for (int sweep = 0; sweep < 200; ++sweep) {
+    float d[13] = {0}, j[13] = {0};
+    for (int g = 0; g < 3; ++g) {
+      for (int i = 0; i < Q; ++i) {
+        const float fi = f_i(i);
+        for (int m = g0[g]; m < g0[g + 1]; ++m) {
+          if (m == 0) { d[0] += fi; j[0] += fi; continue; }
+          const float b = kbasis(m - 1, i);
+          d[m] += fi * b;
+          j[m] += fi * b * b;
+        }
+      }
+      for (int m = g0[g]; m < g0[g + 1]; ++m)
+        la[m] += j[m] > F_FLOOR_EQ ? std::min(std::max(OMEGA * (mt[m] - d[m]) / j[m], -2.0f), 2.0f) : 0.0f;
+    }
+    float res = 0.0f;
+    for (int m = 0; m < 13; ++m) res += (mt[m] - d[m]) * (mt[m] - d[m]);
+    if (res < TOL_SQ) break;
+  }
+  float fe[Q], sum = 0.0f;
+  for (int i = 0; i < Q; ++i) fe[i] = f_i(i);
+  for (int i = 0; i < Q; ++i) sum += fe[i];
+  if (sum > 1e-15f) {
+    const float corr = rho / sum;
+    for (int i = 0; i < Q; ++i) fe[i] *= corr;
+  }
+  for (int i = 0; i < Q; ++i) out[i] = fe[i] < 1e-10f ? 1e-10f : fe[i];
+}
+
+}  // namespace
+
+struct KbcLevel {
+  int device = 0;
+  int32_t nb = 0;
+  const int32_t* d_nbr = nullptr;
+  float* f[2] = {nullptr, nullptr};
+  float* vel[2] = {nullptr, nullptr};
+  float* rho = nullptr;
+  float* lam = nullptr;
+  double* d_mm_part = nullptr;
+  double* d_mm = nullptr;
+  int parity = 0;
+  int64_t bytes = 0;
+  cudaStream_t cap = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  int32_t g_n = 0;
+  int g_parity = -1;
+  oal_step_params g_p{};
+};
+
+namespace {
+
+void release_graph(KbcLevel* L) {
+  if (L->exec) cudaGraphExecDestroy(L->exec);
+  if (L->graph) cudaGraphDestroy(L->graph);
+  L->exec = nullptr; L->graph = nullptr; L->g_n = 0; L->g_parity = -1;
+}
+
+oal_status resolve(const oal_step_params* p, KbcArgs* a) {
+  if (!p) return fail(OAL_E_INVALID_ARG, "null step params");
+  if (p->abi_version != OAL_ABI_VERSION)
+    return fail(OAL_E_ABI_MISMATCH, "oal_step_params.abi_version %u != %d", p->abi_version, OAL_ABI_VERSION);
+  if (p->operator_id != OAL_OP_ENTROPIC_D3Q39)
+    return fail(OAL_E_INVALID_ARG, "a D3Q39 level steps with operator_id OAL_OP_ENTROPIC_D3Q39, not %d", p->operator_id);
+  if (!(p->tau > 0.5f)) return fail(OAL_E_INVALID_ARG, "tau must exceed 1/2 (got %g)", (double)p->tau);
+  if (p->adaptive_omega4 < 0 || p->adaptive_omega4 > 3)
+    return fail(OAL_E_INVALID_ARG, "alpha solver (adaptive_omega4) %d: 0 bisection, 1 Newton, 2 approximate, 3 Taylor",
+                p->adaptive_omega4);
+  if (p->store_post_collision) return fail(OAL_E_UNSUPPORTED, "store_post_collision is not built for the D3Q39 level");
+  if (p->wall_model_active) return fail(OAL_E_UNSUPPORTED, "the wall model needs a level with walls");
+  std::memset(a, 0, sizeof *a);
+  a->solver = p->adaptive_omega4;
+  a->hrr = (p->hrr_hybrid == 1 && p->hrr_sigma < 0.999f) ? 1 : 0;
+  a->tau = p->tau; a->c_wale = p->c_wale; a->nu_bg = p->nu_sgs_background; a->amr_sgs_scale = p->amr_sgs_scale;
+  a->u_inlet = p->u_inlet; a->sigma0 = p->lambda_param; a->hrr_sigma = p->hrr_sigma;
+  a->nu_floor = p->nu_sgs_lattice_floor; a->shock_nu_max = p->shock_nu_max;
+  inlet_equilibrium(p->u_inlet, a->feq_inlet);
+  return OAL_OK;
+}
+
+oal_status enqueue(KbcLevel* L, const KbcArgs& base, cudaStream_t st) {
+  KbcArgs a = base;
+  const int p = L->parity;
+  a.fin = L->f[p]; a.fout = L->f[p ^ 1];
+  a.vin = L->vel[p]; a.vout = L->vel[p ^ 1];
+  a.rho = L->rho; a.lam = L->lam; a.nbr = L->d_nbr; a.nb = L->nb;
+  k_kbc_step<<<(unsigned)L->nb * 4, kThreads, 0, st>>>(a);
+  KBC_TRY(cudaGetLastError());
+  L->parity ^= 1;
+  return OAL_OK;
+}
+
+}  // namespace
+
+oal_status kbc_create(int device, int32_t nb, const int32_t* d_nbr, KbcLevel** out) {
+  if (!out || nb <= 0 || !d_nbr) return fail(OAL_E_INVALID_ARG, "kbc_create: bad arguments");
+  *out = nullptr;
+  if ((int64_t)nb * 4 > 0x7fffffffLL) return fail(OAL_E_TOO_LARGE, "too many blocks");
+  KBC_TRY(cudaSetDevice(device));
+  auto* L = new KbcLevel();
+  L->device = device; L->nb = nb; L->d_nbr = d_nbr;
+  const size_t ncell = (size_t)nb * 512;
+  auto alloc = [&](void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaSuccess) e = cudaMemset(*p, 0, bytes);
+    return e;
+  };
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
+    e = alloc((void**)&L->f[i], ncell * Q * sizeof(float));
+    if (e == cudaSuccess) e = alloc((void**)&L->vel[i], ncell * 3 * sizeof(float));
+  }
+  if (e == cudaSuccess) e = alloc((void**)&L->rho, ncell * sizeof(float));
+  if (e == cudaSuccess) e = alloc((void**)&L->lam, ncell * 13 * sizeof(float));
+  if (e == cudaSuccess) e = alloc((void**)&L->d_mm_part, (size_t)nb * 4 * sizeof(double));
+  if (e == cudaSuccess) e = alloc((void**)&L->d_mm, 4 * sizeof(double));
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&L->cap, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    kbc_destroy(L);
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? OAL_E_OUT_OF_MEMORY : OAL_E_CUDA, "D3Q39 level allocation: %s",
+                cudaGetErrorString(e));
+  }
+  L->bytes = (int64_t)ncell * (2 * Q + 2 * 3 + 1 + 13) * 4 + (int64_t)nb * 32 + 32;
+  *out = L;
+  return OAL_OK;
+}
+
+void kbc_destroy(KbcLevel* L) {
+  if (!L) return;
+  cudaSetDevice(L->device);
+  release_graph(L);
+  for (int i = 0; i < 2; ++i) { cudaFree(L->f[i]); cudaFree(L->vel[i]); }
+  cudaFree(L->rho); cudaFree(L->lam); cudaFree(L->d_mm_part); cudaFree(L->d_mm);
+  if (L->cap) cudaStreamDestroy(L->cap);
+  cudaGetLastError();
+  delete L;
+}
+
+oal_status kbc_init_equilibrium(KbcLevel* L, const double* rho, const double* vel) {
+  if (!L || !rho || !vel) return fail(OAL_E_INVALID_ARG, "null argument");
+  KBC_TRY(cudaSetDevice(L->device));
+  const size_t ncell = (size_t)L->nb * 512;
+  std::vector<float> hr(ncell), hv(3 * ncell);
+  for (size_t i = 0; i < ncell; ++i) hr[i] = (float)rho[i];
+  for (size_t i = 0; i < 3 * ncell; ++i) hv[i] = (float)vel[i];
+  float *d_r = nullptr, *d_v = nullptr;
+  cudaError_t e = cudaMalloc(&d_r, ncell * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&d_v, 3 * ncell * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemcpy(d_r, hr.data(), ncell * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_v, hv.data(), 3 * ncell * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    k_kbc_init<<<(unsigned)L->nb * 4, kThreads>>>(d_r, d_v, L->f[0], L->vel[0], L->rho, L->lam, L->nb);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  cudaFree(d_r); cudaFree(d_v);
+  if (e != cudaSuccess) { cudaGetLastError(); return fail(OAL_E_CUDA, "D3Q39 init_equilibrium: %s", cudaGetErrorString(e)); }
+  L->parity = 0;
+  release_graph(L);
+  return OAL_OK;
+}
+
+oal_status kbc_set_state(KbcLevel* L, const double* f, const double* rho, const double* vel) {
+  if (!L || !f) return fail(OAL_E_INVALID_ARG, "null argument");
+  KBC_TRY(cudaSetDevice(L->device));
+  KBC_TRY(cudaDeviceSynchronize());
+  const int64_t nb = L->nb, ncell = nb * 512;
+  std::vector<float> hf((size_t)ncell * Q);
+  for (int64_t b = 0; b < nb; ++b)
+    for (int k = 0; k < Q; ++k)
+      for (int c = 0; c < 512; ++c) hf[(size_t)((b * Q + k) * 512 + c)] = (float)f[c + 512 * b + ncell * k];
+  L->parity = 0;
+  KBC_TRY(cudaMemcpy(L->f[0], hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice));
+  if (rho) {
+    std::vector<float> hr((size_t)ncell);
+    for (int64_t i = 0; i < ncell; ++i) hr[(size_t)i] = (float)rho[i];
+    KBC_TRY(cudaMemcpy(L->rho, hr.data(), hr.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  if (vel) {
+    std::vector<float> hv((size_t)ncell * 3);
+    for (int64_t i = 0; i < 3 * ncell; ++i) hv[(size_t)i] = (float)vel[i];
+    KBC_TRY(cudaMemcpy(L->vel[0], hv.data(), hv.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  std::vector<float> nan((size_t)ncell * 13, std::numeric_limits<float>::quiet_NaN());
+  KBC_TRY(cudaMemcpy(L->lam, nan.data(), nan.size() * sizeof(float), cudaMemcpyHostToDevice));
+  release_graph(L);
+  return OAL_OK;
+}
+
+oal_status kbc_get_state(KbcLevel* L, double* f, double* rho, double* vel) {
+  if (!L) return fail(OAL_E_INVALID_ARG, "null level");
+  KBC_TRY(cudaSetDevice(L->device));
+  KBC_TRY(cudaDeviceSynchronize());
+  const int64_t nb = L->nb, ncell = nb * 512;
+  const int p = L->parity;
+  if (f) {
+    std::vector<float> hf((size_t)ncell * Q);
+    KBC_TRY(cudaMemcpy(hf.data(), L->f[p], hf.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    for (int64_t b = 0; b < nb; ++b)
+      for (int k = 0; k < Q; ++k)
+        for (int c = 0; c < 512; ++c) f[c + 512 * b + ncell * k] = hf[(size_t)((b * Q + k) * 512 + c)];
+  }
+  if (rho) {
+    std::vector<float> hr((size_t)ncell);
+    KBC_TRY(cudaMemcpy(hr.data(), L->rho, hr.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < ncell; ++i) rho[i] = hr[(size_t)i];
+  }
+  if (vel) {
+    std::vector<float> hv((size_t)ncell * 3);
+    KBC_TRY(cudaMemcpy(hv.data(), L->vel[p], hv.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < 3 * ncell; ++i) vel[i] = hv[(size_t)i];
+  }
+  return OAL_OK;
+}
+
+oal_status kbc_lambda(KbcLevel* L, float* get, const float* set) {
+  if (!L) return fail(OAL_E_INVALID_ARG, "null level");
+  KBC_TRY(cudaSetDevice(L->device));
+  KBC_TRY(cudaDeviceSynchronize());
+  const int64_t nb = L->nb, ncell = nb * 512;
+  std::vector<float> h((size_t)ncell * 13);
+  if (get) {
+    KBC_TRY(cudaMemcpy(h.data(), L->lam, h.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    for (int64_t b = 0; b < nb; ++b)
+      for (int m = 0; m < 13; ++m)
+        for (int c = 0; c < 512; ++c) get[c + 512 * b + ncell * m] = h[(size_t)((b * 13 + m) * 512 + c)];
+  }
+  if (set) {
+    for (int64_t b = 0; b < nb; ++b)
+      for (int m = 0; m < 13; ++m)
+        for (int c = 0; c < 512; ++c) h[(size_t)((b * 13 + m) * 512 + c)] = set[c + 512 * b + ncell * m];
+    KBC_TRY(cudaMemcpy(L->lam, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice));
+    release_graph(L);
+  }
+  return OAL_OK;
+}
+
+oal_status kbc_step(KbcLevel* L, const oal_step_params* p, void* stream) {
+  if (!L) return fail(OAL_E_INVALID_ARG, "null level");
+  KbcArgs a;
+  oal_status s = resolve(p, &a);
+  if (s != OAL_OK) return s;
+  KBC_TRY(cudaSetDevice(L->device));
+  return enqueue(L, a, static_cast<cudaStream_t>(stream));
+}
+
+oal_status kbc_advance(KbcLevel* L, const oal_step_params* p, int32_t n, void* stream) {
+  if (!L) return fail(OAL_E_INVALID_ARG, "null level");
+  if (n <= 0) return fail(OAL_E_INVALID_ARG, "n_steps must be positive");
+  KbcArgs a;
+  oal_status s = resolve(p, &a);
+  if (s != OAL_OK) return s;
+  KBC_TRY(cudaSetDevice(L->device));
+  oal_step_params key = *p;
+  key.time_step_seed = 0;
+  const bool hit = L->exec && L->g_n == n && L->g_parity == L->parity && std::memcmp(&L->g_p, &key, sizeof key) == 0;
+  if (!hit) {
+    release_graph(L);
+    const int start = L->parity;
+    KBC_TRY(cudaStreamBeginCapture(L->cap, cudaStreamCaptureModeThreadLocal));
+    oal_status es = OAL_OK;
+    for (int i = 0; i < n && es == OAL_OK; ++i) es = enqueue(L, a, L->cap);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(L->cap, &graph);
+    L->parity = start;
+    if (es != OAL_OK) { if (graph) cudaGraphDestroy(graph); return es; }
+    if (e != cudaSuccess) { cudaGetLastError(); return fail(OAL_E_CUDA, "graph capture: %s", cudaGetErrorString(e)); }
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(graph);
+      cudaGetLastError();
+      return fail(OAL_E_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    }
+    L->exec = exec; L->graph = graph; L->g_n = n; L->g_parity = start; L->g_p = key;
+  }
+  KBC_TRY(cudaGraphLaunch(L->exec, static_cast<cudaStream_t>(stream)));
+  if (n & 1) L->parity ^= 1;
+  return OAL_OK;
+}
+
+oal_status kbc_mass_momentum(KbcLevel* L, double out[4]) {
+  if (!L || !out) return fail(OAL_E_INVALID_ARG, "null argument");
+  KBC_TRY(cudaSetDevice(L->device));
+  k_kbc_mm_part<<<(unsigned)L->nb, kThreads>>>(L->f[L->parity], L->nb, L->d_mm_part);
+  KBC_TRY(cudaGetLastError());
+  k_kbc_mm_final<<<1, 32>>>(L->d_mm_part, L->nb, L->d_mm);
+  KBC_TRY(cudaGetLastError());
+  KBC_TRY(cudaMemcpy(out, L->d_mm, 4 * sizeof(double), cudaMemcpyDeviceToHost));
+  return OAL_OK;
+}
+
+oal_status kbc_device_state(KbcLevel* L, void** f, void** rho, void** vel) {
+  if (!L) return fail(OAL_E_INVALID_ARG, "null level");
+  if (f) *f = L->f[L->parity];
+  if (rho) *rho = L->rho;
+  if (vel) *vel = L->vel[L->parity];
+  return OAL_OK;
+}
+
+int64_t kbc_device_bytes(const KbcLevel* L) { return L ? L->bytes : 0; }
+
+oal_status kbc_layout(const KbcLevel* L, int64_t out[6]) {
+  if (!L || !out) return fail(OAL_E_INVALID_ARG, "null argument");
+  out[0] = 0; out[1] = out[2] = out[3] = 0; out[4] = (int64_t)Q * 512; out[5] = 512;
+  return OAL_OK;
+}

@@ -12,6 +12,7 @@
 
 #include "common.cuh"
 #include "../../include/oal.h"
+#include "kbc_d3q39.h"
 
 namespace oal {
 template <class S, class R>
@@ -298,6 +299,7 @@ struct oal_level {
   Overlap ov;
   GraphCache gc;
   bool forces_valid = false;
+  KbcLevel* kbc = nullptr;  // D3Q39 entropic levels: the whole state lives here
 };
 
 // ------------------------------------------------------------------------------------------------
@@ -605,6 +607,20 @@ void oal_default_step_params(oal_step_params* p) {
   p->temporal_weight = 1.0f;
   p->use_temporal_interp = 0;
   p->level_visc_physical = 0;
+  p->hrr_hybrid = 0;
+  p->hrr_sigma = 1.0f;            // :2283
+  p->nu_sgs_lattice_floor = 0.0f; // :733
+  p->shock_nu_max = 0.0f;
+}
+
+void oal_default_entropic_params(oal_step_params* p) {
+  oal_default_step_params(p);
+  if (!p) return;
+  p->operator_id = OAL_OP_ENTROPIC_D3Q39;
+  p->lambda_param = 0.0f;         // ENTROPIC_SIGMA, config_loader.jl:1391
+  p->adaptive_omega4 = 0;         // alpha_solver "bisection", config_loader.jl:1386
+  p->omega_bulk = p->omega3 = p->omega4 = 0.0f;  // timestep.jl:1136-1138
+  p->limiter_type = 0;
 }
 
 oal_status oal_build_box_blocks(int32_t bxm, int32_t bym, int32_t bzm, int32_t periodic_mask, int32_t* coords,
@@ -933,6 +949,30 @@ oal_status oal_stream_collide(const oal_geometry* g, const oal_level_fields* fl,
 }
 
 // ---- levels ----
+// D3Q39 entropic level: FP32 populations on a geometry whose blocks all have their 26 neighbours,
+// with no solid cell, no sponge and no wall within 16 cells (the far-bulk branch of the macro
+// realizability clamp, kernel_entropic_d3q39.jl:2149-2156)
+static oal_status create_entropic_level(const oal_geometry* g, int32_t storage, oal_level** out) {
+  if (storage != OAL_STORE_F32)
+    return set_error(OAL_E_UNSUPPORTED, "the D3Q39 entropic level stores FP32 populations (storage %d)", storage);
+  for (int32_t b = 0; b < g->nb; ++b)
+    if (!(g->h_bflags[(size_t)b] & BF_INTERIOR))
+      return set_error(OAL_E_UNSUPPORTED, "the D3Q39 entropic level needs all 26 neighbour blocks (block %d has a domain face)", b);
+  if (g->n_solid > 0) return set_error(OAL_E_UNSUPPORTED, "the D3Q39 entropic level has no solid cells");
+  for (float v : g->h_sponge)
+    if (v > 0.0f) return set_error(OAL_E_UNSUPPORTED, "the D3Q39 entropic level has no sponge");
+  for (float v : g->h_wdist)
+    if (v == v && !(v > 16.0f)) return set_error(OAL_E_UNSUPPORTED, "the D3Q39 entropic level has no wall within 16 cells");
+  KbcLevel* k = nullptr;
+  oal_status s = kbc_create(g->device, g->nb, g->d_nbr, &k);
+  if (s != OAL_OK) return s;
+  auto* L = new oal_level();
+  L->g = g; L->device = g->device; L->op = OAL_OP_ENTROPIC_D3Q39; L->storage = storage; L->kbc = k;
+  ++const_cast<oal_geometry*>(g)->n_levels;
+  *out = L;
+  return OAL_OK;
+}
+
 oal_status oal_level_create(const oal_geometry* g, int32_t op, int32_t storage, oal_level** out) {
   return oal_level_create_ex(g, op, storage, 0u, out);
 }
@@ -940,6 +980,7 @@ oal_status oal_level_create(const oal_geometry* g, int32_t op, int32_t storage, 
 oal_status oal_level_create_ex(const oal_geometry* g, int32_t op, int32_t storage, uint32_t flags, oal_level** out) {
   if (!g || !out) return set_error(OAL_E_INVALID_ARG, "null argument");
   *out = nullptr;
+  if (op == OAL_OP_ENTROPIC_D3Q39) return create_entropic_level(g, storage, out);
   if (op != OAL_OP_CUMULANT_D3Q27) return set_error(OAL_E_UNSUPPORTED, "operator %d has no level state in this build", op);
   if (storage < OAL_STORE_F32 || storage > OAL_STORE_F64) return set_error(OAL_E_INVALID_ARG, "storage %d", storage);
   OAL_CUDA_TRY(cudaSetDevice(g->device));
@@ -1008,6 +1049,13 @@ static void release_graph(oal_level* L) {
 
 void oal_level_destroy(oal_level* L) {
   if (!L) return;
+  if (L->kbc) {
+    kbc_destroy(L->kbc);
+    auto* g = const_cast<oal_geometry*>(L->g);
+    delete L;
+    if (g && --g->n_levels == 0 && g->destroy_requested) geometry_release(g);
+    return;
+  }
   cudaSetDevice(L->device);
   release_graph(L);
   for (int i = 0; i < 2; ++i) { cudaFree(L->f[i]); cudaFree(L->vel[i]); }
@@ -1025,6 +1073,7 @@ void oal_level_destroy(oal_level* L) {
 
 oal_status oal_level_init_equilibrium(oal_level* L, const double* rho, const double* vel, int32_t comp) {
   if (!L || !rho || !vel) return set_error(OAL_E_INVALID_ARG, "null argument");
+  if (L->kbc) return kbc_init_equilibrium(L->kbc, rho, vel);
   OAL_CUDA_TRY(cudaSetDevice(L->g->device));
   const int64_t ncell = (int64_t)L->g->nb * 512;
   double *d_rho = nullptr, *d_vel = nullptr;
@@ -1051,6 +1100,7 @@ oal_status oal_level_init_equilibrium(oal_level* L, const double* rho, const dou
 
 oal_status oal_level_set_state(oal_level* L, const double* f, const double* rho, const double* vel) {
   if (!L || !f) return set_error(OAL_E_INVALID_ARG, "null argument");
+  if (L->kbc) return kbc_set_state(L->kbc, f, rho, vel);
   OAL_CUDA_TRY(cudaSetDevice(L->g->device));
   const int64_t ncell = (int64_t)L->g->nb * 512;
   double *d_f = nullptr, *d_r = nullptr, *d_v = nullptr;
@@ -1081,6 +1131,7 @@ oal_status oal_level_set_state(oal_level* L, const double* f, const double* rho,
 
 oal_status oal_level_get_state(oal_level* L, double* f, double* rho, double* vel) {
   if (!L) return set_error(OAL_E_INVALID_ARG, "null argument");
+  if (L->kbc) return kbc_get_state(L->kbc, f, rho, vel);
   OAL_CUDA_TRY(cudaSetDevice(L->g->device));
   OAL_CUDA_TRY(cudaDeviceSynchronize());
   const int64_t ncell = (int64_t)L->g->nb * 512;
@@ -1153,6 +1204,7 @@ static oal_status enqueue_step(oal_level* L, const CaseParams& cp, cudaStream_t 
 
 oal_status oal_level_step(oal_level* L, const oal_step_params* p, void* stream) {
   if (!L) return set_error(OAL_E_INVALID_ARG, "null level");
+  if (L->kbc) return kbc_step(L->kbc, p, stream);
   CaseParams cp;
   oal_status s = resolve_params(p, L->g, &cp);
   if (s != OAL_OK) return s;
@@ -1163,6 +1215,7 @@ oal_status oal_level_step(oal_level* L, const oal_step_params* p, void* stream) 
 
 oal_status oal_level_advance(oal_level* L, const oal_step_params* p, int32_t n, void* stream) {
   if (!L) return set_error(OAL_E_INVALID_ARG, "null level");
+  if (L->kbc) return kbc_advance(L->kbc, p, n, stream);
   if (n <= 0) return set_error(OAL_E_INVALID_ARG, "n_steps must be positive");
   CaseParams cp;
   oal_status s = resolve_params(p, L->g, &cp);
@@ -1201,6 +1254,7 @@ oal_status oal_level_advance(oal_level* L, const oal_step_params* p, int32_t n, 
 
 oal_status oal_level_get_forces(oal_level* L, double out[3]) {
   if (!L || !out) return set_error(OAL_E_INVALID_ARG, "null argument");
+  if (L->kbc) { out[0] = out[1] = out[2] = 0.0; return OAL_OK; }  // no solid cells
   OAL_CUDA_TRY(cudaSetDevice(L->g->device));
   if (!L->forces_valid) { out[0] = out[1] = out[2] = 0.0; return check_level_error(L); }
   OAL_CUDA_TRY(cudaMemcpy(out, L->d_force, 3 * sizeof(double), cudaMemcpyDeviceToHost));
@@ -1209,6 +1263,7 @@ oal_status oal_level_get_forces(oal_level* L, double out[3]) {
 
 oal_status oal_level_get_forces_async(oal_level* L, double* host_out3, void* stream) {
   if (!L || !host_out3) return set_error(OAL_E_INVALID_ARG, "null argument");
+  if (L->kbc) { host_out3[0] = host_out3[1] = host_out3[2] = 0.0; return OAL_OK; }
   OAL_CUDA_TRY(cudaMemcpyAsync(host_out3, L->d_force, 3 * sizeof(double), cudaMemcpyDeviceToHost,
                                static_cast<cudaStream_t>(stream)));
   return OAL_OK;
@@ -1216,6 +1271,7 @@ oal_status oal_level_get_forces_async(oal_level* L, double* host_out3, void* str
 
 oal_status oal_level_mass_momentum(oal_level* L, double out[4]) {
   if (!L || !out) return set_error(OAL_E_INVALID_ARG, "null argument");
+  if (L->kbc) return kbc_mass_momentum(L->kbc, out);
   OAL_CUDA_TRY(cudaSetDevice(L->g->device));
   cudaError_t e = cudaSuccess;
   switch (L->storage) {
@@ -1231,16 +1287,24 @@ oal_status oal_level_mass_momentum(oal_level* L, double out[4]) {
 
 oal_status oal_level_device_state(oal_level* L, void** f, void** rho, void** vel) {
   if (!L) return set_error(OAL_E_INVALID_ARG, "null level");
+  if (L->kbc) return kbc_device_state(L->kbc, f, rho, vel);
   if (f) *f = L->f[L->parity];
   if (rho) *rho = L->rho;
   if (vel) *vel = L->vel[L->parity];
   return OAL_OK;
 }
 
-int64_t oal_level_device_bytes(const oal_level* L) { return L ? L->bytes : 0; }
+int64_t oal_level_device_bytes(const oal_level* L) { return L ? (L->kbc ? kbc_device_bytes(L->kbc) : L->bytes) : 0; }
+
+oal_status oal_level_entropic_lambda(oal_level* L, float* get_host, const float* set_host) {
+  if (!L) return set_error(OAL_E_INVALID_ARG, "null level");
+  if (!L->kbc) return set_error(OAL_E_INVALID_ARG, "not a D3Q39 entropic level");
+  return kbc_lambda(L->kbc, get_host, set_host);
+}
 
 oal_status oal_level_layout(const oal_level* L, int64_t out[6]) {
   if (!L || !out) return set_error(OAL_E_INVALID_ARG, "null argument");
+  if (L->kbc) return kbc_layout(L->kbc, out);
   int64_t bst, kst;
   level_layout(L, &bst, &kst);
   out[0] = L->dense ? 1 : 0; out[1] = L->PX; out[2] = L->PY; out[3] = L->PZ; out[4] = bst; out[5] = kst;

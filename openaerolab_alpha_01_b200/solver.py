@@ -12,6 +12,10 @@ Names follow the reference (OpenAeroLab, Julia):
   swapped by parity (src/solver/solver_control.jl:85-91).
 * ``Level.execute_timestep_batch`` — ``execute_timestep_batch!`` (src/solver/solver_control.jl:796-828):
   n steps as one captured CUDA graph.
+* ``Level(geom, "entropic")`` — a D3Q39 level stepped by ``stream_collide_entropic_d3q39!``
+  (src/collision/kernel_entropic_d3q39.jl:529-3368) with its multiplier warm-start cache
+  (``Level.lambda_cache``, src/collision/timestep.jl:1447-1450); parameters from
+  ``default_entropic_params`` (timestep.jl:1133-1143).
 
 Arrays use the reference layout flattened to C order: populations ``(Q, n_blocks, 512)``,
 density ``(n_blocks, 512)``, velocity ``(3, n_blocks, 512)``; the cell index inside a block is
@@ -61,6 +65,19 @@ def get_collision_kernel(operator: str) -> int:
 def default_step_params(**overrides) -> capi.StepParams:
     """The reference's configuration defaults (src/io/config_loader.jl:1305-1380) with overrides."""
     return capi.default_params(**overrides)
+
+
+def default_entropic_params(**overrides) -> capi.StepParams:
+    """Defaults of the D3Q39 entropic operator: ``lambda_param`` is the h-damping sigma
+    (ENTROPIC_SIGMA, 0) and ``adaptive_omega4`` the alpha solver (0 bisection, 1 Newton,
+    2 approximate, 3 Taylor; config default bisection), as timestep.jl:1133-1143 passes them."""
+    p = capi.StepParams()
+    lib().oal_default_entropic_params(C.byref(p))
+    for k, v in overrides.items():
+        if not hasattr(p, k):
+            raise AttributeError(k)
+        setattr(p, k, v)
+    return p
 
 
 @dataclass
@@ -185,6 +202,7 @@ class Level:
         check(lib().oal_level_create_ex(geom.handle, self.operator, self.storage, flags, C.byref(h)))
         self.handle = h
         self.n_blocks = geom.dom.n_blocks
+        self.Q = 39 if self.operator == capi.OAL_OP_ENTROPIC_D3Q39 else 27
 
     # -- state ---------------------------------------------------------------------------
     def init_equilibrium(self, rho: np.ndarray, vel: np.ndarray, compressible_corr: int = 0) -> None:
@@ -202,11 +220,19 @@ class Level:
 
     def state(self):
         nb = self.n_blocks
-        f = np.empty((27, nb, 512))
+        f = np.empty((self.Q, nb, 512))
         rho = np.empty((nb, 512))
         vel = np.empty((3, nb, 512))
         check(lib().oal_level_get_state(self.handle, f.ctypes.data, rho.ctypes.data, vel.ctypes.data))
         return f, rho, vel
+
+    def lambda_cache(self, new: Optional[np.ndarray] = None) -> np.ndarray:
+        """D3Q39 levels: the 13-multiplier warm-start cache (13, n_blocks, 512), float32, NaN = none;
+        `new` replaces it after the read."""
+        out = np.empty((13, self.n_blocks, 512), np.float32)
+        src = None if new is None else np.ascontiguousarray(new, dtype=np.float32)
+        check(lib().oal_level_entropic_lambda(self.handle, out.ctypes.data, None if src is None else src.ctypes.data))
+        return out
 
     # -- stepping ------------------------------------------------------------------------
     def perform_timestep(self, params: capi.StepParams, stream=None) -> None:

@@ -18,7 +18,7 @@ import time
 
 import numpy as np
 
-from .cases import taylor_green_case
+from .cases import entropic_taylor_green_case, taylor_green_case
 from .solver import Batch, Geometry, Level
 
 SIZES = (32, 48, 64, 96, 128)
@@ -132,6 +132,41 @@ def config4(steps: int = 2000, n_cases: int = 64, seed: int = 4, storage: str = 
     B.close()
     for g in geoms:
         g.close()
+    return out
+
+
+# algorithmic HBM bytes of one D3Q39 KBC cell update (FP32): populations read + written (2 x 39 x 4),
+# multiplier cache read + written (2 x 13 x 4), velocity read + written (2 x 12), density written (4)
+KBC_BYTES_PER_CELL = 2 * 39 * 4 + 2 * 13 * 4 + 2 * 12 + 4
+
+
+def benchmark_entropic(n: int = 128, steps: int = 50, warmup: int = 5, u0: float = 0.1, re: float = 1000.0) -> dict:
+    """Time `steps` D3Q39 entropic KBC steps of an n^3 periodic Taylor-Green box (one CUDA graph,
+    CUDA events on the launching stream)."""
+    import torch
+    case = entropic_taylor_green_case(n, u0=u0, re=re)
+    geom = Geometry(case.dom)
+    lvl = Level(geom, "entropic")
+    lvl.init_equilibrium(case.rho, case.vel)
+    s = torch.cuda.Stream()
+    lvl.advance(case.params, warmup, s)
+    lvl.advance(case.params, steps, s)  # capture the timed graph outside the timed region
+    s.synchronize()
+    m0 = lvl.mass_momentum()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    lvl.advance(case.params, steps, s)
+    e1.record(s)
+    s.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    m1 = lvl.mass_momentum()
+    cells = n ** 3
+    out = {"workload": f"kbc_d3q39_taylor_green_{n}^3_f32_bisection_wale", "cells": cells, "steps": steps,
+           "ms_per_step": round(ms, 4), "mlups": round(cells / ms / 1e3, 1), "bytes_per_cell": KBC_BYTES_PER_CELL,
+           "achieved_gbs": round(cells * KBC_BYTES_PER_CELL / ms / 1e6, 1),
+           "mass_drift_rel": float(abs(m1[0] - m0[0]) / m0[0]), "gpu_launches": steps}
+    lvl.close()
+    geom.close()
     return out
 
 

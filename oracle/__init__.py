@@ -1,7 +1,8 @@
 """CPU ORACLE — test infrastructure only.
 
-C++ restatements of the reference's D3Q27 cumulant level step (oal_oracle.cpp) and of its D3Q19
-octree level step (oal_oracle_q19.cpp); each source holds the file:line map into the reference.
+C++ restatements of the reference's D3Q27 cumulant level step (oal_oracle.cpp), of its D3Q19
+octree level step (oal_oracle_q19.cpp) and of its D3Q39 entropic KBC level step
+(oal_oracle_q39.cpp); each source holds the file:line map into the reference.
 Only tests/, the smoke check and the CPU-baseline leg of bench.py use it; the product path never
 imports it.
 """
@@ -21,7 +22,8 @@ _lib = None
 
 
 def build(force: bool = False) -> Path:
-    deps = [HERE / "oal_oracle.cpp", HERE / "oal_oracle_q19.cpp", HERE.parent / "include" / "oal.h"]
+    deps = [HERE / "oal_oracle.cpp", HERE / "oal_oracle_q19.cpp", HERE / "oal_oracle_q39.cpp",
+            HERE.parent / "include" / "oal.h", HERE.parent / "openaerolab_alpha_01_b200" / "csrc" / "kbc_math.h"]
     if force or not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < max(d.stat().st_mtime for d in deps):
         subprocess.run(["make", "-s", "-C", str(HERE), "-B" if force else "liboal_oracle.so"], check=True)
     return LIB_PATH
@@ -60,6 +62,13 @@ def lib() -> C.CDLL:
         for suf in ("f32", "f64"):
             getattr(L, f"ora_q19_fill_{suf}").argtypes = [vp, vp, vp, vp, C.c_double, C.c_double, C.c_double, vp, vp, vp]
             getattr(L, f"ora_q19_restrict_{suf}").argtypes = [vp, vp, C.c_double, C.c_double, vp, vp, vp]
+        L.ora_q39_tables.argtypes = [vp] * 5
+        L.ora_q39_exp.argtypes = [i64, vp, vp]
+        L.ora_q39_log.argtypes = [i64, vp, vp]
+        L.ora_q39_equilibrium.argtypes = [i64, vp, vp, vp, vp]
+        L.ora_q39_inlet_equilibrium.argtypes = [C.c_float, vp]
+        L.ora_q39_collide_cells.argtypes = [i64, vp, vp, vp, vp, vp, vp, vp]
+        L.ora_q39_step.argtypes = [i32, vp, vp, vp, vp, vp, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -339,3 +348,98 @@ class OracleQ19Octree:
         for l, S in enumerate(self.levels, start=1):
             out += 8.0 ** (self.L - l) * S.totals()
         return out
+
+
+# ---- D3Q39 entropic KBC (oal_oracle_q39.cpp) ------------------------------------------------------
+
+def q39_tables():
+    cx, cy, cz, opp = (np.zeros(39, np.int32) for _ in range(4))
+    w = np.zeros(39, np.float32)
+    lib().ora_q39_tables(_p(cx), _p(cy), _p(cz), _p(w), _p(opp))
+    return dict(cx=cx, cy=cy, cz=cz, w=w, opp=opp)
+
+
+def q39_exp(x):
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.empty_like(x)
+    lib().ora_q39_exp(x.size, _p(x), _p(y))
+    return y
+
+
+def q39_log(x):
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.empty_like(x)
+    lib().ora_q39_log(x.size, _p(x), _p(y))
+    return y
+
+
+def q39_equilibrium(rho, u):
+    """13-moment equilibrium from the polynomial start: rho (n,), u (n,3) -> feq (n,39), lambda (n,13)."""
+    rho = np.ascontiguousarray(rho, np.float32)
+    u = np.ascontiguousarray(u, np.float32).reshape(-1, 3)
+    n = rho.size
+    feq = np.zeros((n, 39), np.float32)
+    lam = np.zeros((n, 13), np.float32)
+    lib().ora_q39_equilibrium(n, _p(rho), _p(u), _p(feq), _p(lam))
+    return feq, lam
+
+
+def q39_inlet_equilibrium(u_inlet):
+    out = np.zeros(39, np.float32)
+    lib().ora_q39_inlet_equilibrium(float(u_inlet), _p(out))
+    return out
+
+
+def q39_collide(params, f, g, lam):
+    """Collision of independent cells: f (n,39), g (n,9) with g[3a+b] = d u_a / d x_b, lam (n,13)
+    (NaN row = no warm start) -> (f_out, rho, u, lam_out)."""
+    f = np.ascontiguousarray(f, np.float32)
+    n = f.shape[0]
+    g = np.ascontiguousarray(g, np.float32)
+    lam = np.array(lam, np.float32, copy=True, order="C")
+    fo = np.zeros_like(f)
+    rho = np.zeros(n, np.float32)
+    u = np.zeros((n, 3), np.float32)
+    lib().ora_q39_collide_cells(n, C.addressof(params), _p(f), _p(g), _p(lam), _p(fo), _p(rho), _p(u))
+    return fo, rho, u, lam
+
+
+class OracleQ39Level:
+    """D3Q39 entropic level in the reference layout, stepped by the CPU restatement (float32):
+    f (39, nb, 512), rho (nb, 512), vel (3, nb, 512), lam (13, nb, 512) with NaN = no warm start;
+    nbr (27, nb) 1-based with every neighbour present."""
+
+    def __init__(self, nbr):
+        self.nbr = np.ascontiguousarray(nbr, np.int32)
+        self.nb = self.nbr.shape[1]
+        nb = self.nb
+        self.f = np.zeros((39, nb, 512), np.float32)
+        self.g = np.zeros_like(self.f)
+        self.rho = np.ones((nb, 512), np.float32)
+        self.vel = np.zeros((3, nb, 512), np.float32)
+        self.vel_new = np.zeros_like(self.vel)
+        self.lam = np.full((13, nb, 512), np.nan, np.float32)
+
+    def init_equilibrium(self, rho, vel):
+        rho = np.asarray(rho, np.float32).reshape(self.nb * 512)
+        vel = np.asarray(vel, np.float32).reshape(3, self.nb * 512)
+        feq, _ = q39_equilibrium(rho, vel.T)
+        self.f[...] = feq.T.reshape(39, self.nb, 512)
+        self.rho[...] = rho.reshape(self.nb, 512)
+        self.vel[...] = vel.reshape(3, self.nb, 512)
+        self.lam[...] = np.nan
+        return self
+
+    def step(self, params, n=1):
+        for _ in range(n):
+            lib().ora_q39_step(self.nb, _p(self.nbr), C.addressof(params), _p(self.f), _p(self.g), _p(self.vel),
+                               _p(self.vel_new), _p(self.rho), _p(self.lam))
+            self.f, self.g = self.g, self.f
+            self.vel, self.vel_new = self.vel_new, self.vel
+        return self
+
+    def mass_momentum(self):
+        t = q39_tables()
+        f = self.f.astype(np.float64)
+        c = np.stack([t["cx"], t["cy"], t["cz"]]).astype(np.float64)
+        return np.array([f.sum(), *(np.tensordot(c, f, axes=(1, 0)).sum(axis=(1, 2)))])
