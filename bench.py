@@ -197,6 +197,8 @@ def main():
     ap.add_argument("--layout", default="block", choices=["block", "dense"], help="population layout of the level")
     ap.add_argument("--q19-steps", type=int, default=100,
                     help="steps of the D3Q19 octree periodic-box measurement (256^3, FP32 and FP64); 0 skips it")
+    ap.add_argument("--kbc-steps", type=int, default=20,
+                    help="steps of the D3Q39 entropic KBC measurement (128^3 periodic Taylor-Green, FP32); 0 skips it")
     ap.add_argument("--batch-steps", type=int, default=200,
                     help="steps of the batched-vs-plain-loop comparison (64-case config 4); 0 skips it")
     args = ap.parse_args()
@@ -331,6 +333,12 @@ def main():
             c3 = benchmark_naca(steps=args.q19_steps)
             c3["roofline_frac"] = round(c3["achieved_gbs"] / peak, 4)
             line["octree_config3"] = c3
+        if args.kbc_steps > 0:
+            from openaerolab_alpha_01_b200.workloads import benchmark_entropic
+            kb = benchmark_entropic(128, steps=args.kbc_steps, warmup=3)
+            kb["roofline_frac"] = round(kb["achieved_gbs"] / peak, 4)
+            kb["bound"] = "FP32 issue (13-moment Newton sweeps and entropy evaluations), not HBM"
+            line["kbc_d3q39"] = kb
         if args.batch_steps > 0:
             from openaerolab_alpha_01_b200.workloads import config4
             line["batched"] = config4(steps=args.batch_steps, storage=args.storage)
