@@ -272,6 +272,33 @@ oal_status oal_level_entropic_lambda(oal_level* L, float* get_host, const float*
  * Z = l+1); dense = 0: block-major f[b][k][cell], element b*block_stride + k*dir_stride + cell. */
 oal_status oal_level_layout(const oal_level* L, int64_t out[6]);
 
+/* ---- block AMR: D3Q27 levels with 2:1 refinement in space and time --------------------------
+ * Replaces recursive_step! / recursive_step_temporal! / execute_timestep_batch!
+ * (src/solver/solver_control.jl:55-828), the refined levels' parent interpolation
+ * interpolate_with_rescaling (src/collision/physics_interpolation.jl:705-1198, called from
+ * kernel_cumulant.jl:286-316,346-388) and restrict_fine_to_parent! (src/collision/amr_coupling.jl:
+ * 7562-8035, kernel :1900-3242), at the reference's default settings: temporal interpolation on (the
+ * parent's state before and after its step, child substeps at weights 0 and 1/2), cubic Lagrange
+ * macros and f_neq with the extrapolating trilinear fallback, the post-collision f_neq factor, the
+ * children-average restriction with two moment-correction passes. Level l (0-based) has a block grid
+ * of 2^l x the coarse one and a geometry whose nx/ny/nz are 8 x that grid (its cells at its own
+ * resolution; domain faces apply at every level); every block of level l > 0 lies inside a block of
+ * level l - 1. A coarse step steps level 0 once, then (recursively) each finer level twice, then
+ * restricts it onto its parent. */
+typedef struct oal_amr oal_amr;
+typedef struct oal_amr_level_desc {
+  const oal_geometry* geometry;  /* the level's blocks (coordinates in its block grid, 1-based) */
+  int32_t dim[3];                /* block-grid extent of the level */
+  int32_t reserved;
+} oal_amr_level_desc;
+oal_status oal_amr_create(int32_t nlevels, const oal_amr_level_desc* levels, int32_t storage, oal_amr** out);
+void oal_amr_destroy(oal_amr* A);
+/* The state of level `level` (0 = coarsest), owned by the hierarchy: initialise, read or write it with
+ * the oal_level_* calls (init_equilibrium, get_state, set_state, mass_momentum, get_forces). */
+oal_status oal_amr_level(oal_amr* A, int32_t level, oal_level** out);
+/* n coarse steps as one CUDA graph; params[l] are level l's step parameters (tau per level). */
+oal_status oal_amr_advance(oal_amr* A, const oal_step_params* params, int32_t n_coarse_steps, void* stream);
+
 /* ---- batches: many cases stepped by one launch per kernel ------------------------------------ */
 /* A batch owns a block pool (populations in `storage`, macros, masks) and steps every member case
  * with one launch per kernel per step; n steps are one CUDA graph. Members are added and removed

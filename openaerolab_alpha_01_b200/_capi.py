@@ -106,6 +106,14 @@ class GeometryDesc(C.Structure):
     ]
 
 
+class AmrLevelDesc(C.Structure):
+    _fields_ = [
+        ("geometry", C.c_void_p),
+        ("dim", C.c_int32 * 3),
+        ("reserved", C.c_int32),
+    ]
+
+
 class LevelFields(C.Structure):
     _fields_ = [
         ("f_in", C.c_void_p),
@@ -254,6 +262,10 @@ _SIGNATURES = {
     "oal_level_device_bytes": (C.c_int64, [C.c_void_p]),
     "oal_level_layout": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
     "oal_level_entropic_lambda": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "oal_amr_create": (C.c_int32, [C.c_int32, C.POINTER(AmrLevelDesc), C.c_int32, C.POINTER(C.c_void_p)]),
+    "oal_amr_destroy": (None, [C.c_void_p]),
+    "oal_amr_level": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p)]),
+    "oal_amr_advance": (C.c_int32, [C.c_void_p, C.POINTER(StepParams), C.c_int32, C.c_void_p]),
     "oal_batch_create": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                      C.POINTER(C.c_void_p)]),
     "oal_batch_destroy": (None, [C.c_void_p]),

@@ -94,6 +94,40 @@ enum BlockFlags : uint32_t {
 // Kernel argument block of one launch. Element strides address either the reference layout
 // (block stride 512, direction stride 512*n_blocks) or the block-major layout of library-owned
 // state (block stride 512*Q, direction stride 512).
+// The parent level seen from a refined level (block AMR, perform_timestep_v2!'s parent_* arguments):
+// pulls from outside the level's blocks but inside the domain are interpolated from it. ptr == null
+// on level 1.
+struct ParentView {
+  const void* f_new;    // storage type, block-major (block stride 27*512, direction stride 512)
+  const void* f_old;    // the same before the parent's step, or null
+  const void* rho_new;  // compute type, [nb*512]
+  const void* rho_old;
+  const void* vel_new;  // compute type, component stride nb*512
+  const void* vel_old;
+  const int32_t* ptr;   // [dim_x*dim_y*dim_z], x fastest: 1-based parent block, 0 = none
+  int32_t dim_x, dim_y, dim_z, nb;
+  double tau_parent, tau_fine, tw;
+  int32_t use_temporal, level_visc_physical;
+};
+
+// Restriction of a child level onto its parent (block AMR)
+struct RestrictArgs {
+  void* pf;                 // parent's current populations (storage type), block-major
+  void* prho;               // parent's density (compute type), [pnb*512]
+  void* pvel;               // parent's current velocity, component stride pnb*512
+  const int4* pbinfo;       // parent block coordinates (1-based)
+  const int32_t* covered;   // parent blocks that have children
+  int32_t n_covered, pnb;
+  const void* cf;           // child's current populations (storage type), block-major
+  const int32_t* cptr;      // child block pointer [cdx*cdy*cdz], x fastest, 1-based, 0 = none
+  int32_t cdx, cdy, cdz;
+  const uint32_t* cbflags;  // child solid masks (BF_NEAR_SOLID blocks, bit 13 = own cell solid)
+  const int32_t* cmslot;
+  const uint32_t* ccmask;
+  double ratio;             // tau ratio of the f_neq rescale (with the post-collision factor)
+  int32_t comp;
+};
+
 struct StepArgs {
   const void* f_in;
   void* f_out;
@@ -121,6 +155,7 @@ struct StepArgs {
   int32_t PX, PY, PZ;
   uint32_t* err;                  // device error word (bounded waits that gave up), or null
   CaseParams p0;
+  ParentView par;                 // refined levels only (par.ptr == null otherwise)
 };
 
 // Element index of cell (X, Y, Z) of the dense padded population grid (direction 0).

@@ -50,6 +50,226 @@ __device__ __forceinline__ R dec_k(const S* __restrict__ f, int64_t i, int k) {
   return Codec<S>::dec(f[i], R(q27_w(k)), R(1.0 / q27_w(k)));
 }
 
+// ------------------------------------------------------------------------------------------------
+// block AMR: parent interpolation of a refined level's pulls (physics_interpolation.jl:705-1198 at
+// the reference's default flags: cubic Lagrange macros over the 64 parent nodes when all exist,
+// else the trilinear / extrapolated macros of sample_parent_macro_for_fine_cell; cubic f_neq over
+// the time-blended parent nodes; f_neq scaled by (tau_f - 1/2)/(tau_c - 1/2) and the
+// post-collision factor (1 - omega_f)/(1 - omega_c))
+// ------------------------------------------------------------------------------------------------
+template <class R>
+struct PNode {
+  R f, rho, ux, uy, uz, fneq;
+  bool ok;
+};
+
+// parent cell (1-based global index) -> element of the cell (block * 512 + cell), -1 when absent
+__device__ __forceinline__ int64_t parent_cell(const ParentView& P, int pgx, int pgy, int pgz) {
+  if (pgx < 1 || pgy < 1 || pgz < 1) return -1;
+  const int pbx = (pgx - 1) / kBS + 1, pby = (pgy - 1) / kBS + 1, pbz = (pgz - 1) / kBS + 1;
+  if (pbx > P.dim_x || pby > P.dim_y || pbz > P.dim_z) return -1;
+  const int32_t pb = P.ptr[(pbx - 1) + (int64_t)P.dim_x * ((pby - 1) + (int64_t)P.dim_y * (pbz - 1))];
+  if (pb <= 0) return -1;
+  return (int64_t)(pb - 1) * kCells + (((pgx - 1) % kBS) | (((pgy - 1) % kBS) << 3) | (((pgz - 1) % kBS) << 6));
+}
+
+template <class R>
+__device__ __forceinline__ void parent_bracket(R p_cont, int n, int& i0, int& i1, R& w) {
+  if (n <= 1) { i0 = 1; i1 = 1; w = R(0); return; }
+  const R pc = fmin(fmax(p_cont, R(1)), R(n));
+  i0 = min(max((int)floor(pc), 1), n - 1);
+  i1 = i0 + 1;
+  w = fmin(fmax(pc - R(i0), R(0)), R(1));
+}
+
+template <class S, class R>
+__device__ PNode<R> parent_blended(const ParentView& P, int pgx, int pgy, int pgz, int k, R wk, R cx, R cy, R cz,
+                                   bool comp) {
+  const int64_t c = parent_cell(P, pgx, pgy, pgz);
+  if (c < 0) return PNode<R>{wk, R(1), R(0), R(0), R(0), R(0), false};
+  const int64_t n = (int64_t)P.nb * kCells;
+  const int64_t fi = (c >> 9) * (27 * kCells) + k * kCells + (c & 511);
+  const S* fn = static_cast<const S*>(P.f_new);
+  const R* rn = static_cast<const R*>(P.rho_new);
+  const R* vn = static_cast<const R*>(P.vel_new);
+  R f = Codec<S>::dec(fn[fi], R(q27_w(k)), R(1.0 / q27_w(k)));
+  R rho = rn[c], ux = vn[c], uy = vn[c + n], uz = vn[c + 2 * n];
+  if (P.use_temporal == 1 && R(P.tw) < R(0.99) && P.f_old) {
+    const R tw = R(P.tw);
+    const S* fo = static_cast<const S*>(P.f_old);
+    const R* ro = static_cast<const R*>(P.rho_old);
+    const R* vo = static_cast<const R*>(P.vel_old);
+    f = Codec<S>::dec(fo[fi], R(q27_w(k)), R(1.0 / q27_w(k))) * (R(1) - tw) + f * tw;
+    rho = ro[c] * (R(1) - tw) + rho * tw;
+    ux = vo[c] * (R(1) - tw) + ux * tw;
+    uy = vo[c + n] * (R(1) - tw) + uy * tw;
+    uz = vo[c + 2 * n] * (R(1) - tw) + uz * tw;
+  }
+  const R feqc = feq_c<R>(rho, ux, uy, uz, wk, cx, cy, cz, comp);
+  return PNode<R>{f, rho, ux, uy, uz, f - feqc, true};
+}
+
+template <class R>
+__device__ PNode<R> parent_macro(const ParentView& P, int pgx, int pgy, int pgz) {
+  const int64_t c = parent_cell(P, pgx, pgy, pgz);
+  if (c < 0) return PNode<R>{R(0), R(1), R(0), R(0), R(0), R(0), false};
+  const int64_t n = (int64_t)P.nb * kCells;
+  const R* rn = static_cast<const R*>(P.rho_new);
+  const R* vn = static_cast<const R*>(P.vel_new);
+  R rho = rn[c], ux = vn[c], uy = vn[c + n], uz = vn[c + 2 * n];
+  if (P.use_temporal == 1 && R(P.tw) < R(0.99) && P.rho_old) {
+    const R tw = R(P.tw);
+    const R* ro = static_cast<const R*>(P.rho_old);
+    const R* vo = static_cast<const R*>(P.vel_old);
+    rho = ro[c] * (R(1) - tw) + rho * tw;
+    ux = vo[c] * (R(1) - tw) + ux * tw;
+    uy = vo[c + n] * (R(1) - tw) + uy * tw;
+    uz = vo[c + 2 * n] * (R(1) - tw) + uz * tw;
+  }
+  return PNode<R>{R(0), rho, ux, uy, uz, R(0), true};
+}
+
+template <class R>
+__device__ __forceinline__ R lagrange3(int i, R w) {
+  return i == -1 ? (-w * (w - R(1)) * (w - R(2)) / R(6))
+       : i == 0  ? ((w + R(1)) * (w - R(1)) * (w - R(2)) / R(2))
+       : i == 1  ? (-w * (w + R(1)) * (w - R(2)) / R(2))
+                 : (w * (w + R(1)) * (w - R(1)) / R(6));
+}
+
+// sample_parent_macro_for_fine_cell (physics_interpolation.jl:188-346)
+template <class R>
+__device__ bool parent_sample_macro(const ParentView& P, int fgx, int fgy, int fgz, R& r_out, R& x_out, R& y_out,
+                                    R& z_out) {
+  int px0, px1, py0, py1, pz0, pz1;
+  R wx, wy, wz;
+  parent_bracket<R>(R(fgx) * R(0.5) + R(0.25), P.dim_x * kBS, px0, px1, wx);
+  parent_bracket<R>(R(fgy) * R(0.5) + R(0.25), P.dim_y * kBS, py0, py1, wy);
+  parent_bracket<R>(R(fgz) * R(0.5) + R(0.25), P.dim_z * kBS, pz0, pz1, wz);
+  PNode<R> d[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) d[c] = parent_macro<R>(P, (c & 1) ? px1 : px0, (c & 2) ? py1 : py0, (c & 4) ? pz1 : pz0);
+  const R w[8] = {(R(1) - wx) * (R(1) - wy) * (R(1) - wz), wx * (R(1) - wy) * (R(1) - wz),
+                  (R(1) - wx) * wy * (R(1) - wz),         wx * wy * (R(1) - wz),
+                  (R(1) - wx) * (R(1) - wy) * wz,         wx * (R(1) - wy) * wz,
+                  (R(1) - wx) * wy * wz,                  wx * wy * wz};
+  bool all = true, any = false;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) { all = all && d[c].ok; any = any || d[c].ok; }
+  if (!all) {
+    if (!any) { r_out = R(1); x_out = y_out = z_out = R(0); return false; }
+    const int pxm = px0 - 1, pxp = px1 + 1, pym = py0 - 1, pyp = py1 + 1, pzm = pz0 - 1, pzp = pz1 + 1;
+    // edges in the reference's order: along x, then y, then z; (a, b, far of a, far of b)
+    const int ea[12] = {0, 2, 4, 6, 0, 1, 4, 5, 0, 1, 2, 3};
+    const int eb[12] = {1, 3, 5, 7, 2, 3, 6, 7, 4, 5, 6, 7};
+#pragma unroll 1
+    for (int e = 0; e < 12; ++e) {
+      const int a = ea[e], b = eb[e];
+      if (d[a].ok == d[b].ok) continue;
+      const int src = d[a].ok ? a : b, dst = d[a].ok ? b : a;
+      // the far node continues the edge beyond the valid node
+      int gx = (src & 1) ? px1 : px0, gy = (src & 2) ? py1 : py0, gz = (src & 4) ? pz1 : pz0;
+      if (e < 4) gx = d[a].ok ? pxm : pxp;
+      else if (e < 8) gy = d[a].ok ? pym : pyp;
+      else gz = d[a].ok ? pzm : pzp;
+      const PNode<R> fd = parent_macro<R>(P, gx, gy, gz);
+      const PNode<R> s0 = d[src];
+      d[dst].rho = fd.ok ? R(2) * s0.rho - fd.rho : s0.rho;
+      d[dst].ux = fd.ok ? R(2) * s0.ux - fd.ux : s0.ux;
+      d[dst].uy = fd.ok ? R(2) * s0.uy - fd.uy : s0.uy;
+      d[dst].uz = fd.ok ? R(2) * s0.uz - fd.uz : s0.uz;
+      d[dst].ok = true;
+    }
+  }
+  R r = w[0] * d[0].rho, ux = w[0] * d[0].ux, uy = w[0] * d[0].uy, uz = w[0] * d[0].uz;
+#pragma unroll
+  for (int c = 1; c < 8; ++c) {
+    r = r + w[c] * d[c].rho; ux = ux + w[c] * d[c].ux; uy = uy + w[c] * d[c].uy; uz = uz + w[c] * d[c].uz;
+  }
+  r_out = r; x_out = ux; y_out = uy; z_out = uz;
+  return true;
+}
+
+// interpolate_with_rescaling at the fine cell (fgx, fgy, fgz) of the refined level, direction k
+template <class S, class R>
+__device__ __noinline__ R parent_population(const ParentView& P, int fgx, int fgy, int fgz, int k, R cx, R cy, R cz,
+                                            bool comp) {
+  const R wk = R(q27_w(k));
+  const int pnx = P.dim_x * kBS, pny = P.dim_y * kBS, pnz = P.dim_z * kBS;
+  int px0, px1, py0, py1, pz0, pz1;
+  R wx, wy, wz;
+  parent_bracket<R>(R(fgx) * R(0.5) + R(0.25), pnx, px0, px1, wx);
+  parent_bracket<R>(R(fgy) * R(0.5) + R(0.25), pny, py0, py1, wy);
+  parent_bracket<R>(R(fgz) * R(0.5) + R(0.25), pnz, pz0, pz1, wz);
+  const bool use_cubic = px0 - 2 >= 1 && px0 + 2 <= pnx && py0 - 2 >= 1 && py0 + 2 <= pny && pz0 - 2 >= 1 &&
+                         pz0 + 2 <= pnz;
+  PNode<R> d[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c)
+    d[c] = parent_blended<S, R>(P, (c & 1) ? px1 : px0, (c & 2) ? py1 : py0, (c & 4) ? pz1 : pz0, k, wk, cx, cy, cz,
+                                comp);
+  int anchor = 7;
+#pragma unroll
+  for (int c = 6; c >= 0; --c)
+    if (d[c].ok) anchor = c;
+  PNode<R> v[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) v[c] = d[c].ok ? d[c] : d[anchor];
+  auto trilin = [&](R PNode<R>::*m) {
+    const R c00 = (v[0].*m) * (R(1) - wx) + (v[1].*m) * wx;
+    const R c01 = (v[4].*m) * (R(1) - wx) + (v[5].*m) * wx;
+    const R c10 = (v[2].*m) * (R(1) - wx) + (v[3].*m) * wx;
+    const R c11 = (v[6].*m) * (R(1) - wx) + (v[7].*m) * wx;
+    const R c0 = c00 * (R(1) - wy) + c10 * wy;
+    const R c1 = c01 * (R(1) - wy) + c11 * wy;
+    return c0 * (R(1) - wz) + c1 * wz;
+  };
+  bool cubic_all_valid = use_cubic;
+  if (use_cubic) {
+#pragma unroll 1
+    for (int i = 0; i < 64 && cubic_all_valid; ++i)
+      if (parent_cell(P, px0 + (i >> 4) - 1, py0 + ((i >> 2) & 3) - 1, pz0 + (i & 3) - 1) < 0) cubic_all_valid = false;
+  }
+  R rho_i, ux_i, uy_i, uz_i;
+  if (cubic_all_valid) {
+    rho_i = ux_i = uy_i = uz_i = R(0);
+#pragma unroll 1
+    for (int i = 0; i < 64; ++i) {
+      const int a = (i >> 4) - 1, bb = ((i >> 2) & 3) - 1, c = (i & 3) - 1;
+      const PNode<R> m = parent_macro<R>(P, px0 + a, py0 + bb, pz0 + c);
+      const R w3 = lagrange3<R>(a, wx) * lagrange3<R>(bb, wy) * lagrange3<R>(c, wz);
+      rho_i += w3 * m.rho;
+      ux_i += w3 * m.ux;
+      uy_i += w3 * m.uy;
+      uz_i += w3 * m.uz;
+    }
+  } else if (!parent_sample_macro<R>(P, fgx, fgy, fgz, rho_i, ux_i, uy_i, uz_i)) {
+    rho_i = trilin(&PNode<R>::rho); ux_i = trilin(&PNode<R>::ux);
+    uy_i = trilin(&PNode<R>::uy); uz_i = trilin(&PNode<R>::uz);
+  }
+  const R feq_i = feq_c<R>(rho_i, ux_i, uy_i, uz_i, wk, cx, cy, cz, comp);
+  R f_neq = R(0);
+  if (use_cubic) {
+    const R anchor_neq = d[anchor].fneq;
+#pragma unroll 1
+    for (int i = 0; i < 64; ++i) {
+      const int a = (i >> 4) - 1, bb = ((i >> 2) & 3) - 1, c = (i & 3) - 1;
+      const PNode<R> nd = parent_blended<S, R>(P, px0 + a, py0 + bb, pz0 + c, k, wk, cx, cy, cz, comp);
+      f_neq += lagrange3<R>(a, wx) * lagrange3<R>(bb, wy) * lagrange3<R>(c, wz) * (nd.ok ? nd.fneq : anchor_neq);
+    }
+  } else {
+    f_neq = trilin(&PNode<R>::fneq);
+  }
+  const R tau_p = R(P.tau_parent), tau_f = R(P.tau_fine);
+  const R tau_c = tau_p - R(0.5), tau_fm = tau_f - R(0.5);
+  R scale = tau_c > R(1e-6) ? fmin(fmax(tau_fm / tau_c, R(0.01)), R(100)) : R(1);
+  if (P.level_visc_physical == 1) scale = fmin(fmax(tau_f / (R(2) * fmax(tau_p, R(0.500001))), R(0.01)), R(100));
+  const R omega_c = R(1) / fmax(tau_p, R(0.500001)), omega_f = R(1) / fmax(tau_f, R(0.500001));
+  const R one_m_wc = R(1) - omega_c, one_m_wf = R(1) - omega_f;
+  if (fabs(one_m_wc) > R(1e-6)) scale = fmin(fmax(scale * (one_m_wf / one_m_wc), R(0.01)), R(100));
+  return feq_i + f_neq * scale;
+}
+
 // Population arriving at cell (x,y,z) of block b in direction k from outside every block
 // (kernel_cumulant.jl:221-391), level without parent. `nbr` is the block's 27-entry row; entries
 // >= n_real are ghost blocks, which count as missing here. k may be a run-time value.
@@ -95,7 +315,12 @@ __device__ __forceinline__ R face_population_impl(const S* __restrict__ fin, int
           src = bbase + (zw_ix + 8 * zw_iy + 64 * z) + j * kst;
         } else {
           const int zw_nb = nbr[nbr_dir(zw_ix >> 3, zw_iy >> 3, 0)];
-          if (zw_nb >= 0 && zw_nb < n_real) src = (int64_t)zw_nb * bst + j * kst + ((zw_ix & 7) + 8 * (zw_iy & 7) + 64 * z);
+          if (zw_nb >= 0 && zw_nb < n_real) {
+            src = (int64_t)zw_nb * bst + j * kst + ((zw_ix & 7) + 8 * (zw_iy & 7) + 64 * z);
+          } else if (da && da->par.ptr && src_gy >= 1 && src_gy <= cp.ny) {
+            // refined level: the image cell comes from the parent (kernel_cumulant.jl:286-312)
+            return parent_population<S, R>(da->par, src_gx, src_gy, gz, j, R(cx), R(cy), R(-cz), comp);
+          }
         }
       }
     }
@@ -108,6 +333,9 @@ __device__ __forceinline__ R face_population_impl(const S* __restrict__ fin, int
     j = q27_mir_y(k);
   } else if (is_z_min || is_z_max) {
     j = q27_mir_z(k);
+  } else if (da && da->par.ptr) {
+    // refined level: interpolated from the parent (kernel_cumulant.jl:346-388)
+    return parent_population<S, R>(da->par, src_gx, src_gy, src_gz, k, R(cx), R(cy), R(cz), comp);
   } else {
     return R(q27_w(k));  // kernel_cumulant.jl:389-391
   }
@@ -166,7 +394,7 @@ __global__ void __launch_bounds__(256) k_fill_ghosts(const StepArgs a, const uin
     f[slot] = Codec<S>::enc(val, R(q27_w(k)), R(1.0 / q27_w(k)));
   } else {
     const R val = face_population_impl<S, R>(f, (int64_t)b * bst, cell, kst, nbr, a.n_blocks, bst, k, x, y, z, gx, gy,
-                                             gz, cp);
+                                             gz, cp, &a);
     const int sx = x - cx, sy = y - cy, sz = z - cz;
     const int g = nbr[nbr_dir(sx >> 3, sy >> 3, sz >> 3)];
     f[(int64_t)g * bst + k * kst + ((sx & 7) | ((sy & 7) << 3) | ((sz & 7) << 6))] =
@@ -545,6 +773,157 @@ __global__ void __launch_bounds__(128) k_cumulant_gen(const StepArgs a, const in
 // ------------------------------------------------------------------------------------------------
 // launchers
 // ------------------------------------------------------------------------------------------------
+// ------------------------------------------------------------------------------------------------
+// block AMR: restriction of a child level onto its parent (restrict_child_state_to_parent_kernel!,
+// amr_coupling.jl:1900-3242, default flags): every parent cell whose 8 children exist takes the
+// average of its fluid children, f = feq + ratio (avg - feq), two moment-correction passes
+// (solve_shell_moment4, :130-176) and the shell macros. One thread per parent cell of a block
+// that has children; the parent's populations stay in registers (the reference keeps Float32).
+// ------------------------------------------------------------------------------------------------
+template <class R>
+__device__ __forceinline__ bool shell_solve4(R m00, R m01, R m02, R m03, R m11, R m12, R m13, R m22, R m23, R m33,
+                                             R r0, R r1, R r2, R r3, R& x0, R& x1, R& x2, R& x3) {
+  const R eps = R(1e-12);
+  R a00 = m00 + eps, a01 = m01, a02 = m02, a03 = m03, b0 = r0;
+  R a10 = m01, a11 = m11 + eps, a12 = m12, a13 = m13, b1 = r1;
+  R a20 = m02, a21 = m12, a22 = m22 + eps, a23 = m23, b2 = r2;
+  R a30 = m03, a31 = m13, a32 = m23, a33 = m33 + eps, b3 = r3;
+  const bool ok0 = fabs(a00) > eps;
+  const R inv0 = ok0 ? R(1) / a00 : R(0);
+  const R f10 = a10 * inv0, f20 = a20 * inv0, f30 = a30 * inv0;
+  a11 -= f10 * a01; a12 -= f10 * a02; a13 -= f10 * a03; b1 -= f10 * b0;
+  a21 -= f20 * a01; a22 -= f20 * a02; a23 -= f20 * a03; b2 -= f20 * b0;
+  a31 -= f30 * a01; a32 -= f30 * a02; a33 -= f30 * a03; b3 -= f30 * b0;
+  const bool ok1 = fabs(a11) > eps;
+  const R inv1 = ok1 ? R(1) / a11 : R(0);
+  const R f21 = a21 * inv1, f31 = a31 * inv1;
+  a22 -= f21 * a12; a23 -= f21 * a13; b2 -= f21 * b1;
+  a32 -= f31 * a12; a33 -= f31 * a13; b3 -= f31 * b1;
+  const bool ok2 = fabs(a22) > eps;
+  const R inv2 = ok2 ? R(1) / a22 : R(0);
+  const R f32 = a32 * inv2;
+  a33 -= f32 * a23; b3 -= f32 * b2;
+  const bool ok3 = fabs(a33) > eps;
+  const R inv3 = ok3 ? R(1) / a33 : R(0);
+  x3 = b3 * inv3;
+  x2 = (b2 - a23 * x3) * inv2;
+  x1 = (b1 - a12 * x2 - a13 * x3) * inv1;
+  x0 = (b0 - a01 * x1 - a02 * x2 - a03 * x3) * inv0;
+  return ok0 && ok1 && ok2 && ok3;
+}
+
+template <class S, class R>
+__global__ void __launch_bounds__(128) k_restrict(const RestrictArgs r) {
+  const int pb = r.covered[blockIdx.x >> 2];
+  const int cell = ((blockIdx.x & 3) << 7) | threadIdx.x;
+  const int lx = (cell & 7) + 1, ly = ((cell >> 3) & 7) + 1, lz = (cell >> 6) + 1;
+  const int4 bi = r.pbinfo[pb];
+  const int cbx0 = 2 * bi.x - 1, cby0 = 2 * bi.y - 1, cbz0 = 2 * bi.z - 1;
+  int32_t cblk[8], ccell[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int sx = i >> 2, sy = (i >> 1) & 1, sz = i & 1;  // sx outer, sz inner (the reference's order)
+    const int fx = 2 * (lx - 1) + 1 + sx, fy = 2 * (ly - 1) + 1 + sy, fz = 2 * (lz - 1) + 1 + sz;
+    const int cbx = cbx0 + (fx - 1) / kBS, cby = cby0 + (fy - 1) / kBS, cbz = cbz0 + (fz - 1) / kBS;
+    if (cbx < 1 || cby < 1 || cbz < 1 || cbx > r.cdx || cby > r.cdy || cbz > r.cdz) return;
+    const int32_t cb = r.cptr[(cbx - 1) + (int64_t)r.cdx * ((cby - 1) + (int64_t)r.cdy * (cbz - 1))];
+    if (cb == 0) return;
+    cblk[i] = cb - 1;
+    ccell[i] = ((fx - 1) % kBS) | (((fy - 1) % kBS) << 3) | (((fz - 1) % kBS) << 6);
+  }
+  const S* cf = static_cast<const S*>(r.cf);
+  R avg[kQ27];
+#pragma unroll
+  for (int k = 0; k < kQ27; ++k) avg[k] = R(0);
+  int fluid = 0;
+#pragma unroll 1
+  for (int i = 0; i < 8; ++i) {
+    const int cb = cblk[i];
+    if ((r.cbflags[cb] & BF_NEAR_SOLID) && ((r.ccmask[(int64_t)r.cmslot[cb] * kCells + ccell[i]] >> 13) & 1u)) continue;
+    ++fluid;
+    const int64_t base = (int64_t)cb * (27 * kCells) + ccell[i];
+#pragma unroll
+    for (int k = 0; k < kQ27; ++k) avg[k] += Codec<S>::dec(cf[base + k * kCells], R(q27_w(k)), R(1.0 / q27_w(k)));
+  }
+  if (fluid == 0) return;
+  const R inv_children = R(1) / R(fluid);
+  R rho_raw = R(0), jx = R(0), jy = R(0), jz = R(0);
+#pragma unroll
+  for (int k = 0; k < kQ27; ++k) {
+    const R favg = avg[k] * inv_children;
+    avg[k] = favg;
+    rho_raw += favg;
+    jx += favg * R(q27_cx(k));
+    jy += favg * R(q27_cy(k));
+    jz += favg * R(q27_cz(k));
+  }
+  const R rho_p = fmax(rho_raw, R(0.01));
+  const R inv_rho = R(1) / rho_p;
+  const R ux = jx * inv_rho, uy = jy * inv_rho, uz = jz * inv_rho;
+  const bool comp = r.comp != 0;
+  const R ratio = R(r.ratio);
+  S* pf = static_cast<S*>(r.pf);
+  const int64_t pbase = (int64_t)pb * (27 * kCells) + cell;
+  R fp[kQ27];
+#pragma unroll
+  for (int k = 0; k < kQ27; ++k) {
+    const R feq = feq_c<R>(rho_p, ux, uy, uz, R(q27_w(k)), R(q27_cx(k)), R(q27_cy(k)), R(q27_cz(k)), comp);
+    const R prior = Codec<S>::dec(pf[pbase + k * kCells], R(q27_w(k)), R(1.0 / q27_w(k)));
+    const R fr = feq + ratio * (avg[k] - feq);
+    fp[k] = fmax(R(1) * fr + R(0) * prior, R(1e-10));
+  }
+  R m00 = 0, m01 = 0, m02 = 0, m03 = 0, m11 = 0, m12 = 0, m13 = 0, m22 = 0, m23 = 0, m33 = 0;
+#pragma unroll
+  for (int k = 0; k < kQ27; ++k) {
+    const R cx = R(q27_cx(k)), cy = R(q27_cy(k)), cz = R(q27_cz(k)), w = R(q27_w(k));
+    m00 += w; m01 += w * cx; m02 += w * cy; m03 += w * cz;
+    m11 += w * cx * cx; m12 += w * cx * cy; m13 += w * cx * cz;
+    m22 += w * cy * cy; m23 += w * cy * cz; m33 += w * cz * cz;
+  }
+  const R inv_cs2 = R(1) / fmax(R(1.0 / 3.0), R(1e-6));
+#pragma unroll 1
+  for (int pass = 0; pass < 2; ++pass) {
+    R rr = R(0), rx = R(0), ry = R(0), rz = R(0);
+#pragma unroll
+    for (int k = 0; k < kQ27; ++k) {
+      rr += fp[k]; rx += fp[k] * R(q27_cx(k)); ry += fp[k] * R(q27_cy(k)); rz += fp[k] * R(q27_cz(k));
+    }
+    const R dr = rho_p - rr, dx = jx - rx, dy = jy - ry, dz = jz - rz;
+    if (fabs(dr) > R(1e-12) || fabs(dx) > R(1e-12) || fabs(dy) > R(1e-12) || fabs(dz) > R(1e-12)) {
+      R c0, c1, c2, c3;
+      const bool ok = shell_solve4<R>(m00, m01, m02, m03, m11, m12, m13, m22, m23, m33, dr, dx, dy, dz, c0, c1, c2, c3);
+#pragma unroll
+      for (int k = 0; k < kQ27; ++k) {
+        const R cx = R(q27_cx(k)), cy = R(q27_cy(k)), cz = R(q27_cz(k)), w = R(q27_w(k));
+        const R delta = ok ? w * (c0 + c1 * cx + c2 * cy + c3 * cz) : w * (dr + inv_cs2 * (cx * dx + cy * dy + cz * dz));
+        fp[k] = fmax(fp[k] + delta, R(1e-10));
+      }
+    }
+  }
+  R rs = R(0), sx = R(0), sy = R(0), sz = R(0);
+#pragma unroll
+  for (int k = 0; k < kQ27; ++k) {
+    rs += fp[k]; sx += fp[k] * R(q27_cx(k)); sy += fp[k] * R(q27_cy(k)); sz += fp[k] * R(q27_cz(k));
+    pf[pbase + k * kCells] = Codec<S>::enc(fp[k], R(q27_w(k)), R(1.0 / q27_w(k)));
+  }
+  const R rho_s = fmax(rs, R(0.01));
+  const R inv_s = R(1) / rho_s;
+  R* prho = static_cast<R*>(r.prho);
+  R* pvel = static_cast<R*>(r.pvel);
+  const int64_t pc = (int64_t)pb * kCells + cell, pn = (int64_t)r.pnb * kCells;
+  prho[pc] = rho_s;
+  pvel[pc] = sx * inv_s;
+  pvel[pc + pn] = sy * inv_s;
+  pvel[pc + 2 * pn] = sz * inv_s;
+}
+
+template <class S, class R>
+cudaError_t launch_restrict(const RestrictArgs& r, cudaStream_t st) {
+  if (r.n_covered <= 0) return cudaSuccess;
+  k_restrict<S, R><<<(unsigned)r.n_covered * 4, 128, 0, st>>>(r);
+  return cudaGetLastError();
+}
+
 template <class S, class R>
 cudaError_t launch_fill_ghosts(const StepArgs& a, const uint2* entries, int64_t n, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
@@ -581,6 +960,7 @@ cudaError_t launch_general(const StepArgs& a, const int32_t* work, int n_work, c
 
 #define OAL_INST(S, R)                                                                               \
   template cudaError_t launch_fill_ghosts<S, R>(const StepArgs&, const uint2*, int64_t, cudaStream_t); \
+  template cudaError_t launch_restrict<S, R>(const RestrictArgs&, cudaStream_t);                       \
   template cudaError_t launch_fast<S, R>(const StepArgs&, const int32_t*, int, cudaStream_t);         \
   template cudaError_t launch_general<S, R>(const StepArgs&, const int32_t*, int, cudaStream_t);
 OAL_INST(float, float)

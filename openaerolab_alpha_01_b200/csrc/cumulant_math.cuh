@@ -34,6 +34,20 @@ __device__ __forceinline__ V feq_k(int k, V rho, V ux, V uy, V uz, bool comp) {
   return rho * splat<V>(T(q27_w(k))) * val;
 }
 
+// f_eq with a run-time velocity c and weight w (physics_utils.jl:30-35, 65-95), the reference's
+// operation order; the block-AMR transfers evaluate it at interpolated macros
+template <class R>
+__device__ __forceinline__ R feq_c(R rho, R ux, R uy, R uz, R w, R cx, R cy, R cz, bool comp) {
+  const R cu = cx * ux + cy * uy + cz * uz;
+  const R usq = ux * ux + uy * uy + uz * uz;
+  if (!comp) return rho * w * (R(1) + R(3) * cu + R(4.5) * cu * cu - R(1.5) * usq);
+  const R cu2 = cu * cu, cu3 = cu2 * cu, cu4 = cu2 * cu2, usq2 = usq * usq;
+  R val = R(1) + R(3) * cu + R(4.5) * cu2 - R(1.5) * usq;
+  const R ho = (R(4.5) * cu3 - R(4.5) * cu * usq) + (R(3.375) * cu4 - R(6.75) * cu2 * usq + R(1.125) * usq2);
+  val += ho;
+  return rho * w * val;
+}
+
 // WALE eddy viscosity from the velocity gradient g_ij = d u_i / d x_j (kernel_cumulant.jl:505-549)
 template <class V>
 __device__ __forceinline__ V wale_nu(V g11, V g12, V g13, V g21, V g22, V g23, V g31, V g32, V g33, float c_wale) {

@@ -25,6 +25,8 @@ template <class S>
 cudaError_t launch_dense_fast(const StepArgs& a, const int32_t* work, int n_work, int grid, cudaStream_t st);
 template <class S>
 int dense_ctas_per_sm();
+template <class S, class R>
+cudaError_t launch_restrict(const RestrictArgs& r, cudaStream_t st);
 }
 using namespace oal;
 
@@ -300,6 +302,7 @@ struct oal_level {
   GraphCache gc;
   bool forces_valid = false;
   KbcLevel* kbc = nullptr;  // D3Q39 entropic levels: the whole state lives here
+  ParentView par{};         // refined level of a block-AMR hierarchy: its parent (set per step)
 };
 
 // ------------------------------------------------------------------------------------------------
@@ -1173,6 +1176,7 @@ static oal_status enqueue_step(oal_level* L, const CaseParams& cp, cudaStream_t 
   a.force_part = L->d_force_part;
   a.err = L->d_err;
   a.p0 = cp;
+  a.par = L->par;
   if (L->dense) {
     a.dense = 1;
     a.PX = L->PX; a.PY = L->PY; a.PZ = L->PZ;
@@ -1308,6 +1312,301 @@ oal_status oal_level_layout(const oal_level* L, int64_t out[6]) {
   int64_t bst, kst;
   level_layout(L, &bst, &kst);
   out[0] = L->dense ? 1 : 0; out[1] = L->PX; out[2] = L->PY; out[3] = L->PZ; out[4] = bst; out[5] = kst;
+  return OAL_OK;
+}
+
+}  // extern "C"
+
+// ================================================================================================
+// Block AMR: a hierarchy of D3Q27 levels with 2:1 refinement in space and time
+// (recursive_step! / recursive_step_temporal!, src/solver/solver_control.jl:55-560, default flags)
+// ================================================================================================
+struct AmrLevel {
+  oal_level* L = nullptr;
+  const oal_geometry* g = nullptr;
+  int32_t dim[3] = {0, 0, 0};
+  int32_t* d_ptr = nullptr;       // block pointer [dim_x*dim_y*dim_z], x fastest, 1-based
+  int32_t* d_covered = nullptr;   // this level's blocks that have children
+  int32_t n_covered = 0;
+  void* d_f_old = nullptr;        // snapshot before the level's step (levels with children)
+  void* d_rho_old = nullptr;
+  void* d_vel_old = nullptr;
+};
+
+struct oal_amr {
+  int device = 0;
+  int32_t storage = 0;
+  std::vector<AmrLevel> lv;
+  cudaStream_t cap = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  int32_t g_n = 0;
+  int g_parity = -1;
+  std::vector<oal_step_params> g_p;
+};
+
+static void amr_release_graph(oal_amr* A) {
+  if (A->exec) cudaGraphExecDestroy(A->exec);
+  if (A->graph) cudaGraphDestroy(A->graph);
+  A->exec = nullptr; A->graph = nullptr; A->g_n = 0; A->g_parity = -1; A->g_p.clear();
+}
+
+template <class R>
+static double restrict_ratio(R tau_p, R tau_c, int physical) {
+  const R tpc = std::max(tau_p - R(0.5), R(1e-6)), tcc = std::max(tau_c - R(0.5), R(1e-6));
+  R r = std::min(std::max(tpc / tcc, R(0.01)), R(100));
+  if (physical == 1) r = std::min(std::max(R(2) * tau_p / std::max(tau_c, R(0.500001)), R(0.01)), R(100));
+  const R omega_p = R(1) / std::max(tau_p, R(0.500001)), omega_c = R(1) / std::max(tau_c, R(0.500001));
+  const R one_m_wp = R(1) - omega_p, one_m_wc = R(1) - omega_c;
+  if (std::fabs(one_m_wc) > R(1e-6)) r = std::min(std::max(r * (one_m_wp / one_m_wc), R(0.01)), R(100));
+  return (double)r;
+}
+
+// One step of level l (0-based) and, recursively, two substeps of each finer level, then the
+// restriction onto l. t_sub: the level's step index (noise seed); tw: temporal weight of l's parent.
+static oal_status amr_step(oal_amr* A, int l, const std::vector<CaseParams>& cps, const oal_step_params* P,
+                           int64_t t_sub, double tw, cudaStream_t st) {
+  AmrLevel& me = A->lv[(size_t)l];
+  oal_level* L = me.L;
+  const oal_geometry* g = me.g;
+  const bool has_children = l + 1 < (int)A->lv.size();
+  const size_t sb = storage_bytes(A->storage), mb = macro_bytes(A->storage);
+  const size_t ncell = (size_t)g->nb * 512;
+  if (has_children) {  // copy_to_old! (src/geometry/blocks.jl:604-640)
+    const int p = L->parity;
+    OAL_CUDA_TRY(cudaMemcpyAsync(me.d_f_old, L->f[p], ncell * 27 * sb, cudaMemcpyDeviceToDevice, st));
+    OAL_CUDA_TRY(cudaMemcpyAsync(me.d_rho_old, L->rho, ncell * mb, cudaMemcpyDeviceToDevice, st));
+    OAL_CUDA_TRY(cudaMemcpyAsync(me.d_vel_old, L->vel[p], ncell * 3 * mb, cudaMemcpyDeviceToDevice, st));
+  }
+  if (l > 0) {
+    const AmrLevel& pa = A->lv[(size_t)l - 1];
+    ParentView v{};
+    v.f_new = pa.L->f[pa.L->parity];
+    v.f_old = pa.d_f_old;
+    v.rho_new = pa.L->rho;
+    v.rho_old = pa.d_rho_old;
+    v.vel_new = pa.L->vel[pa.L->parity];
+    v.vel_old = pa.d_vel_old;
+    v.ptr = pa.d_ptr;
+    v.dim_x = pa.dim[0]; v.dim_y = pa.dim[1]; v.dim_z = pa.dim[2];
+    v.nb = pa.g->nb;
+    v.tau_parent = P[l - 1].tau;
+    v.tau_fine = P[l].tau;
+    v.tw = tw;
+    v.use_temporal = 1;  // TEMPORAL_INTERPOLATION (config_loader.jl:90)
+    v.level_visc_physical = P[l].level_visc_physical;
+    L->par = v;
+  }
+  CaseParams cp = cps[(size_t)l];
+  cp.time_step_seed = (int32_t)(P[l].time_step_seed + t_sub);
+  oal_status s = enqueue_step(L, cp, st);
+  if (s != OAL_OK) return s;
+  if (has_children) {
+    const double bias = 0.0;  // INTERFACE_TEMPORAL_WEIGHT_BIAS (config_loader.jl:146)
+    s = amr_step(A, l + 1, cps, P, 2 * t_sub, std::min(std::max(0.0 + bias, 0.0), 1.0), st);
+    if (s != OAL_OK) return s;
+    s = amr_step(A, l + 1, cps, P, 2 * t_sub + 1, std::min(std::max(0.5 + bias, 0.0), 1.0), st);
+    if (s != OAL_OK) return s;
+    // restrict_fine_to_parent! (amr_coupling.jl:7562-7640)
+    const AmrLevel& ch = A->lv[(size_t)l + 1];
+    RestrictArgs r{};
+    r.pf = L->f[L->parity];
+    r.prho = L->rho;
+    r.pvel = L->vel[L->parity];
+    r.pbinfo = g->d_binfo;
+    r.covered = me.d_covered;
+    r.n_covered = me.n_covered;
+    r.pnb = g->nb;
+    r.cf = ch.L->f[ch.L->parity];
+    r.cptr = ch.d_ptr;
+    r.cdx = ch.dim[0]; r.cdy = ch.dim[1]; r.cdz = ch.dim[2];
+    r.cbflags = ch.g->d_bflags;
+    r.cmslot = ch.g->d_mslot;
+    r.ccmask = ch.g->d_cmask;
+    r.comp = P[l].compressible_corr;
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (A->storage) {
+      case OAL_STORE_F32:
+        r.ratio = restrict_ratio<float>(P[l].tau, P[l + 1].tau, P[l].level_visc_physical);
+        e = launch_restrict<float, float>(r, st); break;
+      case OAL_STORE_F16_DEV:
+        r.ratio = restrict_ratio<float>(P[l].tau, P[l + 1].tau, P[l].level_visc_physical);
+        e = launch_restrict<__half, float>(r, st); break;
+      case OAL_STORE_BF16_DEV:
+        r.ratio = restrict_ratio<float>(P[l].tau, P[l + 1].tau, P[l].level_visc_physical);
+        e = launch_restrict<__nv_bfloat16, float>(r, st); break;
+      case OAL_STORE_F64:
+        r.ratio = restrict_ratio<double>((double)P[l].tau, (double)P[l + 1].tau, P[l].level_visc_physical);
+        e = launch_restrict<double, double>(r, st); break;
+    }
+    OAL_CUDA_TRY(e);
+  }
+  return OAL_OK;
+}
+
+extern "C" {
+
+void oal_amr_destroy(oal_amr* A) {
+  if (!A) return;
+  cudaSetDevice(A->device);
+  amr_release_graph(A);
+  for (AmrLevel& l : A->lv) {
+    if (l.L) oal_level_destroy(l.L);
+    cudaFree(l.d_ptr); cudaFree(l.d_covered); cudaFree(l.d_f_old); cudaFree(l.d_rho_old); cudaFree(l.d_vel_old);
+  }
+  if (A->cap) cudaStreamDestroy(A->cap);
+  cudaGetLastError();
+  delete A;
+}
+
+oal_status oal_amr_create(int32_t nlevels, const oal_amr_level_desc* levels, int32_t storage, oal_amr** out) {
+  if (!out || !levels || nlevels < 1) return set_error(OAL_E_INVALID_ARG, "oal_amr_create: bad arguments");
+  *out = nullptr;
+  if (storage < OAL_STORE_F32 || storage > OAL_STORE_F64) return set_error(OAL_E_INVALID_ARG, "storage %d", storage);
+  const int device = levels[0].geometry ? levels[0].geometry->device : 0;
+  for (int l = 0; l < nlevels; ++l) {
+    const oal_geometry* g = levels[l].geometry;
+    const int32_t* d = levels[l].dim;
+    if (!g) return set_error(OAL_E_INVALID_ARG, "level %d has no geometry", l);
+    if (g->device != device) return set_error(OAL_E_INVALID_ARG, "levels on different devices");
+    if (d[0] < 1 || d[1] < 1 || d[2] < 1) return set_error(OAL_E_INVALID_ARG, "level %d: block grid extent", l);
+    if (g->nx != 8 * d[0] || g->ny != 8 * d[1] || g->nz != 8 * d[2])
+      return set_error(OAL_E_INVALID_ARG, "level %d: geometry extent %dx%dx%d is not 8 x the block grid %dx%dx%d", l,
+                       g->nx, g->ny, g->nz, d[0], d[1], d[2]);
+    for (int32_t b = 0; b < g->nb; ++b) {
+      const int4 c = g->h_binfo[(size_t)b];
+      if (c.x < 1 || c.y < 1 || c.z < 1 || c.x > d[0] || c.y > d[1] || c.z > d[2])
+        return set_error(OAL_E_INVALID_ARG, "level %d: block %d at (%d,%d,%d) outside the block grid", l, b, c.x, c.y, c.z);
+    }
+    if (l > 0) {
+      const int32_t* pd = levels[l - 1].dim;
+      if (d[0] != 2 * pd[0] || d[1] != 2 * pd[1] || d[2] != 2 * pd[2])
+        return set_error(OAL_E_INVALID_ARG, "level %d: block grid must be twice its parent's", l);
+    }
+  }
+  OAL_CUDA_TRY(cudaSetDevice(device));
+  auto* A = new oal_amr();
+  A->device = device;
+  A->storage = storage;
+  A->lv.resize((size_t)nlevels);
+  auto fail = [&](oal_status s) { oal_amr_destroy(A); return s; };
+  // host block pointers (x fastest) and the nesting check
+  std::vector<std::vector<int32_t>> ptrs((size_t)nlevels);
+  for (int l = 0; l < nlevels; ++l) {
+    const oal_geometry* g = levels[l].geometry;
+    const int32_t* d = levels[l].dim;
+    std::vector<int32_t>& ptr = ptrs[(size_t)l];
+    ptr.assign((size_t)d[0] * d[1] * d[2], 0);
+    for (int32_t b = 0; b < g->nb; ++b) {
+      const int4 c = g->h_binfo[(size_t)b];
+      int32_t& slot = ptr[(size_t)(c.x - 1) + (size_t)d[0] * ((c.y - 1) + (size_t)d[1] * (c.z - 1))];
+      if (slot != 0) { set_error(OAL_E_INVALID_ARG, "level %d: two blocks at (%d,%d,%d)", l, c.x, c.y, c.z); return fail(OAL_E_INVALID_ARG); }
+      slot = b + 1;
+    }
+    if (l > 0) {
+      const int32_t* pd = levels[l - 1].dim;
+      const std::vector<int32_t>& pp = ptrs[(size_t)l - 1];
+      for (int32_t b = 0; b < g->nb; ++b) {
+        const int4 c = g->h_binfo[(size_t)b];
+        const int px = (c.x + 1) / 2, py = (c.y + 1) / 2, pz = (c.z + 1) / 2;
+        if (pp[(size_t)(px - 1) + (size_t)pd[0] * ((py - 1) + (size_t)pd[1] * (pz - 1))] == 0) {
+          set_error(OAL_E_INVALID_ARG, "level %d: block (%d,%d,%d) lies outside its parent level", l, c.x, c.y, c.z);
+          return fail(OAL_E_INVALID_ARG);
+        }
+      }
+    }
+  }
+  for (int l = 0; l < nlevels; ++l) {
+    AmrLevel& me = A->lv[(size_t)l];
+    me.g = levels[l].geometry;
+    std::memcpy(me.dim, levels[l].dim, sizeof me.dim);
+    oal_status s = oal_level_create_ex(me.g, OAL_OP_CUMULANT_D3Q27, storage, 0u, &me.L);
+    if (s != OAL_OK) return fail(s);
+    const std::vector<int32_t>& ptr = ptrs[(size_t)l];
+    cudaError_t e = cudaMalloc(&me.d_ptr, ptr.size() * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMemcpy(me.d_ptr, ptr.data(), ptr.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && l + 1 < nlevels) {
+      // blocks with children: the covered band of the restriction (_restrict_covered_block_list)
+      const oal_geometry* cg = levels[l + 1].geometry;
+      std::vector<uint8_t> has((size_t)me.g->nb, 0);
+      for (int32_t b = 0; b < cg->nb; ++b) {
+        const int4 c = cg->h_binfo[(size_t)b];
+        const int px = (c.x + 1) / 2, py = (c.y + 1) / 2, pz = (c.z + 1) / 2;
+        has[(size_t)ptr[(size_t)(px - 1) + (size_t)me.dim[0] * ((py - 1) + (size_t)me.dim[1] * (pz - 1))] - 1] = 1;
+      }
+      std::vector<int32_t> cov;
+      for (int32_t b = 0; b < me.g->nb; ++b)
+        if (has[(size_t)b]) cov.push_back(b);
+      me.n_covered = (int32_t)cov.size();
+      e = cudaMalloc(&me.d_covered, std::max<size_t>(cov.size(), 1) * sizeof(int32_t));
+      if (e == cudaSuccess && !cov.empty())
+        e = cudaMemcpy(me.d_covered, cov.data(), cov.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+      const size_t ncell = (size_t)me.g->nb * 512;
+      if (e == cudaSuccess) e = cudaMalloc(&me.d_f_old, ncell * 27 * storage_bytes(storage));
+      if (e == cudaSuccess) e = cudaMalloc(&me.d_rho_old, ncell * macro_bytes(storage));
+      if (e == cudaSuccess) e = cudaMalloc(&me.d_vel_old, ncell * 3 * macro_bytes(storage));
+    }
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      set_error(e == cudaErrorMemoryAllocation ? OAL_E_OUT_OF_MEMORY : OAL_E_CUDA, "amr allocation: %s", cudaGetErrorString(e));
+      return fail(e == cudaErrorMemoryAllocation ? OAL_E_OUT_OF_MEMORY : OAL_E_CUDA);
+    }
+  }
+  if (cudaStreamCreateWithFlags(&A->cap, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    set_error(OAL_E_CUDA, "amr stream");
+    return fail(OAL_E_CUDA);
+  }
+  *out = A;
+  return OAL_OK;
+}
+
+oal_status oal_amr_level(oal_amr* A, int32_t level, oal_level** out) {
+  if (!A || !out || level < 0 || level >= (int32_t)A->lv.size()) return set_error(OAL_E_INVALID_ARG, "bad level");
+  *out = A->lv[(size_t)level].L;
+  return OAL_OK;
+}
+
+oal_status oal_amr_advance(oal_amr* A, const oal_step_params* params, int32_t n, void* stream) {
+  if (!A || !params) return set_error(OAL_E_INVALID_ARG, "null argument");
+  if (n <= 0) return set_error(OAL_E_INVALID_ARG, "n_coarse_steps must be positive");
+  const int nl = (int)A->lv.size();
+  std::vector<CaseParams> cps((size_t)nl);
+  for (int l = 0; l < nl; ++l) {
+    oal_status s = resolve_params(&params[l], A->lv[(size_t)l].g, &cps[(size_t)l]);
+    if (s != OAL_OK) return s;
+    if (cps[(size_t)l].flags & CF_STORE_POST) return set_error(OAL_E_UNSUPPORTED, "store_post_collision needs caller-owned arrays");
+  }
+  OAL_CUDA_TRY(cudaSetDevice(A->device));
+  const int start = A->lv[0].L->parity;
+  bool hit = A->exec && A->g_n == n && A->g_parity == start && (int)A->g_p.size() == nl;
+  for (int l = 0; hit && l < nl; ++l) {
+    oal_step_params a = params[l], b = A->g_p[(size_t)l];
+    a.time_step_seed = b.time_step_seed = 0;
+    hit = std::memcmp(&a, &b, sizeof a) == 0 && !(cps[(size_t)l].flags & CF_INLET_NOISE);
+  }
+  std::vector<int> parities((size_t)nl);
+  for (int l = 0; l < nl; ++l) parities[(size_t)l] = A->lv[(size_t)l].L->parity;
+  if (!hit) {
+    amr_release_graph(A);
+    OAL_CUDA_TRY(cudaStreamBeginCapture(A->cap, cudaStreamCaptureModeThreadLocal));
+    oal_status es = OAL_OK;
+    for (int i = 0; i < n && es == OAL_OK; ++i) es = amr_step(A, 0, cps, params, i, 0.0, A->cap);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(A->cap, &graph);
+    for (int l = 0; l < nl; ++l) A->lv[(size_t)l].L->parity = parities[(size_t)l];
+    if (es != OAL_OK) { if (graph) cudaGraphDestroy(graph); return es; }
+    if (e != cudaSuccess) { cudaGetLastError(); return set_error(OAL_E_CUDA, "graph capture: %s", cudaGetErrorString(e)); }
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) { cudaGraphDestroy(graph); cudaGetLastError(); return set_error(OAL_E_CUDA, "graph instantiate: %s", cudaGetErrorString(e)); }
+    A->exec = exec; A->graph = graph; A->g_n = n; A->g_parity = start;
+    A->g_p.assign(params, params + nl);
+  }
+  OAL_CUDA_TRY(cudaGraphLaunch(A->exec, static_cast<cudaStream_t>(stream)));
+  // level l takes n * 2^l steps: only the coarsest level can end on the other buffer
+  if (n & 1) A->lv[0].L->parity ^= 1;
+  for (int l = 0; l < nl; ++l) A->lv[(size_t)l].L->forces_valid = true;
   return OAL_OK;
 }
 

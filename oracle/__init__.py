@@ -62,6 +62,13 @@ def lib() -> C.CDLL:
         for suf in ("f32", "f64"):
             getattr(L, f"ora_q19_fill_{suf}").argtypes = [vp, vp, vp, vp, C.c_double, C.c_double, C.c_double, vp, vp, vp]
             getattr(L, f"ora_q19_restrict_{suf}").argtypes = [vp, vp, C.c_double, C.c_double, vp, vp, vp]
+        for suf in ("f64", "f32"):
+            getattr(L, f"ora_step_d3q27_refined_{suf}").argtypes = (
+                [i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, i32, vp, i32, i32, i32, vp, vp, vp, vp, vp,
+                 vp, C.c_double, C.c_double, i32])
+            getattr(L, f"ora_step_d3q27_refined_{suf}").restype = C.c_int
+            getattr(L, f"ora_restrict_d3q27_{suf}").argtypes = (
+                [i32, vp, vp, vp, vp, i32, vp, i32, i32, i32, vp, vp, C.c_double, C.c_double, i32, i32])
         L.ora_q39_tables.argtypes = [vp] * 5
         L.ora_q39_exp.argtypes = [i64, vp, vp]
         L.ora_q39_log.argtypes = [i64, vp, vp]
@@ -150,6 +157,88 @@ class OracleLevel:
         f = np.ascontiguousarray(self.f, np.float64)
         lib().ora_mass_momentum_f64(self.nb, _p(self.obstacle), _p(f), _p(out))
         return out
+
+
+class OracleAMR:
+    """recursive_step! (src/solver/solver_control.jl:55-560, default flags) over D3Q27 levels held
+    in the reference layout: level 0 steps once per coarse step; every finer level steps twice per
+    step of its parent (temporal weights 0 and 1/2 against the parent's state before and after its
+    step), then is restricted onto the parent. `domains`: objects with coords (n,3), neighbor_table
+    (27,n), obstacle (n,512) or None, bx_max/by_max/bz_max and shape (the level's cell extent)."""
+
+    def __init__(self, domains, dtype=np.float64):
+        self.dtype = np.dtype(dtype)
+        self.levels = []
+        for d in domains:
+            nb = d.coords.shape[0]
+            dims = (int(d.bx_max), int(d.by_max), int(d.bz_max))
+            ptr = np.zeros(dims[0] * dims[1] * dims[2], np.int32)
+            for i, (bx, by, bz) in enumerate(np.asarray(d.coords).tolist()):
+                ptr[(bx - 1) + dims[0] * ((by - 1) + dims[1] * (bz - 1))] = i + 1
+            self.levels.append(dict(
+                nb=nb, dims=dims, shape=tuple(int(v) for v in d.shape), ptr=ptr,
+                coords=np.ascontiguousarray(d.coords, np.int32), nbr=np.ascontiguousarray(d.neighbor_table, np.int32),
+                obstacle=None if d.obstacle is None else np.ascontiguousarray(d.obstacle, np.uint8),
+                f=[np.zeros((27, nb, 512), self.dtype), np.zeros((27, nb, 512), self.dtype)],
+                vel=[np.zeros((3, nb, 512), self.dtype), np.zeros((3, nb, 512), self.dtype)],
+                rho=np.ones((nb, 512), self.dtype), parity=0, f_old=None, rho_old=None, vel_old=None))
+
+    def init_equilibrium(self, l, rho, vel, compressible=0):
+        L = self.levels[l]
+        L["f"][0][...] = init_feq(rho, vel, compressible).astype(self.dtype)
+        L["rho"][...] = rho
+        L["vel"][0][...] = vel
+        L["parity"] = 0
+
+    def state(self, l):
+        L = self.levels[l]
+        return L["f"][L["parity"]], L["rho"], L["vel"][L["parity"]]
+
+    def _suf(self):
+        return "f64" if self.dtype == np.float64 else "f32"
+
+    def _step(self, l, params, t_sub, tw):
+        L = self.levels[l]
+        p = L["parity"]
+        f_in, f_out = L["f"][p], L["f"][p ^ 1]
+        v_in, v_out = L["vel"][p], L["vel"][p ^ 1]
+        has_children = l + 1 < len(self.levels)
+        if has_children:
+            L["f_old"], L["rho_old"], L["vel_old"] = f_in.copy(), L["rho"].copy(), v_in.copy()
+        P = params[l]
+        seed = P.time_step_seed
+        P.time_step_seed = seed + t_sub
+        force = np.zeros(3)
+        nx, ny, nz = L["shape"]
+        if l == 0:
+            fn = getattr(lib(), f"ora_step_d3q27_{self._suf()}")
+            rc = fn(L["nb"], nx, ny, nz, _p(L["coords"]), _p(L["nbr"]), _p(L["obstacle"]), None, None,
+                    C.addressof(P), _p(f_in), _p(f_out), None, _p(L["rho"]), _p(v_out), _p(v_in), _p(force))
+        else:
+            Pa = self.levels[l - 1]
+            pp = Pa["parity"]
+            fn = getattr(lib(), f"ora_step_d3q27_refined_{self._suf()}")
+            rc = fn(L["nb"], nx, ny, nz, _p(L["coords"]), _p(L["nbr"]), _p(L["obstacle"]), C.addressof(P),
+                    _p(f_in), _p(f_out), _p(L["rho"]), _p(v_out), _p(v_in), _p(force), Pa["nb"], _p(Pa["ptr"]),
+                    *Pa["dims"], _p(Pa["f"][pp]), _p(Pa["rho"]), _p(Pa["vel"][pp]), _p(Pa["f_old"]),
+                    _p(Pa["rho_old"]), _p(Pa["vel_old"]), float(params[l - 1].tau), float(tw), 1)
+        P.time_step_seed = seed
+        assert rc == 0
+        L["parity"] ^= 1
+        if has_children:
+            self._step(l + 1, params, 2 * t_sub, 0.0)
+            self._step(l + 1, params, 2 * t_sub + 1, 0.5)
+            Ch = self.levels[l + 1]
+            q = L["parity"]
+            fn = getattr(lib(), f"ora_restrict_d3q27_{self._suf()}")
+            fn(L["nb"], _p(L["coords"]), _p(L["f"][q]), _p(L["rho"]), _p(L["vel"][q]), Ch["nb"], _p(Ch["ptr"]),
+               *Ch["dims"], _p(Ch["obstacle"]), _p(Ch["f"][Ch["parity"]]), float(params[l].tau),
+               float(params[l + 1].tau), int(params[l].compressible_corr), int(params[l].level_visc_physical))
+
+    def advance(self, params, n):
+        for i in range(n):
+            self._step(0, params, i, 0.0)
+        return self
 
 
 # ---- D3Q19 octree (oal_oracle_q19.cpp) ---------------------------------------------------------

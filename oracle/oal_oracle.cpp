@@ -24,6 +24,13 @@
 //   half-way BB + MEM ....... src/octree_q19/src/stream.jl:229-256 (link rule, generalised to the
 //                             27 D3Q27 links; the reference's GPU path has no D3Q27 analogue)
 //   mass / momentum ......... src/octree_q19/src/state.jl:614-637 (Float64 sums)
+//   block AMR (default flags): parent interpolation of a refined level's pulls
+//                             src/collision/physics_interpolation.jl:10-51,128-137,188-346,705-1198
+//                             and kernel_cumulant.jl:286-316,346-388; restriction
+//                             src/collision/amr_coupling.jl:130-190,7562-7640 + kernel :1900-3242
+//                             (children average, f_neq rescale, two moment-correction passes,
+//                             shell macros); the recursion src/solver/solver_control.jl:55-560 is
+//                             driven by oracle/__init__.py (OracleAMR)
 //
 // Parity status: the reference is Julia and cannot run in this environment, so this restatement
 // is pinned by the reference's analytic gates (Taylor-Green decay, conservation, rest state) and
@@ -135,6 +142,20 @@ struct Level {
   const uint8_t* obstacle; // 512*n or null
   const float* sponge;
   const float* wall_dist;
+  const void* parent = nullptr;  // Parent<T> of a refined level (null on level 1)
+};
+
+// The parent level seen from a refined level's kernel (perform_timestep_v2! arguments
+// parent_f, parent_rho, parent_vel, parent_ptr, *_old, parent_dim_*, tau_parent, temporal_weight,
+// use_temporal_interp). Arrays in the reference layout of the parent level.
+template <class T>
+struct Parent {
+  const T* f_new; const T* rho_new; const T* vel_new;
+  const T* f_old; const T* rho_old; const T* vel_old;
+  const int32_t* ptr;  // parent_ptr (dim_x, dim_y, dim_z), Julia column-major, 1-based block, 0 = none
+  int32_t dim_x, dim_y, dim_z, nb;
+  T tau_parent, tau_fine, tw;
+  int use_temporal, comp, level_visc_physical;
 };
 
 inline int64_t cidx(int x, int y, int z) { return (int64_t)x + 8 * y + 64 * z; }  // 0-based
@@ -146,6 +167,222 @@ struct Arr {
   int64_t f(int x, int y, int z, int b, int k) const { return cidx(x, y, z) + 512 * (int64_t)b + 512 * nb * k; }
   int64_t s(int x, int y, int z, int b) const { return cidx(x, y, z) + 512 * (int64_t)b; }
 };
+
+// ---- parent interpolation (physics_interpolation.jl, default flags: no mirror ghost, no periodic-y
+// AMR, no B-spline or quintic macros, extrapolation fallback on) --------------------------------
+struct Bracket { int i0, i1; };
+template <class T>
+void parent_bracket(T p_cont, int n, int& i0, int& i1, T& w) {  // :128-137
+  if (n <= 1) { i0 = 1; i1 = 1; w = T(0); return; }
+  const T pc = std::min(std::max(p_cont, T(1)), T(n));
+  i0 = std::min(std::max((int)std::floor(pc), 1), n - 1);
+  i1 = i0 + 1;
+  w = std::min(std::max(pc - T(i0), T(0)), T(1));
+}
+
+template <class T>
+struct Node { T f, rho, ux, uy, uz, fneq; bool ok; };
+
+// parent cell (1-based global index) -> block (0-based) and cell offset, or -1 outside / absent.
+// Julia's (g - 1) ÷ 8 truncates toward zero, so g < 1 would alias block 1 with an out-of-block
+// local index; such nodes count as absent here.
+template <class T>
+int64_t parent_cell(const Parent<T>& P, int pgx, int pgy, int pgz) {
+  if (pgx < 1 || pgy < 1 || pgz < 1) return -1;
+  const int pbx = (pgx - 1) / BS + 1, pby = (pgy - 1) / BS + 1, pbz = (pgz - 1) / BS + 1;
+  if (pbx > P.dim_x || pby > P.dim_y || pbz > P.dim_z) return -1;
+  const int32_t pb = P.ptr[(pbx - 1) + (int64_t)P.dim_x * ((pby - 1) + (int64_t)P.dim_y * (pbz - 1))];
+  if (pb <= 0) return -1;
+  return cidx((pgx - 1) % BS, (pgy - 1) % BS, (pgz - 1) % BS) + 512 * (int64_t)(pb - 1);
+}
+
+// get_blended (:776-859), time-blended when use_temporal and tw < 0.99
+template <class T>
+Node<T> get_blended(const Parent<T>& P, int pgx, int pgy, int pgz, int k, T wk, T cx, T cy, T cz) {
+  const int64_t c = parent_cell(P, pgx, pgy, pgz);
+  if (c < 0) return Node<T>{wk, T(1), T(0), T(0), T(0), T(0), false};
+  const int64_t n = 512 * (int64_t)P.nb;
+  T f = P.f_new[c + n * k], rho = P.rho_new[c], ux = P.vel_new[c], uy = P.vel_new[c + n], uz = P.vel_new[c + 2 * n];
+  if (P.use_temporal == 1 && P.tw < T(0.99) && P.f_old) {
+    const T tw = P.tw;
+    f = P.f_old[c + n * k] * (T(1) - tw) + f * tw;
+    rho = P.rho_old[c] * (T(1) - tw) + rho * tw;
+    ux = P.vel_old[c] * (T(1) - tw) + ux * tw;
+    uy = P.vel_old[c + n] * (T(1) - tw) + uy * tw;
+    uz = P.vel_old[c + 2 * n] * (T(1) - tw) + uz * tw;
+  }
+  const T feqc = feq_auto<T>(rho, ux, uy, uz, wk, cx, cy, cz, P.comp);
+  return Node<T>{f, rho, ux, uy, uz, f - feqc, true};
+}
+
+// get_macro (:860-923)
+template <class T>
+Node<T> get_macro(const Parent<T>& P, int pgx, int pgy, int pgz) {
+  const int64_t c = parent_cell(P, pgx, pgy, pgz);
+  if (c < 0) return Node<T>{T(0), T(1), T(0), T(0), T(0), T(0), false};
+  const int64_t n = 512 * (int64_t)P.nb;
+  T rho = P.rho_new[c], ux = P.vel_new[c], uy = P.vel_new[c + n], uz = P.vel_new[c + 2 * n];
+  if (P.use_temporal == 1 && P.tw < T(0.99) && P.rho_old) {
+    const T tw = P.tw;
+    rho = P.rho_old[c] * (T(1) - tw) + rho * tw;
+    ux = P.vel_old[c] * (T(1) - tw) + ux * tw;
+    uy = P.vel_old[c + n] * (T(1) - tw) + uy * tw;
+    uz = P.vel_old[c + 2 * n] * (T(1) - tw) + uz * tw;
+  }
+  return Node<T>{T(0), rho, ux, uy, uz, T(0), true};
+}
+
+// cubic Lagrange weights of the stencil node i in -1..2 (:953-960)
+template <class T>
+T lagrange3(int i, T w) {
+  return i == -1 ? (-w * (w - T(1)) * (w - T(2)) / T(6))
+       : i == 0  ? ((w + T(1)) * (w - T(1)) * (w - T(2)) / T(2))
+       : i == 1  ? (-w * (w + T(1)) * (w - T(2)) / T(2))
+                 : (w * (w + T(1)) * (w - T(1)) / T(6));
+}
+
+// sample_parent_macro_for_fine_cell (:188-346): trilinear macros; a missing corner is
+// extrapolated linearly from its partner along x, then y, then z
+template <class T>
+bool sample_parent_macro(const Parent<T>& P, int fgx, int fgy, int fgz, T& r_out, T& x_out, T& y_out, T& z_out) {
+  const int pnx = P.dim_x * BS, pny = P.dim_y * BS, pnz = P.dim_z * BS;
+  int px0, px1, py0, py1, pz0, pz1;
+  T wx, wy, wz;
+  parent_bracket<T>(T(fgx) * T(0.5) + T(0.25), pnx, px0, px1, wx);
+  parent_bracket<T>(T(fgy) * T(0.5) + T(0.25), pny, py0, py1, wy);
+  parent_bracket<T>(T(fgz) * T(0.5) + T(0.25), pnz, pz0, pz1, wz);
+  Node<T> d[8];
+  const int ix[8] = {px0, px1, px0, px1, px0, px1, px0, px1};
+  const int iy[8] = {py0, py0, py1, py1, py0, py0, py1, py1};
+  const int iz[8] = {pz0, pz0, pz0, pz0, pz1, pz1, pz1, pz1};
+  for (int c = 0; c < 8; ++c) d[c] = get_macro<T>(P, ix[c], iy[c], iz[c]);
+  const T w[8] = {(T(1) - wx) * (T(1) - wy) * (T(1) - wz), wx * (T(1) - wy) * (T(1) - wz),
+                  (T(1) - wx) * wy * (T(1) - wz),         wx * wy * (T(1) - wz),
+                  (T(1) - wx) * (T(1) - wy) * wz,         wx * (T(1) - wy) * wz,
+                  (T(1) - wx) * wy * wz,                  wx * wy * wz};
+  bool all = true;
+  for (int c = 0; c < 8; ++c) all = all && d[c].ok;
+  auto acc = [&](T Node<T>::*m) {
+    T s = w[0] * (d[0].*m);
+    for (int c = 1; c < 8; ++c) s = s + w[c] * (d[c].*m);
+    return s;
+  };
+  if (!all) {
+    bool any = false;
+    for (int c = 0; c < 8; ++c) any = any || d[c].ok;
+    if (!any) { r_out = T(1); x_out = y_out = z_out = T(0); return false; }
+    const int pxm = px0 - 1, pxp = px1 + 1, pym = py0 - 1, pyp = py1 + 1, pzm = pz0 - 1, pzp = pz1 + 1;
+    // (a, b, far node of a when b is missing, far node of b when a is missing), reference order
+    struct Edge { int a, b, fa[3], fb[3]; };
+    const Edge edges[12] = {
+        {0, 1, {pxm, py0, pz0}, {pxp, py0, pz0}}, {2, 3, {pxm, py1, pz0}, {pxp, py1, pz0}},
+        {4, 5, {pxm, py0, pz1}, {pxp, py0, pz1}}, {6, 7, {pxm, py1, pz1}, {pxp, py1, pz1}},
+        {0, 2, {px0, pym, pz0}, {px0, pyp, pz0}}, {1, 3, {px1, pym, pz0}, {px1, pyp, pz0}},
+        {4, 6, {px0, pym, pz1}, {px0, pyp, pz1}}, {5, 7, {px1, pym, pz1}, {px1, pyp, pz1}},
+        {0, 4, {px0, py0, pzm}, {px0, py0, pzp}}, {1, 5, {px1, py0, pzm}, {px1, py0, pzp}},
+        {2, 6, {px0, py1, pzm}, {px0, py1, pzp}}, {3, 7, {px1, py1, pzm}, {px1, py1, pzp}}};
+    for (const Edge& e : edges) {
+      if (d[e.a].ok == d[e.b].ok) continue;
+      const int src = d[e.a].ok ? e.a : e.b, dst = d[e.a].ok ? e.b : e.a;
+      const int* far = d[e.a].ok ? e.fa : e.fb;
+      const Node<T> fd = get_macro<T>(P, far[0], far[1], far[2]);
+      Node<T>& o = d[dst];
+      const Node<T>& s0 = d[src];
+      o.rho = fd.ok ? T(2) * s0.rho - fd.rho : s0.rho;
+      o.ux = fd.ok ? T(2) * s0.ux - fd.ux : s0.ux;
+      o.uy = fd.ok ? T(2) * s0.uy - fd.uy : s0.uy;
+      o.uz = fd.ok ? T(2) * s0.uz - fd.uz : s0.uz;
+      o.ok = true;
+    }
+  }
+  r_out = acc(&Node<T>::rho); x_out = acc(&Node<T>::ux); y_out = acc(&Node<T>::uy); z_out = acc(&Node<T>::uz);
+  return true;
+}
+
+// interpolate_with_rescaling (:705-1198) at the fine cell (fgx, fgy, fgz), direction k
+template <class T>
+T interpolate_with_rescaling(const Parent<T>& P, int fgx, int fgy, int fgz, int k, T wk, T cx, T cy, T cz) {
+  const int pnx = P.dim_x * BS, pny = P.dim_y * BS, pnz = P.dim_z * BS;
+  int px0, px1, py0, py1, pz0, pz1;
+  T wx, wy, wz;
+  parent_bracket<T>(T(fgx) * T(0.5) + T(0.25), pnx, px0, px1, wx);
+  parent_bracket<T>(T(fgy) * T(0.5) + T(0.25), pny, py0, py1, wy);
+  parent_bracket<T>(T(fgz) * T(0.5) + T(0.25), pnz, pz0, pz1, wz);
+  const bool use_cubic = px0 - 2 >= 1 && px0 + 2 <= pnx && py0 - 2 >= 1 && py0 + 2 <= pny && pz0 - 2 >= 1 &&
+                         pz0 + 2 <= pnz;
+  Node<T> d[8];
+  const int ix[8] = {px0, px1, px0, px1, px0, px1, px0, px1};
+  const int iy[8] = {py0, py0, py1, py1, py0, py0, py1, py1};
+  const int iz[8] = {pz0, pz0, pz0, pz0, pz1, pz1, pz1, pz1};
+  for (int c = 0; c < 8; ++c) d[c] = get_blended<T>(P, ix[c], iy[c], iz[c], k, wk, cx, cy, cz);
+  int anchor = 7;
+  for (int c = 0; c < 7; ++c)
+    if (d[c].ok) { anchor = c; break; }
+  Node<T> v[8];
+  for (int c = 0; c < 8; ++c) v[c] = d[c].ok ? d[c] : d[anchor];
+  auto trilin = [&](T Node<T>::*m) {
+    const T c00 = (v[0].*m) * (T(1) - wx) + (v[1].*m) * wx;
+    const T c01 = (v[4].*m) * (T(1) - wx) + (v[5].*m) * wx;
+    const T c10 = (v[2].*m) * (T(1) - wx) + (v[3].*m) * wx;
+    const T c11 = (v[6].*m) * (T(1) - wx) + (v[7].*m) * wx;
+    const T c0 = c00 * (T(1) - wy) + c10 * wy;
+    const T c1 = c01 * (T(1) - wy) + c11 * wy;
+    return c0 * (T(1) - wz) + c1 * wz;
+  };
+  bool cubic_all_valid = use_cubic;
+  if (use_cubic) {
+    for (int a = -1; a <= 2 && cubic_all_valid; ++a)
+      for (int bb = -1; bb <= 2 && cubic_all_valid; ++bb)
+        for (int c = -1; c <= 2 && cubic_all_valid; ++c)
+          if (!get_macro<T>(P, px0 + a, py0 + bb, pz0 + c).ok) cubic_all_valid = false;
+  }
+  T rho_int, ux_int, uy_int, uz_int;
+  if (cubic_all_valid) {
+    rho_int = ux_int = uy_int = uz_int = T(0);
+    for (int a = -1; a <= 2; ++a)
+      for (int bb = -1; bb <= 2; ++bb)
+        for (int c = -1; c <= 2; ++c) {
+          const Node<T> m = get_macro<T>(P, px0 + a, py0 + bb, pz0 + c);
+          const T w3 = lagrange3<T>(a, wx) * lagrange3<T>(bb, wy) * lagrange3<T>(c, wz);
+          rho_int += w3 * m.rho;
+          ux_int += w3 * m.ux;
+          uy_int += w3 * m.uy;
+          uz_int += w3 * m.uz;
+        }
+  } else if (!sample_parent_macro<T>(P, fgx, fgy, fgz, rho_int, ux_int, uy_int, uz_int)) {
+    rho_int = trilin(&Node<T>::rho); ux_int = trilin(&Node<T>::ux);
+    uy_int = trilin(&Node<T>::uy); uz_int = trilin(&Node<T>::uz);
+  }
+  const T feq_int = feq_auto<T>(rho_int, ux_int, uy_int, uz_int, wk, cx, cy, cz, P.comp);
+  T f_neq = T(0);
+  if (use_cubic) {
+    const T anchor_neq = d[anchor].fneq;
+    for (int a = -1; a <= 2; ++a) {
+      const T wxv = lagrange3<T>(a, wx);
+      for (int bb = -1; bb <= 2; ++bb) {
+        const T wyv = lagrange3<T>(bb, wy);
+        for (int c = -1; c <= 2; ++c) {
+          const T wzv = lagrange3<T>(c, wz);
+          const Node<T> n = get_blended<T>(P, px0 + a, py0 + bb, pz0 + c, k, wk, cx, cy, cz);
+          f_neq += wxv * wyv * wzv * (n.ok ? n.fneq : anchor_neq);
+        }
+      }
+    }
+  } else {
+    f_neq = trilin(&Node<T>::fneq);
+  }
+  const T tau_c = P.tau_parent - T(0.5), tau_f = P.tau_fine - T(0.5);
+  T scale = tau_c > T(1e-6) ? std::min(std::max(tau_f / tau_c, T(0.01)), T(100)) : T(1);
+  if (P.level_visc_physical == 1)
+    scale = std::min(std::max(P.tau_fine / (T(2) * std::max(P.tau_parent, T(0.500001))), T(0.01)), T(100));
+  {  // _amr_fneq_postcoll_prolong_scale (:39-51), on by default
+    const T omega_c = T(1) / std::max(P.tau_parent, T(0.500001));
+    const T omega_f = T(1) / std::max(P.tau_fine, T(0.500001));
+    const T one_m_wc = T(1) - omega_c, one_m_wf = T(1) - omega_f;
+    if (std::fabs(one_m_wc) > T(1e-6)) scale = std::min(std::max(scale * (one_m_wf / one_m_wc), T(0.01)), T(100));
+  }
+  return feq_int + f_neq * scale;
+}
 
 // physics_utils.jl:2001-2035 get_velocity_neighbor_fluid (sym_y_plane = 0)
 template <class T>
@@ -276,6 +513,10 @@ void step_cell(const Level& L, const oal_step_params& P, const T* f_in, T* f_out
               const int zw_lx = zw_ix < 0 ? zw_ix + BS : (zw_ix >= BS ? zw_ix - BS : zw_ix);
               const int zw_ly = zw_iy < 0 ? zw_iy + BS : (zw_iy >= BS ? zw_iy - BS : zw_iy);
               val = f_in[A.f(zw_lx, zw_ly, z, zw_nb - 1, zw_k)];
+            } else if (L.parent && gy - cy >= 1 && gy - cy <= L.ny) {
+              // refined level: the image cell comes from the parent (kernel_cumulant.jl:286-312)
+              val = interpolate_with_rescaling<T>(*static_cast<const Parent<T>*>(L.parent), gx - cx, gy - cy, gz, zw_k,
+                                                  T(TB.w[zw_k]), T(cx), T(cy), T(-cz));
             } else {
               // level 1: no parent image; the cell's own mirror_z population
               val = f_in[A.f(x, y, z, b, zw_k)];
@@ -293,6 +534,10 @@ void step_cell(const Level& L, const oal_step_params& P, const T* f_in, T* f_out
         val = f_in[A.f(x, y, z, b, TB.mir_y[k])];
       } else if (is_z_min || is_z_max) {
         val = f_in[A.f(x, y, z, b, TB.mir_z[k])];
+      } else if (L.parent) {
+        // refined level: interpolated from the parent (kernel_cumulant.jl:346-388)
+        val = interpolate_with_rescaling<T>(*static_cast<const Parent<T>*>(L.parent), src_gx, src_gy, src_gz, k,
+                                            T(TB.w[k]), T(cx), T(cy), T(cz));
       } else {
         // level 1 (no parent): lattice weight (kernel_cumulant.jl:389-391)
         val = T(TB.w[k]);
@@ -595,6 +840,156 @@ int step_level(const Level& L, const oal_step_params& P, const T* f_in, T* f_out
   return 0;
 }
 
+// ---- restriction (amr_coupling.jl, default flags) --------------------------------------------
+// solve_shell_moment4 (:130-176): 4x4 Gaussian elimination without pivoting
+template <class T>
+bool solve_shell_moment4(T m00, T m01, T m02, T m03, T m11, T m12, T m13, T m22, T m23, T m33, T r0, T r1, T r2,
+                         T r3, T& x0, T& x1, T& x2, T& x3) {
+  const T eps = T(1e-12);
+  T a00 = m00 + eps, a01 = m01, a02 = m02, a03 = m03, b0 = r0;
+  T a10 = m01, a11 = m11 + eps, a12 = m12, a13 = m13, b1 = r1;
+  T a20 = m02, a21 = m12, a22 = m22 + eps, a23 = m23, b2 = r2;
+  T a30 = m03, a31 = m13, a32 = m23, a33 = m33 + eps, b3 = r3;
+  const T p0 = a00;
+  const bool ok0 = std::fabs(p0) > eps;
+  const T inv0 = ok0 ? T(1) / p0 : T(0);
+  const T f10 = a10 * inv0, f20 = a20 * inv0, f30 = a30 * inv0;
+  a11 -= f10 * a01; a12 -= f10 * a02; a13 -= f10 * a03; b1 -= f10 * b0;
+  a21 -= f20 * a01; a22 -= f20 * a02; a23 -= f20 * a03; b2 -= f20 * b0;
+  a31 -= f30 * a01; a32 -= f30 * a02; a33 -= f30 * a03; b3 -= f30 * b0;
+  const T p1 = a11;
+  const bool ok1 = std::fabs(p1) > eps;
+  const T inv1 = ok1 ? T(1) / p1 : T(0);
+  const T f21 = a21 * inv1, f31 = a31 * inv1;
+  a22 -= f21 * a12; a23 -= f21 * a13; b2 -= f21 * b1;
+  a32 -= f31 * a12; a33 -= f31 * a13; b3 -= f31 * b1;
+  const T p2 = a22;
+  const bool ok2 = std::fabs(p2) > eps;
+  const T inv2 = ok2 ? T(1) / p2 : T(0);
+  const T f32 = a32 * inv2;
+  a33 -= f32 * a23; b3 -= f32 * b2;
+  const T p3 = a33;
+  const bool ok3 = std::fabs(p3) > eps;
+  const T inv3 = ok3 ? T(1) / p3 : T(0);
+  x3 = b3 * inv3;
+  x2 = (b2 - a23 * x3) * inv2;
+  x1 = (b1 - a12 * x2 - a13 * x3) * inv1;
+  x0 = (b0 - a01 * x1 - a02 * x2 - a03 * x3) * inv0;
+  return ok0 && ok1 && ok2 && ok3;
+}
+
+// tau_ratio_flow of restrict_fine_to_parent! (:7596-7615): (tau_p - 1/2)/(tau_c - 1/2), or the
+// physical rule, times the post-collision factor (1 - omega_p)/(1 - omega_c)
+template <class T>
+T restrict_tau_ratio(T tau_p, T tau_c, int level_visc_physical) {
+  const T tpc = std::max(tau_p - T(0.5), T(1e-6)), tcc = std::max(tau_c - T(0.5), T(1e-6));
+  T r = std::min(std::max(tpc / tcc, T(0.01)), T(100));
+  if (level_visc_physical == 1) r = std::min(std::max(T(2) * tau_p / std::max(tau_c, T(0.500001)), T(0.01)), T(100));
+  const T omega_p = T(1) / std::max(tau_p, T(0.500001)), omega_c = T(1) / std::max(tau_c, T(0.500001));
+  const T one_m_wp = T(1) - omega_p, one_m_wc = T(1) - omega_c;
+  if (std::fabs(one_m_wc) > T(1e-6)) r = std::min(std::max(r * (one_m_wp / one_m_wc), T(0.01)), T(100));
+  return r;
+}
+
+// restrict_child_state_to_parent_kernel! (:1900-3242) for one parent cell whose 8 children exist:
+// children average, f = feq + ratio (avg - feq), two moment-correction passes, shell macros
+template <class T>
+void restrict_cell(int32_t pnb, const int32_t* pcoords, T* pf, T* prho, T* pvel, int32_t cnb, const int32_t* cptr,
+                   int32_t cdx, int32_t cdy, int32_t cdz, const uint8_t* cobst, const T* cf, T ratio, int comp, int pb,
+                   int lx, int ly, int lz) {
+  const int64_t pn = 512 * (int64_t)pnb, cn = 512 * (int64_t)cnb;
+  const int cbase_x = 2 * pcoords[3 * pb] - 1, cbase_y = 2 * pcoords[3 * pb + 1] - 1, cbase_z = 2 * pcoords[3 * pb + 2] - 1;
+  int64_t ccell[8];
+  int n = 0;
+  for (int sx = 0; sx <= 1; ++sx)
+    for (int sy = 0; sy <= 1; ++sy)
+      for (int sz = 0; sz <= 1; ++sz) {
+        const int fx = 2 * (lx - 1) + 1 + sx, fy = 2 * (ly - 1) + 1 + sy, fz = 2 * (lz - 1) + 1 + sz;
+        const int cbx = cbase_x + (fx - 1) / BS, cby = cbase_y + (fy - 1) / BS, cbz = cbase_z + (fz - 1) / BS;
+        if (cbx < 1 || cby < 1 || cbz < 1 || cbx > cdx || cby > cdy || cbz > cdz) return;
+        const int32_t cb = cptr[(cbx - 1) + (int64_t)cdx * ((cby - 1) + (int64_t)cdy * (cbz - 1))];
+        if (cb == 0) return;
+        ccell[n++] = cidx((fx - 1) % BS, (fy - 1) % BS, (fz - 1) % BS) + 512 * (int64_t)(cb - 1);
+      }
+  T avg[Q];
+  for (int k = 0; k < Q; ++k) avg[k] = T(0);
+  int fluid = 0;
+  for (int c = 0; c < 8; ++c) {
+    if (cobst && cobst[ccell[c]]) continue;
+    ++fluid;
+    for (int k = 0; k < Q; ++k) avg[k] += cf[ccell[c] + cn * k];
+  }
+  if (fluid == 0) return;
+  const T inv_children = T(1) / T(fluid);
+  T rho_raw = T(0), jx = T(0), jy = T(0), jz = T(0);
+  for (int k = 0; k < Q; ++k) {
+    const T favg = avg[k] * inv_children;
+    avg[k] = favg;
+    rho_raw += favg;
+    jx += favg * T(TB.cx[k]);
+    jy += favg * T(TB.cy[k]);
+    jz += favg * T(TB.cz[k]);
+  }
+  const T rho_p = std::max(rho_raw, T(0.01));
+  const T inv_rho = T(1) / rho_p;
+  const T ux = jx * inv_rho, uy = jy * inv_rho, uz = jz * inv_rho;
+  const int64_t pc = cidx(lx - 1, ly - 1, lz - 1) + 512 * (int64_t)pb;
+  const T frac = T(1), one_m_frac = T(0);
+  for (int k = 0; k < Q; ++k) {
+    const T feq = feq_auto<T>(rho_p, ux, uy, uz, T(TB.w[k]), T(TB.cx[k]), T(TB.cy[k]), T(TB.cz[k]), comp);
+    const T prior = pf[pc + pn * k];
+    const T fr = feq + ratio * (avg[k] - feq);
+    pf[pc + pn * k] = std::max(frac * fr + one_m_frac * prior, T(1e-10));
+  }
+  T m00 = 0, m01 = 0, m02 = 0, m03 = 0, m11 = 0, m12 = 0, m13 = 0, m22 = 0, m23 = 0, m33 = 0;
+  for (int k = 0; k < Q; ++k) {
+    const T cx = T(TB.cx[k]), cy = T(TB.cy[k]), cz = T(TB.cz[k]), w = T(TB.w[k]);
+    m00 += w; m01 += w * cx; m02 += w * cy; m03 += w * cz;
+    m11 += w * cx * cx; m12 += w * cx * cy; m13 += w * cx * cz;
+    m22 += w * cy * cy; m23 += w * cy * cz; m33 += w * cz * cz;
+  }
+  const T inv_cs2 = T(1) / std::max(T(1.0 / 3.0), T(1e-6));
+  for (int pass = 0; pass < 2; ++pass) {  // AMR_RESTRICTION_CORRECTION_PASSES = 2
+    T rr = T(0), rx = T(0), ry = T(0), rz = T(0);
+    for (int k = 0; k < Q; ++k) {
+      const T v = pf[pc + pn * k];
+      rr += v; rx += v * T(TB.cx[k]); ry += v * T(TB.cy[k]); rz += v * T(TB.cz[k]);
+    }
+    const T dr = rho_p - rr, dx = jx - rx, dy = jy - ry, dz = jz - rz;
+    if (std::fabs(dr) > T(1e-12) || std::fabs(dx) > T(1e-12) || std::fabs(dy) > T(1e-12) || std::fabs(dz) > T(1e-12)) {
+      T c0, c1, c2, c3;
+      const bool ok = solve_shell_moment4<T>(m00, m01, m02, m03, m11, m12, m13, m22, m23, m33, dr, dx, dy, dz, c0, c1, c2, c3);
+      for (int k = 0; k < Q; ++k) {
+        const T cx = T(TB.cx[k]), cy = T(TB.cy[k]), cz = T(TB.cz[k]), w = T(TB.w[k]);
+        const T delta = ok ? w * (c0 + c1 * cx + c2 * cy + c3 * cz) : w * (dr + inv_cs2 * (cx * dx + cy * dy + cz * dz));
+        pf[pc + pn * k] = std::max(pf[pc + pn * k] + delta, T(1e-10));
+      }
+    }
+  }
+  T rs = T(0), sx = T(0), sy = T(0), sz = T(0);
+  for (int k = 0; k < Q; ++k) {
+    const T v = pf[pc + pn * k];
+    rs += v; sx += v * T(TB.cx[k]); sy += v * T(TB.cy[k]); sz += v * T(TB.cz[k]);
+  }
+  const T rho_s = std::max(rs, T(0.01));
+  const T inv_s = T(1) / rho_s;
+  prho[pc] = rho_s;
+  pvel[pc] = sx * inv_s; pvel[pc + pn] = sy * inv_s; pvel[pc + 2 * pn] = sz * inv_s;
+}
+
+template <class T>
+void restrict_level(int32_t pnb, const int32_t* pcoords, T* pf, T* prho, T* pvel, int32_t cnb, const int32_t* cptr,
+                    int32_t cdx, int32_t cdy, int32_t cdz, const uint8_t* cobst, const T* cf, T tau_p, T tau_c, int comp,
+                    int level_visc_physical) {
+  const T ratio = restrict_tau_ratio<T>(tau_p, tau_c, level_visc_physical);
+#pragma omp parallel for schedule(static)
+  for (int pb = 0; pb < pnb; ++pb)
+    for (int lz = 1; lz <= BS; ++lz)
+      for (int ly = 1; ly <= BS; ++ly)
+        for (int lx = 1; lx <= BS; ++lx)
+          restrict_cell<T>(pnb, pcoords, pf, prho, pvel, cnb, cptr, cdx, cdy, cdz, cobst, cf, ratio, comp, pb, lx, ly, lz);
+}
+
 Level make_level(int32_t nb, int32_t nx, int32_t ny, int32_t nz, const int32_t* coords, const int32_t* nbr,
                  const uint8_t* obstacle, const float* sponge, const float* wall_dist) {
   return Level{nb, nx, ny, nz, coords, nbr, obstacle, sponge, wall_dist};
@@ -689,6 +1084,54 @@ int ora_step_d3q27_f32(int32_t nb, int32_t nx, int32_t ny, int32_t nz, const int
                        float* rho_out, float* vel_out, const float* vel_in, double* force_out) {
   Level L = make_level(nb, nx, ny, nz, coords, nbr, obstacle, sponge, wall_dist);
   return step_level<float>(L, *P, f_in, f_out, f_post, rho_out, vel_out, vel_in, force_out);
+}
+
+// A refined level's step: the level step with its pulls from outside its blocks interpolated from
+// the parent. parent_ptr: (pdx, pdy, pdz) Julia column-major, 1-based parent block or 0;
+// parent arrays in the parent level's reference layout (pnb blocks); the *_old arrays may be null.
+int ora_step_d3q27_refined_f64(int32_t nb, int32_t nx, int32_t ny, int32_t nz, const int32_t* coords,
+                               const int32_t* nbr, const uint8_t* obstacle, const oal_step_params* P,
+                               const double* f_in, double* f_out, double* rho_out, double* vel_out,
+                               const double* vel_in, double* force_out, int32_t pnb, const int32_t* pptr, int32_t pdx,
+                               int32_t pdy, int32_t pdz, const double* pf_new, const double* prho_new,
+                               const double* pvel_new, const double* pf_old, const double* prho_old,
+                               const double* pvel_old, double tau_parent, double tw, int32_t use_temporal) {
+  Parent<double> PP{pf_new, prho_new, pvel_new, pf_old, prho_old, pvel_old, pptr, pdx, pdy, pdz, pnb,
+                    (double)tau_parent, (double)P->tau, tw, use_temporal, P->compressible_corr, P->level_visc_physical};
+  Level L = make_level(nb, nx, ny, nz, coords, nbr, obstacle, nullptr, nullptr);
+  L.parent = &PP;
+  return step_level<double>(L, *P, f_in, f_out, nullptr, rho_out, vel_out, vel_in, force_out);
+}
+
+int ora_step_d3q27_refined_f32(int32_t nb, int32_t nx, int32_t ny, int32_t nz, const int32_t* coords,
+                               const int32_t* nbr, const uint8_t* obstacle, const oal_step_params* P,
+                               const float* f_in, float* f_out, float* rho_out, float* vel_out, const float* vel_in,
+                               double* force_out, int32_t pnb, const int32_t* pptr, int32_t pdx, int32_t pdy,
+                               int32_t pdz, const float* pf_new, const float* prho_new, const float* pvel_new,
+                               const float* pf_old, const float* prho_old, const float* pvel_old, double tau_parent,
+                               double tw, int32_t use_temporal) {
+  Parent<float> PP{pf_new, prho_new, pvel_new, pf_old, prho_old, pvel_old, pptr, pdx, pdy, pdz, pnb,
+                   (float)tau_parent, P->tau, (float)tw, use_temporal, P->compressible_corr, P->level_visc_physical};
+  Level L = make_level(nb, nx, ny, nz, coords, nbr, obstacle, nullptr, nullptr);
+  L.parent = &PP;
+  return step_level<float>(L, *P, f_in, f_out, nullptr, rho_out, vel_out, vel_in, force_out);
+}
+
+// restrict_fine_to_parent! on the parent's current arrays (reference layout): every parent cell
+// whose 8 children exist. child_ptr: (cdx, cdy, cdz) Julia column-major, 1-based child block or 0.
+void ora_restrict_d3q27_f64(int32_t pnb, const int32_t* pcoords, double* pf, double* prho, double* pvel,
+                            int32_t cnb, const int32_t* cptr, int32_t cdx, int32_t cdy, int32_t cdz,
+                            const uint8_t* cobst, const double* cf, double tau_p, double tau_c, int32_t comp,
+                            int32_t level_visc_physical) {
+  restrict_level<double>(pnb, pcoords, pf, prho, pvel, cnb, cptr, cdx, cdy, cdz, cobst, cf, tau_p, tau_c, comp,
+                         level_visc_physical);
+}
+
+void ora_restrict_d3q27_f32(int32_t pnb, const int32_t* pcoords, float* pf, float* prho, float* pvel, int32_t cnb,
+                            const int32_t* cptr, int32_t cdx, int32_t cdy, int32_t cdz, const uint8_t* cobst,
+                            const float* cf, double tau_p, double tau_c, int32_t comp, int32_t level_visc_physical) {
+  restrict_level<float>(pnb, pcoords, pf, prho, pvel, cnb, cptr, cdx, cdy, cdz, cobst, cf, (float)tau_p, (float)tau_c,
+                        comp, level_visc_physical);
 }
 
 // Float64 totals over fluid cells (state.jl:614-637): out = {mass, px, py, pz} from f.
