@@ -171,6 +171,57 @@ def benchmark_entropic(n: int = 128, steps: int = 50, warmup: int = 5, u0: float
     return out
 
 
+def benchmark_amr(steps: int = 50, warmup: int = 5, storage: str = "f16", nx: int = 256, ny: int = 128, nz: int = 128,
+                  diameter_fine: float = 48.0, re: float = 1000.0, u: float = 0.05) -> dict:
+    """Two-level block AMR of the sphere channel: the coarse 256x128x128 channel of config 2 and a
+    fine level (2x resolution) over the box [32,128) x [32,96) x [32,96) coarse cells around the
+    sphere (diameter 24 coarse = 48 fine cells, centred at x = 64). Half-way walls on both levels,
+    the legacy level-viscosity rule (tau_c - 1/2 = 2 (tau_f - 1/2)), Re on the fine diameter. n
+    coarse steps per CUDA graph, timed with CUDA events; MLUPS on the work W = coarse cells +
+    2 x fine cells per coarse step (src/octree_q19/src/run.jl:99 counts AMR work the same way)."""
+    import torch
+    from . import _capi as capi
+    from .amr import Hierarchy, blocks_in_box, level_taus, refine
+    from .solver import apply_analytic_sphere_obstacle, build_box, default_step_params
+    coarse = build_box(nx // 8, ny // 8, nz // 8)
+    centre = (64.0, ny / 2.0, nz / 2.0)
+    apply_analytic_sphere_obstacle(coarse, centre, diameter_fine / 4.0)
+    fine = refine(coarse, blocks_in_box(coarse, (32, 32, 32), (128, 96, 96)))
+    apply_analytic_sphere_obstacle(fine, tuple(2 * c for c in centre), diameter_fine / 2.0)
+    nu_f = u * diameter_fine / re
+    taus = level_taus(3.0 * nu_f + 0.5, 2)
+    P = [default_step_params(tau=t, c_wale=0.2, u_inlet=u, solid_bc=capi.OAL_SOLID_HALFWAY) for t in taus]
+    H = Hierarchy([coarse, fine], storage=storage)
+    for lvl, d in enumerate([coarse, fine]):
+        n = d.n_blocks * 512
+        vel = np.zeros((3, d.n_blocks, 512))
+        vel[0] = u
+        if d.obstacle is not None:
+            vel[0][d.obstacle.astype(bool)] = 0.0
+        H.level(lvl).init_equilibrium(np.ones((d.n_blocks, 512)), vel)
+    s = torch.cuda.Stream()
+    H.advance(P, warmup, s)
+    H.advance(P, steps, s)
+    s.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    H.advance(P, steps, s)
+    e1.record(s)
+    s.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    cells = [coarse.n_blocks * 512, fine.n_blocks * 512]
+    work = cells[0] + 2 * cells[1]
+    bpc = 2 * 27 * {"f16": 2, "bf16": 2, "f32": 4, "f64": 8}[storage]
+    _, rho_f, vel_f = H.level(1).state()
+    ok = bool(np.all(np.isfinite(vel_f)))
+    H.close()
+    return {"workload": f"amr2_sphere_channel_{nx}x{ny}x{nz}_fine_box_96x64x64_{storage}", "coarse_cells": cells[0],
+            "fine_cells": cells[1], "work_per_coarse_step": work, "steps": steps, "ms_per_coarse_step": round(ms, 4),
+            "mlups": round(work / ms / 1e3, 1), "bytes_per_update": bpc,
+            "achieved_gbs": round(work * bpc / ms / 1e6, 1), "finite": ok,
+            "gpu_launches_per_coarse_step": "level 0: ghost fill, fast, general; level 1 (x2): the same; restriction; 3 snapshot copies"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--steps", type=int, default=2000)
