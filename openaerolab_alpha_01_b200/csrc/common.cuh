@@ -108,6 +108,19 @@ struct ParentView {
   int32_t dim_x, dim_y, dim_z, nb;
   double tau_parent, tau_fine, tw;
   int32_t use_temporal, level_visc_physical;
+  // parent nodes evaluated once per substep (k_parent_nodes): node_map[parent cell] = record index
+  // or -1; record = 32 values of the compute type: blended rho, ux, uy, uz, then f_neq of the 27
+  // directions. Null: evaluate nodes on the fly.
+  const int32_t* node_map;
+  const void* node_vals;
+  // interpolation positions (the level's ghost cells whose pulls interpolate): slot_pos[(ghost
+  // block - real blocks) * 512 + cell] = position or -1; pos_nodes[position * 64 + 16(a+1) +
+  // 4(b+1) + (c+1)] = record of parent node (px0+a, py0+b, pz0+c) or -1 (absent); pos_macro =
+  // the interpolated rho, ux, uy, uz of each position (k_parent_positions, once per substep)
+  const int32_t* slot_pos;
+  const int32_t* pos_nodes;
+  const void* pos_macro;
+  int32_t n_pos, n_real;
 };
 
 // Restriction of a child level onto its parent (block AMR)

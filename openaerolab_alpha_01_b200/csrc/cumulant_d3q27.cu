@@ -82,11 +82,9 @@ __device__ __forceinline__ void parent_bracket(R p_cont, int n, int& i0, int& i1
   w = fmin(fmax(pc - R(i0), R(0)), R(1));
 }
 
+// time-blended parent node c (a valid parent cell) in direction k: f, macros and f_neq
 template <class S, class R>
-__device__ PNode<R> parent_blended(const ParentView& P, int pgx, int pgy, int pgz, int k, R wk, R cx, R cy, R cz,
-                                   bool comp) {
-  const int64_t c = parent_cell(P, pgx, pgy, pgz);
-  if (c < 0) return PNode<R>{wk, R(1), R(0), R(0), R(0), R(0), false};
+__device__ PNode<R> parent_blended_at(const ParentView& P, int64_t c, int k, R wk, R cx, R cy, R cz, bool comp) {
   const int64_t n = (int64_t)P.nb * kCells;
   const int64_t fi = (c >> 9) * (27 * kCells) + k * kCells + (c & 511);
   const S* fn = static_cast<const S*>(P.f_new);
@@ -110,9 +108,7 @@ __device__ PNode<R> parent_blended(const ParentView& P, int pgx, int pgy, int pg
 }
 
 template <class R>
-__device__ PNode<R> parent_macro(const ParentView& P, int pgx, int pgy, int pgz) {
-  const int64_t c = parent_cell(P, pgx, pgy, pgz);
-  if (c < 0) return PNode<R>{R(0), R(1), R(0), R(0), R(0), R(0), false};
+__device__ PNode<R> parent_macro_at(const ParentView& P, int64_t c) {
   const int64_t n = (int64_t)P.nb * kCells;
   const R* rn = static_cast<const R*>(P.rho_new);
   const R* vn = static_cast<const R*>(P.vel_new);
@@ -127,6 +123,61 @@ __device__ PNode<R> parent_macro(const ParentView& P, int pgx, int pgy, int pgz)
     uz = vo[c + 2 * n] * (R(1) - tw) + uz * tw;
   }
   return PNode<R>{R(0), rho, ux, uy, uz, R(0), true};
+}
+
+// parent node lookups: the per-substep records when the level has them, else on the fly
+template <class S, class R>
+__device__ __forceinline__ PNode<R> parent_blended(const ParentView& P, int pgx, int pgy, int pgz, int k, R wk, R cx,
+                                                   R cy, R cz, bool comp) {
+  const int64_t c = parent_cell(P, pgx, pgy, pgz);
+  if (c < 0) return PNode<R>{wk, R(1), R(0), R(0), R(0), R(0), false};
+  if (P.node_map) {
+    const int32_t i = P.node_map[c];
+    if (i >= 0) {
+      const R* v = static_cast<const R*>(P.node_vals) + (int64_t)i * 32;
+      return PNode<R>{R(0), v[0], v[1], v[2], v[3], v[4 + k], true};
+    }
+  }
+  return parent_blended_at<S, R>(P, c, k, wk, cx, cy, cz, comp);
+}
+
+template <class R>
+__device__ __forceinline__ PNode<R> parent_macro(const ParentView& P, int pgx, int pgy, int pgz) {
+  const int64_t c = parent_cell(P, pgx, pgy, pgz);
+  if (c < 0) return PNode<R>{R(0), R(1), R(0), R(0), R(0), R(0), false};
+  if (P.node_map) {
+    const int32_t i = P.node_map[c];
+    if (i >= 0) {
+      const R* v = static_cast<const R*>(P.node_vals) + (int64_t)i * 32;
+      return PNode<R>{R(0), v[0], v[1], v[2], v[3], R(0), true};
+    }
+  }
+  return parent_macro_at<R>(P, c);
+}
+
+// One thread per needed parent node: its time-blended macros and the f_neq of the 27 directions,
+// the same expressions the interpolation evaluates per stencil node
+template <class S, class R>
+__global__ void __launch_bounds__(256) k_parent_nodes(const ParentView P, const int32_t* __restrict__ nodes, int32_t n,
+                                                      R* __restrict__ vals, int32_t comp) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t c = nodes[i];
+  R* v = vals + (int64_t)i * 32;
+  const PNode<R> m = parent_macro_at<R>(P, c);
+  v[0] = m.rho; v[1] = m.ux; v[2] = m.uy; v[3] = m.uz;
+#pragma unroll
+  for (int k = 0; k < kQ27; ++k)
+    v[4 + k] = parent_blended_at<S, R>(P, c, k, R(q27_w(k)), R(q27_cx(k)), R(q27_cy(k)), R(q27_cz(k)), comp != 0).fneq;
+  v[31] = R(0);
+}
+
+template <class S, class R>
+cudaError_t launch_parent_nodes(const ParentView& P, const int32_t* nodes, int32_t n, void* vals, int32_t comp,
+                                cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  k_parent_nodes<S, R><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(P, nodes, n, static_cast<R*>(vals), comp);
+  return cudaGetLastError();
 }
 
 template <class R>
@@ -188,6 +239,186 @@ __device__ bool parent_sample_macro(const ParentView& P, int fgx, int fgy, int f
   }
   r_out = r; x_out = ux; y_out = uy; z_out = uz;
   return true;
+}
+
+// ---- interpolation at a precomputed position: the same arithmetic as parent_population below,
+// with the stencil's node records listed per position and its macros evaluated once per substep
+template <class R>
+__device__ __forceinline__ void pos_record(const ParentView& P, const int32_t* nodes, int a, int b, int c,
+                                           bool& ok, const R*& v) {
+  const int32_t i = nodes[16 * (a + 1) + 4 * (b + 1) + (c + 1)];
+  ok = i >= 0;
+  v = static_cast<const R*>(P.node_vals) + (int64_t)(ok ? i : 0) * 32;
+}
+
+// interpolated macros of a position (the macro half of interpolate_with_rescaling, :924-1129)
+template <class R>
+__device__ void pos_macros(const ParentView& P, int32_t pos, int fgx, int fgy, int fgz, R* out) {
+  const int32_t* nodes = P.pos_nodes + (int64_t)pos * 64;
+  const int pnx = P.dim_x * kBS, pny = P.dim_y * kBS, pnz = P.dim_z * kBS;
+  int px0, px1, py0, py1, pz0, pz1;
+  R wx, wy, wz;
+  parent_bracket<R>(R(fgx) * R(0.5) + R(0.25), pnx, px0, px1, wx);
+  parent_bracket<R>(R(fgy) * R(0.5) + R(0.25), pny, py0, py1, wy);
+  parent_bracket<R>(R(fgz) * R(0.5) + R(0.25), pnz, pz0, pz1, wz);
+  const bool use_cubic = px0 - 2 >= 1 && px0 + 2 <= pnx && py0 - 2 >= 1 && py0 + 2 <= pny && pz0 - 2 >= 1 &&
+                         pz0 + 2 <= pnz;
+  bool all_valid = use_cubic;
+  if (use_cubic)
+    for (int i = 0; i < 64 && all_valid; ++i) all_valid = nodes[i] >= 0;
+  R rho_i, ux_i, uy_i, uz_i;
+  if (all_valid) {
+    rho_i = ux_i = uy_i = uz_i = R(0);
+#pragma unroll 4
+    for (int i = 0; i < 64; ++i) {
+      const int a = (i >> 4) - 1, bb = ((i >> 2) & 3) - 1, c = (i & 3) - 1;
+      const R* v = static_cast<const R*>(P.node_vals) + (int64_t)nodes[i] * 32;
+      const R w3 = lagrange3<R>(a, wx) * lagrange3<R>(bb, wy) * lagrange3<R>(c, wz);
+      rho_i += w3 * v[0];
+      ux_i += w3 * v[1];
+      uy_i += w3 * v[2];
+      uz_i += w3 * v[3];
+    }
+  } else {
+    // sample_parent_macro_for_fine_cell on the stencil's corner records (far nodes a, b, c = -1 or 2)
+    PNode<R> d[8];
+#pragma unroll
+    for (int cc = 0; cc < 8; ++cc) {
+      bool ok;
+      const R* v;
+      pos_record<R>(P, nodes, cc & 1, (cc >> 1) & 1, (cc >> 2) & 1, ok, v);
+      d[cc] = ok ? PNode<R>{R(0), v[0], v[1], v[2], v[3], R(0), true} : PNode<R>{R(0), R(1), R(0), R(0), R(0), R(0), false};
+    }
+    const R w[8] = {(R(1) - wx) * (R(1) - wy) * (R(1) - wz), wx * (R(1) - wy) * (R(1) - wz),
+                    (R(1) - wx) * wy * (R(1) - wz),         wx * wy * (R(1) - wz),
+                    (R(1) - wx) * (R(1) - wy) * wz,         wx * (R(1) - wy) * wz,
+                    (R(1) - wx) * wy * wz,                  wx * wy * wz};
+    bool all = true, any = false;
+#pragma unroll
+    for (int cc = 0; cc < 8; ++cc) { all = all && d[cc].ok; any = any || d[cc].ok; }
+    bool sampled = true;
+    if (!all) {
+      if (!any) {
+        sampled = false;
+      } else {
+        const int ea[12] = {0, 2, 4, 6, 0, 1, 4, 5, 0, 1, 2, 3};
+        const int eb[12] = {1, 3, 5, 7, 2, 3, 6, 7, 4, 5, 6, 7};
+#pragma unroll 1
+        for (int e = 0; e < 12; ++e) {
+          const int a = ea[e], b = eb[e];
+          if (d[a].ok == d[b].ok) continue;
+          const int src = d[a].ok ? a : b, dst = d[a].ok ? b : a;
+          int ia = src & 1, ib = (src >> 1) & 1, ic = (src >> 2) & 1;
+          if (e < 4) ia = d[a].ok ? -1 : 2;
+          else if (e < 8) ib = d[a].ok ? -1 : 2;
+          else ic = d[a].ok ? -1 : 2;
+          bool fok;
+          const R* fv;
+          pos_record<R>(P, nodes, ia, ib, ic, fok, fv);
+          const PNode<R> s0 = d[src];
+          d[dst].rho = fok ? R(2) * s0.rho - fv[0] : s0.rho;
+          d[dst].ux = fok ? R(2) * s0.ux - fv[1] : s0.ux;
+          d[dst].uy = fok ? R(2) * s0.uy - fv[2] : s0.uy;
+          d[dst].uz = fok ? R(2) * s0.uz - fv[3] : s0.uz;
+          d[dst].ok = true;
+        }
+      }
+    }
+    if (sampled) {
+      rho_i = w[0] * d[0].rho; ux_i = w[0] * d[0].ux; uy_i = w[0] * d[0].uy; uz_i = w[0] * d[0].uz;
+#pragma unroll
+      for (int cc = 1; cc < 8; ++cc) {
+        rho_i = rho_i + w[cc] * d[cc].rho; ux_i = ux_i + w[cc] * d[cc].ux;
+        uy_i = uy_i + w[cc] * d[cc].uy; uz_i = uz_i + w[cc] * d[cc].uz;
+      }
+    } else {
+      // no corner exists: the trilinear blend of corners that all carry the absent node's
+      // rho = 1, u = 0
+      auto tri = [&](R a) {
+        const R c00 = a * (R(1) - wx) + a * wx, c0 = c00 * (R(1) - wy) + c00 * wy;
+        return c0 * (R(1) - wz) + c0 * wz;
+      };
+      rho_i = tri(R(1)); ux_i = uy_i = uz_i = tri(R(0));
+    }
+  }
+  out[0] = rho_i; out[1] = ux_i; out[2] = uy_i; out[3] = uz_i;
+}
+
+// One thread per interpolation position of the level: its interpolated macros for this substep
+template <class R>
+__global__ void __launch_bounds__(256) k_parent_positions(const ParentView P, const int4* __restrict__ pos_xyz,
+                                                          int32_t n, R* __restrict__ macro) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int4 q = pos_xyz[i];
+  pos_macros<R>(P, i, q.x, q.y, q.z, macro + (int64_t)i * 4);
+}
+
+template <class R>
+cudaError_t launch_parent_positions(const ParentView& P, const int4* pos_xyz, int32_t n, void* macro, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  k_parent_positions<R><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(P, pos_xyz, n, static_cast<R*>(macro));
+  return cudaGetLastError();
+}
+
+// the direction-dependent half at a position: f_neq over the stencil's records, then
+// feq(interpolated macros) + f_neq * scale (:1131-1198)
+template <class R>
+__device__ R pos_population(const ParentView& P, int32_t pos, int fgx, int fgy, int fgz, int k, R cx, R cy, R cz,
+                            bool comp) {
+  const int32_t* nodes = P.pos_nodes + (int64_t)pos * 64;
+  const R* mac = static_cast<const R*>(P.pos_macro) + (int64_t)pos * 4;
+  const R wk = R(q27_w(k));
+  const int pnx = P.dim_x * kBS, pny = P.dim_y * kBS, pnz = P.dim_z * kBS;
+  int px0, px1, py0, py1, pz0, pz1;
+  R wx, wy, wz;
+  parent_bracket<R>(R(fgx) * R(0.5) + R(0.25), pnx, px0, px1, wx);
+  parent_bracket<R>(R(fgy) * R(0.5) + R(0.25), pny, py0, py1, wy);
+  parent_bracket<R>(R(fgz) * R(0.5) + R(0.25), pnz, pz0, pz1, wz);
+  const bool use_cubic = px0 - 2 >= 1 && px0 + 2 <= pnx && py0 - 2 >= 1 && py0 + 2 <= pny && pz0 - 2 >= 1 &&
+                         pz0 + 2 <= pnz;
+  // corner records and the anchor (first existing corner in 000, 100, 010, 110, 001, ... order)
+  int32_t corner[8];
+#pragma unroll
+  for (int cc = 0; cc < 8; ++cc) corner[cc] = nodes[16 * ((cc & 1) + 1) + 4 * (((cc >> 1) & 1) + 1) + ((cc >> 2) & 1) + 1];
+  int anchor = 7;
+#pragma unroll
+  for (int cc = 6; cc >= 0; --cc)
+    if (corner[cc] >= 0) anchor = cc;
+  const R* vals = static_cast<const R*>(P.node_vals);
+  // absent corner of a present anchor: the anchor's f_neq; no corner present: 0 (parent_blended's
+  // absent node)
+  const R anchor_neq = corner[anchor] >= 0 ? vals[(int64_t)corner[anchor] * 32 + 4 + k] : R(0);
+  R f_neq = R(0);
+  if (use_cubic) {
+#pragma unroll 4
+    for (int i = 0; i < 64; ++i) {
+      const int a = (i >> 4) - 1, bb = ((i >> 2) & 3) - 1, c = (i & 3) - 1;
+      const int32_t ni = nodes[i];
+      const R nv = ni >= 0 ? vals[(int64_t)ni * 32 + 4 + k] : anchor_neq;
+      f_neq += lagrange3<R>(a, wx) * lagrange3<R>(bb, wy) * lagrange3<R>(c, wz) * nv;
+    }
+  } else {
+    R v[8];
+#pragma unroll
+    for (int cc = 0; cc < 8; ++cc) v[cc] = corner[cc] >= 0 ? vals[(int64_t)corner[cc] * 32 + 4 + k] : anchor_neq;
+    const R c00 = v[0] * (R(1) - wx) + v[1] * wx;
+    const R c01 = v[4] * (R(1) - wx) + v[5] * wx;
+    const R c10 = v[2] * (R(1) - wx) + v[3] * wx;
+    const R c11 = v[6] * (R(1) - wx) + v[7] * wx;
+    const R c0 = c00 * (R(1) - wy) + c10 * wy;
+    const R c1 = c01 * (R(1) - wy) + c11 * wy;
+    f_neq = c0 * (R(1) - wz) + c1 * wz;
+  }
+  const R feq_i = feq_c<R>(mac[0], mac[1], mac[2], mac[3], wk, cx, cy, cz, comp);
+  const R tau_p = R(P.tau_parent), tau_f = R(P.tau_fine);
+  const R tau_c = tau_p - R(0.5), tau_fm = tau_f - R(0.5);
+  R scale = tau_c > R(1e-6) ? fmin(fmax(tau_fm / tau_c, R(0.01)), R(100)) : R(1);
+  if (P.level_visc_physical == 1) scale = fmin(fmax(tau_f / (R(2) * fmax(tau_p, R(0.500001))), R(0.01)), R(100));
+  const R omega_c = R(1) / fmax(tau_p, R(0.500001)), omega_f = R(1) / fmax(tau_f, R(0.500001));
+  const R one_m_wc = R(1) - omega_c, one_m_wf = R(1) - omega_f;
+  if (fabs(one_m_wc) > R(1e-6)) scale = fmin(fmax(scale * (one_m_wf / one_m_wc), R(0.01)), R(100));
+  return feq_i + f_neq * scale;
 }
 
 // interpolate_with_rescaling at the fine cell (fgx, fgy, fgz) of the refined level, direction k
@@ -334,7 +565,16 @@ __device__ __forceinline__ R face_population_impl(const S* __restrict__ fin, int
   } else if (is_z_min || is_z_max) {
     j = q27_mir_z(k);
   } else if (da && da->par.ptr) {
-    // refined level: interpolated from the parent (kernel_cumulant.jl:346-388)
+    // refined level: interpolated from the parent (kernel_cumulant.jl:346-388); the source is a
+    // ghost cell whose interpolation position may be precomputed
+    if (da->par.slot_pos && !DENSE) {
+      const int sx = x - cx, sy = y - cy, sz = z - cz;
+      const int g = nbr[nbr_dir(sx >> 3, sy >> 3, sz >> 3)];
+      if (g >= n_real) {
+        const int32_t pos = da->par.slot_pos[(int64_t)(g - n_real) * kCells + ((sx & 7) | ((sy & 7) << 3) | ((sz & 7) << 6))];
+        if (pos >= 0) return pos_population<R>(da->par, pos, src_gx, src_gy, src_gz, k, R(cx), R(cy), R(cz), comp);
+      }
+    }
     return parent_population<S, R>(da->par, src_gx, src_gy, src_gz, k, R(cx), R(cy), R(cz), comp);
   } else {
     return R(q27_w(k));  // kernel_cumulant.jl:389-391
@@ -961,6 +1201,8 @@ cudaError_t launch_general(const StepArgs& a, const int32_t* work, int n_work, c
 #define OAL_INST(S, R)                                                                               \
   template cudaError_t launch_fill_ghosts<S, R>(const StepArgs&, const uint2*, int64_t, cudaStream_t); \
   template cudaError_t launch_restrict<S, R>(const RestrictArgs&, cudaStream_t);                       \
+  template cudaError_t launch_parent_nodes<S, R>(const ParentView&, const int32_t*, int32_t, void*, int32_t,  \
+                                                 cudaStream_t);                                            \
   template cudaError_t launch_fast<S, R>(const StepArgs&, const int32_t*, int, cudaStream_t);         \
   template cudaError_t launch_general<S, R>(const StepArgs&, const int32_t*, int, cudaStream_t);
 OAL_INST(float, float)
@@ -968,5 +1210,7 @@ OAL_INST(__half, float)
 OAL_INST(__nv_bfloat16, float)
 OAL_INST(double, double)
 #undef OAL_INST
+template cudaError_t launch_parent_positions<float>(const ParentView&, const int4*, int32_t, void*, cudaStream_t);
+template cudaError_t launch_parent_positions<double>(const ParentView&, const int4*, int32_t, void*, cudaStream_t);
 
 }  // namespace oal

@@ -27,6 +27,11 @@ template <class S>
 int dense_ctas_per_sm();
 template <class S, class R>
 cudaError_t launch_restrict(const RestrictArgs& r, cudaStream_t st);
+template <class S, class R>
+cudaError_t launch_parent_nodes(const ParentView& P, const int32_t* nodes, int32_t n, void* vals, int32_t comp,
+                                cudaStream_t st);
+template <class R>
+cudaError_t launch_parent_positions(const ParentView& P, const int4* pos_xyz, int32_t n, void* macro, cudaStream_t st);
 }
 using namespace oal;
 
@@ -1331,6 +1336,17 @@ struct AmrLevel {
   void* d_f_old = nullptr;        // snapshot before the level's step (levels with children)
   void* d_rho_old = nullptr;
   void* d_vel_old = nullptr;
+  // refined levels: the parent nodes their interpolation stencils touch, evaluated once per substep
+  int32_t* d_nodes = nullptr;     // parent cell ids (block * 512 + cell)
+  int32_t n_nodes = 0;
+  int32_t* d_node_map = nullptr;  // [parent cells] -> record index, -1
+  void* d_node_vals = nullptr;    // [n_nodes * 32] compute type
+  // interpolation positions: the ghost cells whose pulls interpolate from the parent
+  int32_t n_pos = 0;
+  int4* d_pos_xyz = nullptr;      // fine global coordinates of each position
+  int32_t* d_slot_pos = nullptr;  // [ghost blocks * 512] -> position, -1
+  int32_t* d_pos_nodes = nullptr; // [n_pos * 64] stencil records, -1 = absent parent cell
+  void* d_pos_macro = nullptr;    // [n_pos * 4] compute type
 };
 
 struct oal_amr {
@@ -1395,7 +1411,30 @@ static oal_status amr_step(oal_amr* A, int l, const std::vector<CaseParams>& cps
     v.tw = tw;
     v.use_temporal = 1;  // TEMPORAL_INTERPOLATION (config_loader.jl:90)
     v.level_visc_physical = P[l].level_visc_physical;
+    v.node_map = me.d_node_map;
+    v.node_vals = me.d_node_vals;
+    v.slot_pos = me.n_pos > 0 ? me.d_slot_pos : nullptr;
+    v.pos_nodes = me.d_pos_nodes;
+    v.pos_macro = me.d_pos_macro;
+    v.n_pos = me.n_pos;
+    v.n_real = me.g->nb;
     L->par = v;
+    if (me.n_nodes > 0) {
+      cudaError_t e = cudaErrorInvalidValue;
+      const int32_t comp = P[l].compressible_corr;
+      switch (A->storage) {
+        case OAL_STORE_F32: e = launch_parent_nodes<float, float>(v, me.d_nodes, me.n_nodes, me.d_node_vals, comp, st); break;
+        case OAL_STORE_F16_DEV: e = launch_parent_nodes<__half, float>(v, me.d_nodes, me.n_nodes, me.d_node_vals, comp, st); break;
+        case OAL_STORE_BF16_DEV: e = launch_parent_nodes<__nv_bfloat16, float>(v, me.d_nodes, me.n_nodes, me.d_node_vals, comp, st); break;
+        case OAL_STORE_F64: e = launch_parent_nodes<double, double>(v, me.d_nodes, me.n_nodes, me.d_node_vals, comp, st); break;
+      }
+      OAL_CUDA_TRY(e);
+      if (me.n_pos > 0) {
+        e = A->storage == OAL_STORE_F64 ? launch_parent_positions<double>(v, me.d_pos_xyz, me.n_pos, me.d_pos_macro, st)
+                                        : launch_parent_positions<float>(v, me.d_pos_xyz, me.n_pos, me.d_pos_macro, st);
+        OAL_CUDA_TRY(e);
+      }
+    }
   }
   CaseParams cp = cps[(size_t)l];
   cp.time_step_seed = (int32_t)(P[l].time_step_seed + t_sub);
@@ -1453,6 +1492,8 @@ void oal_amr_destroy(oal_amr* A) {
   for (AmrLevel& l : A->lv) {
     if (l.L) oal_level_destroy(l.L);
     cudaFree(l.d_ptr); cudaFree(l.d_covered); cudaFree(l.d_f_old); cudaFree(l.d_rho_old); cudaFree(l.d_vel_old);
+    cudaFree(l.d_nodes); cudaFree(l.d_node_map); cudaFree(l.d_node_vals);
+    cudaFree(l.d_pos_xyz); cudaFree(l.d_slot_pos); cudaFree(l.d_pos_nodes); cudaFree(l.d_pos_macro);
   }
   if (A->cap) cudaStreamDestroy(A->cap);
   cudaGetLastError();
@@ -1545,6 +1586,98 @@ oal_status oal_amr_create(int32_t nlevels, const oal_amr_level_desc* levels, int
       if (e == cudaSuccess) e = cudaMalloc(&me.d_f_old, ncell * 27 * storage_bytes(storage));
       if (e == cudaSuccess) e = cudaMalloc(&me.d_rho_old, ncell * macro_bytes(storage));
       if (e == cudaSuccess) e = cudaMalloc(&me.d_vel_old, ncell * 3 * macro_bytes(storage));
+    }
+    if (e == cudaSuccess && l > 0) {
+      // parent nodes of every interpolation stencil this level's ghost pulls can use: the 4x4x4
+      // parent cells around the bracket of each pull source inside the domain (and of the z-wall
+      // slip image of sources beyond the z faces)
+      const oal_geometry* g = me.g;
+      const AmrLevel& pa = A->lv[(size_t)l - 1];
+      const std::vector<int32_t>& pptr = ptrs[(size_t)l - 1];
+      const int pnx = pa.dim[0] * 8, pny = pa.dim[1] * 8, pnz = pa.dim[2] * 8;
+      std::vector<int32_t> map((size_t)pa.g->nb * 512, -1);
+      std::vector<int32_t> nodes;
+      auto bracket = [](double p, int n) {
+        if (n <= 1) return 1;
+        const double pc = std::min(std::max(p, 1.0), (double)n);
+        return std::min(std::max((int)std::floor(pc), 1), n - 1);
+      };
+      auto add_stencil = [&](int fgx, int fgy, int fgz) {
+        const int px0 = bracket(fgx * 0.5 + 0.25, pnx), py0 = bracket(fgy * 0.5 + 0.25, pny),
+                  pz0 = bracket(fgz * 0.5 + 0.25, pnz);
+        for (int a = -1; a <= 2; ++a)
+          for (int b2 = -1; b2 <= 2; ++b2)
+            for (int c2 = -1; c2 <= 2; ++c2) {
+              const int gx = px0 + a, gy = py0 + b2, gz = pz0 + c2;
+              if (gx < 1 || gy < 1 || gz < 1) continue;
+              const int bx = (gx - 1) / 8 + 1, by = (gy - 1) / 8 + 1, bz = (gz - 1) / 8 + 1;
+              if (bx > pa.dim[0] || by > pa.dim[1] || bz > pa.dim[2]) continue;
+              const int32_t pb = pptr[(size_t)(bx - 1) + (size_t)pa.dim[0] * ((by - 1) + (size_t)pa.dim[1] * (bz - 1))];
+              if (pb <= 0) continue;
+              const int32_t cid = (pb - 1) * 512 + (((gx - 1) % 8) | (((gy - 1) % 8) << 3) | (((gz - 1) % 8) << 6));
+              if (map[(size_t)cid] < 0) { map[(size_t)cid] = (int32_t)nodes.size(); nodes.push_back(cid); }
+            }
+      };
+      // interpolation positions: every ghost cell that an in-domain pull reads (its slot in the
+      // ghost blocks), with the record of each of its 64 stencil nodes
+      std::vector<int32_t> slot_pos((size_t)std::max(g->n_ghost, 1) * 512, -1);
+      std::vector<int4> pos_xyz;
+      for (const uint2& en : g->h_gentries) {
+        const int4 bi = g->h_binfo[en.x];
+        const int cell = (int)(en.y & 511u), k = (int)((en.y >> 9) & 31u);
+        const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
+        const int gx = (bi.x - 1) * 8 + x + 1, gy = (bi.y - 1) * 8 + y + 1, gz = (bi.z - 1) * 8 + z + 1;
+        const int sx = gx - q27_cx(k), sy = gy - q27_cy(k), sz = gz - q27_cz(k);
+        const bool in_x = sx >= 1 && sx <= g->nx, in_y = sy >= 1 && sy <= g->ny, in_z = sz >= 1 && sz <= g->nz;
+        if (in_x && in_y && in_z) {
+          add_stencil(sx, sy, sz);
+          const int lx = x - q27_cx(k), ly = y - q27_cy(k), lz = z - q27_cz(k);
+          const int ox = lx < 0 ? -1 : (lx > 7 ? 1 : 0), oy = ly < 0 ? -1 : (ly > 7 ? 1 : 0),
+                    oz = lz < 0 ? -1 : (lz > 7 ? 1 : 0);
+          const int32_t gb = g->h_nbrg[(size_t)en.x * 27 + nbr_dir(ox, oy, oz)];
+          if (gb >= g->nb && gb < g->nb + g->n_ghost) {
+            const size_t slot = (size_t)(gb - g->nb) * 512 + ((lx & 7) | ((ly & 7) << 3) | ((lz & 7) << 6));
+            if (slot_pos[slot] < 0) { slot_pos[slot] = (int32_t)pos_xyz.size(); pos_xyz.push_back(make_int4(sx, sy, sz, 0)); }
+          }
+        } else if (in_x && in_y && !in_z) {
+          add_stencil(sx, sy, gz);
+        }
+      }
+      std::vector<int32_t> pos_nodes(pos_xyz.size() * 64, -1);
+      for (size_t i = 0; i < pos_xyz.size(); ++i) {
+        const int px0 = bracket(pos_xyz[i].x * 0.5 + 0.25, pnx), py0 = bracket(pos_xyz[i].y * 0.5 + 0.25, pny),
+                  pz0 = bracket(pos_xyz[i].z * 0.5 + 0.25, pnz);
+        for (int a = -1; a <= 2; ++a)
+          for (int b2 = -1; b2 <= 2; ++b2)
+            for (int c2 = -1; c2 <= 2; ++c2) {
+              const int gx = px0 + a, gy = py0 + b2, gz = pz0 + c2;
+              if (gx < 1 || gy < 1 || gz < 1) continue;
+              const int bx = (gx - 1) / 8 + 1, by = (gy - 1) / 8 + 1, bz = (gz - 1) / 8 + 1;
+              if (bx > pa.dim[0] || by > pa.dim[1] || bz > pa.dim[2]) continue;
+              const int32_t pb = pptr[(size_t)(bx - 1) + (size_t)pa.dim[0] * ((by - 1) + (size_t)pa.dim[1] * (bz - 1))];
+              if (pb <= 0) continue;
+              const int32_t cid = (pb - 1) * 512 + (((gx - 1) % 8) | (((gy - 1) % 8) << 3) | (((gz - 1) % 8) << 6));
+              pos_nodes[i * 64 + (size_t)(16 * (a + 1) + 4 * (b2 + 1) + (c2 + 1))] = map[(size_t)cid];
+            }
+      }
+      me.n_nodes = (int32_t)nodes.size();
+      const size_t rb = A->storage == OAL_STORE_F64 ? 8 : 4;
+      e = cudaMalloc(&me.d_nodes, std::max<size_t>(nodes.size(), 1) * sizeof(int32_t));
+      if (e == cudaSuccess && !nodes.empty()) e = cudaMemcpy(me.d_nodes, nodes.data(), nodes.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+      if (e == cudaSuccess) e = cudaMalloc(&me.d_node_map, map.size() * sizeof(int32_t));
+      if (e == cudaSuccess) e = cudaMemcpy(me.d_node_map, map.data(), map.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+      if (e == cudaSuccess) e = cudaMalloc(&me.d_node_vals, std::max<size_t>(nodes.size(), 1) * 32 * rb);
+      me.n_pos = (int32_t)pos_xyz.size();
+      const size_t np1 = std::max<size_t>(pos_xyz.size(), 1);
+      if (e == cudaSuccess) e = cudaMalloc(&me.d_pos_xyz, np1 * sizeof(int4));
+      if (e == cudaSuccess) e = cudaMalloc(&me.d_slot_pos, slot_pos.size() * sizeof(int32_t));
+      if (e == cudaSuccess) e = cudaMalloc(&me.d_pos_nodes, np1 * 64 * sizeof(int32_t));
+      if (e == cudaSuccess) e = cudaMalloc(&me.d_pos_macro, np1 * 4 * rb);
+      if (e == cudaSuccess && me.n_pos > 0) {
+        e = cudaMemcpy(me.d_pos_xyz, pos_xyz.data(), pos_xyz.size() * sizeof(int4), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(me.d_pos_nodes, pos_nodes.data(), pos_nodes.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+      }
+      if (e == cudaSuccess) e = cudaMemcpy(me.d_slot_pos, slot_pos.data(), slot_pos.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
     }
     if (e != cudaSuccess) {
       cudaGetLastError();
