@@ -219,7 +219,7 @@ def benchmark_amr(steps: int = 50, warmup: int = 5, storage: str = "f16", nx: in
             "fine_cells": cells[1], "work_per_coarse_step": work, "steps": steps, "ms_per_coarse_step": round(ms, 4),
             "mlups": round(work / ms / 1e3, 1), "bytes_per_update": bpc,
             "achieved_gbs": round(work * bpc / ms / 1e6, 1), "finite": ok,
-            "gpu_launches_per_coarse_step": "level 0: ghost fill, fast, general; level 1 (x2): the same; restriction; 3 snapshot copies"}
+            "gpu_launches_per_coarse_step": "level 0: ghost fill, fast, general; level 1 (x2): parent nodes, interpolation positions, ghost fill, fast, general; restriction; 3 snapshot copies"}
 
 
 def main():
