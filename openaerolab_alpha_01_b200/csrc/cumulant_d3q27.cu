@@ -504,7 +504,7 @@ __device__ __noinline__ R parent_population(const ParentView& P, int fgx, int fg
 // Population arriving at cell (x,y,z) of block b in direction k from outside every block
 // (kernel_cumulant.jl:221-391), level without parent. `nbr` is the block's 27-entry row; entries
 // >= n_real are ghost blocks, which count as missing here. k may be a run-time value.
-template <class S, class R, bool DENSE = false>
+template <class S, class R, bool DENSE = false, bool PAR = false>
 __device__ __forceinline__ R face_population_impl(const S* __restrict__ fin, int64_t bbase, int cell, int64_t kst,
                                                   const int32_t* nbr, int n_real, int64_t bst, int k, int x, int y,
                                                   int z, int gx, int gy, int gz, const CaseParams& cp,
@@ -548,7 +548,7 @@ __device__ __forceinline__ R face_population_impl(const S* __restrict__ fin, int
           const int zw_nb = nbr[nbr_dir(zw_ix >> 3, zw_iy >> 3, 0)];
           if (zw_nb >= 0 && zw_nb < n_real) {
             src = (int64_t)zw_nb * bst + j * kst + ((zw_ix & 7) + 8 * (zw_iy & 7) + 64 * z);
-          } else if (da && da->par.ptr && src_gy >= 1 && src_gy <= cp.ny) {
+          } else if (PAR && da && da->par.ptr && src_gy >= 1 && src_gy <= cp.ny) {
             // refined level: the image cell comes from the parent (kernel_cumulant.jl:286-312)
             return parent_population<S, R>(da->par, src_gx, src_gy, gz, j, R(cx), R(cy), R(-cz), comp);
           }
@@ -564,7 +564,7 @@ __device__ __forceinline__ R face_population_impl(const S* __restrict__ fin, int
     j = q27_mir_y(k);
   } else if (is_z_min || is_z_max) {
     j = q27_mir_z(k);
-  } else if (da && da->par.ptr) {
+  } else if (PAR && da && da->par.ptr) {
     // refined level: interpolated from the parent (kernel_cumulant.jl:346-388); the source is a
     // ghost cell whose interpolation position may be precomputed
     if (da->par.slot_pos && !DENSE) {
@@ -602,7 +602,9 @@ __device__ __forceinline__ const CaseParams& case_of(const StepArgs& a, int case
 // ------------------------------------------------------------------------------------------------
 // ghost fill: one thread per (destination cell, direction) whose pull source is a ghost cell
 // ------------------------------------------------------------------------------------------------
-template <class S, class R, bool DENSE>
+// PAR: the level has a parent (its ghost pulls from inside the domain interpolate from it); the
+// plain instance carries none of that code and stays small
+template <class S, class R, bool DENSE, bool PAR>
 __global__ void __launch_bounds__(256) k_fill_ghosts(const StepArgs a, const uint2* __restrict__ entries, int64_t n) {
   const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (e >= n) return;
@@ -630,10 +632,10 @@ __global__ void __launch_bounds__(256) k_fill_ghosts(const StepArgs a, const uin
       return;
     }
     const int64_t own = dense_idx(a, gx + 7, gy, gz);
-    const R val = face_population_impl<S, R, true>(f, own, 0, kst, nbr, a.n_blocks, bst, k, x, y, z, gx, gy, gz, cp, &a);
+    const R val = face_population_impl<S, R, true, PAR>(f, own, 0, kst, nbr, a.n_blocks, bst, k, x, y, z, gx, gy, gz, cp, &a);
     f[slot] = Codec<S>::enc(val, R(q27_w(k)), R(1.0 / q27_w(k)));
   } else {
-    const R val = face_population_impl<S, R>(f, (int64_t)b * bst, cell, kst, nbr, a.n_blocks, bst, k, x, y, z, gx, gy,
+    const R val = face_population_impl<S, R, false, PAR>(f, (int64_t)b * bst, cell, kst, nbr, a.n_blocks, bst, k, x, y, z, gx, gy,
                                              gz, cp, &a);
     const int sx = x - cx, sy = y - cy, sz = z - cz;
     const int g = nbr[nbr_dir(sx >> 3, sy >> 3, sz >> 3)];
@@ -792,6 +794,203 @@ __global__ void __launch_bounds__(128, OAL_FAST_MIN_CTAS) k_cumulant_fast(const 
     if constexpr (NL == 2) store2<S>(fout, o[0], o[1], A[k], k);
     else fout[o[0]] = Codec<S>::enc(A[k], T(q27_w(k)), T(1.0 / q27_w(k)));
   }
+}
+
+// ------------------------------------------------------------------------------------------------
+// x-pair kernel: the uniform step with two x-adjacent cells (2i, 2i+1) per thread in packed f32x2
+// ------------------------------------------------------------------------------------------------
+// A direction's two stored values of a pair are one aligned word (2 x 16 bit or 2 x 32 bit), so
+// the pull reads one word where the source pair is aligned (c_x = 0) and two words plus a lane
+// shuffle within the register where it is not (c_x = +-1); the store writes one word. The WALE
+// stencil reads pairs of the previous velocity. Same collision and the same per-cell results as
+// the one-cell-per-lane kernels up to the rounding of the density and momentum sums, which are
+// taken from the velocity-free x sums of the chimera transform.
+template <class S> struct PairWord { using W = uint32_t; };
+template <> struct PairWord<float> { using W = uint2; };
+
+// (high element of q, low element of p): the pair straddling two aligned pairs
+__device__ __forceinline__ uint32_t pair_mid(uint32_t q, uint32_t p) { return __byte_perm(q, p, 0x5432); }
+__device__ __forceinline__ uint2 pair_mid(uint2 q, uint2 p) { return make_uint2(q.y, p.x); }
+
+// the stored word of a direction -> the two values as stored (deviations d for 16-bit codecs)
+template <class S> __device__ __forceinline__ F2 pair_raw(uint32_t w);
+template <> __device__ __forceinline__ F2 pair_raw<__half>(uint32_t w) {
+  const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w));
+  return f2(f.x, f.y);
+}
+template <> __device__ __forceinline__ F2 pair_raw<__nv_bfloat16>(uint32_t w) {
+  const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w));
+  return f2(f.x, f.y);
+}
+__device__ __forceinline__ F2 pair_raw_f32(uint2 w) { return f2(__uint_as_float(w.x), __uint_as_float(w.y)); }
+
+// populations of direction k -> the stored word (encode d = f / w - 1 for 16-bit codecs)
+template <class S> __device__ __forceinline__ typename PairWord<S>::W pair_word(F2 v, int k);
+template <> __device__ __forceinline__ uint32_t pair_word<__half>(F2 v, int k) {
+  float a, b;
+  f2split(vfma(v, splat<F2>(float(1.0 / q27_w(k))), splat<F2>(-1.0f)), a, b);
+  const __half2 h = __floats2half2_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+template <> __device__ __forceinline__ uint32_t pair_word<__nv_bfloat16>(F2 v, int k) {
+  float a, b;
+  f2split(vfma(v, splat<F2>(float(1.0 / q27_w(k))), splat<F2>(-1.0f)), a, b);
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+template <> __device__ __forceinline__ uint2 pair_word<float>(F2 v, int) {
+  float a, b;
+  f2split(v, a, b);
+  return make_uint2(__float_as_uint(a), __float_as_uint(b));
+}
+
+// Library-owned block-major layout; IDX indexes words (pairs): block stride 27*256, direction
+// stride 256, row (y, z) stride 4 and 32.
+template <class S, class IDX>
+__global__ void __launch_bounds__(128, OAL_FAST_MIN_CTAS) k_cumulant_pairs(const StepArgs a, const int32_t* __restrict__ work) {
+  using W = typename PairWord<S>::W;
+  using V = F2;
+  using T = float;
+  constexpr IDX wbst = 27 * kCells / 2, wkst = kCells / 2;
+  __shared__ IDX s_wbase[28];  // first word of each neighbour block
+  __shared__ int32_t s_nbr[28];
+  __shared__ CaseParams s_cp;
+  const int tid = threadIdx.x;
+  const int b = work[blockIdx.x >> 1];
+  const int part = blockIdx.x & 1;
+  if (tid < 27) {
+    const int32_t nb = a.nbr[(int64_t)b * 27 + tid];
+    s_nbr[tid] = nb;
+    s_wbase[tid] = (IDX)nb * wbst;
+  }
+  if (tid >= 32 && tid < 32 + (int)(sizeof(CaseParams) / 4)) {
+    const int case_id = a.cases ? a.binfo[b].w : 0;
+    reinterpret_cast<uint32_t*>(&s_cp)[tid - 32] = reinterpret_cast<const uint32_t*>(&case_of(a, case_id))[tid - 32];
+  }
+  __syncthreads();
+  const CaseParams& cp = s_cp;
+
+  const W* __restrict__ fin = static_cast<const W*>(a.f_in);
+  W* __restrict__ fout = static_cast<W*>(a.f_out);
+  float2* __restrict__ rho_out = static_cast<float2*>(a.rho_out);
+  float* __restrict__ vel_out = static_cast<float*>(a.vel_out);
+  const float* __restrict__ vel_in = static_cast<const float*>(a.vel_in);
+  const IDX vcs = (IDX)a.v_cstride;
+  const int n_real = a.n_blocks;
+
+  const int i = tid & 3, y = (tid >> 2) & 7, z = 4 * part + (tid >> 5);
+
+  // ---- pull (kernel_cumulant.jl:190-220): every source lies in a real or ghost block ----
+  V A[kQ27];
+#pragma unroll
+  for (int n = 0; n < 9; ++n) {
+    // the three directions of one (c_y, c_z): their source rows share the neighbour block
+    const int cy = n % 3 - 1, cz = n / 3 - 1;
+    const int sy = y - cy, sz = z - cz;
+    const int dyz = 3 * ((sy >> 3) + 1) + 9 * ((sz >> 3) + 1);
+    const IDX row = (IDX)(((sy & 7) << 2) | ((sz & 7) << 5));
+    const IDX own = s_wbase[1 + dyz] + row + (IDX)i;
+    // the outer word of the row for the edge pairs: -x block's last pair (i = 0), +x block's first (i = 3)
+    const IDX outer = i == 0 ? s_wbase[dyz] + row + 3 : s_wbase[2 + dyz] + row;
+    const IDX left = i == 0 ? outer : own - 1, right = i == 3 ? outer : own + 1;
+    const int k_m = 3 * n, k_0 = 3 * n + 1, k_p = 3 * n + 2;  // c_x = -1, 0, +1
+    // c_x = -1: source x + 1 = (hi of own pair, lo of the right pair)
+    const W pm = fin[own + (IDX)(k_m * wkst)], rm = fin[right + (IDX)(k_m * wkst)];
+    const W p0 = fin[own + (IDX)(k_0 * wkst)];
+    // c_x = +1: source x - 1 = (hi of the left pair, lo of own pair)
+    const W pp = fin[own + (IDX)(k_p * wkst)], lp = fin[left + (IDX)(k_p * wkst)];
+    if constexpr (std::is_same<S, float>::value) {
+      A[k_m] = pair_raw_f32(pair_mid(pm, rm));
+      A[k_0] = pair_raw_f32(p0);
+      A[k_p] = pair_raw_f32(pair_mid(lp, pp));
+    } else {
+      // deviations; the decode f = w (1 + d) is folded into the x sums below
+      A[k_m] = pair_raw<S>(pair_mid(pm, rm));
+      A[k_0] = pair_raw<S>(p0);
+      A[k_p] = pair_raw<S>(pair_mid(lp, pp));
+    }
+  }
+  // velocity-free x sums of the chimera transform: m0 = a + b + c, m1 = c - a, m2 = a + c
+#pragma unroll
+  for (int n = 0; n < 9; ++n) {
+    V& a0 = A[3 * n];
+    V& b0 = A[3 * n + 1];
+    V& c0 = A[3 * n + 2];
+    if constexpr (std::is_same<S, float>::value) {
+      chimera_xsums(a0, b0, c0);
+    } else {
+      // a = wa (1 + da), b = wb (1 + db), c = wa (1 + dc)
+      const float wa = float(q27_w(3 * n)), wb = float(q27_w(3 * n + 1));
+      const V m2 = vfma(splat<V>(wa), a0 + c0, splat<V>(2.0f * wa));
+      const V m1 = splat<V>(wa) * (c0 - a0);
+      a0 = vfma(splat<V>(wb), b0, m2 + splat<V>(wb));
+      b0 = m1;
+      c0 = m2;
+    }
+  }
+  // density and momentum from the x sums (triplet n has c_y = n % 3 - 1, c_z = n / 3 - 1)
+  const V r0 = (A[0] + A[3]) + A[6], r1 = (A[9] + A[12]) + A[15], r2 = (A[18] + A[21]) + A[24];
+  const V ym = (A[0] + A[9]) + A[18], yp = (A[6] + A[15]) + A[24];
+  V rho = (r0 + r1) + r2;
+  const V jx = (((A[1] + A[4]) + (A[7] + A[10])) + ((A[13] + A[16]) + (A[19] + A[22]))) + A[25];
+  const V jy = yp - ym, jz = r2 - r0;
+
+  // ---- macros (kernel_cumulant.jl:424-431) ----
+  rho = vmaxc(rho, T(0.01));
+  const V inv_rho = vrcp(rho);
+  const V ux = jx * inv_rho, uy = jy * inv_rho, uz = jz * inv_rho;
+  const IDX cown = (IDX)b * kCells + (IDX)(2 * i + 8 * y + 64 * z);  // cell id of the pair's first cell
+  {
+    float r_0, r_1, a0, a1;
+    f2split(rho, r_0, r_1);
+    rho_out[cown >> 1] = make_float2(r_0, r_1);
+    f2split(ux, a0, a1); reinterpret_cast<float2*>(vel_out + cown)[0] = make_float2(a0, a1);
+    f2split(uy, a0, a1); reinterpret_cast<float2*>(vel_out + cown + vcs)[0] = make_float2(a0, a1);
+    f2split(uz, a0, a1); reinterpret_cast<float2*>(vel_out + cown + 2 * vcs)[0] = make_float2(a0, a1);
+  }
+
+  // ---- WALE from the previous step's velocity (kernel_cumulant.jl:496-549) ----
+  V nu_eddy = splat<V>(T(0));
+  if (cp.flags & CF_GRADIENTS) {
+    // a neighbour in a ghost block contributes the own cell's value (physics_utils.jl:2031-2034)
+    const int nb_xm = s_nbr[nbr_dir(-1, 0, 0)], nb_xp = s_nbr[nbr_dir(1, 0, 0)];
+    const int nb_y = s_nbr[nbr_dir(0, y == 0 ? -1 : 0, 0)], nb_Y = s_nbr[nbr_dir(0, y == 7 ? 1 : 0, 0)];
+    const int nb_z = s_nbr[nbr_dir(0, 0, z == 0 ? -1 : 0)], nb_Z = s_nbr[nbr_dir(0, 0, z == 7 ? 1 : 0)];
+    const bool ok_xm = i > 0 || (unsigned)nb_xm < (unsigned)n_real;
+    const bool ok_xp = i < 3 || (unsigned)nb_xp < (unsigned)n_real;
+    const bool ok_ym = (unsigned)nb_y < (unsigned)n_real, ok_yp = (unsigned)nb_Y < (unsigned)n_real;
+    const bool ok_zm = (unsigned)nb_z < (unsigned)n_real, ok_zp = (unsigned)nb_Z < (unsigned)n_real;
+    const IDX c_xm = i > 0 ? cown - 1 : (IDX)nb_xm * kCells + (IDX)(7 + 8 * y + 64 * z);
+    const IDX c_xp = i < 3 ? cown + 2 : (IDX)nb_xp * kCells + (IDX)(8 * y + 64 * z);
+    const IDX c_ym = (IDX)nb_y * kCells + (IDX)(2 * i + 8 * ((y + 7) & 7) + 64 * z);
+    const IDX c_yp = (IDX)nb_Y * kCells + (IDX)(2 * i + 8 * ((y + 1) & 7) + 64 * z);
+    const IDX c_zm = (IDX)nb_z * kCells + (IDX)(2 * i + 8 * y + 64 * ((z + 7) & 7));
+    const IDX c_zp = (IDX)nb_Z * kCells + (IDX)(2 * i + 8 * y + 64 * ((z + 1) & 7));
+    V g[3][3];
+    const V h = splat<V>(T(0.5));
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float* vc = vel_in + (IDX)c * vcs;
+      const float2 o = reinterpret_cast<const float2*>(vc + cown)[0];
+      const float xm = ok_xm ? vc[c_xm] : o.x, xp = ok_xp ? vc[c_xp] : o.y;
+      const float2 ym2 = ok_ym ? reinterpret_cast<const float2*>(vc + c_ym)[0] : o;
+      const float2 yp2 = ok_yp ? reinterpret_cast<const float2*>(vc + c_yp)[0] : o;
+      const float2 zm2 = ok_zm ? reinterpret_cast<const float2*>(vc + c_zm)[0] : o;
+      const float2 zp2 = ok_zp ? reinterpret_cast<const float2*>(vc + c_zp)[0] : o;
+      g[c][0] = h * (f2(o.y, xp) - f2(xm, o.x));
+      g[c][1] = h * (f2(yp2.x, yp2.y) - f2(ym2.x, ym2.y));
+      g[c][2] = h * (f2(zp2.x, zp2.y) - f2(zm2.x, zm2.y));
+    }
+    nu_eddy = wale_nu<V>(g[0][0], g[0][1], g[0][2], g[1][0], g[1][1], g[1][2], g[2][0], g[2][1], g[2][2], cp.c_wale);
+  }
+  const V omega1 = omega1_from<V>(nu_eddy, cp);
+
+  cumulant_collide_xsums<V>(A, rho, ux, uy, uz, omega1, cp);
+
+  // ---- store (kernel_cumulant.jl:889-908 with zero force) ----
+  W* __restrict__ o = fout + (IDX)b * wbst + (IDX)(i + 4 * y + 32 * z);
+#pragma unroll
+  for (int k = 0; k < kQ27; ++k) o[k * wkst] = pair_word<S>(A[k], k);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -1167,8 +1366,14 @@ cudaError_t launch_restrict(const RestrictArgs& r, cudaStream_t st) {
 template <class S, class R>
 cudaError_t launch_fill_ghosts(const StepArgs& a, const uint2* entries, int64_t n, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  if (a.dense) k_fill_ghosts<S, R, true><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, entries, n);
-  else k_fill_ghosts<S, R, false><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(a, entries, n);
+  const unsigned grid = (unsigned)((n + 255) / 256);
+  if (a.par.ptr) {
+    if (a.dense) k_fill_ghosts<S, R, true, true><<<grid, 256, 0, st>>>(a, entries, n);
+    else k_fill_ghosts<S, R, false, true><<<grid, 256, 0, st>>>(a, entries, n);
+  } else {
+    if (a.dense) k_fill_ghosts<S, R, true, false><<<grid, 256, 0, st>>>(a, entries, n);
+    else k_fill_ghosts<S, R, false, false><<<grid, 256, 0, st>>>(a, entries, n);
+  }
   return cudaGetLastError();
 }
 
@@ -1183,9 +1388,13 @@ cudaError_t launch_fast(const StepArgs& a, const int32_t* work, int n_work, cuda
   } else if constexpr (OAL_FAST_CELLS == 1) {
     if (idx32) k_cumulant_fast<S, float, uint32_t><<<(unsigned)n_work * 4u, 128, 0, st>>>(a, work);
     else k_cumulant_fast<S, float, int64_t><<<(unsigned)n_work * 4u, 128, 0, st>>>(a, work);
-  } else {
+  } else if constexpr (OAL_FAST_CELLS == 3) {
     if (idx32) k_cumulant_fast<S, F2, uint32_t><<<(unsigned)n_work * 2u, 128, 0, st>>>(a, work);
     else k_cumulant_fast<S, F2, int64_t><<<(unsigned)n_work * 2u, 128, 0, st>>>(a, work);
+  } else {
+    // x pairs; word indices (half the element count) decide the index width
+    if (idx32) k_cumulant_pairs<S, uint32_t><<<(unsigned)n_work * 2u, 128, 0, st>>>(a, work);
+    else k_cumulant_pairs<S, int64_t><<<(unsigned)n_work * 2u, 128, 0, st>>>(a, work);
   }
   return cudaGetLastError();
 }

@@ -107,10 +107,73 @@ __device__ __forceinline__ void chimera_bwd3(V& a, V& b, V& c, V u, V tu, V u2) 
   c = (m2 + m1) * h;
 }
 
+// the blend of the positivity limiter in the lanes whose minimum population fmin is negative:
+// f = f_eq + alpha (f - f_eq), alpha the largest factor keeping every population >= 0
+// (kernel_cumulant.jl:856-884)
+// opaque copy: the compiler may not assume the value equals its source, so expressions of it are
+// recomputed rather than kept alive from earlier
+__device__ __forceinline__ float opaque(float v) { asm volatile("" : "+f"(v)); return v; }
+__device__ __forceinline__ double opaque(double v) { asm volatile("" : "+d"(v)); return v; }
+__device__ __forceinline__ F2 opaque(F2 v) { asm volatile("" : "+l"(v.v)); return v; }
+
+#ifndef OAL_LIMITER_OUTLINE
+#define OAL_LIMITER_OUTLINE 0
+#endif
+#if OAL_LIMITER_OUTLINE
+#define OAL_LIMITER_LINKAGE __noinline__
+#else
+#define OAL_LIMITER_LINKAGE __forceinline__
+#endif
+
+template <class V>
+__device__ OAL_LIMITER_LINKAGE void positivity_blend(V (&A)[kQ27], V fmin, V rho, V uxe, V uye, V uze, bool comp) {
+  using T = SC<V>;
+  const V zero = splat<V>(T(0)), one = splat<V>(T(1));
+  V alpha = one;
+#pragma unroll
+  for (int k = 0; k < kQ27; ++k) {
+    const V fe = feq_k<V>(k, rho, uxe, uye, uze, comp);
+    const V fneq = A[k] - fe;
+    const V ak = fe * vrcp((fe - fneq) + splat<V>(T(1e-15)));
+    // alpha = min(alpha, ak) where fneq < 0 and fe > 1e-15
+    alpha = vsel_gt(zero, fneq, vsel_gt(fe, splat<V>(T(1e-15)), vmin(alpha, ak), alpha), alpha);
+  }
+  alpha = vmaxc(alpha, T(0));
+  // the equilibria again (not 27 values kept alive across the two loops)
+  rho = opaque(rho); uxe = opaque(uxe); uye = opaque(uye); uze = opaque(uze);
+#pragma unroll
+  for (int k = 0; k < kQ27; ++k) {
+    const V fe = feq_k<V>(k, rho, uxe, uye, uze, comp);
+    A[k] = vsel_gt(zero, fmin, vfma(alpha, A[k] - fe, fe), A[k]);
+  }
+}
+
+// velocity-free half of the forward x pass: (a, b, c) -> (a + b + c, c - a, a + c)
+template <class V>
+__device__ __forceinline__ void chimera_xsums(V& a, V& b, V& c) {
+  const V m0 = (a + b) + c, m1 = c - a, m2 = a + c;
+  a = m0;
+  b = m1;
+  c = m2;
+}
+
 // Cumulant relaxation of A (post-streaming populations) at the equilibrium velocity (uxe,uye,uze)
 // with omega_1 (kernel_cumulant.jl:597-844), then the positivity limiter (:849-884).
 template <class V>
+__device__ __forceinline__ void cumulant_collide_xsums(V (&A)[kQ27], V rho, V uxe, V uye, V uze, V omega1,
+                                                       const CaseParams& cp);
+template <class V>
 __device__ __forceinline__ void cumulant_collide(V (&A)[kQ27], V rho, V uxe, V uye, V uze, V omega1, const CaseParams& cp) {
+#pragma unroll
+  for (int n = 0; n < 9; ++n) chimera_xsums(A[3 * n], A[3 * n + 1], A[3 * n + 2]);
+  cumulant_collide_xsums<V>(A, rho, uxe, uye, uze, omega1, cp);
+}
+
+// The same with the x triplets of A already replaced by their velocity-free sums (chimera_xsums);
+// the x pass then only shifts them to the velocity: b = m1 - u m0, c = m2 - 2u m1 + u^2 m0
+template <class V>
+__device__ __forceinline__ void cumulant_collide_xsums(V (&A)[kQ27], V rho, V uxe, V uye, V uze, V omega1,
+                                                       const CaseParams& cp) {
   using T = SC<V>;
   const uint32_t flags = cp.flags;
   const V one = splat<V>(T(1)), two = splat<V>(T(2)), four = splat<V>(T(4)), third = splat<V>(T(1.0 / 3.0));
@@ -124,11 +187,15 @@ __device__ __forceinline__ void cumulant_collide(V (&A)[kQ27], V rho, V uxe, V u
     omega4_diag = vclamp(Av, splat<V>(T(0.01)), splat<V>(T(2)));
   }
 
-  // chimera forward x, y, z (kernel_cumulant.jl:612-656)
+  // chimera forward x (its velocity shift), y, z (kernel_cumulant.jl:612-656)
   {
     const V nu = uxe * splat<V>(T(-1)), n2u = uxe * splat<V>(T(-2)), u2 = uxe * uxe;
 #pragma unroll
-    for (int n = 0; n < 9; ++n) chimera_fwd3(A[3 * n], A[3 * n + 1], A[3 * n + 2], nu, n2u, u2);
+    for (int n = 0; n < 9; ++n) {
+      const V m0 = A[3 * n], m1 = A[3 * n + 1], m2 = A[3 * n + 2];
+      A[3 * n + 1] = vfma(nu, m0, m1);
+      A[3 * n + 2] = vfma(u2, m0, vfma(n2u, m1, m2));
+    }
   }
   {
     const V nu = uye * splat<V>(T(-1)), n2u = uye * splat<V>(T(-2)), u2 = uye * uye;
@@ -239,24 +306,7 @@ __device__ __forceinline__ void cumulant_collide(V (&A)[kQ27], V rho, V uxe, V u
     V fmin = A[0];
 #pragma unroll
     for (int k = 1; k < kQ27; ++k) fmin = vmin(fmin, A[k]);
-    if (vany_gt(zero, fmin)) {
-      const bool comp = (flags & CF_COMPRESSIBLE) != 0;
-      V alpha = one;
-#pragma unroll
-      for (int k = 0; k < kQ27; ++k) {
-        const V fe = feq_k<V>(k, rho, uxe, uye, uze, comp);
-        const V fneq = A[k] - fe;
-        const V ak = fe * vrcp((fe - fneq) + splat<V>(T(1e-15)));
-        // alpha = min(alpha, ak) where fneq < 0 and fe > 1e-15
-        alpha = vsel_gt(zero, fneq, vsel_gt(fe, splat<V>(T(1e-15)), vmin(alpha, ak), alpha), alpha);
-      }
-      alpha = vmaxc(alpha, T(0));
-#pragma unroll
-      for (int k = 0; k < kQ27; ++k) {
-        const V fe = feq_k<V>(k, rho, uxe, uye, uze, comp);
-        A[k] = vsel_gt(zero, fmin, vfma(alpha, A[k] - fe, fe), A[k]);
-      }
-    }
+    if (vany_gt(zero, fmin)) positivity_blend<V>(A, fmin, rho, uxe, uye, uze, (flags & CF_COMPRESSIBLE) != 0);
   }
 }
 
