@@ -846,7 +846,8 @@ template <> __device__ __forceinline__ uint2 pair_word<float>(F2 v, int) {
 
 // Library-owned block-major layout; IDX indexes words (pairs): block stride 27*256, direction
 // stride 256, row (y, z) stride 4 and 32.
-template <class S, class IDX>
+// POS: some case of the launch uses the positivity limiter (its code is left out otherwise).
+template <class S, class IDX, bool POS>
 __global__ void __launch_bounds__(128, OAL_FAST_MIN_CTAS) k_cumulant_pairs(const StepArgs a, const int32_t* __restrict__ work) {
   using W = typename PairWord<S>::W;
   using V = F2;
@@ -880,6 +881,40 @@ __global__ void __launch_bounds__(128, OAL_FAST_MIN_CTAS) k_cumulant_pairs(const
 
   const int i = tid & 3, y = (tid >> 2) & 7, z = 4 * part + (tid >> 5);
 
+  // ---- WALE stencil of the previous step's velocity (kernel_cumulant.jl:496-549): its loads
+  // are issued before the pull so that both round trips to memory overlap ----
+  const bool grad = (cp.flags & CF_GRADIENTS) != 0;
+  const IDX cown = (IDX)b * kCells + (IDX)(2 * i + 8 * y + 64 * z);  // cell id of the pair's first cell
+  float2 vo[3], vym[3], vyp[3], vzm[3], vzp[3];
+  float vxm[3], vxp[3];
+  if (grad) {
+    // a neighbour in a ghost block contributes the own cell's value (physics_utils.jl:2031-2034)
+    const int nb_xm = s_nbr[nbr_dir(-1, 0, 0)], nb_xp = s_nbr[nbr_dir(1, 0, 0)];
+    const int nb_y = s_nbr[nbr_dir(0, y == 0 ? -1 : 0, 0)], nb_Y = s_nbr[nbr_dir(0, y == 7 ? 1 : 0, 0)];
+    const int nb_z = s_nbr[nbr_dir(0, 0, z == 0 ? -1 : 0)], nb_Z = s_nbr[nbr_dir(0, 0, z == 7 ? 1 : 0)];
+    const bool ok_xm = i > 0 || (unsigned)nb_xm < (unsigned)n_real;
+    const bool ok_xp = i < 3 || (unsigned)nb_xp < (unsigned)n_real;
+    const bool ok_ym = (unsigned)nb_y < (unsigned)n_real, ok_yp = (unsigned)nb_Y < (unsigned)n_real;
+    const bool ok_zm = (unsigned)nb_z < (unsigned)n_real, ok_zp = (unsigned)nb_Z < (unsigned)n_real;
+    const IDX c_xm = i > 0 ? cown - 1 : (IDX)nb_xm * kCells + (IDX)(7 + 8 * y + 64 * z);
+    const IDX c_xp = i < 3 ? cown + 2 : (IDX)nb_xp * kCells + (IDX)(8 * y + 64 * z);
+    const IDX c_ym = (IDX)nb_y * kCells + (IDX)(2 * i + 8 * ((y + 7) & 7) + 64 * z);
+    const IDX c_yp = (IDX)nb_Y * kCells + (IDX)(2 * i + 8 * ((y + 1) & 7) + 64 * z);
+    const IDX c_zm = (IDX)nb_z * kCells + (IDX)(2 * i + 8 * y + 64 * ((z + 7) & 7));
+    const IDX c_zp = (IDX)nb_Z * kCells + (IDX)(2 * i + 8 * y + 64 * ((z + 1) & 7));
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float* vc = vel_in + (IDX)c * vcs;
+      vo[c] = reinterpret_cast<const float2*>(vc + cown)[0];
+      vxm[c] = ok_xm ? vc[c_xm] : vo[c].x;
+      vxp[c] = ok_xp ? vc[c_xp] : vo[c].y;
+      vym[c] = ok_ym ? reinterpret_cast<const float2*>(vc + c_ym)[0] : vo[c];
+      vyp[c] = ok_yp ? reinterpret_cast<const float2*>(vc + c_yp)[0] : vo[c];
+      vzm[c] = ok_zm ? reinterpret_cast<const float2*>(vc + c_zm)[0] : vo[c];
+      vzp[c] = ok_zp ? reinterpret_cast<const float2*>(vc + c_zp)[0] : vo[c];
+    }
+  }
+
   // ---- pull (kernel_cumulant.jl:190-220): every source lies in a real or ghost block ----
   V A[kQ27];
 #pragma unroll
@@ -910,6 +945,20 @@ __global__ void __launch_bounds__(128, OAL_FAST_MIN_CTAS) k_cumulant_pairs(const
       A[k_p] = pair_raw<S>(pair_mid(lp, pp));
     }
   }
+  // WALE eddy viscosity from the stencil
+  V nu_eddy = splat<V>(T(0));
+  if (grad) {
+    V g[3][3];
+    const V h = splat<V>(T(0.5));
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      g[c][0] = h * (f2(vo[c].y, vxp[c]) - f2(vxm[c], vo[c].x));
+      g[c][1] = h * (f2(vyp[c].x, vyp[c].y) - f2(vym[c].x, vym[c].y));
+      g[c][2] = h * (f2(vzp[c].x, vzp[c].y) - f2(vzm[c].x, vzm[c].y));
+    }
+    nu_eddy = wale_nu<V>(g[0][0], g[0][1], g[0][2], g[1][0], g[1][1], g[1][2], g[2][0], g[2][1], g[2][2], cp.c_wale);
+  }
+
   // velocity-free x sums of the chimera transform: m0 = a + b + c, m1 = c - a, m2 = a + c
 #pragma unroll
   for (int n = 0; n < 9; ++n) {
@@ -939,7 +988,6 @@ __global__ void __launch_bounds__(128, OAL_FAST_MIN_CTAS) k_cumulant_pairs(const
   rho = vmaxc(rho, T(0.01));
   const V inv_rho = vrcp(rho);
   const V ux = jx * inv_rho, uy = jy * inv_rho, uz = jz * inv_rho;
-  const IDX cown = (IDX)b * kCells + (IDX)(2 * i + 8 * y + 64 * z);  // cell id of the pair's first cell
   {
     float r_0, r_1, a0, a1;
     f2split(rho, r_0, r_1);
@@ -949,43 +997,9 @@ __global__ void __launch_bounds__(128, OAL_FAST_MIN_CTAS) k_cumulant_pairs(const
     f2split(uz, a0, a1); reinterpret_cast<float2*>(vel_out + cown + 2 * vcs)[0] = make_float2(a0, a1);
   }
 
-  // ---- WALE from the previous step's velocity (kernel_cumulant.jl:496-549) ----
-  V nu_eddy = splat<V>(T(0));
-  if (cp.flags & CF_GRADIENTS) {
-    // a neighbour in a ghost block contributes the own cell's value (physics_utils.jl:2031-2034)
-    const int nb_xm = s_nbr[nbr_dir(-1, 0, 0)], nb_xp = s_nbr[nbr_dir(1, 0, 0)];
-    const int nb_y = s_nbr[nbr_dir(0, y == 0 ? -1 : 0, 0)], nb_Y = s_nbr[nbr_dir(0, y == 7 ? 1 : 0, 0)];
-    const int nb_z = s_nbr[nbr_dir(0, 0, z == 0 ? -1 : 0)], nb_Z = s_nbr[nbr_dir(0, 0, z == 7 ? 1 : 0)];
-    const bool ok_xm = i > 0 || (unsigned)nb_xm < (unsigned)n_real;
-    const bool ok_xp = i < 3 || (unsigned)nb_xp < (unsigned)n_real;
-    const bool ok_ym = (unsigned)nb_y < (unsigned)n_real, ok_yp = (unsigned)nb_Y < (unsigned)n_real;
-    const bool ok_zm = (unsigned)nb_z < (unsigned)n_real, ok_zp = (unsigned)nb_Z < (unsigned)n_real;
-    const IDX c_xm = i > 0 ? cown - 1 : (IDX)nb_xm * kCells + (IDX)(7 + 8 * y + 64 * z);
-    const IDX c_xp = i < 3 ? cown + 2 : (IDX)nb_xp * kCells + (IDX)(8 * y + 64 * z);
-    const IDX c_ym = (IDX)nb_y * kCells + (IDX)(2 * i + 8 * ((y + 7) & 7) + 64 * z);
-    const IDX c_yp = (IDX)nb_Y * kCells + (IDX)(2 * i + 8 * ((y + 1) & 7) + 64 * z);
-    const IDX c_zm = (IDX)nb_z * kCells + (IDX)(2 * i + 8 * y + 64 * ((z + 7) & 7));
-    const IDX c_zp = (IDX)nb_Z * kCells + (IDX)(2 * i + 8 * y + 64 * ((z + 1) & 7));
-    V g[3][3];
-    const V h = splat<V>(T(0.5));
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const float* vc = vel_in + (IDX)c * vcs;
-      const float2 o = reinterpret_cast<const float2*>(vc + cown)[0];
-      const float xm = ok_xm ? vc[c_xm] : o.x, xp = ok_xp ? vc[c_xp] : o.y;
-      const float2 ym2 = ok_ym ? reinterpret_cast<const float2*>(vc + c_ym)[0] : o;
-      const float2 yp2 = ok_yp ? reinterpret_cast<const float2*>(vc + c_yp)[0] : o;
-      const float2 zm2 = ok_zm ? reinterpret_cast<const float2*>(vc + c_zm)[0] : o;
-      const float2 zp2 = ok_zp ? reinterpret_cast<const float2*>(vc + c_zp)[0] : o;
-      g[c][0] = h * (f2(o.y, xp) - f2(xm, o.x));
-      g[c][1] = h * (f2(yp2.x, yp2.y) - f2(ym2.x, ym2.y));
-      g[c][2] = h * (f2(zp2.x, zp2.y) - f2(zm2.x, zm2.y));
-    }
-    nu_eddy = wale_nu<V>(g[0][0], g[0][1], g[0][2], g[1][0], g[1][1], g[1][2], g[2][0], g[2][1], g[2][2], cp.c_wale);
-  }
   const V omega1 = omega1_from<V>(nu_eddy, cp);
 
-  cumulant_collide_xsums<V>(A, rho, ux, uy, uz, omega1, cp);
+  cumulant_collide_xsums<V, POS>(A, rho, ux, uy, uz, omega1, cp);
 
   // ---- store (kernel_cumulant.jl:889-908 with zero force) ----
   W* __restrict__ o = fout + (IDX)b * wbst + (IDX)(i + 4 * y + 32 * z);
@@ -1393,8 +1407,14 @@ cudaError_t launch_fast(const StepArgs& a, const int32_t* work, int n_work, cuda
     else k_cumulant_fast<S, F2, int64_t><<<(unsigned)n_work * 2u, 128, 0, st>>>(a, work);
   } else {
     // x pairs; word indices (half the element count) decide the index width
-    if (idx32) k_cumulant_pairs<S, uint32_t><<<(unsigned)n_work * 2u, 128, 0, st>>>(a, work);
-    else k_cumulant_pairs<S, int64_t><<<(unsigned)n_work * 2u, 128, 0, st>>>(a, work);
+    const unsigned grid = (unsigned)n_work * 2u;
+    if (a.flags_any & CF_LIMITER_POSITIVITY) {
+      if (idx32) k_cumulant_pairs<S, uint32_t, true><<<grid, 128, 0, st>>>(a, work);
+      else k_cumulant_pairs<S, int64_t, true><<<grid, 128, 0, st>>>(a, work);
+    } else {
+      if (idx32) k_cumulant_pairs<S, uint32_t, false><<<grid, 128, 0, st>>>(a, work);
+      else k_cumulant_pairs<S, int64_t, false><<<grid, 128, 0, st>>>(a, work);
+    }
   }
   return cudaGetLastError();
 }

@@ -159,7 +159,7 @@ __device__ __forceinline__ void chimera_xsums(V& a, V& b, V& c) {
 
 // Cumulant relaxation of A (post-streaming populations) at the equilibrium velocity (uxe,uye,uze)
 // with omega_1 (kernel_cumulant.jl:597-844), then the positivity limiter (:849-884).
-template <class V>
+template <class V, bool POS = true>
 __device__ __forceinline__ void cumulant_collide_xsums(V (&A)[kQ27], V rho, V uxe, V uye, V uze, V omega1,
                                                        const CaseParams& cp);
 template <class V>
@@ -170,8 +170,9 @@ __device__ __forceinline__ void cumulant_collide(V (&A)[kQ27], V rho, V uxe, V u
 }
 
 // The same with the x triplets of A already replaced by their velocity-free sums (chimera_xsums);
-// the x pass then only shifts them to the velocity: b = m1 - u m0, c = m2 - 2u m1 + u^2 m0
-template <class V>
+// the x pass then only shifts them to the velocity: b = m1 - u m0, c = m2 - 2u m1 + u^2 m0.
+// POS = false leaves the positivity limiter out (callers whose cases all run without it).
+template <class V, bool POS>
 __device__ __forceinline__ void cumulant_collide_xsums(V (&A)[kQ27], V rho, V uxe, V uye, V uze, V omega1,
                                                        const CaseParams& cp) {
   using T = SC<V>;
@@ -302,7 +303,7 @@ __device__ __forceinline__ void cumulant_collide_xsums(V (&A)[kQ27], V rho, V ux
   }
 
   // positivity limiter (kernel_cumulant.jl:849-884)
-  if (flags & CF_LIMITER_POSITIVITY) {
+  if (POS && (flags & CF_LIMITER_POSITIVITY)) {
     V fmin = A[0];
 #pragma unroll
     for (int k = 1; k < kQ27; ++k) fmin = vmin(fmin, A[k]);

@@ -947,6 +947,7 @@ oal_status oal_stream_collide(const oal_geometry* g, const oal_level_fields* fl,
   a.v_bstride = 512; a.v_cstride = fl->vel_comp_stride > 0 ? fl->vel_comp_stride : 512 * (int64_t)g->nb;
   a.force_part = g->d_force_part;
   a.p0 = cp;
+  a.flags_any = cp.flags;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   OAL_CUDA_TRY(launch_by_storage(fl->storage, g, a, PATH_PLAIN, st));
   if ((cp.flags & CF_COLLECT) && fl->force_out) {
@@ -1181,6 +1182,7 @@ static oal_status enqueue_step(oal_level* L, const CaseParams& cp, cudaStream_t 
   a.force_part = L->d_force_part;
   a.err = L->d_err;
   a.p0 = cp;
+  a.flags_any = cp.flags;
   a.par = L->par;
   if (L->dense) {
     a.dense = 1;
@@ -1867,6 +1869,7 @@ struct oal_batch {
   float* d_sponge = nullptr;     // [R*512] (allocated when a member brings one)
   float* d_wdist = nullptr;
   CaseParams* d_cases = nullptr;  // [max_members]
+  uint32_t flags_any = 0;          // OR of the active members' case flags
   // work lists, rebuilt when membership changes
   uint2* d_gentries = nullptr; int64_t n_gentries = 0, cap_gentries = 0;
   int32_t* d_fast = nullptr; int64_t n_fast = 0;
@@ -1898,6 +1901,7 @@ static oal_status batch_rebuild(oal_batch* B) {
   std::vector<uint2> ge;
   std::vector<int32_t> fast, general, seg(1, 0);
   std::vector<CaseParams> cases((size_t)B->max_members);
+  uint32_t flags_any = 0;
   for (int32_t m = 0; m < B->max_members; ++m) {
     const BatchMember& M = B->mem[(size_t)m];
     if (M.active) {
@@ -1906,6 +1910,7 @@ static oal_status batch_rebuild(oal_batch* B) {
       for (int32_t b : g->h_fast) fast.push_back((int32_t)(M.rb + b));
       for (int32_t b : g->h_general) general.push_back((int32_t)(M.rb + b));
       cases[(size_t)m] = M.cp;
+      flags_any |= M.cp.flags;
     }
     seg.push_back((int32_t)(general.size() * 4));
   }
@@ -1922,6 +1927,7 @@ static oal_status batch_rebuild(oal_batch* B) {
   OAL_CUDA_TRY(upload(B->d_general, general, B->n_general));
   OAL_CUDA_TRY(cudaMemcpy(B->d_seg, seg.data(), seg.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
   OAL_CUDA_TRY(cudaMemcpy(B->d_cases, cases.data(), cases.size() * sizeof(CaseParams), cudaMemcpyHostToDevice));
+  B->flags_any = flags_any;
   B->dirty = false;
   batch_release_graph(B);
   return OAL_OK;
@@ -1960,6 +1966,7 @@ static oal_status batch_enqueue_step(oal_batch* B, int step_offset, cudaStream_t
   a.sponge = B->d_sponge;
   a.wall_dist = B->d_wdist;
   a.cases = B->d_cases;
+  a.flags_any = B->flags_any;
   a.n_blocks = (int32_t)B->R;
   a.n_total_blocks = (int32_t)(B->R + B->G);
   a.block_base = 0;
