@@ -330,8 +330,8 @@ oal_status oal_geometry_blocks(const oal_geometry* g, int64_t out[3]);
 
 /* ---- no-allocation entry point -------------------------------------------------------------- */
 /* No counterpart in the reference. For callers that cannot call cudaMalloc when they need the
- * totals (a step recorded into a CUDA graph, a stream-ordered pool that forbids stray
- * allocations, a host runtime that must not grow device memory between steps): FP64 {mass, px,
+ * totals (a stream-ordered pool that forbids stray allocations, a host runtime such as a Julia
+ * task on CUDA.jl's allocator that must not grow device memory between steps): FP64 {mass, px,
  * py, pz} of the fluid cells of caller-owned populations, with the per-block partial sums kept in
  * a fixed file-scope device array of OAL_NOALLOC_MAX_BLOCKS blocks (2 MiB, held by every GPU that
  * loads the library until the process exits). f: device populations (storage type, element

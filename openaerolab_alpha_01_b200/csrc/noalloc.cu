@@ -1,9 +1,9 @@
 // noalloc.cu — an FP64 mass/momentum reduction that allocates nothing.
 //
 // Some callers cannot call cudaMalloc at the point where they need conservation totals: a
-// solver step recorded into a CUDA graph or run under a stream-ordered pool that forbids stray
-// allocations, or a host (for instance a Julia task holding the GPU through CUDA.jl's allocator)
-// that must not grow device memory between steps. `oal_mass_momentum_noalloc` serves them: the
+// solver step run under a stream-ordered pool that forbids stray allocations, or a host (for
+// instance a Julia task holding the GPU through CUDA.jl's allocator) that must not grow device
+// memory between steps. `oal_mass_momentum_noalloc` serves them: the
 // caller passes the populations and receives {mass, px, py, pz}; the per-block partial sums live
 // in a fixed file-scope device array of OAL_NOALLOC_MAX_BLOCKS * 4 doubles (2 MiB) that every GPU
 // loading this library holds until the process exits.

@@ -2,9 +2,8 @@
 mass/momentum reduction (oal_level_mass_momentum) on the same device state.
 
 The entry point is for callers that cannot call cudaMalloc when they need conservation totals
-(a step recorded into a CUDA graph, a stream-ordered pool that forbids stray allocations, a host
-runtime that must not grow device memory between steps); its scratch is a fixed device array
-inside the library. This file is collected last so that a failure here stops a `-x` run only after
+(a stream-ordered pool that forbids stray allocations, a host runtime that must not grow device
+memory between steps); its scratch is a fixed device array inside the library. This file is collected last so that a failure here stops a `-x` run only after
 every other test ran; it also passes alone in a fresh process.
 """
 import ctypes as C
