@@ -1031,7 +1031,11 @@ oal_status oal_level_create_ex(const oal_geometry* g, int32_t op, int32_t storag
   if ((e = cudaMalloc(&L->d_mm_part, (size_t)g->nb * 4 * sizeof(double))) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&L->d_mm, 4 * sizeof(double))) != cudaSuccess) return fail(e);
   if ((e = cudaStreamCreateWithFlags(&L->cap, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
-  if ((e = cudaStreamCreateWithFlags(&L->ov.side, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+  // the general kernel's side stream at the highest priority: its few, long CTAs (blocks at solids)
+  // start first instead of trailing the uniform kernel's
+  int prio_least = 0, prio_greatest = 0;
+  if ((e = cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest)) != cudaSuccess) return fail(e);
+  if ((e = cudaStreamCreateWithPriority(&L->ov.side, cudaStreamNonBlocking, prio_greatest)) != cudaSuccess) return fail(e);
   if ((e = cudaEventCreateWithFlags(&L->ov.fork, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
   if ((e = cudaEventCreateWithFlags(&L->ov.join, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&L->d_err, sizeof(uint32_t))) != cudaSuccess) return fail(e);
