@@ -99,8 +99,15 @@ enum { OAL_LIMITER_NONE = 0, OAL_LIMITER_FACTORED = 1, OAL_LIMITER_POSITIVITY = 
  *            (kernel_cumulant.jl:402-417); fluid cells pull from solid cells unchanged.
  *   HALFWAY: half-way bounce-back on every fluid->solid link with the momentum-exchange
  *            force of the octree solver (octree_q19/src/stream.jl:229-256) on D3Q27 links;
- *            solid cells hold the rest equilibrium. */
-enum { OAL_SOLID_FULLWAY = 0, OAL_SOLID_HALFWAY = 1 };
+ *            solid cells hold the rest equilibrium.
+ *   GRAD:    FULLWAY, then the Grad-reconstruction wall of the reference's bc_scheme "grad"
+ *            (geometry/grad_wall_kernel.jl:42-144, called from timestep.jl:1738-1751) on every
+ *            fluid cell with a link into a solid cell: all its post-collision populations are
+ *            rebuilt as f_eq(rho, u_wall = 0) + (1 - 1/tau) w_k 4.5 Q_k : Pi_neq (Pi_neq of the
+ *            post-collision populations about (rho, 0), times grad_pineq_scale), floored at
+ *            1e-12, and its velocity output set to 0 (wall velocity mode "none", the default).
+ *            No momentum-exchange force is accumulated (forces come from HALFWAY). */
+enum { OAL_SOLID_FULLWAY = 0, OAL_SOLID_HALFWAY = 1, OAL_SOLID_GRAD = 2 };
 
 /* Scalar step parameters: the scalars of `_kargs` (timestep.jl:1238-1478) that the
  * D3Q27 level-1 path reads. Field meaning and units are the reference's (lattice units). */
@@ -142,7 +149,9 @@ typedef struct oal_step_params {
   float hrr_sigma;               /* HRR blend, used when hrr_hybrid and < 0.999 (default 1) */
   float nu_sgs_lattice_floor;    /* level-independent lattice-viscosity floor (default 0) */
   float shock_nu_max;            /* Mach-pocket viscosity: max(5 shock_nu_max, 0.24) (default 0) */
-  int32_t reserved[4];
+  /* OAL_SOLID_GRAD: share of Pi_neq the wall keeps (config grad_pineq_scale, default 1) */
+  float grad_pineq_scale;
+  int32_t reserved[3];
 } oal_step_params;
 
 /* ---- library ---------------------------------------------------------------------------- */

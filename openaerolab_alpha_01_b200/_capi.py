@@ -46,6 +46,7 @@ OAL_LEVEL_DENSE = 1
 
 OAL_SOLID_FULLWAY = 0
 OAL_SOLID_HALFWAY = 1
+OAL_SOLID_GRAD = 2
 
 STORAGE_NAMES = {"f32": OAL_STORE_F32, "f16": OAL_STORE_F16_DEV, "bf16": OAL_STORE_BF16_DEV, "f64": OAL_STORE_F64}
 
@@ -88,7 +89,8 @@ class StepParams(C.Structure):
         ("hrr_sigma", C.c_float),
         ("nu_sgs_lattice_floor", C.c_float),
         ("shock_nu_max", C.c_float),
-        ("reserved", C.c_int32 * 4),
+        ("grad_pineq_scale", C.c_float),
+        ("reserved", C.c_int32 * 3),
     ]
 
 

@@ -71,7 +71,8 @@ enum CaseFlags : uint32_t {
   CF_INLET_NOISE = 1u << 14,
   CF_PERIODIC_X = 1u << 15,  // periodic axes of a dense (box) level
   CF_PERIODIC_Y = 1u << 16,
-  CF_PERIODIC_Z = 1u << 17
+  CF_PERIODIC_Z = 1u << 17,
+  CF_GRAD_WALL = 1u << 18    // Grad-reconstruction wall on fluid cells with links into solids
 };
 
 struct CaseParams {
@@ -81,7 +82,8 @@ struct CaseParams {
   int32_t time_step_seed;
   uint32_t flags;
   int32_t nx, ny, nz;
-  int32_t pad[3];
+  float grad_pineq_scale;  // CF_GRAD_WALL
+  int32_t pad[2];
 };
 static_assert(sizeof(CaseParams) == 80, "CaseParams layout");
 

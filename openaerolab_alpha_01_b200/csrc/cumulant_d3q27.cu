@@ -1192,17 +1192,25 @@ __global__ void __launch_bounds__(128) k_cumulant_gen(const StepArgs a, const in
       // ---- Guo forcing + store (kernel_cumulant.jl:889-908) ----
       const bool forced = Fx != R(0) || Fy != R(0) || Fz != R(0);
       const R gpre = R(1) - R(0.5) * omega1;
+      if (forced) {
 #pragma unroll
-      for (int k = 0; k < kQ27; ++k) {
-        R fc = A[k];
-        if (forced) {
+        for (int k = 0; k < kQ27; ++k) {
           const R cxf = R(q27_cx(k)), cyf = R(q27_cy(k)), czf = R(q27_cz(k));
           const R cu = cxf * uxe + cyf * uye + czf * uze;
           const R ft = R(q27_w(k)) * R(3) *
                        ((cxf - ux + R(3) * cu * cxf) * Fx + (cyf - uy + R(3) * cu * cyf) * Fy + (czf - uz + R(3) * cu * czf) * Fz);
-          fc = vfma(gpre, ft, A[k]);
+          A[k] = vfma(gpre, ft, A[k]);
         }
-        const S v = Codec<S>::enc(fc, R(q27_w(k)), R(1.0 / q27_w(k)));
+      }
+      if ((flags & CF_GRAD_WALL) && (mask & ~(1u << 13)) != 0u) {
+        // a fluid cell with a link into a solid: the Grad-reconstruction wall overwrites its
+        // post-collision populations and velocity (grad_wall_kernel.jl:42-144, timestep.jl:1738)
+        grad_wall<R>(A, rho, R(1) / R(cp.tau), R(cp.grad_pineq_scale));
+        vel_out[vown] = R(0); vel_out[vown + vcs] = R(0); vel_out[vown + 2 * vcs] = R(0);
+      }
+#pragma unroll
+      for (int k = 0; k < kQ27; ++k) {
+        const S v = Codec<S>::enc(A[k], R(q27_w(k)), R(1.0 / q27_w(k)));
         if (store_post) fpost[own + k * kst] = v;
         fout[own + k * kst] = v;
       }

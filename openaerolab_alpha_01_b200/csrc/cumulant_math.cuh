@@ -110,6 +110,33 @@ __device__ __forceinline__ void chimera_bwd3(V& a, V& b, V& c, V u, V tu, V u2) 
 // the blend of the positivity limiter in the lanes whose minimum population fmin is negative:
 // f = f_eq + alpha (f - f_eq), alpha the largest factor keeping every population >= 0
 // (kernel_cumulant.jl:856-884)
+// Grad-reconstruction wall at wall velocity 0 (grad_wall_kernel.jl:100-136): Pi_neq of the
+// post-collision populations A about (rho, 0), scaled by pineq_scale, then every population
+// rebuilt as rho w_k + (1 - omega) w_k 4.5 Q_k : Pi_neq, Q_ab = c_a c_b - delta_ab / 3, floored at
+// 1e-12 (NaN passes, as the reference's max).
+template <class R>
+__device__ __forceinline__ void grad_wall(R (&A)[kQ27], R rho, R omega, R pineq_scale) {
+  R pxx = R(0), pyy = R(0), pzz = R(0), pxy = R(0), pyz = R(0), pzx = R(0);
+#pragma unroll
+  for (int k = 0; k < kQ27; ++k) {
+    const R cx = R(q27_cx(k)), cy = R(q27_cy(k)), cz = R(q27_cz(k));
+    const R fneq = A[k] - rho * R(q27_w(k));
+    pxx = pxx + fneq * cx * cx; pyy = pyy + fneq * cy * cy; pzz = pzz + fneq * cz * cz;
+    pxy = pxy + fneq * cx * cy; pyz = pyz + fneq * cy * cz; pzx = pzx + fneq * cz * cx;
+  }
+  pxx = pxx * pineq_scale; pyy = pyy * pineq_scale; pzz = pzz * pineq_scale;
+  pxy = pxy * pineq_scale; pyz = pyz * pineq_scale; pzx = pzx * pineq_scale;
+  const R cs2 = R(1) / R(3), inv_2cs4 = R(0.5) / (cs2 * cs2), one_m_w = R(1) - omega;
+#pragma unroll
+  for (int k = 0; k < kQ27; ++k) {
+    const R cx = R(q27_cx(k)), cy = R(q27_cy(k)), cz = R(q27_cz(k)), wk = R(q27_w(k));
+    const R qxx = cx * cx - cs2, qyy = cy * cy - cs2, qzz = cz * cz - cs2;
+    const R reg = wk * inv_2cs4 *
+                  (pxx * qxx + pyy * qyy + pzz * qzz + R(2) * (pxy * cx * cy + pyz * cy * cz + pzx * cz * cx));
+    A[k] = vmaxc(rho * wk + one_m_w * reg, R(1e-12));
+  }
+}
+
 // opaque copy: the compiler may not assume the value equals its source, so expressions of it are
 // recomputed rather than kept alive from earlier
 __device__ __forceinline__ float opaque(float v) { asm volatile("" : "+f"(v)); return v; }

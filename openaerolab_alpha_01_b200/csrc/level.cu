@@ -322,7 +322,7 @@ static oal_status resolve_params(const oal_step_params* p, const oal_geometry* g
   if (!(p->tau > 0.5f) || !std::isfinite(p->tau)) return set_error(OAL_E_INVALID_ARG, "tau must be > 0.5 (got %g)", p->tau);
   if (p->limiter_type < 0 || p->limiter_type > 2) return set_error(OAL_E_INVALID_ARG, "limiter_type %d", p->limiter_type);
   if (p->zwall_bc < 0 || p->zwall_bc > 2) return set_error(OAL_E_INVALID_ARG, "zwall_bc %d", p->zwall_bc);
-  if (p->solid_bc != OAL_SOLID_FULLWAY && p->solid_bc != OAL_SOLID_HALFWAY)
+  if (p->solid_bc != OAL_SOLID_FULLWAY && p->solid_bc != OAL_SOLID_HALFWAY && p->solid_bc != OAL_SOLID_GRAD)
     return set_error(OAL_E_INVALID_ARG, "solid_bc %d", p->solid_bc);
   std::memset(cp, 0, sizeof *cp);
   cp->tau = p->tau;
@@ -351,6 +351,8 @@ static oal_status resolve_params(const oal_step_params* p, const oal_geometry* g
   if (p->sponge_blend_distributions == 1) f |= CF_SPONGE_BLEND;
   if (p->transverse_freestream == 1) f |= CF_TRANSVERSE_FS;
   if (p->solid_bc == OAL_SOLID_HALFWAY) f |= CF_HALFWAY;
+  if (p->solid_bc == OAL_SOLID_GRAD) f |= CF_GRAD_WALL;
+  cp->grad_pineq_scale = p->grad_pineq_scale;
   if (p->collect_forces) f |= CF_COLLECT;
   if (p->store_post_collision == 1) f |= CF_STORE_POST;
   if (p->c_wale != 0.0f) f |= CF_GRADIENTS;
@@ -619,6 +621,7 @@ void oal_default_step_params(oal_step_params* p) {
   p->hrr_sigma = 1.0f;            // :2283
   p->nu_sgs_lattice_floor = 0.0f; // :733
   p->shock_nu_max = 0.0f;
+  p->grad_pineq_scale = 1.0f;     // config_loader.jl:898
 }
 
 void oal_default_entropic_params(oal_step_params* p) {

@@ -23,6 +23,8 @@
 //   Guo forcing + store ..... src/collision/kernel_cumulant.jl:889-908
 //   half-way BB + MEM ....... src/octree_q19/src/stream.jl:229-256 (link rule, generalised to the
 //                             27 D3Q27 links; the reference's GPU path has no D3Q27 analogue)
+//   Grad wall ............... src/geometry/grad_wall_kernel.jl:42-144 (velocity mode 0), called
+//                             from src/collision/timestep.jl:1738-1751
 //   mass / momentum ......... src/octree_q19/src/state.jl:614-637 (Float64 sums)
 //   block AMR (default flags): parent interpolation of a refined level's pulls
 //                             src/collision/physics_interpolation.jl:10-51,128-137,188-346,705-1198
@@ -459,6 +461,7 @@ void step_cell(const Level& L, const oal_step_params& P, const T* f_in, T* f_out
   T rho = T(0), jx = T(0), jy = T(0), jz = T(0);
   T fs[Q];
   double mx = 0, my = 0, mz = 0;
+  bool wall_cell = false;  // a pull source is solid (the reference's Bouzidi/Grad boundary-cell list)
   for (int k = 0; k < Q; ++k) {
     const int cx = TB.cx[k], cy = TB.cy[k], cz = TB.cz[k];
     const int sx = x - cx, sy = y - cy, sz = z - cz;
@@ -467,6 +470,7 @@ void step_cell(const Level& L, const oal_step_params& P, const T* f_in, T* f_out
     int sb = src_block(L, b, sx, sy, sz, lx, ly, lz);
     if (sb >= 0) {
       const bool src_solid = L.obstacle && L.obstacle[A.s(lx, ly, lz, sb)];
+      wall_cell = wall_cell || src_solid;
       if (halfway && src_solid) {
         // link opp(k) of this cell is cut: the population this cell sent toward the wall
         // returns (octree_q19/src/stream.jl:229-233, half-way rule, wall at rest)
@@ -807,15 +811,47 @@ void step_cell(const Level& L, const oal_step_params& P, const T* f_in, T* f_out
   }
 
   // STEP 10: Guo forcing + store (kernel_cumulant.jl:889-908)
+  T fcs[Q];
   for (int k = 0; k < Q; ++k) {
     const T cxf = T(TB.cx[k]), cyf = T(TB.cy[k]), czf = T(TB.cz[k]);
     const T cu = cxf * ux_eq + cyf * uy_eq + czf * uz_eq;
     const T force_term = T(TB.w[k]) * T(3) *
                          ((cxf - ux + T(3) * cu * cxf) * Fx + (cyf - uy + T(3) * cu * cyf) * Fy +
                           (czf - uz + T(3) * cu * czf) * Fz);
-    const T fc = Am[k] + (T(1) - T(0.5) * omega1) * force_term;
-    if (store_post) f_post[A.f(x, y, z, b, k)] = fc;
-    f_out[A.f(x, y, z, b, k)] = fc;
+    fcs[k] = Am[k] + (T(1) - T(0.5) * omega1) * force_term;
+  }
+  if (P.solid_bc == OAL_SOLID_GRAD && wall_cell) {
+    // Grad-reconstruction wall (geometry/grad_wall_kernel.jl:62-144 with grad_vel_mode 0, called
+    // from collision/timestep.jl:1738-1751 with omega_wall = 1/tau): rebuild every population of
+    // a fluid cell with a wall-crossing link from (rho_out, u_wall = 0, Pi_neq of the
+    // post-collision populations); the velocity output becomes the wall velocity.
+    const T uw = T(0);
+    T pxx = T(0), pyy = T(0), pzz = T(0), pxy = T(0), pyz = T(0), pzx = T(0);
+    for (int k = 0; k < Q; ++k) {
+      const T cxf = T(TB.cx[k]), cyf = T(TB.cy[k]), czf = T(TB.cz[k]);
+      const T fe = feq2<T>(rho, uw, uw, uw, T(TB.w[k]), cxf, cyf, czf);
+      const T fneq = fcs[k] - fe;
+      pxx += fneq * cxf * cxf; pyy += fneq * cyf * cyf; pzz += fneq * czf * czf;
+      pxy += fneq * cxf * cyf; pyz += fneq * cyf * czf; pzx += fneq * czf * cxf;
+    }
+    const T sc = T(P.grad_pineq_scale);
+    pxx *= sc; pyy *= sc; pzz *= sc; pxy *= sc; pyz *= sc; pzx *= sc;
+    const T cs2 = T(1) / T(3), inv_2cs4 = T(0.5) / (cs2 * cs2);
+    const T one_m_w = T(1) - T(1) / T(P.tau);
+    for (int k = 0; k < Q; ++k) {
+      const T cxf = T(TB.cx[k]), cyf = T(TB.cy[k]), czf = T(TB.cz[k]), wk = T(TB.w[k]);
+      const T fe = feq2<T>(rho, uw, uw, uw, wk, cxf, cyf, czf);
+      const T qxx = cxf * cxf - cs2, qyy = cyf * cyf - cs2, qzz = czf * czf - cs2;
+      const T reg = wk * inv_2cs4 *
+                    (pxx * qxx + pyy * qyy + pzz * qzz + T(2) * (pxy * cxf * cyf + pyz * cyf * czf + pzx * czf * cxf));
+      const T fc = fe + one_m_w * reg;
+      fcs[k] = fc < T(1e-12) ? T(1e-12) : fc;  // max(fc, 1e-12), NaN passes
+    }
+    vel_out[own] = uw; vel_out[own + cs] = uw; vel_out[own + 2 * cs] = uw;
+  }
+  for (int k = 0; k < Q; ++k) {
+    if (store_post) f_post[A.f(x, y, z, b, k)] = fcs[k];
+    f_out[A.f(x, y, z, b, k)] = fcs[k];
   }
 }
 

@@ -101,6 +101,8 @@ VARIANTS = {
     "relaxation_rates": dict(omega_bulk=0.7, omega3=0.9, nu_sgs_background=1e-3),
     "compressible": dict(compressible_corr=1),
     "no_wale": dict(c_wale=0.0),
+    "grad_wall": dict(solid_bc=capi.OAL_SOLID_GRAD, collect_forces=0),
+    "grad_wall_half_stress": dict(solid_bc=capi.OAL_SOLID_GRAD, collect_forces=0, grad_pineq_scale=0.5),
 }
 
 

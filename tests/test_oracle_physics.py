@@ -116,3 +116,60 @@ def test_planted_mistakes_are_detected(oracle_lib):
         B.step(pb)
     rel = np.max(np.abs(A.f - B.f)) / np.max(np.abs(A.f))
     assert rel > 1e-7
+
+
+def test_grad_wall_properties(oracle_lib):
+    """The Grad-reconstruction wall (bc_scheme "grad", geometry/grad_wall_kernel.jl): every fluid
+    cell with a link into the sphere leaves the step with zero velocity output, populations of
+    the rebuilt form rho w_k + (1 - 1/tau) w_k 4.5 Q_k : Pi (so each cell keeps its density and
+    carries zero momentum), at least 1e-12; with grad_pineq_scale 0 the wall cells hold exactly
+    the rest equilibrium rho w_k. Cells away from the wall step as with the full-way treatment."""
+    from openaerolab_alpha_01_b200 import _capi as capi
+    from openaerolab_alpha_01_b200.cases import sphere_channel_case
+    case = sphere_channel_case(32, 16, 16, diameter=6.0, centre_x=12.0, u_inlet=0.05, re=200.0)
+    d = case.dom
+    k = np.arange(27)
+    c = np.stack([k % 3 - 1, (k // 3) % 3 - 1, k // 9 - 1]).astype(np.float64)
+    w = np.array([{0: 8 / 27, 1: 2 / 27, 2: 1 / 54, 3: 1 / 216}[int(v)] for v in (c * c).sum(0)])
+
+    def run(bc, scale=1.0, steps=3):
+        O = oracle_lib.OracleLevel(d.coords, d.neighbor_table, d.shape, obstacle=d.obstacle, dtype=np.float64)
+        O.init_equilibrium(case.rho, case.vel)
+        p = capi.default_params(**{f: getattr(case.params, f) for f, _ in capi.StepParams._fields_ if f != "reserved"})
+        p.solid_bc, p.collect_forces, p.grad_pineq_scale = bc, 0, scale
+        for i in range(steps):
+            p.time_step_seed = i
+            O.step(p)
+        return O
+    # fluid cells with a solid pull source
+    solid = d.obstacle.astype(bool)
+    X, Y, Z = d.cell_positions()
+    sx, sy, sz = d.shape
+    occ = np.zeros((sx + 2, sy + 2, sz + 2), bool)
+    occ[X[solid], Y[solid], Z[solid]] = True
+    wall = np.zeros_like(solid)
+    for q in range(27):
+        wall |= occ[X - c[0, q].astype(int), Y - c[1, q].astype(int), Z - c[2, q].astype(int)]
+    wall &= ~solid
+    assert wall.sum() > 50
+    G = run(capi.OAL_SOLID_GRAD)
+    F = run(capi.OAL_SOLID_FULLWAY)
+    assert np.all(G.vel[:, wall] == 0.0)
+    fw = G.f[:, wall]                                   # (27, n_wall)
+    assert np.all(fw >= 1e-12)
+    rho = fw.sum(0)
+    assert np.allclose(rho, G.rho[wall], rtol=1e-12)
+    assert np.max(np.abs(c @ fw)) < 1e-13
+    G0 = run(capi.OAL_SOLID_GRAD, scale=0.0, steps=1)
+    assert np.allclose(G0.f[:, wall], w[:, None] * G0.rho[wall][None, :], rtol=1e-13, atol=0)
+    # away from the wall (two cells or more from any wall cell after three steps) nothing differs
+    far = ~solid & ~wall
+    for _ in range(3):
+        grown = far.copy()
+        occ2 = np.ones((sx + 2, sy + 2, sz + 2), bool)
+        occ2[X[~far], Y[~far], Z[~far]] = False
+        for q in range(27):
+            grown &= occ2[X - c[0, q].astype(int), Y - c[1, q].astype(int), Z - c[2, q].astype(int)]
+        far = grown
+    assert far.sum() > 1000
+    assert np.array_equal(G.f[:, far], F.f[:, far])
