@@ -8,13 +8,15 @@
 // half-way link rule with momentum exchange is the octree solver's
 // (src/octree_q19/src/stream.jl:229-256) on the 27 links.
 //
-// Three kernels share the collision code (cumulant_math.cuh):
+// The kernels share the collision code (cumulant_math.cuh):
 //   k_fill_ghosts   writes, into ghost blocks around the level, the value every domain-face pull
 //                   receives (inlet equilibrium, outlet copy, mirrors, walls, lattice weight), so
 //                   the main kernel needs no face logic;
-//   k_cumulant_fast the uniform step of blocks without solids, sponge or wall model: a CTA of
-//                   128 threads covers half a block, two cells per thread in packed f32x2
-//                   arithmetic (a quarter block, one cell per thread, in FP64);
+//   k_cumulant_pairs the uniform step of blocks without solids, sponge or wall model (FP32 and
+//                   16-bit storage): two x-adjacent cells per thread in packed f32x2 arithmetic,
+//                   one warp per z plane of a block;
+//   k_cumulant_fast the same step one cell per thread (FP64 storage: a CTA of 128 threads covers
+//                   a quarter block);
 //   k_cumulant_gen  everything else, one cell per thread: per-cell solid masks (full-way or
 //                   half-way walls with FP64 momentum exchange), sponge, wall model, Guo forcing,
 //                   and the face conditions when the level has no ghost blocks (caller-owned
@@ -32,6 +34,11 @@
 #endif
 #ifndef OAL_FAST_CELLS
 #define OAL_FAST_CELLS 2
+#endif
+// threads per CTA of the x-pair kernel, one warp per z plane of a block: 32, 64, 128 or 256
+// (measured on the config-2 channel: 64 best, 128 1 % slower, 32 2 %, 256 12 %)
+#ifndef OAL_PAIRS_THREADS
+#define OAL_PAIRS_THREADS 64
 #endif
 
 namespace oal {
@@ -848,7 +855,7 @@ template <> __device__ __forceinline__ uint2 pair_word<float>(F2 v, int) {
 // stride 256, row (y, z) stride 4 and 32.
 // POS: some case of the launch uses the positivity limiter (its code is left out otherwise).
 template <class S, class IDX, bool POS>
-__global__ void __launch_bounds__(128, OAL_FAST_MIN_CTAS) k_cumulant_pairs(const StepArgs a, const int32_t* __restrict__ work) {
+__global__ void __launch_bounds__(OAL_PAIRS_THREADS, OAL_FAST_MIN_CTAS * 128 / OAL_PAIRS_THREADS) k_cumulant_pairs(const StepArgs a, const int32_t* __restrict__ work) {
   using W = typename PairWord<S>::W;
   using V = F2;
   using T = float;
@@ -857,16 +864,20 @@ __global__ void __launch_bounds__(128, OAL_FAST_MIN_CTAS) k_cumulant_pairs(const
   __shared__ int32_t s_nbr[28];
   __shared__ CaseParams s_cp;
   const int tid = threadIdx.x;
-  const int b = work[blockIdx.x >> 1];
-  const int part = blockIdx.x & 1;
+  // a CTA covers OAL_PAIRS_THREADS / 32 z planes of a block (one warp per plane)
+  constexpr int CPB = 256 / OAL_PAIRS_THREADS;
+  const int b = work[blockIdx.x / CPB];
+  const int part = blockIdx.x % CPB;
   if (tid < 27) {
     const int32_t nb = a.nbr[(int64_t)b * 27 + tid];
     s_nbr[tid] = nb;
     s_wbase[tid] = (IDX)nb * wbst;
   }
-  if (tid >= 32 && tid < 32 + (int)(sizeof(CaseParams) / 4)) {
+  // the case parameters: copied by the second warp, or by the first one in one-warp CTAs
+  const int cw = OAL_PAIRS_THREADS >= 64 ? tid - 32 : tid;
+  if (cw >= 0 && cw < (int)(sizeof(CaseParams) / 4)) {
     const int case_id = a.cases ? a.binfo[b].w : 0;
-    reinterpret_cast<uint32_t*>(&s_cp)[tid - 32] = reinterpret_cast<const uint32_t*>(&case_of(a, case_id))[tid - 32];
+    reinterpret_cast<uint32_t*>(&s_cp)[cw] = reinterpret_cast<const uint32_t*>(&case_of(a, case_id))[cw];
   }
   __syncthreads();
   const CaseParams& cp = s_cp;
@@ -879,7 +890,7 @@ __global__ void __launch_bounds__(128, OAL_FAST_MIN_CTAS) k_cumulant_pairs(const
   const IDX vcs = (IDX)a.v_cstride;
   const int n_real = a.n_blocks;
 
-  const int i = tid & 3, y = (tid >> 2) & 7, z = 4 * part + (tid >> 5);
+  const int i = tid & 3, y = (tid >> 2) & 7, z = (OAL_PAIRS_THREADS / 32) * part + (tid >> 5);
 
   // ---- WALE stencil of the previous step's velocity (kernel_cumulant.jl:496-549): its loads
   // are issued before the pull so that both round trips to memory overlap ----
@@ -1415,13 +1426,13 @@ cudaError_t launch_fast(const StepArgs& a, const int32_t* work, int n_work, cuda
     else k_cumulant_fast<S, F2, int64_t><<<(unsigned)n_work * 2u, 128, 0, st>>>(a, work);
   } else {
     // x pairs; word indices (half the element count) decide the index width
-    const unsigned grid = (unsigned)n_work * 2u;
+    const unsigned grid = (unsigned)n_work * (256u / OAL_PAIRS_THREADS);
     if (a.flags_any & CF_LIMITER_POSITIVITY) {
-      if (idx32) k_cumulant_pairs<S, uint32_t, true><<<grid, 128, 0, st>>>(a, work);
-      else k_cumulant_pairs<S, int64_t, true><<<grid, 128, 0, st>>>(a, work);
+      if (idx32) k_cumulant_pairs<S, uint32_t, true><<<grid, OAL_PAIRS_THREADS, 0, st>>>(a, work);
+      else k_cumulant_pairs<S, int64_t, true><<<grid, OAL_PAIRS_THREADS, 0, st>>>(a, work);
     } else {
-      if (idx32) k_cumulant_pairs<S, uint32_t, false><<<grid, 128, 0, st>>>(a, work);
-      else k_cumulant_pairs<S, int64_t, false><<<grid, 128, 0, st>>>(a, work);
+      if (idx32) k_cumulant_pairs<S, uint32_t, false><<<grid, OAL_PAIRS_THREADS, 0, st>>>(a, work);
+      else k_cumulant_pairs<S, int64_t, false><<<grid, OAL_PAIRS_THREADS, 0, st>>>(a, work);
     }
   }
   return cudaGetLastError();
