@@ -35,6 +35,19 @@
 #ifndef OAL_FAST_CELLS
 #define OAL_FAST_CELLS 2
 #endif
+// refined levels' ghost fill: resident CTAs per SM its registers are sized for, and whether the
+// interpolation at a precomputed position is inlined
+#ifndef OAL_PAR_FILL_MIN_CTAS
+#define OAL_PAR_FILL_MIN_CTAS 4
+#endif
+#ifndef OAL_POS_NOINLINE
+#define OAL_POS_NOINLINE 0
+#endif
+#if OAL_POS_NOINLINE
+#define OAL_POS_LINKAGE __noinline__
+#else
+#define OAL_POS_LINKAGE
+#endif
 // threads per CTA of the x-pair kernel, one warp per z plane of a block: 32, 64, 128 or 256
 // (measured on the config-2 channel: 64 best, 128 1 % slower, 32 2 %, 256 12 %)
 #ifndef OAL_PAIRS_THREADS
@@ -371,7 +384,7 @@ cudaError_t launch_parent_positions(const ParentView& P, const int4* pos_xyz, in
 // the direction-dependent half at a position: f_neq over the stencil's records, then
 // feq(interpolated macros) + f_neq * scale (:1131-1198)
 template <class R>
-__device__ R pos_population(const ParentView& P, int32_t pos, int fgx, int fgy, int fgz, int k, R cx, R cy, R cz,
+__device__ OAL_POS_LINKAGE R pos_population(const ParentView& P, int32_t pos, int fgx, int fgy, int fgz, int k, R cx, R cy, R cz,
                             bool comp) {
   const int32_t* nodes = P.pos_nodes + (int64_t)pos * 64;
   const R* mac = static_cast<const R*>(P.pos_macro) + (int64_t)pos * 4;
@@ -612,7 +625,7 @@ __device__ __forceinline__ const CaseParams& case_of(const StepArgs& a, int case
 // PAR: the level has a parent (its ghost pulls from inside the domain interpolate from it); the
 // plain instance carries none of that code and stays small
 template <class S, class R, bool DENSE, bool PAR>
-__global__ void __launch_bounds__(256) k_fill_ghosts(const StepArgs a, const uint2* __restrict__ entries, int64_t n) {
+__global__ void __launch_bounds__(256, PAR ? OAL_PAR_FILL_MIN_CTAS : 1) k_fill_ghosts(const StepArgs a, const uint2* __restrict__ entries, int64_t n) {
   const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (e >= n) return;
   const uint2 en = entries[e];

@@ -1693,6 +1693,20 @@ oal_status oal_amr_create(int32_t nlevels, const oal_amr_level_desc* levels, int
         if (e == cudaSuccess) e = cudaMemcpy(me.d_pos_nodes, pos_nodes.data(), pos_nodes.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
       }
       if (e == cudaSuccess) e = cudaMemcpy(me.d_slot_pos, slot_pos.data(), slot_pos.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+      // a refined level's fill runs in cell-major entry order (block, cell, direction): the
+      // interpolations of one ghost position's directions then read its stencil records together,
+      // which outweighs the coalescing of the direction-major order of plain levels. The order of
+      // entries carries no meaning (each writes its own slot), so the level's geometry is re-ordered
+      // in place.
+      if (e == cudaSuccess && g->n_gentries > 0) {
+        oal_geometry* gm = const_cast<oal_geometry*>(g);
+        auto key = [](const uint2& v) {
+          return ((uint64_t)v.x << 14) | ((uint64_t)(v.y & 511u) << 5) | (uint64_t)((v.y >> 9) & 31u);
+        };
+        std::stable_sort(gm->h_gentries.begin(), gm->h_gentries.end(),
+                         [&](const uint2& p, const uint2& q) { return key(p) < key(q); });
+        e = cudaMemcpy(gm->d_gentries, gm->h_gentries.data(), gm->h_gentries.size() * sizeof(uint2), cudaMemcpyHostToDevice);
+      }
     }
     if (e != cudaSuccess) {
       cudaGetLastError();
