@@ -268,8 +268,9 @@ oal_status oal_level_mass_momentum(oal_level* L, double out[4]);
 oal_status oal_level_device_state(oal_level* L, void** f, void** rho, void** vel);
 /* Bytes of device memory this level holds. */
 int64_t oal_level_device_bytes(const oal_level* L);
-/* D3Q39 entropic levels (operator OAL_OP_ENTROPIC_D3Q39, storage OAL_STORE_F32, a geometry whose
- * blocks all have their 26 neighbours, no solid cell, no sponge, no wall within 16 cells): the
+/* D3Q39 entropic levels (operator OAL_OP_ENTROPIC_D3Q39, storage OAL_STORE_F32, a library-built
+ * geometry with no sponge and no wall distance within 16 cells; domain faces and solid cells are
+ * taken as the reference's default boundary options and full-way bounce-back): the
  * 13-multiplier warm-start cache of the equilibrium solve (timestep.jl:1447-1450), host float in
  * the reference layout lambda(8,8,8,n_blocks,13), NaN = no warm start. get_host receives the
  * cache, set_host (after the get) replaces it; either may be NULL. Init and set_state reset it to

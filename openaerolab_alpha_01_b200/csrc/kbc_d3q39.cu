@@ -1,8 +1,10 @@
 // kbc_d3q39.cu — the D3Q39 entropic KBC level step on B200: the reference's
-// stream_collide_entropic_d3q39! (src/collision/kernel_entropic_d3q39.jl:529-3368) on a level whose
-// blocks all have their 26 neighbours (periodic boxes: no obstacle, sponge, wall model, AMR
-// parent, thermal coupling or lattice shift), with its lambda warm-start cache
-// (src/collision/timestep.jl:1447-1450) and the level ping-pong.
+// stream_collide_entropic_d3q39! (src/collision/kernel_entropic_d3q39.jl:529-3368) on a level
+// without sponge, wall model, AMR parent, thermal coupling or lattice shift, with its lambda
+// warm-start cache (src/collision/timestep.jl:1447-1450) and the level ping-pong. Domain faces
+// take the default boundary options (:983-1278): k_kbc_fill writes each face value into the ghost
+// slot its pull reads before the step; the inlet face is pinned to the inlet equilibrium's mass and
+// momentum (:1313-1352); solid cells bounce back (:1602-1613).
 //
 // One thread per cell, 128 threads per CTA (a quarter of an 8^3 block), 4 CTAs per SM. A thread
 // pulls its 39 populations through the block's 27-entry neighbour table (|c| <= 3 < 8, so at most
@@ -64,6 +66,7 @@ __host__ __device__ constexpr int kopp(int k) {
                         19, 24, 23, 22, 21, 28, 27, 26, 25, 32, 31, 30, 29, 34, 33, 36, 35, 38, 37};
   return t[k];
 }
+__host__ __device__ constexpr int nbr13(int ox, int oy, int oz) { return (ox + 1) + 3 * (oy + 1) + 9 * (oz + 1); }
 __host__ __device__ constexpr float kw(int k) {
   return k < 7 ? float(1.0 / 12) : k < 15 ? float(1.0 / 27) : k < 21 ? float(2.0 / 135) : k < 33 ? float(1.0 / 432)
                                                                                              : float(1.0 / 1620);
@@ -103,7 +106,26 @@ struct KbcArgs {
   int32_t hrr;     // HRR blend active (hrr_hybrid and hrr_sigma < 0.999)
   float tau, c_wale, nu_bg, amr_sgs_scale, u_inlet, sigma0, hrr_sigma, nu_floor, shock_nu_max;
   float feq_inlet[Q];
+  // domain faces and solids (null / 0 on periodic boxes without obstacles)
+  const int4* binfo;        // 1-based block coordinates: the inlet-face pin applies at global x = 1
+  const uint32_t* bflags;   // BF_NEAR_SOLID blocks carry per-cell solid masks
+  const int32_t* mslot;
+  const uint32_t* cmask;
+  int32_t faces;            // the level has ghost blocks
+  float trho, tjx, tjy, tjz;  // moments of feq_inlet, the inlet-face pin's targets
 };
+
+// the face fill of one step: every ghost slot a real cell pulls receives its face value
+struct KbcFillArgs {
+  float* f;                 // populations in (real + ghost blocks)
+  const uint2* entries;     // (block, cell | k << 9) of the pulls whose source is a ghost cell
+  int64_t n;
+  const int32_t* nbr;
+  const int4* binfo;
+  kbc::FaceParams F;
+  float feq_inlet[Q];
+};
+constexpr uint32_t kNearSolid = 1u << 1;  // BF_NEAR_SOLID of the geometry
 
 // pair index of direction k > 0 (k and opp(k) share it)
 __host__ __device__ constexpr int kpair(int k) {
@@ -418,6 +440,24 @@ __device__ __forceinline__ bool alpha_taylor(const Tables& T, const float* sf, c
   return true;
 }
 
+// The face fill (kernel_entropic_d3q39.jl:983-1278 at the default boundary options): one thread per
+// pull whose source lies outside the domain; its value goes to the ghost slot the pull reads (the
+// slot (source cell, k) has exactly one reader, the source + c_k).
+__global__ void __launch_bounds__(256) k_kbc_fill(const KbcFillArgs a) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= a.n) return;
+  const uint2 en = a.entries[e];
+  const int b = (int)en.x, cell = (int)(en.y & 511u), k = (int)((en.y >> 9) & 63u);
+  const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
+  const int4 bi = a.binfo[b];
+  const int gx = (bi.x - 1) * 8 + x + 1, gy = (bi.y - 1) * 8 + y + 1, gz = (bi.z - 1) * 8 + z + 1;
+  const float v = kbc::face_value(a.F, a.f + (int64_t)b * Q * 512 + cell, 512, a.feq_inlet, k, gx, gy, gz);
+  const int sx = x - kcx(k), sy = y - kcy(k), sz = z - kcz(k);
+  const int ox = sx < 0 ? -1 : (sx > 7 ? 1 : 0), oy = sy < 0 ? -1 : (sy > 7 ? 1 : 0), oz = sz < 0 ? -1 : (sz > 7 ? 1 : 0);
+  const int g = a.nbr[(int64_t)b * 27 + (ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)];
+  a.f[((int64_t)g * Q + k) * 512 + ((sx & 7) | ((sy & 7) << 3) | ((sz & 7) << 6))] = v;
+}
+
 // One cell per thread (kernel_entropic_d3q39.jl:859-3368 on such a level). The thread's populations
 // live in its shared-memory column (the pulled f, then a_k, then the post-collision values) and the
 // per-direction loops run rolled over the CTA's tables, which keeps the step's code small enough to
@@ -438,6 +478,8 @@ __global__ void __launch_bounds__(kThreads, KBC_MIN_BLOCKS) k_kbc_step(const Kbc
   const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
   const int64_t N = (int64_t)a.nb * 512;
   const int64_t ci = (int64_t)b * 512 + cell;
+  // solid cells: the cell itself (bit 13) and its face neighbours (WALE stencil)
+  const uint32_t solid_mask = (a.cmask && (a.bflags[b] & kNearSolid)) ? a.cmask[(int64_t)a.mslot[b] * 512 + cell] : 0u;
 
   // STEP 1-2: pull, moments, density floor and NaN reset (:898-1290, 1616-1650)
   float rho, ux, uy, uz, inv_rho;
@@ -457,6 +499,28 @@ __global__ void __launch_bounds__(kThreads, KBC_MIN_BLOCKS) k_kbc_step(const Kbc
       jx += f * float(cx);
       jy += f * float(cy);
       jz += f * float(cz);
+    }
+    if (solid_mask & (1u << 13)) {
+      // simple bounce-back inside the obstacle (:1602-1613); the multiplier cache is left as it is
+      a.vout[ci] = 0.0f; a.vout[ci + N] = 0.0f; a.vout[ci + 2 * N] = 0.0f;
+      a.rho[ci] = 1.0f;
+#pragma unroll 1
+      for (int k = 0; k < Q; ++k) a.fout[((int64_t)b * Q + k) * 512 + cell] = sf[kopp(k) * kThreads];
+      return;
+    }
+    if (a.faces && x == 0 && s_nbr[nbr13(-1, 0, 0)] >= a.nb && a.binfo[b].x == 1) {
+      // a cell on the inlet face (global x = 1): mass and momentum pinned to the inlet
+      // equilibrium's (:1313-1352), then the moments again
+      kbc::four_moment_pin(sf, kThreads, a.trho, a.tjx, a.tjy, a.tjz);
+      rho = 0.0f; jx = 0.0f; jy = 0.0f; jz = 0.0f;
+#pragma unroll 1
+      for (int k = 0; k < Q; ++k) {
+        const float f = sf[k * kThreads];
+        rho += f;
+        jx += f * float(kcx(k));
+        jy += f * float(kcy(k));
+        jz += f * float(kcz(k));
+      }
     }
     const float rho_raw = rho;
     rho = jmax(rho_raw, 0.01f);
@@ -553,7 +617,11 @@ __global__ void __launch_bounds__(kThreads, KBC_MIN_BLOCKS) k_kbc_step(const Kbc
         const int px = x + (ax == 0 ? d : 0), py = y + (ax == 1 ? d : 0), pz = z + (ax == 2 ? d : 0);
         const int ox = px < 0 ? -1 : (px > 7 ? 1 : 0), oy = py < 0 ? -1 : (py > 7 ? 1 : 0), oz = pz < 0 ? -1 : (pz > 7 ? 1 : 0);
         const int bo = s_nbr[(ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)];
-        const int64_t c = ((px & 7) | ((py & 7) << 3) | ((pz & 7) << 6)) + 512 * (int64_t)bo;
+        // a neighbour outside the domain (ghost block) or in a solid cell contributes the own
+        // velocity (physics_utils.jl:1981-2035); mask bit of the D3Q27 direction whose source it is
+        const int sbit = ax == 0 ? (s == 0 ? 12 : 14) : ax == 1 ? (s == 0 ? 10 : 16) : (s == 0 ? 4 : 22);
+        const bool own = bo >= a.nb || ((solid_mask >> sbit) & 1u);
+        const int64_t c = own ? ci : ((px & 7) | ((py & 7) << 3) | ((pz & 7) << 6)) + 512 * (int64_t)bo;
 #pragma unroll
         for (int comp = 0; comp < 3; ++comp) (s == 0 ? up : um)[ax][comp] = a.vin[c + N * comp];
       }
@@ -911,6 +979,9 @@ struct KbcLevel {
   int device = 0;
   int32_t nb = 0;
   const int32_t* d_nbr = nullptr;
+  KbcGeometry G;
+  uint2* d_entries = nullptr;  // face-fill entries
+  int64_t n_entries = 0;
   float* f[2] = {nullptr, nullptr};
   float* vel[2] = {nullptr, nullptr};
   float* rho = nullptr;
@@ -954,15 +1025,34 @@ oal_status resolve(const oal_step_params* p, KbcArgs* a) {
   a->u_inlet = p->u_inlet; a->sigma0 = p->lambda_param; a->hrr_sigma = p->hrr_sigma;
   a->nu_floor = p->nu_sgs_lattice_floor; a->shock_nu_max = p->shock_nu_max;
   inlet_equilibrium(p->u_inlet, a->feq_inlet);
+  for (int k = 0; k < Q; ++k) {
+    const float fe = a->feq_inlet[k];
+    a->trho += fe;
+    a->tjx += fe * float(kcx(k));
+    a->tjy += fe * float(kcy(k));
+    a->tjz += fe * float(kcz(k));
+  }
   return OAL_OK;
 }
 
-oal_status enqueue(KbcLevel* L, const KbcArgs& base, cudaStream_t st) {
+oal_status enqueue(KbcLevel* L, const KbcArgs& base, const oal_step_params* p_in, int32_t seed, cudaStream_t st) {
   KbcArgs a = base;
   const int p = L->parity;
   a.fin = L->f[p]; a.fout = L->f[p ^ 1];
   a.vin = L->vel[p]; a.vout = L->vel[p ^ 1];
   a.rho = L->rho; a.lam = L->lam; a.nbr = L->d_nbr; a.nb = L->nb;
+  a.binfo = static_cast<const int4*>(L->G.d_binfo);
+  a.faces = L->n_entries > 0 ? 1 : 0;
+  if (L->G.has_solid) { a.bflags = L->G.d_bflags; a.mslot = L->G.d_mslot; a.cmask = L->G.d_cmask; }
+  if (L->n_entries > 0) {
+    KbcFillArgs fa;
+    fa.f = L->f[p]; fa.entries = L->d_entries; fa.n = L->n_entries; fa.nbr = L->d_nbr; fa.binfo = a.binfo;
+    fa.F = kbc::FaceParams{L->G.nx, L->G.ny, L->G.nz, p_in->ymin_wall_bc, p_in->transverse_freestream, seed,
+                           p_in->transverse_freestream_blend, p_in->inlet_turbulence, p_in->u_inlet};
+    for (int k = 0; k < Q; ++k) fa.feq_inlet[k] = a.feq_inlet[k];
+    k_kbc_fill<<<(unsigned)((L->n_entries + 255) / 256), 256, 0, st>>>(fa);
+    KBC_TRY(cudaGetLastError());
+  }
   k_kbc_step<<<(unsigned)L->nb * 4, kThreads, 0, st>>>(a);
   KBC_TRY(cudaGetLastError());
   L->parity ^= 1;
@@ -971,14 +1061,35 @@ oal_status enqueue(KbcLevel* L, const KbcArgs& base, cudaStream_t st) {
 
 }  // namespace
 
-oal_status kbc_create(int device, int32_t nb, const int32_t* d_nbr, KbcLevel** out) {
-  if (!out || nb <= 0 || !d_nbr) return fail(OAL_E_INVALID_ARG, "kbc_create: bad arguments");
+oal_status kbc_create(int device, const KbcGeometry& G, KbcLevel** out) {
+  const int32_t nb = G.nb;
+  if (!out || nb <= 0 || !G.d_nbr || !G.h_nbr || !G.d_binfo || !G.h_bflags)
+    return fail(OAL_E_INVALID_ARG, "kbc_create: bad arguments");
   *out = nullptr;
   if ((int64_t)nb * 4 > 0x7fffffffLL) return fail(OAL_E_TOO_LARGE, "too many blocks");
   KBC_TRY(cudaSetDevice(device));
+  // face-fill entries: every (cell, k) of a block with a missing neighbour whose source lies in a
+  // ghost block
+  std::vector<uint2> entries;
+  for (int32_t b = 0; b < nb; ++b) {
+    if (G.h_bflags[b] & 1u) continue;  // BF_INTERIOR: all 26 neighbours present
+    for (int cell = 0; cell < 512; ++cell) {
+      const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
+      for (int k = 0; k < Q; ++k) {
+        const int sx = x - kcx(k), sy = y - kcy(k), sz = z - kcz(k);
+        const int ox = sx < 0 ? -1 : (sx > 7 ? 1 : 0), oy = sy < 0 ? -1 : (sy > 7 ? 1 : 0), oz = sz < 0 ? -1 : (sz > 7 ? 1 : 0);
+        if ((ox | oy | oz) == 0) continue;
+        const int32_t g = G.h_nbr[(size_t)b * 27 + nbr13(ox, oy, oz)];
+        if (g >= nb && g < nb + G.n_ghost) entries.push_back(make_uint2((uint32_t)b, (uint32_t)cell | ((uint32_t)k << 9)));
+      }
+    }
+  }
   auto* L = new KbcLevel();
-  L->device = device; L->nb = nb; L->d_nbr = d_nbr;
+  L->device = device; L->nb = nb; L->d_nbr = G.d_nbr; L->G = G;
+  L->G.h_nbr = nullptr; L->G.h_bflags = nullptr;  // host tables are only read here
+  L->n_entries = (int64_t)entries.size();
   const size_t ncell = (size_t)nb * 512;
+  const size_t fcell = ncell + (entries.empty() ? 0 : (size_t)G.n_ghost * 512);
   auto alloc = [&](void** p, size_t bytes) {
     cudaError_t e = cudaMalloc(p, bytes);
     if (e == cudaSuccess) e = cudaMemset(*p, 0, bytes);
@@ -986,7 +1097,7 @@ oal_status kbc_create(int device, int32_t nb, const int32_t* d_nbr, KbcLevel** o
   };
   cudaError_t e = cudaSuccess;
   for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
-    e = alloc((void**)&L->f[i], ncell * Q * sizeof(float));
+    e = alloc((void**)&L->f[i], fcell * Q * sizeof(float));
     if (e == cudaSuccess) e = alloc((void**)&L->vel[i], ncell * 3 * sizeof(float));
   }
   if (e == cudaSuccess) e = alloc((void**)&L->rho, ncell * sizeof(float));
@@ -994,13 +1105,18 @@ oal_status kbc_create(int device, int32_t nb, const int32_t* d_nbr, KbcLevel** o
   if (e == cudaSuccess) e = alloc((void**)&L->d_mm_part, (size_t)nb * 4 * sizeof(double));
   if (e == cudaSuccess) e = alloc((void**)&L->d_mm, 4 * sizeof(double));
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&L->cap, cudaStreamNonBlocking);
+  if (e == cudaSuccess && !entries.empty()) {
+    e = cudaMalloc((void**)&L->d_entries, entries.size() * sizeof(uint2));
+    if (e == cudaSuccess) e = cudaMemcpy(L->d_entries, entries.data(), entries.size() * sizeof(uint2), cudaMemcpyHostToDevice);
+  }
   if (e != cudaSuccess) {
     kbc_destroy(L);
     cudaGetLastError();
     return fail(e == cudaErrorMemoryAllocation ? OAL_E_OUT_OF_MEMORY : OAL_E_CUDA, "D3Q39 level allocation: %s",
                 cudaGetErrorString(e));
   }
-  L->bytes = (int64_t)ncell * (2 * Q + 2 * 3 + 1 + 13) * 4 + (int64_t)nb * 32 + 32;
+  L->bytes = (int64_t)fcell * 2 * Q * 4 + (int64_t)ncell * (2 * 3 + 1 + 13) * 4 + (int64_t)nb * 32 + 32 +
+             (int64_t)entries.size() * 8;
   *out = L;
   return OAL_OK;
 }
@@ -1010,7 +1126,7 @@ void kbc_destroy(KbcLevel* L) {
   cudaSetDevice(L->device);
   release_graph(L);
   for (int i = 0; i < 2; ++i) { cudaFree(L->f[i]); cudaFree(L->vel[i]); }
-  cudaFree(L->rho); cudaFree(L->lam); cudaFree(L->d_mm_part); cudaFree(L->d_mm);
+  cudaFree(L->rho); cudaFree(L->lam); cudaFree(L->d_mm_part); cudaFree(L->d_mm); cudaFree(L->d_entries);
   if (L->cap) cudaStreamDestroy(L->cap);
   cudaGetLastError();
   delete L;
@@ -1121,7 +1237,7 @@ oal_status kbc_step(KbcLevel* L, const oal_step_params* p, void* stream) {
   oal_status s = resolve(p, &a);
   if (s != OAL_OK) return s;
   KBC_TRY(cudaSetDevice(L->device));
-  return enqueue(L, a, static_cast<cudaStream_t>(stream));
+  return enqueue(L, a, p, p->time_step_seed, static_cast<cudaStream_t>(stream));
 }
 
 oal_status kbc_advance(KbcLevel* L, const oal_step_params* p, int32_t n, void* stream) {
@@ -1132,14 +1248,14 @@ oal_status kbc_advance(KbcLevel* L, const oal_step_params* p, int32_t n, void* s
   if (s != OAL_OK) return s;
   KBC_TRY(cudaSetDevice(L->device));
   oal_step_params key = *p;
-  key.time_step_seed = 0;
+  if (!(p->inlet_turbulence > 0.0f && L->n_entries > 0)) key.time_step_seed = 0;  // the seed only feeds inlet noise
   const bool hit = L->exec && L->g_n == n && L->g_parity == L->parity && std::memcmp(&L->g_p, &key, sizeof key) == 0;
   if (!hit) {
     release_graph(L);
     const int start = L->parity;
     KBC_TRY(cudaStreamBeginCapture(L->cap, cudaStreamCaptureModeThreadLocal));
     oal_status es = OAL_OK;
-    for (int i = 0; i < n && es == OAL_OK; ++i) es = enqueue(L, a, L->cap);
+    for (int i = 0; i < n && es == OAL_OK; ++i) es = enqueue(L, a, p, p->time_step_seed + i, L->cap);
     cudaGraph_t graph = nullptr;
     cudaError_t e = cudaStreamEndCapture(L->cap, &graph);
     L->parity = start;

@@ -6,9 +6,22 @@
 
 struct KbcLevel;
 
-// A D3Q39 level on a geometry whose blocks all have their 26 neighbours (d_nbr: device [nb*27],
-// 0-based, the block itself at entry 13).
-oal_status kbc_create(int device, int32_t nb, const int32_t* d_nbr, KbcLevel** out);
+// What a D3Q39 level reads of its geometry. The neighbour table is ghost-indexed: a missing
+// neighbour block is one of n_ghost ghost blocks (ids nb .. nb + n_ghost - 1), whose populations
+// the level's face fill writes before each step; solid cells come from the per-block masks of the
+// D3Q27 geometry (bit 13: the cell itself; bits 4, 10, 12, 14, 16, 22: its face neighbours).
+struct KbcGeometry {
+  int32_t nb = 0, n_ghost = 0, nx = 0, ny = 0, nz = 0;
+  const int32_t* d_nbr = nullptr;       // [nb*27] 0-based, the block itself at entry 13
+  const int32_t* h_nbr = nullptr;       // host copy
+  const void* d_binfo = nullptr;        // [nb] int4 (bx, by, bz, case), 1-based
+  const uint32_t* h_bflags = nullptr;   // [nb] host
+  const uint32_t* d_bflags = nullptr;   // [nb]
+  const int32_t* d_mslot = nullptr;     // [nb] mask slot or -1
+  const uint32_t* d_cmask = nullptr;    // [slots*512]
+  bool has_solid = false;
+};
+oal_status kbc_create(int device, const KbcGeometry& G, KbcLevel** out);
 void kbc_destroy(KbcLevel* L);
 oal_status kbc_init_equilibrium(KbcLevel* L, const double* rho_host, const double* vel_host);
 oal_status kbc_set_state(KbcLevel* L, const double* f_host, const double* rho_host, const double* vel_host);

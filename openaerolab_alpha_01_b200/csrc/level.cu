@@ -973,16 +973,20 @@ oal_status oal_stream_collide(const oal_geometry* g, const oal_level_fields* fl,
 static oal_status create_entropic_level(const oal_geometry* g, int32_t storage, oal_level** out) {
   if (storage != OAL_STORE_F32)
     return set_error(OAL_E_UNSUPPORTED, "the D3Q39 entropic level stores FP32 populations (storage %d)", storage);
-  for (int32_t b = 0; b < g->nb; ++b)
-    if (!(g->h_bflags[(size_t)b] & BF_INTERIOR))
-      return set_error(OAL_E_UNSUPPORTED, "the D3Q39 entropic level needs all 26 neighbour blocks (block %d has a domain face)", b);
-  if (g->n_solid > 0) return set_error(OAL_E_UNSUPPORTED, "the D3Q39 entropic level has no solid cells");
   for (float v : g->h_sponge)
     if (v > 0.0f) return set_error(OAL_E_UNSUPPORTED, "the D3Q39 entropic level has no sponge");
   for (float v : g->h_wdist)
     if (v == v && !(v > 16.0f)) return set_error(OAL_E_UNSUPPORTED, "the D3Q39 entropic level has no wall within 16 cells");
+  if (!g->d_nbr_ghost || g->h_nbrg.size() != (size_t)g->nb * 27 || g->h_binfo.size() != (size_t)g->nb)
+    return set_error(OAL_E_UNSUPPORTED, "the D3Q39 entropic level needs a library-built geometry");
+  KbcGeometry G;
+  G.nb = g->nb; G.n_ghost = g->n_ghost; G.nx = g->nx; G.ny = g->ny; G.nz = g->nz;
+  G.d_nbr = g->d_nbr_ghost; G.h_nbr = g->h_nbrg.data();
+  G.d_binfo = g->d_binfo; G.h_bflags = g->h_bflags.data();
+  G.d_bflags = g->d_bflags; G.d_mslot = g->d_mslot; G.d_cmask = g->d_cmask;
+  G.has_solid = g->n_solid > 0;
   KbcLevel* k = nullptr;
-  oal_status s = kbc_create(g->device, g->nb, g->d_nbr, &k);
+  oal_status s = kbc_create(g->device, G, &k);
   if (s != OAL_OK) return s;
   auto* L = new oal_level();
   L->g = g; L->device = g->device; L->op = OAL_OP_ENTROPIC_D3Q39; L->storage = storage; L->kbc = k;

@@ -2,8 +2,8 @@
 
 Requests arrive (Poisson, rate lambda); each asks for `steps` steps of a cubic domain, either D3Q27
 cumulant — a sphere-in-channel (sphere diameter 0.2 N, inlet u = 0.05, half-way walls with the
-FP64 drag) or a periodic Taylor-Green box — or D3Q39 entropic KBC on a periodic Taylor-Green box
-(the KBC level of this library takes periodic boxes without obstacles). The server keeps every
+FP64 drag) or a periodic Taylor-Green box — or D3Q39 entropic KBC on the same two kinds of domain
+(the KBC channel has no momentum-exchange drag). The server keeps every
 admitted D3Q27 solve resident in one `Batch`, advanced together in ticks of `tick_steps` steps
 (one CUDA graph per tick, one launch per kernel per step for the whole mix), and every admitted
 KBC solve resident as its own level on its own stream, advanced in the same ticks so that its
@@ -30,7 +30,7 @@ import numpy as np
 
 from . import _capi as capi
 from .cases import entropic_taylor_green_case, sphere_channel_case, taylor_green_case
-from .solver import Batch, Geometry, Level
+from .solver import Batch, Geometry, Level, default_entropic_params
 
 # device bytes of one block in a pool (populations x2, rho, velocity x2)
 _POP_BYTES = {"f16": 2, "bf16": 2, "f32": 4, "f64": 8}
@@ -71,8 +71,8 @@ class Request:
 
 def make_requests(n_requests: int = 48, rate: float = 20.0, steps: int = 5000, n_min: int = 32, n_max: int = 192,
                   seed: int = 5, kbc_share: float = 0.0) -> list[Request]:
-    """Poisson arrivals; edge log-uniform in [n_min, n_max] rounded to a multiple of 8; a fraction
-    `kbc_share` of D3Q39 KBC boxes, the rest half channels, half boxes of D3Q27."""
+    """Poisson arrivals; edge log-uniform in [n_min, n_max] rounded to a multiple of 8; half
+    channels, half boxes; a fraction `kbc_share` of them D3Q39 KBC, the rest D3Q27."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
@@ -84,13 +84,18 @@ def make_requests(n_requests: int = 48, rate: float = 20.0, steps: int = 5000, n
         re = float(math.exp(rng.uniform(math.log(100.0), math.log(5000.0))))
         operator = "cumulant"
         if kbc_share > 0.0 and rng.uniform() < kbc_share:
-            operator, kind = "entropic", "box"
+            operator = "entropic"
         out.append(Request(i, t, n, kind, re, steps, operator=operator))
     return out
 
 
 def build_case(req: Request):
     if req.operator == "entropic":
+        if req.kind == "channel":
+            case = sphere_channel_case(req.n, req.n, req.n, diameter=0.2 * req.n, centre_x=req.n / 4.0,
+                                       u_inlet=req.u0, re=req.re)
+            case.params = default_entropic_params(tau=float(case.params.tau), c_wale=0.2, u_inlet=req.u0)
+            return case
         return entropic_taylor_green_case(req.n, u0=req.u0, re=req.re, c_wale=0.2)
     if req.kind == "channel":
         return sphere_channel_case(req.n, req.n, req.n, diameter=0.2 * req.n, centre_x=req.n / 4.0,

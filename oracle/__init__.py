@@ -76,6 +76,7 @@ def lib() -> C.CDLL:
         L.ora_q39_inlet_equilibrium.argtypes = [C.c_float, vp]
         L.ora_q39_collide_cells.argtypes = [i64, vp, vp, vp, vp, vp, vp, vp]
         L.ora_q39_step.argtypes = [i32, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.ora_q39_step_ex.argtypes = [i32, vp, vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -496,11 +497,16 @@ def q39_collide(params, f, g, lam):
 class OracleQ39Level:
     """D3Q39 entropic level in the reference layout, stepped by the CPU restatement (float32):
     f (39, nb, 512), rho (nb, 512), vel (3, nb, 512), lam (13, nb, 512) with NaN = no warm start;
-    nbr (27, nb) 1-based with every neighbour present."""
+    nbr (27, nb) 1-based. Without `coords` every neighbour must be present (periodic box); with
+    `coords` (nb, 3, 1-based block coordinates) and `shape` (cells) missing neighbours are domain
+    faces, and `obstacle` (nb, 512) marks solid cells."""
 
-    def __init__(self, nbr):
+    def __init__(self, nbr, coords=None, shape=None, obstacle=None):
         self.nbr = np.ascontiguousarray(nbr, np.int32)
         self.nb = self.nbr.shape[1]
+        self.coords = None if coords is None else np.ascontiguousarray(coords, np.int32)
+        self.shape = shape
+        self.obstacle = None if obstacle is None else np.ascontiguousarray(obstacle, np.uint8)
         nb = self.nb
         self.f = np.zeros((39, nb, 512), np.float32)
         self.g = np.zeros_like(self.f)
@@ -521,8 +527,15 @@ class OracleQ39Level:
 
     def step(self, params, n=1):
         for _ in range(n):
-            lib().ora_q39_step(self.nb, _p(self.nbr), C.addressof(params), _p(self.f), _p(self.g), _p(self.vel),
-                               _p(self.vel_new), _p(self.rho), _p(self.lam))
+            if self.coords is None:
+                lib().ora_q39_step(self.nb, _p(self.nbr), C.addressof(params), _p(self.f), _p(self.g), _p(self.vel),
+                                   _p(self.vel_new), _p(self.rho), _p(self.lam))
+            else:
+                nx, ny, nz = self.shape
+                lib().ora_q39_step_ex(self.nb, _p(self.nbr), _p(self.coords), nx, ny, nz,
+                                      None if self.obstacle is None else _p(self.obstacle), C.addressof(params),
+                                      _p(self.f), _p(self.g), _p(self.vel), _p(self.vel_new), _p(self.rho),
+                                      _p(self.lam))
             self.f, self.g = self.g, self.f
             self.vel, self.vel_new = self.vel_new, self.vel
         return self

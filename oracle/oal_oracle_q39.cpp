@@ -1,7 +1,8 @@
 // oal_oracle_q39.cpp — CPU ORACLE (test infrastructure only) of the reference's D3Q39 entropic KBC
 // level step (OpenAeroLab src/collision, Julia/KernelAbstractions, GPU), restated in binary32 with
-// -ffp-contract=off, for a level whose blocks all have their 26 neighbours (periodic boxes, no
-// obstacle, sponge, wall model, AMR parent, thermal coupling or lattice shift).
+// -ffp-contract=off, for a level without sponge, wall model, AMR parent, thermal coupling or
+// lattice shift: periodic boxes (every block has its 26 neighbours), and levels with domain faces
+// and obstacle cells (ora_q39_step_ex).
 //
 // Followed (paths inside the reference project):
 //   D3Q39 velocity set, weights, opposites ........ src/collision/lattice.jl:177-262
@@ -9,6 +10,12 @@
 //   staleness gate, evaluation, mass correction ... src/collision/physics_utils.jl:493-796
 //   host inlet equilibrium (NaN-reset populations)  physics_utils.jl:280-460, timestep.jl:1169-1188
 //   pull over |c| <= 3 through the neighbour table  src/collision/kernel_entropic_d3q39.jl:898-1290
+//   domain faces (default boundary options) ...... kernel_entropic_d3q39.jl:983-1278 (kbc::face_value)
+//   inlet-face mass + momentum pin ................ kernel_entropic_d3q39.jl:1313-1352,
+//                                                   physics_utils.jl:830-900 (kbc::four_moment_pin)
+//   obstacle cells (full-way bounce-back) ......... kernel_entropic_d3q39.jl:1602-1613
+//   gradient neighbours: own value across a missing
+//   block or into a solid cell .................... physics_utils.jl:1981-2035
 //   macros, density floor, NaN reset .............. kernel_entropic_d3q39.jl:1616-1650
 //   macro realizability clamp (far bulk), equilibrium
 //   velocity cap .................................. kernel_entropic_d3q39.jl:2112-2287
@@ -640,6 +647,30 @@ void velocity_gradient(int b, int x, int y, int z, int nb, const int32_t* nbr, c
     for (int bb = 0; bb < 3; ++bb) g[3 * a + bb] = 0.5f * (ue[bb][0][a] - ue[bb][1][a]);
 }
 
+// the same with the level's faces and obstacles: a missing neighbour block or a solid neighbour
+// cell contributes the own velocity (get_velocity_neighbor_fluid, physics_utils.jl:1981-2035)
+void velocity_gradient_ex(int b, int x, int y, int z, int nb, const int32_t* nbr, const uint8_t* obst,
+                          const float* vel, int64_t N, float* g) {
+  const int64_t own = x + 8 * y + 64 * z + 512 * (int64_t)b;
+  float ue[3][2][3];
+  for (int ax = 0; ax < 3; ++ax)
+    for (int s = 0; s < 2; ++s) {
+      int p[3] = {x, y, z};
+      p[ax] += s == 0 ? 1 : -1;
+      const int ox = p[0] < 0 ? -1 : (p[0] > 7 ? 1 : 0), oy = p[1] < 0 ? -1 : (p[1] > 7 ? 1 : 0),
+                oz = p[2] < 0 ? -1 : (p[2] > 7 ? 1 : 0);
+      const int bo = (ox | oy | oz) == 0 ? b : nbr[b + (int64_t)nb * ((ox + 1) + 3 * (oy + 1) + 9 * (oz + 1))] - 1;
+      int64_t c = own;
+      if (bo >= 0) {
+        const int64_t cn = (p[0] - 8 * ox) + 8 * (p[1] - 8 * oy) + 64 * (p[2] - 8 * oz) + 512 * (int64_t)bo;
+        if (!(obst && obst[cn])) c = cn;
+      }
+      for (int a = 0; a < 3; ++a) ue[ax][s][a] = vel[c + N * a];
+    }
+  for (int a = 0; a < 3; ++a)
+    for (int bb = 0; bb < 3; ++bb) g[3 * a + bb] = 0.5f * (ue[bb][0][a] - ue[bb][1][a]);
+}
+
 }  // namespace
 
 extern "C" {
@@ -707,6 +738,69 @@ void ora_q39_step(int32_t nb, const int32_t* nbr, const oal_step_params* P, cons
       float g[9];
       velocity_gradient(b, x, y, z, nb, nbr, vel_in, N, g);
       const int64_t ci = cell + 512 * (int64_t)b;
+      float la[13];
+      for (int m = 0; m < 13; ++m) la[m] = lam[ci + N * m];
+      float fo[Q];
+      CellOut o;
+      collide_cell(f, g, *P, f_eq_inlet, la, fo, o);
+      for (int m = 0; m < 13; ++m) lam[ci + N * m] = la[m];
+      for (int k = 0; k < Q; ++k) fout[ci + N * k] = fo[k];
+      rho_out[ci] = o.rho;
+      for (int a = 0; a < 3; ++a) vel_out[ci + N * a] = o.u[a];
+    }
+}
+
+// One step of a level with domain faces and obstacle cells, reference layout as ora_q39_step;
+// nbr (nb,27) 1-based with 0 for a missing neighbour block, coords (nb,3) 1-based block
+// coordinates, domain nx x ny x nz cells, obstacle (8,8,8,nb) uint8 or null.
+void ora_q39_step_ex(int32_t nb, const int32_t* nbr, const int32_t* coords, int32_t nx, int32_t ny, int32_t nz,
+                     const uint8_t* obstacle, const oal_step_params* P, const float* fin, float* fout,
+                     const float* vel_in, float* vel_out, float* rho_out, float* lam) {
+  build_tables();
+  const int64_t N = (int64_t)nb * 512;
+  float f_eq_inlet[Q];
+  inlet_equilibrium(P->u_inlet, f_eq_inlet);
+  // moments of the inlet equilibrium, the target of the inlet-face pin (:1315-1326)
+  float trho = 0.0f, tjx = 0.0f, tjy = 0.0f, tjz = 0.0f;
+  for (int k = 0; k < Q; ++k) {
+    const float fe = f_eq_inlet[k];
+    trho += fe;
+    tjx += fe * float(CX[k]);
+    tjy += fe * float(CY[k]);
+    tjz += fe * float(CZ[k]);
+  }
+  kbc::FaceParams F{nx, ny, nz, P->ymin_wall_bc, P->transverse_freestream, P->time_step_seed,
+                    P->transverse_freestream_blend, P->inlet_turbulence, P->u_inlet};
+#pragma omp parallel for schedule(static)
+  for (int b = 0; b < nb; ++b)
+    for (int cell = 0; cell < 512; ++cell) {
+      const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
+      const int gx = (coords[3 * b] - 1) * 8 + x + 1, gy = (coords[3 * b + 1] - 1) * 8 + y + 1,
+                gz = (coords[3 * b + 2] - 1) * 8 + z + 1;
+      const int64_t ci = cell + 512 * (int64_t)b;
+      float f[Q];
+      bool saw_inlet = false;
+      for (int k = 0; k < Q; ++k) {
+        const int sx = x - CX[k], sy = y - CY[k], sz = z - CZ[k];
+        const int ox = sx < 0 ? -1 : (sx > 7 ? 1 : 0), oy = sy < 0 ? -1 : (sy > 7 ? 1 : 0), oz = sz < 0 ? -1 : (sz > 7 ? 1 : 0);
+        const int bo = (ox | oy | oz) == 0 ? b : nbr[b + (int64_t)nb * ((ox + 1) + 3 * (oy + 1) + 9 * (oz + 1))] - 1;
+        if (bo >= 0) {
+          f[k] = fin[(sx - 8 * ox) + 8 * (sy - 8 * oy) + 64 * (sz - 8 * oz) + 512 * (int64_t)bo + N * k];
+        } else {
+          saw_inlet = saw_inlet || gx - CX[k] < 1;
+          f[k] = kbc::face_value(F, fin + ci, (int)N, f_eq_inlet, k, gx, gy, gz);
+        }
+      }
+      if (obstacle && obstacle[ci]) {
+        // simple bounce-back inside the obstacle; the multiplier cache is left as it is
+        vel_out[ci] = 0.0f; vel_out[ci + N] = 0.0f; vel_out[ci + 2 * N] = 0.0f;
+        rho_out[ci] = 1.0f;
+        for (int k = 0; k < Q; ++k) fout[ci + N * k] = f[OPP[k]];
+        continue;
+      }
+      if (saw_inlet && gx == 1) kbc::four_moment_pin(f, 1, trho, tjx, tjy, tjz);
+      float g[9];
+      velocity_gradient_ex(b, x, y, z, nb, nbr, obstacle, vel_in, N, g);
       float la[13];
       for (int m = 0; m < 13; ++m) la[m] = lam[ci + N * m];
       float fo[Q];

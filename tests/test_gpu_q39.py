@@ -188,10 +188,6 @@ def test_lambda_cache_round_trip_and_mass_momentum(env):
 def test_refused_configurations(env):
     oracle, solver = env
     from openaerolab_alpha_01_b200._capi import OALError
-    dom = solver.build_box(2, 2, 2, periodic=(True, False, True))
-    geom = solver.Geometry(dom)
-    with pytest.raises(OALError):
-        solver.Level(geom, "entropic")           # domain faces
     dom = solver.build_box(2, 2, 2, periodic=(True, True, True))
     geom = solver.Geometry(dom)
     with pytest.raises(OALError):
@@ -238,3 +234,61 @@ def test_conservation_and_viscosity_at_scale(env):
     assert np.max(np.abs(m1[1:] - m0[1:])) / (n * 200) < 1e-7
     nu = np.log(amp[0] / amp[1]) / 100 / k ** 2
     assert abs(nu / (CS2 * (tau - 0.5)) - 1) < 0.03, nu
+
+
+def channel_pair(env, **kw):
+    """A 32 x 16 x 16 channel with a sphere (diameter 6): velocity inlet, zero-gradient outlet,
+    mirror faces in y and z, full-way bounce-back in the sphere."""
+    oracle, solver = env
+    from openaerolab_alpha_01_b200.cases import sphere_channel_case
+    case = sphere_channel_case(32, 16, 16, diameter=6.0, centre_x=12.0, u_inlet=0.05, re=200.0)
+    d = case.dom
+    geom = solver.Geometry(d)
+    lvl = solver.Level(geom, "entropic")
+    rng = np.random.default_rng(5)
+    vel = case.vel + 0.005 * rng.standard_normal(case.vel.shape) * (d.obstacle == 0)
+    lvl.init_equilibrium(case.rho, vel)
+    ora = oracle.OracleQ39Level(d.neighbor_table, d.coords, d.shape, d.obstacle).init_equilibrium(case.rho, vel)
+    p = solver.default_entropic_params(tau=0.56, c_wale=0.2, u_inlet=0.05, **kw)
+    return d, geom, lvl, ora, p
+
+
+FACE_CONFIGS = {
+    "faces": dict(),
+    "inlet_noise": dict(inlet_turbulence=0.05),
+    "ground_wall": dict(ymin_wall_bc=1),
+    "transverse_freestream": dict(transverse_freestream=1, transverse_freestream_blend=0.3),
+}
+
+
+@pytest.mark.parametrize("name", list(FACE_CONFIGS))
+def test_channel_faces_and_obstacle_bitwise(env, name):
+    """Domain faces (inlet with its mass/momentum pin, outlet, mirrors, ground, transverse
+    freestream, inlet noise) and the obstacle's bounce-back: the oracle's bits after 4 steps."""
+    d, geom, lvl, ora, p = channel_pair(env, **FACE_CONFIGS[name])
+    for i in range(4):
+        p.time_step_seed = 7 + i
+        lvl.step(p)
+        ora.step(p)
+    assert_same_state(lvl, ora)
+    _, _, v = lvl.state()
+    assert np.all(v[:, d.obstacle.astype(bool)] == 0.0)
+    assert np.all(np.isfinite(ora.f))
+
+
+def test_channel_advance_graph_equals_steps(env):
+    """n steps in one graph advance the noise seed by one per step, as single steps do."""
+    d, geom, a, _, p = channel_pair(env, inlet_turbulence=0.05)
+    oracle, solver = env
+    b = solver.Level(geom, "entropic")
+    fa, ra, va = a.state()
+    b.set_state(fa, ra, va)
+    p.time_step_seed = 3
+    a.advance(p, 4)
+    for i in range(4):
+        q = solver.default_entropic_params(tau=0.56, c_wale=0.2, u_inlet=0.05, inlet_turbulence=0.05)
+        q.time_step_seed = 3 + i
+        b.step(q)
+    fa, ra, va = a.state()
+    fb, rb, vb = b.state()
+    assert same_bits(fa, fb) and same_bits(ra, rb) and same_bits(va, vb)

@@ -241,3 +241,26 @@ def test_transonic_guards_keep_state_finite(oracle_lib):
     assert np.all(np.isfinite(lvl.f)) and lvl.f.min() > 0
     m1 = lvl.mass_momentum()
     assert abs(m1[0] - m0[0]) / (nb * 512) < 1e-5
+
+
+def test_channel_inlet_pin_and_obstacle(oracle_lib, t):
+    """A channel with domain faces and a sphere (kernel_entropic_d3q39.jl:983-1352, 1602-1613):
+    the cells of the inlet face leave the step with the inlet equilibrium's mass (their pulled
+    populations are pinned to its mass and momentum before the collision, which keeps mass; the
+    momentum then relaxes with the collision), solid cells hold the bounce-back of their pulls with
+    zero velocity and unit density, and the state stays finite."""
+    from openaerolab_alpha_01_b200 import solver
+    from openaerolab_alpha_01_b200.cases import sphere_channel_case
+    case = sphere_channel_case(32, 16, 16, diameter=6.0, centre_x=12.0, u_inlet=0.05, re=200.0)
+    d = case.dom
+    O = oracle_lib.OracleQ39Level(d.neighbor_table, d.coords, d.shape, d.obstacle).init_equilibrium(case.rho, case.vel)
+    p = solver.default_entropic_params(tau=0.56, c_wale=0.2, u_inlet=0.05)
+    O.step(p, 3)
+    feq_in = oracle_lib.q39_inlet_equilibrium(0.05)
+    gx, _, _ = d.cell_positions()
+    solid = d.obstacle.astype(bool)
+    inlet = (gx == 1) & ~solid
+    assert inlet.sum() == 16 * 16
+    assert np.allclose(O.rho[inlet], feq_in.astype(np.float64).sum(), rtol=2e-6)
+    assert np.all(O.vel[:, solid] == 0.0) and np.all(O.rho[solid] == 1.0)
+    assert np.all(np.isfinite(O.f)) and np.all(O.f[:, ~solid] > 0)
