@@ -462,6 +462,9 @@ __global__ void __launch_bounds__(256) k_kbc_fill(const KbcFillArgs a) {
 // live in its shared-memory column (the pulled f, then a_k, then the post-collision values) and the
 // per-direction loops run rolled over the CTA's tables, which keeps the step's code small enough to
 // stay in the instruction cache. f_eq is recomputed from its multipliers where a pass needs it.
+// EDGES: the level has domain faces or solid cells (the pin, bounce-back and gradient fall-backs
+// are compiled in); periodic boxes without obstacles run the instance without them.
+template <bool EDGES>
 __global__ void __launch_bounds__(kThreads, KBC_MIN_BLOCKS) k_kbc_step(const KbcArgs a) {
   __shared__ Tables T;
   __shared__ int32_t s_nbr[27];
@@ -479,7 +482,8 @@ __global__ void __launch_bounds__(kThreads, KBC_MIN_BLOCKS) k_kbc_step(const Kbc
   const int64_t N = (int64_t)a.nb * 512;
   const int64_t ci = (int64_t)b * 512 + cell;
   // solid cells: the cell itself (bit 13) and its face neighbours (WALE stencil)
-  const uint32_t solid_mask = (a.cmask && (a.bflags[b] & kNearSolid)) ? a.cmask[(int64_t)a.mslot[b] * 512 + cell] : 0u;
+  const uint32_t solid_mask =
+      (EDGES && a.cmask && (a.bflags[b] & kNearSolid)) ? a.cmask[(int64_t)a.mslot[b] * 512 + cell] : 0u;
 
   // STEP 1-2: pull, moments, density floor and NaN reset (:898-1290, 1616-1650)
   float rho, ux, uy, uz, inv_rho;
@@ -500,7 +504,7 @@ __global__ void __launch_bounds__(kThreads, KBC_MIN_BLOCKS) k_kbc_step(const Kbc
       jy += f * float(cy);
       jz += f * float(cz);
     }
-    if (solid_mask & (1u << 13)) {
+    if (EDGES && (solid_mask & (1u << 13))) {
       // simple bounce-back inside the obstacle (:1602-1613); the multiplier cache is left as it is
       a.vout[ci] = 0.0f; a.vout[ci + N] = 0.0f; a.vout[ci + 2 * N] = 0.0f;
       a.rho[ci] = 1.0f;
@@ -508,7 +512,7 @@ __global__ void __launch_bounds__(kThreads, KBC_MIN_BLOCKS) k_kbc_step(const Kbc
       for (int k = 0; k < Q; ++k) a.fout[((int64_t)b * Q + k) * 512 + cell] = sf[kopp(k) * kThreads];
       return;
     }
-    if (a.faces && x == 0 && s_nbr[nbr13(-1, 0, 0)] >= a.nb && a.binfo[b].x == 1) {
+    if (EDGES && a.faces && x == 0 && s_nbr[nbr13(-1, 0, 0)] >= a.nb && a.binfo[b].x == 1) {
       // a cell on the inlet face (global x = 1): mass and momentum pinned to the inlet
       // equilibrium's (:1313-1352), then the moments again
       kbc::four_moment_pin(sf, kThreads, a.trho, a.tjx, a.tjy, a.tjz);
@@ -620,7 +624,7 @@ __global__ void __launch_bounds__(kThreads, KBC_MIN_BLOCKS) k_kbc_step(const Kbc
         // a neighbour outside the domain (ghost block) or in a solid cell contributes the own
         // velocity (physics_utils.jl:1981-2035); mask bit of the D3Q27 direction whose source it is
         const int sbit = ax == 0 ? (s == 0 ? 12 : 14) : ax == 1 ? (s == 0 ? 10 : 16) : (s == 0 ? 4 : 22);
-        const bool own = bo >= a.nb || ((solid_mask >> sbit) & 1u);
+        const bool own = EDGES && (bo >= a.nb || ((solid_mask >> sbit) & 1u));
         const int64_t c = own ? ci : ((px & 7) | ((py & 7) << 3) | ((pz & 7) << 6)) + 512 * (int64_t)bo;
 #pragma unroll
         for (int comp = 0; comp < 3; ++comp) (s == 0 ? up : um)[ax][comp] = a.vin[c + N * comp];
@@ -1053,7 +1057,8 @@ oal_status enqueue(KbcLevel* L, const KbcArgs& base, const oal_step_params* p_in
     k_kbc_fill<<<(unsigned)((L->n_entries + 255) / 256), 256, 0, st>>>(fa);
     KBC_TRY(cudaGetLastError());
   }
-  k_kbc_step<<<(unsigned)L->nb * 4, kThreads, 0, st>>>(a);
+  if (a.faces || a.cmask) k_kbc_step<true><<<(unsigned)L->nb * 4, kThreads, 0, st>>>(a);
+  else k_kbc_step<false><<<(unsigned)L->nb * 4, kThreads, 0, st>>>(a);
   KBC_TRY(cudaGetLastError());
   L->parity ^= 1;
   return OAL_OK;
