@@ -22,6 +22,7 @@ reference's generator restated natively); refined meshes are refused (OAL_E_UNSU
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -708,3 +709,180 @@ def benchmark_naca(steps: int = 100, warmup: int = 20, precision=np.float32, **k
 
 if __name__ == "__main__":
     main()
+
+
+# ---- the mesh file (octree.jl:158-233) ---------------------------------------------------------
+MESH_MAGIC = b"OCTQ19M\0"
+MESH_FORMAT = 5
+
+
+def _w_i64(buf, v):
+    buf += np.array([v], "<i8").tobytes()
+
+
+def _w_string(buf, s: str):
+    b = s.encode()
+    _w_i64(buf, len(b))
+    buf += b
+
+
+def _w_array(buf, a: np.ndarray, julia_dims):
+    """_write_array: ndims, the dims in Julia's order, the elements in memory order (the C-order
+    array whose shape is julia_dims reversed)."""
+    _w_i64(buf, len(julia_dims))
+    for d in julia_dims:
+        _w_i64(buf, int(d))
+    buf += np.ascontiguousarray(a).tobytes()
+
+
+def _toml(counts: dict) -> str:
+    """The generator's counts as TOML: integers, and per_level as an array of tables."""
+    lines = [f"{k} = {int(v)}" for k, v in counts.items() if not isinstance(v, (list, dict))]
+    for t in counts.get("per_level", []):
+        lines.append("")
+        lines.append("[[per_level]]")
+        lines += [f"{k} = {int(v)}" for k, v in t.items()]
+    return "\n".join(lines) + "\n"
+
+
+def write_mesh(path, mesh: OctMesh, triangles=None, offset=(0.0, 0.0, 0.0), config_sha: str = "",
+               stl_sha: str = "") -> str:
+    """Write `mesh` as the reference's mesh file (write_mesh, octree.jl:172-204): magic, format,
+    domain, offset, periodic axes, the two hashes, the counts (TOML), the placed triangles and every
+    level's tables in Julia's element order, followed by the SHA-256 of all that. Returns the hex
+    digest."""
+    import hashlib
+    spec = mesh.spec
+    tri = np.zeros((0, 3, 3)) if triangles is None else np.asarray(triangles, np.float64).reshape(-1, 3, 3)
+    buf = bytearray(MESH_MAGIC)
+    _w_i64(buf, MESH_FORMAT)
+    buf += np.asarray(spec.domain, "<f8").tobytes()
+    buf += np.asarray(offset, "<f8").tobytes()
+    buf += np.asarray([bool(p) for p in spec.periodic], np.uint8).tobytes()
+    _w_string(buf, config_sha)
+    _w_string(buf, stl_sha)
+    _w_string(buf, _toml(mesh.counts))
+    _w_i64(buf, tri.shape[0])
+    _w_array(buf, tri.astype("<f8"), (3, 3, tri.shape[0]))
+    _w_i64(buf, mesh.nlevels)
+    for lv in mesh.levels:
+        _w_i64(buf, lv.level)
+        buf += np.array([lv.dx], "<f8").tobytes()
+        for v in lv.n:
+            _w_i64(buf, v)
+        _w_i64(buf, lv.nocts)
+        no = lv.nocts
+        _w_array(buf, lv.origin.astype("<i4"), (3, no))
+        _w_array(buf, (lv.real != 0).astype(np.uint8), (no,))
+        _w_array(buf, lv.kind.astype(np.uint8), (8, no))
+        _w_array(buf, lv.face.astype(np.uint8), (8, no))
+        _w_array(buf, lv.onbr.astype("<i4"), (27, no))
+        _w_array(buf, lv.cutidx.astype("<i4"), (8, no))
+        _w_array(buf, lv.special.astype("<u4"), (8, no))
+        for name, dt in (("cut_slot", "<i4"), ("cut_off", "<i4"), ("cut_dir", np.uint8), ("cut_q", "<f4"),
+                         ("cut_tri", "<i4")):
+            a = getattr(lv, name).astype(dt)
+            _w_array(buf, a, (a.shape[0],))
+        cp = (lv.cut_partner != 0).astype(np.uint8)
+        _w_array(buf, cp, (cp.shape[0],))
+        ng, nr = lv.ghost_slot.shape[0], lv.restrict_slot.shape[0]
+        _w_array(buf, lv.ghost_slot.astype("<i4"), (ng,))
+        _w_array(buf, lv.ghost_donor.astype("<i4"), (64, ng))
+        _w_array(buf, lv.ghost_w.astype("<f4"), (64, ng))
+        _w_array(buf, lv.restrict_slot.astype("<i4"), (nr,))
+        _w_array(buf, lv.restrict_src.astype("<i4"), (64, nr))
+        _w_array(buf, (lv.restrict_cubic != 0).astype(np.uint8), (nr,))
+    digest = hashlib.sha256(bytes(buf)).digest()
+    tmp = str(path) + ".tmp"
+    with open(tmp, "wb") as io:
+        io.write(bytes(buf))
+        io.write(digest)
+    os.replace(tmp, path)
+    return digest.hex()
+
+
+class _Reader:
+    def __init__(self, data: bytes):
+        self.d, self.o = data, 0
+
+    def take(self, n: int) -> bytes:
+        b = self.d[self.o:self.o + n]
+        if len(b) != n:
+            raise ValueError("mesh file ends early")
+        self.o += n
+        return b
+
+    def i64(self) -> int:
+        return int(np.frombuffer(self.take(8), "<i8")[0])
+
+    def f64(self, n=1):
+        return np.frombuffer(self.take(8 * n), "<f8").copy()
+
+    def string(self) -> str:
+        return self.take(self.i64()).decode()
+
+    def array(self, dt):
+        nd = self.i64()
+        dims = [self.i64() for _ in range(nd)]
+        n = int(np.prod(dims)) if dims else 1
+        a = np.frombuffer(self.take(n * np.dtype(dt).itemsize), dt).copy()
+        return a.reshape(tuple(reversed(dims)))
+
+
+def read_mesh(path, faces=("periodic",) * 6) -> OctMesh:
+    """Read a mesh file written by the reference's write_mesh or by write_mesh here (read_mesh,
+    octree.jl:206-233): checks the SHA-256 trailer, the magic and the format. The domain-face
+    conditions are not part of the file; `faces` names them (-x +x -y +y -z +z) as MeshSpec does.
+    The triangles are returned as the mesh's `triangles` (ntri, 3, 3)."""
+    import hashlib
+    import tomllib
+    data = open(path, "rb").read()
+    if len(data) <= 32:
+        raise ValueError(f"{path} is not a mesh file")
+    if hashlib.sha256(data[:-32]).digest() != data[-32:]:
+        raise ValueError(f"{path}: hash mismatch (the file is damaged or truncated)")
+    r = _Reader(data[:-32])
+    if r.take(len(MESH_MAGIC)) != MESH_MAGIC:
+        raise ValueError(f"{path}: not an octree D3Q19 mesh")
+    fmt = r.i64()
+    if fmt != MESH_FORMAT:
+        raise ValueError(f"{path}: mesh format {fmt}, expected {MESH_FORMAT}")
+    domain = tuple(float(v) for v in r.f64(3))
+    offset = tuple(float(v) for v in r.f64(3))
+    periodic = tuple(bool(v) for v in np.frombuffer(r.take(3), np.uint8))
+    config_sha, stl_sha = r.string(), r.string()
+    counts = tomllib.loads(r.string())
+    nt = r.i64()
+    tri = r.array("<f8").reshape(nt, 3, 3)
+    nl = r.i64()
+    face_codes = [capi.Q19_FACE_NAMES[f] for f in faces]
+    levels = []
+    for _ in range(nl):
+        level = r.i64()
+        dx = float(r.f64(1)[0])
+        n = tuple(r.i64() for _ in range(3))
+        nocts = r.i64()
+        arrays = {"origin": r.array("<i4"), "real": r.array(np.uint8), "kind": r.array(np.uint8),
+                  "face": r.array(np.uint8), "onbr": r.array("<i4"), "cutidx": r.array("<i4"),
+                  "special": r.array("<u4")}
+        for name, dt in (("cut_slot", "<i4"), ("cut_off", "<i4"), ("cut_dir", np.uint8), ("cut_q", "<f4"),
+                         ("cut_tri", "<i4"), ("cut_partner", np.uint8), ("ghost_slot", "<i4"),
+                         ("ghost_donor", "<i4"), ("ghost_w", "<f4"), ("restrict_slot", "<i4"),
+                         ("restrict_src", "<i4"), ("restrict_cubic", np.uint8)):
+            arrays[name] = r.array(dt)
+        arrays = {k: np.ascontiguousarray(v.astype(v.dtype.newbyteorder("="))) for k, v in arrays.items()}
+        if arrays["onbr"].shape[0] != nocts:
+            raise ValueError(f"{path}: level {level} holds {arrays['onbr'].shape[0]} octs, header says {nocts}")
+        per = counts.get("per_level", [])
+        m = Mesh(arrays, n, dx, face_codes, nt, per[level - 1] if level - 1 < len(per) else {})
+        m.level = level
+        m.domain = tuple(v * dx for v in n)
+        levels.append(m)
+    if r.o != len(r.d):
+        raise ValueError(f"{path}: {len(r.d) - r.o} bytes after the last level")
+    spec = MeshSpec(domain=domain, periodic=periodic, levels=nl, dx_finest=levels[-1].dx if levels else 1.0,
+                    faces=tuple(faces))
+    mesh = OctMesh(levels, {k: v for k, v in counts.items()}, spec)
+    mesh.triangles = tri
+    mesh.offset, mesh.config_sha, mesh.stl_sha = offset, config_sha, stl_sha
+    return mesh
