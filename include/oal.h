@@ -106,8 +106,12 @@ enum { OAL_LIMITER_NONE = 0, OAL_LIMITER_FACTORED = 1, OAL_LIMITER_POSITIVITY = 
  *            rebuilt as f_eq(rho, u_wall = 0) + (1 - 1/tau) w_k 4.5 Q_k : Pi_neq (Pi_neq of the
  *            post-collision populations about (rho, 0), times grad_pineq_scale), floored at
  *            1e-12, and its velocity output set to 0 (wall velocity mode "none", the default).
- *            No momentum-exchange force is accumulated (forces come from HALFWAY). */
-enum { OAL_SOLID_FULLWAY = 0, OAL_SOLID_HALFWAY = 1, OAL_SOLID_GRAD = 2 };
+ *            No momentum-exchange force is accumulated (forces come from HALFWAY).
+ *   BOUZIDI: FULLWAY, then the linear Bouzidi correction of the reference's default bc_scheme
+ *            "bouzidi_linear" (geometry/bouzidi_kernel.jl:150-380, called from timestep.jl:1752-1768)
+ *            on the boundary cells and q values attached by oal_level_set_bouzidi; no attached
+ *            cells = FULLWAY. No momentum-exchange force is accumulated. */
+enum { OAL_SOLID_FULLWAY = 0, OAL_SOLID_HALFWAY = 1, OAL_SOLID_GRAD = 2, OAL_SOLID_BOUZIDI = 3 };
 
 /* Scalar step parameters: the scalars of `_kargs` (timestep.jl:1238-1478) that the
  * D3Q27 level-1 path reads. Field meaning and units are the reference's (lattice units). */
@@ -260,6 +264,27 @@ oal_status oal_level_advance(oal_level* L, const oal_step_params* p, int32_t n_s
 /* Momentum-exchange force of the last step that collected it (lattice units, FP64).
  * Synchronises the level's stream. */
 oal_status oal_level_get_forces(oal_level* L, double out[3]);
+
+/* Boundary cells and link fractions of the linear Bouzidi wall (OAL_SOLID_BOUZIDI). Replaces
+ * the per-level BouzidiDataSparse of the reference (geometry/bouzidi_common.jl:15-23, built by
+ * compute_bouzidi_qmap_sparse, geometry/bouzidi_setup.jl:175-390) and the scalars that
+ * apply_bouzidi_correction! takes (geometry/bouzidi_kernel.jl:382-432).
+ *   cell_block, cell_x, cell_y, cell_z: n_cells 1-based entries (block of the level, x, y, z in
+ *     1..8), the reference's bouzidi_cell_* arrays;
+ *   q_half: n_cells x 27 IEEE binary16 link fractions, direction fastest in the D3Q27 order of
+ *     the level (q_map[x, y, z, b, k] of each listed cell); a link is corrected when
+ *     q_min_threshold < q <= 1;
+ *   ff_fallback: 0 halfway_bb (default), 1 wall_eq, 2 bounce_back (config ff_fallback);
+ *   limiter_rel_cap, limiter_abs_cap: wall_pop_limiter_rel_cap / _abs_cap (0 = off).
+ * After every step of L with solid_bc OAL_SOLID_BOUZIDI, for each listed cell x and link k:
+ * f_out[x, opp k] = 2q f*_k(x) + (1-2q) f*_k(x - c_k) if q < 1/2 (the fall-back when x - c_k is
+ * solid or absent), else f*_k(x)/(2q) + (2q-1)/(2q) f*_opp k(x), f* the step's post-collision
+ * populations. n_cells = 0 detaches. Plain levels only (no parent, not entropic). Copies the
+ * arrays; invalidates L's captured step graphs. */
+oal_status oal_level_set_bouzidi(oal_level* L, int32_t n_cells, const int32_t* cell_block, const int32_t* cell_x,
+                                 const int32_t* cell_y, const int32_t* cell_z, const uint16_t* q_half,
+                                 float q_min_threshold, int32_t ff_fallback, float limiter_rel_cap,
+                                 float limiter_abs_cap);
 /* Non-blocking variant: enqueue the copy of the force into a host buffer (pinned for overlap). */
 oal_status oal_level_get_forces_async(oal_level* L, double* host_out3, void* stream);
 /* FP64 on-device reduction of the current state: out = {mass, px, py, pz} over fluid cells. */

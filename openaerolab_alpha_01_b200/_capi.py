@@ -47,6 +47,7 @@ OAL_LEVEL_DENSE = 1
 OAL_SOLID_FULLWAY = 0
 OAL_SOLID_HALFWAY = 1
 OAL_SOLID_GRAD = 2
+OAL_SOLID_BOUZIDI = 3
 
 STORAGE_NAMES = {"f32": OAL_STORE_F32, "f16": OAL_STORE_F16_DEV, "bf16": OAL_STORE_BF16_DEV, "f64": OAL_STORE_F64}
 
@@ -257,6 +258,9 @@ _SIGNATURES = {
     "oal_level_step": (C.c_int32, [C.c_void_p, C.POINTER(StepParams), C.c_void_p]),
     "oal_level_advance": (C.c_int32, [C.c_void_p, C.POINTER(StepParams), C.c_int32, C.c_void_p]),
     "oal_level_get_forces": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double)]),
+    "oal_level_set_bouzidi": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                          C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_uint16),
+                                          C.c_float, C.c_int32, C.c_float, C.c_float]),
     "oal_level_get_forces_async": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "oal_level_mass_momentum": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double)]),
     "oal_level_device_state": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),

@@ -72,7 +72,8 @@ enum CaseFlags : uint32_t {
   CF_PERIODIC_X = 1u << 15,  // periodic axes of a dense (box) level
   CF_PERIODIC_Y = 1u << 16,
   CF_PERIODIC_Z = 1u << 17,
-  CF_GRAD_WALL = 1u << 18    // Grad-reconstruction wall on fluid cells with links into solids
+  CF_GRAD_WALL = 1u << 18,   // Grad-reconstruction wall on fluid cells with links into solids
+  CF_BOUZIDI = 1u << 19      // linear Bouzidi correction after the step (the step itself is full-way)
 };
 
 struct CaseParams {
@@ -178,5 +179,22 @@ struct StepArgs {
 __host__ __device__ __forceinline__ int64_t dense_idx(const StepArgs& a, int X, int Y, int Z) {
   return ((int64_t)Z * a.PY + Y) * a.PX + X;
 }
+
+// Element index of (block b, cell, direction k) in either population layout of a level.
+struct PopIndex {
+  const int4* binfo;
+  int dense;
+  int PX, PY;
+  int64_t bst, kst;
+  __device__ __forceinline__ int64_t operator()(int64_t b, int cell, int k) const {
+    if (dense) {
+      const int4 bi = binfo[b];
+      const int X = (bi.x - 1) * kBS + (cell & 7) + 8, Y = (bi.y - 1) * kBS + ((cell >> 3) & 7) + 1,
+                Z = (bi.z - 1) * kBS + (cell >> 6) + 1;
+      return ((int64_t)Z * PY + Y) * PX + X + k * kst;
+    }
+    return b * bst + k * kst + cell;
+  }
+};
 
 }  // namespace oal

@@ -12,6 +12,7 @@
 
 #include "common.cuh"
 #include "../../include/oal.h"
+#include "bouzidi_d3q27.h"
 #include "kbc_d3q39.h"
 
 namespace oal {
@@ -34,6 +35,21 @@ template <class R>
 cudaError_t launch_parent_positions(const ParentView& P, const int4* pos_xyz, int32_t n, void* macro, cudaStream_t st);
 }
 using namespace oal;
+
+// IEEE binary16 bits -> float (the reference stores q maps as Float16).
+static float half_bits_to_float(uint16_t h) {
+  const int e = (h >> 10) & 31, m = h & 1023;
+  float v;
+  if (e == 0) v = std::ldexp((float)m, -24);                      // zero and subnormals: m 2^-24
+  else if (e == 31) v = m ? NAN : INFINITY;
+  else v = std::ldexp((float)(m | 1024), e - 25);                 // (1 + m/1024) 2^(e-15)
+  return (h & 0x8000) ? -v : v;
+}
+
+static void bouzidi_free(BouzidiSet* B) {
+  cudaFree(B->cells); cudaFree(B->q); cudaFree(B->vals);
+  B->cells = nullptr; B->q = nullptr; B->vals = nullptr; B->n = 0;
+}
 
 // ------------------------------------------------------------------------------------------------
 // error reporting
@@ -102,23 +118,6 @@ __global__ void k_reduce4(const double* __restrict__ part, int64_t n, double* __
   if (t == 0)
     for (int c = 0; c < 4; ++c) out[c] = s[c][0];
 }
-
-// Element of (block b, cell, direction k) in either population layout of a library-owned level.
-struct PopIndex {
-  const int4* binfo;
-  int dense;
-  int PX, PY;
-  int64_t bst, kst;
-  __device__ __forceinline__ int64_t operator()(int64_t b, int cell, int k) const {
-    if (dense) {
-      const int4 bi = binfo[b];
-      const int X = (bi.x - 1) * kBS + (cell & 7) + 8, Y = (bi.y - 1) * kBS + ((cell >> 3) & 7) + 1,
-                Z = (bi.z - 1) * kBS + (cell >> 6) + 1;
-      return ((int64_t)Z * PY + Y) * PX + X + k * kst;
-    }
-    return b * bst + k * kst + cell;
-  }
-};
 
 // Per-block FP64 mass and momentum of the fluid cells (state.jl:614-637): one CTA per block.
 template <class S, class R>
@@ -308,6 +307,7 @@ struct oal_level {
   bool forces_valid = false;
   KbcLevel* kbc = nullptr;  // D3Q39 entropic levels: the whole state lives here
   ParentView par{};         // refined level of a block-AMR hierarchy: its parent (set per step)
+  BouzidiSet bz;            // linear Bouzidi boundary cells (oal_level_set_bouzidi)
 };
 
 // ------------------------------------------------------------------------------------------------
@@ -322,7 +322,8 @@ static oal_status resolve_params(const oal_step_params* p, const oal_geometry* g
   if (!(p->tau > 0.5f) || !std::isfinite(p->tau)) return set_error(OAL_E_INVALID_ARG, "tau must be > 0.5 (got %g)", p->tau);
   if (p->limiter_type < 0 || p->limiter_type > 2) return set_error(OAL_E_INVALID_ARG, "limiter_type %d", p->limiter_type);
   if (p->zwall_bc < 0 || p->zwall_bc > 2) return set_error(OAL_E_INVALID_ARG, "zwall_bc %d", p->zwall_bc);
-  if (p->solid_bc != OAL_SOLID_FULLWAY && p->solid_bc != OAL_SOLID_HALFWAY && p->solid_bc != OAL_SOLID_GRAD)
+  if (p->solid_bc != OAL_SOLID_FULLWAY && p->solid_bc != OAL_SOLID_HALFWAY && p->solid_bc != OAL_SOLID_GRAD &&
+      p->solid_bc != OAL_SOLID_BOUZIDI)
     return set_error(OAL_E_INVALID_ARG, "solid_bc %d", p->solid_bc);
   std::memset(cp, 0, sizeof *cp);
   cp->tau = p->tau;
@@ -352,6 +353,7 @@ static oal_status resolve_params(const oal_step_params* p, const oal_geometry* g
   if (p->transverse_freestream == 1) f |= CF_TRANSVERSE_FS;
   if (p->solid_bc == OAL_SOLID_HALFWAY) f |= CF_HALFWAY;
   if (p->solid_bc == OAL_SOLID_GRAD) f |= CF_GRAD_WALL;
+  if (p->solid_bc == OAL_SOLID_BOUZIDI) f |= CF_BOUZIDI;
   cp->grad_pineq_scale = p->grad_pineq_scale;
   if (p->collect_forces) f |= CF_COLLECT;
   if (p->store_post_collision == 1) f |= CF_STORE_POST;
@@ -942,6 +944,8 @@ oal_status oal_stream_collide(const oal_geometry* g, const oal_level_fields* fl,
   CaseParams cp;
   oal_status s = resolve_params(p, g, &cp);
   if (s != OAL_OK) return s;
+  if (cp.flags & CF_BOUZIDI)
+    return set_error(OAL_E_UNSUPPORTED, "OAL_SOLID_BOUZIDI: the boundary cells attach to plain levels, not to caller-owned arrays (oal_stream_collide)");
   if (!fl->f_in || !fl->f_out || !fl->rho_out || !fl->vel_out || !fl->vel_in)
     return set_error(OAL_E_INVALID_ARG, "f_in, f_out, rho_out, vel_out and vel_in are required");
   if (fl->f_in == fl->f_out) return set_error(OAL_E_INVALID_ARG, "f_in and f_out must differ (pull scheme)");
@@ -1084,6 +1088,7 @@ void oal_level_destroy(oal_level* L) {
   }
   cudaSetDevice(L->device);
   release_graph(L);
+  bouzidi_free(&L->bz);
   for (int i = 0; i < 2; ++i) { cudaFree(L->f[i]); cudaFree(L->vel[i]); }
   cudaFree(L->rho); cudaFree(L->d_force_part); cudaFree(L->d_force); cudaFree(L->d_mm_part); cudaFree(L->d_mm);
   if (L->cap) cudaStreamDestroy(L->cap);
@@ -1216,6 +1221,8 @@ static oal_status enqueue_step(oal_level* L, const CaseParams& cp, cudaStream_t 
   } else {
     OAL_CUDA_TRY(launch_by_storage(L->storage, g, a, PATH_GHOSTED, st, &L->ov));
   }
+  if ((cp.flags & CF_BOUZIDI) && L->bz.n > 0)
+    OAL_CUDA_TRY(bouzidi_enqueue(L->bz, L->storage, a.f_out, pop_index(L), g->d_nbr, g->d_mslot, g->d_cmask, st));
   if (cp.flags & CF_COLLECT) {
     // the momentum exchange lives on the general kernel's CTAs (blocks near solids)
     if (g->n_general > 0) {
@@ -1277,6 +1284,49 @@ oal_status oal_level_advance(oal_level* L, const oal_step_params* p, int32_t n, 
   OAL_CUDA_TRY(cudaGraphLaunch(L->gc.exec, st));
   if (n & 1) L->parity ^= 1;
   if (cp.flags & CF_COLLECT) L->forces_valid = true;
+  return OAL_OK;
+}
+
+oal_status oal_level_set_bouzidi(oal_level* L, int32_t n_cells, const int32_t* cell_block, const int32_t* cell_x,
+                                 const int32_t* cell_y, const int32_t* cell_z, const uint16_t* q_half,
+                                 float q_min_threshold, int32_t ff_fallback, float limiter_rel_cap,
+                                 float limiter_abs_cap) {
+  if (!L) return set_error(OAL_E_INVALID_ARG, "null level");
+  if (L->kbc) return set_error(OAL_E_UNSUPPORTED, "linear Bouzidi walls are a D3Q27 level path");
+  if (L->par.ptr) return set_error(OAL_E_UNSUPPORTED, "linear Bouzidi walls attach to plain levels, not to refined ones");
+  if (n_cells < 0) return set_error(OAL_E_INVALID_ARG, "n_cells %d", n_cells);
+  if (ff_fallback < 0 || ff_fallback > 2) return set_error(OAL_E_INVALID_ARG, "ff_fallback %d (0, 1 or 2)", ff_fallback);
+  if (!(limiter_rel_cap >= 0.0f) || !(limiter_abs_cap >= 0.0f) || !std::isfinite(q_min_threshold))
+    return set_error(OAL_E_INVALID_ARG, "limiter caps must be >= 0 and q_min_threshold finite");
+  const oal_geometry* g = L->g;
+  std::vector<int2> cells((size_t)n_cells);
+  std::vector<float> q((size_t)n_cells * 27);
+  if (n_cells > 0) {
+    if (!cell_block || !cell_x || !cell_y || !cell_z || !q_half) return set_error(OAL_E_INVALID_ARG, "null array");
+    for (int32_t i = 0; i < n_cells; ++i) {
+      const int32_t b = cell_block[i], x = cell_x[i], y = cell_y[i], z = cell_z[i];
+      if (b < 1 || b > g->nb || x < 1 || x > 8 || y < 1 || y > 8 || z < 1 || z > 8)
+        return set_error(OAL_E_INVALID_ARG, "boundary cell %d: block %d, cell (%d, %d, %d) outside the level", i, b, x, y, z);
+      cells[(size_t)i] = make_int2(b - 1, (x - 1) | ((y - 1) << 3) | ((z - 1) << 6));
+    }
+    for (size_t j = 0; j < q.size(); ++j) q[j] = half_bits_to_float(q_half[j]);
+  }
+  OAL_CUDA_TRY(cudaSetDevice(g->device));
+  OAL_CUDA_TRY(cudaDeviceSynchronize());  // a step in flight may still read the old set
+  release_graph(L);
+  bouzidi_free(&L->bz);
+  L->bz.q_min = q_min_threshold;
+  L->bz.ff_fallback = ff_fallback;
+  L->bz.rel_cap = limiter_rel_cap;
+  L->bz.abs_cap = limiter_abs_cap;
+  if (n_cells == 0) return OAL_OK;
+  const size_t rsz = L->storage == OAL_STORE_F64 ? sizeof(double) : sizeof(float);
+  OAL_CUDA_TRY(cudaMalloc(&L->bz.cells, cells.size() * sizeof(int2)));
+  OAL_CUDA_TRY(cudaMalloc(&L->bz.q, q.size() * sizeof(float)));
+  OAL_CUDA_TRY(cudaMalloc(&L->bz.vals, q.size() * rsz));
+  OAL_CUDA_TRY(cudaMemcpy(L->bz.cells, cells.data(), cells.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  OAL_CUDA_TRY(cudaMemcpy(L->bz.q, q.data(), q.size() * sizeof(float), cudaMemcpyHostToDevice));
+  L->bz.n = n_cells;
   return OAL_OK;
 }
 
@@ -1741,6 +1791,8 @@ oal_status oal_amr_advance(oal_amr* A, const oal_step_params* params, int32_t n,
   for (int l = 0; l < nl; ++l) {
     oal_status s = resolve_params(&params[l], A->lv[(size_t)l].g, &cps[(size_t)l]);
     if (s != OAL_OK) return s;
+    if (cps[(size_t)l].flags & CF_BOUZIDI)
+      return set_error(OAL_E_UNSUPPORTED, "OAL_SOLID_BOUZIDI: the boundary cells attach to plain levels, not to refined levels (oal_amr_*)");
     if (cps[(size_t)l].flags & CF_STORE_POST) return set_error(OAL_E_UNSUPPORTED, "store_post_collision needs caller-owned arrays");
   }
   OAL_CUDA_TRY(cudaSetDevice(A->device));
@@ -2141,6 +2193,8 @@ oal_status oal_batch_add(oal_batch* B, const oal_geometry* g, const oal_step_par
   CaseParams cp;
   oal_status s = resolve_params(p, g, &cp);
   if (s != OAL_OK) return s;
+  if (cp.flags & CF_BOUZIDI)
+    return set_error(OAL_E_UNSUPPORTED, "OAL_SOLID_BOUZIDI: the boundary cells attach to plain levels, not to batched cases (oal_batch_*)");
   if (cp.flags & CF_STORE_POST) return set_error(OAL_E_UNSUPPORTED, "store_post_collision needs caller-owned arrays");
   int32_t m = -1;
   for (int32_t i = 0; i < B->max_members; ++i)
@@ -2234,6 +2288,8 @@ oal_status oal_batch_set_params(oal_batch* B, int32_t m, const oal_step_params* 
   CaseParams cp;
   oal_status s = resolve_params(p, B->mem[(size_t)m].g, &cp);
   if (s != OAL_OK) return s;
+  if (cp.flags & CF_BOUZIDI)
+    return set_error(OAL_E_UNSUPPORTED, "OAL_SOLID_BOUZIDI: the boundary cells attach to plain levels, not to batched cases (oal_batch_*)");
   B->mem[(size_t)m].p = *p; B->mem[(size_t)m].cp = cp;
   B->dirty = true;
   return OAL_OK;

@@ -245,6 +245,22 @@ class Level:
 
     advance = execute_timestep_batch
 
+    def set_bouzidi(self, cells: np.ndarray, q: np.ndarray, q_min_threshold: float = 0.001, ff_fallback: int = 0,
+                    limiter_rel_cap: float = 0.0, limiter_abs_cap: float = 0.0) -> None:
+        """Attach the linear Bouzidi boundary cells (solid_bc OAL_SOLID_BOUZIDI): cells (n, 4) int32
+        (block, x, y, z) 1-based, q (n, 27) link fractions stored as float16 like the reference's
+        q_map. An empty list detaches."""
+        cells = np.ascontiguousarray(cells, dtype=np.int32).reshape(-1, 4)
+        qh = np.ascontiguousarray(np.asarray(q, dtype=np.float16).reshape(-1, 27)).view(np.uint16)
+        if qh.shape[0] != cells.shape[0]:
+            raise ValueError("q must hold 27 values per boundary cell")
+        cols = [np.ascontiguousarray(cells[:, j]) for j in range(4)]
+        n = int(cells.shape[0])
+        ptrs = [c.ctypes.data_as(_i32p) if n else None for c in cols]
+        check(lib().oal_level_set_bouzidi(self.handle, n, *ptrs, qh.ctypes.data_as(C.POINTER(C.c_uint16)) if n else None,
+                                          float(q_min_threshold), int(ff_fallback), float(limiter_rel_cap),
+                                          float(limiter_abs_cap)))
+
     def forces(self) -> np.ndarray:
         out = (C.c_double * 3)()
         check(lib().oal_level_get_forces(self.handle, out))

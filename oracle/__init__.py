@@ -69,6 +69,10 @@ def lib() -> C.CDLL:
             getattr(L, f"ora_step_d3q27_refined_{suf}").restype = C.c_int
             getattr(L, f"ora_restrict_d3q27_{suf}").argtypes = (
                 [i32, vp, vp, vp, vp, i32, vp, i32, i32, i32, vp, vp, C.c_double, C.c_double, i32, i32])
+        for suf in ("f64", "f32"):
+            getattr(L, f"ora_bouzidi_linear_{suf}").argtypes = [i32, vp, vp, i32, vp, vp, C.c_float, i32, C.c_float,
+                                                                 C.c_float, vp, vp]
+            getattr(L, f"ora_bouzidi_linear_{suf}").restype = C.c_int
         L.ora_q39_tables.argtypes = [vp] * 5
         L.ora_q39_exp.argtypes = [i64, vp, vp]
         L.ora_q39_log.argtypes = [i64, vp, vp]
@@ -151,6 +155,30 @@ class OracleLevel:
         self.vel, self.vel_new = self.vel_new, self.vel
         if params.collect_forces:
             self.force = force
+        return self
+
+    def step_bouzidi(self, params, bz):
+        """One step followed by the linear Bouzidi correction (timestep.jl:1752-1768): `bz` holds
+        cells (n, 4) int32 (block, x, y, z) 1-based, q (n, 27) float16, q_min, ff_fallback,
+        rel_cap, abs_cap."""
+        p = type(params).from_buffer_copy(params)
+        p.store_post_collision = 1
+        post = np.zeros_like(self.f)
+        fn = lib().ora_step_d3q27_f64 if self.dtype == np.float64 else lib().ora_step_d3q27_f32
+        force = np.zeros(3)
+        rc = fn(self.nb, *self.shape, _p(self.coords), _p(self.nbr), _p(self.obstacle), _p(self.sponge),
+                _p(self.wall_dist), C.addressof(p), _p(self.f), _p(self.g), _p(post), _p(self.rho),
+                _p(self.vel_new), _p(self.vel), _p(force))
+        assert rc == 0
+        cells = np.ascontiguousarray(bz["cells"], np.int32)
+        q = np.ascontiguousarray(np.asarray(bz["q"], np.float16).astype(np.float32))
+        fb = lib().ora_bouzidi_linear_f64 if self.dtype == np.float64 else lib().ora_bouzidi_linear_f32
+        rc = fb(self.nb, _p(self.nbr), _p(self.obstacle), int(cells.shape[0]), _p(cells), _p(q),
+                bz.get("q_min", 0.001), int(bz.get("ff_fallback", 0)), bz.get("rel_cap", 0.0),
+                bz.get("abs_cap", 0.0), _p(post), _p(self.g))
+        assert rc == 0
+        self.f, self.g = self.g, self.f
+        self.vel, self.vel_new = self.vel_new, self.vel
         return self
 
     def mass_momentum(self):

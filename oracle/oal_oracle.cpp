@@ -25,6 +25,8 @@
 //                             27 D3Q27 links; the reference's GPU path has no D3Q27 analogue)
 //   Grad wall ............... src/geometry/grad_wall_kernel.jl:42-144 (velocity mode 0), called
 //                             from src/collision/timestep.jl:1738-1751
+//   linear Bouzidi wall ..... src/geometry/bouzidi_kernel.jl:150-380 (unshifted D3Q27), called from
+//                             src/collision/timestep.jl:1752-1768 after the step
 //   mass / momentum ......... src/octree_q19/src/state.jl:614-637 (Float64 sums)
 //   block AMR (default flags): parent interpolation of a refined level's pulls
 //                             src/collision/physics_interpolation.jl:10-51,128-137,188-346,705-1198
@@ -1033,6 +1035,82 @@ Level make_level(int32_t nb, int32_t nx, int32_t ny, int32_t nz, const int32_t* 
 
 }  // namespace
 
+// ---- linear Bouzidi wall (geometry/bouzidi_kernel.jl:150-380, default D3Q27 options) ---------
+// bouzidi_correction_kernel_fixed! on the unshifted lattice (out_k = opp k, shifted-wall scale 0):
+// for every listed fluid cell x and link k with q_min < q <= 1, from the post-collision
+// populations f* of the step, f_out[x, opp k] =
+//   q < 1/2:  2q f*_k(x) + (1-2q) f*_k(x_ff), x_ff = x + c_{opp k} when it exists and is fluid,
+//             else (ff_fallback) 0: f*_k(x), 1: w_k rho_f, 2: f*_{opp k}(x)        (:223-287)
+//   q >= 1/2: f*_k(x)/(2q) + (2q-1)/(2q) f*_{opp k}(x)                             (:320-328)
+// then, with a limiter cap > 0, clamp to w_{opp k} rho_f +- max(abs, rel max(|.|, 1e-12)) and
+// floor at 1e-12 (_limit_wall_population, :65-87); rho_f = sum of f*(x) in direction order.
+// cells: n x 4 int32 (block, x, y, z), 1-based like the reference's bouzidi_cell_* arrays.
+template <class T>
+void bouzidi_linear(const Level& L, int32_t n, const int32_t* cells, const float* q, float q_min, int ff,
+                    float rel_cap, float abs_cap, const T* fpost, T* fout) {
+  Arr<T> A{L.nb};
+  for (int32_t i = 0; i < n; ++i) {
+    const int b = cells[4 * i] - 1, x = cells[4 * i + 1] - 1, y = cells[4 * i + 2] - 1, z = cells[4 * i + 3] - 1;
+    bool rho_valid = false;
+    T rho_f = T(0);
+    auto density = [&]() {
+      if (!rho_valid) {
+        T s = T(0);
+        for (int kk = 0; kk < Q; ++kk) s += fpost[A.f(x, y, z, b, kk)];
+        rho_f = s;
+        rho_valid = true;
+      }
+      return rho_f;
+    };
+    for (int k = 0; k < Q; ++k) {
+      const float qf = q[(size_t)i * Q + k];
+      if (!(qf > q_min && qf <= 1.0f)) continue;
+      const int ok = TB.opp[k];
+      const T qq = T(qf);
+      const T fk = fpost[A.f(x, y, z, b, k)];
+      T raw;
+      if (qq < T(0.5)) {
+        const int nx = x + TB.cx[ok], ny = y + TB.cy[ok], nz = z + TB.cz[ok];
+        T fff = fk;
+        bool have = false;
+        if (nx >= 0 && nx < BS && ny >= 0 && ny < BS && nz >= 0 && nz < BS) {
+          if (!(L.obstacle && L.obstacle[A.s(nx, ny, nz, b)])) { fff = fpost[A.f(nx, ny, nz, b, k)]; have = true; }
+        } else {
+          const int ox = nx < 0 ? -1 : (nx >= BS ? 1 : 0), oy = ny < 0 ? -1 : (ny >= BS ? 1 : 0),
+                    oz = nz < 0 ? -1 : (nz >= BS ? 1 : 0);
+          const int dir = (ox + 1) + 3 * (oy + 1) + 9 * (oz + 1);
+          const int nbb = L.nbr[b + (int64_t)L.nb * dir];
+          if (nbb > 0) {
+            const int lx = nx - BS * ox, ly = ny - BS * oy, lz = nz - BS * oz;
+            if (!(L.obstacle && L.obstacle[A.s(lx, ly, lz, nbb - 1)])) {
+              fff = fpost[A.f(lx, ly, lz, nbb - 1, k)];
+              have = true;
+            }
+          }
+        }
+        if (!have && ff == 1) fff = density() * T(TB.w[k]);
+        else if (!have && ff == 2) fff = fpost[A.f(x, y, z, b, ok)];
+        const T c1 = T(2) * qq;
+        raw = c1 * fk + (T(1) - c1) * fff;
+      } else {
+        const T fo = fpost[A.f(x, y, z, b, ok)];
+        const T inv_2q = T(1) / (T(2) * qq);
+        const T c2 = (T(2) * qq - T(1)) * inv_2q;
+        raw = inv_2q * fk + c2 * fo;
+      }
+      if (rel_cap > 0.0f || abs_cap > 0.0f) {
+        const T target = density() * T(TB.w[ok]);
+        const T scale = std::max(std::fabs(target), T(1e-12f));
+        const T cap = std::max(T(abs_cap), T(rel_cap) * scale);
+        const T lo = target - cap, hi = target + cap;
+        raw = raw > hi ? hi : (raw < lo ? lo : raw);
+        raw = raw < T(1e-12f) ? T(1e-12f) : raw;
+      }
+      fout[A.f(x, y, z, b, ok)] = raw;
+    }
+  }
+}
+
 extern "C" {
 
 // D3Q27 tables in the reference order (0-based indices for opp/mirrors).
@@ -1182,6 +1260,23 @@ void ora_mass_momentum_f64(int32_t nb, const uint8_t* obstacle, const double* f,
     }
   }
   out[0] = m; out[1] = px; out[2] = py; out[3] = pz;
+}
+
+// Bouzidi correction of one step's output: f_post = the step's post-collision populations,
+// f_out = its output (overwritten on the corrected links). Arrays in the reference layout.
+int ora_bouzidi_linear_f64(int32_t nb, const int32_t* nbr, const uint8_t* obstacle, int32_t n, const int32_t* cells,
+                           const float* q, float q_min, int32_t ff, float rel_cap, float abs_cap,
+                           const double* f_post, double* f_out) {
+  Level L = make_level(nb, 0, 0, 0, nullptr, nbr, obstacle, nullptr, nullptr);
+  bouzidi_linear<double>(L, n, cells, q, q_min, ff, rel_cap, abs_cap, f_post, f_out);
+  return 0;
+}
+int ora_bouzidi_linear_f32(int32_t nb, const int32_t* nbr, const uint8_t* obstacle, int32_t n, const int32_t* cells,
+                           const float* q, float q_min, int32_t ff, float rel_cap, float abs_cap,
+                           const float* f_post, float* f_out) {
+  Level L = make_level(nb, 0, 0, 0, nullptr, nbr, obstacle, nullptr, nullptr);
+  bouzidi_linear<float>(L, n, cells, q, q_min, ff, rel_cap, abs_cap, f_post, f_out);
+  return 0;
 }
 
 }  // extern "C"

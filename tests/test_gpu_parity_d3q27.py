@@ -213,3 +213,80 @@ def test_rejects_bad_params(oal):
     with pytest.raises(capi.OALError) as e:
         L.perform_timestep(p)
     assert e.value.status == capi.OAL_E_UNSUPPORTED
+
+
+BOUZIDI_OPTS = {"halfway_bb": {}, "wall_eq": dict(ff_fallback=1), "bounce_back": dict(ff_fallback=2),
+                "limiter": dict(limiter_rel_cap=0.05, limiter_abs_cap=1e-4)}
+
+
+# The linear Bouzidi wall (bc_scheme "bouzidi_linear") on the sphere's analytic q map, every
+# fall-back and the wall-population limiter, on both layouts.
+@pytest.mark.parametrize("storage,dtype,tol,layout", [("f64", np.float64, 1e-11, "block"),
+                                                      ("f32", np.float32, 2e-5, "block"),
+                                                      ("f32", np.float32, 2e-5, "dense"),
+                                                      ("f16", np.float64, 2e-3, "block")])
+@pytest.mark.parametrize("opt", sorted(BOUZIDI_OPTS))
+def test_bouzidi_linear_wall(oal, oracle_lib, channel, opt, storage, dtype, tol, layout):
+    from openaerolab_alpha_01_b200.bouzidi import sphere_qmap
+    d = channel.dom
+    cells, q = sphere_qmap(d, (10.0, 8.0, 8.0), 3.0)
+    kw = BOUZIDI_OPTS[opt]
+    p = capi.default_params(**{f: getattr(channel.params, f) for f, _ in capi.StepParams._fields_ if f != "reserved"})
+    p.solid_bc = capi.OAL_SOLID_BOUZIDI
+    p.collect_forces = 0
+    g = Geometry(d)
+    L = Level(g, storage=storage, layout=layout)
+    L.init_equilibrium(channel.rho, channel.vel)
+    L.set_bouzidi(cells, q, **kw)
+    O = oracle_lib.OracleLevel(d.coords, d.neighbor_table, d.shape, obstacle=d.obstacle, dtype=dtype)
+    O.init_equilibrium(channel.rho, channel.vel)
+    bz = dict(cells=cells, q=q, ff_fallback=kw.get("ff_fallback", 0), rel_cap=kw.get("limiter_rel_cap", 0.0),
+              abs_cap=kw.get("limiter_abs_cap", 0.0))
+    for i in range(12):
+        p.time_step_seed = i
+        L.perform_timestep(p)
+        O.step_bouzidi(p, bz)
+    f, rho, vel = L.state()
+    L.close(); g.close()
+    assert rel(f, O.f) < tol, opt
+    assert rel(vel, O.vel) < tol * 50, opt
+
+
+def test_bouzidi_graph_detach_and_refusals(oal, channel):
+    from openaerolab_alpha_01_b200.bouzidi import sphere_qmap
+    from openaerolab_alpha_01_b200.solver import Batch
+    from openaerolab_alpha_01_b200._capi import OALError
+    d = channel.dom
+    cells, q = sphere_qmap(d, (10.0, 8.0, 8.0), 3.0)
+    p = capi.default_params(**{f: getattr(channel.params, f) for f, _ in capi.StepParams._fields_ if f != "reserved"})
+    p.solid_bc = capi.OAL_SOLID_BOUZIDI
+    p.collect_forces = 0
+    g = Geometry(d)
+    A, B, C_ = (Level(g, storage="f32") for _ in range(3))
+    for X in (A, B, C_):
+        X.init_equilibrium(channel.rho, channel.vel)
+    A.set_bouzidi(cells, q)
+    B.set_bouzidi(cells, q)
+    for _ in range(6):
+        A.perform_timestep(p)
+    B.execute_timestep_batch(p, 6)  # the correction is captured with the step
+    assert np.array_equal(A.state()[0], B.state()[0])
+    # detached: OAL_SOLID_BOUZIDI without cells is the full-way step
+    B.set_bouzidi(np.zeros((0, 4), np.int32), np.zeros((0, 27)))
+    pf = capi.default_params(**{f: getattr(p, f) for f, _ in capi.StepParams._fields_ if f != "reserved"})
+    pf.solid_bc = capi.OAL_SOLID_FULLWAY
+    C_.set_state(*B.state())
+    B.execute_timestep_batch(p, 3)
+    C_.execute_timestep_batch(pf, 3)
+    assert np.array_equal(B.state()[0], C_.state()[0])
+    bad = cells.copy()
+    bad[0, 1] = 9
+    with pytest.raises(OALError):
+        A.set_bouzidi(bad, q)
+    bat = Batch(storage="f32", max_real_blocks=64, max_ghost_blocks=64)
+    with pytest.raises(OALError):
+        bat.add(g, p, channel.rho, channel.vel)
+    bat.close()
+    for X in (A, B, C_):
+        X.close()
+    g.close()
