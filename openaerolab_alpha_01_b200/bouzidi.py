@@ -70,3 +70,75 @@ def sphere_qmap(dom: BlockDomain, centre, radius: float, dx: float = 1.0):
     bi, ci = np.nonzero(has)
     cells = np.stack([bi + 1, (ci & 7) + 1, ((ci >> 3) & 7) + 1, (ci >> 6) + 1], axis=1).astype(np.int32)
     return cells, q[bi, ci].astype(np.float16)
+
+
+def ray_triangle_hits(origin: np.ndarray, dir_unit: np.ndarray, tris: np.ndarray) -> np.ndarray:
+    """Two-sided Moller-Trumbore distances (ray_triangle_intersection, bouzidi_math.jl:9-50) of
+    every origin (m, 3) along dir_unit (3,) to every triangle (t, 3, 3): (m, t), inf = no hit.
+    |det| < 1e-9 misses, the barycentric test admits 64 eps of round-off on the edges, and only
+    hits at t > 1e-9 count."""
+    eps, bary = 1.0e-9, 64 * np.finfo(np.float64).eps
+    v1 = tris[:, 0]
+    e1, e2 = tris[:, 1] - v1, tris[:, 2] - v1
+    h = np.cross(dir_unit, e2)                       # (t, 3)
+    a = np.einsum("ti,ti->t", e1, h)
+    ok_a = np.abs(a) >= eps
+    f = np.where(ok_a, 1.0 / np.where(ok_a, a, 1.0), 0.0)
+    s = origin[:, None, :] - v1[None, :, :]          # (m, t, 3)
+    u = f[None, :] * np.einsum("mti,ti->mt", s, h)
+    qv = np.cross(s, e1[None, :, :])
+    v = f[None, :] * (qv @ dir_unit)
+    t = f[None, :] * np.einsum("mti,ti->mt", qv, e2)
+    hit = (ok_a[None, :] & (u >= -bary) & (u <= 1.0 + bary) & (v >= -bary) & (u + v <= 1.0 + bary) & (t > eps))
+    return np.where(hit, t, np.inf)
+
+
+def stl_qmap(dom: BlockDomain, triangles, mesh_offset=(0.0, 0.0, 0.0), dx: float = 1.0):
+    """Boundary cells, q (float16) and the 1-based triangle of each kept link for a triangle mesh
+    (q_geometry "stl_ray": compute_q_for_cell, bouzidi_math.jl:57-125, over the triangles near each
+    block, build_block_triangle_map_for_bouzidi, bouzidi_setup.jl:12-58). triangles (T, 3, 3) in
+    mesh coordinates; mesh_offset is added to every vertex. Returns (cells (n, 4) int32, q (n, 27)
+    float16, tri (n, 27) int32, 0 = none)."""
+    if dom.obstacle is None:
+        raise ValueError("the q map keeps links into solid cells: the domain needs an obstacle mask")
+    tris = np.asarray(triangles, np.float64).reshape(-1, 3, 3) + np.asarray(mesh_offset, np.float64)
+    nb = dom.n_blocks
+    solid = dom.obstacle.reshape(nb, 512) != 0
+    margin = dx * (np.sqrt(3.0) + 1.0)                # max |c| of D3Q27 plus one cell
+    bmin = np.floor((tris.min(axis=1) - margin) / (8 * dx)).astype(np.int64) + 1
+    bmax = np.floor((tris.max(axis=1) + margin) / (8 * dx)).astype(np.int64) + 1
+    cell = np.arange(512)
+    lx, ly, lz = cell & 7, (cell >> 3) & 7, cell >> 6
+    nbr = dom.neighbor_table
+    q = np.zeros((nb, 512, 27), np.float64)
+    tri_of = np.zeros((nb, 512, 27), np.int32)
+    for b in range(nb):
+        bc = dom.coords[b].astype(np.int64)
+        near = np.nonzero(np.all((bmin <= bc) & (bc <= bmax), axis=1))[0]
+        if near.size == 0:
+            continue
+        centre = np.stack([((bc[0] - 1) * 8 + lx + 0.5) * dx, ((bc[1] - 1) * 8 + ly + 0.5) * dx,
+                           ((bc[2] - 1) * 8 + lz + 0.5) * dx], axis=1)
+        for k in range(27):
+            if k == 13:
+                continue
+            nx, ny, nz = lx + CX[k], ly + CY[k], lz + CZ[k]
+            d = (nx // 8 + 1) + 3 * (ny // 8 + 1) + 9 * (nz // 8 + 1)
+            nbb = nbr[d, b]
+            ncell = (nx & 7) | ((ny & 7) << 3) | ((nz & 7) << 6)
+            cand = np.nonzero((nbb > 0) & solid[np.maximum(nbb - 1, 0), ncell] & ~solid[b])[0]
+            if cand.size == 0:
+                continue
+            c = np.array([CX[k], CY[k], CZ[k]], np.float64)
+            cmag = float(np.linalg.norm(c))
+            t = ray_triangle_hits(centre[cand], c / cmag, tris[near])
+            j = np.argmin(t, axis=1)                  # the first of equal distances, like `t < min_t`
+            tmin = t[np.arange(cand.size), j]
+            qk = tmin / (dx * cmag)
+            ok = np.isfinite(qk) & (qk > 0.0) & (qk <= 1.0)
+            q[b, cand[ok], k] = qk[ok]
+            tri_of[b, cand[ok], k] = near[j[ok]] + 1
+    has = (q > 0.0).any(axis=2)
+    bi, ci = np.nonzero(has)
+    cells = np.stack([bi + 1, (ci & 7) + 1, ((ci >> 3) & 7) + 1, (ci >> 6) + 1], axis=1).astype(np.int32)
+    return cells, q[bi, ci].astype(np.float16), tri_of[bi, ci]

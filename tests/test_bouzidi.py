@@ -155,3 +155,54 @@ def test_oracle_bouzidi_channel_runs_and_conserves_nothing_spurious():
     # the sphere sits on the channel axis: the transverse momentum stays at rounding level
     mm = O.mass_momentum()
     assert abs(mm[2]) < 1e-9 * abs(mm[1]) and abs(mm[3]) < 1e-9 * abs(mm[1])
+
+
+def box_mesh(lo, hi):
+    """The 12 triangles of an axis-aligned box."""
+    (x0, y0, z0), (x1, y1, z1) = lo, hi
+    v = np.array([[x0, y0, z0], [x1, y0, z0], [x1, y1, z0], [x0, y1, z0],
+                  [x0, y0, z1], [x1, y0, z1], [x1, y1, z1], [x0, y1, z1]])
+    faces = [(0, 1, 2), (0, 2, 3), (4, 6, 5), (4, 7, 6), (0, 5, 1), (0, 4, 5),
+             (3, 2, 6), (3, 6, 7), (0, 3, 7), (0, 7, 4), (1, 5, 6), (1, 6, 2)]
+    return np.array([[v[i], v[j], v[k]] for i, j, k in faces])
+
+
+def test_stl_qmap_of_a_box_matches_the_slab_distances():
+    from openaerolab_alpha_01_b200.bouzidi import stl_qmap
+    dom = build_box(4, 3, 3)
+    lo, hi = np.array([11.3, 9.6, 8.7]), np.array([18.2, 14.45, 15.9])
+    gx, gy, gz = dom.cell_positions()
+    cen = np.stack([gx - 0.5, gy - 0.5, gz - 0.5], axis=-1)
+    dom.obstacle = np.all((cen > lo) & (cen < hi), axis=-1).astype(np.uint8)
+    tris = box_mesh(lo - 1.0, hi - 1.0)  # mesh coordinates, shifted back by the offset below
+    cells, q, tri = stl_qmap(dom, tris, mesh_offset=(1.0, 1.0, 1.0))
+    assert cells.shape[0] > 0
+    n_links = 0
+    for (b, x, y, z), qr, tr in zip(cells, q, tri):
+        o = (dom.coords[b - 1] - 1) * 8 + np.array([x, y, z]) - 0.5
+        for k in range(27):
+            c = np.array([CX[k], CY[k], CZ[k]], float)
+            if qr[k] == 0:
+                continue
+            n_links += 1
+            assert 1 <= tr[k] <= 12
+            # entry distance of the ray into the box (slab method), in units of the link
+            with np.errstate(divide="ignore", invalid="ignore"):
+                t0, t1 = (lo - o) / c, (hi - o) / c
+            tn = np.nanmax(np.where(c != 0, np.minimum(t0, t1), -np.inf))
+            assert float(qr[k]) == np.float16(tn)
+    assert n_links > 100
+    # the analytic sphere and a fine triangulation of it give close q values on the same links
+    dom2 = build_box(4, 2, 2)
+    centre, radius = (16.0, 8.0, 8.0), 4.3
+    apply_analytic_sphere_obstacle(dom2, centre, radius)
+    th, ph = np.meshgrid(np.linspace(0, np.pi, 61), np.linspace(0, 2 * np.pi, 121), indexing="ij")
+    P = np.stack([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)], -1) * radius + centre
+    quads = [(P[i, j], P[i + 1, j], P[i + 1, j + 1], P[i, j + 1]) for i in range(60) for j in range(120)]
+    tris = np.array([t for a, b_, c, d in quads for t in ((a, b_, c), (a, c, d))])
+    c_s, q_s = sphere_qmap(dom2, centre, radius)
+    c_t, q_t, _ = stl_qmap(dom2, tris)
+    assert np.array_equal(c_s, c_t)
+    both = (q_s > 0) & (q_t > 0)
+    assert both.sum() > 0.99 * (q_s > 0).sum()
+    assert np.max(np.abs(q_s[both].astype(float) - q_t[both].astype(float))) < 0.02
