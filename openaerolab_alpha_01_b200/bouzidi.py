@@ -142,3 +142,54 @@ def stl_qmap(dom: BlockDomain, triangles, mesh_offset=(0.0, 0.0, 0.0), dx: float
     bi, ci = np.nonzero(has)
     cells = np.stack([bi + 1, (ci & 7) + 1, ((ci >> 3) & 7) + 1, (ci >> 6) + 1], axis=1).astype(np.int32)
     return cells, q[bi, ci].astype(np.float16), tri_of[bi, ci]
+
+
+def bench_step_cost(steps: int = 200, storage: str = "f16") -> dict:
+    """Step time of the 256 x 128 x 128 sphere channel (D = 24, Re 1000) with full-way solid cells and
+    with the linear Bouzidi wall, alternating, each on CUDA events over `steps` graph-captured steps
+    after 10 warm-up steps."""
+    import time
+
+    import torch
+
+    from . import _capi as capi
+    from .cases import sphere_channel_case
+    from .solver import Geometry, Level
+
+    case = sphere_channel_case(256, 128, 128, diameter=24.0, centre_x=64.0, u_inlet=0.05, re=1000.0)
+    t0 = time.time()
+    cells, q = sphere_qmap(case.dom, (64.0, 64.0, 64.0), 12.0)
+    out = {"workload": "sphere_channel_256x128x128_D24_Re1000", "storage": storage,
+           "boundary_cells": int(cells.shape[0]), "links": int((q > 0).sum()), "qmap_s": round(time.time() - t0, 2)}
+    g = Geometry(case.dom)
+    st = torch.cuda.current_stream()
+    for run, bc in (("fullway", capi.OAL_SOLID_FULLWAY), ("bouzidi", capi.OAL_SOLID_BOUZIDI),
+                    ("fullway_2", capi.OAL_SOLID_FULLWAY), ("bouzidi_2", capi.OAL_SOLID_BOUZIDI)):
+        L = Level(g, storage=storage)
+        L.init_equilibrium(case.rho, case.vel)
+        if bc == capi.OAL_SOLID_BOUZIDI:
+            L.set_bouzidi(cells, q)
+        p = capi.default_params(**{f: getattr(case.params, f) for f, _ in capi.StepParams._fields_ if f != "reserved"})
+        p.solid_bc = bc
+        p.collect_forces = 0
+        L.execute_timestep_batch(p, 10, stream=st)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        L.execute_timestep_batch(p, steps, stream=st)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        f = L.state()[0]
+        out[run] = {"ms_per_step": round(ms, 4), "mlups": round(256 * 128 * 128 / ms / 1e3, 1),
+                    "finite": bool(np.isfinite(f).all())}
+        L.close()
+    g.close()
+    return out
+
+
+if __name__ == "__main__":
+    import json
+    import sys
+
+    print(json.dumps(bench_step_cost(int(sys.argv[1]) if len(sys.argv) > 1 else 200)))
