@@ -279,8 +279,9 @@ oal_status oal_level_get_forces(oal_level* L, double out[3]);
  * After every step of L with solid_bc OAL_SOLID_BOUZIDI, for each listed cell x and link k:
  * f_out[x, opp k] = 2q f*_k(x) + (1-2q) f*_k(x - c_k) if q < 1/2 (the fall-back when x - c_k is
  * solid or absent), else f*_k(x)/(2q) + (2q-1)/(2q) f*_opp k(x), f* the step's post-collision
- * populations. n_cells = 0 detaches. Plain levels only (no parent, not entropic). Copies the
- * arrays; invalidates L's captured step graphs. */
+ * populations. n_cells = 0 detaches. D3Q27 levels, on their own or of a hierarchy (oal_amr_level:
+ * the correction follows each step of that level, before the restriction onto its parent); not
+ * entropic levels, not batched cases. Copies the arrays; invalidates the captured step graphs. */
 oal_status oal_level_set_bouzidi(oal_level* L, int32_t n_cells, const int32_t* cell_block, const int32_t* cell_x,
                                  const int32_t* cell_y, const int32_t* cell_z, const uint16_t* q_half,
                                  float q_min_threshold, int32_t ff_fallback, float limiter_rel_cap,

@@ -308,6 +308,7 @@ struct oal_level {
   KbcLevel* kbc = nullptr;  // D3Q39 entropic levels: the whole state lives here
   ParentView par{};         // refined level of a block-AMR hierarchy: its parent (set per step)
   BouzidiSet bz;            // linear Bouzidi boundary cells (oal_level_set_bouzidi)
+  uint32_t bz_gen = 0;      // bumped by every oal_level_set_bouzidi (hierarchy graphs compare it)
 };
 
 // ------------------------------------------------------------------------------------------------
@@ -1293,7 +1294,6 @@ oal_status oal_level_set_bouzidi(oal_level* L, int32_t n_cells, const int32_t* c
                                  float limiter_abs_cap) {
   if (!L) return set_error(OAL_E_INVALID_ARG, "null level");
   if (L->kbc) return set_error(OAL_E_UNSUPPORTED, "linear Bouzidi walls are a D3Q27 level path");
-  if (L->par.ptr) return set_error(OAL_E_UNSUPPORTED, "linear Bouzidi walls attach to plain levels, not to refined ones");
   if (n_cells < 0) return set_error(OAL_E_INVALID_ARG, "n_cells %d", n_cells);
   if (ff_fallback < 0 || ff_fallback > 2) return set_error(OAL_E_INVALID_ARG, "ff_fallback %d (0, 1 or 2)", ff_fallback);
   if (!(limiter_rel_cap >= 0.0f) || !(limiter_abs_cap >= 0.0f) || !std::isfinite(q_min_threshold))
@@ -1315,6 +1315,7 @@ oal_status oal_level_set_bouzidi(oal_level* L, int32_t n_cells, const int32_t* c
   OAL_CUDA_TRY(cudaDeviceSynchronize());  // a step in flight may still read the old set
   release_graph(L);
   bouzidi_free(&L->bz);
+  ++L->bz_gen;
   L->bz.q_min = q_min_threshold;
   L->bz.ff_fallback = ff_fallback;
   L->bz.rel_cap = limiter_rel_cap;
@@ -1428,6 +1429,7 @@ struct oal_amr {
   int32_t g_n = 0;
   int g_parity = -1;
   std::vector<oal_step_params> g_p;
+  std::vector<uint32_t> g_bz;  // the levels' Bouzidi generations the graph was captured with
 };
 
 static void amr_release_graph(oal_amr* A) {
@@ -1791,8 +1793,6 @@ oal_status oal_amr_advance(oal_amr* A, const oal_step_params* params, int32_t n,
   for (int l = 0; l < nl; ++l) {
     oal_status s = resolve_params(&params[l], A->lv[(size_t)l].g, &cps[(size_t)l]);
     if (s != OAL_OK) return s;
-    if (cps[(size_t)l].flags & CF_BOUZIDI)
-      return set_error(OAL_E_UNSUPPORTED, "OAL_SOLID_BOUZIDI: the boundary cells attach to plain levels, not to refined levels (oal_amr_*)");
     if (cps[(size_t)l].flags & CF_STORE_POST) return set_error(OAL_E_UNSUPPORTED, "store_post_collision needs caller-owned arrays");
   }
   OAL_CUDA_TRY(cudaSetDevice(A->device));
@@ -1801,7 +1801,8 @@ oal_status oal_amr_advance(oal_amr* A, const oal_step_params* params, int32_t n,
   for (int l = 0; hit && l < nl; ++l) {
     oal_step_params a = params[l], b = A->g_p[(size_t)l];
     a.time_step_seed = b.time_step_seed = 0;
-    hit = std::memcmp(&a, &b, sizeof a) == 0 && !(cps[(size_t)l].flags & CF_INLET_NOISE);
+    hit = std::memcmp(&a, &b, sizeof a) == 0 && !(cps[(size_t)l].flags & CF_INLET_NOISE) &&
+          A->g_bz.size() == (size_t)nl && A->g_bz[(size_t)l] == A->lv[(size_t)l].L->bz_gen;
   }
   std::vector<int> parities((size_t)nl);
   for (int l = 0; l < nl; ++l) parities[(size_t)l] = A->lv[(size_t)l].L->parity;
@@ -1820,6 +1821,8 @@ oal_status oal_amr_advance(oal_amr* A, const oal_step_params* params, int32_t n,
     if (e != cudaSuccess) { cudaGraphDestroy(graph); cudaGetLastError(); return set_error(OAL_E_CUDA, "graph instantiate: %s", cudaGetErrorString(e)); }
     A->exec = exec; A->graph = graph; A->g_n = n; A->g_parity = start;
     A->g_p.assign(params, params + nl);
+    A->g_bz.resize((size_t)nl);
+    for (int l = 0; l < nl; ++l) A->g_bz[(size_t)l] = A->lv[(size_t)l].L->bz_gen;
   }
   OAL_CUDA_TRY(cudaGraphLaunch(A->exec, static_cast<cudaStream_t>(stream)));
   // level l takes n * 2^l steps: only the coarsest level can end on the other buffer

@@ -210,7 +210,12 @@ class OracleAMR:
                 obstacle=None if d.obstacle is None else np.ascontiguousarray(d.obstacle, np.uint8),
                 f=[np.zeros((27, nb, 512), self.dtype), np.zeros((27, nb, 512), self.dtype)],
                 vel=[np.zeros((3, nb, 512), self.dtype), np.zeros((3, nb, 512), self.dtype)],
-                rho=np.ones((nb, 512), self.dtype), parity=0, f_old=None, rho_old=None, vel_old=None))
+                rho=np.ones((nb, 512), self.dtype), parity=0, f_old=None, rho_old=None, vel_old=None, bz=None))
+
+    def set_bouzidi(self, l, bz):
+        """Linear Bouzidi cells of level l (the dict of OracleLevel.step_bouzidi), applied after each of
+        its steps (timestep.jl:1752-1768), before the restriction onto its parent."""
+        self.levels[l]["bz"] = bz
 
     def init_equilibrium(self, l, rho, vel, compressible=0):
         L = self.levels[l]
@@ -253,6 +258,15 @@ class OracleAMR:
                     _p(Pa["rho_old"]), _p(Pa["vel_old"]), float(params[l - 1].tau), float(tw), 1)
         P.time_step_seed = seed
         assert rc == 0
+        bz = L["bz"]
+        if bz is not None and P.solid_bc == 3:
+            post = f_out.copy()  # the step stores the post-collision populations as its output
+            cells = np.ascontiguousarray(bz["cells"], np.int32)
+            qf = np.ascontiguousarray(np.asarray(bz["q"], np.float16).astype(np.float32))
+            fb = getattr(lib(), f"ora_bouzidi_linear_{self._suf()}")
+            assert fb(L["nb"], _p(L["nbr"]), _p(L["obstacle"]), int(cells.shape[0]), _p(cells), _p(qf),
+                      bz.get("q_min", 0.001), int(bz.get("ff_fallback", 0)), bz.get("rel_cap", 0.0),
+                      bz.get("abs_cap", 0.0), _p(post), _p(f_out)) == 0
         L["parity"] ^= 1
         if has_children:
             self._step(l + 1, params, 2 * t_sub, 0.0)

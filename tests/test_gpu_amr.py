@@ -145,3 +145,46 @@ def test_uniform_flow_fp32(env):
         _, r, v = H.level(l).state()
         assert np.max(np.abs(r - 1)) < 2e-6 and np.max(np.abs(v[0] - u)) < 2e-6 and np.max(np.abs(v[1:])) < 2e-6
     H.close()
+
+
+@pytest.mark.parametrize("storage,tol", [("f64", 1e-10), ("f32", 5e-5)])
+def test_channel_bouzidi_on_the_fine_level(env, storage, tol):
+    """The linear Bouzidi wall on the sphere of the refined level (the reference applies it on the
+    finest level, bouzidi_levels = 1): the correction follows each fine step, before the
+    restriction, in the captured hierarchy graph; a second advance reuses the graph."""
+    oracle, amr, solver = env
+    from openaerolab_alpha_01_b200 import _capi as capi
+    from openaerolab_alpha_01_b200.bouzidi import sphere_qmap
+    coarse = solver.build_box(6, 2, 2)
+    fine = amr.refine(coarse, amr.blocks_in_box(coarse, (16, 0, 0), (32, 16, 16)))
+    solver.apply_analytic_sphere_obstacle(fine, (48.0, 16.0, 16.0), 5.0)
+    cells, q = sphere_qmap(fine, (48.0, 16.0, 16.0), 5.0)
+    doms = [coarse, fine]
+    u = 0.05
+    rho_fn = lambda X, Y, Z: np.ones_like(X)
+    vel_fn = lambda X, Y, Z: np.stack([u + 0 * X, 0.01 * np.sin(2 * np.pi * Y / 16), 0 * X])
+    P = params(amr.level_taus(0.53, 2), c_wale=0.2, u_inlet=u)
+    for p in P:
+        p.solid_bc = capi.OAL_SOLID_BOUZIDI
+        p.collect_forces = 0
+    dt = np.float64 if storage == "f64" else np.float32
+    ora = oracle.OracleAMR(doms, dt)
+    H = amr.Hierarchy(doms, storage=storage)
+    for l, d in enumerate(doms):
+        gx, gy, gz = d.cell_positions()
+        s = 2.0 ** l
+        X, Y, Z = (gx - 0.5) / s, (gy - 0.5) / s, (gz - 0.5) / s
+        H.level(l).init_equilibrium(rho_fn(X, Y, Z), vel_fn(X, Y, Z))
+    for l in range(2):
+        f, r, v = H.level(l).state()
+        ora.levels[l]["f"][0][...] = f
+        ora.levels[l]["rho"][...] = r
+        ora.levels[l]["vel"][0][...] = v
+    H.level(1).set_bouzidi(cells, q)
+    ora.set_bouzidi(1, dict(cells=cells, q=q))
+    H.advance(P, 2)
+    ora.advance(P, 2)
+    H.advance(P, 2)
+    ora.advance(P, 2)
+    compare(H, ora, 2, tol)
+    H.close()
