@@ -65,7 +65,8 @@ def traffic_record(storage):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 20 ms while the sampler is open; the
+    timed region starts only after the first sample has been written."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -80,10 +81,17 @@ class ClockSampler:
         try:
             self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=self.file, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return self
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.proc.poll() is None:
+            self.file.flush()
+            if os.path.getsize(self.file.name) > 0:
+                break
+            time.sleep(0.01)
         return self
 
     def __exit__(self, *a):
@@ -124,20 +132,18 @@ class ClockSampler:
 # ---------------------------------------------------------------------------------------------
 def cpu_sample_case():
     """Bounded sample of the workload: a 256 x 128 x 16 slab of the channel (same inlet, outlet,
-    mirror faces and sphere centre line, sphere cut by the slab), 524,288 cells."""
-    from openaerolab_alpha_01_b200.cases import sphere_channel_case
-    return sphere_channel_case(256, 128, 16, diameter=24.0, centre_x=64.0)
+    mirror faces and sphere centre line, sphere cut by the slab), 524,288 cells, built by the
+    oracle's own block builder and sphere mask (the product library is not loaded)."""
+    import oracle
+    return oracle.sphere_channel(256, 128, 16, diameter=24.0, centre_x=64.0)
 
 
 def run_cpu_arm(steps, warmup, target_s=None):
     """Time the FP32 oracle on every host thread; returns (MLUPS, cores, steps_done, seconds)."""
-    import oracle
     cores = os.cpu_count() or 1
     os.environ["OMP_NUM_THREADS"] = str(cores)
     case = cpu_sample_case()
-    d = case.dom
-    O = oracle.OracleLevel(d.coords, d.neighbor_table, d.shape, obstacle=d.obstacle, dtype=np.float32)
-    O.init_equilibrium(case.rho, case.vel)
+    O = case.level(np.float32)
     p = case.params
     for _ in range(warmup):
         O.step(p)
@@ -152,7 +158,7 @@ def run_cpu_arm(steps, warmup, target_s=None):
         if target_s is not None and (el >= target_s or done >= steps):
             break
     el = time.perf_counter() - t0
-    cells = d.n_blocks * 512
+    cells = case.n_blocks * 512
     return cells * done / el / 1e6, cores, done, el, cells
 
 
@@ -199,8 +205,19 @@ def main():
                     help="steps of the D3Q19 octree periodic-box measurement (256^3, FP32 and FP64); 0 skips it")
     ap.add_argument("--kbc-steps", type=int, default=20,
                     help="steps of the D3Q39 entropic KBC measurement (128^3 periodic Taylor-Green, FP32); 0 skips it")
-    ap.add_argument("--batch-steps", type=int, default=200,
+    ap.add_argument("--batch-steps", type=int, default=2000,
                     help="steps of the batched-vs-plain-loop comparison (64-case config 4); 0 skips it")
+    ap.add_argument("--steady-seconds", type=float, default=1.0,
+                    help="length of the steady-state pass timed after the K steps (clock record and MLUPS)")
+    ap.add_argument("--tgv-steps", type=int, default=1000,
+                    help="steps of the 64^3 FP64 Taylor-Green accuracy run (config 1); 0 skips it")
+    ap.add_argument("--drag-steps", type=int, default=20000,
+                    help="steps of the config-2 drag accuracy run per storage (FP64, FP32, FP16, BF16); 0 skips it")
+    ap.add_argument("--drag-avg", type=int, default=5000, help="steps the drag coefficient is averaged over")
+    ap.add_argument("--serve-requests", type=int, default=24,
+                    help="requests of the served-vs-sequential comparison (config 5 mix); 0 skips it")
+    ap.add_argument("--serve-steps", type=int, default=2000, help="steps per served request")
+    ap.add_argument("--serve-kbc-share", type=float, default=0.25, help="fraction of D3Q39 KBC requests served")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -265,13 +282,25 @@ def main():
                 ev[i][1].record(stream)
             t_end.record(stream)
         torch.cuda.synchronize()
+        # steady-state pass of at least --steady-seconds, so that the clock record holds samples
+        # under load even when the K timed steps take milliseconds
+        n_steady = max(args.steps, int(args.steady_seconds * 1e3 / max(t_begin.elapsed_time(t_end) / args.steps, 1e-3)))
+        s_begin, s_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            s_begin.record(stream)
+            for i in range(n_steady):
+                p.time_step_seed = args.warmup + args.steps + i
+                level.perform_timestep(p, sh)
+            s_end.record(stream)
+        torch.cuda.synchronize()
     barrier()
     total_ms = t_begin.elapsed_time(t_end)
+    steady_ms = s_begin.elapsed_time(s_end)
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    t = torch.tensor([total_ms, steady_ms], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms, steady_ms = float(t[0].item()), float(t[1].item())
     force = level.forces()
 
     # ---- end-to-end through the public API: per step the step parameters go from pinned host
@@ -283,7 +312,7 @@ def main():
     t0 = time.perf_counter()
     with torch.cuda.stream(stream):
         for i in range(e2e_steps):
-            p.time_step_seed = args.warmup + args.steps + i
+            p.time_step_seed = args.warmup + args.steps + n_steady + i
             level.perform_timestep(p, sh)
             level.forces_async(pinned_force.data_ptr(), sh)
             stream.synchronize()
@@ -320,9 +349,15 @@ def main():
             # per step: ghost fill, fast kernel, general kernel (blocks at the sphere), FP64 drag reduction
             "gpu_launches": 4 * args.steps,
             "clocks": cs,
+            "steady": {"steps": n_steady, "seconds": round(steady_ms / 1e3, 3),
+                       "ms_per_step": round(steady_ms / n_steady, 4),
+                       "mlups": round(world * cells * n_steady / (steady_ms * 1e-3) / 1e6, 2),
+                       "note": "timed after the K steps under the same clock record"},
             "drag_fx_lattice": force[0],
-            "cd": force[0] * case.meta["drag_scale"],
+            "cd_after_timed_steps": force[0] * case.meta["drag_scale"],
         }
+    extras = rank == 0 and world == 1
+    if extras:
         if args.q19_steps > 0:
             from openaerolab_alpha_01_b200.octree import benchmark_periodic_box
             q = [benchmark_periodic_box(256, args.q19_steps, precision=dt) for dt in (np.float32, np.float64)]
@@ -342,6 +377,17 @@ def main():
         if args.batch_steps > 0:
             from openaerolab_alpha_01_b200.workloads import config4
             line["batched"] = config4(steps=args.batch_steps, storage=args.storage)
+        if args.tgv_steps > 0:
+            from openaerolab_alpha_01_b200.validation import taylor_green_64
+            line["config1"] = [taylor_green_64(steps=args.tgv_steps, c_wale=cw) for cw in (0.0, 0.2)]
+        if args.drag_steps > 0:
+            from openaerolab_alpha_01_b200.validation import sphere_drag
+            line["drag_check"] = sphere_drag(args.drag_steps, args.drag_avg)
+        if args.serve_requests > 0:
+            from openaerolab_alpha_01_b200.server import config5
+            line["served"] = config5(args.serve_requests, 20.0, args.serve_steps, args.storage,
+                                     kbc_share=args.serve_kbc_share)
+    if rank == 0:
         print(json.dumps(line), flush=True)
 
     level.close()

@@ -73,7 +73,8 @@ enum CaseFlags : uint32_t {
   CF_PERIODIC_Y = 1u << 16,
   CF_PERIODIC_Z = 1u << 17,
   CF_GRAD_WALL = 1u << 18,   // Grad-reconstruction wall on fluid cells with links into solids
-  CF_BOUZIDI = 1u << 19      // linear Bouzidi correction after the step (the step itself is full-way)
+  CF_BOUZIDI = 1u << 19,     // linear Bouzidi correction after the step (the step itself is full-way)
+  CF_GENERAL_RATES = 1u << 20  // omega_bulk, omega3 or omega4 differs from 1 (the configuration default)
 };
 
 struct CaseParams {

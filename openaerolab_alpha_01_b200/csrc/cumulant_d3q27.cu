@@ -26,6 +26,7 @@
 #include "common.cuh"
 #include "vmath.cuh"
 #include "cumulant_math.cuh"
+#include "pairs_math.cuh"
 
 // Tuning knobs of the uniform kernel (compile time): resident CTAs per SM the register budget
 // is sized for, and cells per thread (2 = packed f32x2 pairs, 1 = scalar float).
@@ -52,6 +53,11 @@
 // (measured on the config-2 channel: 64 best, 128 1 % slower, 32 2 %, 256 12 %)
 #ifndef OAL_PAIRS_THREADS
 #define OAL_PAIRS_THREADS 64
+#endif
+// resident warps per SM the x-pair kernel's registers are sized for (20: 96 registers, no
+// spills; 16 was 11 % slower on the config-2 channel, 24 spills and was 2 % slower)
+#ifndef OAL_PAIRS_WARPS
+#define OAL_PAIRS_WARPS 20
 #endif
 
 namespace oal {
@@ -864,11 +870,30 @@ template <> __device__ __forceinline__ uint2 pair_word<float>(F2 v, int) {
   return make_uint2(__float_as_uint(a), __float_as_uint(b));
 }
 
+// two deviations -> the stored 16-bit pair, rounded to nearest
+template <class S> __device__ __forceinline__ uint32_t pack_dev(F2 d);
+template <> __device__ __forceinline__ uint32_t pack_dev<__half>(F2 d) {
+  float a, b;
+  f2split(d, a, b);
+  const __half2 h = __floats2half2_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+template <> __device__ __forceinline__ uint32_t pack_dev<__nv_bfloat16>(F2 d) {
+  float a, b;
+  f2split(d, a, b);
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+template <> __device__ __forceinline__ uint32_t pack_dev<float>(F2) { return 0u; }
+
 // Library-owned block-major layout; IDX indexes words (pairs): block stride 27*256, direction
 // stride 256, row (y, z) stride 4 and 32.
 // POS: some case of the launch uses the positivity limiter (its code is left out otherwise).
-template <class S, class IDX, bool POS>
-__global__ void __launch_bounds__(OAL_PAIRS_THREADS, OAL_FAST_MIN_CTAS * 128 / OAL_PAIRS_THREADS) k_cumulant_pairs(const StepArgs a, const int32_t* __restrict__ work) {
+// GEN: some case of the launch relaxes with omega_bulk, omega3 or omega4 other than 1.
+template <class S, class IDX, bool POS, bool GEN>
+__global__ void __launch_bounds__(OAL_PAIRS_THREADS, OAL_PAIRS_WARPS * 32 / OAL_PAIRS_THREADS) k_cumulant_pairs(const StepArgs a, const int32_t* __restrict__ work) {
+  constexpr bool DEV = !std::is_same<S, float>::value;  // 16-bit deviation codec
+  constexpr float E = PairScale<DEV>::E;
   using W = typename PairWord<S>::W;
   using V = F2;
   using T = float;
@@ -972,46 +997,25 @@ __global__ void __launch_bounds__(OAL_PAIRS_THREADS, OAL_FAST_MIN_CTAS * 128 / O
   // WALE eddy viscosity from the stencil
   V nu_eddy = splat<V>(T(0));
   if (grad) {
+    // twice the central differences (wale_nu_2g absorbs the factor)
     V g[3][3];
-    const V h = splat<V>(T(0.5));
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      g[c][0] = h * (f2(vo[c].y, vxp[c]) - f2(vxm[c], vo[c].x));
-      g[c][1] = h * (f2(vyp[c].x, vyp[c].y) - f2(vym[c].x, vym[c].y));
-      g[c][2] = h * (f2(vzp[c].x, vzp[c].y) - f2(vzm[c].x, vzm[c].y));
+      g[c][0] = f2(vo[c].y, vxp[c]) - f2(vxm[c], vo[c].x);
+      g[c][1] = f2(vyp[c].x, vyp[c].y) - f2(vym[c].x, vym[c].y);
+      g[c][2] = f2(vzp[c].x, vzp[c].y) - f2(vzm[c].x, vzm[c].y);
     }
-    nu_eddy = wale_nu<V>(g[0][0], g[0][1], g[0][2], g[1][0], g[1][1], g[1][2], g[2][0], g[2][1], g[2][2], cp.c_wale);
+    nu_eddy = wale_nu_2g(g[0][0], g[0][1], g[0][2], g[1][0], g[1][1], g[1][2], g[2][0], g[2][1], g[2][2], cp.c_wale);
   }
 
-  // velocity-free x sums of the chimera transform: m0 = a + b + c, m1 = c - a, m2 = a + c
-#pragma unroll
-  for (int n = 0; n < 9; ++n) {
-    V& a0 = A[3 * n];
-    V& b0 = A[3 * n + 1];
-    V& c0 = A[3 * n + 2];
-    if constexpr (std::is_same<S, float>::value) {
-      chimera_xsums(a0, b0, c0);
-    } else {
-      // a = wa (1 + da), b = wb (1 + db), c = wa (1 + dc)
-      const float wa = float(q27_w(3 * n)), wb = float(q27_w(3 * n + 1));
-      const V m2 = vfma(splat<V>(wa), a0 + c0, splat<V>(2.0f * wa));
-      const V m1 = splat<V>(wa) * (c0 - a0);
-      a0 = vfma(splat<V>(wb), b0, m2 + splat<V>(wb));
-      b0 = m1;
-      c0 = m2;
-    }
-  }
-  // density and momentum from the x sums (triplet n has c_y = n % 3 - 1, c_z = n / 3 - 1)
-  const V r0 = (A[0] + A[3]) + A[6], r1 = (A[9] + A[12]) + A[15], r2 = (A[18] + A[21]) + A[24];
-  const V ym = (A[0] + A[9]) + A[18], yp = (A[6] + A[15]) + A[24];
-  V rho = (r0 + r1) + r2;
-  const V jx = (((A[1] + A[4]) + (A[7] + A[10])) + ((A[13] + A[16]) + (A[19] + A[22]))) + A[25];
-  const V jy = yp - ym, jz = r2 - r0;
-
-  // ---- macros (kernel_cumulant.jl:424-431) ----
-  rho = vmaxc(rho, T(0.01));
-  const V inv_rho = vrcp(rho);
-  const V ux = jx * inv_rho, uy = jy * inv_rho, uz = jz * inv_rho;
+  // raw moments (density and momentum among them), then the macros (kernel_cumulant.jl:424-431)
+  raw_moments<DEV, GEN>(A);
+  const V m000 = A[0];  // E x the unclamped density
+  const V rc = pmaxc(m000, 0.01f * E);
+  const V inv = vrcp(rc);
+  const V i4 = DEV ? inv * splat<V>(0.25f) : inv;
+  const V ux = i4 * A[1], uy = i4 * A[3], uz = i4 * A[9];
+  const V rho = DEV ? rc * splat<V>(1.0f / E) : rc;
   {
     float r_0, r_1, a0, a1;
     f2split(rho, r_0, r_1);
@@ -1021,14 +1025,37 @@ __global__ void __launch_bounds__(OAL_PAIRS_THREADS, OAL_FAST_MIN_CTAS * 128 / O
     f2split(uz, a0, a1); reinterpret_cast<float2*>(vel_out + cown + 2 * vcs)[0] = make_float2(a0, a1);
   }
 
-  const V omega1 = omega1_from<V>(nu_eddy, cp);
+  const V omega1 = omega1_pairs(nu_eddy, cp);
+  collide_scaled<DEV, GEN>(A, inv, ux, uy, uz, omega1, cp);
 
-  cumulant_collide_xsums<V, POS>(A, rho, ux, uy, uz, omega1, cp);
-
-  // ---- store (kernel_cumulant.jl:889-908 with zero force) ----
+  // ---- store (kernel_cumulant.jl:889-908 with zero force): A[k] = f_k 2^n / rho_raw ----
   W* __restrict__ o = fout + (IDX)b * wbst + (IDX)(i + 4 * y + 32 * z);
+  if (POS && (cp.flags & CF_LIMITER_POSITIVITY)) {
+    // positivity limiter (kernel_cumulant.jl:849-884) on the populations themselves
+    const V rr = DEV ? m000 * splat<V>(1.0f / E) : m000;
+    const V sc[4] = {rr, rr * splat<V>(0.5f), rr * splat<V>(0.25f), rr * splat<V>(0.125f)};
 #pragma unroll
-  for (int k = 0; k < kQ27; ++k) o[k * wkst] = pair_word<S>(A[k], k);
+    for (int k = 0; k < kQ27; ++k) A[k] = A[k] * sc[q27_d2(k)];
+    V fmin = A[0];
+#pragma unroll
+    for (int k = 1; k < kQ27; ++k) fmin = vmin(fmin, A[k]);
+    if (vany_gt(splat<V>(0.0f), fmin)) positivity_blend<V>(A, fmin, rho, ux, uy, uz, (cp.flags & CF_COMPRESSIBLE) != 0);
+#pragma unroll
+    for (int k = 0; k < kQ27; ++k) o[k * wkst] = pair_word<S>(A[k], k);
+    return;
+  }
+  if constexpr (DEV) {
+    // d_k = f_k / w_k - 1 = A[k] (27/8 rho_raw) 2^n - 1
+    const V c0 = m000, c1 = c0 + c0, c2 = c1 + c1, c3 = c2 + c2;
+    const V sc[4] = {c0, c1, c2, c3};
+#pragma unroll
+    for (int k = 0; k < kQ27; ++k) o[k * wkst] = pack_dev<S>(vfma(A[k], sc[q27_d2(k)], splat<V>(-1.0f)));
+  } else {
+    const V c0 = m000, c1 = c0 * splat<V>(0.5f), c2 = c0 * splat<V>(0.25f), c3 = c0 * splat<V>(0.125f);
+    const V sc[4] = {c0, c1, c2, c3};
+#pragma unroll
+    for (int k = 0; k < kQ27; ++k) o[k * wkst] = pair_word<S>(A[k] * sc[q27_d2(k)], k);
+  }
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -1440,12 +1467,13 @@ cudaError_t launch_fast(const StepArgs& a, const int32_t* work, int n_work, cuda
   } else {
     // x pairs; word indices (half the element count) decide the index width
     const unsigned grid = (unsigned)n_work * (256u / OAL_PAIRS_THREADS);
-    if (a.flags_any & CF_LIMITER_POSITIVITY) {
-      if (idx32) k_cumulant_pairs<S, uint32_t, true><<<grid, OAL_PAIRS_THREADS, 0, st>>>(a, work);
-      else k_cumulant_pairs<S, int64_t, true><<<grid, OAL_PAIRS_THREADS, 0, st>>>(a, work);
+    const bool pos = (a.flags_any & CF_LIMITER_POSITIVITY) != 0, gen = (a.flags_any & CF_GENERAL_RATES) != 0;
+    if (pos || gen) {
+      if (idx32) k_cumulant_pairs<S, uint32_t, true, true><<<grid, OAL_PAIRS_THREADS, 0, st>>>(a, work);
+      else k_cumulant_pairs<S, int64_t, true, true><<<grid, OAL_PAIRS_THREADS, 0, st>>>(a, work);
     } else {
-      if (idx32) k_cumulant_pairs<S, uint32_t, false><<<grid, OAL_PAIRS_THREADS, 0, st>>>(a, work);
-      else k_cumulant_pairs<S, int64_t, false><<<grid, OAL_PAIRS_THREADS, 0, st>>>(a, work);
+      if (idx32) k_cumulant_pairs<S, uint32_t, false, false><<<grid, OAL_PAIRS_THREADS, 0, st>>>(a, work);
+      else k_cumulant_pairs<S, int64_t, false, false><<<grid, OAL_PAIRS_THREADS, 0, st>>>(a, work);
     }
   }
   return cudaGetLastError();

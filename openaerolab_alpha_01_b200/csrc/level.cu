@@ -360,6 +360,7 @@ static oal_status resolve_params(const oal_step_params* p, const oal_geometry* g
   if (p->store_post_collision == 1) f |= CF_STORE_POST;
   if (p->c_wale != 0.0f) f |= CF_GRADIENTS;
   if (p->inlet_turbulence > 0.0f) f |= CF_INLET_NOISE;
+  if (p->omega_bulk != 1.0f || p->omega3 != 1.0f || p->omega4 != 1.0f) f |= CF_GENERAL_RATES;
   cp->flags = f;
   return OAL_OK;
 }

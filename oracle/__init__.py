@@ -38,6 +38,7 @@ def lib() -> C.CDLL:
         vp = C.c_void_p
         i32 = C.c_int32
         L.ora_d3q27_tables.argtypes = [vp] * 7
+        L.ora_default_step_params.argtypes = [vp]
         L.ora_build_box.argtypes = [i32, i32, i32, i32, vp, vp]
         L.ora_sphere.argtypes = [i32, vp, C.c_double, C.c_double, C.c_double, C.c_double, vp]
         L.ora_sphere.restype = C.c_int64
@@ -109,6 +110,51 @@ def sphere(coords, centre, radius):
     obst = np.zeros((nb, 512), np.uint8)
     n = lib().ora_sphere(nb, _p(np.ascontiguousarray(coords, np.int32)), *map(float, centre), float(radius), _p(obst))
     return obst, int(n)
+
+
+def default_step_params(**overrides):
+    """oal_step_params with the reference's configuration defaults, filled by the oracle library
+    (the struct type is the product's ctypes mirror of include/oal.h; no product code is loaded)."""
+    from openaerolab_alpha_01_b200._capi import StepParams
+    p = StepParams()
+    lib().ora_default_step_params(C.addressof(p))
+    for k, v in overrides.items():
+        if not hasattr(p, k):
+            raise AttributeError(k)
+        setattr(p, k, v)
+    return p
+
+
+class OracleCase:
+    """A case built by the oracle alone: coords, neighbour table, obstacle, shape, initial fields
+    and the step parameters."""
+
+    def __init__(self, coords, nbr, shape, obstacle, rho, vel, params, meta):
+        self.coords, self.nbr, self.shape, self.obstacle = coords, nbr, shape, obstacle
+        self.rho, self.vel, self.params, self.meta = rho, vel, params, meta
+
+    @property
+    def n_blocks(self):
+        return int(self.coords.shape[0])
+
+    def level(self, dtype=np.float32):
+        L = OracleLevel(self.coords, self.nbr, self.shape, obstacle=self.obstacle, dtype=dtype)
+        L.init_equilibrium(self.rho, self.vel)
+        return L
+
+
+def sphere_channel(nx=256, ny=128, nz=128, diameter=24.0, centre_x=64.0, u_inlet=0.05, re=1000.0, c_wale=0.2):
+    """The sphere channel (inlet at x_min, zero-gradient outlet, lateral mirrors, analytic sphere with
+    half-way walls and the drag collected) from the oracle's own block builder and sphere mask."""
+    coords, nbr = build_box(nx // 8, ny // 8, nz // 8, 0)
+    obst, n_solid = sphere(coords, (centre_x, ny / 2.0, nz / 2.0), diameter / 2.0)
+    nb = coords.shape[0]
+    rho = np.ones((nb, 512))
+    vel = np.zeros((3, nb, 512))
+    vel[0] = np.where(obst != 0, 0.0, u_inlet)
+    nu = u_inlet * diameter / re
+    p = default_step_params(tau=3.0 * nu + 0.5, c_wale=c_wale, u_inlet=u_inlet, solid_bc=1, collect_forces=1)
+    return OracleCase(coords, nbr, (nx, ny, nz), obst, rho, vel, p, dict(n_solid=n_solid, nu=nu))
 
 
 def init_feq(rho, vel, compressible=0):

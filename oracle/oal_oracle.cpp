@@ -1113,6 +1113,31 @@ void bouzidi_linear(const Level& L, int32_t n, const int32_t* cells, const float
 
 extern "C" {
 
+// Configuration defaults of the cumulant level step (src/io/config_loader.jl:1305-1380,
+// src/collision/timestep.jl:1127), so that CPU-only callers need nothing from the product library.
+void ora_default_step_params(oal_step_params* p) {
+  std::memset(p, 0, sizeof *p);
+  p->abi_version = OAL_ABI_VERSION;
+  p->operator_id = OAL_OP_CUMULANT_D3Q27;
+  p->tau = 0.6f;
+  p->tau_parent = 0.6f;
+  p->c_wale = 0.20f;                 // config_loader.jl:1305
+  p->amr_sgs_scale = 1.0f;           // timestep.jl:1127
+  p->omega_bulk = 1.0f;              // config_loader.jl:1373
+  p->omega3 = 1.0f;                  // :1374
+  p->omega4 = 1.0f;                  // :1375
+  p->adaptive_omega4 = 1;            // :1376
+  p->lambda_param = 1.0f / 6.0f;     // :1377
+  p->limiter_type = OAL_LIMITER_FACTORED;  // :1379
+  p->u_inlet = 0.05f;
+  p->wall_model_max_distance = 10.0f;
+  p->transverse_freestream_blend = 1.0f;
+  p->solid_bc = OAL_SOLID_FULLWAY;
+  p->temporal_weight = 1.0f;
+  p->hrr_sigma = 1.0f;
+  p->grad_pineq_scale = 1.0f;        // config_loader.jl:898
+}
+
 // D3Q27 tables in the reference order (0-based indices for opp/mirrors).
 void ora_d3q27_tables(int32_t* cx, int32_t* cy, int32_t* cz, double* w, int32_t* opp, int32_t* mir_y,
                       int32_t* mir_z) {
