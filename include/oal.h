@@ -242,7 +242,16 @@ oal_status oal_level_create(const oal_geometry* g, int32_t operator_id, int32_t 
                             oal_level** out);
 void oal_level_destroy(oal_level* L);
 /* Level creation options (bits of `flags`). */
-enum { OAL_LEVEL_DENSE = 1 /* box levels in FP32/FP16/BF16: dense padded population grid */ };
+enum {
+  OAL_LEVEL_DENSE = 1,         /* box levels in FP32/FP16/BF16: dense padded population grid */
+  OAL_LEVEL_ROUND_NEAREST = 2  /* FP16/BF16 deviation storage: the step kernels round the stored
+                                  deviations to nearest. Default: stochastic rounding (hardware
+                                  cvt.rs, random bits hashed from the cell's position in its case
+                                  and its new macros), unbiased in expectation, which keeps
+                                  integrated quantities such as the drag free of the rounding bias
+                                  of a slowly varying state. No counterpart in the reference (its
+                                  populations are Float32). */
+};
 /* oal_level_create with options; flags = 0 is oal_level_create. */
 oal_status oal_level_create_ex(const oal_geometry* g, int32_t operator_id, int32_t storage, uint32_t flags,
                                oal_level** out);

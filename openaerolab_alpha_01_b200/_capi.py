@@ -43,6 +43,7 @@ OAL_LIMITER_FACTORED = 1
 OAL_LIMITER_POSITIVITY = 2
 
 OAL_LEVEL_DENSE = 1
+OAL_LEVEL_ROUND_NEAREST = 2
 
 OAL_SOLID_FULLWAY = 0
 OAL_SOLID_HALFWAY = 1

@@ -172,6 +172,7 @@ struct StepArgs {
   int32_t PX, PY, PZ;
   uint32_t* err;                  // device error word (bounded waits that gave up), or null
   uint32_t flags_any;             // OR of the flags of every case of the launch (kernel selection)
+  int32_t round_nearest;          // 16-bit codecs: round stored deviations to nearest (else stochastically)
   CaseParams p0;
   ParentView par;                 // refined levels only (par.ptr == null otherwise)
 };

@@ -54,10 +54,15 @@
 #ifndef OAL_PAIRS_THREADS
 #define OAL_PAIRS_THREADS 64
 #endif
-// resident warps per SM the x-pair kernel's registers are sized for (20: 96 registers, no
-// spills; 16 was 11 % slower on the config-2 channel, 24 spills and was 2 % slower)
+// resident warps per SM the x-pair kernel's registers are sized for, 16-bit storage (20: 96
+// registers; 16 was 11 % slower on the FP16 config-2 channel, 24 spilled and was 2 % slower) and
+// FP32 storage and the general-rate or positivity-limiter instances (whose wider state needs the
+// 128 registers of 16 warps)
 #ifndef OAL_PAIRS_WARPS
 #define OAL_PAIRS_WARPS 20
+#endif
+#ifndef OAL_PAIRS_WARPS_WIDE
+#define OAL_PAIRS_WARPS_WIDE 16
 #endif
 
 namespace oal {
@@ -870,6 +875,51 @@ template <> __device__ __forceinline__ uint2 pair_word<float>(F2 v, int) {
   return make_uint2(__float_as_uint(a), __float_as_uint(b));
 }
 
+// Stochastic rounding of the 16-bit deviations (the default writer of FP16/BF16 levels): the
+// hardware conversion cvt.rs adds the random bits below the format's last place and truncates,
+// so a stored value is unbiased in expectation; rounding to nearest rounds a slowly varying state
+// the same way step after step, a bias that shows in integrated quantities (the sphere drag of
+// the 256 x 128 x 128 channel drifts 3-5 % from FP64 in FP16 and up to 25 % in BF16 within 10,000
+// steps with nearest rounding, 0.1-0.3 % and ~1 % with stochastic rounding). The random bits
+// are a hash of the cell's position in its case and the low bits of the cell's new density and
+// velocity, which change whenever the state does: a deterministic function of the case's own
+// state, so single steps, captured graphs and batched members store identical values (no step
+// counter to keep in step). The random operand's low 16 bits feed the lower half of the pair and
+// its high 16 bits the upper half.
+__device__ __forceinline__ uint32_t sr_hash(int gx, int gy, int gz, uint32_t state) {
+  uint32_t h = (uint32_t)gx * 0x9E3779B1u ^ (uint32_t)gy * 0x85EBCA77u ^ (uint32_t)gz * 0xC2B2AE3Du ^ state;
+  h ^= h >> 16; h *= 0x7feb352du; h ^= h >> 15; h *= 0x846ca68bu; h ^= h >> 16;
+  return h;
+}
+// odd multipliers: independent random words per direction from one hash
+__host__ __device__ constexpr uint32_t sr_mult(int k) { return (2u * (uint32_t)k + 1u) * 0x9E3779B1u; }
+template <class S> __device__ __forceinline__ uint32_t pack_dev_rs(F2 d, uint32_t r);
+template <> __device__ __forceinline__ uint32_t pack_dev_rs<__half>(F2 d, uint32_t r) {
+  float a, b;
+  f2split(d, a, b);
+  uint32_t out;
+  asm("cvt.rs.satfinite.f16x2.f32 %0, %1, %2, %3;" : "=r"(out) : "f"(b), "f"(a), "r"(r));
+  return out;
+}
+template <> __device__ __forceinline__ uint32_t pack_dev_rs<__nv_bfloat16>(F2 d, uint32_t r) {
+  float a, b;
+  f2split(d, a, b);
+  uint32_t out;
+  asm("cvt.rs.satfinite.bf16x2.f32 %0, %1, %2, %3;" : "=r"(out) : "f"(b), "f"(a), "r"(r));
+  return out;
+}
+template <> __device__ __forceinline__ uint32_t pack_dev_rs<float>(F2, uint32_t) { return 0u; }
+// one deviation (lower half of the conversion, low 16 random bits)
+template <class S> __device__ __forceinline__ S enc_rs(float d, uint32_t r) {
+  uint32_t out;
+  if constexpr (std::is_same<S, __half>::value)
+    asm("cvt.rs.satfinite.f16x2.f32 %0, %1, %2, %3;" : "=r"(out) : "f"(0.0f), "f"(d), "r"(r));
+  else
+    asm("cvt.rs.satfinite.bf16x2.f32 %0, %1, %2, %3;" : "=r"(out) : "f"(0.0f), "f"(d), "r"(r));
+  const unsigned short lo = (unsigned short)(out & 0xFFFFu);
+  return *reinterpret_cast<const S*>(&lo);
+}
+
 // two deviations -> the stored 16-bit pair, rounded to nearest
 template <class S> __device__ __forceinline__ uint32_t pack_dev(F2 d);
 template <> __device__ __forceinline__ uint32_t pack_dev<__half>(F2 d) {
@@ -891,7 +941,7 @@ template <> __device__ __forceinline__ uint32_t pack_dev<float>(F2) { return 0u;
 // POS: some case of the launch uses the positivity limiter (its code is left out otherwise).
 // GEN: some case of the launch relaxes with omega_bulk, omega3 or omega4 other than 1.
 template <class S, class IDX, bool POS, bool GEN>
-__global__ void __launch_bounds__(OAL_PAIRS_THREADS, OAL_PAIRS_WARPS * 32 / OAL_PAIRS_THREADS) k_cumulant_pairs(const StepArgs a, const int32_t* __restrict__ work) {
+__global__ void __launch_bounds__(OAL_PAIRS_THREADS, ((sizeof(S) == 4 || GEN || POS) ? OAL_PAIRS_WARPS_WIDE : OAL_PAIRS_WARPS) * 32 / OAL_PAIRS_THREADS) k_cumulant_pairs(const StepArgs a, const int32_t* __restrict__ work) {
   constexpr bool DEV = !std::is_same<S, float>::value;  // 16-bit deviation codec
   constexpr float E = PairScale<DEV>::E;
   using W = typename PairWord<S>::W;
@@ -900,6 +950,7 @@ __global__ void __launch_bounds__(OAL_PAIRS_THREADS, OAL_PAIRS_WARPS * 32 / OAL_
   constexpr IDX wbst = 27 * kCells / 2, wkst = kCells / 2;
   __shared__ IDX s_wbase[28];  // first word of each neighbour block
   __shared__ int32_t s_nbr[28];
+  __shared__ int4 s_bi;        // the block's coordinates in its case (stochastic rounding)
   __shared__ CaseParams s_cp;
   const int tid = threadIdx.x;
   // a CTA covers OAL_PAIRS_THREADS / 32 z planes of a block (one warp per plane)
@@ -910,6 +961,8 @@ __global__ void __launch_bounds__(OAL_PAIRS_THREADS, OAL_PAIRS_WARPS * 32 / OAL_
     const int32_t nb = a.nbr[(int64_t)b * 27 + tid];
     s_nbr[tid] = nb;
     s_wbase[tid] = (IDX)nb * wbst;
+  } else if (DEV && tid == 27) {
+    s_bi = a.binfo[b];
   }
   // the case parameters: copied by the second warp, or by the first one in one-warp CTAs
   const int cw = OAL_PAIRS_THREADS >= 64 ? tid - 32 : tid;
@@ -1048,8 +1101,15 @@ __global__ void __launch_bounds__(OAL_PAIRS_THREADS, OAL_PAIRS_WARPS * 32 / OAL_
     // d_k = f_k / w_k - 1 = A[k] (27/8 rho_raw) 2^n - 1
     const V c0 = m000, c1 = c0 + c0, c2 = c1 + c1, c3 = c2 + c2;
     const V sc[4] = {c0, c1, c2, c3};
+    if (a.round_nearest) {
 #pragma unroll
-    for (int k = 0; k < kQ27; ++k) o[k * wkst] = pack_dev<S>(vfma(A[k], sc[q27_d2(k)], splat<V>(-1.0f)));
+      for (int k = 0; k < kQ27; ++k) o[k * wkst] = pack_dev<S>(vfma(A[k], sc[q27_d2(k)], splat<V>(-1.0f)));
+    } else {
+      const uint32_t st = __float_as_uint(f2lo(ux)) * 0x2545F491u + __float_as_uint(f2hi(uy)) + __float_as_uint(f2lo(uz));
+      const uint32_t h = sr_hash((s_bi.x - 1) * kBS + 2 * i, (s_bi.y - 1) * kBS + y, (s_bi.z - 1) * kBS + z, st);
+#pragma unroll
+      for (int k = 0; k < kQ27; ++k) o[k * wkst] = pack_dev_rs<S>(vfma(A[k], sc[q27_d2(k)], splat<V>(-1.0f)), h * sr_mult(k));
+    }
   } else {
     const V c0 = m000, c1 = c0 * splat<V>(0.5f), c2 = c0 * splat<V>(0.25f), c3 = c0 * splat<V>(0.125f);
     const V sc[4] = {c0, c1, c2, c3};
@@ -1259,9 +1319,23 @@ __global__ void __launch_bounds__(128) k_cumulant_gen(const StepArgs a, const in
         grad_wall<R>(A, rho, R(1) / R(cp.tau), R(cp.grad_pineq_scale));
         vel_out[vown] = R(0); vel_out[vown + vcs] = R(0); vel_out[vown + 2 * vcs] = R(0);
       }
+      uint32_t hsr = 0u;
+      if constexpr (sizeof(S) == 2) {
+        if (!a.round_nearest) {
+          const uint32_t st = __float_as_uint(float(uxe)) * 0x2545F491u + __float_as_uint(float(uye)) +
+                              __float_as_uint(float(uze) + float(rho));
+          hsr = sr_hash(gx - 1, gy - 1, gz - 1, st);
+        }
+      }
 #pragma unroll
       for (int k = 0; k < kQ27; ++k) {
-        const S v = Codec<S>::enc(A[k], R(q27_w(k)), R(1.0 / q27_w(k)));
+        S v;
+        if constexpr (sizeof(S) == 2) {
+          if (a.round_nearest) v = Codec<S>::enc(A[k], R(q27_w(k)), R(1.0 / q27_w(k)));
+          else v = enc_rs<S>(fmaf(float(A[k]), float(1.0 / q27_w(k)), -1.0f), hsr * sr_mult(k));
+        } else {
+          v = Codec<S>::enc(A[k], R(q27_w(k)), R(1.0 / q27_w(k)));
+        }
         if (store_post) fpost[own + k * kst] = v;
         fout[own + k * kst] = v;
       }

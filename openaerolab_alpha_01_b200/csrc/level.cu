@@ -289,6 +289,7 @@ struct oal_level {
   int32_t op = 0, storage = 0;
   // dense padded layout (box levels, FP32/FP16/BF16)
   bool dense = false;
+  bool round_nearest = false;  // OAL_LEVEL_ROUND_NEAREST
   int32_t PX = 0, PY = 0, PZ = 0;
   int32_t dense_grid = 0;
   uint32_t* d_err = nullptr;
@@ -1019,6 +1020,7 @@ oal_status oal_level_create_ex(const oal_geometry* g, int32_t op, int32_t storag
   // box levels in FP32/FP16/BF16: dense padded grid; otherwise the real blocks followed by the
   // ghost blocks
   L->dense = (flags & OAL_LEVEL_DENSE) && g->box && storage != OAL_STORE_F64;
+  L->round_nearest = (flags & OAL_LEVEL_ROUND_NEAREST) != 0;
   if (L->dense) {
     oal_status ds = build_dense_tables(const_cast<oal_geometry*>(g));
     if (ds != OAL_OK) { delete L; return ds; }
@@ -1207,6 +1209,7 @@ static oal_status enqueue_step(oal_level* L, const CaseParams& cp, cudaStream_t 
   a.err = L->d_err;
   a.p0 = cp;
   a.flags_any = cp.flags;
+  a.round_nearest = L->round_nearest ? 1 : 0;
   a.par = L->par;
   if (L->dense) {
     a.dense = 1;

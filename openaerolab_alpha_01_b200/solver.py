@@ -191,13 +191,20 @@ class Geometry:
 class Level:
     """Library-owned state of one level: ping-pong populations, density, velocity."""
 
-    def __init__(self, geom: Geometry, operator: str = "cumulant", storage: str = "f32", layout: str = "block"):
+    def __init__(self, geom: Geometry, operator: str = "cumulant", storage: str = "f32", layout: str = "block",
+                 rounding: str = "stochastic"):
         """layout "block": block-major populations with ghost blocks (default); "dense": the
-        padded grid with shared-memory-staged streaming (box levels in FP32/FP16/BF16)."""
+        padded grid with shared-memory-staged streaming (box levels in FP32/FP16/BF16).
+        rounding (FP16/BF16 deviation storage): "stochastic" (default, unbiased in expectation) or
+        "nearest"."""
         self.geom = geom
         self.storage = capi.STORAGE_NAMES[storage]
         self.operator = get_collision_kernel(operator)
+        if rounding not in ("stochastic", "nearest"):
+            raise ValueError("rounding must be 'stochastic' or 'nearest'")
         flags = capi.OAL_LEVEL_DENSE if layout == "dense" else 0
+        if rounding == "nearest":
+            flags |= capi.OAL_LEVEL_ROUND_NEAREST
         h = C.c_void_p()
         check(lib().oal_level_create_ex(geom.handle, self.operator, self.storage, flags, C.byref(h)))
         self.handle = h
