@@ -173,6 +173,10 @@ struct StepArgs {
   uint32_t* err;                  // device error word (bounded waits that gave up), or null
   uint32_t flags_any;             // OR of the flags of every case of the launch (kernel selection)
   int32_t round_nearest;          // 16-bit codecs: round stored deviations to nearest (else stochastically)
+  const int32_t* fast_rec;        // x-pair kernel: per work entry 32 ints (27-entry neighbour row,
+                                  // block coordinates + case, block index), in work-list order
+  double* force_out;              // general kernel of a single level: the last CTA sums the
+  uint32_t* force_ticket;         // momentum-exchange partials into force_out (ticket reset to 0)
   CaseParams p0;
   ParentView par;                 // refined levels only (par.ptr == null otherwise)
 };

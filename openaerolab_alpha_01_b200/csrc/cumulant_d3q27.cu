@@ -950,28 +950,32 @@ __global__ void __launch_bounds__(OAL_PAIRS_THREADS, ((sizeof(S) == 4 || GEN || 
   constexpr IDX wbst = 27 * kCells / 2, wkst = kCells / 2;
   __shared__ IDX s_wbase[28];  // first word of each neighbour block
   __shared__ int32_t s_nbr[28];
-  __shared__ int4 s_bi;        // the block's coordinates in its case (stochastic rounding)
+  __shared__ int32_t s_tail[5];  // the block's coordinates and case (stochastic rounding), its index
   __shared__ CaseParams s_cp;
   const int tid = threadIdx.x;
-  // a CTA covers OAL_PAIRS_THREADS / 32 z planes of a block (one warp per plane)
+  // a CTA covers OAL_PAIRS_THREADS / 32 z planes of a block (one warp per plane); the block's
+  // neighbour row, coordinates and index come in one coalesced 128-byte record
   constexpr int CPB = 256 / OAL_PAIRS_THREADS;
-  const int b = work[blockIdx.x / CPB];
+  const int32_t* __restrict__ rec = a.fast_rec + (int64_t)(blockIdx.x / CPB) * 32;
   const int part = blockIdx.x % CPB;
-  if (tid < 27) {
-    const int32_t nb = a.nbr[(int64_t)b * 27 + tid];
-    s_nbr[tid] = nb;
-    s_wbase[tid] = (IDX)nb * wbst;
-  } else if (DEV && tid == 27) {
-    s_bi = a.binfo[b];
+  if (tid < 32) {
+    const int32_t v = rec[tid];
+    if (tid < 27) {
+      s_nbr[tid] = v;
+      s_wbase[tid] = (IDX)v * wbst;
+    } else {
+      s_tail[tid - 27] = v;
+    }
   }
   // the case parameters: copied by the second warp, or by the first one in one-warp CTAs
   const int cw = OAL_PAIRS_THREADS >= 64 ? tid - 32 : tid;
   if (cw >= 0 && cw < (int)(sizeof(CaseParams) / 4)) {
-    const int case_id = a.cases ? a.binfo[b].w : 0;
+    const int case_id = a.cases ? rec[30] : 0;
     reinterpret_cast<uint32_t*>(&s_cp)[cw] = reinterpret_cast<const uint32_t*>(&case_of(a, case_id))[cw];
   }
   __syncthreads();
   const CaseParams& cp = s_cp;
+  const int b = s_tail[4];
 
   const W* __restrict__ fin = static_cast<const W*>(a.f_in);
   W* __restrict__ fout = static_cast<W*>(a.f_out);
@@ -1106,7 +1110,7 @@ __global__ void __launch_bounds__(OAL_PAIRS_THREADS, ((sizeof(S) == 4 || GEN || 
       for (int k = 0; k < kQ27; ++k) o[k * wkst] = pack_dev<S>(vfma(A[k], sc[q27_d2(k)], splat<V>(-1.0f)));
     } else {
       const uint32_t st = __float_as_uint(f2lo(ux)) * 0x2545F491u + __float_as_uint(f2hi(uy)) + __float_as_uint(f2lo(uz));
-      const uint32_t h = sr_hash((s_bi.x - 1) * kBS + 2 * i, (s_bi.y - 1) * kBS + y, (s_bi.z - 1) * kBS + z, st);
+      const uint32_t h = sr_hash((s_tail[0] - 1) * kBS + 2 * i, (s_tail[1] - 1) * kBS + y, (s_tail[2] - 1) * kBS + z, st);
 #pragma unroll
       for (int k = 0; k < kQ27; ++k) o[k * wkst] = pack_dev_rs<S>(vfma(A[k], sc[q27_d2(k)], splat<V>(-1.0f)), h * sr_mult(k));
     }
@@ -1173,8 +1177,24 @@ __global__ void __launch_bounds__(128) k_cumulant_gen(const StepArgs a, const in
     rho_out[vown] = R(1);
     vel_out[vown] = R(0); vel_out[vown + vcs] = R(0); vel_out[vown + 2 * vcs] = R(0);
   } else {
-    // ---- pull (kernel_cumulant.jl:190-400) ----
+    // ---- pull (kernel_cumulant.jl:190-400): where every source lies in a block (ghost blocks
+    // included), the stored word of the neighbour and, for half-way links, the own cell's
+    // opposite word are both read without a branch, so that all loads are in flight together ----
     R A[kQ27];
+    S raw[kQ27], rawo[kQ27];
+#pragma unroll
+    for (int k = 0; k < kQ27; ++k) {
+      const int cx = q27_cx(k), cy = q27_cy(k), cz = q27_cz(k);
+      const int sx = x - cx, sy = y - cy, sz = z - cz;
+      const int nb = DENSE ? 0 : s_nbr[nbr_dir(sx >> 3, sy >> 3, sz >> 3)];
+      if (DENSE) {
+        // the padded grid holds every source, ghost frame included
+        raw[k] = fin[own - cx - (int64_t)cy * a.PX - (int64_t)cz * a.PX * a.PY + k * kst];
+      } else {
+        raw[k] = fin[(int64_t)(nb >= 0 ? nb : b) * bst + k * kst + ((sx & 7) | ((sy & 7) << 3) | ((sz & 7) << 6))];
+      }
+      rawo[k] = halfway ? fin[own + q27_opp(k) * kst] : raw[k];
+    }
 #pragma unroll
     for (int k = 0; k < kQ27; ++k) {
       const int cx = q27_cx(k), cy = q27_cy(k), cz = q27_cz(k);
@@ -1185,17 +1205,14 @@ __global__ void __launch_bounds__(128) k_cumulant_gen(const StepArgs a, const in
         if (halfway && ((mask >> k) & 1u)) {
           // the link opp(k) of this cell is cut: its own post-collision population returns
           const int i = q27_opp(k);
-          const R fi = dec_k<S, R>(fin, own + i * kst, i);
+          const R fi = Codec<S>::dec(rawo[k], R(q27_w(i)), R(1.0 / q27_w(i)));
           val = fi;
           if (flags & CF_COLLECT) {
             const double mom = 2.0 * (double)fi;  // (f_i* + f_k(t+1)) c_i with c_i = -c_k
             mx -= mom * cx; my -= mom * cy; mz -= mom * cz;
           }
-        } else if (DENSE) {
-          // the padded grid holds every source, ghost frame included
-          val = dec_k<S, R>(fin, own - cx - (int64_t)cy * a.PX - (int64_t)cz * a.PX * a.PY + k * kst, k);
         } else {
-          val = dec_k<S, R>(fin, (int64_t)nb * bst + k * kst + ((sx & 7) | ((sy & 7) << 3) | ((sz & 7) << 6)), k);
+          val = Codec<S>::dec(raw[k], R(q27_w(k)), R(1.0 / q27_w(k)));
         }
       } else {
         val = face_population<S, R>(fin, (int64_t)b * bst, cell, kst, s_nbr, n_real, bst, k, x, y, z, gx, gy, gz, cp);
@@ -1280,8 +1297,8 @@ __global__ void __launch_bounds__(128) k_cumulant_gen(const StepArgs a, const in
         auto nbv = [&](int dx, int dy, int dz, int c, uint32_t solid) -> R {
           const int nx = x + dx, ny = y + dy, nz = z + dz;
           const int nb = s_nbr[nbr_dir(nx >> 3, ny >> 3, nz >> 3)];
-          if (nb < 0 || nb >= n_real || solid) return vel_in[vown + c * vcs];
-          return vel_in[(int64_t)nb * kCells + ((nx & 7) | ((ny & 7) << 3) | ((nz & 7) << 6)) + c * vcs];
+          const bool own_v = nb < 0 || nb >= n_real || solid;
+          return vel_in[(own_v ? vown : (int64_t)nb * kCells + ((nx & 7) | ((ny & 7) << 3) | ((nz & 7) << 6))) + c * vcs];
         };
         const uint32_t sE = (mask >> 12) & 1u, sW = (mask >> 14) & 1u, sN = (mask >> 10) & 1u;
         const uint32_t sS = (mask >> 16) & 1u, sT = (mask >> 4) & 1u, sB = (mask >> 22) & 1u;
@@ -1353,7 +1370,100 @@ __global__ void __launch_bounds__(128) k_cumulant_gen(const StepArgs a, const in
     if ((tid & 31) == 0) { s_mom[tid >> 5][0] = mx; s_mom[tid >> 5][1] = my; s_mom[tid >> 5][2] = mz; }
     __syncthreads();
     if (tid < 3) a.force_part[(int64_t)blockIdx.x * 3 + tid] = ((s_mom[0][tid] + s_mom[1][tid]) + s_mom[2][tid]) + s_mom[3][tid];
+    if (a.force_out) {
+      // the CTA that finishes last sums every CTA's partial in a fixed order (strided per thread,
+      // then a fixed tree), so the total does not depend on which CTA that is
+      __shared__ uint32_t s_last;
+      __shared__ double s_red[3][128];
+      __threadfence();
+      __syncthreads();
+      if (tid == 0) s_last = atomicAdd(a.force_ticket, 1u) == gridDim.x - 1 ? 1u : 0u;
+      __syncthreads();
+      if (s_last) {
+        double r0 = 0.0, r1 = 0.0, r2 = 0.0;
+        for (int64_t i = tid; i < (int64_t)gridDim.x; i += blockDim.x) {
+          r0 += __ldcg(a.force_part + 3 * i); r1 += __ldcg(a.force_part + 3 * i + 1); r2 += __ldcg(a.force_part + 3 * i + 2);
+        }
+        s_red[0][tid] = r0; s_red[1][tid] = r1; s_red[2][tid] = r2;
+        __syncthreads();
+        for (int w = 64; w > 0; w >>= 1) {
+          if (tid < w) { s_red[0][tid] += s_red[0][tid + w]; s_red[1][tid] += s_red[1][tid + w]; s_red[2][tid] += s_red[2][tid + w]; }
+          __syncthreads();
+        }
+        if (tid < 3) a.force_out[tid] = s_red[tid][0];
+        if (tid == 0) *a.force_ticket = 0u;
+      }
+    }
   }
+}
+
+// ------------------------------------------------------------------------------------------------
+// ghost fill by copy list: for the default face conditions every ghost value is either a stored
+// word of a real cell (zero-gradient outlet: the cell's own direction k; mirrors and walls: the
+// mirrored or opposite direction, which has the same lattice weight, so the stored word itself),
+// the inlet equilibrium (kernel_cumulant.jl:235-239 without noise) or the lattice weight. Entry
+// (dst, code): code < 2^31 is the source element; 0x80000000 | k the inlet value of direction k;
+// 0xC0000000 | k the weight of direction k.
+// ------------------------------------------------------------------------------------------------
+// Four entries per thread (a stride of the grid apart, so that a warp's accesses stay
+// contiguous), their loads issued before any store.
+template <class S, class R>
+__global__ void __launch_bounds__(256) k_fill_copy(const StepArgs a, const uint2* __restrict__ entries, int64_t n) {
+  constexpr int E = 4;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t e0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  S* __restrict__ f = const_cast<S*>(static_cast<const S*>(a.f_in));
+  uint2 en[E];
+  S v[E];
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    const int64_t e = e0 + j * stride;
+    en[j] = e < n ? entries[e] : make_uint2(0xFFFFFFFFu, 0x80000000u);
+  }
+#pragma unroll
+  for (int j = 0; j < E; ++j)
+    if (en[j].x != 0xFFFFFFFFu && !(en[j].y & 0x80000000u)) v[j] = f[en[j].y];
+#pragma unroll
+  for (int j = 0; j < E; ++j) {
+    if (en[j].x == 0xFFFFFFFFu) continue;
+    if (en[j].y & 0x80000000u) {
+      const int k = (int)(en[j].y & 31u);
+      const R w = R(q27_w(k));
+      R val = w;
+      if (!(en[j].y & 0x40000000u)) {
+        const CaseParams& cp = a.p0;
+        val = feq_k<R>(k, R(1), R(cp.u_inlet), R(0), R(0), (cp.flags & CF_COMPRESSIBLE) != 0);
+      }
+      v[j] = Codec<S>::enc(val, w, R(1) / w);
+    }
+    f[en[j].x] = v[j];
+  }
+}
+
+// per work entry of the x-pair kernel: its block's neighbour row, coordinates + case, index
+__global__ void k_fast_records(const int32_t* __restrict__ work, int n, const int32_t* __restrict__ nbr,
+                               const int4* __restrict__ binfo, int32_t* __restrict__ rec) {
+  const int f = blockIdx.x, l = threadIdx.x;
+  if (f >= n || l >= 32) return;
+  const int32_t b = work[f];
+  int32_t v = b;
+  if (l < 27) v = nbr[(int64_t)b * 27 + l];
+  else if (l < 31) { const int4 bi = binfo[b]; v = l == 27 ? bi.x : l == 28 ? bi.y : l == 29 ? bi.z : bi.w; }
+  rec[(int64_t)f * 32 + l] = v;
+}
+
+cudaError_t build_fast_records(const int32_t* work, int n, const int32_t* nbr, const int4* binfo, int32_t* rec,
+                               cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  k_fast_records<<<(unsigned)n, 32, 0, st>>>(work, n, nbr, binfo, rec);
+  return cudaGetLastError();
+}
+
+template <class S, class R>
+cudaError_t launch_fill_copy(const StepArgs& a, const uint2* entries, int64_t n, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  k_fill_copy<S, R><<<(unsigned)((n + 1023) / 1024), 256, 0, st>>>(a, entries, n);
+  return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -1563,6 +1673,7 @@ cudaError_t launch_general(const StepArgs& a, const int32_t* work, int n_work, c
 
 #define OAL_INST(S, R)                                                                               \
   template cudaError_t launch_fill_ghosts<S, R>(const StepArgs&, const uint2*, int64_t, cudaStream_t); \
+  template cudaError_t launch_fill_copy<S, R>(const StepArgs&, const uint2*, int64_t, cudaStream_t);   \
   template cudaError_t launch_restrict<S, R>(const RestrictArgs&, cudaStream_t);                       \
   template cudaError_t launch_parent_nodes<S, R>(const ParentView&, const int32_t*, int32_t, void*, int32_t,  \
                                                  cudaStream_t);                                            \

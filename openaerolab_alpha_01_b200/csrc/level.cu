@@ -19,6 +19,10 @@ namespace oal {
 template <class S, class R>
 cudaError_t launch_fill_ghosts(const StepArgs& a, const uint2* entries, int64_t n, cudaStream_t st);
 template <class S, class R>
+cudaError_t launch_fill_copy(const StepArgs& a, const uint2* entries, int64_t n, cudaStream_t st);
+cudaError_t build_fast_records(const int32_t* work, int n, const int32_t* nbr, const int4* binfo, int32_t* rec,
+                               cudaStream_t st);
+template <class S, class R>
 cudaError_t launch_fast(const StepArgs& a, const int32_t* work, int n_work, cudaStream_t st);
 template <class S, class R>
 cudaError_t launch_general(const StepArgs& a, const int32_t* work, int n_work, cudaStream_t st);
@@ -233,8 +237,20 @@ struct oal_geometry {
   uint2* d_gentries = nullptr;     // ghost fill entries (block, cell | k << 9)
   int64_t n_gentries = 0;
   int32_t* d_fast = nullptr;       // blocks for the uniform kernel
+  int32_t* d_fast_rec = nullptr;   // their 32-int records (neighbour row, coordinates, index)
+  int32_t n_fast_in = 0;           // the first n_fast_in fast blocks read no ghost slot
   int32_t* d_general = nullptr;    // blocks for the general kernel
   int32_t n_fast = 0, n_general = 0;
+  // ghost fill split by face conditions (one entry per key of fill_key_of, kept until the
+  // geometry is destroyed: captured graphs may hold the pointers)
+  struct FillLists {
+    uint32_t key;
+    uint2* copy;   // raw copies, inlet and weight values (k_fill_copy)
+    int64_t n_copy;
+    uint2* rest;   // entries for the general fill kernel
+    int64_t n_rest;
+  };
+  std::vector<FillLists> fills;
   int4* d_binfo = nullptr;
   uint32_t* d_bflags = nullptr;
   int32_t* d_mslot = nullptr;
@@ -298,6 +314,7 @@ struct oal_level {
   void* rho = nullptr;
   double* d_force_part = nullptr;
   double* d_force = nullptr;
+  uint32_t* d_ticket = nullptr;  // the general kernel's last-CTA ticket (fused drag sum)
   double* d_mm_part = nullptr;
   double* d_mm = nullptr;
   int parity = 0;
@@ -366,24 +383,149 @@ static oal_status resolve_params(const oal_step_params* p, const oal_geometry* g
   return OAL_OK;
 }
 
+// The case flags that decide where a ghost value comes from.
+static uint32_t fill_key_of(uint32_t flags) {
+  return flags & (CF_YMIN_WALL | CF_ZWALL_SLIP | CF_ZWALL_NOSLIP | CF_TRANSVERSE_FS | CF_INLET_NOISE);
+}
+
+// Split the ghost fill entries for the face conditions of `flags` (the branches of
+// face_population_impl for a level without parent): a stored word of a real cell of the same
+// lattice weight (outlet, mirrors, walls, the slip image), the inlet equilibrium without noise,
+// the lattice weight, or anything else (transverse freestream blend, inlet noise), which stays on
+// the general fill. Built on the host once per key, outside any stream capture.
+static oal_status build_fill_lists(oal_geometry* g, uint32_t flags) {
+  const uint32_t key = fill_key_of(flags);
+  for (const auto& c : g->fills)
+    if (c.key == key) return OAL_OK;
+  const int64_t bst = 27 * kCells, kst = kCells;
+  if ((int64_t)(g->nb + g->n_ghost) * bst >= (1ll << 31)) return OAL_OK;  // element index must fit 31 bits
+  std::vector<uint2> copy, rest;
+  copy.reserve(g->h_gentries.size());
+  const int nx = g->nx, ny = g->ny, nz = g->nz;
+  for (const uint2& en : g->h_gentries) {
+    const int64_t b = en.x;
+    const int cell = (int)(en.y & 511u), k = (int)((en.y >> 9) & 31u);
+    const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
+    const int4 bi = g->h_binfo[(size_t)b];
+    const int gx = (bi.x - 1) * kBS + x + 1, gy = (bi.y - 1) * kBS + y + 1, gz = (bi.z - 1) * kBS + z + 1;
+    const int cx = q27_cx(k), cy = q27_cy(k), cz = q27_cz(k);
+    const int sx = x - cx, sy = y - cy, sz = z - cz;
+    const int32_t gblk = g->h_nbrg[(size_t)b * 27 + nbr_dir(sx >> 3, sy >> 3, sz >> 3)];
+    const uint32_t dst = (uint32_t)((int64_t)gblk * bst + k * kst + ((sx & 7) | ((sy & 7) << 3) | ((sz & 7) << 6)));
+    const int sgx = gx - cx, sgy = gy - cy, sgz = gz - cz;
+    const bool zmin = sgz < 1, zmax = sgz > nz, ymin = sgy < 1, ymax = sgy > ny;
+    int j = k;
+    int64_t src = -1;
+    uint32_t code = 0;
+    bool general = false, constant = false;
+    if (sgx < 1) {
+      if (flags & CF_INLET_NOISE) general = true;
+      else { code = 0x80000000u | (uint32_t)k; constant = true; }
+    } else if (sgx > nx) {
+      j = k;
+    } else if ((flags & (CF_ZWALL_SLIP | CF_ZWALL_NOSLIP)) && (zmin || zmax)) {
+      if (flags & CF_ZWALL_NOSLIP) {
+        j = q27_opp(k);
+      } else {
+        j = q27_mir_z(k);
+        const int ix = x - cx, iy = y - cy;
+        if (ix >= 0 && ix < kBS && iy >= 0 && iy < kBS) {
+          src = b * bst + j * kst + (ix + 8 * iy + 64 * z);
+        } else {
+          const int32_t nb2 = g->h_nbrg[(size_t)b * 27 + nbr_dir(ix >> 3, iy >> 3, 0)];
+          if (nb2 >= 0 && nb2 < g->nb) src = (int64_t)nb2 * bst + j * kst + ((ix & 7) + 8 * (iy & 7) + 64 * z);
+        }
+      }
+    } else if ((flags & CF_TRANSVERSE_FS) && (ymin || ymax || zmin || zmax)) {
+      general = true;
+    } else if (ymin && (flags & CF_YMIN_WALL)) {
+      j = q27_opp(k);
+    } else if (ymin || ymax) {
+      j = q27_mir_y(k);
+    } else if (zmin || zmax) {
+      j = q27_mir_z(k);
+    } else {
+      code = 0xC0000000u | (uint32_t)k;
+      constant = true;
+    }
+    if (general) { rest.push_back(en); continue; }
+    if (!constant) code = (uint32_t)(src >= 0 ? src : b * bst + j * kst + cell);
+    copy.push_back(make_uint2(dst, code));
+  }
+  // consecutive threads write consecutive slots
+  std::sort(copy.begin(), copy.end(), [](const uint2& p, const uint2& q) { return p.x < q.x; });
+  oal_geometry::FillLists fl{key, nullptr, (int64_t)copy.size(), nullptr, (int64_t)rest.size()};
+  cudaError_t e = cudaSuccess;
+  if (!copy.empty()) {
+    e = cudaMalloc(&fl.copy, copy.size() * sizeof(uint2));
+    if (e == cudaSuccess) e = cudaMemcpy(fl.copy, copy.data(), copy.size() * sizeof(uint2), cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess && !rest.empty()) {
+    e = cudaMalloc(&fl.rest, rest.size() * sizeof(uint2));
+    if (e == cudaSuccess) e = cudaMemcpy(fl.rest, rest.data(), rest.size() * sizeof(uint2), cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    cudaFree(fl.copy); cudaFree(fl.rest);
+    OAL_CUDA_TRY(e);
+  }
+  g->fills.push_back(fl);
+  return OAL_OK;
+}
+
+// Builds the fill lists of the level's face conditions when the stream is not being captured
+// (a level with a parent or a dense layout keeps the general fill).
+static oal_status prepare_fill(oal_level* L, const CaseParams& cp, cudaStream_t st) {
+  if (L->dense || L->par.ptr || L->g->n_gentries == 0) return OAL_OK;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  OAL_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return OAL_OK;
+  return build_fill_lists(const_cast<oal_geometry*>(L->g), cp.flags);
+}
+
 // Which kernels one step launches.
 enum StepPath { PATH_PLAIN = 0, PATH_GHOSTED = 1 };
 
+// x-pair blocks [first, first + count) of a fast list and its records
 template <class S, class R>
-static cudaError_t launch_step_t(const oal_geometry* g, const StepArgs& a, StepPath path, cudaStream_t st,
+static cudaError_t launch_fast_range(const StepArgs& a, const int32_t* work, int first, int count, cudaStream_t st) {
+  if (count <= 0) return cudaSuccess;
+  StepArgs b = a;
+  if (b.fast_rec) b.fast_rec += (int64_t)first * 32;
+  return launch_fast<S, R>(b, work + first, count, st);
+}
+
+template <class S, class R>
+static cudaError_t launch_step_t(const oal_geometry* g, const StepArgs& a0, StepPath path, cudaStream_t st,
                                  const Overlap* ov) {
   cudaError_t e;
-  if (path == PATH_PLAIN) return launch_general<S, R>(a, nullptr, g->nb, st);
-  if ((e = launch_fill_ghosts<S, R>(a, g->d_gentries, g->n_gentries, st)) != cudaSuccess) return e;
-  const bool fork = ov && ov->side && g->n_general > 0 && g->n_fast > 0;
+  if (path == PATH_PLAIN) return launch_general<S, R>(a0, nullptr, g->nb, st);
+  StepArgs a = a0;
+  a.fast_rec = g->d_fast_rec;
+  const oal_geometry::FillLists* fl = nullptr;
+  if (!a.par.ptr && !a.dense && !a.cases)
+    for (const auto& c : g->fills)
+      if (c.key == fill_key_of(a.p0.flags)) fl = &c;
+  auto fill = [&](cudaStream_t s) -> cudaError_t {
+    cudaError_t r;
+    if (!fl) return launch_fill_ghosts<S, R>(a, g->d_gentries, g->n_gentries, s);
+    if ((r = launch_fill_copy<S, R>(a, fl->copy, fl->n_copy, s)) != cudaSuccess) return r;
+    return launch_fill_ghosts<S, R>(a, fl->rest, fl->n_rest, s);
+  };
+  // high-priority side stream: ghost fill, then the blocks that read ghost slots (general kernel,
+  // boundary x-pair blocks); main stream: the interior x-pair blocks, which read none
+  const int n_in = g->n_fast_in, n_bd = g->n_fast - g->n_fast_in;
+  const bool fork = ov && ov->side && n_in > 0 && (g->n_general > 0 || n_bd > 0);
   if (fork) {
     if ((e = cudaEventRecord(ov->fork, st)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(ov->side, ov->fork, 0)) != cudaSuccess) return e;
+    if ((e = fill(ov->side)) != cudaSuccess) return e;
     if ((e = launch_general<S, R>(a, g->d_general, g->n_general, ov->side)) != cudaSuccess) return e;
+    if ((e = launch_fast_range<S, R>(a, g->d_fast, n_in, n_bd, ov->side)) != cudaSuccess) return e;
     if ((e = cudaEventRecord(ov->join, ov->side)) != cudaSuccess) return e;
-    if ((e = launch_fast<S, R>(a, g->d_fast, g->n_fast, st)) != cudaSuccess) return e;
+    if ((e = launch_fast_range<S, R>(a, g->d_fast, 0, n_in, st)) != cudaSuccess) return e;
     return cudaStreamWaitEvent(st, ov->join, 0);
   }
+  if ((e = fill(st)) != cudaSuccess) return e;
   if ((e = launch_fast<S, R>(a, g->d_fast, g->n_fast, st)) != cudaSuccess) return e;
   return launch_general<S, R>(a, g->d_general, g->n_general, st);
 }
@@ -824,6 +966,9 @@ oal_status oal_geometry_create(const oal_geometry_desc* d, int32_t device, oal_g
     }
     (gen ? general : fast).push_back((int32_t)b);
   }
+  // interior blocks first: they pull no ghost slot, so their step need not wait for the fill
+  std::stable_partition(fast.begin(), fast.end(), [&](int32_t b) { return (bflags[(size_t)b] & BF_INTERIOR) != 0; });
+  g->n_fast_in = (int32_t)std::count_if(fast.begin(), fast.end(), [&](int32_t b) { return (bflags[(size_t)b] & BF_INTERIOR) != 0; });
   g->n_fast = (int32_t)fast.size();
   g->n_general = (int32_t)general.size();
 
@@ -911,6 +1056,11 @@ oal_status oal_geometry_create(const oal_geometry_desc* d, int32_t device, oal_g
     GTRY(cudaMalloc(&g->d_general, general.size() * sizeof(int32_t)));
     GTRY(cudaMemcpy(g->d_general, general.data(), general.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
   }
+  if (!fast.empty()) {
+    GTRY(cudaMalloc(&g->d_fast_rec, fast.size() * 32 * sizeof(int32_t)));
+    GTRY(build_fast_records(g->d_fast, (int)fast.size(), g->d_nbr_ghost, g->d_binfo, g->d_fast_rec, nullptr));
+    GTRY(cudaDeviceSynchronize());
+  }
   GTRY(cudaMalloc(&g->d_force_part, (size_t)nb * 4 * 3 * sizeof(double)));
   GTRY(cudaMalloc(&g->d_force, 3 * sizeof(double)));
   GTRY(cudaMemset(g->d_force, 0, 3 * sizeof(double)));
@@ -922,6 +1072,9 @@ oal_status oal_geometry_create(const oal_geometry_desc* d, int32_t device, oal_g
 static void geometry_release(oal_geometry* g) {
   cudaSetDevice(g->device);
   cudaFree(g->d_nbr_ghost); cudaFree(g->d_gentries); cudaFree(g->d_fast); cudaFree(g->d_general);
+  cudaFree(g->d_fast_rec);
+  for (auto& c : g->fills) { cudaFree(c.copy); cudaFree(c.rest); }
+  g->fills.clear();
   cudaFree(g->d_dense_gentries); cudaFree(g->d_dense_fast);
   cudaFree(g->d_nbr); cudaFree(g->d_binfo); cudaFree(g->d_bflags); cudaFree(g->d_mslot);
   cudaFree(g->d_cmask); cudaFree(g->d_sponge); cudaFree(g->d_wdist);
@@ -1049,6 +1202,8 @@ oal_status oal_level_create_ex(const oal_geometry* g, int32_t op, int32_t storag
   if ((e = cudaMalloc(&L->d_force_part, (size_t)g->nb * 4 * 3 * sizeof(double))) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&L->d_force, 3 * sizeof(double))) != cudaSuccess) return fail(e);
   if ((e = cudaMemset(L->d_force, 0, 3 * sizeof(double))) != cudaSuccess) return fail(e);
+  if ((e = cudaMalloc(&L->d_ticket, sizeof(uint32_t))) != cudaSuccess) return fail(e);
+  if ((e = cudaMemset(L->d_ticket, 0, sizeof(uint32_t))) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&L->d_mm_part, (size_t)g->nb * 4 * sizeof(double))) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&L->d_mm, 4 * sizeof(double))) != cudaSuccess) return fail(e);
   if ((e = cudaStreamCreateWithFlags(&L->cap, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
@@ -1095,6 +1250,7 @@ void oal_level_destroy(oal_level* L) {
   bouzidi_free(&L->bz);
   for (int i = 0; i < 2; ++i) { cudaFree(L->f[i]); cudaFree(L->vel[i]); }
   cudaFree(L->rho); cudaFree(L->d_force_part); cudaFree(L->d_force); cudaFree(L->d_mm_part); cudaFree(L->d_mm);
+  cudaFree(L->d_ticket);
   if (L->cap) cudaStreamDestroy(L->cap);
   if (L->ov.side) cudaStreamDestroy(L->ov.side);
   if (L->ov.fork) cudaEventDestroy(L->ov.fork);
@@ -1210,6 +1366,7 @@ static oal_status enqueue_step(oal_level* L, const CaseParams& cp, cudaStream_t 
   a.p0 = cp;
   a.flags_any = cp.flags;
   a.round_nearest = L->round_nearest ? 1 : 0;
+  if (!L->dense) { a.force_out = L->d_force; a.force_ticket = L->d_ticket; }
   a.par = L->par;
   if (L->dense) {
     a.dense = 1;
@@ -1229,11 +1386,12 @@ static oal_status enqueue_step(oal_level* L, const CaseParams& cp, cudaStream_t 
   if ((cp.flags & CF_BOUZIDI) && L->bz.n > 0)
     OAL_CUDA_TRY(bouzidi_enqueue(L->bz, L->storage, a.f_out, pop_index(L), g->d_nbr, g->d_mslot, g->d_cmask, st));
   if (cp.flags & CF_COLLECT) {
-    // the momentum exchange lives on the general kernel's CTAs (blocks near solids)
-    if (g->n_general > 0) {
+    // the momentum exchange lives on the general kernel's CTAs (blocks near solids); in the
+    // block layout the last of them sums the partials (a.force_out)
+    if (g->n_general > 0 && L->dense) {
       k_reduce3<<<1, 256, 0, st>>>(L->d_force_part, (int64_t)g->n_general * 4, L->d_force);
       OAL_CUDA_TRY(cudaGetLastError());
-    } else {
+    } else if (g->n_general == 0) {
       OAL_CUDA_TRY(cudaMemsetAsync(L->d_force, 0, 3 * sizeof(double), st));
     }
     L->forces_valid = true;
@@ -1250,6 +1408,7 @@ oal_status oal_level_step(oal_level* L, const oal_step_params* p, void* stream) 
   if (s != OAL_OK) return s;
   if (cp.flags & CF_STORE_POST) return set_error(OAL_E_UNSUPPORTED, "store_post_collision needs caller-owned arrays (oal_stream_collide)");
   OAL_CUDA_TRY(cudaSetDevice(L->g->device));
+  if ((s = prepare_fill(L, cp, static_cast<cudaStream_t>(stream))) != OAL_OK) return s;
   return enqueue_step(L, cp, static_cast<cudaStream_t>(stream));
 }
 
@@ -1263,6 +1422,7 @@ oal_status oal_level_advance(oal_level* L, const oal_step_params* p, int32_t n, 
   if (cp.flags & CF_STORE_POST) return set_error(OAL_E_UNSUPPORTED, "store_post_collision needs caller-owned arrays");
   OAL_CUDA_TRY(cudaSetDevice(L->g->device));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if ((s = prepare_fill(L, cp, st)) != OAL_OK) return s;
   oal_step_params key = *p;
   if (!(cp.flags & CF_INLET_NOISE)) key.time_step_seed = 0;  // the seed only matters with inlet noise
   const bool hit = L->gc.exec && L->gc.n == n && L->gc.parity == L->parity && std::memcmp(&L->gc.p, &key, sizeof key) == 0;
@@ -1963,6 +2123,8 @@ struct oal_batch {
   // work lists, rebuilt when membership changes
   uint2* d_gentries = nullptr; int64_t n_gentries = 0, cap_gentries = 0;
   int32_t* d_fast = nullptr; int64_t n_fast = 0;
+  int32_t* d_fast_rec = nullptr;  // x-pair kernel records of d_fast
+  int64_t n_fast_in = 0;          // the first n_fast_in fast blocks read no ghost slot
   int32_t* d_general = nullptr; int64_t n_general = 0;
   int32_t* d_seg = nullptr;       // [max_members + 1] general-CTA segments per member
   double* d_part = nullptr;       // [R*4*3]
@@ -1989,7 +2151,7 @@ static void batch_release_graph(oal_batch* B) {
 // Combined work lists over the active members (host concatenation, then upload).
 static oal_status batch_rebuild(oal_batch* B) {
   std::vector<uint2> ge;
-  std::vector<int32_t> fast, general, seg(1, 0);
+  std::vector<int32_t> fast, fast_bd, general, seg(1, 0);
   std::vector<CaseParams> cases((size_t)B->max_members);
   uint32_t flags_any = 0;
   for (int32_t m = 0; m < B->max_members; ++m) {
@@ -1997,7 +2159,8 @@ static oal_status batch_rebuild(oal_batch* B) {
     if (M.active) {
       const oal_geometry* g = M.g;
       for (const uint2& e : g->h_gentries) ge.push_back(make_uint2((uint32_t)(M.rb + e.x), e.y));
-      for (int32_t b : g->h_fast) fast.push_back((int32_t)(M.rb + b));
+      for (int32_t i = 0; i < g->n_fast_in; ++i) fast.push_back((int32_t)(M.rb + g->h_fast[(size_t)i]));
+      for (size_t i = (size_t)g->n_fast_in; i < g->h_fast.size(); ++i) fast_bd.push_back((int32_t)(M.rb + g->h_fast[i]));
       for (int32_t b : g->h_general) general.push_back((int32_t)(M.rb + b));
       cases[(size_t)m] = M.cp;
       flags_any |= M.cp.flags;
@@ -2013,7 +2176,16 @@ static oal_status batch_rebuild(oal_batch* B) {
     return e;
   };
   OAL_CUDA_TRY(upload(B->d_gentries, ge, B->n_gentries));
+  B->n_fast_in = (int64_t)fast.size();
+  fast.insert(fast.end(), fast_bd.begin(), fast_bd.end());
   OAL_CUDA_TRY(upload(B->d_fast, fast, B->n_fast));
+  cudaFree(B->d_fast_rec);
+  B->d_fast_rec = nullptr;
+  if (B->n_fast > 0) {
+    OAL_CUDA_TRY(cudaMalloc(&B->d_fast_rec, (size_t)B->n_fast * 32 * sizeof(int32_t)));
+    OAL_CUDA_TRY(build_fast_records(B->d_fast, (int)B->n_fast, B->d_nbr, B->d_binfo, B->d_fast_rec, nullptr));
+    OAL_CUDA_TRY(cudaDeviceSynchronize());
+  }
   OAL_CUDA_TRY(upload(B->d_general, general, B->n_general));
   OAL_CUDA_TRY(cudaMemcpy(B->d_seg, seg.data(), seg.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
   OAL_CUDA_TRY(cudaMemcpy(B->d_cases, cases.data(), cases.size() * sizeof(CaseParams), cudaMemcpyHostToDevice));
@@ -2026,16 +2198,21 @@ static oal_status batch_rebuild(oal_batch* B) {
 template <class S, class R>
 static cudaError_t batch_step_t(oal_batch* B, const StepArgs& a, cudaStream_t st) {
   cudaError_t e;
-  if ((e = launch_fill_ghosts<S, R>(a, B->d_gentries, B->n_gentries, st)) != cudaSuccess) return e;
-  const bool fork = B->n_general > 0 && B->n_fast > 0;
+  // as for a single level: fill, general and boundary blocks on the side stream, interior blocks
+  // (no ghost reads) on the main stream
+  const int n_in = (int)B->n_fast_in, n_bd = (int)(B->n_fast - B->n_fast_in);
+  const bool fork = n_in > 0 && (B->n_general > 0 || n_bd > 0);
   if (fork) {
     if ((e = cudaEventRecord(B->ov.fork, st)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(B->ov.side, B->ov.fork, 0)) != cudaSuccess) return e;
+    if ((e = launch_fill_ghosts<S, R>(a, B->d_gentries, B->n_gentries, B->ov.side)) != cudaSuccess) return e;
     if ((e = launch_general<S, R>(a, B->d_general, (int)B->n_general, B->ov.side)) != cudaSuccess) return e;
+    if ((e = launch_fast_range<S, R>(a, B->d_fast, n_in, n_bd, B->ov.side)) != cudaSuccess) return e;
     if ((e = cudaEventRecord(B->ov.join, B->ov.side)) != cudaSuccess) return e;
-    if ((e = launch_fast<S, R>(a, B->d_fast, (int)B->n_fast, st)) != cudaSuccess) return e;
+    if ((e = launch_fast_range<S, R>(a, B->d_fast, 0, n_in, st)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(st, B->ov.join, 0)) != cudaSuccess) return e;
   } else {
+    if ((e = launch_fill_ghosts<S, R>(a, B->d_gentries, B->n_gentries, st)) != cudaSuccess) return e;
     if ((e = launch_fast<S, R>(a, B->d_fast, (int)B->n_fast, st)) != cudaSuccess) return e;
     if ((e = launch_general<S, R>(a, B->d_general, (int)B->n_general, st)) != cudaSuccess) return e;
   }
@@ -2057,6 +2234,7 @@ static oal_status batch_enqueue_step(oal_batch* B, int step_offset, cudaStream_t
   a.wall_dist = B->d_wdist;
   a.cases = B->d_cases;
   a.flags_any = B->flags_any;
+  a.fast_rec = B->d_fast_rec;
   a.n_blocks = (int32_t)B->R;
   a.n_total_blocks = (int32_t)(B->R + B->G);
   a.block_base = 0;
@@ -2125,6 +2303,7 @@ void oal_batch_destroy(oal_batch* B) {
   cudaFree(B->rho); cudaFree(B->d_nbr); cudaFree(B->d_binfo); cudaFree(B->d_bflags); cudaFree(B->d_mslot);
   cudaFree(B->d_cmask); cudaFree(B->d_sponge); cudaFree(B->d_wdist); cudaFree(B->d_cases);
   cudaFree(B->d_gentries); cudaFree(B->d_fast); cudaFree(B->d_general); cudaFree(B->d_seg);
+  cudaFree(B->d_fast_rec);
   cudaFree(B->d_part); cudaFree(B->d_forces); cudaFree(B->d_mm_part); cudaFree(B->d_mm);
   if (B->cap) cudaStreamDestroy(B->cap);
   if (B->ov.side) cudaStreamDestroy(B->ov.side);
