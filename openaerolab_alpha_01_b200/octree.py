@@ -335,6 +335,8 @@ class State:
     def __init__(self, mesh, cfg: CaseConfig, precision=None, device: int = 0):
         """`mesh`: a PeriodicBox, one level (Mesh) or an OctMesh; an OctMesh of several levels is
         stepped as the reference's step_recursive! (the coarse step of advance!)."""
+        self.config_sha = str(getattr(mesh, "config_sha", "") or "")
+        self.stl_sha = str(getattr(mesh, "stl_sha", "") or "")
         if isinstance(mesh, OctMesh) and mesh.nlevels == 1:
             mesh = mesh.levels[0]
         self.mesh = mesh
@@ -886,3 +888,156 @@ def read_mesh(path, faces=("periodic",) * 6) -> OctMesh:
     mesh.triangles = tri
     mesh.offset, mesh.config_sha, mesh.stl_sha = offset, config_sha, stl_sha
     return mesh
+
+
+# ---------------------------------------------------------------- checkpoint
+CHECKPOINT_MAGIC = b"OCTQ19C\0"
+CHECKPOINT_FORMAT = 1
+
+
+def _sha64(s: str) -> bytes:
+    """A hash string as the checkpoint holds it: space-padded or cut to 64 bytes (rpad(s, 64)[1:64])."""
+    b = s.encode()
+    return (b + b" " * 64)[:64]
+
+
+def pack_checkpoint(levels, precision, step: int, u_inlet: float, mass0: float, n_avg: int = 0, sums=None,
+                    config_sha: str = "", stl_sha: str = "") -> bytes:
+    """The checkpoint file of write_checkpoint! (io_run.jl:277-291), version 1: magic, version,
+    sizeof(T), the config and STL hashes (64 bytes each), step, u_inlet, mass0, the force averages'
+    count and nine sums, the level count, then per level the oct count and f, g, u, v, rho, rhob
+    (both buffers, the current one first) and the wall-model friction velocities tau_w. `levels`:
+    per level a dict of C-order arrays f (nocts, 19, 8), g, u (nocts, 3, 8), v, rho (nocts, 8),
+    rhob, tau_w (ncut,), whose memory is the reference's column-major (8, 19, nocts) etc."""
+    dt = np.dtype(precision).newbyteorder("<")
+    if dt.itemsize not in (4, 8):
+        raise ValueError("precision must be float32 or float64")
+    sums = np.zeros(9) if sums is None else np.asarray(sums, np.float64).reshape(9)
+    out = bytearray(CHECKPOINT_MAGIC)
+    out += np.array([CHECKPOINT_FORMAT, dt.itemsize], "<i8").tobytes()
+    out += _sha64(config_sha) + _sha64(stl_sha)
+    out += np.array([step], "<i8").tobytes() + np.array([u_inlet, mass0], "<f8").tobytes()
+    out += np.array([n_avg], "<i8").tobytes() + sums.astype("<f8").tobytes()
+    out += np.array([len(levels)], "<i8").tobytes()
+    for lv in levels:
+        no = int(lv["f"].shape[0])
+        shapes = {"f": (no, 19, 8), "g": (no, 19, 8), "u": (no, 3, 8), "v": (no, 3, 8), "rho": (no, 8), "rhob": (no, 8)}
+        out += np.array([no], "<i8").tobytes()
+        for name in ("f", "g", "u", "v", "rho", "rhob"):
+            a = np.asarray(lv[name])
+            if a.shape != shapes[name]:
+                raise ValueError(f"checkpoint array {name}: shape {a.shape}, expected {shapes[name]}")
+            out += np.ascontiguousarray(a, dt).tobytes()
+        tw = np.asarray(lv.get("tau_w", np.zeros(0)))
+        out += np.array([tw.size], "<i8").tobytes() + np.ascontiguousarray(tw, dt).tobytes()
+    return bytes(out)
+
+
+def unpack_checkpoint(data: bytes, precision=None, config_sha: str | None = None, stl_sha: str | None = None,
+                      octs=None, ncut=None) -> dict:
+    """Parse a checkpoint (read_checkpoint!, io_run.jl:294-314) with the reference's checks: the
+    magic, the version, the precision (when given), the case hashes (when given; compared after
+    stripping the padding), the level count and each level's oct count and tau_w size (when
+    given), and no trailing data. Returns the header fields and the per-level arrays."""
+    r = _Reader(data)
+
+    def fail(msg):
+        raise ValueError(msg)
+
+    try:
+        if r.take(len(CHECKPOINT_MAGIC)) != CHECKPOINT_MAGIC:
+            fail("not a checkpoint")
+        if r.i64() != CHECKPOINT_FORMAT:
+            fail("checkpoint format")
+        size = r.i64()
+        if size not in (4, 8) or (precision is not None and size != np.dtype(precision).itemsize):
+            fail("checkpoint precision differs from the run's")
+        dt = np.dtype("<f4" if size == 4 else "<f8")
+        csha, ssha = r.take(64).decode().strip(), r.take(64).decode().strip()
+        if (config_sha is not None and csha != config_sha) or (stl_sha is not None and ssha != stl_sha):
+            fail("checkpoint belongs to another case (config or STL hash differs)")
+        step = r.i64()
+        u_inlet, mass0 = (float(v) for v in r.f64(2))
+        n_avg = r.i64()
+        sums = r.f64(9)
+        nl = r.i64()
+        if octs is not None and nl != len(octs):
+            fail("checkpoint level count differs")
+        levels = []
+        for l in range(nl):
+            no = r.i64()
+            if octs is not None and no != octs[l]:
+                fail("checkpoint oct count differs")
+            lv = {}
+            for name, shape in (("f", (no, 19, 8)), ("g", (no, 19, 8)), ("u", (no, 3, 8)), ("v", (no, 3, 8)),
+                                ("rho", (no, 8)), ("rhob", (no, 8))):
+                n = int(np.prod(shape))
+                lv[name] = np.frombuffer(r.take(n * size), dt).reshape(shape).astype(dt.newbyteorder("="))
+            nw = r.i64()
+            if ncut is not None and nw != ncut[l]:
+                fail("checkpoint wall-model size differs")
+            lv["tau_w"] = np.frombuffer(r.take(nw * size), dt).astype(dt.newbyteorder("="))
+            levels.append(lv)
+    except ValueError as e:
+        if str(e) == "mesh file ends early":
+            raise ValueError("checkpoint ends early") from None
+        raise
+    if r.o != len(r.d):
+        raise ValueError("checkpoint has unexpected trailing data")
+    return dict(precision=dt.newbyteorder("="), config_sha=csha, stl_sha=ssha, step=step, u_inlet=u_inlet,
+                mass0=mass0, n_avg=n_avg, sums=sums, levels=levels)
+
+
+def _level_ncut(m) -> int:
+    cs = getattr(m, "cut_slot", None)
+    return 0 if cs is None else int(cs.shape[0])
+
+
+def write_checkpoint(st: "State", out, n_avg: int = 0, sums=None, keep: int = 2) -> str:
+    """write_checkpoint! (io_run.jl:277-291): `out`/checkpoints/checkpoint_<step, 9 digits>.bin,
+    written to a .tmp file and renamed; keeps the newest `keep`. The device holds one population
+    buffer per level between steps (the step reads nothing from the other), so the current state
+    fills both of the file's buffers. tau_w is zero (the octree wall model is not built here)."""
+    d = os.path.join(str(out), "checkpoints")
+    os.makedirs(d, exist_ok=True)
+    levels = []
+    for l, m in enumerate(st.level_meshes, start=1):
+        f, u, rho = st.state(l)
+        levels.append(dict(f=f, g=f, u=u, v=u, rho=rho, rhob=rho, tau_w=np.zeros(_level_ncut(m), st.dtype)))
+    data = pack_checkpoint(levels, st.dtype, st.step, float(st.cfg.u_lattice), float(st.mass0), n_avg, sums,
+                           st.config_sha, st.stl_sha)
+    path = os.path.join(d, f"checkpoint_{st.step:09d}.bin")
+    with open(path + ".tmp", "wb") as io:
+        io.write(data)
+    os.replace(path + ".tmp", path)
+    files = sorted(f for f in os.listdir(d) if f.startswith("checkpoint_") and f.endswith(".bin"))
+    for f in files[:max(0, len(files) - keep)]:
+        os.remove(os.path.join(d, f))
+    return path
+
+
+def read_checkpoint(st: "State", path) -> dict:
+    """read_checkpoint! (io_run.jl:294-314): the case and precision must match the state; restores
+    every level's current populations, velocity and density, the step and mass0. Returns the
+    header (with n_avg and the nine force sums for the caller's histories)."""
+    with open(path, "rb") as io:
+        data = io.read()
+    ck = unpack_checkpoint(data, st.dtype, st.config_sha, st.stl_sha, [m.nocts for m in st.level_meshes],
+                           [_level_ncut(m) for m in st.level_meshes])
+    for l, lv in enumerate(ck["levels"], start=1):
+        st.set_state(lv["f"], lv["u"], lv["rho"], l)
+    st.step = ck["step"]
+    st.mass0 = ck["mass0"]
+    return ck
+
+
+def resume_checkpoint(st: "State", out):
+    """resume_checkpoint! (io_run.jl:317-323): restore the latest checkpoint under `out`; returns
+    its step, or None when there is none."""
+    d = os.path.join(str(out), "checkpoints")
+    if not os.path.isdir(d):
+        return None
+    files = sorted(f for f in os.listdir(d) if f.startswith("checkpoint_") and f.endswith(".bin"))
+    if not files:
+        return None
+    return read_checkpoint(st, os.path.join(d, files[-1]))["step"]
