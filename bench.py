@@ -370,9 +370,13 @@ def main():
             line["octree_config3"] = c3
         if args.kbc_steps > 0:
             from openaerolab_alpha_01_b200.workloads import benchmark_entropic
-            kb = benchmark_entropic(128, steps=args.kbc_steps, warmup=3)
+            kb = benchmark_entropic(128, steps=args.kbc_steps, warmup=3, math="fast")
             kb["roofline_frac"] = round(kb["achieved_gbs"] / peak, 4)
             kb["bound"] = "FP32 issue (13-moment Newton sweeps and entropy evaluations), not HBM"
+            ex = benchmark_entropic(128, steps=args.kbc_steps, warmup=3, math="exact")
+            kb["exact_math"] = {"mlups": ex["mlups"], "ms_per_step": ex["ms_per_step"],
+                                "note": "software exp/log shared with the oracle (bit-identical to it)"}
+            kb["speedup_vs_exact"] = round(kb["mlups"] / ex["mlups"], 3)
             line["kbc_d3q39"] = kb
         if args.batch_steps > 0:
             from openaerolab_alpha_01_b200.workloads import config4

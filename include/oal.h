@@ -155,7 +155,15 @@ typedef struct oal_step_params {
   float shock_nu_max;            /* Mach-pocket viscosity: max(5 shock_nu_max, 0.24) (default 0) */
   /* OAL_SOLID_GRAD: share of Pi_neq the wall keeps (config grad_pineq_scale, default 1) */
   float grad_pineq_scale;
-  int32_t reserved[3];
+  /* Variable eddy viscosity of the D3Q27 step (kernel_cumulant.jl:546-588): 0 = WALE with the
+   * background floor (VARIABLE_NU_SGS false, the default); 1 = nu_sgs from the previous step's
+   * post-collision Pi_neq, c_pi |Pi_pre| / (rho cs^2) (VARIABLE_NU_SGS); 2 = the Germano-Lilly
+   * dynamic coefficient from a 7-point test filter of the velocity (kernel_dynamic_sgs.jl,
+   * DYNAMIC_SGS_ENABLED). Modes 1 and 2 floor nu_sgs at nu_sgs_floor and cap it at 0.1; every
+   * block of the level then steps in the general kernel. Library-owned levels only. */
+  int32_t variable_nu_sgs;
+  float c_pi;                    /* VARIABLE_NU_SGS_C_PI (default 0.2) */
+  float nu_sgs_floor;            /* VARIABLE_NU_SGS_FLOOR (default 0.002) */
 } oal_step_params;
 
 /* ---- library ---------------------------------------------------------------------------- */
@@ -244,13 +252,17 @@ void oal_level_destroy(oal_level* L);
 /* Level creation options (bits of `flags`). */
 enum {
   OAL_LEVEL_DENSE = 1,         /* box levels in FP32/FP16/BF16: dense padded population grid */
-  OAL_LEVEL_ROUND_NEAREST = 2  /* FP16/BF16 deviation storage: the step kernels round the stored
+  OAL_LEVEL_ROUND_NEAREST = 2, /* FP16/BF16 deviation storage: the step kernels round the stored
                                   deviations to nearest. Default: stochastic rounding (hardware
                                   cvt.rs, random bits hashed from the cell's position in its case
                                   and its new macros), unbiased in expectation, which keeps
                                   integrated quantities such as the drag free of the rounding bias
                                   of a slowly varying state. No counterpart in the reference (its
                                   populations are Float32). */
+  OAL_LEVEL_EXACT_MATH = 4     /* D3Q39 entropic levels: exp and log by the software routines the
+                                  CPU restatement shares (the step is then bit-identical to it).
+                                  Default: CUDA's expf / logf, the functions the reference's
+                                  Float32 exp and log compile to on its CUDA backend. */
 };
 /* oal_level_create with options; flags = 0 is oal_level_create. */
 oal_status oal_level_create_ex(const oal_geometry* g, int32_t operator_id, int32_t storage, uint32_t flags,
@@ -297,8 +309,41 @@ oal_status oal_level_set_bouzidi(oal_level* L, int32_t n_cells, const int32_t* c
                                  float limiter_abs_cap);
 /* Non-blocking variant: enqueue the copy of the force into a host buffer (pinned for overlap). */
 oal_status oal_level_get_forces_async(oal_level* L, double* host_out3, void* stream);
+/* Surface-stress force mapping of a D3Q27 level: the reference's compute_aerodynamics!
+ * (src/forces/surface.jl:1577-1587) with its default Prandtl force method, i.e.
+ * map_stresses_kernel! (:636-1031) over the triangles, compute_stress_from_cell (:180-269) and
+ * integrate_forces_kernel! (:1265-1331). Triangles: centroid, unit outward normal and area per
+ * row (tri[n * 7], cell units: cell (i, j, k), 1-based, is centred at (i - 1/2, j - 1/2, k - 1/2);
+ * the reference's mesh_offset and dx folded in by the caller). oal_level_set_surface copies them
+ * (n_tri = 0 detaches). */
+oal_status oal_level_set_surface(oal_level* L, int32_t n_tri, const float* tri);
+typedef struct oal_surface_params {
+  uint32_t abi_version;     /* OAL_ABI_VERSION */
+  int32_t search_radius;    /* probe steps along the normal (reference default 8) */
+  int32_t recover_normal;   /* 1: closed bodies may take the opposite side (reference default) */
+  float tau;                /* molecular relaxation time of the level */
+  float c_wale;             /* C_SMAGO (config c_wale, default 0.20) */
+  float nu_sgs_background;  /* NU_SGS_BACKGROUND (default 0) */
+  float pressure_scale;     /* rho_phys u_scale^2 (1: lattice units) */
+  float stress_scale;       /* the same for the shear (the reference uses pressure_scale) */
+  float moment_center[3];   /* moment reference point (cell units) */
+  int32_t reserved[3];
+} oal_surface_params;
+/* Fills `sp` with the reference's defaults. */
+void oal_default_surface_params(oal_surface_params* sp);
+/* Maps the stresses on the attached triangles from the level's current density and velocity.
+ * out[9] = pressure force, viscous force, moment about moment_center (FP64, summed in a fixed
+ * order; the reference adds Float32 atomics). per_tri (optional, host float[n * 6]): pressure,
+ * shear x, y, z, normal sign (-1 where the opposite side was taken), probe wall distance (0: no
+ * fluid found). Synchronous. */
+oal_status oal_level_surface_forces(oal_level* L, const oal_surface_params* sp, double out[9], float* per_tri);
+
 /* FP64 on-device reduction of the current state: out = {mass, px, py, pz} over fluid cells. */
 oal_status oal_level_mass_momentum(oal_level* L, double out[4]);
+/* Non-equilibrium stress of the current state (compute_pi_neq_kernel!, kernel_pi_neq.jl:39-180,
+ * D3Q27): Pi_ab = sum_k c_a c_b (f_k - f_eq_k(rho, u)) at every cell, 0 in solid or unphysical
+ * cells; host float out[6][n_blocks * 512] in the order xx, yy, zz, xy, xz, yz. */
+oal_status oal_level_pi_neq(oal_level* L, float* out);
 /* Device pointers of the current state (for zero-copy interop): f, rho, vel. */
 oal_status oal_level_device_state(oal_level* L, void** f, void** rho, void** vel);
 /* Bytes of device memory this level holds. */
@@ -383,7 +428,10 @@ oal_status oal_geometry_blocks(const oal_geometry* g, int64_t out[3]);
  * strides as in oal_level_fields); obstacle: device uint8[512*n_blocks] or NULL; out: device
  * double[4]. n_blocks above the maximum returns OAL_E_TOO_LARGE. The first call on a device looks
  * up the array's device address (cudaGetSymbolAddress) and should come before any stream capture.
- * All calls share the array: calls that overlap on the GPU race and must be serialised. */
+ * All calls share the array: calls that overlap on the GPU race and must be serialised. The
+ * looked-up address is kept per device number for the life of the process: after a
+ * cudaDeviceReset (or any new primary context) on that device the kept address is stale, so a
+ * process that resets a device must not call this entry point on it again. */
 #define OAL_NOALLOC_MAX_BLOCKS 65536
 oal_status oal_mass_momentum_noalloc(const void* f, int32_t storage, int64_t f_block_stride, int64_t f_dir_stride,
                                      const uint8_t* obstacle, int32_t n_blocks, double* out, void* stream);

@@ -44,6 +44,7 @@ OAL_LIMITER_POSITIVITY = 2
 
 OAL_LEVEL_DENSE = 1
 OAL_LEVEL_ROUND_NEAREST = 2
+OAL_LEVEL_EXACT_MATH = 4
 
 OAL_SOLID_FULLWAY = 0
 OAL_SOLID_HALFWAY = 1
@@ -92,6 +93,24 @@ class StepParams(C.Structure):
         ("nu_sgs_lattice_floor", C.c_float),
         ("shock_nu_max", C.c_float),
         ("grad_pineq_scale", C.c_float),
+        ("variable_nu_sgs", C.c_int32),
+        ("c_pi", C.c_float),
+        ("nu_sgs_floor", C.c_float),
+    ]
+
+
+class SurfaceParams(C.Structure):
+    """oal_surface_params (include/oal.h): the surface-stress mapping's settings."""
+    _fields_ = [
+        ("abi_version", C.c_uint32),
+        ("search_radius", C.c_int32),
+        ("recover_normal", C.c_int32),
+        ("tau", C.c_float),
+        ("c_wale", C.c_float),
+        ("nu_sgs_background", C.c_float),
+        ("pressure_scale", C.c_float),
+        ("stress_scale", C.c_float),
+        ("moment_center", C.c_float * 3),
         ("reserved", C.c_int32 * 3),
     ]
 
@@ -264,6 +283,10 @@ _SIGNATURES = {
                                           C.c_float, C.c_int32, C.c_float, C.c_float]),
     "oal_level_get_forces_async": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "oal_level_mass_momentum": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double)]),
+    "oal_level_set_surface": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p]),
+    "oal_default_surface_params": (None, [C.c_void_p]),
+    "oal_level_surface_forces": (C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_void_p]),
+    "oal_level_pi_neq": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "oal_level_device_state": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                            C.POINTER(C.c_void_p)]),
     "oal_level_device_bytes": (C.c_int64, [C.c_void_p]),

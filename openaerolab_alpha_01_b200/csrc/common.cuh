@@ -74,7 +74,9 @@ enum CaseFlags : uint32_t {
   CF_PERIODIC_Z = 1u << 17,
   CF_GRAD_WALL = 1u << 18,   // Grad-reconstruction wall on fluid cells with links into solids
   CF_BOUZIDI = 1u << 19,     // linear Bouzidi correction after the step (the step itself is full-way)
-  CF_GENERAL_RATES = 1u << 20  // omega_bulk, omega3 or omega4 differs from 1 (the configuration default)
+  CF_GENERAL_RATES = 1u << 20, // omega_bulk, omega3 or omega4 differs from 1 (the configuration default)
+  CF_SGS_PI = 1u << 21,        // variable nu_sgs from the stored post-collision Pi_neq
+  CF_SGS_DYNAMIC = 1u << 22    // variable nu_sgs from the Germano-Lilly dynamic coefficient
 };
 
 struct CaseParams {
@@ -85,7 +87,7 @@ struct CaseParams {
   uint32_t flags;
   int32_t nx, ny, nz;
   float grad_pineq_scale;  // CF_GRAD_WALL
-  int32_t pad[2];
+  float c_pi, nu_sgs_floor;  // CF_SGS_PI / CF_SGS_DYNAMIC
 };
 static_assert(sizeof(CaseParams) == 80, "CaseParams layout");
 
@@ -175,6 +177,8 @@ struct StepArgs {
   int32_t round_nearest;          // 16-bit codecs: round stored deviations to nearest (else stochastically)
   const int32_t* fast_rec;        // x-pair kernel: per work entry 32 ints (27-entry neighbour row,
                                   // block coordinates + case, block index), in work-list order
+  void* pi_neq;                   // CF_SGS_PI: post-collision Pi_neq (compute type, [6][nb*512]),
+                                  // read at the cell, then rewritten with this step's
   double* force_out;              // general kernel of a single level: the last CTA sums the
   uint32_t* force_ticket;         // momentum-exchange partials into force_out (ticket reset to 0)
   CaseParams p0;

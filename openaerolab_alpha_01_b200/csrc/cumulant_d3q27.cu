@@ -1149,6 +1149,7 @@ __global__ void __launch_bounds__(128) k_cumulant_gen(const StepArgs a, const in
   R* __restrict__ rho_out = static_cast<R*>(a.rho_out);
   R* __restrict__ vel_out = static_cast<R*>(a.vel_out);
   const R* __restrict__ vel_in = static_cast<const R*>(a.vel_in);
+  R* __restrict__ pi_neq = static_cast<R*>(a.pi_neq);
   const int64_t bst = a.f_bstride, kst = a.f_kstride, vcs = a.v_cstride;
   const int n_real = a.n_blocks;
 
@@ -1176,6 +1177,10 @@ __global__ void __launch_bounds__(128) k_cumulant_gen(const StepArgs a, const in
     }
     rho_out[vown] = R(1);
     vel_out[vown] = R(0); vel_out[vown + vcs] = R(0); vel_out[vown + 2 * vcs] = R(0);
+    if (flags & CF_SGS_PI) {
+#pragma unroll
+      for (int m = 0; m < 6; ++m) pi_neq[vown + m * vcs] = R(0);
+    }
   } else {
     // ---- pull (kernel_cumulant.jl:190-400): where every source lies in a block (ghost blocks
     // included), the stored word of the neighbour and, for half-way links, the own cell's
@@ -1239,6 +1244,10 @@ __global__ void __launch_bounds__(128) k_cumulant_gen(const StepArgs a, const in
         fout[own + k * kst] = v;
         if (store_post) fpost[own + k * kst] = v;
       }
+      if (flags & CF_SGS_PI) {
+#pragma unroll
+        for (int m = 0; m < 6; ++m) pi_neq[vown + m * vcs] = R(0);
+      }
     } else {
       // ---- macros, sponge, wall model (kernel_cumulant.jl:420-491) ----
       rho = vmaxc(rho, R(0.01));
@@ -1292,7 +1301,7 @@ __global__ void __launch_bounds__(128) k_cumulant_gen(const StepArgs a, const in
       vel_out[vown] = ux; vel_out[vown + vcs] = uy; vel_out[vown + 2 * vcs] = uz;
 
       // ---- WALE (kernel_cumulant.jl:496-549): own value for missing, ghost or solid neighbours ----
-      R nu_eddy = R(0);
+      R nu_eddy = R(0), nu_dyn = R(0);
       if (flags & CF_GRADIENTS) {
         auto nbv = [&](int dx, int dy, int dz, int c, uint32_t solid) -> R {
           const int nx = x + dx, ny = y + dy, nz = z + dz;
@@ -1313,8 +1322,44 @@ __global__ void __launch_bounds__(128) k_cumulant_gen(const StepArgs a, const in
         const R g32 = h * (nbv(0, 1, 0, 2, sN) - nbv(0, -1, 0, 2, sS));
         const R g33 = h * (nbv(0, 0, 1, 2, sT) - nbv(0, 0, -1, 2, sB));
         nu_eddy = wale_nu<R>(g11, g12, g13, g21, g22, g23, g31, g32, g33, cp.c_wale);
+        if (flags & CF_SGS_DYNAMIC) {
+          // Germano-Lilly (kernel_cumulant.jl:553-565): the face neighbours' previous-step
+          // velocities, this cell's current one for missing, ghost or solid neighbours
+          // (kernel_dynamic_sgs.jl:57-103)
+          R c[3] = {ux, uy, uz}, n[6][3];
+          auto nbd = [&](int dx, int dy, int dz, uint32_t solid, R (&o)[3]) {
+            const int nx = x + dx, ny = y + dy, nz = z + dz;
+            const int nb = s_nbr[nbr_dir(nx >> 3, ny >> 3, nz >> 3)];
+            if (nb < 0 || nb >= n_real || solid) { o[0] = ux; o[1] = uy; o[2] = uz; return; }
+            const int64_t v = (int64_t)nb * kCells + ((nx & 7) | ((ny & 7) << 3) | ((nz & 7) << 6));
+            o[0] = vel_in[v]; o[1] = vel_in[v + vcs]; o[2] = vel_in[v + 2 * vcs];
+          };
+          nbd(1, 0, 0, sE, n[0]); nbd(-1, 0, 0, sW, n[1]); nbd(0, 1, 0, sN, n[2]);
+          nbd(0, -1, 0, sS, n[3]); nbd(0, 0, 1, sT, n[4]); nbd(0, 0, -1, sB, n[5]);
+          const R S12 = h * (g12 + g21), S13 = h * (g13 + g31), S23 = h * (g23 + g32);
+          const R cd = dynamic_cs2<R>(c, n, g11, g22, g33, S12, S13, S23);
+          const R s_sq = R(2) * (g11 * g11 + g22 * g22 + g33 * g33) + R(4) * (S12 * S12 + S13 * S13 + S23 * S23);
+          const R s_mag = sqrt(s_sq > R(1e-30) ? s_sq : R(1e-30));
+          const R nd = cd * s_mag * R(cp.amr_sgs_scale);
+          nu_dyn = nd < R(0.1) ? nd : R(0.1);
+        }
       }
-      const R omega1 = omega1_from<R>(nu_eddy, cp);
+      R omega1;
+      if (flags & (CF_SGS_PI | CF_SGS_DYNAMIC)) {
+        // variable nu_sgs (kernel_cumulant.jl:551-586): max(WALE, model stress, floor)
+        R stress = nu_dyn;
+        if (flags & CF_SGS_PI) {
+          R pv[6];
+#pragma unroll
+          for (int m = 0; m < 6; ++m) pv[m] = pi_neq[vown + m * vcs];
+          stress = pi_stress_nu<R>(pv, rho, cp);
+        }
+        R nu = nu_eddy * R(cp.amr_sgs_scale);
+        nu = fmax(fmax(nu, stress), R(cp.nu_sgs_floor) * R(cp.amr_sgs_scale));
+        omega1 = omega1_of_nu<R>(nu, cp);
+      } else {
+        omega1 = omega1_from<R>(nu_eddy, cp);
+      }
       cumulant_collide<R>(A, rho, uxe, uye, uze, omega1, cp);
 
       // ---- Guo forcing + store (kernel_cumulant.jl:889-908) ----
@@ -1335,6 +1380,16 @@ __global__ void __launch_bounds__(128) k_cumulant_gen(const StepArgs a, const in
         // post-collision populations and velocity (grad_wall_kernel.jl:42-144, timestep.jl:1738)
         grad_wall<R>(A, rho, R(1) / R(cp.tau), R(cp.grad_pineq_scale));
         vel_out[vown] = R(0); vel_out[vown + vcs] = R(0); vel_out[vown + 2 * vcs] = R(0);
+        ux = R(0); uy = R(0); uz = R(0);
+      }
+      if (flags & CF_SGS_PI) {
+        // Pi_neq refresh of the post-collision populations against the stored macros
+        // (refresh_pi_neq!, kernel_pi_neq.jl:39-180, fused into the store)
+        const bool skip = !isfinite(rho) || rho < R(0.01) || rho > R(10) || !isfinite(ux) || !isfinite(uy) || !isfinite(uz);
+        R pv[6];
+        pi_neq_of<R>(A, rho, ux, uy, uz, comp, skip, pv);
+#pragma unroll
+        for (int m = 0; m < 6; ++m) pi_neq[vown + m * vcs] = pv[m];
       }
       uint32_t hsr = 0u;
       if constexpr (sizeof(S) == 2) {

@@ -78,15 +78,96 @@ __device__ __forceinline__ V wale_nu(V g11, V g12, V g13, V g21, V g22, V g23, V
   return vsel_gt(OP1, eps, vsel_gt(den, eps, nu, zero), zero);
 }
 
-// omega_1 from the eddy viscosity (kernel_cumulant.jl:585-590, background SGS path)
+// Germano-Lilly dynamic Smagorinsky coefficient Cs^2 in [0, 0.25] (kernel_dynamic_sgs.jl:128-240):
+// 7-point box test filter of the velocity (the cell's current velocity c and its six face
+// neighbours' previous-step velocities, the centre value standing in for missing or solid ones),
+// Leonard stress, test-scale modelled stress from the grid strain (g11, g22, g33 and the
+// symmetric S12, S13, S23), Lilly's least-squares contraction. Dx = 1.
+template <class R>
+__device__ __forceinline__ R dynamic_cs2(const R (&c)[3], const R (&n)[6][3], R g11, R g22, R g33, R S12, R S13, R S23) {
+  const R inv7 = R(1) / R(7);
+  R ut[3], uu[6];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    R sum = c[a];
+#pragma unroll
+    for (int j = 0; j < 6; ++j) sum = sum + n[j][a];
+    ut[a] = inv7 * sum;
+  }
+  const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+  for (int m = 0; m < 6; ++m) {
+    R sum = c[ia[m]] * c[ib[m]];
+#pragma unroll
+    for (int j = 0; j < 6; ++j) sum = sum + n[j][ia[m]] * n[j][ib[m]];
+    uu[m] = inv7 * sum;
+  }
+  const R Lxx = uu[0] - ut[0] * ut[0], Lyy = uu[1] - ut[1] * ut[1], Lzz = uu[2] - ut[2] * ut[2];
+  const R Lxy = uu[3] - ut[0] * ut[1], Lxz = uu[4] - ut[0] * ut[2], Lyz = uu[5] - ut[1] * ut[2];
+  const R Ltr = (Lxx + Lyy + Lzz) * (R(1) / R(3));
+  const R Lxx_d = Lxx - Ltr, Lyy_d = Lyy - Ltr, Lzz_d = Lzz - Ltr;
+  const R S_sq = R(2) * (g11 * g11 + g22 * g22 + g33 * g33) + R(4) * (S12 * S12 + S13 * S13 + S23 * S23);
+  const R S_mag = sqrt(S_sq > R(1e-30) ? S_sq : R(1e-30));
+  const R M_coeff = R(2) * R(1) * R(1) * R(3.659306f) * S_mag;
+  const R Mxx = M_coeff * g11, Myy = M_coeff * g22, Mzz = M_coeff * g33;
+  const R Mxy = M_coeff * S12, Mxz = M_coeff * S13, Myz = M_coeff * S23;
+  const R Mtr = (Mxx + Myy + Mzz) * (R(1) / R(3));
+  const R Mxx_d = Mxx - Mtr, Myy_d = Myy - Mtr, Mzz_d = Mzz - Mtr;
+  const R LM = Lxx_d * Mxx_d + Lyy_d * Myy_d + Lzz_d * Mzz_d + R(2) * (Lxy * Mxy + Lxz * Mxz + Lyz * Myz);
+  const R MM = Mxx_d * Mxx_d + Myy_d * Myy_d + Mzz_d * Mzz_d + R(2) * (Mxy * Mxy + Mxz * Mxz + Myz * Myz);
+  const R cd = R(0.5) * LM / (MM + R(1e-20));
+  return cd > R(0.25) ? R(0.25) : (cd < R(0) ? R(0) : cd);
+}
+
+// nu_sgs of the stored post-collision Pi_neq (kernel_cumulant.jl:567-586): c_pi |Pi_pre| / (rho cs^2),
+// |Pi_pre| = |tau / (tau - 1)| |Pi_post|, capped at 0.1
+template <class R>
+__device__ __forceinline__ R pi_stress_nu(const R (&pi)[6], R rho, const CaseParams& cp) {
+  const R mag = sqrt(pi[0] * pi[0] + pi[1] * pi[1] + pi[2] * pi[2] +
+                     R(2) * (pi[3] * pi[3] + pi[4] * pi[4] + pi[5] * pi[5]));
+  const R denom = R(cp.tau) - R(1);
+  const R corr = fabs(denom) < R(1e-3) ? R(1) : R(cp.tau) / denom;
+  const R pre = fabs(corr) * mag;
+  const R rc = (!isfinite(rho) || rho < R(0.01)) ? R(1) : rho;
+  const R nu = R(cp.c_pi) * pre / (rc * (R(1) / R(3)) + R(1e-10)) * R(cp.amr_sgs_scale);
+  return nu < R(0.1) ? nu : R(0.1);
+}
+
+// Pi_neq_ab = sum_k c_a c_b (f_k - f_eq_k(rho, u)) of one cell (kernel_pi_neq.jl:120-180); zero for
+// solid or unphysical cells
+template <class R>
+__device__ __forceinline__ void pi_neq_of(const R (&f)[kQ27], R rho, R ux, R uy, R uz, bool comp, bool skip, R (&pi)[6]) {
+  const R rs = skip ? R(0) : rho, us = skip ? R(0) : ux, vs = skip ? R(0) : uy, ws = skip ? R(0) : uz;
+  R p[6] = {R(0), R(0), R(0), R(0), R(0), R(0)};
+#pragma unroll
+  for (int k = 0; k < kQ27; ++k) {
+    const R cx = R(q27_cx(k)), cy = R(q27_cy(k)), cz = R(q27_cz(k));
+    const R fe = feq_c<R>(rs, us, vs, ws, R(q27_w(k)), cx, cy, cz, comp);
+    const R fn = (skip ? R(0) : f[k]) - fe;
+    p[0] = p[0] + cx * cx * fn; p[1] = p[1] + cy * cy * fn; p[2] = p[2] + cz * cz * fn;
+    p[3] = p[3] + cx * cy * fn; p[4] = p[4] + cx * cz * fn; p[5] = p[5] + cy * cz * fn;
+  }
+  const R mask = skip ? R(0) : R(1);
+#pragma unroll
+  for (int m = 0; m < 6; ++m) pi[m] = p[m] * mask;
+}
+
+// omega_1 from the final eddy viscosity (kernel_cumulant.jl:591-594)
+template <class V>
+__device__ __forceinline__ V omega1_of_nu(V nu_eddy, const CaseParams& cp) {
+  using T = SC<V>;
+  const T nu_mol = (T(cp.tau) - T(0.5)) * T(1.0 / 3.0);
+  const V tau_eff = vfma(splat<V>(T(3)), splat<V>(nu_mol) + nu_eddy, splat<V>(T(0.5)));
+  return vrcp(vmaxc(tau_eff, T(0.500001)));
+}
+
+// omega_1 from the WALE eddy viscosity with the background floor (kernel_cumulant.jl:546-590)
 template <class V>
 __device__ __forceinline__ V omega1_from(V nu_eddy, const CaseParams& cp) {
   using T = SC<V>;
   nu_eddy = nu_eddy * splat<V>(T(cp.amr_sgs_scale));
   nu_eddy = vmaxc(nu_eddy, T(cp.nu_sgs_bg) * T(cp.amr_sgs_scale));
-  const T nu_mol = (T(cp.tau) - T(0.5)) * T(1.0 / 3.0);
-  const V tau_eff = vfma(splat<V>(T(3)), splat<V>(nu_mol) + nu_eddy, splat<V>(T(0.5)));
-  return vrcp(vmaxc(tau_eff, T(0.500001)));
+  return omega1_of_nu<V>(nu_eddy, cp);
 }
 
 template <class V>

@@ -41,6 +41,20 @@ namespace {
 
 constexpr int Q = 39;
 constexpr int kThreads = 128;
+// Fast path (CUDA's expf / logf): the cached multipliers start the solve whenever their
+// equilibrium matches the target moments within sqrt(KBC_FAST_WARM_GATE * TOL_SQ), i.e. to ~3e-2
+// relative. The reference's staleness gate (factor 100, ~2.7e-5 relative) rejects them in nearly
+// every cell of an unsteady flow, so every solve restarts from the polynomial guess; both starts
+// converge to the same multipliers within the solve's tolerance.
+#ifndef KBC_FAST_WARM_GATE
+#define KBC_FAST_WARM_GATE 1e8f
+#endif
+#ifndef KBC_FAST_TOL_SCALE
+#define KBC_FAST_TOL_SCALE 1.0f
+#endif
+#ifndef KBC_FAST_MAX_SWEEPS
+#define KBC_FAST_MAX_SWEEPS 200
+#endif
 #ifndef KBC_MIN_BLOCKS
 #define KBC_MIN_BLOCKS 6  // CTAs per SM the register budget is cut for (33 KB of shared memory each)
 #endif
@@ -91,7 +105,24 @@ __device__ __forceinline__ float jmax(float a, float b) { return (a != a || b !=
 __device__ __forceinline__ float jmin(float a, float b) { return (a != a || b != b) ? qnan() : (a < b ? a : b); }
 __device__ __forceinline__ float jclamp(float v, float lo, float hi) { return v > hi ? hi : (v < lo ? lo : v); }
 __device__ __forceinline__ float smooth(float t) { return t * t * (3.0f - 2.0f * t); }
-__device__ __forceinline__ float safe_log(float x) { return x > 0.0f ? kbc::log(x) : -88.0f; }
+// exp and log: FAST = CUDA's expf / logf (what the reference's Float32 exp and log compile to on
+// its CUDA backend, within 2 ulp); otherwise the software routines shared with the CPU restatement
+// (kbc_math.h), so that the step is bit-identical to it
+template <bool FAST> __device__ __forceinline__ float kexp(float x) {
+  if constexpr (FAST) return __expf(x);
+  else return kbc::exp(x);
+}
+template <bool FAST> __device__ __forceinline__ float klog(float x) {
+  if constexpr (FAST) return __logf(x);
+  else return kbc::log(x);
+}
+// s + a b: one rounding when FAST (fused), the reference's two otherwise
+template <bool FAST> __device__ __forceinline__ float kmad(float a, float b, float s) {
+  if constexpr (FAST) return __fmaf_rn(a, b, s);
+  else return s + a * b;
+}
+template <bool FAST = false>
+__device__ __forceinline__ float safe_log(float x) { return x > 0.0f ? klog<FAST>(x) : -88.0f; }
 
 struct KbcArgs {
   const float* fin;
@@ -113,6 +144,8 @@ struct KbcArgs {
   const uint32_t* cmask;
   int32_t faces;            // the level has ghost blocks
   float trho, tjx, tjy, tjz;  // moments of feq_inlet, the inlet-face pin's targets
+  float warm_gate;          // fast path: squared moment residual (in TOL_SQ units) up to which
+                            // the cached multipliers start the solve (the reference: 100)
 };
 
 // the face fill of one step: every ghost slot a real cell pulls receives its face value
@@ -174,7 +207,8 @@ __device__ __forceinline__ void build_tables(Tables& T) {
     r[9] = cx * efl; r[10] = cy * efl; r[11] = cz * efl;
     r[12] = k < 7 ? float(1.0 / 12) : k < 15 ? float(1.0 / 27) : k < 21 ? float(2.0 / 135) : k < 33 ? float(1.0 / 432)
                                                                                                : float(1.0 / 1620);
-    r[13] = r[14] = r[15] = 0.0f;
+    r[13] = 1.0f / r[12];  // inverse weight (the fast path's entropy sums)
+    r[14] = r[15] = 0.0f;
     T.ps[k] = k == 0 ? (NP | 0x200) : (pair | (opp < k ? 0x100 : 0x200));
     T.c[k] = (cxi + 3) | ((cyi + 3) << 4) | ((czi + 3) << 8) | (opp << 12);
   }
@@ -182,8 +216,17 @@ __device__ __forceinline__ void build_tables(Tables& T) {
 
 // exp argument la0 + la1 b0 + ... + la12 b11 of one direction (physics_utils.jl:589-593), every
 // term written out in the reference's order
+template <bool FAST = false>
 __device__ __forceinline__ float lda_row(const float (&la)[13], const float4* row) {
   const float4 r0 = row[0], r1 = row[1], r2 = row[2];
+  if constexpr (FAST) {
+    float l = __fmaf_rn(la[1], r0.x, la[0]);
+    l = __fmaf_rn(la[2], r0.y, l); l = __fmaf_rn(la[3], r0.z, l); l = __fmaf_rn(la[4], r0.w, l);
+    l = __fmaf_rn(la[5], r1.x, l); l = __fmaf_rn(la[6], r1.y, l); l = __fmaf_rn(la[7], r1.z, l);
+    l = __fmaf_rn(la[8], r1.w, l); l = __fmaf_rn(la[9], r2.x, l); l = __fmaf_rn(la[10], r2.y, l);
+    l = __fmaf_rn(la[11], r2.z, l);
+    return __fmaf_rn(la[12], r2.w, l);
+  }
   float l = la[0] + la[1] * r0.x;
   l = l + la[2] * r0.y;
   l = l + la[3] * r0.z;
@@ -199,16 +242,19 @@ __device__ __forceinline__ float lda_row(const float (&la)[13], const float4* ro
   return l;
 }
 // max(rho w_k exp(clamp(lda)), 1e-15) (physics_utils.jl:594, 759-760)
+template <bool FAST = false>
 __device__ __forceinline__ float fi_row(float rho, const float (&la)[13], const float4* row) {
-  return maxc(rho * row[3].x * kbc::exp(jclamp(lda_row(la, row), -20.0f, 20.0f)), 1e-15f);
+  return maxc(rho * row[3].x * kexp<FAST>(jclamp(lda_row<FAST>(la, row), -20.0f, 20.0f)), 1e-15f);
 }
 
 // physics_utils.jl:493-736: 13 multipliers by block-Jacobi Newton sweeps, warm-started from the
 // cached multipliers when they pass the staleness gate
-__device__ __forceinline__ void solve_lambdas(const Tables& T, float rho, float ux, float uy, float uz, float (&la)[13]) {
+template <bool FAST = false>
+__device__ __forceinline__ void solve_lambdas(const Tables& T, float rho, float ux, float uy, float uz, float (&la)[13],
+                                              float warm_gate = 100.0f) {
   const float OMEGA = 1.5f, F_FLOOR_EQ = 1e-15f;
   const float eps = 1.1920928955078125e-7f;
-  const float TOL_SQ = 507.0f * eps * eps * rho * rho * 1.0f;
+  const float TOL_SQ = 507.0f * eps * eps * rho * rho * (FAST ? KBC_FAST_TOL_SCALE : 1.0f);
   const float eR = CS2;
   const float usq = ux * ux + uy * uy + uz * uz;
   const float dT = 1.0f - 1.0f;
@@ -235,7 +281,7 @@ __device__ __forceinline__ void solve_lambdas(const Tables& T, float rho, float 
 #pragma unroll 1
     for (int k = 0; k < Q; ++k) {
       const float4* row = T.b[k];
-      const float fi = fi_row(rho, la, row);
+      const float fi = fi_row<FAST>(rho, la, row);
       const float4 r0 = row[0], r1 = row[1], r2 = row[2];
       gd[0] += fi;
       gd[1] += fi * r0.x; gd[2] += fi * r0.y; gd[3] += fi * r0.z; gd[4] += fi * r0.w;
@@ -245,49 +291,49 @@ __device__ __forceinline__ void solve_lambdas(const Tables& T, float rho, float 
     float gres = 0.0f;
 #pragma unroll
     for (int m = 0; m < 13; ++m) gres += (mt[m] - gd[m]) * (mt[m] - gd[m]);
-    if (gres > 100.0f * TOL_SQ) poly_start();
+    if (gres > (FAST ? warm_gate : 100.0f) * TOL_SQ) poly_start();
   }
   auto upd = [&](int m, float d, float j) {
     la[m] += j > F_FLOOR_EQ ? jclamp(OMEGA * (mt[m] - d) / j, -2.0f, 2.0f) : 0.0f;
   };
-  for (int sweep = 0; sweep < 200; ++sweep) {
+  for (int sweep = 0; sweep < (FAST ? KBC_FAST_MAX_SWEEPS : 200); ++sweep) {
     float d[13], j[13];
 #pragma unroll
     for (int m = 0; m < 13; ++m) { d[m] = 0.0f; j[m] = 0.0f; }
 #pragma unroll 3
     for (int k = 0; k < Q; ++k) {
       const float4* row = T.b[k];
-      const float fi = fi_row(rho, la, row);
+      const float fi = fi_row<FAST>(rho, la, row);
       const float4 r0 = row[0];
       d[0] += fi; j[0] += fi;
-      d[1] += fi * r0.x; j[1] += fi * r0.x * r0.x;
-      d[2] += fi * r0.y; j[2] += fi * r0.y * r0.y;
-      d[3] += fi * r0.z; j[3] += fi * r0.z * r0.z;
+      d[1] = kmad<FAST>(fi, r0.x, d[1]); j[1] = kmad<FAST>(fi * r0.x, r0.x, j[1]);
+      d[2] = kmad<FAST>(fi, r0.y, d[2]); j[2] = kmad<FAST>(fi * r0.y, r0.y, j[2]);
+      d[3] = kmad<FAST>(fi, r0.z, d[3]); j[3] = kmad<FAST>(fi * r0.z, r0.z, j[3]);
     }
 #pragma unroll
     for (int m = 0; m < 4; ++m) upd(m, d[m], j[m]);
 #pragma unroll 3
     for (int k = 0; k < Q; ++k) {
       const float4* row = T.b[k];
-      const float fi = fi_row(rho, la, row);
+      const float fi = fi_row<FAST>(rho, la, row);
       const float4 r0 = row[0], r1 = row[1], r2 = row[2];
-      d[4] += fi * r0.w; j[4] += fi * r0.w * r0.w;
-      d[5] += fi * r1.x; j[5] += fi * r1.x * r1.x;
-      d[6] += fi * r1.y; j[6] += fi * r1.y * r1.y;
-      d[7] += fi * r1.z; j[7] += fi * r1.z * r1.z;
-      d[8] += fi * r1.w; j[8] += fi * r1.w * r1.w;
-      d[9] += fi * r2.x; j[9] += fi * r2.x * r2.x;
+      d[4] = kmad<FAST>(fi, r0.w, d[4]); j[4] = kmad<FAST>(fi * r0.w, r0.w, j[4]);
+      d[5] = kmad<FAST>(fi, r1.x, d[5]); j[5] = kmad<FAST>(fi * r1.x, r1.x, j[5]);
+      d[6] = kmad<FAST>(fi, r1.y, d[6]); j[6] = kmad<FAST>(fi * r1.y, r1.y, j[6]);
+      d[7] = kmad<FAST>(fi, r1.z, d[7]); j[7] = kmad<FAST>(fi * r1.z, r1.z, j[7]);
+      d[8] = kmad<FAST>(fi, r1.w, d[8]); j[8] = kmad<FAST>(fi * r1.w, r1.w, j[8]);
+      d[9] = kmad<FAST>(fi, r2.x, d[9]); j[9] = kmad<FAST>(fi * r2.x, r2.x, j[9]);
     }
 #pragma unroll
     for (int m = 4; m < 10; ++m) upd(m, d[m], j[m]);
 #pragma unroll 3
     for (int k = 0; k < Q; ++k) {
       const float4* row = T.b[k];
-      const float fi = fi_row(rho, la, row);
+      const float fi = fi_row<FAST>(rho, la, row);
       const float4 r2 = row[2];
-      d[10] += fi * r2.y; j[10] += fi * r2.y * r2.y;
-      d[11] += fi * r2.z; j[11] += fi * r2.z * r2.z;
-      d[12] += fi * r2.w; j[12] += fi * r2.w * r2.w;
+      d[10] = kmad<FAST>(fi, r2.y, d[10]); j[10] = kmad<FAST>(fi * r2.y, r2.y, j[10]);
+      d[11] = kmad<FAST>(fi, r2.z, d[11]); j[11] = kmad<FAST>(fi * r2.z, r2.z, j[11]);
+      d[12] = kmad<FAST>(fi, r2.w, d[12]); j[12] = kmad<FAST>(fi * r2.w, r2.w, j[12]);
     }
 #pragma unroll
     for (int m = 10; m < 13; ++m) upd(m, d[m], j[m]);
@@ -300,10 +346,11 @@ __device__ __forceinline__ void solve_lambdas(const Tables& T, float rho, float 
 
 // The mass-corrected equilibrium, kept as its multipliers: f_eq_k = corr * fi_k
 // (physics_utils.jl:738-795, kernel_entropic_d3q39.jl:2365-2385)
+template <bool FAST = false>
 struct Eq {
   float la[13];
   float rho, corr;
-  __device__ __forceinline__ float operator()(const Tables& T, int k) const { return corr * fi_row(rho, la, T.b[k]); }
+  __device__ __forceinline__ float operator()(const Tables& T, int k) const { return corr * fi_row<FAST>(rho, la, T.b[k]); }
 };
 
 // HRR blend of the stress part (kernel_entropic_d3q39.jl:2991-3034); k and opp(k) give the same s_fd
@@ -332,19 +379,21 @@ __device__ __forceinline__ float h_at(const Tables& T, const float* sh, int k) {
 }
 
 // kernel_entropic_d3q39.jl:113-133
+template <bool FAST = false>
 __device__ __forceinline__ float entropy_ah(const Tables& T, const float* sa, const float* sh, float coeff_h) {
   float H = 0.0f;
 #pragma unroll 3
   for (int k = 0; k < Q; ++k) {
     float fk = sa[k * kThreads] + coeff_h * h_at(T, sh, k);
     fk = maxc(fk, F_FLOOR);
-    H += fk * safe_log(fk / T.b[k][3].x);
+    H = kmad<FAST>(fk, safe_log<FAST>(FAST ? fk * T.b[k][3].y : fk / T.b[k][3].x), H);
   }
   return H;
 }
 
 // kernel_entropic_d3q39.jl:417-442: the lower and upper brackets, then up to max_iter midpoints,
 // through one entropy evaluation site
+template <bool FAST = false>
 __device__ __forceinline__ float alpha_bisection(const Tables& T, const float* sa, const float* sh, float beta,
                                                  float H_pre, int max_iter) {
   const float inv_2beta = 0.5f / jmax(beta, 0.01f);
@@ -352,7 +401,7 @@ __device__ __forceinline__ float alpha_bisection(const Tables& T, const float* s
   float H_lo = 0.0f;
   for (int it = -2; it < max_iter; ++it) {
     const float al = it == -2 ? lo : it == -1 ? hi : 0.5f * (lo + hi);
-    const float H = entropy_ah(T, sa, sh, 1.0f - 2.0f * beta * al);
+    const float H = entropy_ah<FAST>(T, sa, sh, 1.0f - 2.0f * beta * al);
     if (it == -2) { H_lo = H; continue; }
     if (it == -1) {
       if (!((H_lo - H_pre) * (H - H_pre) < 0.0f)) return inv_2beta;
@@ -365,6 +414,7 @@ __device__ __forceinline__ float alpha_bisection(const Tables& T, const float* s
 }
 
 // kernel_entropic_d3q39.jl:444-462 with entropy_and_deriv_at_alpha_39_fused (:192-215)
+template <bool FAST = false>
 __device__ __forceinline__ float alpha_newton(const Tables& T, const float* sa, const float* sh, float beta, float H_pre) {
   float alpha = 2.0f;
   const float inv_2beta = 0.5f / jmax(beta, 0.01f);
@@ -376,7 +426,7 @@ __device__ __forceinline__ float alpha_newton(const Tables& T, const float* sa, 
       const float hk = h_at(T, sh, k);
       float fk = sa[k * kThreads] + coeff_h * hk;
       fk = maxc(fk, F_FLOOR);
-      const float lr = safe_log(fk / T.b[k][3].x);
+      const float lr = safe_log<FAST>(FAST ? fk * T.b[k][3].y : fk / T.b[k][3].x);
       H += fk * lr;
       dH += (-2.0f * beta * hk) * (1.0f + lr);
     }
@@ -394,7 +444,8 @@ __device__ __forceinline__ float alpha_newton(const Tables& T, const float* sa, 
 
 // kernel_entropic_d3q39.jl:481-528 without its bisection fallback (false: the cell's deviation needs
 // the bisection); runs on the arriving populations before the split
-__device__ __forceinline__ bool alpha_taylor(const Tables& T, const float* sf, const Eq& eq, float h_scale, const Hrr& hr,
+template <bool FAST = false>
+__device__ __forceinline__ bool alpha_taylor(const Tables& T, const float* sf, const Eq<FAST>& eq, float h_scale, const Hrr& hr,
                                              float beta, float& alpha) {
   auto fneq_of = [&](int k, float& fe) {
     const int kb = (T.c[k] >> 12) & 63;
@@ -464,7 +515,7 @@ __global__ void __launch_bounds__(256) k_kbc_fill(const KbcFillArgs a) {
 // stay in the instruction cache. f_eq is recomputed from its multipliers where a pass needs it.
 // EDGES: the level has domain faces or solid cells (the pin, bounce-back and gradient fall-backs
 // are compiled in); periodic boxes without obstacles run the instance without them.
-template <bool EDGES>
+template <bool EDGES, bool FAST>
 __global__ void __launch_bounds__(kThreads, KBC_MIN_BLOCKS) k_kbc_step(const KbcArgs a) {
   __shared__ Tables T;
   __shared__ int32_t s_nbr[27];
@@ -593,18 +644,18 @@ __global__ void __launch_bounds__(kThreads, KBC_MIN_BLOCKS) k_kbc_step(const Kbc
   a.vout[ci + N] = uy;
   a.vout[ci + 2 * N] = uz;
   // STEP 3a: multipliers (warm start from the cache) and the mass correction (:2330-2385)
-  Eq eq;
+  Eq<FAST> eq;
   eq.rho = rho;
   {
     float* lam = a.lam + (int64_t)b * 13 * 512 + cell;
 #pragma unroll
     for (int m = 0; m < 13; ++m) eq.la[m] = lam[m * 512];
-    solve_lambdas(T, rho, ux_rel, uy_rel, uz_rel, eq.la);
+    solve_lambdas<FAST>(T, rho, ux_rel, uy_rel, uz_rel, eq.la, a.warm_gate);
 #pragma unroll
     for (int m = 0; m < 13; ++m) lam[m * 512] = eq.la[m];
     float sum = 0.0f;
 #pragma unroll 3
-    for (int k = 0; k < Q; ++k) sum += fi_row(rho, eq.la, T.b[k]);
+    for (int k = 0; k < Q; ++k) sum += fi_row<FAST>(rho, eq.la, T.b[k]);
     eq.corr = sum > 1e-15f ? rho / sum : 1.0f;
   }
   // STEP 3: WALE from the previous velocity (physics_utils.jl:2217-2233, :2588-2700)
@@ -746,12 +797,12 @@ __global__ void __launch_bounds__(kThreads, KBC_MIN_BLOCKS) k_kbc_step(const Kbc
 #pragma unroll 3
   for (int k = 0; k < Q; ++k) {
     const float fk = maxc(sf[k * kThreads], F_FLOOR);
-    H_pre += fk * safe_log(fk / T.b[k][3].x);
+    H_pre = kmad<FAST>(fk, safe_log<FAST>(FAST ? fk * T.b[k][3].y : fk / T.b[k][3].x), H_pre);
   }
   const float inv_2beta = 0.5f / jmax(beta, 0.01f);
   float alpha = 2.0f;
   bool alpha_done = false;
-  if (a.solver == 3) alpha_done = alpha_taylor(T, sf, eq, h_scale, hr, beta, alpha);
+  if (a.solver == 3) alpha_done = alpha_taylor<FAST>(T, sf, eq, h_scale, hr, beta, alpha);
   // STEP 5: split per pair, a_k = f_eq_k + coeff_s s_k over f_k (:2962-3095)
   const float coeff_s = 1.0f - 2.0f * beta;
 #pragma unroll 1
@@ -774,7 +825,7 @@ __global__ void __launch_bounds__(kThreads, KBC_MIN_BLOCKS) k_kbc_step(const Kbc
   }
   // STEP 6: alpha (:3109-3150)
   if (h_norm_sq > 1e-20f) {
-    if (a.solver == 1) { alpha = alpha_newton(T, sf, sh, beta, H_pre); alpha_done = true; }
+    if (a.solver == 1) { alpha = alpha_newton<FAST>(T, sf, sh, beta, H_pre); alpha_done = true; }
     else if (a.solver == 2) {
       float fn = 0.0f;
 #pragma unroll 1
@@ -785,7 +836,7 @@ __global__ void __launch_bounds__(kThreads, KBC_MIN_BLOCKS) k_kbc_step(const Kbc
       alpha = jclamp(2.0f - 0.5f * (h_norm_sq / jmax(fn, 1e-15f)), inv_2beta, 4.0f);
       alpha_done = true;
     }
-    if (!alpha_done) alpha = alpha_bisection(T, sf, sh, beta, H_pre, 10);
+    if (!alpha_done) alpha = alpha_bisection<FAST>(T, sf, sh, beta, H_pre, 10);
     if (!(alpha > 0.0f)) alpha = inv_2beta;
     alpha = jclamp(alpha, inv_2beta, 6.0f);
   } else {
@@ -854,7 +905,7 @@ __global__ void __launch_bounds__(kThreads) k_kbc_init(const float* rho_in, cons
   const int cell = ((blockIdx.x & 3) << 7) | threadIdx.x;
   const int64_t N = (int64_t)nb * 512, ci = (int64_t)b * 512 + cell;
   const float r = rho_in[ci], ux = vel_in[ci], uy = vel_in[ci + N], uz = vel_in[ci + 2 * N];
-  Eq eq;
+  Eq<> eq;
   eq.rho = r;
   eq.la[0] = qnan();
   solve_lambdas(T, r, ux, uy, uz, eq.la);
@@ -1000,6 +1051,7 @@ struct KbcLevel {
   int32_t g_n = 0;
   int g_parity = -1;
   oal_step_params g_p{};
+  bool exact_math = false;  // kbc_set_exact_math
 };
 
 namespace {
@@ -1057,8 +1109,15 @@ oal_status enqueue(KbcLevel* L, const KbcArgs& base, const oal_step_params* p_in
     k_kbc_fill<<<(unsigned)((L->n_entries + 255) / 256), 256, 0, st>>>(fa);
     KBC_TRY(cudaGetLastError());
   }
-  if (a.faces || a.cmask) k_kbc_step<true><<<(unsigned)L->nb * 4, kThreads, 0, st>>>(a);
-  else k_kbc_step<false><<<(unsigned)L->nb * 4, kThreads, 0, st>>>(a);
+  const unsigned grid = (unsigned)L->nb * 4;
+  a.warm_gate = KBC_FAST_WARM_GATE;
+  if (L->exact_math) {
+    if (a.faces || a.cmask) k_kbc_step<true, false><<<grid, kThreads, 0, st>>>(a);
+    else k_kbc_step<false, false><<<grid, kThreads, 0, st>>>(a);
+  } else {
+    if (a.faces || a.cmask) k_kbc_step<true, true><<<grid, kThreads, 0, st>>>(a);
+    else k_kbc_step<false, true><<<grid, kThreads, 0, st>>>(a);
+  }
   KBC_TRY(cudaGetLastError());
   L->parity ^= 1;
   return OAL_OK;
@@ -1124,6 +1183,12 @@ oal_status kbc_create(int device, const KbcGeometry& G, KbcLevel** out) {
              (int64_t)entries.size() * 8;
   *out = L;
   return OAL_OK;
+}
+
+void kbc_set_exact_math(KbcLevel* L, bool exact) {
+  if (!L || L->exact_math == exact) return;
+  L->exact_math = exact;
+  release_graph(L);  // a captured graph holds the other kernel
 }
 
 void kbc_destroy(KbcLevel* L) {

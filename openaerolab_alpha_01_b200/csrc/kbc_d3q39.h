@@ -22,6 +22,9 @@ struct KbcGeometry {
   bool has_solid = false;
 };
 oal_status kbc_create(int device, const KbcGeometry& G, KbcLevel** out);
+// exp and log of the step: exact = the software routines shared with the CPU restatement
+// (bit-identical to it), otherwise CUDA's expf / logf
+void kbc_set_exact_math(KbcLevel* L, bool exact);
 void kbc_destroy(KbcLevel* L);
 oal_status kbc_init_equilibrium(KbcLevel* L, const double* rho_host, const double* vel_host);
 oal_status kbc_set_state(KbcLevel* L, const double* f_host, const double* rho_host, const double* vel_host);

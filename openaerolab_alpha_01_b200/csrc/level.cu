@@ -11,9 +11,11 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "cumulant_math.cuh"
 #include "../../include/oal.h"
 #include "bouzidi_d3q27.h"
 #include "kbc_d3q39.h"
+#include "surface_d3q27.h"
 
 namespace oal {
 template <class S, class R>
@@ -210,6 +212,28 @@ __global__ void k_from_double(const double* __restrict__ src, int64_t n, R* __re
   if (i < n) dst[i] = R(src[i]);
 }
 
+// Non-equilibrium stress of the stored state (compute_pi_neq_kernel!, kernel_pi_neq.jl:39-180):
+// one thread per cell, f decoded from the current buffer, rho and u from the level's macros.
+template <class S, class R, class O>
+__global__ void k_pi_neq(const S* __restrict__ f, PopIndex pi, const R* __restrict__ rho, const R* __restrict__ vel,
+                         const uint32_t* __restrict__ bflags, const int32_t* __restrict__ mslot,
+                         const uint32_t* __restrict__ cmask, int64_t ncell, int comp, O* __restrict__ out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= ncell) return;
+  const int64_t b = i >> 9;
+  const int cell = (int)(i & 511);
+  const bool obs = (bflags[b] & BF_NEAR_SOLID) && ((cmask[(int64_t)mslot[b] * kCells + cell] >> 13) & 1u);
+  const R r = rho[i], ux = vel[i], uy = vel[i + ncell], uz = vel[i + 2 * ncell];
+  const bool skip = obs || !isfinite(r) || r < R(0.01) || r > R(10) || !isfinite(ux) || !isfinite(uy) || !isfinite(uz);
+  R fk[kQ27];
+#pragma unroll
+  for (int k = 0; k < kQ27; ++k) fk[k] = Codec<S>::dec(f[pi(b, cell, k)], R(q27_w(k)), R(1.0 / q27_w(k)));
+  R p[6];
+  pi_neq_of<R>(fk, r, ux, uy, uz, comp != 0, skip, p);
+#pragma unroll
+  for (int m = 0; m < 6; ++m) out[i + m * ncell] = O(p[m]);
+}
+
 inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 size_t storage_bytes(int32_t storage) {
@@ -249,6 +273,8 @@ struct oal_geometry {
     int64_t n_copy;
     uint2* rest;   // entries for the general fill kernel
     int64_t n_rest;
+    std::vector<uint2> h_copies;  // host: the raw copies alone (dst, src) (batches rebase them)
+    std::vector<uint2> h_other;   // host: every other entry as a fill entry (block, cell | k << 9)
   };
   std::vector<FillLists> fills;
   int4* d_binfo = nullptr;
@@ -326,7 +352,18 @@ struct oal_level {
   KbcLevel* kbc = nullptr;  // D3Q39 entropic levels: the whole state lives here
   ParentView par{};         // refined level of a block-AMR hierarchy: its parent (set per step)
   BouzidiSet bz;            // linear Bouzidi boundary cells (oal_level_set_bouzidi)
+  // surface-stress mapping (oal_level_set_surface): triangles, block pointer, outputs
+  float* s_tri = nullptr;
+  int32_t s_n = 0;
+  int32_t* s_ptr = nullptr;
+  float* s_out = nullptr;
+  double* s_part = nullptr;
+  double* s_sum = nullptr;
   uint32_t bz_gen = 0;      // bumped by every oal_level_set_bouzidi (hierarchy graphs compare it)
+  // variable nu_sgs from Pi_neq: the post-collision non-equilibrium stress of the previous step,
+  // 6 components x n_blocks x 512 in the compute type, refreshed in place by the general kernel
+  void* pi_neq = nullptr;
+  bool comp = false;        // the last step's compressible equilibrium (oal_level_pi_neq)
 };
 
 // ------------------------------------------------------------------------------------------------
@@ -344,6 +381,11 @@ static oal_status resolve_params(const oal_step_params* p, const oal_geometry* g
   if (p->solid_bc != OAL_SOLID_FULLWAY && p->solid_bc != OAL_SOLID_HALFWAY && p->solid_bc != OAL_SOLID_GRAD &&
       p->solid_bc != OAL_SOLID_BOUZIDI)
     return set_error(OAL_E_INVALID_ARG, "solid_bc %d", p->solid_bc);
+  if (p->variable_nu_sgs < 0 || p->variable_nu_sgs > 2)
+    return set_error(OAL_E_INVALID_ARG, "variable_nu_sgs %d (0 off, 1 Pi_neq, 2 dynamic)", p->variable_nu_sgs);
+  if (p->solid_bc == OAL_SOLID_BOUZIDI && p->collect_forces)
+    return set_error(OAL_E_UNSUPPORTED, "collect_forces with OAL_SOLID_BOUZIDI: the momentum exchange would be the full-way "
+                                        "wall's, computed before the Bouzidi correction; use the surface-stress forces");
   std::memset(cp, 0, sizeof *cp);
   cp->tau = p->tau;
   cp->c_wale = p->c_wale;
@@ -379,6 +421,10 @@ static oal_status resolve_params(const oal_step_params* p, const oal_geometry* g
   if (p->c_wale != 0.0f) f |= CF_GRADIENTS;
   if (p->inlet_turbulence > 0.0f) f |= CF_INLET_NOISE;
   if (p->omega_bulk != 1.0f || p->omega3 != 1.0f || p->omega4 != 1.0f) f |= CF_GENERAL_RATES;
+  if (p->variable_nu_sgs == 1) f |= CF_SGS_PI;
+  if (p->variable_nu_sgs == 2) f |= CF_SGS_DYNAMIC | CF_GRADIENTS;
+  cp->c_pi = p->c_pi;
+  cp->nu_sgs_floor = p->nu_sgs_floor;
   cp->flags = f;
   return OAL_OK;
 }
@@ -399,7 +445,7 @@ static oal_status build_fill_lists(oal_geometry* g, uint32_t flags) {
     if (c.key == key) return OAL_OK;
   const int64_t bst = 27 * kCells, kst = kCells;
   if ((int64_t)(g->nb + g->n_ghost) * bst >= (1ll << 31)) return OAL_OK;  // element index must fit 31 bits
-  std::vector<uint2> copy, rest;
+  std::vector<uint2> copy, rest, copies, other;
   copy.reserve(g->h_gentries.size());
   const int nx = g->nx, ny = g->ny, nz = g->nz;
   for (const uint2& en : g->h_gentries) {
@@ -448,13 +494,17 @@ static oal_status build_fill_lists(oal_geometry* g, uint32_t flags) {
       code = 0xC0000000u | (uint32_t)k;
       constant = true;
     }
-    if (general) { rest.push_back(en); continue; }
+    if (general) { rest.push_back(en); other.push_back(en); continue; }
     if (!constant) code = (uint32_t)(src >= 0 ? src : b * bst + j * kst + cell);
     copy.push_back(make_uint2(dst, code));
+    if (constant) other.push_back(en);
+    else copies.push_back(make_uint2(dst, code));
   }
   // consecutive threads write consecutive slots
   std::sort(copy.begin(), copy.end(), [](const uint2& p, const uint2& q) { return p.x < q.x; });
-  oal_geometry::FillLists fl{key, nullptr, (int64_t)copy.size(), nullptr, (int64_t)rest.size()};
+  std::sort(copies.begin(), copies.end(), [](const uint2& p, const uint2& q) { return p.x < q.x; });
+  oal_geometry::FillLists fl{key, nullptr, (int64_t)copy.size(), nullptr, (int64_t)rest.size(), std::move(copies),
+                             std::move(other)};
   cudaError_t e = cudaSuccess;
   if (!copy.empty()) {
     e = cudaMalloc(&fl.copy, copy.size() * sizeof(uint2));
@@ -468,7 +518,7 @@ static oal_status build_fill_lists(oal_geometry* g, uint32_t flags) {
     cudaFree(fl.copy); cudaFree(fl.rest);
     OAL_CUDA_TRY(e);
   }
-  g->fills.push_back(fl);
+  g->fills.push_back(std::move(fl));
   return OAL_OK;
 }
 
@@ -480,6 +530,19 @@ static oal_status prepare_fill(oal_level* L, const CaseParams& cp, cudaStream_t 
   OAL_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
   if (cs != cudaStreamCaptureStatusNone) return OAL_OK;
   return build_fill_lists(const_cast<oal_geometry*>(L->g), cp.flags);
+}
+
+// The Pi_neq field of variable nu_sgs mode 1, zero at first use (allocated outside a capture).
+static oal_status prepare_sgs(oal_level* L, const CaseParams& cp, cudaStream_t st) {
+  if (!(cp.flags & CF_SGS_PI) || L->pi_neq) return OAL_OK;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  OAL_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return set_error(OAL_E_UNSUPPORTED, "variable_nu_sgs 1: first step inside a stream capture");
+  const size_t bytes = (size_t)L->g->nb * 512 * 6 * macro_bytes(L->storage);
+  OAL_CUDA_TRY(cudaMalloc(&L->pi_neq, bytes));
+  OAL_CUDA_TRY(cudaMemset(L->pi_neq, 0, bytes));
+  L->bytes += (int64_t)bytes;
+  return OAL_OK;
 }
 
 // Which kernels one step launches.
@@ -511,6 +574,11 @@ static cudaError_t launch_step_t(const oal_geometry* g, const StepArgs& a0, Step
     if ((r = launch_fill_copy<S, R>(a, fl->copy, fl->n_copy, s)) != cudaSuccess) return r;
     return launch_fill_ghosts<S, R>(a, fl->rest, fl->n_rest, s);
   };
+  if (a.flags_any & (CF_SGS_PI | CF_SGS_DYNAMIC)) {
+    // variable nu_sgs: every block in the general kernel (per-cell test filter / Pi_neq refresh)
+    if ((e = fill(st)) != cudaSuccess) return e;
+    return launch_general<S, R>(a, nullptr, g->nb, st);
+  }
   // high-priority side stream: ghost fill, then the blocks that read ghost slots (general kernel,
   // boundary x-pair blocks); main stream: the interior x-pair blocks, which read none
   const int n_in = g->n_fast_in, n_bd = g->n_fast - g->n_fast_in;
@@ -613,6 +681,7 @@ static cudaError_t dense_step_t(oal_level* L, const StepArgs& a, cudaStream_t st
   const oal_geometry* g = L->g;
   cudaError_t e;
   if ((e = launch_fill_ghosts<S, R>(a, g->d_dense_gentries, g->n_dense_gentries, st)) != cudaSuccess) return e;
+  if (a.flags_any & (CF_SGS_PI | CF_SGS_DYNAMIC)) return launch_general<S, R>(a, nullptr, g->nb, st);
   const int n_fast = (int)(g->nb - g->n_general);
   if (g->n_general > 0) {
     if ((e = cudaEventRecord(L->ov.fork, st)) != cudaSuccess) return e;
@@ -623,6 +692,17 @@ static cudaError_t dense_step_t(oal_level* L, const StepArgs& a, cudaStream_t st
   if ((e = launch_dense_fast<S>(a, g->d_dense_fast, n_fast, L->dense_grid, st)) != cudaSuccess) return e;
   if (g->n_general > 0) return cudaStreamWaitEvent(st, L->ov.join, 0);
   return cudaSuccess;
+}
+
+// Pi_neq of the state in buffer `parity` into d_out (6 x n_blocks x 512, type O).
+template <class S, class R, class O>
+static cudaError_t pi_neq_t(oal_level* L, int parity, O* d_out, cudaStream_t st) {
+  const oal_geometry* g = L->g;
+  const int64_t ncell = (int64_t)g->nb * 512;
+  k_pi_neq<S, R, O><<<nblk(ncell, 128), 128, 0, st>>>(static_cast<const S*>(L->f[parity]), pop_index(L),
+                                                      static_cast<const R*>(L->rho), static_cast<const R*>(L->vel[parity]),
+                                                      g->d_bflags, g->d_mslot, g->d_cmask, ncell, L->comp ? 1 : 0, d_out);
+  return cudaGetLastError();
 }
 
 // Reads (and clears) the level's device error word after a synchronisation.
@@ -769,6 +849,9 @@ void oal_default_step_params(oal_step_params* p) {
   p->nu_sgs_lattice_floor = 0.0f; // :733
   p->shock_nu_max = 0.0f;
   p->grad_pineq_scale = 1.0f;     // config_loader.jl:898
+  p->variable_nu_sgs = 0;         // VARIABLE_NU_SGS, config_loader.jl:237
+  p->c_pi = 0.2f;                 // :238
+  p->nu_sgs_floor = 0.002f;       // :239
 }
 
 void oal_default_entropic_params(oal_step_params* p) {
@@ -1102,6 +1185,8 @@ oal_status oal_stream_collide(const oal_geometry* g, const oal_level_fields* fl,
   if (s != OAL_OK) return s;
   if (cp.flags & CF_BOUZIDI)
     return set_error(OAL_E_UNSUPPORTED, "OAL_SOLID_BOUZIDI: the boundary cells attach to plain levels, not to caller-owned arrays (oal_stream_collide)");
+  if (cp.flags & (CF_SGS_PI | CF_SGS_DYNAMIC))
+    return set_error(OAL_E_UNSUPPORTED, "variable_nu_sgs: the Pi_neq field and the test filter belong to plain levels, not to caller-owned arrays (oal_stream_collide)");
   if (!fl->f_in || !fl->f_out || !fl->rho_out || !fl->vel_out || !fl->vel_in)
     return set_error(OAL_E_INVALID_ARG, "f_in, f_out, rho_out, vel_out and vel_in are required");
   if (fl->f_in == fl->f_out) return set_error(OAL_E_INVALID_ARG, "f_in and f_out must differ (pull scheme)");
@@ -1130,7 +1215,7 @@ oal_status oal_stream_collide(const oal_geometry* g, const oal_level_fields* fl,
 // D3Q39 entropic level: FP32 populations on a geometry whose blocks all have their 26 neighbours,
 // with no solid cell, no sponge and no wall within 16 cells (the far-bulk branch of the macro
 // realizability clamp, kernel_entropic_d3q39.jl:2149-2156)
-static oal_status create_entropic_level(const oal_geometry* g, int32_t storage, oal_level** out) {
+static oal_status create_entropic_level(const oal_geometry* g, int32_t storage, uint32_t flags, oal_level** out) {
   if (storage != OAL_STORE_F32)
     return set_error(OAL_E_UNSUPPORTED, "the D3Q39 entropic level stores FP32 populations (storage %d)", storage);
   for (float v : g->h_sponge)
@@ -1148,6 +1233,7 @@ static oal_status create_entropic_level(const oal_geometry* g, int32_t storage, 
   KbcLevel* k = nullptr;
   oal_status s = kbc_create(g->device, G, &k);
   if (s != OAL_OK) return s;
+  kbc_set_exact_math(k, (flags & OAL_LEVEL_EXACT_MATH) != 0);
   auto* L = new oal_level();
   L->g = g; L->device = g->device; L->op = OAL_OP_ENTROPIC_D3Q39; L->storage = storage; L->kbc = k;
   ++const_cast<oal_geometry*>(g)->n_levels;
@@ -1162,7 +1248,7 @@ oal_status oal_level_create(const oal_geometry* g, int32_t op, int32_t storage, 
 oal_status oal_level_create_ex(const oal_geometry* g, int32_t op, int32_t storage, uint32_t flags, oal_level** out) {
   if (!g || !out) return set_error(OAL_E_INVALID_ARG, "null argument");
   *out = nullptr;
-  if (op == OAL_OP_ENTROPIC_D3Q39) return create_entropic_level(g, storage, out);
+  if (op == OAL_OP_ENTROPIC_D3Q39) return create_entropic_level(g, storage, flags, out);
   if (op != OAL_OP_CUMULANT_D3Q27) return set_error(OAL_E_UNSUPPORTED, "operator %d has no level state in this build", op);
   if (storage < OAL_STORE_F32 || storage > OAL_STORE_F64) return set_error(OAL_E_INVALID_ARG, "storage %d", storage);
   OAL_CUDA_TRY(cudaSetDevice(g->device));
@@ -1250,7 +1336,8 @@ void oal_level_destroy(oal_level* L) {
   bouzidi_free(&L->bz);
   for (int i = 0; i < 2; ++i) { cudaFree(L->f[i]); cudaFree(L->vel[i]); }
   cudaFree(L->rho); cudaFree(L->d_force_part); cudaFree(L->d_force); cudaFree(L->d_mm_part); cudaFree(L->d_mm);
-  cudaFree(L->d_ticket);
+  cudaFree(L->d_ticket); cudaFree(L->pi_neq);
+  cudaFree(L->s_tri); cudaFree(L->s_ptr); cudaFree(L->s_out); cudaFree(L->s_part); cudaFree(L->s_sum);
   if (L->cap) cudaStreamDestroy(L->cap);
   if (L->ov.side) cudaStreamDestroy(L->ov.side);
   if (L->ov.fork) cudaEventDestroy(L->ov.fork);
@@ -1282,6 +1369,7 @@ oal_status oal_level_init_equilibrium(oal_level* L, const double* rho, const dou
   }
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   cudaFree(d_rho); cudaFree(d_vel);
+  if (e == cudaSuccess && L->pi_neq) e = cudaMemset(L->pi_neq, 0, (size_t)ncell * 6 * macro_bytes(L->storage));
   if (e != cudaSuccess) return set_error(OAL_E_CUDA, "init_equilibrium: %s", cudaGetErrorString(e));
   L->parity = 0;
   L->forces_valid = false;
@@ -1366,6 +1454,8 @@ static oal_status enqueue_step(oal_level* L, const CaseParams& cp, cudaStream_t 
   a.p0 = cp;
   a.flags_any = cp.flags;
   a.round_nearest = L->round_nearest ? 1 : 0;
+  a.pi_neq = L->pi_neq;
+  if ((cp.flags & CF_SGS_PI) && !L->pi_neq) return set_error(OAL_E_UNSUPPORTED, "variable_nu_sgs 1 without its Pi_neq field");
   if (!L->dense) { a.force_out = L->d_force; a.force_ticket = L->d_ticket; }
   a.par = L->par;
   if (L->dense) {
@@ -1385,13 +1475,27 @@ static oal_status enqueue_step(oal_level* L, const CaseParams& cp, cudaStream_t 
   }
   if ((cp.flags & CF_BOUZIDI) && L->bz.n > 0)
     OAL_CUDA_TRY(bouzidi_enqueue(L->bz, L->storage, a.f_out, pop_index(L), g->d_nbr, g->d_mslot, g->d_cmask, st));
+  if ((cp.flags & CF_SGS_PI) && (cp.flags & CF_BOUZIDI) && L->bz.n > 0) {
+    // the Bouzidi correction rewrote populations after the fused refresh: refresh Pi_neq again
+    // from the corrected state (timestep.jl:1818-1834)
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (L->storage) {
+      case OAL_STORE_F32: e = pi_neq_t<float, float, float>(L, p ^ 1, static_cast<float*>(L->pi_neq), st); break;
+      case OAL_STORE_F16_DEV: e = pi_neq_t<__half, float, float>(L, p ^ 1, static_cast<float*>(L->pi_neq), st); break;
+      case OAL_STORE_BF16_DEV: e = pi_neq_t<__nv_bfloat16, float, float>(L, p ^ 1, static_cast<float*>(L->pi_neq), st); break;
+      case OAL_STORE_F64: e = pi_neq_t<double, double, double>(L, p ^ 1, static_cast<double*>(L->pi_neq), st); break;
+    }
+    OAL_CUDA_TRY(e);
+  }
   if (cp.flags & CF_COLLECT) {
     // the momentum exchange lives on the general kernel's CTAs (blocks near solids); in the
     // block layout the last of them sums the partials (a.force_out)
-    if (g->n_general > 0 && L->dense) {
-      k_reduce3<<<1, 256, 0, st>>>(L->d_force_part, (int64_t)g->n_general * 4, L->d_force);
+    const bool all_general = (cp.flags & (CF_SGS_PI | CF_SGS_DYNAMIC)) != 0;
+    const int64_t n_gen = all_general ? g->nb : g->n_general;
+    if (n_gen > 0 && L->dense) {
+      k_reduce3<<<1, 256, 0, st>>>(L->d_force_part, n_gen * 4, L->d_force);
       OAL_CUDA_TRY(cudaGetLastError());
-    } else if (g->n_general == 0) {
+    } else if (n_gen == 0) {
       OAL_CUDA_TRY(cudaMemsetAsync(L->d_force, 0, 3 * sizeof(double), st));
     }
     L->forces_valid = true;
@@ -1409,6 +1513,8 @@ oal_status oal_level_step(oal_level* L, const oal_step_params* p, void* stream) 
   if (cp.flags & CF_STORE_POST) return set_error(OAL_E_UNSUPPORTED, "store_post_collision needs caller-owned arrays (oal_stream_collide)");
   OAL_CUDA_TRY(cudaSetDevice(L->g->device));
   if ((s = prepare_fill(L, cp, static_cast<cudaStream_t>(stream))) != OAL_OK) return s;
+  if ((s = prepare_sgs(L, cp, static_cast<cudaStream_t>(stream))) != OAL_OK) return s;
+  L->comp = (cp.flags & CF_COMPRESSIBLE) != 0;
   return enqueue_step(L, cp, static_cast<cudaStream_t>(stream));
 }
 
@@ -1423,6 +1529,8 @@ oal_status oal_level_advance(oal_level* L, const oal_step_params* p, int32_t n, 
   OAL_CUDA_TRY(cudaSetDevice(L->g->device));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if ((s = prepare_fill(L, cp, st)) != OAL_OK) return s;
+  if ((s = prepare_sgs(L, cp, st)) != OAL_OK) return s;
+  L->comp = (cp.flags & CF_COMPRESSIBLE) != 0;
   oal_step_params key = *p;
   if (!(cp.flags & CF_INLET_NOISE)) key.time_step_seed = 0;  // the seed only matters with inlet noise
   const bool hit = L->gc.exec && L->gc.n == n && L->gc.parity == L->parity && std::memcmp(&L->gc.p, &key, sizeof key) == 0;
@@ -1495,6 +1603,79 @@ oal_status oal_level_set_bouzidi(oal_level* L, int32_t n_cells, const int32_t* c
   return OAL_OK;
 }
 
+void oal_default_surface_params(oal_surface_params* sp) {
+  if (!sp) return;
+  std::memset(sp, 0, sizeof *sp);
+  sp->abi_version = OAL_ABI_VERSION;
+  sp->search_radius = 8;      // map_surface_stresses! default (surface.jl:1335)
+  sp->recover_normal = 1;     // :1336
+  sp->tau = 0.6f;
+  sp->c_wale = 0.20f;         // C_SMAGO, config_loader.jl:82
+  sp->nu_sgs_background = 0.0f;
+  sp->pressure_scale = 1.0f;
+  sp->stress_scale = 1.0f;
+}
+
+oal_status oal_level_set_surface(oal_level* L, int32_t n_tri, const float* tri) {
+  if (!L) return set_error(OAL_E_INVALID_ARG, "null level");
+  if (L->kbc) return set_error(OAL_E_UNSUPPORTED, "the surface-stress mapping is a D3Q27 level path");
+  if (n_tri < 0 || (n_tri > 0 && !tri)) return set_error(OAL_E_INVALID_ARG, "n_tri %d", n_tri);
+  for (int64_t i = 0; i < (int64_t)n_tri * 7; ++i)
+    if (!std::isfinite(tri[i])) return set_error(OAL_E_INVALID_ARG, "triangle value %lld is not finite", (long long)i);
+  OAL_CUDA_TRY(cudaSetDevice(L->g->device));
+  OAL_CUDA_TRY(cudaDeviceSynchronize());
+  cudaFree(L->s_tri); cudaFree(L->s_out); cudaFree(L->s_part);
+  L->s_tri = nullptr; L->s_out = nullptr; L->s_part = nullptr; L->s_n = 0;
+  if (n_tri == 0) return OAL_OK;
+  const oal_geometry* g = L->g;
+  if (!L->s_ptr) {
+    // block pointer of the level's block grid (get_cell_at_position, surface.jl:271-307)
+    const int dx = g->nx / kBS, dy = g->ny / kBS, dz = g->nz / kBS;
+    std::vector<int32_t> ptr((size_t)dx * dy * dz, 0);
+    for (int32_t b = 0; b < g->nb; ++b) {
+      const int4 bi = g->h_binfo[(size_t)b];
+      if (bi.x < 1 || bi.y < 1 || bi.z < 1 || bi.x > dx || bi.y > dy || bi.z > dz)
+        return set_error(OAL_E_UNSUPPORTED, "block %d lies outside the level's %dx%dx%d block grid", b, dx, dy, dz);
+      ptr[(size_t)(bi.x - 1) + (size_t)dx * ((bi.y - 1) + (size_t)dy * (bi.z - 1))] = b + 1;
+    }
+    OAL_CUDA_TRY(cudaMalloc(&L->s_ptr, ptr.size() * sizeof(int32_t)));
+    OAL_CUDA_TRY(cudaMemcpy(L->s_ptr, ptr.data(), ptr.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    OAL_CUDA_TRY(cudaMalloc(&L->s_sum, 9 * sizeof(double)));
+  }
+  OAL_CUDA_TRY(cudaMalloc(&L->s_tri, (size_t)n_tri * 7 * sizeof(float)));
+  OAL_CUDA_TRY(cudaMemcpy(L->s_tri, tri, (size_t)n_tri * 7 * sizeof(float), cudaMemcpyHostToDevice));
+  OAL_CUDA_TRY(cudaMalloc(&L->s_out, (size_t)n_tri * 6 * sizeof(float)));
+  OAL_CUDA_TRY(cudaMalloc(&L->s_part, (size_t)n_tri * 9 * sizeof(double)));
+  L->s_n = n_tri;
+  return OAL_OK;
+}
+
+oal_status oal_level_surface_forces(oal_level* L, const oal_surface_params* sp, double out[9], float* per_tri) {
+  if (!L || !sp || !out) return set_error(OAL_E_INVALID_ARG, "null argument");
+  if (L->kbc) return set_error(OAL_E_UNSUPPORTED, "the surface-stress mapping is a D3Q27 level path");
+  if (sp->abi_version != OAL_ABI_VERSION) return set_error(OAL_E_ABI_MISMATCH, "oal_surface_params.abi_version %u", sp->abi_version);
+  if (sp->search_radius < 1 || sp->search_radius > 64) return set_error(OAL_E_INVALID_ARG, "search_radius %d (1..64)", sp->search_radius);
+  if (!(sp->tau > 0.5f)) return set_error(OAL_E_INVALID_ARG, "tau must exceed 1/2");
+  for (int c = 0; c < 9; ++c) out[c] = 0.0;
+  if (L->s_n == 0) return OAL_OK;
+  OAL_CUDA_TRY(cudaSetDevice(L->g->device));
+  const oal_geometry* g = L->g;
+  SurfArgs a{};
+  a.tri = L->s_tri; a.n = L->s_n;
+  a.rho = L->rho; a.vel = L->vel[L->parity]; a.vcs = (int64_t)g->nb * kCells;
+  a.ptr = L->s_ptr; a.dim_x = g->nx / kBS; a.dim_y = g->ny / kBS; a.dim_z = g->nz / kBS;
+  a.mslot = g->d_mslot; a.cmask = g->d_cmask;
+  a.radius = sp->search_radius; a.recover = sp->recover_normal ? 1 : 0;
+  a.tau = sp->tau; a.c_wale = sp->c_wale; a.nu_bg = sp->nu_sgs_background;
+  a.pscale = sp->pressure_scale; a.sscale = sp->stress_scale; a.cs2 = 1.0f / 3.0f;
+  a.mcx = sp->moment_center[0]; a.mcy = sp->moment_center[1]; a.mcz = sp->moment_center[2];
+  a.out = L->s_out; a.part = L->s_part;
+  OAL_CUDA_TRY(launch_surface(a, L->storage == OAL_STORE_F64, L->s_sum, nullptr));
+  OAL_CUDA_TRY(cudaMemcpy(out, L->s_sum, 9 * sizeof(double), cudaMemcpyDeviceToHost));
+  if (per_tri) OAL_CUDA_TRY(cudaMemcpy(per_tri, L->s_out, (size_t)L->s_n * 6 * sizeof(float), cudaMemcpyDeviceToHost));
+  return check_level_error(L);
+}
+
 oal_status oal_level_get_forces(oal_level* L, double out[3]) {
   if (!L || !out) return set_error(OAL_E_INVALID_ARG, "null argument");
   if (L->kbc) { out[0] = out[1] = out[2] = 0.0; return OAL_OK; }  // no solid cells
@@ -1526,6 +1707,26 @@ oal_status oal_level_mass_momentum(oal_level* L, double out[4]) {
   if (e != cudaSuccess) return set_error(OAL_E_CUDA, "mass_momentum: %s", cudaGetErrorString(e));
   OAL_CUDA_TRY(cudaMemcpy(out, L->d_mm, 4 * sizeof(double), cudaMemcpyDeviceToHost));
   return check_level_error(L);
+}
+
+oal_status oal_level_pi_neq(oal_level* L, float* out) {
+  if (!L || !out) return set_error(OAL_E_INVALID_ARG, "null argument");
+  if (L->kbc) return set_error(OAL_E_UNSUPPORTED, "oal_level_pi_neq: D3Q27 levels");
+  OAL_CUDA_TRY(cudaSetDevice(L->g->device));
+  const int64_t ncell = (int64_t)L->g->nb * 512;
+  float* d_out = nullptr;
+  OAL_CUDA_TRY(cudaMalloc(&d_out, (size_t)ncell * 6 * sizeof(float)));
+  cudaError_t e = cudaErrorInvalidValue;
+  switch (L->storage) {
+    case OAL_STORE_F32: e = pi_neq_t<float, float, float>(L, L->parity, d_out, 0); break;
+    case OAL_STORE_F16_DEV: e = pi_neq_t<__half, float, float>(L, L->parity, d_out, 0); break;
+    case OAL_STORE_BF16_DEV: e = pi_neq_t<__nv_bfloat16, float, float>(L, L->parity, d_out, 0); break;
+    case OAL_STORE_F64: e = pi_neq_t<double, double, float>(L, L->parity, d_out, 0); break;
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out, d_out, (size_t)ncell * 6 * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(d_out);
+  if (e != cudaSuccess) return set_error(OAL_E_CUDA, "pi_neq: %s", cudaGetErrorString(e));
+  return OAL_OK;
 }
 
 oal_status oal_level_device_state(oal_level* L, void** f, void** rho, void** vel) {
@@ -1958,6 +2159,8 @@ oal_status oal_amr_advance(oal_amr* A, const oal_step_params* params, int32_t n,
     oal_status s = resolve_params(&params[l], A->lv[(size_t)l].g, &cps[(size_t)l]);
     if (s != OAL_OK) return s;
     if (cps[(size_t)l].flags & CF_STORE_POST) return set_error(OAL_E_UNSUPPORTED, "store_post_collision needs caller-owned arrays");
+    if (cps[(size_t)l].flags & (CF_SGS_PI | CF_SGS_DYNAMIC))
+      return set_error(OAL_E_UNSUPPORTED, "variable_nu_sgs: plain levels only, not the levels of a block-AMR hierarchy");
   }
   OAL_CUDA_TRY(cudaSetDevice(A->device));
   const int start = A->lv[0].L->parity;
@@ -2122,6 +2325,7 @@ struct oal_batch {
   uint32_t flags_any = 0;          // OR of the active members' case flags
   // work lists, rebuilt when membership changes
   uint2* d_gentries = nullptr; int64_t n_gentries = 0, cap_gentries = 0;
+  uint2* d_fcopy = nullptr; int64_t n_fcopy = 0;  // raw ghost copies of the members (pool elements)
   int32_t* d_fast = nullptr; int64_t n_fast = 0;
   int32_t* d_fast_rec = nullptr;  // x-pair kernel records of d_fast
   int64_t n_fast_in = 0;          // the first n_fast_in fast blocks read no ghost slot
@@ -2152,13 +2356,31 @@ static void batch_release_graph(oal_batch* B) {
 static oal_status batch_rebuild(oal_batch* B) {
   std::vector<uint2> ge;
   std::vector<int32_t> fast, fast_bd, general, seg(1, 0);
+  std::vector<uint2> fcopy;
+  const int64_t pool_elems = (B->R + B->G) * 27 * kCells;
   std::vector<CaseParams> cases((size_t)B->max_members);
   uint32_t flags_any = 0;
   for (int32_t m = 0; m < B->max_members; ++m) {
     const BatchMember& M = B->mem[(size_t)m];
     if (M.active) {
       const oal_geometry* g = M.g;
-      for (const uint2& e : g->h_gentries) ge.push_back(make_uint2((uint32_t)(M.rb + e.x), e.y));
+      // the member's raw ghost copies, rebased into the pool (as a single level of the same
+      // geometry copies them); its other fill entries stay with the general fill
+      const oal_geometry::FillLists* fl = nullptr;
+      if (build_fill_lists(const_cast<oal_geometry*>(g), M.cp.flags) == OAL_OK && pool_elems < (1ll << 31))
+        for (const auto& c : g->fills)
+          if (c.key == fill_key_of(M.cp.flags)) fl = &c;
+      if (fl) {
+        const int64_t bst = 27 * kCells;
+        for (const uint2& c : fl->h_copies) {
+          const int64_t db = c.x / bst, sb = c.y / bst;
+          const int64_t dpool = B->R + M.gb + (db - g->nb), spool = M.rb + sb;
+          fcopy.push_back(make_uint2((uint32_t)(dpool * bst + c.x % bst), (uint32_t)(spool * bst + c.y % bst)));
+        }
+        for (const uint2& e : fl->h_other) ge.push_back(make_uint2((uint32_t)(M.rb + e.x), e.y));
+      } else {
+        for (const uint2& e : g->h_gentries) ge.push_back(make_uint2((uint32_t)(M.rb + e.x), e.y));
+      }
       for (int32_t i = 0; i < g->n_fast_in; ++i) fast.push_back((int32_t)(M.rb + g->h_fast[(size_t)i]));
       for (size_t i = (size_t)g->n_fast_in; i < g->h_fast.size(); ++i) fast_bd.push_back((int32_t)(M.rb + g->h_fast[i]));
       for (int32_t b : g->h_general) general.push_back((int32_t)(M.rb + b));
@@ -2176,6 +2398,8 @@ static oal_status batch_rebuild(oal_batch* B) {
     return e;
   };
   OAL_CUDA_TRY(upload(B->d_gentries, ge, B->n_gentries));
+  std::sort(fcopy.begin(), fcopy.end(), [](const uint2& p, const uint2& q) { return p.x < q.x; });
+  OAL_CUDA_TRY(upload(B->d_fcopy, fcopy, B->n_fcopy));
   B->n_fast_in = (int64_t)fast.size();
   fast.insert(fast.end(), fast_bd.begin(), fast_bd.end());
   OAL_CUDA_TRY(upload(B->d_fast, fast, B->n_fast));
@@ -2205,6 +2429,7 @@ static cudaError_t batch_step_t(oal_batch* B, const StepArgs& a, cudaStream_t st
   if (fork) {
     if ((e = cudaEventRecord(B->ov.fork, st)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(B->ov.side, B->ov.fork, 0)) != cudaSuccess) return e;
+    if ((e = launch_fill_copy<S, R>(a, B->d_fcopy, B->n_fcopy, B->ov.side)) != cudaSuccess) return e;
     if ((e = launch_fill_ghosts<S, R>(a, B->d_gentries, B->n_gentries, B->ov.side)) != cudaSuccess) return e;
     if ((e = launch_general<S, R>(a, B->d_general, (int)B->n_general, B->ov.side)) != cudaSuccess) return e;
     if ((e = launch_fast_range<S, R>(a, B->d_fast, n_in, n_bd, B->ov.side)) != cudaSuccess) return e;
@@ -2212,6 +2437,7 @@ static cudaError_t batch_step_t(oal_batch* B, const StepArgs& a, cudaStream_t st
     if ((e = launch_fast_range<S, R>(a, B->d_fast, 0, n_in, st)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(st, B->ov.join, 0)) != cudaSuccess) return e;
   } else {
+    if ((e = launch_fill_copy<S, R>(a, B->d_fcopy, B->n_fcopy, st)) != cudaSuccess) return e;
     if ((e = launch_fill_ghosts<S, R>(a, B->d_gentries, B->n_gentries, st)) != cudaSuccess) return e;
     if ((e = launch_fast<S, R>(a, B->d_fast, (int)B->n_fast, st)) != cudaSuccess) return e;
     if ((e = launch_general<S, R>(a, B->d_general, (int)B->n_general, st)) != cudaSuccess) return e;
@@ -2303,7 +2529,7 @@ void oal_batch_destroy(oal_batch* B) {
   cudaFree(B->rho); cudaFree(B->d_nbr); cudaFree(B->d_binfo); cudaFree(B->d_bflags); cudaFree(B->d_mslot);
   cudaFree(B->d_cmask); cudaFree(B->d_sponge); cudaFree(B->d_wdist); cudaFree(B->d_cases);
   cudaFree(B->d_gentries); cudaFree(B->d_fast); cudaFree(B->d_general); cudaFree(B->d_seg);
-  cudaFree(B->d_fast_rec);
+  cudaFree(B->d_fast_rec); cudaFree(B->d_fcopy);
   cudaFree(B->d_part); cudaFree(B->d_forces); cudaFree(B->d_mm_part); cudaFree(B->d_mm);
   if (B->cap) cudaStreamDestroy(B->cap);
   if (B->ov.side) cudaStreamDestroy(B->ov.side);
@@ -2381,6 +2607,8 @@ oal_status oal_batch_add(oal_batch* B, const oal_geometry* g, const oal_step_par
   if (s != OAL_OK) return s;
   if (cp.flags & CF_BOUZIDI)
     return set_error(OAL_E_UNSUPPORTED, "OAL_SOLID_BOUZIDI: the boundary cells attach to plain levels, not to batched cases (oal_batch_*)");
+  if (cp.flags & (CF_SGS_PI | CF_SGS_DYNAMIC))
+    return set_error(OAL_E_UNSUPPORTED, "variable_nu_sgs: plain levels only, not batched cases (oal_batch_*)");
   if (cp.flags & CF_STORE_POST) return set_error(OAL_E_UNSUPPORTED, "store_post_collision needs caller-owned arrays");
   int32_t m = -1;
   for (int32_t i = 0; i < B->max_members; ++i)
@@ -2476,6 +2704,8 @@ oal_status oal_batch_set_params(oal_batch* B, int32_t m, const oal_step_params* 
   if (s != OAL_OK) return s;
   if (cp.flags & CF_BOUZIDI)
     return set_error(OAL_E_UNSUPPORTED, "OAL_SOLID_BOUZIDI: the boundary cells attach to plain levels, not to batched cases (oal_batch_*)");
+  if (cp.flags & (CF_SGS_PI | CF_SGS_DYNAMIC))
+    return set_error(OAL_E_UNSUPPORTED, "variable_nu_sgs: plain levels only, not batched cases (oal_batch_*)");
   B->mem[(size_t)m].p = *p; B->mem[(size_t)m].cp = cp;
   B->dirty = true;
   return OAL_OK;

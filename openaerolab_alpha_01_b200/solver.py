@@ -67,6 +67,21 @@ def default_step_params(**overrides) -> capi.StepParams:
     return capi.default_params(**overrides)
 
 
+def default_surface_params(**overrides) -> capi.SurfaceParams:
+    """The surface-stress mapping's defaults (src/forces/surface.jl:1333-1336, config c_wale)."""
+    p = capi.SurfaceParams()
+    lib().oal_default_surface_params(C.byref(p))
+    for k, v in overrides.items():
+        if not hasattr(p, k):
+            raise AttributeError(k)
+        if k == "moment_center":
+            for i in range(3):
+                p.moment_center[i] = float(v[i])
+        else:
+            setattr(p, k, v)
+    return p
+
+
 def default_entropic_params(**overrides) -> capi.StepParams:
     """Defaults of the D3Q39 entropic operator: ``lambda_param`` is the h-damping sigma
     (ENTROPIC_SIGMA, 0) and ``adaptive_omega4`` the alpha solver (0 bisection, 1 Newton,
@@ -192,11 +207,12 @@ class Level:
     """Library-owned state of one level: ping-pong populations, density, velocity."""
 
     def __init__(self, geom: Geometry, operator: str = "cumulant", storage: str = "f32", layout: str = "block",
-                 rounding: str = "stochastic"):
+                 rounding: str = "stochastic", math: str = "fast"):
         """layout "block": block-major populations with ghost blocks (default); "dense": the
         padded grid with shared-memory-staged streaming (box levels in FP32/FP16/BF16).
         rounding (FP16/BF16 deviation storage): "stochastic" (default, unbiased in expectation) or
-        "nearest"."""
+        "nearest". math (D3Q39 entropic levels): "fast" (CUDA's expf / logf, default) or "exact"
+        (the software exp / log shared with the CPU oracle: bit-identical to it)."""
         self.geom = geom
         self.storage = capi.STORAGE_NAMES[storage]
         self.operator = get_collision_kernel(operator)
@@ -205,6 +221,10 @@ class Level:
         flags = capi.OAL_LEVEL_DENSE if layout == "dense" else 0
         if rounding == "nearest":
             flags |= capi.OAL_LEVEL_ROUND_NEAREST
+        if math not in ("fast", "exact"):
+            raise ValueError("math must be 'fast' or 'exact'")
+        if math == "exact":
+            flags |= capi.OAL_LEVEL_EXACT_MATH
         h = C.c_void_p()
         check(lib().oal_level_create_ex(geom.handle, self.operator, self.storage, flags, C.byref(h)))
         self.handle = h
@@ -273,6 +293,33 @@ class Level:
         check(lib().oal_level_get_forces(self.handle, out))
         return np.array(out[:])
 
+    def set_surface(self, tri: Optional[np.ndarray]) -> None:
+        """Attach triangles for the surface-stress mapping: rows (centroid x, y, z, unit outward
+        normal x, y, z, area) in cell units; None or an empty array detaches."""
+        if tri is None or len(tri) == 0:
+            check(lib().oal_level_set_surface(self.handle, 0, None))
+            self._surface_n = 0
+            return
+        t = np.ascontiguousarray(tri, dtype=np.float32).reshape(-1, 7)
+        check(lib().oal_level_set_surface(self.handle, int(t.shape[0]), t.ctypes.data_as(_f32p)))
+        self._surface_n = int(t.shape[0])
+
+    def surface_forces(self, params: Optional[capi.SurfaceParams] = None, per_triangle: bool = False):
+        """compute_aerodynamics! on the attached triangles: {"pressure", "viscous", "moment"} (FP64),
+        and with per_triangle the (n, 6) map (pressure, shear x y z, normal sign, wall distance)."""
+        if params is None:
+            params = default_surface_params()
+        out = (C.c_double * 9)()
+        n = getattr(self, "_surface_n", 0)
+        per = np.zeros((n, 6), np.float32) if per_triangle else None
+        check(lib().oal_level_surface_forces(self.handle, C.byref(params), out,
+                                             None if per is None else per.ctypes.data_as(_f32p)))
+        v = np.array(out[:])
+        res = {"pressure": v[0:3], "viscous": v[3:6], "moment": v[6:9], "total": v[0:3] + v[3:6]}
+        if per_triangle:
+            res["per_triangle"] = per
+        return res
+
     def forces_async(self, host_buf_ptr: int, stream=None) -> None:
         check(lib().oal_level_get_forces_async(self.handle, host_buf_ptr, _stream_handle(stream)))
 
@@ -280,6 +327,13 @@ class Level:
         out = (C.c_double * 4)()
         check(lib().oal_level_mass_momentum(self.handle, out))
         return np.array(out[:])
+
+    def pi_neq(self) -> np.ndarray:
+        """Non-equilibrium stress of the current state (compute_pi_neq_kernel!,
+        kernel_pi_neq.jl:39-180): float32 (6, n_blocks, 512), xx yy zz xy xz yz, 0 in solid cells."""
+        out = np.zeros((6, self.n_blocks, 512), np.float32)
+        check(lib().oal_level_pi_neq(self.handle, out.ctypes.data))
+        return out
 
     def layout(self) -> dict:
         out = (C.c_int64 * 6)()

@@ -141,13 +141,15 @@ def config4(steps: int = 2000, n_cases: int = 64, seed: int = 4, storage: str = 
 KBC_BYTES_PER_CELL = 2 * 39 * 4 + 2 * 13 * 4
 
 
-def benchmark_entropic(n: int = 128, steps: int = 50, warmup: int = 5, u0: float = 0.1, re: float = 1000.0) -> dict:
+def benchmark_entropic(n: int = 128, steps: int = 50, warmup: int = 5, u0: float = 0.1, re: float = 1000.0,
+                       math: str = "fast") -> dict:
     """Time `steps` D3Q39 entropic KBC steps of an n^3 periodic Taylor-Green box (one CUDA graph,
-    CUDA events on the launching stream)."""
+    CUDA events on the launching stream). math "fast": CUDA's expf / logf; "exact": the software
+    exp / log shared with the oracle."""
     import torch
     case = entropic_taylor_green_case(n, u0=u0, re=re)
     geom = Geometry(case.dom)
-    lvl = Level(geom, "entropic")
+    lvl = Level(geom, "entropic", math=math)
     lvl.init_equilibrium(case.rho, case.vel)
     s = torch.cuda.Stream()
     lvl.advance(case.params, warmup, s)
@@ -162,7 +164,7 @@ def benchmark_entropic(n: int = 128, steps: int = 50, warmup: int = 5, u0: float
     ms = e0.elapsed_time(e1) / steps
     m1 = lvl.mass_momentum()
     cells = n ** 3
-    out = {"workload": f"kbc_d3q39_taylor_green_{n}^3_f32_bisection_wale", "cells": cells, "steps": steps,
+    out = {"workload": f"kbc_d3q39_taylor_green_{n}^3_f32_bisection_wale_{math}_math", "cells": cells, "steps": steps,
            "ms_per_step": round(ms, 4), "mlups": round(cells / ms / 1e3, 1), "bytes_per_cell": KBC_BYTES_PER_CELL,
            "achieved_gbs": round(cells * KBC_BYTES_PER_CELL / ms / 1e6, 1),
            "mass_drift_rel": float(abs(m1[0] - m0[0]) / m0[0]), "gpu_launches": steps}

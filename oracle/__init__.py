@@ -22,7 +22,7 @@ _lib = None
 
 
 def build(force: bool = False) -> Path:
-    deps = [HERE / "oal_oracle.cpp", HERE / "oal_oracle_q19.cpp", HERE / "oal_oracle_q39.cpp",
+    deps = [HERE / "oal_oracle.cpp", HERE / "oal_oracle_q19.cpp", HERE / "oal_oracle_q39.cpp", HERE / "oal_oracle_surface.cpp",
             HERE.parent / "include" / "oal.h", HERE.parent / "openaerolab_alpha_01_b200" / "csrc" / "kbc_math.h"]
     if force or not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < max(d.stat().st_mtime for d in deps):
         subprocess.run(["make", "-s", "-C", str(HERE), "-B" if force else "liboal_oracle.so"], check=True)
@@ -39,6 +39,7 @@ def lib() -> C.CDLL:
         i32 = C.c_int32
         L.ora_d3q27_tables.argtypes = [vp] * 7
         L.ora_default_step_params.argtypes = [vp]
+        L.ora_surface_map.argtypes = [i32, vp, vp, vp, C.c_int64, vp, vp, i32, i32, i32, i32, i32] + [C.c_float] * 6 + [vp, vp, vp]
         L.ora_build_box.argtypes = [i32, i32, i32, i32, vp, vp]
         L.ora_sphere.argtypes = [i32, vp, C.c_double, C.c_double, C.c_double, C.c_double, vp]
         L.ora_sphere.restype = C.c_int64
@@ -47,6 +48,10 @@ def lib() -> C.CDLL:
             getattr(L, n).argtypes = [i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
             getattr(L, n).restype = C.c_int
         L.ora_mass_momentum_f64.argtypes = [i32, vp, vp, vp]
+        for n in ("ora_step_d3q27_pi_f64", "ora_step_d3q27_pi_f32"):
+            getattr(L, n).argtypes = [i32, i32, i32, i32] + [vp] * 14
+            getattr(L, n).restype = C.c_int
+        L.ora_pi_neq_f64.argtypes = [i32, vp, vp, vp, vp, i32, vp]
         L.ora_q19_tables.argtypes = [vp] * 6
         L.ora_q19_periodic_box.argtypes = [i32, i32, i32, vp, vp]
         L.ora_q19_periodic_box.restype = C.c_int
@@ -157,6 +162,26 @@ def sphere_channel(nx=256, ny=128, nz=128, diameter=24.0, centre_x=64.0, u_inlet
     return OracleCase(coords, nbr, (nx, ny, nz), obst, rho, vel, p, dict(n_solid=n_solid, nu=nu))
 
 
+def surface_map(tri, rho, vel, obstacle, ptr, dims, radius=8, recover=1, tau=0.6, c_wale=0.2, nu_bg=0.0,
+                pscale=1.0, sscale=1.0, moment_center=(0.0, 0.0, 0.0)):
+    """Surface-stress mapping (src/forces/surface.jl:636-1331) on host fields in the reference
+    layout (rho (nb, 512), vel (3, nb, 512), obstacle (nb, 512)); ptr: 1-based block pointer over
+    the dims block grid, x fastest. Returns (per-triangle (n, 6) float32, per-triangle force and
+    moment (n, 9) float64)."""
+    tri = np.ascontiguousarray(tri, np.float32).reshape(-1, 7)
+    n = tri.shape[0]
+    rho = np.ascontiguousarray(rho, np.float32)
+    vel = np.ascontiguousarray(vel, np.float32)
+    obst = np.ascontiguousarray(obstacle if obstacle is not None else np.zeros(rho.shape, np.uint8), np.uint8)
+    ptr = np.ascontiguousarray(ptr, np.int32)
+    mc = np.ascontiguousarray(moment_center, np.float32)
+    out = np.zeros((n, 6), np.float32)
+    part = np.zeros((n, 9))
+    lib().ora_surface_map(n, _p(tri), _p(rho), _p(vel), int(rho.size), _p(obst), _p(ptr), *map(int, dims), int(radius),
+                          int(recover), tau, c_wale, nu_bg, pscale, sscale, 1.0 / 3.0, _p(mc), _p(out), _p(part))
+    return out, part
+
+
 def init_feq(rho, vel, compressible=0):
     nb = rho.shape[0]
     f = np.zeros((27, nb, 512))
@@ -183,19 +208,28 @@ class OracleLevel:
         self.rho = np.ones((nb, 512), self.dtype)
         self.vel = np.zeros((3, nb, 512), self.dtype)
         self.vel_new = np.zeros_like(self.vel)
+        self.pi_neq = np.zeros((6, nb, 512), self.dtype)
         self.force = np.zeros(3)
 
     def init_equilibrium(self, rho, vel, compressible=0):
         self.f[...] = init_feq(rho, vel, compressible).astype(self.dtype)
         self.rho[...] = rho
         self.vel[...] = vel
+        self.pi_neq[...] = 0
 
     def step(self, params):
-        fn = lib().ora_step_d3q27_f64 if self.dtype == np.float64 else lib().ora_step_d3q27_f32
         force = np.zeros(3)
-        rc = fn(self.nb, *self.shape, _p(self.coords), _p(self.nbr), _p(self.obstacle), _p(self.sponge),
-                _p(self.wall_dist), C.addressof(params), _p(self.f), _p(self.g), None, _p(self.rho),
-                _p(self.vel_new), _p(self.vel), _p(force))
+        if params.variable_nu_sgs:
+            # variable nu_sgs: Pi_neq carried from step to step (kernel_cumulant.jl:546-588)
+            fn = lib().ora_step_d3q27_pi_f64 if self.dtype == np.float64 else lib().ora_step_d3q27_pi_f32
+            rc = fn(self.nb, *self.shape, _p(self.coords), _p(self.nbr), _p(self.obstacle), _p(self.sponge),
+                    _p(self.wall_dist), C.addressof(params), _p(self.f), _p(self.g), None, _p(self.rho),
+                    _p(self.vel_new), _p(self.vel), _p(self.pi_neq), _p(force))
+        else:
+            fn = lib().ora_step_d3q27_f64 if self.dtype == np.float64 else lib().ora_step_d3q27_f32
+            rc = fn(self.nb, *self.shape, _p(self.coords), _p(self.nbr), _p(self.obstacle), _p(self.sponge),
+                    _p(self.wall_dist), C.addressof(params), _p(self.f), _p(self.g), None, _p(self.rho),
+                    _p(self.vel_new), _p(self.vel), _p(force))
         assert rc == 0
         self.f, self.g = self.g, self.f
         self.vel, self.vel_new = self.vel_new, self.vel
@@ -210,11 +244,17 @@ class OracleLevel:
         p = type(params).from_buffer_copy(params)
         p.store_post_collision = 1
         post = np.zeros_like(self.f)
-        fn = lib().ora_step_d3q27_f64 if self.dtype == np.float64 else lib().ora_step_d3q27_f32
         force = np.zeros(3)
-        rc = fn(self.nb, *self.shape, _p(self.coords), _p(self.nbr), _p(self.obstacle), _p(self.sponge),
-                _p(self.wall_dist), C.addressof(p), _p(self.f), _p(self.g), _p(post), _p(self.rho),
-                _p(self.vel_new), _p(self.vel), _p(force))
+        if p.variable_nu_sgs:
+            fn = lib().ora_step_d3q27_pi_f64 if self.dtype == np.float64 else lib().ora_step_d3q27_pi_f32
+            rc = fn(self.nb, *self.shape, _p(self.coords), _p(self.nbr), _p(self.obstacle), _p(self.sponge),
+                    _p(self.wall_dist), C.addressof(p), _p(self.f), _p(self.g), _p(post), _p(self.rho),
+                    _p(self.vel_new), _p(self.vel), _p(self.pi_neq), _p(force))
+        else:
+            fn = lib().ora_step_d3q27_f64 if self.dtype == np.float64 else lib().ora_step_d3q27_f32
+            rc = fn(self.nb, *self.shape, _p(self.coords), _p(self.nbr), _p(self.obstacle), _p(self.sponge),
+                    _p(self.wall_dist), C.addressof(p), _p(self.f), _p(self.g), _p(post), _p(self.rho),
+                    _p(self.vel_new), _p(self.vel), _p(force))
         assert rc == 0
         cells = np.ascontiguousarray(bz["cells"], np.int32)
         q = np.ascontiguousarray(np.asarray(bz["q"], np.float16).astype(np.float32))
@@ -225,7 +265,20 @@ class OracleLevel:
         assert rc == 0
         self.f, self.g = self.g, self.f
         self.vel, self.vel_new = self.vel_new, self.vel
+        if p.variable_nu_sgs == 1:
+            # the correction rewrote populations after the refresh: refresh again from the
+            # corrected state (timestep.jl:1818-1834)
+            self.pi_neq[...] = self.state_pi_neq(p.compressible_corr)
         return self
+
+    def state_pi_neq(self, compressible=0):
+        """Pi_neq of the stored state (compute_pi_neq_kernel!, kernel_pi_neq.jl:39-180): (6, nb, 512)
+        in the order xx, yy, zz, xy, xz, yz, zero in solid cells."""
+        out = np.zeros((6, self.nb, 512))
+        c = lambda a: np.ascontiguousarray(a, np.float64)
+        lib().ora_pi_neq_f64(self.nb, _p(self.obstacle), _p(c(self.f)), _p(c(self.rho)), _p(c(self.vel)),
+                             int(compressible), _p(out))
+        return out
 
     def mass_momentum(self):
         out = np.zeros(4)

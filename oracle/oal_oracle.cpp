@@ -147,6 +147,7 @@ struct Level {
   const float* sponge;
   const float* wall_dist;
   const void* parent = nullptr;  // Parent<T> of a refined level (null on level 1)
+  void* pi_neq = nullptr;        // T[6][512 * nb]: Pi_neq of variable nu_sgs mode 1 (read, then refreshed)
 };
 
 // The parent level seen from a refined level's kernel (perform_timestep_v2! arguments
@@ -420,6 +421,79 @@ void vel_nb_fluid(const Level& L, const T* vel_in, int x, int y, int z, int b, i
   ux = ux0; uy = uy0; uz = uz0;
 }
 
+// Neighbour velocity of the dynamic test filter (kernel_dynamic_sgs.jl:57-103): the previous
+// step's velocity of a fluid neighbour, else the given centre velocity (missing or solid).
+template <class T>
+void vel_nb_centre(const Level& L, const T* vel_in, int x, int y, int z, int b, int dx, int dy, int dz,
+                   T cx, T cy, T cz, T (&o)[3]) {
+  Arr<T> A{L.nb};
+  const int64_t cs = 512 * (int64_t)L.nb;
+  const int nx = x + dx, ny = y + dy, nz = z + dz;
+  int64_t i = -1;
+  if (nx >= 0 && nx < BS && ny >= 0 && ny < BS && nz >= 0 && nz < BS) {
+    i = A.s(nx, ny, nz, b);
+  } else {
+    const int ox = nx < 0 ? -1 : (nx >= BS ? 1 : 0);
+    const int oy = ny < 0 ? -1 : (ny >= BS ? 1 : 0);
+    const int oz = nz < 0 ? -1 : (nz >= BS ? 1 : 0);
+    const int nbi = L.nbr[b + (int64_t)L.nb * ((ox + 1) + (oy + 1) * 3 + (oz + 1) * 9)];
+    if (nbi > 0) i = A.s((nx + BS) % BS, (ny + BS) % BS, (nz + BS) % BS, nbi - 1);
+  }
+  if (i < 0 || (L.obstacle && L.obstacle[i])) { o[0] = cx; o[1] = cy; o[2] = cz; return; }
+  o[0] = vel_in[i]; o[1] = vel_in[i + cs]; o[2] = vel_in[i + 2 * cs];
+}
+
+// Germano-Lilly Cs^2 (compute_dynamic_cs2_inline, kernel_dynamic_sgs.jl:124-240), Dx = 1
+template <class T>
+T dynamic_cs2(const T (&c)[3], const T (&n)[6][3], T g11, T g22, T g33, T S12, T S13, T S23) {
+  const T inv7 = T(1) / T(7);
+  T ut[3], uu[6];
+  for (int a = 0; a < 3; ++a) {
+    T sum = c[a];
+    for (int j = 0; j < 6; ++j) sum += n[j][a];
+    ut[a] = inv7 * sum;
+  }
+  const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
+  for (int m = 0; m < 6; ++m) {
+    T sum = c[ia[m]] * c[ib[m]];
+    for (int j = 0; j < 6; ++j) sum += n[j][ia[m]] * n[j][ib[m]];
+    uu[m] = inv7 * sum;
+  }
+  const T Lxx = uu[0] - ut[0] * ut[0], Lyy = uu[1] - ut[1] * ut[1], Lzz = uu[2] - ut[2] * ut[2];
+  const T Lxy = uu[3] - ut[0] * ut[1], Lxz = uu[4] - ut[0] * ut[2], Lyz = uu[5] - ut[1] * ut[2];
+  const T Ltr = (Lxx + Lyy + Lzz) * (T(1) / T(3));
+  const T Lxx_d = Lxx - Ltr, Lyy_d = Lyy - Ltr, Lzz_d = Lzz - Ltr;
+  const T S_sq = T(2) * (g11 * g11 + g22 * g22 + g33 * g33) + T(4) * (S12 * S12 + S13 * S13 + S23 * S23);
+  const T S_mag = std::sqrt(std::max(S_sq, T(1e-30)));
+  const T M_coeff = T(2) * T(1) * T(1) * T(3.659306f) * S_mag;
+  const T Mxx = M_coeff * g11, Myy = M_coeff * g22, Mzz = M_coeff * g33;
+  const T Mxy = M_coeff * S12, Mxz = M_coeff * S13, Myz = M_coeff * S23;
+  const T Mtr = (Mxx + Myy + Mzz) * (T(1) / T(3));
+  const T Mxx_d = Mxx - Mtr, Myy_d = Myy - Mtr, Mzz_d = Mzz - Mtr;
+  const T LM = Lxx_d * Mxx_d + Lyy_d * Myy_d + Lzz_d * Mzz_d + T(2) * (Lxy * Mxy + Lxz * Mxz + Lyz * Myz);
+  const T MM = Mxx_d * Mxx_d + Myy_d * Myy_d + Mzz_d * Mzz_d + T(2) * (Mxy * Mxy + Mxz * Mxz + Myz * Myz);
+  const T cd = T(0.5) * LM / (MM + T(1e-20));
+  return std::min(std::max(cd, T(0)), T(0.25));
+}
+
+// Pi_neq_ab = sum_k c_a c_b (f_k - f_eq_k) (compute_pi_neq_kernel!, kernel_pi_neq.jl:61-180, D3Q27)
+template <class T>
+void pi_neq_cell(const T* fk, T rho, T ux, T uy, T uz, int comp, T (&pi)[6]) {
+  const bool skip = !std::isfinite(rho) || rho < T(0.01) || rho > T(10) || !std::isfinite(ux) ||
+                    !std::isfinite(uy) || !std::isfinite(uz);
+  const T rs = skip ? T(0) : rho, us = skip ? T(0) : ux, vs = skip ? T(0) : uy, ws = skip ? T(0) : uz;
+  T p[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+  for (int k = 0; k < Q; ++k) {
+    const T cx = T(TB.cx[k]), cy = T(TB.cy[k]), cz = T(TB.cz[k]);
+    const T fe = feq_auto<T>(rs, us, vs, ws, T(TB.w[k]), cx, cy, cz, comp);
+    const T fn = (skip ? T(0) : fk[k]) - fe;
+    p[0] += cx * cx * fn; p[1] += cy * cy * fn; p[2] += cz * cz * fn;
+    p[3] += cx * cy * fn; p[4] += cx * cz * fn; p[5] += cy * cz * fn;
+  }
+  const T mask = skip ? T(0) : T(1);
+  for (int m = 0; m < 6; ++m) pi[m] = p[m] * mask;
+}
+
 // Source cell of the pull x - c_k: block index (0-based, -1 = none) and local coordinates.
 inline int src_block(const Level& L, int b, int sx, int sy, int sz, int& lx, int& ly, int& lz) {
   if (sx >= 0 && sx < BS && sy >= 0 && sy < BS && sz >= 0 && sz < BS) { lx = sx; ly = sy; lz = sz; return b; }
@@ -448,10 +522,13 @@ void step_cell(const Level& L, const oal_step_params& P, const T* f_in, T* f_out
   const T u_inlet = T(P.u_inlet);
   const bool store_post = P.store_post_collision == 1 && f_post != nullptr;
 
+  T* pi_neq = P.variable_nu_sgs == 1 ? static_cast<T*>(L.pi_neq) : nullptr;
   if (halfway && is_obs) {
     // Half-way mode: a solid cell holds the rest equilibrium; no fluid cell reads it.
     vel_out[own] = T(0); vel_out[own + cs] = T(0); vel_out[own + 2 * cs] = T(0);
     rho_out[own] = T(1);
+    if (pi_neq)
+      for (int m = 0; m < 6; ++m) pi_neq[own + m * cs] = T(0);
     for (int k = 0; k < Q; ++k) {
       f_out[A.f(x, y, z, b, k)] = T(TB.w[k]);
       if (store_post) f_post[A.f(x, y, z, b, k)] = T(TB.w[k]);
@@ -563,6 +640,8 @@ void step_cell(const Level& L, const oal_step_params& P, const T* f_in, T* f_out
   if (is_obs) {
     vel_out[own] = T(0); vel_out[own + cs] = T(0); vel_out[own + 2 * cs] = T(0);
     rho_out[own] = T(1);
+    if (pi_neq)
+      for (int m = 0; m < 6; ++m) pi_neq[own + m * cs] = T(0);
     for (int k = 0; k < Q; ++k) {
       T fc = fs[TB.opp[k]];
       f_out[A.f(x, y, z, b, k)] = fc;
@@ -659,7 +738,36 @@ void step_cell(const Level& L, const oal_step_params& P, const T* f_in, T* f_out
     if (denom > T(1e-12)) nu_eddy = (T(P.c_wale) * T(P.c_wale)) * OP1_32 / denom;
   }
   nu_eddy = nu_eddy * T(P.amr_sgs_scale);
-  nu_eddy = std::max(nu_eddy, T(P.nu_sgs_background) * T(P.amr_sgs_scale));
+  if (P.variable_nu_sgs == 2) {
+    // Germano-Lilly dynamic coefficient (kernel_cumulant.jl:553-565)
+    const T c[3] = {ux, uy, uz};
+    T n[6][3];
+    vel_nb_centre(L, vel_in, x, y, z, b, 1, 0, 0, ux, uy, uz, n[0]);
+    vel_nb_centre(L, vel_in, x, y, z, b, -1, 0, 0, ux, uy, uz, n[1]);
+    vel_nb_centre(L, vel_in, x, y, z, b, 0, 1, 0, ux, uy, uz, n[2]);
+    vel_nb_centre(L, vel_in, x, y, z, b, 0, -1, 0, ux, uy, uz, n[3]);
+    vel_nb_centre(L, vel_in, x, y, z, b, 0, 0, 1, ux, uy, uz, n[4]);
+    vel_nb_centre(L, vel_in, x, y, z, b, 0, 0, -1, ux, uy, uz, n[5]);
+    const T c_d = dynamic_cs2<T>(c, n, g11, g22, g33, S12, S13, S23);
+    const T S_mag = std::sqrt(std::max(T(2) * (g11 * g11 + g22 * g22 + g33 * g33) +
+                                       T(4) * (S12 * S12 + S13 * S13 + S23 * S23), T(1e-30)));
+    const T stress = std::min(c_d * S_mag * T(P.amr_sgs_scale), T(0.1));
+    nu_eddy = std::max(std::max(nu_eddy, stress), T(P.nu_sgs_floor) * T(P.amr_sgs_scale));
+  } else if (P.variable_nu_sgs == 1) {
+    // nu_sgs from the previous step's post-collision Pi_neq (kernel_cumulant.jl:566-586)
+    const T* pn = static_cast<const T*>(L.pi_neq);
+    const T pxx = pn[own], pyy = pn[own + cs], pzz = pn[own + 2 * cs];
+    const T pxy = pn[own + 3 * cs], pxz = pn[own + 4 * cs], pyz = pn[own + 5 * cs];
+    const T mag = std::sqrt(pxx * pxx + pyy * pyy + pzz * pzz + T(2) * (pxy * pxy + pxz * pxz + pyz * pyz));
+    const T denom_tau = T(P.tau) - T(1);
+    const T tau_corr = std::fabs(denom_tau) < T(1e-3) ? T(1) : T(P.tau) / denom_tau;
+    const T pre = std::fabs(tau_corr) * mag;
+    const T rho_cell = (!std::isfinite(rho) || rho < T(0.01)) ? T(1) : rho;
+    const T stress = std::min(T(P.c_pi) * pre / (rho_cell * (T(1) / T(3)) + T(1e-10)) * T(P.amr_sgs_scale), T(0.1));
+    nu_eddy = std::max(std::max(nu_eddy, stress), T(P.nu_sgs_floor) * T(P.amr_sgs_scale));
+  } else {
+    nu_eddy = std::max(nu_eddy, T(P.nu_sgs_background) * T(P.amr_sgs_scale));
+  }
   const T nu_mol = (T(P.tau) - T(0.5)) / T(3);
   const T nu_eff = nu_mol + nu_eddy;
   const T tau_eff = T(0.5) + T(3) * nu_eff;
@@ -854,6 +962,13 @@ void step_cell(const Level& L, const oal_step_params& P, const T* f_in, T* f_out
   for (int k = 0; k < Q; ++k) {
     if (store_post) f_post[A.f(x, y, z, b, k)] = fcs[k];
     f_out[A.f(x, y, z, b, k)] = fcs[k];
+  }
+  if (pi_neq) {
+    // refresh_pi_neq! after the step (timestep.jl:1828, solver_control.jl:152): the stored
+    // populations against the stored macros
+    T pv[6];
+    pi_neq_cell<T>(fcs, rho_out[own], vel_out[own], vel_out[own + cs], vel_out[own + 2 * cs], comp, pv);
+    for (int m = 0; m < 6; ++m) pi_neq[own + m * cs] = pv[m];
   }
 }
 
@@ -1136,6 +1251,9 @@ void ora_default_step_params(oal_step_params* p) {
   p->temporal_weight = 1.0f;
   p->hrr_sigma = 1.0f;
   p->grad_pineq_scale = 1.0f;        // config_loader.jl:898
+  p->variable_nu_sgs = 0;            // VARIABLE_NU_SGS, config_loader.jl:237
+  p->c_pi = 0.2f;                    // :238
+  p->nu_sgs_floor = 0.002f;          // :239
 }
 
 // D3Q27 tables in the reference order (0-based indices for opp/mirrors).
@@ -1223,6 +1341,44 @@ int ora_step_d3q27_f32(int32_t nb, int32_t nx, int32_t ny, int32_t nz, const int
                        float* rho_out, float* vel_out, const float* vel_in, double* force_out) {
   Level L = make_level(nb, nx, ny, nz, coords, nbr, obstacle, sponge, wall_dist);
   return step_level<float>(L, *P, f_in, f_out, f_post, rho_out, vel_out, vel_in, force_out);
+}
+
+// The level step with variable nu_sgs: pi_neq (T[6][512 * nb], xx yy zz xy xz yz; mode 1) holds
+// the previous step's Pi_neq on entry and this step's on return; f_post may be null.
+int ora_step_d3q27_pi_f64(int32_t nb, int32_t nx, int32_t ny, int32_t nz, const int32_t* coords, const int32_t* nbr,
+                          const uint8_t* obstacle, const float* sponge, const float* wall_dist,
+                          const oal_step_params* P, const double* f_in, double* f_out, double* f_post, double* rho_out,
+                          double* vel_out, const double* vel_in, double* pi_neq, double* force_out) {
+  Level L = make_level(nb, nx, ny, nz, coords, nbr, obstacle, sponge, wall_dist);
+  L.pi_neq = pi_neq;
+  if (P->variable_nu_sgs == 1 && !pi_neq) return -1;
+  return step_level<double>(L, *P, f_in, f_out, f_post, rho_out, vel_out, vel_in, force_out);
+}
+
+int ora_step_d3q27_pi_f32(int32_t nb, int32_t nx, int32_t ny, int32_t nz, const int32_t* coords, const int32_t* nbr,
+                          const uint8_t* obstacle, const float* sponge, const float* wall_dist,
+                          const oal_step_params* P, const float* f_in, float* f_out, float* f_post, float* rho_out,
+                          float* vel_out, const float* vel_in, float* pi_neq, double* force_out) {
+  Level L = make_level(nb, nx, ny, nz, coords, nbr, obstacle, sponge, wall_dist);
+  L.pi_neq = pi_neq;
+  if (P->variable_nu_sgs == 1 && !pi_neq) return -1;
+  return step_level<float>(L, *P, f_in, f_out, f_post, rho_out, vel_out, vel_in, force_out);
+}
+
+// Pi_neq of a stored state (compute_pi_neq_kernel!, kernel_pi_neq.jl:39-180, D3Q27): out
+// double[6][512 * nb]; a solid cell enters with a non-finite density, which the unphysical-state
+// test zeroes.
+void ora_pi_neq_f64(int32_t nb, const uint8_t* obstacle, const double* f, const double* rho, const double* vel,
+                    int32_t comp, double* out) {
+  const int64_t n = 512 * (int64_t)nb;
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; ++i) {
+    double fk[Q], pv[6];
+    for (int k = 0; k < Q; ++k) fk[k] = f[i + n * k];
+    const bool obs = obstacle && obstacle[i];
+    pi_neq_cell<double>(fk, obs ? std::nan("") : rho[i], vel[i], vel[i + n], vel[i + 2 * n], comp, pv);
+    for (int m = 0; m < 6; ++m) out[i + m * n] = pv[m];
+  }
 }
 
 // A refined level's step: the level step with its pulls from outside its blocks interpolated from

@@ -195,6 +195,42 @@ def test_caller_owned_arrays_reference_layout(oal, oracle_lib):
     assert abs(force[0].item() - O.force[0]) / abs(O.force[0]) < 1e-4
 
 
+@pytest.mark.parametrize("solid_bc", [capi.OAL_SOLID_FULLWAY, capi.OAL_SOLID_HALFWAY])
+def test_store_post_collision_on_caller_arrays(oal, oracle_lib, solid_bc):
+    """kernel_cumulant.jl:889-908: with store_post_collision the post-collision populations are
+    also written to f_post_collision (every cell, solid ones included); the Bouzidi correction
+    reads them from there."""
+    import torch
+    case = sphere_channel_case(32, 16, 16, diameter=6.0, centre_x=10.0, u_inlet=0.05, re=100.0)
+    g = Geometry(case.dom)
+    nb = case.dom.n_blocks
+    p = capi.default_params(**{f: getattr(case.params, f) for f, _ in capi.StepParams._fields_ if f != "reserved"})
+    p.solid_bc = solid_bc
+    p.store_post_collision = 1
+    f0 = oracle_lib.init_feq(case.rho, case.vel)
+    fa = torch.tensor(f0, dtype=torch.float32, device="cuda").contiguous()
+    fb = torch.empty_like(fa)
+    post = torch.full_like(fa, float("nan"))
+    va = torch.tensor(case.vel, dtype=torch.float32, device="cuda").contiguous()
+    vb = torch.empty_like(va)
+    rho = torch.empty((nb, 512), dtype=torch.float32, device="cuda")
+    force = torch.zeros(3, dtype=torch.float64, device="cuda")
+    steps = 6
+    for i in range(steps):
+        fl = capi.LevelFields(fa.data_ptr(), fb.data_ptr(), post.data_ptr(), rho.data_ptr(), vb.data_ptr(),
+                              va.data_ptr(), capi.OAL_STORE_F32, 0, 512, 512 * nb, 512 * nb, force.data_ptr())
+        capi.check(capi.lib().oal_stream_collide(g.handle, C.byref(fl), C.byref(p), None))
+        fa, fb = fb, fa
+        va, vb = vb, va
+    torch.cuda.synchronize()
+    g.close()
+    got_post, got_f = post.cpu().numpy(), fa.cpu().numpy()
+    assert not np.isnan(got_post).any()
+    assert np.array_equal(got_post, got_f)
+    O = run_oracle(oracle_lib, case, steps, np.float32, params=p)
+    assert rel(got_post, O.f) < 2e-5
+
+
 def test_rejects_bad_params(oal):
     case = taylor_green_case(16)
     g = Geometry(case.dom)
@@ -287,6 +323,12 @@ def test_bouzidi_graph_detach_and_refusals(oal, channel):
     with pytest.raises(OALError):
         bat.add(g, p, channel.rho, channel.vel)
     bat.close()
+    # the momentum exchange belongs to the full-way wall, not to the corrected links: refused
+    pc = capi.default_params(**{f: getattr(p, f) for f, _ in capi.StepParams._fields_ if f != "reserved"})
+    pc.collect_forces = 1
+    with pytest.raises(OALError) as e:
+        A.perform_timestep(pc)
+    assert e.value.status == capi.OAL_E_UNSUPPORTED
     for X in (A, B, C_):
         X.close()
     g.close()

@@ -55,6 +55,32 @@ def test_noalloc_matches_level_reduction_twice(oal, storage):
     g.close()
 
 
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16", "f64"])
+def test_noalloc_on_the_level_buffer_in_its_stored_type(oal, storage):
+    """The level's own population buffer (block-major, stored type, the level's strides) handed
+    to the entry point: every storage branch of the reduction runs on the GPU."""
+    import torch
+    case = sphere_channel_case(32, 16, 16, diameter=6.0, centre_x=10.0, u_inlet=0.05, re=100.0)
+    g = Geometry(case.dom)
+    L = Level(g, storage=storage, layout="block")
+    L.init_equilibrium(case.rho, case.vel)
+    for _ in range(4):
+        L.perform_timestep(case.params)
+    lay = L.layout()
+    f_dev = C.c_void_p()
+    capi.check(capi.lib().oal_level_device_state(L.handle, C.byref(f_dev), None, None))
+    obst = torch.tensor(case.dom.obstacle, dtype=torch.uint8, device="cuda").contiguous()
+    out = torch.full((4,), np.nan, dtype=torch.float64, device="cuda")
+    capi.check(capi.lib().oal_mass_momentum_noalloc(f_dev.value, capi.STORAGE_NAMES[storage], lay["block_stride"],
+                                                    lay["dir_stride"], obst.data_ptr(), case.dom.n_blocks,
+                                                    out.data_ptr(), None))
+    torch.cuda.synchronize()
+    expect = L.mass_momentum()
+    np.testing.assert_allclose(out.cpu().numpy(), expect, rtol=RTOL, atol=1e-12 * abs(expect[0]))
+    L.close()
+    g.close()
+
+
 def test_noalloc_periodic_without_obstacle(oal):
     import torch
     case = taylor_green_case(16, u0=0.05, re=100.0, c_wale=0.2)
