@@ -545,7 +545,11 @@ typedef struct oal_q19_mesh_spec {
   double wake_margin;          /* body extents (0.1) */
   int32_t nregions;
   const oal_q19_region* regions;
-  int32_t reserved[4];
+  /* seal_cavities (generator.jl:37, 383-414, off by default): fluid slots inside the body's
+   * bounding box (one coarsest cell of margin) that axis-ray parity puts inside the surface stay
+   * out of the flood fill, so the interior of a leaky model stays solid */
+  int32_t seal_cavities;
+  int32_t reserved[3];
 } oal_q19_mesh_spec;
 typedef struct oal_q19_mesh oal_q19_mesh;
 
@@ -563,6 +567,9 @@ int32_t oal_q19_mesh_levels(const oal_q19_mesh* mesh);
  * real octs, listed ghosts, restricted slots}; level 0: the same summed over the levels (n0..n2
  * of the finest level, the leak / unreached / triangle counts of the mesh) */
 oal_status oal_q19_mesh_counts(const oal_q19_mesh* mesh, int32_t level, int64_t* out);
+/* the cavity-sealing report of the mesh (generator.jl:411-412): out[2] = {sealed_cells,
+ * cavity_unbracketed_parity_cells} (both 0 without seal_cavities) */
+oal_status oal_q19_mesh_seal_counts(const oal_q19_mesh* mesh, int64_t* out);
 /* level `level` (1..L) as a descriptor (pointers valid while the mesh lives) */
 oal_status oal_q19_mesh_level_desc(const oal_q19_mesh* mesh, int32_t level, oal_q19_level_desc* out);
 

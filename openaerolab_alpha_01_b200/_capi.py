@@ -242,7 +242,8 @@ class Q19MeshSpec(C.Structure):
         ("wake_margin", C.c_double),
         ("nregions", C.c_int32),
         ("regions", C.c_void_p),
-        ("reserved", C.c_int32 * 4),
+        ("seal_cavities", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 
@@ -323,6 +324,7 @@ _SIGNATURES = {
     "oal_q19_mesh_generate": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(Q19MeshSpec), C.POINTER(C.c_void_p)]),
     "oal_q19_mesh_destroy": (C.c_int32, [C.c_void_p]),
     "oal_q19_mesh_counts": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64)]),
+    "oal_q19_mesh_seal_counts": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64)]),
     "oal_q19_mesh_level_desc": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(Q19LevelDesc)]),
     "oal_q19_mesh_levels": (C.c_int32, [C.c_void_p]),
     "oal_q19_octree_create": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.POINTER(C.c_void_p)]),

@@ -263,21 +263,21 @@ struct BVH {
     return std::min(best, 1.0);
   }
 
-  // crossings of the +axis ray from p (geometry.jl:235-262). Hits at the same ray parameter (a ray
-  // through an edge or vertex shared by several triangles) count once; the reference counts each
-  // triangle, which miscounts a ray through a shared edge.
-  int ray_crossings(V3 p, int axis, std::vector<int32_t>& stack) const {
+  // crossings of the ray from p along +axis (dirn 1) or -axis (dirn -1) (geometry.jl:235-268). Hits
+  // at the same ray parameter (a ray through an edge or vertex shared by several triangles) count
+  // once; the reference counts each triangle, which miscounts a ray through a shared edge.
+  int ray_crossings(V3 p, int axis, std::vector<int32_t>& stack, int dirn = 1) const {
     thread_local std::vector<double> hits;
     hits.clear();
     int sp = 0;
     stack[sp++] = 0;
     const int b1 = axis == 0 ? 1 : 0, b2 = axis == 2 ? 1 : 2;
     V3 dir{0, 0, 0};
-    dir[axis] = 1.0;
+    dir[axis] = dirn > 0 ? 1.0 : -1.0;
     while (sp > 0) {
       const int id = stack[--sp];
       const V3 l = lo[id], h = hi[id];
-      if (h[axis] < p[axis] || p[b1] < l[b1] || p[b1] > h[b1] || p[b2] < l[b2] || p[b2] > h[b2]) continue;
+      if ((dirn > 0 ? h[axis] < p[axis] : l[axis] > p[axis]) || p[b1] < l[b1] || p[b1] > h[b1] || p[b2] < l[b2] || p[b2] > h[b2]) continue;
       if (left[id] < 0) {
         for (int k = first[id]; k < first[id] + count[id]; ++k) {
           const Tri& t = (*tri)[order[k]];
@@ -309,6 +309,21 @@ struct BVH {
 
   bool is_inside(V3 p, std::vector<int32_t>& stack) const {
     return (ray_crossings(p, 0, stack) & 1) + (ray_crossings(p, 1, stack) & 1) + (ray_crossings(p, 2, stack) & 1) >= 2;
+  }
+
+  // cavity sealing (cavity_seal_decision, geometry.jl:275-295): 0 outside by the majority of the
+  // +axis parities; 1 inside (near the surface the majority suffices, farther away two axes must
+  // also have odd -axis parity); 2 majority inside but not bracketed on two axes
+  uint8_t seal_decision(V3 p, std::vector<int32_t>& stack, bool near_surface) const {
+    bool pos[3];
+    int npos = 0;
+    for (int a = 0; a < 3; ++a) npos += (pos[a] = (ray_crossings(p, a, stack) & 1) != 0);
+    if (npos < 2) return 0;
+    if (near_surface) return 1;
+    int pairs = 0;
+    for (int a = 0; a < 3; ++a)
+      if (pos[a] && (ray_crossings(p, a, stack, -1) & 1) && ++pairs >= 2) return 1;
+    return 2;
   }
 };
 
@@ -520,6 +535,7 @@ struct oal_q19_mesh {
   int32_t ntri = 0;
   std::vector<LevelMesh> levels;
   int64_t counts[16] = {};
+  int64_t sealed = 0, unbracketed = 0;  // cavity-sealing report
 };
 
 namespace {
@@ -932,6 +948,35 @@ oal_status generate(const double* tri_in, int32_t ntri_in, const oal_q19_mesh_sp
     const int32_t row = nearrow[l][s];
     return row ? cq[l][18 * (int64_t)(row - 1) + i - 1] : 1.0f;
   };
+  // ---- 4b. sealed cavities (generator.jl:383-414): fluid slots inside the body's bounding box
+  // (one coarsest cell of margin) that parity puts inside the surface stay out of the fill
+  std::vector<std::vector<uint8_t>> sealed(L + 1);
+  for (int l = 1; l <= L; ++l) sealed[l].assign(8 * (int64_t)M->levels[l - 1].nocts, 0);
+  if (spec->seal_cavities && !no_geometry) {
+    const V3 mlo{blo.x - dxs[1], blo.y - dxs[1], blo.z - dxs[1]}, mhi{bhi.x + dxs[1], bhi.y + dxs[1], bhi.z + dxs[1]};
+    for (int l = 1; l <= L; ++l) {
+      const LevelMesh& Lv = M->levels[l - 1];
+      std::vector<int64_t> cand;
+      for (int64_t s = 0; s < 8 * (int64_t)Lv.nocts; ++s) {
+        if (Lv.kind[s] != K_FLUID) continue;
+        const V3 c = Lv.centre(s);
+        if (c.x >= mlo.x && c.x <= mhi.x && c.y >= mlo.y && c.y <= mhi.y && c.z >= mlo.z && c.z <= mhi.z) cand.push_back(s);
+      }
+      std::vector<uint8_t> flags(cand.size(), 0);
+      parallel_for((int64_t)cand.size(), [&](int, int64_t b, int64_t e) {
+        std::vector<int32_t> st(stack_size);
+        for (int64_t i = b; i < e; ++i) flags[i] = bvh.seal_decision(Lv.centre(cand[i]), st, near[l][cand[i]] != 0);
+      });
+      for (size_t i = 0; i < cand.size(); ++i) {
+        if (flags[i] == 1) {
+          sealed[l][cand[i]] = 1;
+          ++M->sealed;
+        } else if (flags[i] == 2) {
+          ++M->unbracketed;
+        }
+      }
+    }
+  }
   std::vector<std::pair<int, int64_t>> queue;
   {
     std::vector<int32_t> st(stack_size);
@@ -967,7 +1012,7 @@ oal_status generate(const double* tri_in, int32_t ntri_in, const oal_q19_mesh_sp
           if (cs < 0) continue;
           const uint8_t ck = Lf.kind[cs];
           if (ck == K_FLUID) {
-            if (!reached[l + 1][cs]) {
+            if (!reached[l + 1][cs] && !sealed[l + 1][cs]) {
               reached[l + 1][cs] = 1;
               queue.push_back({l + 1, cs});
             }
@@ -989,7 +1034,7 @@ oal_status generate(const double* tri_in, int32_t ntri_in, const oal_q19_mesh_sp
       if (crossq(l, s, i) < 1.0f || crossq(l, ns, opp(i)) < 1.0f) continue;
       const uint8_t nk = Lv.kind[ns];
       if (nk == K_FLUID) {
-        if (!reached[l][ns]) {
+        if (!reached[l][ns] && !sealed[l][ns]) {
           reached[l][ns] = 1;
           queue.push_back({l, ns});
         }
@@ -1002,7 +1047,7 @@ oal_status generate(const double* tri_in, int32_t ntri_in, const oal_q19_mesh_sp
         const int nc[3] = {c[0] + e[0], c[1] + e[1], c[2] + e[2]};
         const int64_t ps = Lp.find_slot(nc[0] >> 1, nc[1] >> 1, nc[2] >> 1);
         if (ps < 0) continue;
-        if (Lp.kind[ps] == K_FLUID && !reached[l - 1][ps]) {
+        if (Lp.kind[ps] == K_FLUID && !reached[l - 1][ps] && !sealed[l - 1][ps]) {
           reached[l - 1][ps] = 1;
           queue.push_back({l - 1, ps});
         }
@@ -1412,6 +1457,13 @@ oal_status generate(const double* tri_in, int32_t ntri_in, const oal_q19_mesh_sp
 }  // namespace
 
 extern "C" {
+
+oal_status oal_q19_mesh_seal_counts(const oal_q19_mesh* mesh, int64_t* out) {
+  if (!mesh || !out) return fail(OAL_E_INVALID_ARG, "null argument");
+  out[0] = mesh->sealed;
+  out[1] = mesh->unbracketed;
+  return OAL_OK;
+}
 
 oal_status oal_q19_default_mesh_spec(oal_q19_mesh_spec* s) {
   if (!s) return fail(OAL_E_INVALID_ARG, "null argument");

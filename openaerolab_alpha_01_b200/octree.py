@@ -93,6 +93,7 @@ class MeshSpec:
     wake_margin: float = 0.1
     regions: tuple = ()
     faces: tuple = ("inlet", "outlet", "slip", "slip", "slip", "slip")
+    seal_cavities: bool = False
 
     def native(self):
         s = capi.Q19MeshSpec()
@@ -108,6 +109,7 @@ class MeshSpec:
         s.wake_length = float(self.wake_length)
         s.wake_level_offset = int(self.wake_level_offset)
         s.wake_margin = float(self.wake_margin)
+        s.seal_cavities = int(bool(self.seal_cavities))
         for f in range(6):
             s.faces[f] = capi.Q19_FACE_NAMES[self.faces[f]]
         regs = (capi.Q19Region * max(len(self.regions), 1))()
@@ -254,6 +256,8 @@ def generate(tri, spec: MeshSpec) -> OctMesh:
         levels = [Mesh.from_native(h, l) for l in range(1, L + 1)]
         cnt = (C.c_int64 * 16)()
         check(lib().oal_q19_mesh_counts(h, 0, cnt))
+        seal = (C.c_int64 * 2)()
+        check(lib().oal_q19_mesh_seal_counts(h, seal))
     finally:
         lib().oal_q19_mesh_destroy(h)
     for l, m in enumerate(levels, start=1):
@@ -261,6 +265,7 @@ def generate(tri, spec: MeshSpec) -> OctMesh:
         m.dx = float(spec.dx_finest) * 2.0 ** (L - l)
         m.domain = tuple(v * m.dx for v in m.n)
     counts = {k: int(v) for k, v in zip(COUNT_NAMES, cnt[:len(COUNT_NAMES)])}
+    counts["sealed_cells"], counts["cavity_unbracketed_parity_cells"] = int(seal[0]), int(seal[1])
     counts["per_level"] = [m.counts for m in levels]
     return OctMesh(levels, counts, spec)
 
