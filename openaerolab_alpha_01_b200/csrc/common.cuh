@@ -175,6 +175,8 @@ struct StepArgs {
   uint32_t* err;                  // device error word (bounded waits that gave up), or null
   uint32_t flags_any;             // OR of the flags of every case of the launch (kernel selection)
   int32_t round_nearest;          // 16-bit codecs: round stored deviations to nearest (else stochastically)
+  int32_t prefetch_ctas;          // x-pair kernel: CTA j also prefetches CTA j + prefetch_ctas's
+                                  // populations and velocities into L2 (0 = off; launch tuning)
   const int32_t* fast_rec;        // x-pair kernel: per work entry 32 ints (27-entry neighbour row,
                                   // block coordinates + case, block index), in work-list order
   void* pi_neq;                   // CF_SGS_PI: post-collision Pi_neq (compute type, [6][nb*512]),
@@ -184,6 +186,12 @@ struct StepArgs {
   CaseParams p0;
   ParentView par;                 // refined levels only (par.ptr == null otherwise)
 };
+
+// Bulk prefetch of [p, p + bytes) from global memory into L2 (no register result, no wait): the
+// address and the size are multiples of 16 bytes.
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "r"(bytes) : "memory");
+}
 
 // Element index of cell (X, Y, Z) of the dense padded population grid (direction 0).
 __host__ __device__ __forceinline__ int64_t dense_idx(const StepArgs& a, int X, int Y, int Z) {

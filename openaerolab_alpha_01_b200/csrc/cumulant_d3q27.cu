@@ -967,6 +967,13 @@ __global__ void __launch_bounds__(OAL_PAIRS_THREADS, ((sizeof(S) == 4 || GEN || 
       s_tail[tid - 27] = v;
     }
   }
+  // L2 prefetch of a later CTA's data (the CTA prefetch_ctas ahead in this launch): its block
+  // index now, the bulk prefetches once this CTA's own loads are in flight
+  __shared__ int32_t s_pf;
+  if (tid == 32 % OAL_PAIRS_THREADS) {
+    const unsigned pf_cta = blockIdx.x + (unsigned)a.prefetch_ctas;
+    s_pf = (a.prefetch_ctas > 0 && pf_cta < gridDim.x) ? a.fast_rec[(int64_t)(pf_cta / CPB) * 32 + 31] : -1;
+  }
   // the case parameters: copied by the second warp, or by the first one in one-warp CTAs
   const int cw = OAL_PAIRS_THREADS >= 64 ? tid - 32 : tid;
   if (cw >= 0 && cw < (int)(sizeof(CaseParams) / 4)) {
@@ -986,6 +993,16 @@ __global__ void __launch_bounds__(OAL_PAIRS_THREADS, ((sizeof(S) == 4 || GEN || 
   const int n_real = a.n_blocks;
 
   const int i = tid & 3, y = (tid >> 2) & 7, z = (OAL_PAIRS_THREADS / 32) * part + (tid >> 5);
+  if (tid < 30 && s_pf >= 0) {
+    // one lane per direction: the later CTA's z planes of that direction are contiguous
+    // (OAL_PAIRS_THREADS words); three lanes for its velocity components
+    const IDX pz = (IDX)((OAL_PAIRS_THREADS / 32) * ((blockIdx.x + (unsigned)a.prefetch_ctas) % CPB));
+    if (tid < 27) {
+      prefetch_l2(fin + (IDX)s_pf * wbst + (IDX)tid * wkst + 32 * pz, OAL_PAIRS_THREADS * (uint32_t)sizeof(W));
+    } else if (cp.flags & CF_GRADIENTS) {
+      prefetch_l2(vel_in + (IDX)(tid - 27) * vcs + (IDX)s_pf * kCells + 64 * pz, (OAL_PAIRS_THREADS / 32) * 64 * 4u);
+    }
+  }
 
   // ---- WALE stencil of the previous step's velocity (kernel_cumulant.jl:496-549): its loads
   // are issued before the pull so that both round trips to memory overlap ----

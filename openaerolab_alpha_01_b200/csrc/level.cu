@@ -364,6 +364,7 @@ struct oal_level {
   // 6 components x n_blocks x 512 in the compute type, refreshed in place by the general kernel
   void* pi_neq = nullptr;
   bool comp = false;        // the last step's compressible equilibrium (oal_level_pi_neq)
+  int32_t prefetch_ctas = 0;  // launch tuning (OAL_TUNE_PREFETCH_CTAS)
 };
 
 // ------------------------------------------------------------------------------------------------
@@ -1454,6 +1455,7 @@ static oal_status enqueue_step(oal_level* L, const CaseParams& cp, cudaStream_t 
   a.p0 = cp;
   a.flags_any = cp.flags;
   a.round_nearest = L->round_nearest ? 1 : 0;
+  a.prefetch_ctas = L->prefetch_ctas;
   a.pi_neq = L->pi_neq;
   if ((cp.flags & CF_SGS_PI) && !L->pi_neq) return set_error(OAL_E_UNSUPPORTED, "variable_nu_sgs 1 without its Pi_neq field");
   if (!L->dense) { a.force_out = L->d_force; a.force_ticket = L->d_ticket; }
@@ -1726,6 +1728,136 @@ oal_status oal_level_pi_neq(oal_level* L, float* out) {
   if (e == cudaSuccess) e = cudaMemcpy(out, d_out, (size_t)ncell * 6 * sizeof(float), cudaMemcpyDeviceToHost);
   cudaFree(d_out);
   if (e != cudaSuccess) return set_error(OAL_E_CUDA, "pi_neq: %s", cudaGetErrorString(e));
+  return OAL_OK;
+}
+
+// ---- launch tuning and the autotuner --------------------------------------------------------
+}  // extern "C"
+
+// Device copies of a level's or pool's state buffers: the autotuner restores them between
+// candidates, so that tuning leaves the simulation where it was.
+struct StateSnapshot {
+  std::vector<void*> live, copy;
+  std::vector<size_t> bytes;
+  cudaError_t add(void* p, size_t n) {
+    if (!p || !n) return cudaSuccess;
+    void* c = nullptr;
+    cudaError_t e = cudaMalloc(&c, n);
+    if (e != cudaSuccess) return e;
+    live.push_back(p); copy.push_back(c); bytes.push_back(n);
+    return cudaMemcpy(c, p, n, cudaMemcpyDeviceToDevice);
+  }
+  cudaError_t restore() const {
+    for (size_t i = 0; i < live.size(); ++i) {
+      cudaError_t e = cudaMemcpy(live[i], copy[i], bytes[i], cudaMemcpyDeviceToDevice);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  }
+  ~StateSnapshot() { for (void* c : copy) cudaFree(c); }
+};
+
+// The prefetch distances the autotuner tries: {0, 4, 8, 16} x the SM count of the device.
+static cudaError_t tune_candidates(int device, int64_t* cand) {
+  int nsm = 0;
+  cudaError_t e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  const int64_t mult[OAL_TUNE_CANDIDATES] = {0, 4, 8, 16};
+  for (int c = 0; c < OAL_TUNE_CANDIDATES; ++c) cand[c] = mult[c] * nsm;
+  return e;
+}
+
+// Times `run` (n steps) once untimed, then once between two events on `st`, after `reset`.
+template <class Run, class Reset>
+static oal_status time_candidate(Run run, Reset reset, int32_t n, cudaStream_t st, double* ms) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  OAL_CUDA_TRY(cudaEventCreate(&e0));
+  cudaError_t ce = cudaEventCreate(&e1);
+  oal_status s = ce == cudaSuccess ? OAL_OK : set_error(OAL_E_CUDA, "autotune: %s", cudaGetErrorString(ce));
+  if (s == OAL_OK) s = reset();
+  if (s == OAL_OK) s = run(st);
+  if (s == OAL_OK && (ce = cudaStreamSynchronize(st)) != cudaSuccess) s = set_error(OAL_E_CUDA, "autotune: %s", cudaGetErrorString(ce));
+  if (s == OAL_OK) s = reset();
+  if (s == OAL_OK && (ce = cudaEventRecord(e0, st)) != cudaSuccess) s = set_error(OAL_E_CUDA, "autotune: %s", cudaGetErrorString(ce));
+  if (s == OAL_OK) s = run(st);
+  if (s == OAL_OK && (ce = cudaEventRecord(e1, st)) != cudaSuccess) s = set_error(OAL_E_CUDA, "autotune: %s", cudaGetErrorString(ce));
+  if (s == OAL_OK && (ce = cudaEventSynchronize(e1)) != cudaSuccess) s = set_error(OAL_E_CUDA, "autotune: %s", cudaGetErrorString(ce));
+  float t = 0.0f;
+  if (s == OAL_OK && (ce = cudaEventElapsedTime(&t, e0, e1)) != cudaSuccess) s = set_error(OAL_E_CUDA, "autotune: %s", cudaGetErrorString(ce));
+  *ms = (double)t / n;
+  cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  return s;
+}
+
+extern "C" {
+
+oal_status oal_level_set_tuning(oal_level* L, int32_t key, int64_t value) {
+  if (!L) return set_error(OAL_E_INVALID_ARG, "null level");
+  if (key != OAL_TUNE_PREFETCH_CTAS) return set_error(OAL_E_INVALID_ARG, "unknown tuning key %d", key);
+  if (value < 0 || value > (1 << 24)) return set_error(OAL_E_INVALID_ARG, "prefetch distance %lld", (long long)value);
+  if (L->prefetch_ctas != (int32_t)value) {
+    L->prefetch_ctas = (int32_t)value;
+    release_graph(L);  // the captured launches hold the old value
+  }
+  return OAL_OK;
+}
+
+oal_status oal_level_get_tuning(const oal_level* L, int32_t key, int64_t* value) {
+  if (!L || !value) return set_error(OAL_E_INVALID_ARG, "null argument");
+  if (key != OAL_TUNE_PREFETCH_CTAS) return set_error(OAL_E_INVALID_ARG, "unknown tuning key %d", key);
+  *value = L->prefetch_ctas;
+  return OAL_OK;
+}
+
+oal_status oal_level_autotune(oal_level* L, const oal_step_params* p, int32_t n_steps, int64_t* values,
+                              double* ms_per_step) {
+  if (!L || !p) return set_error(OAL_E_INVALID_ARG, "null argument");
+  if (n_steps <= 0) return set_error(OAL_E_INVALID_ARG, "n_steps must be positive");
+  if (L->kbc) return set_error(OAL_E_UNSUPPORTED, "autotune: D3Q27 levels (the D3Q39 kernel has no tuning key)");
+  OAL_CUDA_TRY(cudaSetDevice(L->g->device));
+  OAL_CUDA_TRY(cudaDeviceSynchronize());
+  const oal_geometry* g = L->g;
+  const size_t ncell = (size_t)g->nb * 512, mb = macro_bytes(L->storage);
+  const size_t fbytes = L->dense ? (size_t)27 * L->PX * L->PY * L->PZ * storage_bytes(L->storage)
+                                 : (size_t)(g->nb + g->n_ghost) * 512 * 27 * storage_bytes(L->storage);
+  StateSnapshot snap;
+  cudaError_t e = snap.add(L->f[L->parity], fbytes);
+  if (e == cudaSuccess) e = snap.add(L->vel[L->parity], ncell * 3 * mb);
+  if (e == cudaSuccess) e = snap.add(L->rho, ncell * mb);
+  if (e == cudaSuccess) e = snap.add(L->pi_neq, ncell * 6 * mb);
+  if (e != cudaSuccess)
+    return set_error(e == cudaErrorMemoryAllocation ? OAL_E_OUT_OF_MEMORY : OAL_E_CUDA, "autotune snapshot: %s", cudaGetErrorString(e));
+  int64_t cand[OAL_TUNE_CANDIDATES];
+  OAL_CUDA_TRY(tune_candidates(L->g->device, cand));
+  const int parity0 = L->parity;
+  const int32_t keep = L->prefetch_ctas;
+  cudaStream_t st = nullptr;
+  OAL_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  oal_status s = OAL_OK;
+  double best = 0.0;
+  int best_c = -1;
+  for (int c = 0; c < OAL_TUNE_CANDIDATES && s == OAL_OK; ++c) {
+    if ((s = oal_level_set_tuning(L, OAL_TUNE_PREFETCH_CTAS, cand[c])) != OAL_OK) break;
+    double ms = 0.0;
+    s = time_candidate([&](cudaStream_t q) { return oal_level_advance(L, p, n_steps, q); },
+                       [&]() -> oal_status {
+                         cudaError_t re = snap.restore();
+                         L->parity = parity0;
+                         return re == cudaSuccess ? OAL_OK : set_error(OAL_E_CUDA, "autotune restore: %s", cudaGetErrorString(re));
+                       },
+                       n_steps, st, &ms);
+    if (values) values[c] = cand[c];
+    if (ms_per_step) ms_per_step[c] = ms;
+    if (s == OAL_OK && (best_c < 0 || ms < best)) { best = ms; best_c = c; }
+  }
+  cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  cudaError_t re = snap.restore();
+  L->parity = parity0;
+  L->forces_valid = false;
+  oal_level_set_tuning(L, OAL_TUNE_PREFETCH_CTAS, s == OAL_OK && best_c >= 0 ? cand[best_c] : keep);
+  if (s != OAL_OK) return s;
+  if (re != cudaSuccess) return set_error(OAL_E_CUDA, "autotune restore: %s", cudaGetErrorString(re));
   return OAL_OK;
 }
 
@@ -2344,6 +2476,7 @@ struct oal_batch {
   int32_t graph_n = 0;
   int graph_parity = -1;
   int64_t bytes = 0;
+  int32_t prefetch_ctas = 0;  // launch tuning (OAL_TUNE_PREFETCH_CTAS)
 };
 
 static void batch_release_graph(oal_batch* B) {
@@ -2461,6 +2594,7 @@ static oal_status batch_enqueue_step(oal_batch* B, int step_offset, cudaStream_t
   a.cases = B->d_cases;
   a.flags_any = B->flags_any;
   a.fast_rec = B->d_fast_rec;
+  a.prefetch_ctas = B->prefetch_ctas;
   a.n_blocks = (int32_t)B->R;
   a.n_total_blocks = (int32_t)(B->R + B->G);
   a.block_base = 0;
@@ -2748,6 +2882,75 @@ oal_status oal_batch_advance(oal_batch* B, int32_t n, void* stream) {
   }
   for (auto& M : B->mem)
     if (M.active && (M.cp.flags & CF_COLLECT)) M.forces_valid = true;
+  return OAL_OK;
+}
+
+oal_status oal_batch_set_tuning(oal_batch* B, int32_t key, int64_t value) {
+  if (!B) return set_error(OAL_E_INVALID_ARG, "null batch");
+  if (key != OAL_TUNE_PREFETCH_CTAS) return set_error(OAL_E_INVALID_ARG, "unknown tuning key %d", key);
+  if (value < 0 || value > (1 << 24)) return set_error(OAL_E_INVALID_ARG, "prefetch distance %lld", (long long)value);
+  if (B->prefetch_ctas != (int32_t)value) {
+    B->prefetch_ctas = (int32_t)value;
+    batch_release_graph(B);
+  }
+  return OAL_OK;
+}
+
+oal_status oal_batch_get_tuning(const oal_batch* B, int32_t key, int64_t* value) {
+  if (!B || !value) return set_error(OAL_E_INVALID_ARG, "null argument");
+  if (key != OAL_TUNE_PREFETCH_CTAS) return set_error(OAL_E_INVALID_ARG, "unknown tuning key %d", key);
+  *value = B->prefetch_ctas;
+  return OAL_OK;
+}
+
+oal_status oal_batch_autotune(oal_batch* B, int32_t n_steps, int64_t* values, double* ms_per_step) {
+  if (!B) return set_error(OAL_E_INVALID_ARG, "null batch");
+  if (n_steps <= 0) return set_error(OAL_E_INVALID_ARG, "n_steps must be positive");
+  OAL_CUDA_TRY(cudaSetDevice(B->device));
+  OAL_CUDA_TRY(cudaDeviceSynchronize());
+  if (B->dirty) {
+    oal_status rs = batch_rebuild(B);
+    if (rs != OAL_OK) return rs;
+  }
+  const size_t ncell = (size_t)B->R * 512, mb = macro_bytes(B->storage);
+  const size_t fbytes = (size_t)(B->R + B->G) * 27 * 512 * storage_bytes(B->storage);
+  StateSnapshot snap;
+  cudaError_t e = snap.add(B->f[B->parity], fbytes);
+  if (e == cudaSuccess) e = snap.add(B->vel[B->parity], ncell * 3 * mb);
+  if (e == cudaSuccess) e = snap.add(B->rho, ncell * mb);
+  if (e != cudaSuccess)
+    return set_error(e == cudaErrorMemoryAllocation ? OAL_E_OUT_OF_MEMORY : OAL_E_CUDA, "autotune snapshot: %s", cudaGetErrorString(e));
+  int64_t cand[OAL_TUNE_CANDIDATES];
+  OAL_CUDA_TRY(tune_candidates(B->device, cand));
+  const int parity0 = B->parity;
+  const int32_t keep = B->prefetch_ctas;
+  cudaStream_t st = nullptr;
+  OAL_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  oal_status s = OAL_OK;
+  double best = 0.0;
+  int best_c = -1;
+  for (int c = 0; c < OAL_TUNE_CANDIDATES && s == OAL_OK; ++c) {
+    if ((s = oal_batch_set_tuning(B, OAL_TUNE_PREFETCH_CTAS, cand[c])) != OAL_OK) break;
+    double ms = 0.0;
+    s = time_candidate([&](cudaStream_t q) { return oal_batch_advance(B, n_steps, q); },
+                       [&]() -> oal_status {
+                         cudaError_t re = snap.restore();
+                         B->parity = parity0;
+                         return re == cudaSuccess ? OAL_OK : set_error(OAL_E_CUDA, "autotune restore: %s", cudaGetErrorString(re));
+                       },
+                       n_steps, st, &ms);
+    if (values) values[c] = cand[c];
+    if (ms_per_step) ms_per_step[c] = ms;
+    if (s == OAL_OK && (best_c < 0 || ms < best)) { best = ms; best_c = c; }
+  }
+  cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  cudaError_t re = snap.restore();
+  B->parity = parity0;
+  for (auto& M : B->mem) M.forces_valid = false;
+  oal_batch_set_tuning(B, OAL_TUNE_PREFETCH_CTAS, s == OAL_OK && best_c >= 0 ? cand[best_c] : keep);
+  if (s != OAL_OK) return s;
+  if (re != cudaSuccess) return set_error(OAL_E_CUDA, "autotune restore: %s", cudaGetErrorString(re));
   return OAL_OK;
 }
 

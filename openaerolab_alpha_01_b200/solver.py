@@ -328,6 +328,25 @@ class Level:
         check(lib().oal_level_mass_momentum(self.handle, out))
         return np.array(out[:])
 
+    # -- launch tuning (results do not depend on it)
+    @property
+    def prefetch_ctas(self) -> int:
+        v = C.c_int64()
+        check(lib().oal_level_get_tuning(self.handle, capi.OAL_TUNE_PREFETCH_CTAS, C.byref(v)))
+        return int(v.value)
+
+    @prefetch_ctas.setter
+    def prefetch_ctas(self, value: int) -> None:
+        check(lib().oal_level_set_tuning(self.handle, capi.OAL_TUNE_PREFETCH_CTAS, int(value)))
+
+    def autotune(self, params: capi.StepParams, n_steps: int = 20) -> dict:
+        """Time every candidate launch tuning over n_steps from the current state (restored after
+        each) and keep the fastest: {"prefetch_ctas": chosen, "candidates": [(value, ms/step)]}."""
+        vals = np.zeros(capi.OAL_TUNE_CANDIDATES, np.int64)
+        ms = np.zeros(capi.OAL_TUNE_CANDIDATES)
+        check(lib().oal_level_autotune(self.handle, C.byref(params), int(n_steps), vals.ctypes.data, ms.ctypes.data))
+        return {"prefetch_ctas": self.prefetch_ctas, "candidates": [(int(v), float(t)) for v, t in zip(vals, ms)]}
+
     def pi_neq(self) -> np.ndarray:
         """Non-equilibrium stress of the current state (compute_pi_neq_kernel!,
         kernel_pi_neq.jl:39-180): float32 (6, n_blocks, 512), xx yy zz xy xz yz, 0 in solid cells."""
@@ -395,6 +414,23 @@ class Batch:
 
     def advance(self, n_steps: int, stream=None) -> None:
         check(lib().oal_batch_advance(self.handle, int(n_steps), _stream_handle(stream)))
+
+    @property
+    def prefetch_ctas(self) -> int:
+        v = C.c_int64()
+        check(lib().oal_batch_get_tuning(self.handle, capi.OAL_TUNE_PREFETCH_CTAS, C.byref(v)))
+        return int(v.value)
+
+    @prefetch_ctas.setter
+    def prefetch_ctas(self, value: int) -> None:
+        check(lib().oal_batch_set_tuning(self.handle, capi.OAL_TUNE_PREFETCH_CTAS, int(value)))
+
+    def autotune(self, n_steps: int = 20) -> dict:
+        """The pool's autotuner (oal_batch_autotune): the members' state is restored afterwards."""
+        vals = np.zeros(capi.OAL_TUNE_CANDIDATES, np.int64)
+        ms = np.zeros(capi.OAL_TUNE_CANDIDATES)
+        check(lib().oal_batch_autotune(self.handle, int(n_steps), vals.ctypes.data, ms.ctypes.data))
+        return {"prefetch_ctas": self.prefetch_ctas, "candidates": [(int(v), float(t)) for v, t in zip(vals, ms)]}
 
     def state(self, member: int):
         nb = self._geoms[member].dom.n_blocks

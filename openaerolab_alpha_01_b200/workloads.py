@@ -60,6 +60,8 @@ def run_batched(cases, steps: int, storage: str = "f16", chunk: int = 100):
     for m in ids:
         B.remove(m)
     ids = [B.add(g, c.params, c.rho, c.vel) for g, c in zip(geoms, cases)]
+    # the pool's autotuner (its candidates run from this state, which it restores)
+    B.tuning = B.autotune(20)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     _cuda_sync()
     e0.record(s)
@@ -73,14 +75,17 @@ def run_batched(cases, steps: int, storage: str = "f16", chunk: int = 100):
     return e0.elapsed_time(e1) / 1e3, B, ids, geoms
 
 
-def run_plain_loop(cases, steps: int, storage: str = "f16"):
-    """The cases one after another, one step call per step; returns (seconds, final states)."""
+def run_plain_loop(cases, steps: int, storage: str = "f16", prefetch_ctas: int = 0):
+    """The cases one after another, one step call per step; returns (seconds, final states).
+    `prefetch_ctas`: the launch tuning every level uses (the batch's choice, for a like-for-like
+    comparison)."""
     import torch
     s = torch.cuda.Stream()
     levels = []
     for c in cases:
         g = Geometry(c.dom)
         L = Level(g, storage=storage)
+        L.prefetch_ctas = prefetch_ctas
         L.init_equilibrium(c.rho, c.vel)
         L.perform_timestep(c.params, s)  # warm-up of the code path
         L.init_equilibrium(c.rho, c.vel)
@@ -100,7 +105,7 @@ def config4(steps: int = 2000, n_cases: int = 64, seed: int = 4, storage: str = 
     cases = config4_cases(n_cases, seed)
     cells = sum(c.dom.n_blocks * 512 for c in cases)
     tb, B, ids, geoms = run_batched(cases, steps, storage)
-    tp, levels = run_plain_loop(cases, steps, storage)
+    tp, levels = run_plain_loop(cases, steps, storage, B.tuning["prefetch_ctas"])
     # batch invariance on the first members: bit-identical to the plain loop's result
     same = 0
     for i in range(min(check_members, len(cases))):
@@ -124,6 +129,7 @@ def config4(steps: int = 2000, n_cases: int = 64, seed: int = 4, storage: str = 
         "plain_loop": {"seconds": round(tp, 4), "cases_per_s": round(n_cases / tp, 3),
                        "mlups": round(cells * steps / tp / 1e6, 1)},
         "speedup": round(tp / tb, 3),
+        "tuning": B.tuning,
         "bit_identical_members_checked": f"{same}/{min(check_members, len(cases))}",
         "tgv_ke_rel_error_max": float(max(errs)) if errs else None,
     }
