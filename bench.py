@@ -220,6 +220,8 @@ def main():
     ap.add_argument("--serve-kbc-share", type=float, default=0.25, help="fraction of D3Q39 KBC requests served")
     ap.add_argument("--no-autotune", action="store_true",
                     help="skip the launch autotuner (oal_level_autotune) before the warm-up")
+    ap.add_argument("--prefetch", type=int, default=-1,
+                    help="set the x-pair kernel's L2 prefetch distance (CTAs) instead of autotuning it")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -265,7 +267,11 @@ def main():
 
     # the project's autotuner picks the x-pair kernel's L2 prefetch distance on this workload; it
     # restores the level's state, so the warm-up and the timed steps start from the initial state
-    tuning = None if args.no_autotune else level.autotune(p, 20)
+    if args.prefetch >= 0:
+        level.prefetch_ctas = args.prefetch
+        tuning = {"prefetch_ctas": args.prefetch, "candidates": None}
+    else:
+        tuning = None if args.no_autotune else level.autotune(p, 20)
 
     with torch.cuda.stream(stream):
         for i in range(args.warmup):

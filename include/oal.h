@@ -550,7 +550,14 @@ typedef struct oal_q19_region {
   double lo[3], hi[3], centre[3], radius;
 } oal_q19_region;
 
-/* MeshSpec (generator.jl:21-36) without per-box surface levels. */
+/* a box of its own surface level (SurfaceLevel, generator.jl:18-21): cells whose centre lies in
+ * [lo, hi] take max(surface_level, level) as their surface level */
+typedef struct oal_q19_surface_level {
+  int32_t level;
+  double lo[3], hi[3];
+} oal_q19_surface_level;
+
+/* MeshSpec (generator.jl:21-36). */
 typedef struct oal_q19_mesh_spec {
   double domain[3];            /* metres; periodic axes an even number of coarse cells */
   double dx;                   /* finest cell size, metres */
@@ -569,7 +576,9 @@ typedef struct oal_q19_mesh_spec {
    * bounding box (one coarsest cell of margin) that axis-ray parity puts inside the surface stay
    * out of the flood fill, so the interior of a leaky model stays solid */
   int32_t seal_cavities;
-  int32_t reserved[3];
+  int32_t nsurface_levels;     /* per-box surface levels (generator.jl:35, 185) */
+  const oal_q19_surface_level* surface_levels;
+  int32_t reserved[2];
 } oal_q19_mesh_spec;
 typedef struct oal_q19_mesh oal_q19_mesh;
 
@@ -610,6 +619,11 @@ oal_status oal_q19_level_advance(oal_q19_level* level, const oal_q19_params* p, 
 oal_status oal_q19_level_forces(oal_q19_level* level, double* total, double* per_triangle);
 oal_status oal_q19_level_get_state(oal_q19_level* level, void* f, void* u, void* rho);       /* host, nullable */
 oal_status oal_q19_level_set_state(oal_q19_level* level, const void* f, const void* u, const void* rho);
+/* either population/macro buffer: which 0 = the current one (the reference's S.f, S.u, S.rho),
+ * 1 = the other (S.g, S.v, S.rhob: the previous step's, which the time blend of a refined mesh's
+ * ghost fill reads); host, nullable on get */
+oal_status oal_q19_level_get_buffer(oal_q19_level* level, int32_t which, void* f, void* u, void* rho);
+oal_status oal_q19_level_set_buffer(oal_q19_level* level, int32_t which, const void* f, const void* u, const void* rho);
 oal_status oal_q19_level_device_state(oal_q19_level* level, void** f, void** u, void** rho, int64_t* steps);
 /* out[5] = {mass, px, py, pz, kinetic energy sum 0.5 rho |u|^2}, FP64, fixed reduction order */
 oal_status oal_q19_level_totals(oal_q19_level* level, double* out, void* stream);

@@ -245,8 +245,15 @@ class Q19MeshSpec(C.Structure):
         ("nregions", C.c_int32),
         ("regions", C.c_void_p),
         ("seal_cavities", C.c_int32),
-        ("reserved", C.c_int32 * 3),
+        ("nsurface_levels", C.c_int32),
+        ("surface_levels", C.c_void_p),
+        ("reserved", C.c_int32 * 2),
     ]
+
+
+class Q19SurfaceLevel(C.Structure):
+    """oal_q19_surface_level (include/oal.h): SurfaceLevel of generator.jl:18-21."""
+    _fields_ = [("level", C.c_int32), ("lo", C.c_double * 3), ("hi", C.c_double * 3)]
 
 
 class OALError(RuntimeError):
@@ -344,6 +351,8 @@ _SIGNATURES = {
     "oal_q19_octree_totals": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double)]),
     "oal_q19_level_get_state": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "oal_q19_level_set_state": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "oal_q19_level_get_buffer": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "oal_q19_level_set_buffer": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "oal_q19_level_device_state": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                                C.POINTER(C.c_void_p), C.POINTER(C.c_int64)]),
     "oal_q19_level_totals": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double), C.c_void_p]),

@@ -1357,6 +1357,30 @@ oal_status oal_q19_level_set_state(oal_q19_level* L, const void* f, const void* 
   return OAL_OK;
 }
 
+oal_status oal_q19_level_get_buffer(oal_q19_level* L, int32_t which, void* f, void* u, void* rho) {
+  if (!L || (which != 0 && which != 1)) return fail(OAL_E_INVALID_ARG, "null level or buffer %d", which);
+  DeviceGuard g(L->device);
+  const size_t ns = (size_t)L->nocts * 8;
+  const int b = L->cur ^ which;
+  Q19_TRY(cudaDeviceSynchronize());
+  if (f) Q19_TRY(cudaMemcpy(f, L->f[b], L->es * ns * Q, cudaMemcpyDeviceToHost));
+  if (u) Q19_TRY(cudaMemcpy(u, L->u[b], L->es * ns * 3, cudaMemcpyDeviceToHost));
+  if (rho) Q19_TRY(cudaMemcpy(rho, L->rho[b], L->es * ns, cudaMemcpyDeviceToHost));
+  return OAL_OK;
+}
+
+oal_status oal_q19_level_set_buffer(oal_q19_level* L, int32_t which, const void* f, const void* u, const void* rho) {
+  if (!L || !f || !u || !rho || (which != 0 && which != 1)) return fail(OAL_E_INVALID_ARG, "null argument or buffer %d", which);
+  DeviceGuard g(L->device);
+  const size_t ns = (size_t)L->nocts * 8;
+  const int b = L->cur ^ which;
+  Q19_TRY(cudaDeviceSynchronize());
+  Q19_TRY(cudaMemcpy(L->f[b], f, L->es * ns * Q, cudaMemcpyHostToDevice));
+  Q19_TRY(cudaMemcpy(L->u[b], u, L->es * ns * 3, cudaMemcpyHostToDevice));
+  Q19_TRY(cudaMemcpy(L->rho[b], rho, L->es * ns, cudaMemcpyHostToDevice));
+  return OAL_OK;
+}
+
 oal_status oal_q19_level_device_state(oal_q19_level* L, void** f, void** u, void** rho, int64_t* steps) {
   if (!L) return fail(OAL_E_INVALID_ARG, "null level");
   if (f) *f = L->f[L->cur];

@@ -555,6 +555,11 @@ oal_status generate(const double* tri_in, int32_t ntri_in, const oal_q19_mesh_sp
   const int Ls0 = spec->surface_level > 0 ? spec->surface_level : L;
   if (L < 1 || L > 12) return fail(OAL_E_INVALID_ARG, "levels must lie in 1..12 (got %d)", L);
   if (Ls0 > L) return fail(OAL_E_INVALID_ARG, "surface_level must be in 1..levels");
+  if (spec->nsurface_levels < 0 || (spec->nsurface_levels > 0 && !spec->surface_levels))
+    return fail(OAL_E_INVALID_ARG, "surface_levels: %d boxes without an array", spec->nsurface_levels);
+  for (int i = 0; i < spec->nsurface_levels; ++i)
+    if (spec->surface_levels[i].level < 1 || spec->surface_levels[i].level > L)
+      return fail(OAL_E_INVALID_ARG, "surface_levels[%d].level must be in 1..levels", i);
   std::vector<double> dxs(L + 1);
   for (int l = 1; l <= L; ++l) dxs[l] = spec->dx * std::ldexp(1.0, L - l);
   const double domain_in[3] = {spec->domain[0], spec->domain[1], spec->domain[2]};
@@ -687,6 +692,17 @@ oal_status generate(const double* tri_in, int32_t ntri_in, const oal_q19_mesh_sp
     for (int m = l; m <= Ls - 1; ++m) d += spec->band * dxs[m];
     return d;
   };
+  // the surface level at a point: the global one, raised inside per-box surface levels
+  // (local_surface_level, generator.jl:185)
+  auto local_surface_level = [&](const V3& p) {
+    int ls = Ls0;
+    for (int i = 0; i < spec->nsurface_levels; ++i) {
+      const oal_q19_surface_level& b = spec->surface_levels[i];
+      if (p.x >= b.lo[0] && p.x <= b.hi[0] && p.y >= b.lo[1] && p.y <= b.hi[1] && p.z >= b.lo[2] && p.z <= b.hi[2])
+        ls = std::max(ls, b.level);
+    }
+    return ls;
+  };
   const double inner_band = 1.0;
   std::vector<Mask> R(L + 1);
   R[1] = Mask(sizes[1][0], sizes[1][1], sizes[1][2], true);
@@ -718,7 +734,7 @@ oal_status generate(const double* tri_in, int32_t ntri_in, const oal_q19_mesh_sp
               for (int cci = 0; cci < 2; ++cci) {
                 const int ii = 2 * i + cci, jj = 2 * j + cj, kk = 2 * k + ck;
                 const V3 cc{(ii + 0.5) * dxc, (jj + 0.5) * dxc, (kk + 0.5) * dxc};
-                const double dl = band_distance(l, Ls0);
+                const double dl = band_distance(l, local_surface_level(cc));
                 if (dl < 0) continue;
                 int ti = -1;
                 const double dc = bvh.nearest(cc, dl + hdc + dxc, st, &ti);

@@ -77,10 +77,19 @@ class Region:
 
 
 @dataclass
+class SurfaceLevel:
+    """A box with its own surface level (generator.jl:18-21): cells whose centre lies in [lo, hi]
+    are refined to max(MeshSpec.surface_level, level) in the surface band."""
+    level: int
+    lo: tuple
+    hi: tuple
+
+
+@dataclass
 class MeshSpec:
     """MeshSpec of the reference (generator.jl:21-36): the domain in metres, the periodic axes, the
     number of levels and the finest cell size, the surface bands, regions and the condition of each
-    domain face (-x +x -y +y -z +z). Per-box surface levels are not supported."""
+    domain face (-x +x -y +y -z +z), per-box surface levels and cavity sealing."""
     domain: tuple
     periodic: tuple = (False, False, False)
     levels: int = 1
@@ -94,6 +103,7 @@ class MeshSpec:
     regions: tuple = ()
     faces: tuple = ("inlet", "outlet", "slip", "slip", "slip", "slip")
     seal_cavities: bool = False
+    surface_levels: tuple = ()   # SurfaceLevel(level, lo, hi): boxes with their own surface level
 
     def native(self):
         s = capi.Q19MeshSpec()
@@ -121,7 +131,14 @@ class MeshSpec:
             regs[i].radius = float(r.radius)
         s.nregions = len(self.regions)
         s.regions = C.cast(regs, C.c_void_p) if self.regions else None
-        return s, regs
+        sl = (capi.Q19SurfaceLevel * max(len(self.surface_levels), 1))()
+        for i, b in enumerate(self.surface_levels):
+            sl[i].level = int(b.level)
+            for a in range(3):
+                sl[i].lo[a], sl[i].hi[a] = float(b.lo[a]), float(b.hi[a])
+        s.nsurface_levels = len(self.surface_levels)
+        s.surface_levels = C.cast(sl, C.c_void_p) if self.surface_levels else None
+        return s, (regs, sl)
 
 
 _DESC_ARRAYS = [("origin", np.int32, (3,)), ("real", np.uint8, ()), ("onbr", np.int32, (27,)),
@@ -168,7 +185,11 @@ class Mesh:
         arrays = {}
         for name, dt, shape in _DESC_ARRAYS:
             n = no * int(np.prod(shape))
-            buf = (C.c_char * (n * np.dtype(dt).itemsize)).from_address(getattr(d, name))
+            ptr = getattr(d, name)
+            if not n or not ptr:  # a level without octs
+                arrays[name] = np.zeros((no,) + shape, dt)
+                continue
+            buf = (C.c_char * (n * np.dtype(dt).itemsize)).from_address(ptr)
             arrays[name] = np.frombuffer(buf, dt).reshape((no,) + shape).copy()
         def view(ptr, n, dt):
             if not n or not ptr:
@@ -512,6 +533,22 @@ class State:
         rho = np.empty((no, 8), self.dtype)
         check(lib().oal_q19_level_get_state(self._level_handle(level), _ptr(f), _ptr(u), _ptr(rho)))
         return f, u, rho
+
+    def buffer(self, which: int, level: int = 1):
+        """(f, u, rho) of buffer `which` of `level`: 0 the current state, 1 the other one (the
+        previous step's; the reference's S.g, S.v, S.rhob)."""
+        no = self.level_meshes[level - 1].nocts
+        f = np.empty((no, 19, 8), self.dtype)
+        u = np.empty((no, 3, 8), self.dtype)
+        rho = np.empty((no, 8), self.dtype)
+        check(lib().oal_q19_level_get_buffer(self._level_handle(level), int(which), _ptr(f), _ptr(u), _ptr(rho)))
+        return f, u, rho
+
+    def set_buffer(self, which: int, f, u, rho, level: int = 1):
+        f = np.ascontiguousarray(f, self.dtype)
+        u = np.ascontiguousarray(u, self.dtype)
+        rho = np.ascontiguousarray(rho, self.dtype)
+        check(lib().oal_q19_level_set_buffer(self._level_handle(level), int(which), _ptr(f), _ptr(u), _ptr(rho)))
 
     def set_state(self, f, u, rho, level: int = 1):
         f = np.ascontiguousarray(f, self.dtype)
@@ -1000,15 +1037,16 @@ def _level_ncut(m) -> int:
 
 def write_checkpoint(st: "State", out, n_avg: int = 0, sums=None, keep: int = 2) -> str:
     """write_checkpoint! (io_run.jl:277-291): `out`/checkpoints/checkpoint_<step, 9 digits>.bin,
-    written to a .tmp file and renamed; keeps the newest `keep`. The device holds one population
-    buffer per level between steps (the step reads nothing from the other), so the current state
-    fills both of the file's buffers. tau_w is zero (the octree wall model is not built here)."""
+    written to a .tmp file and renamed; keeps the newest `keep`. Both buffers of every level are
+    written (the current one first; a refined mesh's ghost fill blends the previous one). tau_w is
+    zero (the octree wall model is not built here)."""
     d = os.path.join(str(out), "checkpoints")
     os.makedirs(d, exist_ok=True)
     levels = []
     for l, m in enumerate(st.level_meshes, start=1):
-        f, u, rho = st.state(l)
-        levels.append(dict(f=f, g=f, u=u, v=u, rho=rho, rhob=rho, tau_w=np.zeros(_level_ncut(m), st.dtype)))
+        f, u, rho = st.buffer(0, l)
+        g, v, rhob = st.buffer(1, l)
+        levels.append(dict(f=f, g=g, u=u, v=v, rho=rho, rhob=rhob, tau_w=np.zeros(_level_ncut(m), st.dtype)))
     data = pack_checkpoint(levels, st.dtype, st.step, float(st.cfg.u_lattice), float(st.mass0), n_avg, sums,
                            st.config_sha, st.stl_sha)
     path = os.path.join(d, f"checkpoint_{st.step:09d}.bin")
@@ -1023,14 +1061,15 @@ def write_checkpoint(st: "State", out, n_avg: int = 0, sums=None, keep: int = 2)
 
 def read_checkpoint(st: "State", path) -> dict:
     """read_checkpoint! (io_run.jl:294-314): the case and precision must match the state; restores
-    every level's current populations, velocity and density, the step and mass0. Returns the
-    header (with n_avg and the nine force sums for the caller's histories)."""
+    both buffers of every level, the step and mass0. Returns the header (with n_avg and the nine
+    force sums for the caller's histories)."""
     with open(path, "rb") as io:
         data = io.read()
     ck = unpack_checkpoint(data, st.dtype, st.config_sha, st.stl_sha, [m.nocts for m in st.level_meshes],
                            [_level_ncut(m) for m in st.level_meshes])
     for l, lv in enumerate(ck["levels"], start=1):
-        st.set_state(lv["f"], lv["u"], lv["rho"], l)
+        st.set_buffer(0, lv["f"], lv["u"], lv["rho"], l)
+        st.set_buffer(1, lv["g"], lv["v"], lv["rhob"], l)
     st.step = ck["step"]
     st.mass0 = ck["mass0"]
     return ck

@@ -80,3 +80,26 @@ def test_sealing_leaves_a_closed_body_alone(meshes, oal):
     for a, b in zip(closed.levels, m.levels):
         assert np.array_equal(a.kind, b.kind)
     assert m.counts["leak_cells"] == 0
+
+
+def test_per_box_surface_levels(oal):
+    """SurfaceLevel boxes (generator.jl:18-21, 185): the surface band reaches the box's level only
+    for cells whose centre lies in the box; elsewhere the global surface level holds."""
+    tri = sphere_tris(24, 48, c=(2.0, 2.0, 2.0))
+    base = dict(domain=(6.0, 4.0, 4.0), levels=3, dx_finest=0.025, band_fine=4, band=3, surface_level=2)
+    coarse = octree.generate(tri, octree.MeshSpec(**base))
+    assert coarse.levels[2].counts["fluid_total"] == 0
+    box = octree.SurfaceLevel(3, (1.0, 1.0, 2.0), (3.0, 3.0, 3.0))   # the upper half of the sphere
+    m = octree.generate(tri, octree.MeshSpec(surface_levels=(box,), **base))
+    fine = m.levels[2]
+    assert fine.counts["fluid_total"] > 0
+    # the finest level's cells hug the upper half: their centres lie above the box's floor, less a
+    # band and the 2:1 buffers of the coarser levels
+    cells = fine.slot_centres().transpose(0, 2, 1).reshape(-1, 3)[fine.kind.reshape(-1) == capi.OAL_Q19_K_FLUID]
+    assert cells[:, 2].min() > 2.0 - 0.5 and cells[:, 2].max() < 3.0
+    # a box of the global level changes nothing
+    same = octree.generate(tri, octree.MeshSpec(surface_levels=(octree.SurfaceLevel(2, (0, 0, 0), (6, 4, 4)),), **base))
+    for a, b in zip(coarse.levels, same.levels):
+        assert np.array_equal(a.kind, b.kind)
+    with pytest.raises(capi.OALError):
+        octree.generate(tri, octree.MeshSpec(surface_levels=(octree.SurfaceLevel(4, (0, 0, 0), (1, 1, 1)),), **base))
