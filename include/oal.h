@@ -344,6 +344,25 @@ oal_status oal_level_mass_momentum(oal_level* L, double out[4]);
  * D3Q27): Pi_ab = sum_k c_a c_b (f_k - f_eq_k(rho, u)) at every cell, 0 in solid or unphysical
  * cells; host float out[6][n_blocks * 512] in the order xx, yy, zz, xy, xz, yz. */
 oal_status oal_level_pi_neq(oal_level* L, float* out);
+/* ---- characteristic outlet (NSCBC, kernel_nscbc_outlet.jl) ---------------------------------- */
+/* Poinsot-Lele outflow on the +x outlet plane (apply_nscbc_outlet_kernel!, :80-340), applied
+ * after every step of a library-owned D3Q27 level: LODI relaxation of the incoming acoustic
+ * characteristic toward p_target for subsonic outflow, capped Euler update of the face
+ * macros (tangential characteristics dropped at lateral-wall corners), face populations rebuilt
+ * as the equilibrium of the new state plus neq_blend times the interior cell's non-equilibrium
+ * part. Athermal (T = 1, p = rho cs^2). Off by default. */
+typedef struct oal_nscbc_params {
+  int32_t enabled;      /* OUTLET_NSCBC_ENABLED (false) */
+  int32_t all_blocks;   /* 0: the x = 8 plane of the blocks on the +x face; 1: of every block, the
+                           range apply_nscbc_outlet! launches (its kernel checks no block coordinate) */
+  float p_target;       /* OUTLET_NSCBC_P_TARGET (1.0) */
+  float sigma_relax;    /* OUTLET_NSCBC_SIGMA (0.27) */
+  float neq_blend;      /* OUTLET_NSCBC_NEQ_BLEND (0.5) */
+  int32_t reserved[3];
+} oal_nscbc_params;
+void oal_default_nscbc_params(oal_nscbc_params* np);
+oal_status oal_level_set_nscbc(oal_level* L, const oal_nscbc_params* np);
+
 /* ---- launch tuning (no counterpart in the reference; results do not depend on it) ---------- */
 /* OAL_TUNE_PREFETCH_CTAS: the x-pair kernel's CTA j also bulk-prefetches into L2 the populations
  * and velocities of the CTA prefetch_ctas launches ahead in its launch (0 = off, the default). */

@@ -117,6 +117,18 @@ class SurfaceParams(C.Structure):
     ]
 
 
+class NscbcParams(C.Structure):
+    """oal_nscbc_params (include/oal.h): the characteristic outlet's settings."""
+    _fields_ = [
+        ("enabled", C.c_int32),
+        ("all_blocks", C.c_int32),
+        ("p_target", C.c_float),
+        ("sigma_relax", C.c_float),
+        ("neq_blend", C.c_float),
+        ("reserved", C.c_int32 * 3),
+    ]
+
+
 class GeometryDesc(C.Structure):
     _fields_ = [
         ("n_blocks", C.c_int32),
@@ -297,6 +309,8 @@ _SIGNATURES = {
     "oal_default_surface_params": (None, [C.c_void_p]),
     "oal_level_surface_forces": (C.c_int32, [C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.c_void_p]),
     "oal_level_pi_neq": (C.c_int32, [C.c_void_p, C.c_void_p]),
+    "oal_default_nscbc_params": (None, [C.c_void_p]),
+    "oal_level_set_nscbc": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "oal_level_set_tuning": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int64]),
     "oal_level_get_tuning": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64)]),
     "oal_level_autotune": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),

@@ -234,6 +234,82 @@ __global__ void k_pi_neq(const S* __restrict__ f, PopIndex pi, const R* __restri
   for (int m = 0; m < 6; ++m) out[i + m * ncell] = O(p[m]);
 }
 
+// Characteristic (NSCBC) outlet, apply_nscbc_outlet_kernel! (kernel_nscbc_outlet.jl:80-340),
+// athermal: one thread per (y, z) of the x = 8 plane of a listed block, face cell x = 8 and its
+// interior neighbour x = 7; both fluid. Macros in, new macros and face populations out (the
+// library is compiled without FMA contraction, so each operation rounds as written).
+struct NscbcArgs {
+  float p_target, k_relax, neq_blend;
+  int32_t ny, nz;  // global cells of the domain (the corner test)
+};
+template <class S, class R>
+__global__ void __launch_bounds__(64) k_nscbc(S* __restrict__ f, PopIndex pi, R* __restrict__ rho, R* __restrict__ vel,
+                                              int64_t vcs, const int32_t* __restrict__ blocks, int32_t n,
+                                              const int4* __restrict__ binfo, const uint32_t* __restrict__ bflags,
+                                              const int32_t* __restrict__ mslot, const uint32_t* __restrict__ cmask,
+                                              NscbcArgs na) {
+  if ((int)blockIdx.x >= n) return;
+  const int64_t b = blocks[blockIdx.x];
+  const int y = threadIdx.x & 7, z = threadIdx.x >> 3;
+  const int cf = 7 | (y << 3) | (z << 6), ci = 6 | (y << 3) | (z << 6);
+  if (bflags[b] & BF_NEAR_SOLID) {
+    const uint32_t* m = cmask + (int64_t)mslot[b] * kCells;
+    if (((m[cf] >> 13) & 1u) || ((m[ci] >> 13) & 1u)) return;
+  }
+  const int4 bi = binfo[b];
+  const int gy = (bi.y - 1) * kBS + y + 1, gz = (bi.z - 1) * kBS + z + 1;
+  const bool corner = gy == 1 || gy == na.ny || gz == 1 || gz == na.nz;
+  const int64_t vf = b * kCells + cf, vi = b * kCells + ci;
+  const R rf = rho[vf], uf = vel[vf], vff = vel[vf + vcs], wf = vel[vf + 2 * vcs];
+  const R ri = rho[vi], ui = vel[vi], vi_ = vel[vi + vcs], wi = vel[vi + 2 * vcs];
+  const R Ru = R(1) / R(3), T = R(1);  // p = rho R T with R = cs^2 and T = 1
+  const R pf = rf * Ru * T, pint = ri * Ru * T;
+  const R g = R(1);
+  const R c = sqrt(fmax(g * Ru * T, R(1e-12)));
+  const R drho = rf - ri, du = uf - ui, dv = vff - vi_, dw = wf - wi, dp = pf - pint;
+  const R un = uf;
+  const R mach = un / fmax(c, R(1e-6));
+  R L1 = (un - c) * (dp - rf * c * du);
+  const R L2 = un * (c * c * drho - dp);
+  const R L3 = corner ? R(0) : un * dv;
+  const R L4 = corner ? R(0) : un * dw;
+  const R L5 = (un + c) * (dp + rf * c * du);
+  if (mach < R(1) && un > R(0)) {
+    const R mc = fmin(fmax(mach, R(0.05f)), R(0.95f));
+    L1 = R(na.k_relax) * (R(1) - mc * mc) * (pf - R(na.p_target));
+  }
+  const R d1 = (R(1) / (c * c)) * (L2 + R(0.5) * (L5 + L1));
+  const R d2 = R(0.5) * (L5 + L1);
+  const R d3 = (L5 - L1) / (R(2) * rf * c + R(1e-12));
+  auto cl = [](R x, R lo, R hi) { return x > hi ? hi : (x < lo ? lo : x); };
+  const R cap = corner ? R(0.10f) : R(0.20f);
+  const R d1c = cl(d1, -cap * rf, cap * rf), d2c = cl(d2, R(-0.10f) * pf, R(0.10f) * pf);
+  const R d3c = cl(d3, R(-0.10f) * c, R(0.10f) * c);
+  const R L3c = cl(L3, R(-0.10f) * c, R(0.10f) * c), L4c = cl(L4, R(-0.10f) * c, R(0.10f) * c);
+  R rn = rf - d1c;
+  const R un2 = uf - d3c;
+  const R vn = corner ? vi_ : vff - L3c;
+  const R wn = corner ? wi : wf - L4c;
+  R pn = pf - d2c;
+  rn = cl(rn, R(0.1f), R(10));
+  pn = fmax(pn, R(1e-6));
+  const R Tn = cl(pn / (rn * Ru + R(1e-12)), R(0.1f), R(10));
+  rho[vf] = rn;
+  vel[vf] = un2; vel[vf + vcs] = vn; vel[vf + 2 * vcs] = wn;
+  const R inv_n = R(1) / fmax(Ru * Tn, R(1e-12)), inv_i = R(1) / fmax(Ru * T, R(1e-12));
+  const R usq_n = un2 * un2 + vn * vn + wn * wn, usq_i = ui * ui + vi_ * vi_ + wi * wi;
+#pragma unroll
+  for (int k = 0; k < kQ27; ++k) {
+    const R cx = R(q27_cx(k)), cy = R(q27_cy(k)), cz = R(q27_cz(k)), w = R(q27_w(k));
+    const R cun = cx * un2 + cy * vn + cz * wn;
+    const R fen = fmax(rn * w * (R(1) + cun * inv_n + R(0.5) * cun * cun * inv_n * inv_n - R(0.5) * usq_n * inv_n), R(1e-15));
+    const R cui = cx * ui + cy * vi_ + cz * wi;
+    const R fei = fmax(ri * w * (R(1) + cui * inv_i + R(0.5) * cui * cui * inv_i * inv_i - R(0.5) * usq_i * inv_i), R(1e-15));
+    const R fi = Codec<S>::dec(f[pi(b, ci, k)], w, R(1.0 / q27_w(k)));
+    f[pi(b, cf, k)] = Codec<S>::enc(fen + R(na.neq_blend) * (fi - fei), w, R(1.0 / q27_w(k)));
+  }
+}
+
 inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 size_t storage_bytes(int32_t storage) {
@@ -365,6 +441,10 @@ struct oal_level {
   void* pi_neq = nullptr;
   bool comp = false;        // the last step's compressible equilibrium (oal_level_pi_neq)
   int32_t prefetch_ctas = 0;  // launch tuning (OAL_TUNE_PREFETCH_CTAS)
+  // characteristic outlet (oal_level_set_nscbc): settings and the listed blocks
+  oal_nscbc_params nscbc{};
+  int32_t* d_nscbc_blocks = nullptr;
+  int32_t n_nscbc = 0;
 };
 
 // ------------------------------------------------------------------------------------------------
@@ -703,6 +783,23 @@ static cudaError_t pi_neq_t(oal_level* L, int parity, O* d_out, cudaStream_t st)
   k_pi_neq<S, R, O><<<nblk(ncell, 128), 128, 0, st>>>(static_cast<const S*>(L->f[parity]), pop_index(L),
                                                       static_cast<const R*>(L->rho), static_cast<const R*>(L->vel[parity]),
                                                       g->d_bflags, g->d_mslot, g->d_cmask, ncell, L->comp ? 1 : 0, d_out);
+  return cudaGetLastError();
+}
+
+template <class S, class R>
+static cudaError_t nscbc_t(oal_level* L, void* f, void* vel, cudaStream_t st) {
+  const oal_geometry* g = L->g;
+  NscbcArgs na;
+  na.p_target = L->nscbc.p_target;
+  na.neq_blend = L->nscbc.neq_blend;
+  // K = sigma c_ref / L_ref with c_ref = sqrt(gamma R) at gamma 1, R 2/3 (the driver's athermal
+  // defaults, kernel_nscbc_outlet.jl:366-368) and L_ref the domain length in x
+  const float c_ref = std::sqrt(1.0f * float(2.0 / 3.0));
+  na.k_relax = L->nscbc.sigma_relax * c_ref / std::max((float)g->nx, 1.0f);
+  na.ny = g->ny; na.nz = g->nz;
+  k_nscbc<S, R><<<(unsigned)L->n_nscbc, 64, 0, st>>>(static_cast<S*>(f), pop_index(L), static_cast<R*>(L->rho),
+                                                      static_cast<R*>(vel), (int64_t)g->nb * 512, L->d_nscbc_blocks,
+                                                      L->n_nscbc, g->d_binfo, g->d_bflags, g->d_mslot, g->d_cmask, na);
   return cudaGetLastError();
 }
 
@@ -1337,7 +1434,7 @@ void oal_level_destroy(oal_level* L) {
   bouzidi_free(&L->bz);
   for (int i = 0; i < 2; ++i) { cudaFree(L->f[i]); cudaFree(L->vel[i]); }
   cudaFree(L->rho); cudaFree(L->d_force_part); cudaFree(L->d_force); cudaFree(L->d_mm_part); cudaFree(L->d_mm);
-  cudaFree(L->d_ticket); cudaFree(L->pi_neq);
+  cudaFree(L->d_ticket); cudaFree(L->pi_neq); cudaFree(L->d_nscbc_blocks);
   cudaFree(L->s_tri); cudaFree(L->s_ptr); cudaFree(L->s_out); cudaFree(L->s_part); cudaFree(L->s_sum);
   if (L->cap) cudaStreamDestroy(L->cap);
   if (L->ov.side) cudaStreamDestroy(L->ov.side);
@@ -1475,11 +1572,22 @@ static oal_status enqueue_step(oal_level* L, const CaseParams& cp, cudaStream_t 
   } else {
     OAL_CUDA_TRY(launch_by_storage(L->storage, g, a, PATH_GHOSTED, st, &L->ov));
   }
+  if (L->nscbc.enabled && L->n_nscbc > 0) {
+    // characteristic outlet after the step, before the wall corrections (timestep.jl:1617-1664)
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (L->storage) {
+      case OAL_STORE_F32: e = nscbc_t<float, float>(L, a.f_out, a.vel_out, st); break;
+      case OAL_STORE_F16_DEV: e = nscbc_t<__half, float>(L, a.f_out, a.vel_out, st); break;
+      case OAL_STORE_BF16_DEV: e = nscbc_t<__nv_bfloat16, float>(L, a.f_out, a.vel_out, st); break;
+      case OAL_STORE_F64: e = nscbc_t<double, double>(L, a.f_out, a.vel_out, st); break;
+    }
+    OAL_CUDA_TRY(e);
+  }
   if ((cp.flags & CF_BOUZIDI) && L->bz.n > 0)
     OAL_CUDA_TRY(bouzidi_enqueue(L->bz, L->storage, a.f_out, pop_index(L), g->d_nbr, g->d_mslot, g->d_cmask, st));
-  if ((cp.flags & CF_SGS_PI) && (cp.flags & CF_BOUZIDI) && L->bz.n > 0) {
-    // the Bouzidi correction rewrote populations after the fused refresh: refresh Pi_neq again
-    // from the corrected state (timestep.jl:1818-1834)
+  if ((cp.flags & CF_SGS_PI) && (((cp.flags & CF_BOUZIDI) && L->bz.n > 0) || (L->nscbc.enabled && L->n_nscbc > 0))) {
+    // the Bouzidi correction or the outlet rewrote populations after the fused refresh: refresh
+    // Pi_neq again from the corrected state (timestep.jl:1818-1834)
     cudaError_t e = cudaErrorInvalidValue;
     switch (L->storage) {
       case OAL_STORE_F32: e = pi_neq_t<float, float, float>(L, p ^ 1, static_cast<float*>(L->pi_neq), st); break;
@@ -1790,6 +1898,43 @@ static oal_status time_candidate(Run run, Reset reset, int32_t n, cudaStream_t s
 }
 
 extern "C" {
+
+void oal_default_nscbc_params(oal_nscbc_params* np) {
+  if (!np) return;
+  std::memset(np, 0, sizeof *np);
+  np->enabled = 0;          // OUTLET_NSCBC_ENABLED, config_loader.jl:751
+  np->p_target = 1.0f;      // :752
+  np->sigma_relax = 0.27f;  // :753
+  np->neq_blend = 0.5f;     // :754
+}
+
+oal_status oal_level_set_nscbc(oal_level* L, const oal_nscbc_params* np) {
+  if (!L || !np) return set_error(OAL_E_INVALID_ARG, "null argument");
+  if (L->kbc) return set_error(OAL_E_UNSUPPORTED, "the characteristic outlet is built for D3Q27 levels");
+  if (L->par.ptr) return set_error(OAL_E_UNSUPPORTED, "the characteristic outlet acts on the coarsest level only");
+  if (np->enabled && !(np->sigma_relax >= 0.0f && std::isfinite(np->p_target) && std::isfinite(np->neq_blend)))
+    return set_error(OAL_E_INVALID_ARG, "nscbc: sigma_relax >= 0 and finite p_target, neq_blend");
+  OAL_CUDA_TRY(cudaSetDevice(L->g->device));
+  std::vector<int32_t> list;
+  if (np->enabled) {
+    const oal_geometry* g = L->g;
+    int32_t bxmax = 0;
+    for (const int4& bi : g->h_binfo) bxmax = std::max(bxmax, bi.x);
+    for (int32_t b = 0; b < g->nb; ++b)
+      if (np->all_blocks || g->h_binfo[(size_t)b].x == bxmax) list.push_back(b);
+  }
+  cudaFree(L->d_nscbc_blocks);
+  L->d_nscbc_blocks = nullptr;
+  L->n_nscbc = 0;
+  if (!list.empty()) {
+    OAL_CUDA_TRY(cudaMalloc(&L->d_nscbc_blocks, list.size() * sizeof(int32_t)));
+    OAL_CUDA_TRY(cudaMemcpy(L->d_nscbc_blocks, list.data(), list.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    L->n_nscbc = (int32_t)list.size();
+  }
+  L->nscbc = *np;
+  release_graph(L);  // the captured steps hold the old setting
+  return OAL_OK;
+}
 
 oal_status oal_level_set_tuning(oal_level* L, int32_t key, int64_t value) {
   if (!L) return set_error(OAL_E_INVALID_ARG, "null level");

@@ -328,6 +328,21 @@ class Level:
         check(lib().oal_level_mass_momentum(self.handle, out))
         return np.array(out[:])
 
+    def set_nscbc(self, enabled: bool = True, all_blocks: bool = False, **kw) -> capi.NscbcParams:
+        """The characteristic (NSCBC) outlet after every step (apply_nscbc_outlet!,
+        kernel_nscbc_outlet.jl): p_target, sigma_relax, neq_blend as the reference's outlet_nscbc
+        settings; all_blocks as the reference's driver launches it (the x = 8 plane of every block)."""
+        p = capi.NscbcParams()
+        lib().oal_default_nscbc_params(C.byref(p))
+        p.enabled = int(bool(enabled))
+        p.all_blocks = int(bool(all_blocks))
+        for k, v in kw.items():
+            if not hasattr(p, k):
+                raise AttributeError(k)
+            setattr(p, k, v)
+        check(lib().oal_level_set_nscbc(self.handle, C.byref(p)))
+        return p
+
     # -- launch tuning (results do not depend on it)
     @property
     def prefetch_ctas(self) -> int:

@@ -52,6 +52,8 @@ def lib() -> C.CDLL:
             getattr(L, n).argtypes = [i32, i32, i32, i32] + [vp] * 14
             getattr(L, n).restype = C.c_int
         L.ora_pi_neq_f64.argtypes = [i32, vp, vp, vp, vp, i32, vp]
+        for n in ("ora_nscbc_outlet_f64", "ora_nscbc_outlet_f32"):
+            getattr(L, n).argtypes = [i32, i32, i32, i32, vp, vp, i32, C.c_float, C.c_float, C.c_float, vp, vp, vp]
         L.ora_q19_tables.argtypes = [vp] * 6
         L.ora_q19_periodic_box.argtypes = [i32, i32, i32, vp, vp]
         L.ora_q19_periodic_box.restype = C.c_int
@@ -269,6 +271,14 @@ class OracleLevel:
             # the correction rewrote populations after the refresh: refresh again from the
             # corrected state (timestep.jl:1818-1834)
             self.pi_neq[...] = self.state_pi_neq(p.compressible_corr)
+        return self
+
+    def nscbc(self, all_blocks=False, p_target=1.0, sigma_relax=0.27, neq_blend=0.5):
+        """The characteristic outlet on the current state (apply_nscbc_outlet_kernel!,
+        kernel_nscbc_outlet.jl:80-340), athermal."""
+        fn = lib().ora_nscbc_outlet_f64 if self.dtype == np.float64 else lib().ora_nscbc_outlet_f32
+        fn(self.nb, *self.shape, _p(self.coords), _p(self.obstacle), int(bool(all_blocks)), p_target, sigma_relax,
+           neq_blend, _p(self.f), _p(self.rho), _p(self.vel))
         return self
 
     def state_pi_neq(self, compressible=0):

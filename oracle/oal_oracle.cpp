@@ -1148,6 +1148,75 @@ Level make_level(int32_t nb, int32_t nx, int32_t ny, int32_t nz, const int32_t* 
   return Level{nb, nx, ny, nz, coords, nbr, obstacle, sponge, wall_dist};
 }
 
+// Characteristic outlet (apply_nscbc_outlet_kernel!, kernel_nscbc_outlet.jl:80-340; driver
+// apply_nscbc_outlet!, :343-393), athermal (T = 1): for every face cell x = 8 (1-based) of the
+// blocks on the +x face (or of every block, the range the reference's driver launches) whose
+// cell and interior neighbour x = 7 are fluid, in the reference's operation order.
+template <class T>
+void nscbc_outlet(const Level& L, int all_blocks, float p_target, float sigma, float blend, T* f, T* rho, T* vel) {
+  Arr<T> A{L.nb};
+  const int64_t cs = 512 * (int64_t)L.nb;
+  int bxmax = 0;
+  for (int b = 0; b < L.nb; ++b) bxmax = std::max(bxmax, L.coords[3 * b]);
+  const float c_ref = std::sqrt(1.0f * float(2.0 / 3.0));
+  const float k_relax = sigma * c_ref / std::max(float(L.nx), 1.0f);
+  for (int b = 0; b < L.nb; ++b) {
+    if (!all_blocks && L.coords[3 * b] != bxmax) continue;
+    for (int z = 0; z < BS; ++z)
+      for (int y = 0; y < BS; ++y) {
+        const int64_t of = A.s(7, y, z, b), oi = A.s(6, y, z, b);
+        if (L.obstacle && (L.obstacle[of] || L.obstacle[oi])) continue;
+        const int gy = (L.coords[3 * b + 1] - 1) * BS + y + 1, gz = (L.coords[3 * b + 2] - 1) * BS + z + 1;
+        const bool corner = gy == 1 || gy == L.ny || gz == 1 || gz == L.nz;
+        const T rf = rho[of], uf = vel[of], vf = vel[of + cs], wf = vel[of + 2 * cs];
+        const T ri = rho[oi], ui = vel[oi], vi = vel[oi + cs], wi = vel[oi + 2 * cs];
+        const T Ru = T(1) / T(3), Tt = T(1);
+        const T pf = rf * Ru * Tt, pi = ri * Ru * Tt;
+        const T c = std::sqrt(std::max(T(1) * Ru * Tt, T(1e-12)));
+        const T drho = rf - ri, du = uf - ui, dv = vf - vi, dw = wf - wi, dp = pf - pi;
+        const T un = uf;
+        const T mach = un / std::max(c, T(1e-6));
+        T L1 = (un - c) * (dp - rf * c * du);
+        const T L2 = un * (c * c * drho - dp);
+        const T L3 = corner ? T(0) : un * dv;
+        const T L4 = corner ? T(0) : un * dw;
+        const T L5 = (un + c) * (dp + rf * c * du);
+        if (mach < T(1) && un > T(0)) {
+          const T mc = std::min(std::max(mach, T(0.05f)), T(0.95f));
+          L1 = T(k_relax) * (T(1) - mc * mc) * (pf - T(p_target));
+        }
+        const T d1 = (T(1) / (c * c)) * (L2 + T(0.5) * (L5 + L1));
+        const T d2 = T(0.5) * (L5 + L1);
+        const T d3 = (L5 - L1) / (T(2) * rf * c + T(1e-12));
+        auto cl = [](T x, T lo, T hi) { return x > hi ? hi : (x < lo ? lo : x); };
+        const T cap = corner ? T(0.10f) : T(0.20f);
+        const T d1c = cl(d1, -cap * rf, cap * rf), d2c = cl(d2, T(-0.10f) * pf, T(0.10f) * pf);
+        const T d3c = cl(d3, T(-0.10f) * c, T(0.10f) * c);
+        const T L3c = cl(L3, T(-0.10f) * c, T(0.10f) * c), L4c = cl(L4, T(-0.10f) * c, T(0.10f) * c);
+        T rn = rf - d1c;
+        const T un2 = uf - d3c;
+        const T vn = corner ? vi : vf - L3c;
+        const T wn = corner ? wi : wf - L4c;
+        T pn = pf - d2c;
+        rn = cl(rn, T(0.1f), T(10));
+        pn = std::max(pn, T(1e-6));
+        const T Tn = cl(pn / (rn * Ru + T(1e-12)), T(0.1f), T(10));
+        rho[of] = rn;
+        vel[of] = un2; vel[of + cs] = vn; vel[of + 2 * cs] = wn;
+        const T inv_n = T(1) / std::max(Ru * Tn, T(1e-12)), inv_i = T(1) / std::max(Ru * Tt, T(1e-12));
+        const T usq_n = un2 * un2 + vn * vn + wn * wn, usq_i = ui * ui + vi * vi + wi * wi;
+        for (int k = 0; k < Q; ++k) {
+          const T cx = T(TB.cx[k]), cy = T(TB.cy[k]), cz = T(TB.cz[k]), w = T(TB.w[k]);
+          const T cun = cx * un2 + cy * vn + cz * wn;
+          const T fen = std::max(rn * w * (T(1) + cun * inv_n + T(0.5) * cun * cun * inv_n * inv_n - T(0.5) * usq_n * inv_n), T(1e-15));
+          const T cui = cx * ui + cy * vi + cz * wi;
+          const T fei = std::max(ri * w * (T(1) + cui * inv_i + T(0.5) * cui * cui * inv_i * inv_i - T(0.5) * usq_i * inv_i), T(1e-15));
+          f[A.f(7, y, z, b, k)] = fen + T(blend) * (f[A.f(6, y, z, b, k)] - fei);
+        }
+      }
+  }
+}
+
 }  // namespace
 
 // ---- linear Bouzidi wall (geometry/bouzidi_kernel.jl:150-380, default D3Q27 options) ---------
@@ -1363,6 +1432,18 @@ int ora_step_d3q27_pi_f32(int32_t nb, int32_t nx, int32_t ny, int32_t nz, const 
   L.pi_neq = pi_neq;
   if (P->variable_nu_sgs == 1 && !pi_neq) return -1;
   return step_level<float>(L, *P, f_in, f_out, f_post, rho_out, vel_out, vel_in, force_out);
+}
+
+void ora_nscbc_outlet_f64(int32_t nb, int32_t nx, int32_t ny, int32_t nz, const int32_t* coords, const uint8_t* obstacle,
+                          int32_t all_blocks, float p_target, float sigma, float blend, double* f, double* rho, double* vel) {
+  Level L = make_level(nb, nx, ny, nz, coords, nullptr, obstacle, nullptr, nullptr);
+  nscbc_outlet<double>(L, all_blocks, p_target, sigma, blend, f, rho, vel);
+}
+
+void ora_nscbc_outlet_f32(int32_t nb, int32_t nx, int32_t ny, int32_t nz, const int32_t* coords, const uint8_t* obstacle,
+                          int32_t all_blocks, float p_target, float sigma, float blend, float* f, float* rho, float* vel) {
+  Level L = make_level(nb, nx, ny, nz, coords, nullptr, obstacle, nullptr, nullptr);
+  nscbc_outlet<float>(L, all_blocks, p_target, sigma, blend, f, rho, vel);
 }
 
 // Pi_neq of a stored state (compute_pi_neq_kernel!, kernel_pi_neq.jl:39-180, D3Q27): out
