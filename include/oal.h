@@ -439,6 +439,12 @@ oal_status oal_batch_add(oal_batch* B, const oal_geometry* g, const oal_step_par
                          const double* vel_host, int32_t* member_out);
 oal_status oal_batch_remove(oal_batch* B, int32_t member);
 oal_status oal_batch_set_params(oal_batch* B, int32_t member, const oal_step_params* p);
+/* a member's linear Bouzidi boundary cells (as oal_level_set_bouzidi, block indices of the
+ * member's geometry); the member's steps with solid_bc OAL_SOLID_BOUZIDI apply them */
+oal_status oal_batch_set_bouzidi(oal_batch* B, int32_t member, int32_t n_cells, const int32_t* cell_block,
+                                 const int32_t* cell_x, const int32_t* cell_y, const int32_t* cell_z,
+                                 const uint16_t* q_half, float q_min_threshold, int32_t ff_fallback,
+                                 float limiter_rel_cap, float limiter_abs_cap);
 oal_status oal_batch_advance(oal_batch* B, int32_t n_steps, void* stream);
 /* Launch tuning of the pool's kernels (OAL_TUNE_* keys as for levels) and the autotuner over the
  * current members: each candidate advances n_steps from the pool's current state, which is

@@ -303,6 +303,9 @@ _SIGNATURES = {
     "oal_level_set_bouzidi": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                           C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_uint16),
                                           C.c_float, C.c_int32, C.c_float, C.c_float]),
+    "oal_batch_set_bouzidi": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                          C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_uint16),
+                                          C.c_float, C.c_int32, C.c_float, C.c_float]),
     "oal_level_get_forces_async": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "oal_level_mass_momentum": (C.c_int32, [C.c_void_p, C.POINTER(C.c_double)]),
     "oal_level_set_surface": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p]),

@@ -18,6 +18,7 @@ struct BouzidiArgs {
   float q_min, rel_cap, abs_cap;
   int32_t ff;
   const int32_t* __restrict__ nbr;    // [nb*27] 0-based, -1 = no neighbour (the real topology)
+  int32_t n_real;                     // neighbour indices >= n_real (a pool's ghost blocks) count as none
   const int32_t* __restrict__ mslot;  // per-block mask slot or -1 (no solid cell in the block)
   const uint32_t* __restrict__ cmask; // bit 13: the cell itself is solid
   PopIndex pi;
@@ -69,7 +70,7 @@ __global__ void __launch_bounds__(256) k_bouzidi_eval(const BouzidiArgs a, const
       const int ox = nx < 0 ? -1 : (nx >= kBS ? 1 : 0), oy = ny < 0 ? -1 : (ny >= kBS ? 1 : 0),
                 oz = nz < 0 ? -1 : (nz >= kBS ? 1 : 0);
       const int32_t nb = a.nbr[b * kQ27 + nbr_dir(ox, oy, oz)];
-      if (nb >= 0) {
+      if (nb >= 0 && nb < a.n_real) {
         const int nc = (nx & 7) | ((ny & 7) << 3) | ((nz & 7) << 6);
         if (!cell_solid(a, nb, nc)) { fff = load_pop<S, R>(f, a.pi, nb, nc, k); have = true; }
       }
@@ -123,12 +124,12 @@ static cudaError_t enqueue_t(const BouzidiArgs& a, void* f, void* vals, cudaStre
 }
 
 cudaError_t bouzidi_enqueue(const BouzidiSet& B, int32_t storage, void* f, const PopIndex& pi, const int32_t* nbr,
-                            const int32_t* mslot, const uint32_t* cmask, cudaStream_t st) {
+                            const int32_t* mslot, const uint32_t* cmask, cudaStream_t st, int32_t n_real) {
   if (B.n <= 0) return cudaSuccess;
   BouzidiArgs a;
   a.cells = B.cells; a.q = B.q; a.n = B.n;
   a.q_min = B.q_min; a.rel_cap = B.rel_cap; a.abs_cap = B.abs_cap; a.ff = B.ff_fallback;
-  a.nbr = nbr; a.mslot = mslot; a.cmask = cmask; a.pi = pi;
+  a.nbr = nbr; a.n_real = n_real; a.mslot = mslot; a.cmask = cmask; a.pi = pi;
   switch (storage) {
     case 0: return enqueue_t<float, float>(a, f, B.vals, st);
     case 1: return enqueue_t<__half, float>(a, f, B.vals, st);

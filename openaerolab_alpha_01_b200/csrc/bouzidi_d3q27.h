@@ -20,8 +20,9 @@ struct BouzidiSet {
 };
 
 // Enqueue the correction of the populations f (the step's output, post-collision at every cell)
-// on st: storage 0 F32, 1 F16 deviation, 2 BF16 deviation, 3 F64 (OAL_STORE_*).
+// on st: storage 0 F32, 1 F16 deviation, 2 BF16 deviation, 3 F64 (OAL_STORE_*). nbr: the real
+// topology (-1 = none); indices >= n_real (a pool's ghost blocks) count as none as well.
 cudaError_t bouzidi_enqueue(const BouzidiSet& B, int32_t storage, void* f, const PopIndex& pi, const int32_t* nbr,
-                            const int32_t* mslot, const uint32_t* cmask, cudaStream_t st);
+                            const int32_t* mslot, const uint32_t* cmask, cudaStream_t st, int32_t n_real = 0x7fffffff);
 
 }  // namespace oal

@@ -85,6 +85,46 @@ oal_status oal_internal_set_error(oal_status s, const char* msg) { return set_er
                        #expr, cudaGetErrorString(_e), __FILE__, __LINE__);                           \
   } while (0)
 
+// Validates a boundary-cell list (1-based block of a geometry of nb blocks, 1-based x, y, z, binary16
+// q per direction) and uploads it as a Bouzidi set whose blocks are offset by `base` (a pool's
+// range); replaces the set's previous contents.
+static oal_status bouzidi_upload(BouzidiSet* bz, int32_t storage, int64_t nb, int64_t base, int32_t n_cells,
+                                 const int32_t* cell_block, const int32_t* cell_x, const int32_t* cell_y,
+                                 const int32_t* cell_z, const uint16_t* q_half, float q_min_threshold,
+                                 int32_t ff_fallback, float limiter_rel_cap, float limiter_abs_cap) {
+  if (n_cells < 0) return set_error(OAL_E_INVALID_ARG, "n_cells %d", n_cells);
+  if (ff_fallback < 0 || ff_fallback > 2) return set_error(OAL_E_INVALID_ARG, "ff_fallback %d (0, 1 or 2)", ff_fallback);
+  if (!(limiter_rel_cap >= 0.0f) || !(limiter_abs_cap >= 0.0f) || !std::isfinite(q_min_threshold))
+    return set_error(OAL_E_INVALID_ARG, "limiter caps must be >= 0 and q_min_threshold finite");
+  std::vector<int2> cells((size_t)n_cells);
+  std::vector<float> q((size_t)n_cells * 27);
+  if (n_cells > 0) {
+    if (!cell_block || !cell_x || !cell_y || !cell_z || !q_half) return set_error(OAL_E_INVALID_ARG, "null array");
+    for (int32_t i = 0; i < n_cells; ++i) {
+      const int32_t b = cell_block[i], x = cell_x[i], y = cell_y[i], z = cell_z[i];
+      if (b < 1 || b > nb || x < 1 || x > 8 || y < 1 || y > 8 || z < 1 || z > 8)
+        return set_error(OAL_E_INVALID_ARG, "boundary cell %d: block %d, cell (%d, %d, %d) outside the level", i, b, x, y, z);
+      cells[(size_t)i] = make_int2((int)(base + b - 1), (x - 1) | ((y - 1) << 3) | ((z - 1) << 6));
+    }
+    for (size_t j = 0; j < q.size(); ++j) q[j] = half_bits_to_float(q_half[j]);
+  }
+  bouzidi_free(bz);
+  bz->q_min = q_min_threshold;
+  bz->ff_fallback = ff_fallback;
+  bz->rel_cap = limiter_rel_cap;
+  bz->abs_cap = limiter_abs_cap;
+  if (n_cells == 0) return OAL_OK;
+  const size_t rsz = storage == OAL_STORE_F64 ? sizeof(double) : sizeof(float);
+  OAL_CUDA_TRY(cudaMalloc(&bz->cells, cells.size() * sizeof(int2)));
+  OAL_CUDA_TRY(cudaMalloc(&bz->q, q.size() * sizeof(float)));
+  OAL_CUDA_TRY(cudaMalloc(&bz->vals, q.size() * rsz));
+  OAL_CUDA_TRY(cudaMemcpy(bz->cells, cells.data(), cells.size() * sizeof(int2), cudaMemcpyHostToDevice));
+  OAL_CUDA_TRY(cudaMemcpy(bz->q, q.data(), q.size() * sizeof(float), cudaMemcpyHostToDevice));
+  bz->n = n_cells;
+  return OAL_OK;
+}
+
+
 // ------------------------------------------------------------------------------------------------
 // device helper kernels
 // ------------------------------------------------------------------------------------------------
@@ -1676,41 +1716,12 @@ oal_status oal_level_set_bouzidi(oal_level* L, int32_t n_cells, const int32_t* c
                                  float limiter_abs_cap) {
   if (!L) return set_error(OAL_E_INVALID_ARG, "null level");
   if (L->kbc) return set_error(OAL_E_UNSUPPORTED, "linear Bouzidi walls are a D3Q27 level path");
-  if (n_cells < 0) return set_error(OAL_E_INVALID_ARG, "n_cells %d", n_cells);
-  if (ff_fallback < 0 || ff_fallback > 2) return set_error(OAL_E_INVALID_ARG, "ff_fallback %d (0, 1 or 2)", ff_fallback);
-  if (!(limiter_rel_cap >= 0.0f) || !(limiter_abs_cap >= 0.0f) || !std::isfinite(q_min_threshold))
-    return set_error(OAL_E_INVALID_ARG, "limiter caps must be >= 0 and q_min_threshold finite");
-  const oal_geometry* g = L->g;
-  std::vector<int2> cells((size_t)n_cells);
-  std::vector<float> q((size_t)n_cells * 27);
-  if (n_cells > 0) {
-    if (!cell_block || !cell_x || !cell_y || !cell_z || !q_half) return set_error(OAL_E_INVALID_ARG, "null array");
-    for (int32_t i = 0; i < n_cells; ++i) {
-      const int32_t b = cell_block[i], x = cell_x[i], y = cell_y[i], z = cell_z[i];
-      if (b < 1 || b > g->nb || x < 1 || x > 8 || y < 1 || y > 8 || z < 1 || z > 8)
-        return set_error(OAL_E_INVALID_ARG, "boundary cell %d: block %d, cell (%d, %d, %d) outside the level", i, b, x, y, z);
-      cells[(size_t)i] = make_int2(b - 1, (x - 1) | ((y - 1) << 3) | ((z - 1) << 6));
-    }
-    for (size_t j = 0; j < q.size(); ++j) q[j] = half_bits_to_float(q_half[j]);
-  }
-  OAL_CUDA_TRY(cudaSetDevice(g->device));
+  OAL_CUDA_TRY(cudaSetDevice(L->g->device));
   OAL_CUDA_TRY(cudaDeviceSynchronize());  // a step in flight may still read the old set
   release_graph(L);
-  bouzidi_free(&L->bz);
   ++L->bz_gen;
-  L->bz.q_min = q_min_threshold;
-  L->bz.ff_fallback = ff_fallback;
-  L->bz.rel_cap = limiter_rel_cap;
-  L->bz.abs_cap = limiter_abs_cap;
-  if (n_cells == 0) return OAL_OK;
-  const size_t rsz = L->storage == OAL_STORE_F64 ? sizeof(double) : sizeof(float);
-  OAL_CUDA_TRY(cudaMalloc(&L->bz.cells, cells.size() * sizeof(int2)));
-  OAL_CUDA_TRY(cudaMalloc(&L->bz.q, q.size() * sizeof(float)));
-  OAL_CUDA_TRY(cudaMalloc(&L->bz.vals, q.size() * rsz));
-  OAL_CUDA_TRY(cudaMemcpy(L->bz.cells, cells.data(), cells.size() * sizeof(int2), cudaMemcpyHostToDevice));
-  OAL_CUDA_TRY(cudaMemcpy(L->bz.q, q.data(), q.size() * sizeof(float), cudaMemcpyHostToDevice));
-  L->bz.n = n_cells;
-  return OAL_OK;
+  return bouzidi_upload(&L->bz, L->storage, L->g->nb, 0, n_cells, cell_block, cell_x, cell_y, cell_z, q_half,
+                        q_min_threshold, ff_fallback, limiter_rel_cap, limiter_abs_cap);
 }
 
 void oal_default_surface_params(oal_surface_params* sp) {
@@ -2579,6 +2590,7 @@ struct BatchMember {
   int64_t rb = 0, gb = 0, mb = 0;  // pool bases: real blocks, ghost blocks, mask slots
   int64_t nb = 0, ng = 0, nm = 0;
   bool forces_valid = false;
+  BouzidiSet bz;  // linear Bouzidi boundary cells (oal_batch_set_bouzidi), pool block indices
 };
 
 struct oal_batch {
@@ -2758,6 +2770,14 @@ static oal_status batch_enqueue_step(oal_batch* B, int step_offset, cudaStream_t
     case OAL_STORE_F64: e = batch_step_t<double, double>(B, a, st); break;
   }
   OAL_CUDA_TRY(e);
+  // the members' linear Bouzidi walls on the step's output (their cells in pool indices)
+  PopIndex pix{};
+  pix.binfo = B->d_binfo;
+  pix.bst = 27 * 512;
+  pix.kst = 512;
+  for (const auto& M : B->mem)
+    if (M.active && (M.cp.flags & CF_BOUZIDI) && M.bz.n > 0)
+      OAL_CUDA_TRY(bouzidi_enqueue(M.bz, B->storage, a.f_out, pix, B->d_nbr, B->d_mslot, B->d_cmask, st, (int32_t)B->R));
   B->parity ^= 1;
   return OAL_OK;
 }
@@ -2814,6 +2834,7 @@ void oal_batch_destroy(oal_batch* B) {
   if (B->ov.side) cudaStreamDestroy(B->ov.side);
   if (B->ov.fork) cudaEventDestroy(B->ov.fork);
   if (B->ov.join) cudaEventDestroy(B->ov.join);
+  for (auto& M : B->mem) bouzidi_free(&M.bz);
   for (auto& M : B->mem)
     if (M.active && M.g) {
       auto* g = const_cast<oal_geometry*>(M.g);
@@ -2884,8 +2905,6 @@ oal_status oal_batch_add(oal_batch* B, const oal_geometry* g, const oal_step_par
   CaseParams cp;
   oal_status s = resolve_params(p, g, &cp);
   if (s != OAL_OK) return s;
-  if (cp.flags & CF_BOUZIDI)
-    return set_error(OAL_E_UNSUPPORTED, "OAL_SOLID_BOUZIDI: the boundary cells attach to plain levels, not to batched cases (oal_batch_*)");
   if (cp.flags & (CF_SGS_PI | CF_SGS_DYNAMIC))
     return set_error(OAL_E_UNSUPPORTED, "variable_nu_sgs: plain levels only, not batched cases (oal_batch_*)");
   if (cp.flags & CF_STORE_POST) return set_error(OAL_E_UNSUPPORTED, "store_post_collision needs caller-owned arrays");
@@ -2970,10 +2989,26 @@ oal_status oal_batch_remove(oal_batch* B, int32_t m) {
   BatchMember& M = B->mem[(size_t)m];
   B->ar.release(M.rb, M.nb); B->ag.release(M.gb, M.ng); B->am.release(M.mb, M.nm);
   auto* g = const_cast<oal_geometry*>(M.g);
+  cudaSetDevice(B->device);
+  cudaDeviceSynchronize();  // a step in flight may still read the member's Bouzidi set
+  bouzidi_free(&M.bz);
   M = BatchMember();
   if (--g->n_levels == 0 && g->destroy_requested) geometry_release(g);
   B->dirty = true;
   return OAL_OK;
+}
+
+oal_status oal_batch_set_bouzidi(oal_batch* B, int32_t m, int32_t n_cells, const int32_t* cell_block,
+                                 const int32_t* cell_x, const int32_t* cell_y, const int32_t* cell_z,
+                                 const uint16_t* q_half, float q_min_threshold, int32_t ff_fallback,
+                                 float limiter_rel_cap, float limiter_abs_cap) {
+  if (!B || m < 0 || m >= B->max_members || !B->mem[(size_t)m].active) return set_error(OAL_E_INVALID_ARG, "no such member");
+  BatchMember& M = B->mem[(size_t)m];
+  OAL_CUDA_TRY(cudaSetDevice(B->device));
+  OAL_CUDA_TRY(cudaDeviceSynchronize());  // a step in flight may still read the old set
+  batch_release_graph(B);
+  return bouzidi_upload(&M.bz, B->storage, M.nb, M.rb, n_cells, cell_block, cell_x, cell_y, cell_z, q_half,
+                        q_min_threshold, ff_fallback, limiter_rel_cap, limiter_abs_cap);
 }
 
 oal_status oal_batch_set_params(oal_batch* B, int32_t m, const oal_step_params* p) {
@@ -2981,8 +3016,6 @@ oal_status oal_batch_set_params(oal_batch* B, int32_t m, const oal_step_params* 
   CaseParams cp;
   oal_status s = resolve_params(p, B->mem[(size_t)m].g, &cp);
   if (s != OAL_OK) return s;
-  if (cp.flags & CF_BOUZIDI)
-    return set_error(OAL_E_UNSUPPORTED, "OAL_SOLID_BOUZIDI: the boundary cells attach to plain levels, not to batched cases (oal_batch_*)");
   if (cp.flags & (CF_SGS_PI | CF_SGS_DYNAMIC))
     return set_error(OAL_E_UNSUPPORTED, "variable_nu_sgs: plain levels only, not batched cases (oal_batch_*)");
   B->mem[(size_t)m].p = *p; B->mem[(size_t)m].cp = cp;

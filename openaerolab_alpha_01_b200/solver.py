@@ -203,6 +203,19 @@ class Geometry:
             pass
 
 
+def _bouzidi_args(cells, q):
+    """(n, block, x, y, z, q binary16) ctypes arguments of a boundary-cell list."""
+    cells = np.ascontiguousarray(cells, dtype=np.int32).reshape(-1, 4)
+    qh = np.ascontiguousarray(np.asarray(q, dtype=np.float16).reshape(-1, 27)).view(np.uint16)
+    if qh.shape[0] != cells.shape[0]:
+        raise ValueError("q must hold 27 values per boundary cell")
+    n = int(cells.shape[0])
+    cols = [np.ascontiguousarray(cells[:, j]) for j in range(4)]
+    _bouzidi_args.keep = (cols, qh)  # alive for the call
+    ptrs = [c.ctypes.data_as(_i32p) if n else None for c in cols]
+    return (n, *ptrs, qh.ctypes.data_as(C.POINTER(C.c_uint16)) if n else None)
+
+
 class Level:
     """Library-owned state of one level: ping-pong populations, density, velocity."""
 
@@ -277,16 +290,9 @@ class Level:
         """Attach the linear Bouzidi boundary cells (solid_bc OAL_SOLID_BOUZIDI): cells (n, 4) int32
         (block, x, y, z) 1-based, q (n, 27) link fractions stored as float16 like the reference's
         q_map. An empty list detaches."""
-        cells = np.ascontiguousarray(cells, dtype=np.int32).reshape(-1, 4)
-        qh = np.ascontiguousarray(np.asarray(q, dtype=np.float16).reshape(-1, 27)).view(np.uint16)
-        if qh.shape[0] != cells.shape[0]:
-            raise ValueError("q must hold 27 values per boundary cell")
-        cols = [np.ascontiguousarray(cells[:, j]) for j in range(4)]
-        n = int(cells.shape[0])
-        ptrs = [c.ctypes.data_as(_i32p) if n else None for c in cols]
-        check(lib().oal_level_set_bouzidi(self.handle, n, *ptrs, qh.ctypes.data_as(C.POINTER(C.c_uint16)) if n else None,
-                                          float(q_min_threshold), int(ff_fallback), float(limiter_rel_cap),
-                                          float(limiter_abs_cap)))
+        args = _bouzidi_args(cells, q)
+        check(lib().oal_level_set_bouzidi(self.handle, *args, float(q_min_threshold), int(ff_fallback),
+                                          float(limiter_rel_cap), float(limiter_abs_cap)))
 
     def forces(self) -> np.ndarray:
         out = (C.c_double * 3)()
@@ -429,6 +435,14 @@ class Batch:
 
     def advance(self, n_steps: int, stream=None) -> None:
         check(lib().oal_batch_advance(self.handle, int(n_steps), _stream_handle(stream)))
+
+    def set_bouzidi(self, member: int, cells: np.ndarray, q: np.ndarray, q_min_threshold: float = 0.001,
+                    ff_fallback: int = 0, limiter_rel_cap: float = 0.0, limiter_abs_cap: float = 0.0) -> None:
+        """A member's linear Bouzidi boundary cells, as Level.set_bouzidi (block indices of the
+        member's geometry)."""
+        args = _bouzidi_args(cells, q)
+        check(lib().oal_batch_set_bouzidi(self.handle, int(member), *args, float(q_min_threshold), int(ff_fallback),
+                                          float(limiter_rel_cap), float(limiter_abs_cap)))
 
     @property
     def prefetch_ctas(self) -> int:

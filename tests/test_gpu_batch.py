@@ -79,3 +79,37 @@ def test_admission_by_pool_capacity(oal):
     B.remove(m2)
     assert B.try_add(g, case.params, case.rho, case.vel) is not None
     B.close()
+
+
+@pytest.mark.parametrize("storage", ["f16", "f32"])
+def test_member_with_bouzidi_walls_matches_alone(oal, storage):
+    """A member with linear Bouzidi walls (oal_batch_set_bouzidi) beside members without: its
+    populations equal the same case stepped alone with oal_level_set_bouzidi, bit for bit."""
+    from openaerolab_alpha_01_b200.bouzidi import sphere_qmap
+    ch = sphere_channel_case(32, 16, 16, diameter=6.0, centre_x=10.0, u_inlet=0.05, re=100.0,
+                             solid_bc=capi.OAL_SOLID_BOUZIDI)
+    ch.params.collect_forces = 0
+    cells, q = sphere_qmap(ch.dom, (10.0, 8.0, 8.0), 3.0)
+    others = [taylor_green_case(16, u0=0.05, re=100.0, c_wale=0.2),
+              sphere_channel_case(24, 16, 16, diameter=5.0, centre_x=8.0, u_inlet=0.04, re=80.0)]
+    steps = 8
+    g = Geometry(ch.dom)
+    L = Level(g, storage=storage)
+    L.init_equilibrium(ch.rho, ch.vel)
+    L.set_bouzidi(cells, q, ff_fallback=1)
+    L.execute_timestep_batch(ch.params, steps)
+    ref = L.state()[0]
+    L.close()
+    geoms = [Geometry(c.dom) for c in others]
+    B = Batch(storage=storage, max_real_blocks=256, max_ghost_blocks=256, max_mask_blocks=64, max_members=4)
+    ids = [B.add(gg, c.params, c.rho, c.vel) for gg, c in zip(geoms, others)]
+    m = B.add(g, ch.params, ch.rho, ch.vel)
+    B.set_bouzidi(m, cells, q, ff_fallback=1)
+    B.advance(steps)
+    assert np.array_equal(B.state(m)[0], ref)
+    for i, c in zip(ids, others):
+        assert np.array_equal(B.state(i)[0], alone(c, storage, steps)[0])
+    B.close()
+    for gg in geoms:
+        gg.close()
+    g.close()

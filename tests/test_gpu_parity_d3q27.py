@@ -319,10 +319,6 @@ def test_bouzidi_graph_detach_and_refusals(oal, channel):
     bad[0, 1] = 9
     with pytest.raises(OALError):
         A.set_bouzidi(bad, q)
-    bat = Batch(storage="f32", max_real_blocks=64, max_ghost_blocks=64)
-    with pytest.raises(OALError):
-        bat.add(g, p, channel.rho, channel.vel)
-    bat.close()
     # the momentum exchange belongs to the full-way wall, not to the corrected links: refused
     pc = capi.default_params(**{f: getattr(p, f) for f, _ in capi.StepParams._fields_ if f != "reserved"})
     pc.collect_forces = 1
