@@ -344,6 +344,20 @@ oal_status oal_level_mass_momentum(oal_level* L, double out[4]);
  * D3Q27): Pi_ab = sum_k c_a c_b (f_k - f_eq_k(rho, u)) at every cell, 0 in solid or unphysical
  * cells; host float out[6][n_blocks * 512] in the order xx, yy, zz, xy, xz, yz. */
 oal_status oal_level_pi_neq(oal_level* L, float* out);
+/* ---- linear Bouzidi walls on caller-owned arrays ------------------------------------------- */
+/* apply_bouzidi_correction! (bouzidi_kernel.jl:150-380) as its own call, as perform_timestep_v2!
+ * makes it after the kernel (timestep.jl:1752-1768): a set of boundary cells of a geometry
+ * (arguments as oal_level_set_bouzidi), applied to the populations of a step that ran through
+ * oal_stream_collide with solid_bc OAL_SOLID_BOUZIDI (full-way in the step); it reads and
+ * corrects fl->f_out in the caller's layout. */
+typedef struct oal_bouzidi oal_bouzidi;
+oal_status oal_bouzidi_create(const oal_geometry* g, int32_t storage, int32_t n_cells, const int32_t* cell_block,
+                              const int32_t* cell_x, const int32_t* cell_y, const int32_t* cell_z,
+                              const uint16_t* q_half, float q_min_threshold, int32_t ff_fallback,
+                              float limiter_rel_cap, float limiter_abs_cap, oal_bouzidi** out);
+void oal_bouzidi_destroy(oal_bouzidi* bz);
+oal_status oal_bouzidi_apply(const oal_geometry* g, oal_bouzidi* bz, const oal_level_fields* fl, void* stream);
+
 /* ---- characteristic outlet (NSCBC, kernel_nscbc_outlet.jl) ---------------------------------- */
 /* Poinsot-Lele outflow on the +x outlet plane (apply_nscbc_outlet_kernel!, :80-340), applied
  * after every step of a library-owned D3Q27 level: LODI relaxation of the incoming acoustic

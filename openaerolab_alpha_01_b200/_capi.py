@@ -303,6 +303,11 @@ _SIGNATURES = {
     "oal_level_set_bouzidi": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                           C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_uint16),
                                           C.c_float, C.c_int32, C.c_float, C.c_float]),
+    "oal_bouzidi_create": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                       C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_uint16),
+                                       C.c_float, C.c_int32, C.c_float, C.c_float, C.POINTER(C.c_void_p)]),
+    "oal_bouzidi_destroy": (None, [C.c_void_p]),
+    "oal_bouzidi_apply": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "oal_batch_set_bouzidi": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                           C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_uint16),
                                           C.c_float, C.c_int32, C.c_float, C.c_float]),

@@ -1321,8 +1321,6 @@ oal_status oal_stream_collide(const oal_geometry* g, const oal_level_fields* fl,
   CaseParams cp;
   oal_status s = resolve_params(p, g, &cp);
   if (s != OAL_OK) return s;
-  if (cp.flags & CF_BOUZIDI)
-    return set_error(OAL_E_UNSUPPORTED, "OAL_SOLID_BOUZIDI: the boundary cells attach to plain levels, not to caller-owned arrays (oal_stream_collide)");
   if (cp.flags & (CF_SGS_PI | CF_SGS_DYNAMIC))
     return set_error(OAL_E_UNSUPPORTED, "variable_nu_sgs: the Pi_neq field and the test filter belong to plain levels, not to caller-owned arrays (oal_stream_collide)");
   if (!fl->f_in || !fl->f_out || !fl->rho_out || !fl->vel_out || !fl->vel_in)
@@ -1346,6 +1344,56 @@ oal_status oal_stream_collide(const oal_geometry* g, const oal_level_fields* fl,
     k_reduce3<<<1, 256, 0, st>>>(g->d_force_part, (int64_t)g->nb * 4, fl->force_out);
     OAL_CUDA_TRY(cudaGetLastError());
   }
+  return OAL_OK;
+}
+
+struct oal_bouzidi {
+  const oal_geometry* g = nullptr;
+  int32_t storage = 0;
+  BouzidiSet bz;
+};
+
+oal_status oal_bouzidi_create(const oal_geometry* g, int32_t storage, int32_t n_cells, const int32_t* cell_block,
+                              const int32_t* cell_x, const int32_t* cell_y, const int32_t* cell_z,
+                              const uint16_t* q_half, float q_min_threshold, int32_t ff_fallback,
+                              float limiter_rel_cap, float limiter_abs_cap, oal_bouzidi** out) {
+  if (!g || !out) return set_error(OAL_E_INVALID_ARG, "null argument");
+  if (storage < OAL_STORE_F32 || storage > OAL_STORE_F64) return set_error(OAL_E_INVALID_ARG, "storage %d", storage);
+  *out = nullptr;
+  OAL_CUDA_TRY(cudaSetDevice(g->device));
+  auto* B = new oal_bouzidi();
+  B->g = g;
+  B->storage = storage;
+  oal_status s = bouzidi_upload(&B->bz, storage, g->nb, 0, n_cells, cell_block, cell_x, cell_y, cell_z, q_half,
+                                q_min_threshold, ff_fallback, limiter_rel_cap, limiter_abs_cap);
+  if (s != OAL_OK) {
+    bouzidi_free(&B->bz);
+    delete B;
+    return s;
+  }
+  *out = B;
+  return OAL_OK;
+}
+
+void oal_bouzidi_destroy(oal_bouzidi* B) {
+  if (!B) return;
+  cudaSetDevice(B->g->device);
+  bouzidi_free(&B->bz);
+  delete B;
+}
+
+oal_status oal_bouzidi_apply(const oal_geometry* g, oal_bouzidi* B, const oal_level_fields* fl, void* stream) {
+  if (!g || !B || !fl || !fl->f_out) return set_error(OAL_E_INVALID_ARG, "null argument");
+  if (B->g != g) return set_error(OAL_E_INVALID_ARG, "the boundary cells belong to another geometry");
+  if (fl->storage != B->storage) return set_error(OAL_E_INVALID_ARG, "storage %d, the set was built for %d", fl->storage, B->storage);
+  if (fl->f_block_stride < 512 || fl->f_dir_stride < 512) return set_error(OAL_E_INVALID_ARG, "bad population strides");
+  OAL_CUDA_TRY(cudaSetDevice(g->device));
+  PopIndex pix{};
+  pix.binfo = g->d_binfo;
+  pix.bst = fl->f_block_stride;
+  pix.kst = fl->f_dir_stride;
+  OAL_CUDA_TRY(bouzidi_enqueue(B->bz, B->storage, fl->f_out, pix, g->d_nbr, g->d_mslot, g->d_cmask,
+                               static_cast<cudaStream_t>(stream)));
   return OAL_OK;
 }
 

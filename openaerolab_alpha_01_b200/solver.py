@@ -216,6 +216,30 @@ def _bouzidi_args(cells, q):
     return (n, *ptrs, qh.ctypes.data_as(C.POINTER(C.c_uint16)) if n else None)
 
 
+class BouzidiCells:
+    """Linear Bouzidi boundary cells for caller-owned arrays (oal_bouzidi_create): `apply(fields)`
+    corrects the populations of a step run through oal_stream_collide with OAL_SOLID_BOUZIDI, as
+    the reference calls apply_bouzidi_correction! after its kernel."""
+
+    def __init__(self, geom: "Geometry", cells: np.ndarray, q: np.ndarray, storage: str = "f32",
+                 q_min_threshold: float = 0.001, ff_fallback: int = 0, limiter_rel_cap: float = 0.0,
+                 limiter_abs_cap: float = 0.0):
+        self.geom = geom
+        h = C.c_void_p()
+        args = _bouzidi_args(cells, q)
+        check(lib().oal_bouzidi_create(geom.handle, capi.STORAGE_NAMES[storage], *args, float(q_min_threshold),
+                                       int(ff_fallback), float(limiter_rel_cap), float(limiter_abs_cap), C.byref(h)))
+        self.handle = h
+
+    def apply(self, fields: capi.LevelFields, stream=None) -> None:
+        check(lib().oal_bouzidi_apply(self.geom.handle, self.handle, C.byref(fields), _stream_handle(stream)))
+
+    def close(self) -> None:
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            lib().oal_bouzidi_destroy(self.handle)
+            self.handle = None
+
+
 class Level:
     """Library-owned state of one level: ping-pong populations, density, velocity."""
 

@@ -231,6 +231,45 @@ def test_store_post_collision_on_caller_arrays(oal, oracle_lib, solid_bc):
     assert rel(got_post, O.f) < 2e-5
 
 
+def test_caller_owned_arrays_with_bouzidi_walls(oal, oracle_lib):
+    """oal_stream_collide with OAL_SOLID_BOUZIDI, then oal_bouzidi_apply on the caller's arrays
+    (the reference's separate apply_bouzidi_correction! call), against the oracle's step +
+    correction."""
+    import torch
+    from openaerolab_alpha_01_b200.bouzidi import sphere_qmap
+    from openaerolab_alpha_01_b200.solver import BouzidiCells
+    case = sphere_channel_case(32, 16, 16, diameter=6.0, centre_x=10.0, u_inlet=0.05, re=100.0)
+    d = case.dom
+    cells, q = sphere_qmap(d, (10.0, 8.0, 8.0), 3.0)
+    p = capi.default_params(**{f: getattr(case.params, f) for f, _ in capi.StepParams._fields_ if f != "reserved"})
+    p.solid_bc = capi.OAL_SOLID_BOUZIDI
+    p.collect_forces = 0
+    g = Geometry(d)
+    bz = BouzidiCells(g, cells, q, storage="f32", ff_fallback=1)
+    nb = d.n_blocks
+    fa = torch.tensor(oracle_lib.init_feq(case.rho, case.vel), dtype=torch.float32, device="cuda").contiguous()
+    fb = torch.empty_like(fa)
+    va = torch.tensor(case.vel, dtype=torch.float32, device="cuda").contiguous()
+    vb = torch.empty_like(va)
+    rho = torch.empty((nb, 512), dtype=torch.float32, device="cuda")
+    steps = 8
+    for _ in range(steps):
+        fl = capi.LevelFields(fa.data_ptr(), fb.data_ptr(), None, rho.data_ptr(), vb.data_ptr(), va.data_ptr(),
+                              capi.OAL_STORE_F32, 0, 512, 512 * nb, 512 * nb, None)
+        capi.check(capi.lib().oal_stream_collide(g.handle, C.byref(fl), C.byref(p), None))
+        bz.apply(fl)
+        fa, fb = fb, fa
+        va, vb = vb, va
+    torch.cuda.synchronize()
+    O = oracle_lib.OracleLevel(d.coords, d.neighbor_table, d.shape, obstacle=d.obstacle, dtype=np.float32)
+    O.init_equilibrium(case.rho, case.vel)
+    for _ in range(steps):
+        O.step_bouzidi(p, dict(cells=cells, q=q, ff_fallback=1))
+    assert rel(fa.cpu().numpy(), O.f) < 2e-5
+    bz.close()
+    g.close()
+
+
 def test_rejects_bad_params(oal):
     case = taylor_green_case(16)
     g = Geometry(case.dom)
