@@ -52,6 +52,12 @@ constexpr int kThreads = 128;
 #ifndef KBC_FAST_TOL_SCALE
 #define KBC_FAST_TOL_SCALE 1.0f
 #endif
+#ifndef KBC_NEWTON_MAX
+#define KBC_NEWTON_MAX 8  // fast path: full Newton steps before the block-Jacobi fallback
+#endif
+#ifndef KBC_FAST_MIN_BLOCKS
+#define KBC_FAST_MIN_BLOCKS 3  // fast path: CTAs per SM (the 13 x 13 Newton system lives in registers)
+#endif
 #ifndef KBC_FAST_MAX_SWEEPS
 #define KBC_FAST_MAX_SWEEPS 200
 #endif
@@ -146,6 +152,9 @@ struct KbcArgs {
   float trho, tjx, tjy, tjz;  // moments of feq_inlet, the inlet-face pin's targets
   float warm_gate;          // fast path: squared moment residual (in TOL_SQ units) up to which
                             // the cached multipliers start the solve (the reference: 100)
+  const float* sponge;      // [nb*512] or null: the sponge blend toward the inlet state
+  const float* wdist;       // [nb*512] or null: wall distance, NaN where there is none
+  int32_t sponge_blend;     // sponge_blend_distributions
 };
 
 // the face fill of one step: every ghost slot a real cell pulls receives its face value
@@ -247,8 +256,71 @@ __device__ __forceinline__ float fi_row(float rho, const float (&la)[13], const 
   return maxc(rho * row[3].x * kexp<FAST>(jclamp(lda_row<FAST>(la, row), -20.0f, 20.0f)), 1e-15f);
 }
 
+// The fast path's full Newton pass: at the multipliers la, the moments d = sum_k f_k b_k and the
+// Hessian of the dual problem H = sum_k f_k b_k b_k^T (b_k = (1, basis row k)), H packed lower
+// triangular, (i, j <= i) at i (i + 1) / 2 + j.
+__device__ __forceinline__ void newton_pass(const Tables& T, float rho, const float (&la)[13], float (&d)[13],
+                                            float (&H)[91]) {
+#pragma unroll
+  for (int m = 0; m < 13; ++m) d[m] = 0.0f;
+#pragma unroll
+  for (int n = 0; n < 91; ++n) H[n] = 0.0f;
+#pragma unroll 1
+  for (int k = 0; k < Q; ++k) {
+    const float4* row = T.b[k];
+    const float fi = fi_row<true>(rho, la, row);
+    const float4 r0 = row[0], r1 = row[1], r2 = row[2];
+    const float b[13] = {1.0f, r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w};
+#pragma unroll
+    for (int i = 0; i < 13; ++i) {
+      const float fb = fi * b[i];
+      d[i] += fb;
+#pragma unroll
+      for (int j = 0; j <= i; ++j) H[i * (i + 1) / 2 + j] = __fmaf_rn(fb, b[j], H[i * (i + 1) / 2 + j]);
+    }
+  }
+}
+
+// Solves H x = r in place (r becomes x) by a Cholesky factorisation of the packed H; false when
+// H is not numerically positive definite.
+__device__ __forceinline__ bool newton_solve(float (&H)[91], float (&r)[13]) {
+  float inv[13];
+#pragma unroll
+  for (int j = 0; j < 13; ++j) {
+    float s = H[j * (j + 1) / 2 + j];
+#pragma unroll
+    for (int k = 0; k < j; ++k) s = __fmaf_rn(-H[j * (j + 1) / 2 + k], H[j * (j + 1) / 2 + k], s);
+    if (!(s > 0.0f)) return false;
+    inv[j] = rsqrtf(s);
+#pragma unroll
+    for (int i = j + 1; i < 13; ++i) {
+      float t = H[i * (i + 1) / 2 + j];
+#pragma unroll
+      for (int k = 0; k < j; ++k) t = __fmaf_rn(-H[i * (i + 1) / 2 + k], H[j * (j + 1) / 2 + k], t);
+      H[i * (i + 1) / 2 + j] = t * inv[j];
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 13; ++i) {
+    float t = r[i];
+#pragma unroll
+    for (int k = 0; k < i; ++k) t = __fmaf_rn(-H[i * (i + 1) / 2 + k], r[k], t);
+    r[i] = t * inv[i];
+  }
+#pragma unroll
+  for (int i = 12; i >= 0; --i) {
+    float t = r[i];
+#pragma unroll
+    for (int k = i + 1; k < 13; ++k) t = __fmaf_rn(-H[k * (k + 1) / 2 + i], r[k], t);
+    r[i] = t * inv[i];
+  }
+  return true;
+}
+
 // physics_utils.jl:493-736: 13 multipliers by block-Jacobi Newton sweeps, warm-started from the
-// cached multipliers when they pass the staleness gate
+// cached multipliers when they pass the staleness gate. The fast path solves the same moment
+// equations to the same residual tolerance by full Newton steps first (one or two from a warm
+// start), keeping the sweeps as its fallback.
 template <bool FAST = false>
 __device__ __forceinline__ void solve_lambdas(const Tables& T, float rho, float ux, float uy, float uz, float (&la)[13],
                                               float warm_gate = 100.0f) {
@@ -271,7 +343,30 @@ __device__ __forceinline__ void solve_lambdas(const Tables& T, float rho, float 
     la[7] = inv_cs4 * ux * uy; la[8] = inv_cs4 * ux * uz; la[9] = inv_cs4 * uy * uz;
     la[10] = 0.0f; la[11] = 0.0f; la[12] = 0.0f;
   };
-  if (la[0] != la[0]) {
+  if constexpr (FAST) {
+    bool cold = la[0] != la[0];
+    if (cold) poly_start();
+    for (int it = 0; it < KBC_NEWTON_MAX; ++it) {
+      float d[13], H[91], r[13];
+      newton_pass(T, rho, la, d, H);
+      float res = 0.0f;
+#pragma unroll
+      for (int m = 0; m < 13; ++m) {
+        r[m] = mt[m] - d[m];
+        res = __fmaf_rn(r[m], r[m], res);
+      }
+      if (res < TOL_SQ) return;
+      if (!cold && it == 0 && res > warm_gate * TOL_SQ) {
+        // staleness gate on the warm start (physics_utils.jl:603-634)
+        poly_start();
+        cold = true;
+        continue;
+      }
+      if (!newton_solve(H, r)) break;
+#pragma unroll
+      for (int m = 0; m < 13; ++m) la[m] += jclamp(r[m], -2.0f, 2.0f);
+    }
+  } else if (la[0] != la[0]) {
     poly_start();
   } else {
     // staleness gate (physics_utils.jl:603-634)
@@ -516,7 +611,7 @@ __global__ void __launch_bounds__(256) k_kbc_fill(const KbcFillArgs a) {
 // EDGES: the level has domain faces or solid cells (the pin, bounce-back and gradient fall-backs
 // are compiled in); periodic boxes without obstacles run the instance without them.
 template <bool EDGES, bool FAST>
-__global__ void __launch_bounds__(kThreads, KBC_MIN_BLOCKS) k_kbc_step(const KbcArgs a) {
+__global__ void __launch_bounds__(kThreads, FAST ? KBC_FAST_MIN_BLOCKS : KBC_MIN_BLOCKS) k_kbc_step(const KbcArgs a) {
   __shared__ Tables T;
   __shared__ int32_t s_nbr[27];
   __shared__ float s_f[Q * kThreads];
@@ -588,7 +683,35 @@ __global__ void __launch_bounds__(kThreads, KBC_MIN_BLOCKS) k_kbc_step(const Kbc
       for (int k = 0; k < Q; ++k) sf[k * kThreads] = a.feq_inlet[k];
     }
   }
-  // macro realizability, far bulk (:2112-2229)
+  // sponge (kernel_entropic_d3q39.jl:1662, 1787-1841; athermal, pre-collision form)
+  const float sp = a.sponge ? a.sponge[ci] : 0.0f;
+  if (sp > 0.0f) {
+    rho = rho * (1.0f - sp) + 1.0f * sp;
+    ux = ux * (1.0f - sp) + a.u_inlet * sp;
+    uy = uy * (1.0f - sp);
+    uz = uz * (1.0f - sp);
+    if (a.sponge_blend) {
+      // the populations toward the inlet equilibrium, then the macros again from them
+      rho = 0.0f;
+      float jx = 0.0f, jy = 0.0f, jz = 0.0f;
+#pragma unroll 1
+      for (int k = 0; k < Q; ++k) {
+        const float f = sf[k * kThreads] * (1.0f - sp) + a.feq_inlet[k] * sp;
+        sf[k * kThreads] = f;
+        rho += f;
+        jx += f * float(kcx(k));
+        jy += f * float(kcy(k));
+        jz += f * float(kcz(k));
+      }
+      rho = jmax(rho, 0.01f);
+      inv_rho = 1.0f / rho;
+      ux = jx * inv_rho; uy = jy * inv_rho; uz = jz * inv_rho;
+    }
+  }
+  // macro realizability (:2112-2229): the far-bulk bounds away from walls and sponges, the
+  // near-wall ones (MacroBoundsPack defaults 0.35 / 2.40) elsewhere
+  const float wd = a.wdist ? a.wdist[ci] : __int_as_float(0x7fc00000);
+  const bool far_bulk = (wd != wd || wd > 16.0f) && sp < 0.03f;
   bool macro_limited = false;
   {
     const float u_trans = sqrtf(uy * uy + uz * uz);
@@ -598,12 +721,14 @@ __global__ void __launch_bounds__(kThreads, KBC_MIN_BLOCKS) k_kbc_step(const Kbc
     const float u_ref = jmax(jmax(a.u_inlet, 0.1f), 0.1f);
     float u_cap = jmin(1.00f, jmax(0.80f, 1.35f * u_ref + 0.15f));
     float u_trans_cap = jmin(0.92f, jmax(0.55f, 1.15f * u_ref + 0.12f));
-    u_cap = jmin(u_cap, jmin(0.78f, jmax(0.48f, 1.12f * u_ref + 0.08f)));
-    u_trans_cap = jmin(u_trans_cap, jmin(0.46f, jmax(0.18f, 0.68f * u_ref + 0.04f)));
+    if (far_bulk) {
+      u_cap = jmin(u_cap, jmin(0.78f, jmax(0.48f, 1.12f * u_ref + 0.08f)));
+      u_trans_cap = jmin(u_trans_cap, jmin(0.46f, jmax(0.18f, 0.68f * u_ref + 0.04f)));
+    }
     const bool speed_path = u_rel > u_cap;
     const bool trans_path = u_trans > u_trans_cap;
-    const float rho_floor = 0.42f, rho_ceil = 2.10f;
-    const bool density_path = rho < 0.30f || rho > 2.80f || (rho < rho_floor || rho > rho_ceil) ||
+    const float rho_floor = far_bulk ? 0.42f : 0.35f, rho_ceil = far_bulk ? 2.10f : 2.40f;
+    const bool density_path = rho < 0.30f || rho > 2.80f || (far_bulk && (rho < rho_floor || rho > rho_ceil)) ||
                               ((rho < 0.45f || rho > 2.20f) && (speed_path || trans_path));
     if (density_path) {
       rho = jclamp(rho, rho_floor, rho_ceil);
@@ -1079,6 +1204,7 @@ oal_status resolve(const oal_step_params* p, KbcArgs* a) {
   a->hrr = (p->hrr_hybrid == 1 && p->hrr_sigma < 0.999f) ? 1 : 0;
   a->tau = p->tau; a->c_wale = p->c_wale; a->nu_bg = p->nu_sgs_background; a->amr_sgs_scale = p->amr_sgs_scale;
   a->u_inlet = p->u_inlet; a->sigma0 = p->lambda_param; a->hrr_sigma = p->hrr_sigma;
+  a->sponge_blend = p->sponge_blend_distributions == 1 ? 1 : 0;
   a->nu_floor = p->nu_sgs_lattice_floor; a->shock_nu_max = p->shock_nu_max;
   inlet_equilibrium(p->u_inlet, a->feq_inlet);
   for (int k = 0; k < Q; ++k) {
@@ -1100,6 +1226,8 @@ oal_status enqueue(KbcLevel* L, const KbcArgs& base, const oal_step_params* p_in
   a.binfo = static_cast<const int4*>(L->G.d_binfo);
   a.faces = L->n_entries > 0 ? 1 : 0;
   if (L->G.has_solid) { a.bflags = L->G.d_bflags; a.mslot = L->G.d_mslot; a.cmask = L->G.d_cmask; }
+  a.sponge = L->G.d_sponge;
+  a.wdist = L->G.d_wdist;
   if (L->n_entries > 0) {
     KbcFillArgs fa;
     fa.f = L->f[p]; fa.entries = L->d_entries; fa.n = L->n_entries; fa.nbr = L->d_nbr; fa.binfo = a.binfo;

@@ -20,6 +20,8 @@ struct KbcGeometry {
   const int32_t* d_mslot = nullptr;     // [nb] mask slot or -1
   const uint32_t* d_cmask = nullptr;    // [slots*512]
   bool has_solid = false;
+  const float* d_sponge = nullptr;      // [nb*512] sponge strength or null
+  const float* d_wdist = nullptr;       // [nb*512] wall distance (NaN = none) or null
 };
 oal_status kbc_create(int device, const KbcGeometry& G, KbcLevel** out);
 // exp and log of the step: exact = the software routines shared with the CPU restatement

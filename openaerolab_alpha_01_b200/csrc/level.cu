@@ -1398,16 +1398,11 @@ oal_status oal_bouzidi_apply(const oal_geometry* g, oal_bouzidi* B, const oal_le
 }
 
 // ---- levels ----
-// D3Q39 entropic level: FP32 populations on a geometry whose blocks all have their 26 neighbours,
-// with no solid cell, no sponge and no wall within 16 cells (the far-bulk branch of the macro
-// realizability clamp, kernel_entropic_d3q39.jl:2149-2156)
+// D3Q39 entropic level: FP32 populations on a library-built geometry (faces, solids, sponge and
+// wall distance as the geometry carries them; the wall model is not built for it)
 static oal_status create_entropic_level(const oal_geometry* g, int32_t storage, uint32_t flags, oal_level** out) {
   if (storage != OAL_STORE_F32)
     return set_error(OAL_E_UNSUPPORTED, "the D3Q39 entropic level stores FP32 populations (storage %d)", storage);
-  for (float v : g->h_sponge)
-    if (v > 0.0f) return set_error(OAL_E_UNSUPPORTED, "the D3Q39 entropic level has no sponge");
-  for (float v : g->h_wdist)
-    if (v == v && !(v > 16.0f)) return set_error(OAL_E_UNSUPPORTED, "the D3Q39 entropic level has no wall within 16 cells");
   if (!g->d_nbr_ghost || g->h_nbrg.size() != (size_t)g->nb * 27 || g->h_binfo.size() != (size_t)g->nb)
     return set_error(OAL_E_UNSUPPORTED, "the D3Q39 entropic level needs a library-built geometry");
   KbcGeometry G;
@@ -1416,6 +1411,8 @@ static oal_status create_entropic_level(const oal_geometry* g, int32_t storage, 
   G.d_binfo = g->d_binfo; G.h_bflags = g->h_bflags.data();
   G.d_bflags = g->d_bflags; G.d_mslot = g->d_mslot; G.d_cmask = g->d_cmask;
   G.has_solid = g->n_solid > 0;
+  G.d_sponge = g->d_sponge;
+  G.d_wdist = g->d_wdist;
   KbcLevel* k = nullptr;
   oal_status s = kbc_create(g->device, G, &k);
   if (s != OAL_OK) return s;

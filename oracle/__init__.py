@@ -88,7 +88,7 @@ def lib() -> C.CDLL:
         L.ora_q39_inlet_equilibrium.argtypes = [C.c_float, vp]
         L.ora_q39_collide_cells.argtypes = [i64, vp, vp, vp, vp, vp, vp, vp]
         L.ora_q39_step.argtypes = [i32, vp, vp, vp, vp, vp, vp, vp, vp]
-        L.ora_q39_step_ex.argtypes = [i32, vp, vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.ora_q39_step_ex.argtypes = [i32, vp, vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -652,12 +652,14 @@ class OracleQ39Level:
     `coords` (nb, 3, 1-based block coordinates) and `shape` (cells) missing neighbours are domain
     faces, and `obstacle` (nb, 512) marks solid cells."""
 
-    def __init__(self, nbr, coords=None, shape=None, obstacle=None):
+    def __init__(self, nbr, coords=None, shape=None, obstacle=None, sponge=None, wall_dist=None):
         self.nbr = np.ascontiguousarray(nbr, np.int32)
         self.nb = self.nbr.shape[1]
         self.coords = None if coords is None else np.ascontiguousarray(coords, np.int32)
         self.shape = shape
         self.obstacle = None if obstacle is None else np.ascontiguousarray(obstacle, np.uint8)
+        self.sponge = None if sponge is None else np.ascontiguousarray(sponge, np.float32)
+        self.wall_dist = None if wall_dist is None else np.ascontiguousarray(wall_dist, np.float32)
         nb = self.nb
         self.f = np.zeros((39, nb, 512), np.float32)
         self.g = np.zeros_like(self.f)
@@ -684,7 +686,8 @@ class OracleQ39Level:
             else:
                 nx, ny, nz = self.shape
                 lib().ora_q39_step_ex(self.nb, _p(self.nbr), _p(self.coords), nx, ny, nz,
-                                      None if self.obstacle is None else _p(self.obstacle), C.addressof(params),
+                                      None if self.obstacle is None else _p(self.obstacle), _p(self.sponge),
+                                      _p(self.wall_dist), C.addressof(params),
                                       _p(self.f), _p(self.g), _p(self.vel), _p(self.vel_new), _p(self.rho),
                                       _p(self.lam))
             self.f, self.g = self.g, self.f

@@ -364,7 +364,7 @@ struct CellOut {
 // lam (13, warm start in, solution out), f_eq_inlet (39) -> fout (39), rho and u for the level's
 // macro arrays.
 void collide_cell(float* f, const float* g, const oal_step_params& P, const float* f_eq_inlet, float* lam,
-                  float* fout, CellOut& out) {
+                  float* fout, CellOut& out, float sp = 0.0f, float wd = std::numeric_limits<float>::quiet_NaN()) {
   // moments of the pulled populations (kernel_entropic_d3q39.jl:1281-1287)
   float rho = 0.0f, jx = 0.0f, jy = 0.0f, jz = 0.0f;
   for (int k = 0; k < Q; ++k) {
@@ -383,7 +383,30 @@ void collide_cell(float* f, const float* g, const oal_step_params& P, const floa
     rho = 1.0f; ux = P.u_inlet; uy = 0.0f; uz = 0.0f; inv_rho = 1.0f;
     for (int k = 0; k < Q; ++k) f[k] = f_eq_inlet[k];
   }
-  // macro realizability, far bulk: no wall distance and no sponge (:2112-2229)
+  // sponge (:1662, 1787-1841; athermal, pre-collision form)
+  if (sp > 0.0f) {
+    rho = rho * (1.0f - sp) + 1.0f * sp;
+    ux = ux * (1.0f - sp) + P.u_inlet * sp;
+    uy = uy * (1.0f - sp);
+    uz = uz * (1.0f - sp);
+    if (P.sponge_blend_distributions == 1) {
+      for (int k = 0; k < Q; ++k) f[k] = f[k] * (1.0f - sp) + f_eq_inlet[k] * sp;
+      rho = 0.0f;
+      float sjx = 0.0f, sjy = 0.0f, sjz = 0.0f;
+      for (int k = 0; k < Q; ++k) {
+        rho += f[k];
+        sjx += f[k] * float(CX[k]);
+        sjy += f[k] * float(CY[k]);
+        sjz += f[k] * float(CZ[k]);
+      }
+      rho = maxf(rho, 0.01f);
+      inv_rho = 1.0f / rho;
+      ux = sjx * inv_rho; uy = sjy * inv_rho; uz = sjz * inv_rho;
+    }
+  }
+  // macro realizability (:2112-2229): far-bulk bounds away from walls and sponges, near-wall ones
+  // (MacroBoundsPack defaults 0.35 / 2.40) elsewhere
+  const bool far_bulk = (wd != wd || wd > 16.0f) && sp < 0.03f;
   bool macro_limited = false;
   {
     const float u_trans = std::sqrt(uy * uy + uz * uz);
@@ -393,12 +416,14 @@ void collide_cell(float* f, const float* g, const oal_step_params& P, const floa
     const float u_ref = maxf(maxf(P.u_inlet, 0.1f), 0.1f);
     float u_cap = minf(1.00f, maxf(0.80f, 1.35f * u_ref + 0.15f));
     float u_trans_cap = minf(0.92f, maxf(0.55f, 1.15f * u_ref + 0.12f));
-    u_cap = minf(u_cap, minf(0.78f, maxf(0.48f, 1.12f * u_ref + 0.08f)));
-    u_trans_cap = minf(u_trans_cap, minf(0.46f, maxf(0.18f, 0.68f * u_ref + 0.04f)));
+    if (far_bulk) {
+      u_cap = minf(u_cap, minf(0.78f, maxf(0.48f, 1.12f * u_ref + 0.08f)));
+      u_trans_cap = minf(u_trans_cap, minf(0.46f, maxf(0.18f, 0.68f * u_ref + 0.04f)));
+    }
     const bool speed_path = u_rel > u_cap;
     const bool trans_path = u_trans > u_trans_cap;
-    const float rho_floor = 0.42f, rho_ceil = 2.10f;  // MacroBoundsPack defaults, far bulk
-    const bool density_path = rho < 0.30f || rho > 2.80f || (rho < rho_floor || rho > rho_ceil) ||
+    const float rho_floor = far_bulk ? 0.42f : 0.35f, rho_ceil = far_bulk ? 2.10f : 2.40f;  // MacroBoundsPack defaults
+    const bool density_path = rho < 0.30f || rho > 2.80f || (far_bulk && (rho < rho_floor || rho > rho_ceil)) ||
                               ((rho < 0.45f || rho > 2.20f) && (speed_path || trans_path));
     if (density_path) {
       rho = clampf(rho, rho_floor, rho_ceil);
@@ -754,8 +779,8 @@ void ora_q39_step(int32_t nb, const int32_t* nbr, const oal_step_params* P, cons
 // nbr (nb,27) 1-based with 0 for a missing neighbour block, coords (nb,3) 1-based block
 // coordinates, domain nx x ny x nz cells, obstacle (8,8,8,nb) uint8 or null.
 void ora_q39_step_ex(int32_t nb, const int32_t* nbr, const int32_t* coords, int32_t nx, int32_t ny, int32_t nz,
-                     const uint8_t* obstacle, const oal_step_params* P, const float* fin, float* fout,
-                     const float* vel_in, float* vel_out, float* rho_out, float* lam) {
+                     const uint8_t* obstacle, const float* sponge, const float* wall_dist, const oal_step_params* P,
+                     const float* fin, float* fout, const float* vel_in, float* vel_out, float* rho_out, float* lam) {
   build_tables();
   const int64_t N = (int64_t)nb * 512;
   float f_eq_inlet[Q];
@@ -805,7 +830,8 @@ void ora_q39_step_ex(int32_t nb, const int32_t* nbr, const int32_t* coords, int3
       for (int m = 0; m < 13; ++m) la[m] = lam[ci + N * m];
       float fo[Q];
       CellOut o;
-      collide_cell(f, g, *P, f_eq_inlet, la, fo, o);
+      collide_cell(f, g, *P, f_eq_inlet, la, fo, o, sponge ? sponge[ci] : 0.0f,
+                   wall_dist ? wall_dist[ci] : std::numeric_limits<float>::quiet_NaN());
       for (int m = 0; m < 13; ++m) lam[ci + N * m] = la[m];
       for (int k = 0; k < Q; ++k) fout[ci + N * k] = fo[k];
       rho_out[ci] = o.rho;

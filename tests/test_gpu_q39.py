@@ -276,6 +276,39 @@ def test_channel_faces_and_obstacle_bitwise(env, name):
     assert np.all(np.isfinite(ora.f))
 
 
+@pytest.mark.parametrize("blend", [0, 1])
+def test_channel_sponge_and_near_wall_bitwise(env, blend):
+    """The sponge toward the inlet state (with and without the population blend) and the near-wall
+    bounds of the macro realizability clamp (wall distance under 16 cells around the sphere and
+    the sponge strips): the oracle's bits after 4 steps, on a state pushed into the clamp."""
+    oracle, solver = env
+    from openaerolab_alpha_01_b200.cases import sphere_channel_case
+    case = sphere_channel_case(32, 16, 16, diameter=6.0, centre_x=12.0, u_inlet=0.05, re=200.0)
+    d = case.dom
+    gx, gy, gz = d.cell_positions()
+    d.sponge = (np.clip((gx - 24.0) / 8.0, 0.0, 1.0) * 0.6).astype(np.float32)
+    r = np.sqrt((gx - 0.5 - 12.0) ** 2 + (gy - 0.5 - 8.0) ** 2 + (gz - 0.5 - 8.0) ** 2) - 3.0
+    d.wall_dist = np.where(d.obstacle != 0, 0.0, np.maximum(r, 0.0)).astype(np.float32)
+    geom = solver.Geometry(d)
+    lvl = solver.Level(geom, "entropic", math="exact")
+    rng = np.random.default_rng(7)
+    vel = case.vel + 0.005 * rng.standard_normal(case.vel.shape) * (d.obstacle == 0)
+    rho = case.rho.copy()
+    # a dense pocket near the sphere and a fast one in the far field: both clamp branches fire
+    rho[(r > 0) & (r < 3)] = 2.3
+    vel[0][(r > 10) & (gx < 24)] = 0.7
+    lvl.init_equilibrium(rho, vel)
+    ora = oracle.OracleQ39Level(d.neighbor_table, d.coords, d.shape, d.obstacle, sponge=d.sponge,
+                                wall_dist=d.wall_dist).init_equilibrium(rho, vel)
+    p = solver.default_entropic_params(tau=0.56, c_wale=0.2, u_inlet=0.05, sponge_blend_distributions=blend)
+    for i in range(4):
+        p.time_step_seed = 11 + i
+        lvl.step(p)
+        ora.step(p)
+    assert_same_state(lvl, ora)
+    assert np.all(np.isfinite(ora.f))
+
+
 def test_channel_advance_graph_equals_steps(env):
     """n steps in one graph advance the noise seed by one per step, as single steps do."""
     d, geom, a, _, p = channel_pair(env, inlet_turbulence=0.05)
