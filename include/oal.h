@@ -309,7 +309,7 @@ oal_status oal_level_set_bouzidi(oal_level* L, int32_t n_cells, const int32_t* c
                                  float limiter_abs_cap);
 /* Non-blocking variant: enqueue the copy of the force into a host buffer (pinned for overlap). */
 oal_status oal_level_get_forces_async(oal_level* L, double* host_out3, void* stream);
-/* Surface-stress force mapping of a D3Q27 level: the reference's compute_aerodynamics!
+/* Surface-stress force mapping of a D3Q27 or D3Q39 level (CS2_PHYSICS 1/3 or 2/3): the reference's compute_aerodynamics!
  * (src/forces/surface.jl:1577-1587) with its default Prandtl force method, i.e.
  * map_stresses_kernel! (:636-1031) over the triangles, compute_stress_from_cell (:180-269) and
  * integrate_forces_kernel! (:1265-1331). Triangles: centroid, unit outward normal and area per

@@ -1784,7 +1784,6 @@ void oal_default_surface_params(oal_surface_params* sp) {
 
 oal_status oal_level_set_surface(oal_level* L, int32_t n_tri, const float* tri) {
   if (!L) return set_error(OAL_E_INVALID_ARG, "null level");
-  if (L->kbc) return set_error(OAL_E_UNSUPPORTED, "the surface-stress mapping is a D3Q27 level path");
   if (n_tri < 0 || (n_tri > 0 && !tri)) return set_error(OAL_E_INVALID_ARG, "n_tri %d", n_tri);
   for (int64_t i = 0; i < (int64_t)n_tri * 7; ++i)
     if (!std::isfinite(tri[i])) return set_error(OAL_E_INVALID_ARG, "triangle value %lld is not finite", (long long)i);
@@ -1818,7 +1817,6 @@ oal_status oal_level_set_surface(oal_level* L, int32_t n_tri, const float* tri) 
 
 oal_status oal_level_surface_forces(oal_level* L, const oal_surface_params* sp, double out[9], float* per_tri) {
   if (!L || !sp || !out) return set_error(OAL_E_INVALID_ARG, "null argument");
-  if (L->kbc) return set_error(OAL_E_UNSUPPORTED, "the surface-stress mapping is a D3Q27 level path");
   if (sp->abi_version != OAL_ABI_VERSION) return set_error(OAL_E_ABI_MISMATCH, "oal_surface_params.abi_version %u", sp->abi_version);
   if (sp->search_radius < 1 || sp->search_radius > 64) return set_error(OAL_E_INVALID_ARG, "search_radius %d (1..64)", sp->search_radius);
   if (!(sp->tau > 0.5f)) return set_error(OAL_E_INVALID_ARG, "tau must exceed 1/2");
@@ -1829,17 +1827,29 @@ oal_status oal_level_surface_forces(oal_level* L, const oal_surface_params* sp, 
   SurfArgs a{};
   a.tri = L->s_tri; a.n = L->s_n;
   a.rho = L->rho; a.vel = L->vel[L->parity]; a.vcs = (int64_t)g->nb * kCells;
+  float cs2 = 1.0f / 3.0f;
+  bool f64 = L->storage == OAL_STORE_F64;
+  if (L->kbc) {
+    // a D3Q39 level: its FP32 macros and the lattice's cs^2 = 2/3 (CS2_PHYSICS)
+    void* r = nullptr;
+    void* v = nullptr;
+    oal_status ks = kbc_device_state(L->kbc, nullptr, &r, &v);
+    if (ks != OAL_OK) return ks;
+    a.rho = r; a.vel = v;
+    cs2 = 2.0f / 3.0f;
+    f64 = false;
+  }
   a.ptr = L->s_ptr; a.dim_x = g->nx / kBS; a.dim_y = g->ny / kBS; a.dim_z = g->nz / kBS;
   a.mslot = g->d_mslot; a.cmask = g->d_cmask;
   a.radius = sp->search_radius; a.recover = sp->recover_normal ? 1 : 0;
   a.tau = sp->tau; a.c_wale = sp->c_wale; a.nu_bg = sp->nu_sgs_background;
-  a.pscale = sp->pressure_scale; a.sscale = sp->stress_scale; a.cs2 = 1.0f / 3.0f;
+  a.pscale = sp->pressure_scale; a.sscale = sp->stress_scale; a.cs2 = cs2;
   a.mcx = sp->moment_center[0]; a.mcy = sp->moment_center[1]; a.mcz = sp->moment_center[2];
   a.out = L->s_out; a.part = L->s_part;
-  OAL_CUDA_TRY(launch_surface(a, L->storage == OAL_STORE_F64, L->s_sum, nullptr));
+  OAL_CUDA_TRY(launch_surface(a, f64, L->s_sum, nullptr));
   OAL_CUDA_TRY(cudaMemcpy(out, L->s_sum, 9 * sizeof(double), cudaMemcpyDeviceToHost));
   if (per_tri) OAL_CUDA_TRY(cudaMemcpy(per_tri, L->s_out, (size_t)L->s_n * 6 * sizeof(float), cudaMemcpyDeviceToHost));
-  return check_level_error(L);
+  return L->kbc ? OAL_OK : check_level_error(L);
 }
 
 oal_status oal_level_get_forces(oal_level* L, double out[3]) {

@@ -165,7 +165,7 @@ def sphere_channel(nx=256, ny=128, nz=128, diameter=24.0, centre_x=64.0, u_inlet
 
 
 def surface_map(tri, rho, vel, obstacle, ptr, dims, radius=8, recover=1, tau=0.6, c_wale=0.2, nu_bg=0.0,
-                pscale=1.0, sscale=1.0, moment_center=(0.0, 0.0, 0.0)):
+                pscale=1.0, sscale=1.0, moment_center=(0.0, 0.0, 0.0), cs2=1.0 / 3.0):
     """Surface-stress mapping (src/forces/surface.jl:636-1331) on host fields in the reference
     layout (rho (nb, 512), vel (3, nb, 512), obstacle (nb, 512)); ptr: 1-based block pointer over
     the dims block grid, x fastest. Returns (per-triangle (n, 6) float32, per-triangle force and
@@ -180,7 +180,7 @@ def surface_map(tri, rho, vel, obstacle, ptr, dims, radius=8, recover=1, tau=0.6
     out = np.zeros((n, 6), np.float32)
     part = np.zeros((n, 9))
     lib().ora_surface_map(n, _p(tri), _p(rho), _p(vel), int(rho.size), _p(obst), _p(ptr), *map(int, dims), int(radius),
-                          int(recover), tau, c_wale, nu_bg, pscale, sscale, 1.0 / 3.0, _p(mc), _p(out), _p(part))
+                          int(recover), tau, c_wale, nu_bg, pscale, sscale, cs2, _p(mc), _p(out), _p(part))
     return out, part
 
 

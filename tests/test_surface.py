@@ -146,3 +146,35 @@ def test_gpu_surface_drag_beside_momentum_exchange(oal):
     cd_surf = float(r["coefficients"][0])
     assert cd_mem > 0 and cd_surf > 0
     assert abs(cd_surf - cd_mem) / cd_mem < 0.25, (cd_surf, cd_mem)
+
+
+@pytest.mark.gpu
+def test_gpu_surface_map_on_a_d3q39_level(oal, oracle_lib):
+    """A D3Q39 (KBC) channel: the same mapping on the level's FP32 macros with cs^2 = 2/3,
+    bit for bit against the oracle."""
+    from openaerolab_alpha_01_b200.cases import sphere_channel_case
+    from openaerolab_alpha_01_b200.solver import Geometry, Level, default_entropic_params, default_surface_params
+    from openaerolab_alpha_01_b200.surface import sphere_mesh
+    case = sphere_channel_case(64, 32, 32, diameter=10.0, centre_x=20.0, u_inlet=0.05, re=200.0)
+    g = Geometry(case.dom)
+    L = Level(g, "entropic")
+    L.init_equilibrium(case.rho, case.vel)
+    p = default_entropic_params(tau=float(case.params.tau), c_wale=0.2, u_inlet=0.05)
+    L.advance(p, 30)
+    tri = sphere_mesh(case.meta["centre"], 5.0, 24, 48)
+    L.set_surface(tri)
+    r = L.surface_forces(default_surface_params(tau=float(case.params.tau)), per_triangle=True)
+    _, rho, vel = L.state()
+    L.close()
+    g.close()
+    d = case.dom
+    dims = (d.bx_max, d.by_max, d.bz_max)
+    out, part = oracle_lib.surface_map(tri, rho.astype(np.float32), vel.astype(np.float32), d.obstacle,
+                                       block_ptr(d.coords, dims), dims, tau=float(case.params.tau), c_wale=0.2,
+                                       cs2=2.0 / 3.0)
+    per = r["per_triangle"]
+    ok = ~np.isnan(out[:, 0])
+    assert np.array_equal(np.isnan(per[:, 0]), ~ok)
+    assert np.array_equal(per[ok].view(np.uint32), out[ok].view(np.uint32))
+    F = part.sum(axis=0)
+    assert np.allclose(np.concatenate([r["pressure"], r["viscous"]]), F[:6], rtol=1e-12, atol=1e-15 * np.max(np.abs(F)))
