@@ -1443,8 +1443,10 @@ __global__ void __launch_bounds__(128) k_cumulant_gen(const StepArgs a, const in
     __syncthreads();
     if (tid < 3) a.force_part[(int64_t)blockIdx.x * 3 + tid] = ((s_mom[0][tid] + s_mom[1][tid]) + s_mom[2][tid]) + s_mom[3][tid];
     if (a.force_out) {
-      // the CTA that finishes last sums every CTA's partial in a fixed order (strided per thread,
-      // then a fixed tree), so the total does not depend on which CTA that is
+      // the CTA that finishes last sums every CTA's partial in a fixed order, so the total does
+      // not depend on which CTA that is: the order of the 256-lane strided sum and tree of the
+      // pool's per-member reduction (k_reduce3_segments), each thread carrying lanes t and
+      // t + 128, so that a case gets the same bits alone and in a pool
       __shared__ uint32_t s_last;
       __shared__ double s_red[3][128];
       __threadfence();
@@ -1452,11 +1454,14 @@ __global__ void __launch_bounds__(128) k_cumulant_gen(const StepArgs a, const in
       if (tid == 0) s_last = atomicAdd(a.force_ticket, 1u) == gridDim.x - 1 ? 1u : 0u;
       __syncthreads();
       if (s_last) {
-        double r0 = 0.0, r1 = 0.0, r2 = 0.0;
-        for (int64_t i = tid; i < (int64_t)gridDim.x; i += blockDim.x) {
+        double r0 = 0.0, r1 = 0.0, r2 = 0.0, q0 = 0.0, q1 = 0.0, q2 = 0.0;
+        for (int64_t i = tid; i < (int64_t)gridDim.x; i += 256) {
           r0 += __ldcg(a.force_part + 3 * i); r1 += __ldcg(a.force_part + 3 * i + 1); r2 += __ldcg(a.force_part + 3 * i + 2);
         }
-        s_red[0][tid] = r0; s_red[1][tid] = r1; s_red[2][tid] = r2;
+        for (int64_t i = tid + 128; i < (int64_t)gridDim.x; i += 256) {
+          q0 += __ldcg(a.force_part + 3 * i); q1 += __ldcg(a.force_part + 3 * i + 1); q2 += __ldcg(a.force_part + 3 * i + 2);
+        }
+        s_red[0][tid] = r0 + q0; s_red[1][tid] = r1 + q1; s_red[2][tid] = r2 + q2;
         __syncthreads();
         for (int w = 64; w > 0; w >>= 1) {
           if (tid < w) { s_red[0][tid] += s_red[0][tid + w]; s_red[1][tid] += s_red[1][tid + w]; s_red[2][tid] += s_red[2][tid + w]; }

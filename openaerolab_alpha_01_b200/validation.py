@@ -145,6 +145,8 @@ def sphere_drag(steps: int = 20000, avg_last: int = 5000, storages=("f64", "f32"
         d = {"cd_mean": cd, "cd_std": float(np.std(r["cd"][-avg_last:])),
              "cl_y_mean": float(np.mean(r["cl_y"][-avg_last:])), "cl_z_mean": float(np.mean(r["cl_z"][-avg_last:])),
              "ms_per_step": round(r["ms_per_step"], 4), "finite": r["finite"]}
+        bad = np.flatnonzero(~np.isfinite(r["cd"]))
+        d["first_nonfinite_step"] = int(bad[0]) + 1 if bad.size else None
         if win:
             d["cd_window_mean"] = float(np.mean(r["cd"][w0:w1]))
         if ref is not None and st != "f64":

@@ -113,3 +113,22 @@ def test_member_with_bouzidi_walls_matches_alone(oal, storage):
     for gg in geoms:
         gg.close()
     g.close()
+
+
+def test_large_channel_member_matches_alone(oal):
+    """A channel whose sphere spans more than 128 general-kernel CTAs: the drag summed by the
+    level's last CTA and by the pool's per-member reduction take the same order (same bits)."""
+    big = sphere_channel_case(128, 64, 64, diameter=24.0, centre_x=32.0, u_inlet=0.05, re=200.0)
+    small = taylor_green_case(16, u0=0.05, re=100.0, c_wale=0.2)
+    steps = 6
+    f, rho, vel, force, mm = alone(big, "f16", steps)
+    geoms = [Geometry(c.dom) for c in (small, big)]
+    B = Batch(storage="f16", max_real_blocks=1024, max_ghost_blocks=1024, max_mask_blocks=256, max_members=2)
+    ids = [B.add(g, c.params, c.rho, c.vel) for g, c in zip(geoms, (small, big))]
+    B.advance(steps)
+    assert np.array_equal(B.state(ids[1])[0], f)
+    assert np.array_equal(B.forces(ids[1]), force)
+    assert np.array_equal(B.mass_momentum(ids[1]), mm)
+    B.close()
+    for g in geoms:
+        g.close()
