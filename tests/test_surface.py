@@ -127,25 +127,33 @@ def test_gpu_surface_map_matches_oracle_bitwise(oal, oracle_lib, storage):
 @pytest.mark.gpu
 def test_gpu_surface_drag_beside_momentum_exchange(oal):
     """The reference's Cd method (surface stresses) and the momentum-exchange drag of the same
-    half-way sphere after the start-up transient: same sign and within 25 % of each other."""
+    half-way sphere at Re 100 after the start-up transient, at D = 16 and D = 32 cells. The surface
+    method reads the wall shear as u_t / d at the probe distance (1.5 cells) with a surrogate eddy
+    viscosity (surface.jl:180-240), so it underestimates the friction of a boundary layer a few
+    cells thick: it stays below the momentum exchange and approaches it with resolution, while the
+    pressure part changes little (measured on B200: ratios 0.66 and 0.78, pressure Cd 0.572 and
+    0.567)."""
     from openaerolab_alpha_01_b200.cases import sphere_channel_case
     from openaerolab_alpha_01_b200.solver import Geometry, Level
     from openaerolab_alpha_01_b200.surface import compute_aerodynamics, sphere_mesh
-    case = sphere_channel_case(128, 64, 64, diameter=16.0, centre_x=32.0, u_inlet=0.05, re=100.0)
-    g = Geometry(case.dom)
-    L = Level(g, storage="f32")
-    L.init_equilibrium(case.rho, case.vel)
-    L.advance(case.params, 3000)
-    mem = L.forces()[0]
-    area = np.pi * 8.0 ** 2
-    r = compute_aerodynamics(L, sphere_mesh(case.meta["centre"], 8.0), tau=float(case.params.tau), u_ref=0.05,
-                             area_ref=area)
-    L.close()
-    g.close()
-    cd_mem = mem / (0.5 * 0.05 ** 2 * area)
-    cd_surf = float(r["coefficients"][0])
-    assert cd_mem > 0 and cd_surf > 0
-    assert abs(cd_surf - cd_mem) / cd_mem < 0.25, (cd_surf, cd_mem)
+    out = []
+    for n, D, steps in ((128, 16.0, 3000), (256, 32.0, 8000)):
+        case = sphere_channel_case(n, n // 2, n // 2, diameter=D, centre_x=n / 4, u_inlet=0.05, re=100.0)
+        g = Geometry(case.dom)
+        L = Level(g, storage="f32")
+        L.init_equilibrium(case.rho, case.vel)
+        L.advance(case.params, steps)
+        area = np.pi * (D / 2) ** 2
+        cd_mem = L.forces()[0] / (0.5 * 0.05 ** 2 * area)
+        r = compute_aerodynamics(L, sphere_mesh(case.meta["centre"], D / 2), tau=float(case.params.tau), u_ref=0.05,
+                                 area_ref=area)
+        L.close()
+        g.close()
+        out.append((cd_mem, float(r["coefficients"][0]), float(r["pressure_coefficients"][0])))
+    (m16, s16, p16), (m32, s32, p32) = out
+    assert m16 > 0 and s16 > 0
+    assert 0.55 < s16 / m16 < 0.85 and s16 / m16 < s32 / m32 < 1.0
+    assert abs(p32 - p16) < 0.05 * p16
 
 
 @pytest.mark.gpu
