@@ -379,18 +379,22 @@ oal_status oal_level_set_nscbc(oal_level* L, const oal_nscbc_params* np);
 
 /* ---- launch tuning (no counterpart in the reference; results do not depend on it) ---------- */
 /* OAL_TUNE_PREFETCH_CTAS: the x-pair kernel's CTA j also bulk-prefetches into L2 the populations
- * and velocities of the CTA prefetch_ctas launches ahead in its launch (0 = off, the default). */
+ * and velocities of the CTA prefetch_ctas launches ahead in its launch (0 = off, the default).
+ * OAL_TUNE_PERSISTENT: 1 launches the x-pair kernel in its persistent form, as many CTAs as stay
+ * resident walking the launch's units (0 = one CTA per unit, the default). */
 #define OAL_TUNE_PREFETCH_CTAS 1
-#define OAL_TUNE_CANDIDATES 4
+#define OAL_TUNE_PERSISTENT 2
+#define OAL_TUNE_CANDIDATES 8
 oal_status oal_level_set_tuning(oal_level* L, int32_t key, int64_t value);
 oal_status oal_level_get_tuning(const oal_level* L, int32_t key, int64_t* value);
 /* The autotuner: times n_steps steps (CUDA events, after one untimed run of the same n_steps) for
- * each of the OAL_TUNE_CANDIDATES prefetch distances {0, 4, 8, 16} x the SM count, each from the
- * level's current state, which is restored afterwards (the level ends where it started), and
- * keeps the fastest. values[c] and ms_per_step[c] (host, nullable) report every candidate. Needs
- * device memory for one copy of the state. */
-oal_status oal_level_autotune(oal_level* L, const oal_step_params* p, int32_t n_steps, int64_t* values,
-                              double* ms_per_step);
+ * each of the OAL_TUNE_CANDIDATES settings (plain and persistent launch x prefetch distances
+ * {0, 4, 8, 16} x the SM count), each from the level's current state, which is restored
+ * afterwards (the level ends where it started), and keeps the fastest. prefetch[c],
+ * persistent[c] and ms_per_step[c] (host, nullable) report every candidate. Needs device memory
+ * for one copy of the state. */
+oal_status oal_level_autotune(oal_level* L, const oal_step_params* p, int32_t n_steps, int64_t* prefetch,
+                              int32_t* persistent, double* ms_per_step);
 /* Device pointers of the current state (for zero-copy interop): f, rho, vel. */
 oal_status oal_level_device_state(oal_level* L, void** f, void** rho, void** vel);
 /* Bytes of device memory this level holds. */
@@ -465,7 +469,8 @@ oal_status oal_batch_advance(oal_batch* B, int32_t n_steps, void* stream);
  * restored afterwards. */
 oal_status oal_batch_set_tuning(oal_batch* B, int32_t key, int64_t value);
 oal_status oal_batch_get_tuning(const oal_batch* B, int32_t key, int64_t* value);
-oal_status oal_batch_autotune(oal_batch* B, int32_t n_steps, int64_t* values, double* ms_per_step);
+oal_status oal_batch_autotune(oal_batch* B, int32_t n_steps, int64_t* prefetch, int32_t* persistent,
+                              double* ms_per_step);
 /* Member state in the reference layout (double); synchronises. Any pointer may be NULL. */
 oal_status oal_batch_get_state(oal_batch* B, int32_t member, double* f, double* rho, double* vel);
 /* Momentum-exchange force of the member's last collecting step (FP64, lattice units); synchronises. */

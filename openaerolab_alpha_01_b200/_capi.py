@@ -46,7 +46,8 @@ OAL_LEVEL_DENSE = 1
 OAL_LEVEL_ROUND_NEAREST = 2
 OAL_LEVEL_EXACT_MATH = 4
 OAL_TUNE_PREFETCH_CTAS = 1
-OAL_TUNE_CANDIDATES = 4
+OAL_TUNE_PERSISTENT = 2
+OAL_TUNE_CANDIDATES = 8
 
 OAL_SOLID_FULLWAY = 0
 OAL_SOLID_HALFWAY = 1
@@ -321,7 +322,7 @@ _SIGNATURES = {
     "oal_level_set_nscbc": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "oal_level_set_tuning": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int64]),
     "oal_level_get_tuning": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64)]),
-    "oal_level_autotune": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    "oal_level_autotune": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "oal_level_device_state": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                            C.POINTER(C.c_void_p)]),
     "oal_level_device_bytes": (C.c_int64, [C.c_void_p]),
@@ -341,7 +342,7 @@ _SIGNATURES = {
     "oal_batch_advance": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p]),
     "oal_batch_set_tuning": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int64]),
     "oal_batch_get_tuning": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64)]),
-    "oal_batch_autotune": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    "oal_batch_autotune": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "oal_batch_get_state": (C.c_int32, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "oal_batch_get_forces": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),
     "oal_batch_mass_momentum": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),

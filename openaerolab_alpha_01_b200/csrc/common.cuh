@@ -177,6 +177,8 @@ struct StepArgs {
   int32_t round_nearest;          // 16-bit codecs: round stored deviations to nearest (else stochastically)
   int32_t prefetch_ctas;          // x-pair kernel: CTA j also prefetches CTA j + prefetch_ctas's
                                   // populations and velocities into L2 (0 = off; launch tuning)
+  int32_t persistent;             // x-pair kernel: resident CTAs walk the units (launch tuning)
+  int32_t pairs_units;            // set by the launcher: units of a persistent launch (0 = one per CTA)
   const int32_t* fast_rec;        // x-pair kernel: per work entry 32 ints (27-entry neighbour row,
                                   // block coordinates + case, block index), in work-list order
   void* pi_neq;                   // CF_SGS_PI: post-collision Pi_neq (compute type, [6][nb*512]),

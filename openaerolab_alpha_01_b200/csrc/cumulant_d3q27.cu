@@ -21,6 +21,9 @@
 //                   half-way walls with FP64 momentum exchange), sponge, wall model, Guo forcing,
 //                   and the face conditions when the level has no ghost blocks (caller-owned
 //                   arrays).
+#include <algorithm>
+#include <utility>
+#include <vector>
 #include <type_traits>
 
 #include "common.cuh"
@@ -938,26 +941,23 @@ template <> __device__ __forceinline__ uint32_t pack_dev<float>(F2) { return 0u;
 
 // Library-owned block-major layout; IDX indexes words (pairs): block stride 27*256, direction
 // stride 256, row (y, z) stride 4 and 32.
-// POS: some case of the launch uses the positivity limiter (its code is left out otherwise).
-// GEN: some case of the launch relaxes with omega_bulk, omega3 or omega4 other than 1.
+// One unit (a block's OAL_PAIRS_THREADS / 32 z planes) of the x-pair step; `unit` and `n_units`
+// index the launch's units (the CTA's own in the plain form, a walked sequence in the persistent one).
 template <class S, class IDX, bool POS, bool GEN>
-__global__ void __launch_bounds__(OAL_PAIRS_THREADS, ((sizeof(S) == 4 || GEN || POS) ? OAL_PAIRS_WARPS_WIDE : OAL_PAIRS_WARPS) * 32 / OAL_PAIRS_THREADS) k_cumulant_pairs(const StepArgs a, const int32_t* __restrict__ work) {
+__device__ __forceinline__ void pairs_unit(const StepArgs& a, unsigned unit, unsigned n_units, IDX* s_wbase,
+                                           int32_t* s_nbr, int32_t* s_tail, CaseParams& s_cp, int32_t& s_pf) {
   constexpr bool DEV = !std::is_same<S, float>::value;  // 16-bit deviation codec
   constexpr float E = PairScale<DEV>::E;
   using W = typename PairWord<S>::W;
   using V = F2;
   using T = float;
   constexpr IDX wbst = 27 * kCells / 2, wkst = kCells / 2;
-  __shared__ IDX s_wbase[28];  // first word of each neighbour block
-  __shared__ int32_t s_nbr[28];
-  __shared__ int32_t s_tail[5];  // the block's coordinates and case (stochastic rounding), its index
-  __shared__ CaseParams s_cp;
   const int tid = threadIdx.x;
   // a CTA covers OAL_PAIRS_THREADS / 32 z planes of a block (one warp per plane); the block's
   // neighbour row, coordinates and index come in one coalesced 128-byte record
   constexpr int CPB = 256 / OAL_PAIRS_THREADS;
-  const int32_t* __restrict__ rec = a.fast_rec + (int64_t)(blockIdx.x / CPB) * 32;
-  const int part = blockIdx.x % CPB;
+  const int32_t* __restrict__ rec = a.fast_rec + (int64_t)(unit / CPB) * 32;
+  const int part = unit % CPB;
   if (tid < 32) {
     const int32_t v = rec[tid];
     if (tid < 27) {
@@ -969,10 +969,9 @@ __global__ void __launch_bounds__(OAL_PAIRS_THREADS, ((sizeof(S) == 4 || GEN || 
   }
   // L2 prefetch of a later CTA's data (the CTA prefetch_ctas ahead in this launch): its block
   // index now, the bulk prefetches once this CTA's own loads are in flight
-  __shared__ int32_t s_pf;
   if (tid == 32 % OAL_PAIRS_THREADS) {
-    const unsigned pf_cta = blockIdx.x + (unsigned)a.prefetch_ctas;
-    s_pf = (a.prefetch_ctas > 0 && pf_cta < gridDim.x) ? a.fast_rec[(int64_t)(pf_cta / CPB) * 32 + 31] : -1;
+    const unsigned pf_cta = unit + (unsigned)a.prefetch_ctas;
+    s_pf = (a.prefetch_ctas > 0 && pf_cta < n_units) ? a.fast_rec[(int64_t)(pf_cta / CPB) * 32 + 31] : -1;
   }
   // the case parameters: copied by the second warp, or by the first one in one-warp CTAs
   const int cw = OAL_PAIRS_THREADS >= 64 ? tid - 32 : tid;
@@ -996,7 +995,7 @@ __global__ void __launch_bounds__(OAL_PAIRS_THREADS, ((sizeof(S) == 4 || GEN || 
   if (tid < 30 && s_pf >= 0) {
     // one lane per direction: the later CTA's z planes of that direction are contiguous
     // (OAL_PAIRS_THREADS words); three lanes for its velocity components
-    const IDX pz = (IDX)((OAL_PAIRS_THREADS / 32) * ((blockIdx.x + (unsigned)a.prefetch_ctas) % CPB));
+    const IDX pz = (IDX)((OAL_PAIRS_THREADS / 32) * ((unit + (unsigned)a.prefetch_ctas) % CPB));
     if (tid < 27) {
       prefetch_l2(fin + (IDX)s_pf * wbst + (IDX)tid * wkst + 32 * pz, OAL_PAIRS_THREADS * (uint32_t)sizeof(W));
     } else if (cp.flags & CF_GRADIENTS) {
@@ -1136,6 +1135,29 @@ __global__ void __launch_bounds__(OAL_PAIRS_THREADS, ((sizeof(S) == 4 || GEN || 
     const V sc[4] = {c0, c1, c2, c3};
 #pragma unroll
     for (int k = 0; k < kQ27; ++k) o[k * wkst] = pair_word<S>(A[k] * sc[q27_d2(k)], k);
+  }
+
+}
+
+// POS: some case of the launch uses the positivity limiter (its code is left out otherwise).
+// GEN: some case of the launch relaxes with omega_bulk, omega3 or omega4 other than 1.
+// PERS: the persistent form, resident CTAs walking the launch's units (launch tuning).
+template <class S, class IDX, bool POS, bool GEN, bool PERS>
+__global__ void __launch_bounds__(OAL_PAIRS_THREADS, ((sizeof(S) == 4 || GEN || POS) ? OAL_PAIRS_WARPS_WIDE : OAL_PAIRS_WARPS) * 32 / OAL_PAIRS_THREADS) k_cumulant_pairs(const StepArgs a, const int32_t* __restrict__ work) {
+  (void)work;
+  __shared__ IDX s_wbase[28];  // first word of each neighbour block
+  __shared__ int32_t s_nbr[28];
+  __shared__ int32_t s_tail[5];  // the block's coordinates and case (stochastic rounding), its index
+  __shared__ CaseParams s_cp;
+  __shared__ int32_t s_pf;
+  if constexpr (PERS) {
+    const unsigned n_units = (unsigned)a.pairs_units;
+    for (unsigned unit = blockIdx.x; unit < n_units; unit += gridDim.x) {
+      if (unit != blockIdx.x) __syncthreads();  // the previous unit no longer reads shared memory
+      pairs_unit<S, IDX, POS, GEN>(a, unit, n_units, s_wbase, s_nbr, s_tail, s_cp, s_pf);
+    }
+  } else {
+    pairs_unit<S, IDX, POS, GEN>(a, blockIdx.x, gridDim.x, s_wbase, s_nbr, s_tail, s_cp, s_pf);
   }
 }
 
@@ -1727,15 +1749,38 @@ cudaError_t launch_fast(const StepArgs& a, const int32_t* work, int n_work, cuda
     else k_cumulant_fast<S, F2, int64_t><<<(unsigned)n_work * 2u, 128, 0, st>>>(a, work);
   } else {
     // x pairs; word indices (half the element count) decide the index width
-    const unsigned grid = (unsigned)n_work * (256u / OAL_PAIRS_THREADS);
+    const unsigned units = (unsigned)n_work * (256u / OAL_PAIRS_THREADS);
     const bool pos = (a.flags_any & CF_LIMITER_POSITIVITY) != 0, gen = (a.flags_any & CF_GENERAL_RATES) != 0;
+    auto go = [&](auto plain, auto pers) -> cudaError_t {
+      if (!a.persistent) {
+        plain<<<units, OAL_PAIRS_THREADS, 0, st>>>(a, work);
+        return cudaGetLastError();
+      }
+      // persistent: as many CTAs as stay resident on the device at once, each walking the units
+      static thread_local std::vector<std::pair<const void*, int>> resident;
+      int n = 0;
+      for (const auto& r : resident)
+        if (r.first == reinterpret_cast<const void*>(pers)) n = r.second;
+      if (n == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pers, OAL_PAIRS_THREADS, 0);
+        if (e != cudaSuccess) return e;
+        n = std::max(1, sms * per_sm);
+        resident.emplace_back(reinterpret_cast<const void*>(pers), n);
+      }
+      StepArgs b = a;
+      b.pairs_units = (int32_t)units;
+      pers<<<std::min(units, (unsigned)n), OAL_PAIRS_THREADS, 0, st>>>(b, work);
+      return cudaGetLastError();
+    };
     if (pos || gen) {
-      if (idx32) k_cumulant_pairs<S, uint32_t, true, true><<<grid, OAL_PAIRS_THREADS, 0, st>>>(a, work);
-      else k_cumulant_pairs<S, int64_t, true, true><<<grid, OAL_PAIRS_THREADS, 0, st>>>(a, work);
-    } else {
-      if (idx32) k_cumulant_pairs<S, uint32_t, false, false><<<grid, OAL_PAIRS_THREADS, 0, st>>>(a, work);
-      else k_cumulant_pairs<S, int64_t, false, false><<<grid, OAL_PAIRS_THREADS, 0, st>>>(a, work);
+      if (idx32) return go(k_cumulant_pairs<S, uint32_t, true, true, false>, k_cumulant_pairs<S, uint32_t, true, true, true>);
+      return go(k_cumulant_pairs<S, int64_t, true, true, false>, k_cumulant_pairs<S, int64_t, true, true, true>);
     }
+    if (idx32) return go(k_cumulant_pairs<S, uint32_t, false, false, false>, k_cumulant_pairs<S, uint32_t, false, false, true>);
+    return go(k_cumulant_pairs<S, int64_t, false, false, false>, k_cumulant_pairs<S, int64_t, false, false, true>);
   }
   return cudaGetLastError();
 }

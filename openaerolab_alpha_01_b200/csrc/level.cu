@@ -481,6 +481,7 @@ struct oal_level {
   void* pi_neq = nullptr;
   bool comp = false;        // the last step's compressible equilibrium (oal_level_pi_neq)
   int32_t prefetch_ctas = 0;  // launch tuning (OAL_TUNE_PREFETCH_CTAS)
+  int32_t persistent = 0;     // launch tuning (OAL_TUNE_PERSISTENT)
   // characteristic outlet (oal_level_set_nscbc): settings and the listed blocks
   oal_nscbc_params nscbc{};
   int32_t* d_nscbc_blocks = nullptr;
@@ -1638,6 +1639,7 @@ static oal_status enqueue_step(oal_level* L, const CaseParams& cp, cudaStream_t 
   a.flags_any = cp.flags;
   a.round_nearest = L->round_nearest ? 1 : 0;
   a.prefetch_ctas = L->prefetch_ctas;
+  a.persistent = L->persistent;
   a.pi_neq = L->pi_neq;
   if ((cp.flags & CF_SGS_PI) && !L->pi_neq) return set_error(OAL_E_UNSUPPORTED, "variable_nu_sgs 1 without its Pi_neq field");
   if (!L->dense) { a.force_out = L->d_force; a.force_ticket = L->d_ticket; }
@@ -1931,12 +1933,16 @@ struct StateSnapshot {
   ~StateSnapshot() { for (void* c : copy) cudaFree(c); }
 };
 
-// The prefetch distances the autotuner tries: {0, 4, 8, 16} x the SM count of the device.
-static cudaError_t tune_candidates(int device, int64_t* cand) {
+// The settings the autotuner tries: the plain and the persistent launch, each with the prefetch
+// distances {0, 4, 8, 16} x the SM count of the device.
+static cudaError_t tune_candidates(int device, int64_t* cand, int32_t* pers) {
   int nsm = 0;
   cudaError_t e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-  const int64_t mult[OAL_TUNE_CANDIDATES] = {0, 4, 8, 16};
-  for (int c = 0; c < OAL_TUNE_CANDIDATES; ++c) cand[c] = mult[c] * nsm;
+  const int64_t mult[4] = {0, 4, 8, 16};
+  for (int c = 0; c < OAL_TUNE_CANDIDATES; ++c) {
+    cand[c] = mult[c % 4] * nsm;
+    pers[c] = c / 4;
+  }
   return e;
 }
 
@@ -2004,10 +2010,12 @@ oal_status oal_level_set_nscbc(oal_level* L, const oal_nscbc_params* np) {
 
 oal_status oal_level_set_tuning(oal_level* L, int32_t key, int64_t value) {
   if (!L) return set_error(OAL_E_INVALID_ARG, "null level");
-  if (key != OAL_TUNE_PREFETCH_CTAS) return set_error(OAL_E_INVALID_ARG, "unknown tuning key %d", key);
-  if (value < 0 || value > (1 << 24)) return set_error(OAL_E_INVALID_ARG, "prefetch distance %lld", (long long)value);
-  if (L->prefetch_ctas != (int32_t)value) {
-    L->prefetch_ctas = (int32_t)value;
+  int32_t* slot = key == OAL_TUNE_PREFETCH_CTAS ? &L->prefetch_ctas : key == OAL_TUNE_PERSISTENT ? &L->persistent : nullptr;
+  if (!slot) return set_error(OAL_E_INVALID_ARG, "unknown tuning key %d", key);
+  if (value < 0 || value > (key == OAL_TUNE_PERSISTENT ? 1 : (1 << 24)))
+    return set_error(OAL_E_INVALID_ARG, "tuning key %d: value %lld", key, (long long)value);
+  if (*slot != (int32_t)value) {
+    *slot = (int32_t)value;
     release_graph(L);  // the captured launches hold the old value
   }
   return OAL_OK;
@@ -2015,13 +2023,14 @@ oal_status oal_level_set_tuning(oal_level* L, int32_t key, int64_t value) {
 
 oal_status oal_level_get_tuning(const oal_level* L, int32_t key, int64_t* value) {
   if (!L || !value) return set_error(OAL_E_INVALID_ARG, "null argument");
-  if (key != OAL_TUNE_PREFETCH_CTAS) return set_error(OAL_E_INVALID_ARG, "unknown tuning key %d", key);
-  *value = L->prefetch_ctas;
+  if (key == OAL_TUNE_PREFETCH_CTAS) *value = L->prefetch_ctas;
+  else if (key == OAL_TUNE_PERSISTENT) *value = L->persistent;
+  else return set_error(OAL_E_INVALID_ARG, "unknown tuning key %d", key);
   return OAL_OK;
 }
 
-oal_status oal_level_autotune(oal_level* L, const oal_step_params* p, int32_t n_steps, int64_t* values,
-                              double* ms_per_step) {
+oal_status oal_level_autotune(oal_level* L, const oal_step_params* p, int32_t n_steps, int64_t* prefetch,
+                              int32_t* persistent, double* ms_per_step) {
   if (!L || !p) return set_error(OAL_E_INVALID_ARG, "null argument");
   if (n_steps <= 0) return set_error(OAL_E_INVALID_ARG, "n_steps must be positive");
   if (L->kbc) return set_error(OAL_E_UNSUPPORTED, "autotune: D3Q27 levels (the D3Q39 kernel has no tuning key)");
@@ -2039,9 +2048,10 @@ oal_status oal_level_autotune(oal_level* L, const oal_step_params* p, int32_t n_
   if (e != cudaSuccess)
     return set_error(e == cudaErrorMemoryAllocation ? OAL_E_OUT_OF_MEMORY : OAL_E_CUDA, "autotune snapshot: %s", cudaGetErrorString(e));
   int64_t cand[OAL_TUNE_CANDIDATES];
-  OAL_CUDA_TRY(tune_candidates(L->g->device, cand));
+  int32_t pers[OAL_TUNE_CANDIDATES];
+  OAL_CUDA_TRY(tune_candidates(L->g->device, cand, pers));
   const int parity0 = L->parity;
-  const int32_t keep = L->prefetch_ctas;
+  const int32_t keep = L->prefetch_ctas, keep_p = L->persistent;
   cudaStream_t st = nullptr;
   OAL_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   oal_status s = OAL_OK;
@@ -2049,6 +2059,7 @@ oal_status oal_level_autotune(oal_level* L, const oal_step_params* p, int32_t n_
   int best_c = -1;
   for (int c = 0; c < OAL_TUNE_CANDIDATES && s == OAL_OK; ++c) {
     if ((s = oal_level_set_tuning(L, OAL_TUNE_PREFETCH_CTAS, cand[c])) != OAL_OK) break;
+    if ((s = oal_level_set_tuning(L, OAL_TUNE_PERSISTENT, pers[c])) != OAL_OK) break;
     double ms = 0.0;
     s = time_candidate([&](cudaStream_t q) { return oal_level_advance(L, p, n_steps, q); },
                        [&]() -> oal_status {
@@ -2057,7 +2068,8 @@ oal_status oal_level_autotune(oal_level* L, const oal_step_params* p, int32_t n_
                          return re == cudaSuccess ? OAL_OK : set_error(OAL_E_CUDA, "autotune restore: %s", cudaGetErrorString(re));
                        },
                        n_steps, st, &ms);
-    if (values) values[c] = cand[c];
+    if (prefetch) prefetch[c] = cand[c];
+    if (persistent) persistent[c] = pers[c];
     if (ms_per_step) ms_per_step[c] = ms;
     if (s == OAL_OK && (best_c < 0 || ms < best)) { best = ms; best_c = c; }
   }
@@ -2067,6 +2079,7 @@ oal_status oal_level_autotune(oal_level* L, const oal_step_params* p, int32_t n_
   L->parity = parity0;
   L->forces_valid = false;
   oal_level_set_tuning(L, OAL_TUNE_PREFETCH_CTAS, s == OAL_OK && best_c >= 0 ? cand[best_c] : keep);
+  oal_level_set_tuning(L, OAL_TUNE_PERSISTENT, s == OAL_OK && best_c >= 0 ? pers[best_c] : keep_p);
   if (s != OAL_OK) return s;
   if (re != cudaSuccess) return set_error(OAL_E_CUDA, "autotune restore: %s", cudaGetErrorString(re));
   return OAL_OK;
@@ -2689,6 +2702,7 @@ struct oal_batch {
   int graph_parity = -1;
   int64_t bytes = 0;
   int32_t prefetch_ctas = 0;  // launch tuning (OAL_TUNE_PREFETCH_CTAS)
+  int32_t persistent = 0;     // launch tuning (OAL_TUNE_PERSISTENT)
 };
 
 static void batch_release_graph(oal_batch* B) {
@@ -2807,6 +2821,7 @@ static oal_status batch_enqueue_step(oal_batch* B, int step_offset, cudaStream_t
   a.flags_any = B->flags_any;
   a.fast_rec = B->d_fast_rec;
   a.prefetch_ctas = B->prefetch_ctas;
+  a.persistent = B->persistent;
   a.n_blocks = (int32_t)B->R;
   a.n_total_blocks = (int32_t)(B->R + B->G);
   a.block_base = 0;
@@ -3120,10 +3135,12 @@ oal_status oal_batch_advance(oal_batch* B, int32_t n, void* stream) {
 
 oal_status oal_batch_set_tuning(oal_batch* B, int32_t key, int64_t value) {
   if (!B) return set_error(OAL_E_INVALID_ARG, "null batch");
-  if (key != OAL_TUNE_PREFETCH_CTAS) return set_error(OAL_E_INVALID_ARG, "unknown tuning key %d", key);
-  if (value < 0 || value > (1 << 24)) return set_error(OAL_E_INVALID_ARG, "prefetch distance %lld", (long long)value);
-  if (B->prefetch_ctas != (int32_t)value) {
-    B->prefetch_ctas = (int32_t)value;
+  int32_t* slot = key == OAL_TUNE_PREFETCH_CTAS ? &B->prefetch_ctas : key == OAL_TUNE_PERSISTENT ? &B->persistent : nullptr;
+  if (!slot) return set_error(OAL_E_INVALID_ARG, "unknown tuning key %d", key);
+  if (value < 0 || value > (key == OAL_TUNE_PERSISTENT ? 1 : (1 << 24)))
+    return set_error(OAL_E_INVALID_ARG, "tuning key %d: value %lld", key, (long long)value);
+  if (*slot != (int32_t)value) {
+    *slot = (int32_t)value;
     batch_release_graph(B);
   }
   return OAL_OK;
@@ -3131,12 +3148,14 @@ oal_status oal_batch_set_tuning(oal_batch* B, int32_t key, int64_t value) {
 
 oal_status oal_batch_get_tuning(const oal_batch* B, int32_t key, int64_t* value) {
   if (!B || !value) return set_error(OAL_E_INVALID_ARG, "null argument");
-  if (key != OAL_TUNE_PREFETCH_CTAS) return set_error(OAL_E_INVALID_ARG, "unknown tuning key %d", key);
-  *value = B->prefetch_ctas;
+  if (key == OAL_TUNE_PREFETCH_CTAS) *value = B->prefetch_ctas;
+  else if (key == OAL_TUNE_PERSISTENT) *value = B->persistent;
+  else return set_error(OAL_E_INVALID_ARG, "unknown tuning key %d", key);
   return OAL_OK;
 }
 
-oal_status oal_batch_autotune(oal_batch* B, int32_t n_steps, int64_t* values, double* ms_per_step) {
+oal_status oal_batch_autotune(oal_batch* B, int32_t n_steps, int64_t* prefetch, int32_t* persistent,
+                              double* ms_per_step) {
   if (!B) return set_error(OAL_E_INVALID_ARG, "null batch");
   if (n_steps <= 0) return set_error(OAL_E_INVALID_ARG, "n_steps must be positive");
   OAL_CUDA_TRY(cudaSetDevice(B->device));
@@ -3154,9 +3173,10 @@ oal_status oal_batch_autotune(oal_batch* B, int32_t n_steps, int64_t* values, do
   if (e != cudaSuccess)
     return set_error(e == cudaErrorMemoryAllocation ? OAL_E_OUT_OF_MEMORY : OAL_E_CUDA, "autotune snapshot: %s", cudaGetErrorString(e));
   int64_t cand[OAL_TUNE_CANDIDATES];
-  OAL_CUDA_TRY(tune_candidates(B->device, cand));
+  int32_t pers[OAL_TUNE_CANDIDATES];
+  OAL_CUDA_TRY(tune_candidates(B->device, cand, pers));
   const int parity0 = B->parity;
-  const int32_t keep = B->prefetch_ctas;
+  const int32_t keep = B->prefetch_ctas, keep_p = B->persistent;
   cudaStream_t st = nullptr;
   OAL_CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   oal_status s = OAL_OK;
@@ -3164,6 +3184,7 @@ oal_status oal_batch_autotune(oal_batch* B, int32_t n_steps, int64_t* values, do
   int best_c = -1;
   for (int c = 0; c < OAL_TUNE_CANDIDATES && s == OAL_OK; ++c) {
     if ((s = oal_batch_set_tuning(B, OAL_TUNE_PREFETCH_CTAS, cand[c])) != OAL_OK) break;
+    if ((s = oal_batch_set_tuning(B, OAL_TUNE_PERSISTENT, pers[c])) != OAL_OK) break;
     double ms = 0.0;
     s = time_candidate([&](cudaStream_t q) { return oal_batch_advance(B, n_steps, q); },
                        [&]() -> oal_status {
@@ -3172,7 +3193,8 @@ oal_status oal_batch_autotune(oal_batch* B, int32_t n_steps, int64_t* values, do
                          return re == cudaSuccess ? OAL_OK : set_error(OAL_E_CUDA, "autotune restore: %s", cudaGetErrorString(re));
                        },
                        n_steps, st, &ms);
-    if (values) values[c] = cand[c];
+    if (prefetch) prefetch[c] = cand[c];
+    if (persistent) persistent[c] = pers[c];
     if (ms_per_step) ms_per_step[c] = ms;
     if (s == OAL_OK && (best_c < 0 || ms < best)) { best = ms; best_c = c; }
   }
@@ -3182,6 +3204,7 @@ oal_status oal_batch_autotune(oal_batch* B, int32_t n_steps, int64_t* values, do
   B->parity = parity0;
   for (auto& M : B->mem) M.forces_valid = false;
   oal_batch_set_tuning(B, OAL_TUNE_PREFETCH_CTAS, s == OAL_OK && best_c >= 0 ? cand[best_c] : keep);
+  oal_batch_set_tuning(B, OAL_TUNE_PERSISTENT, s == OAL_OK && best_c >= 0 ? pers[best_c] : keep_p);
   if (s != OAL_OK) return s;
   if (re != cudaSuccess) return set_error(OAL_E_CUDA, "autotune restore: %s", cudaGetErrorString(re));
   return OAL_OK;

@@ -384,13 +384,27 @@ class Level:
     def prefetch_ctas(self, value: int) -> None:
         check(lib().oal_level_set_tuning(self.handle, capi.OAL_TUNE_PREFETCH_CTAS, int(value)))
 
+    @property
+    def persistent(self) -> bool:
+        v = C.c_int64()
+        check(lib().oal_level_get_tuning(self.handle, capi.OAL_TUNE_PERSISTENT, C.byref(v)))
+        return bool(v.value)
+
+    @persistent.setter
+    def persistent(self, value: bool) -> None:
+        check(lib().oal_level_set_tuning(self.handle, capi.OAL_TUNE_PERSISTENT, int(bool(value))))
+
     def autotune(self, params: capi.StepParams, n_steps: int = 20) -> dict:
         """Time every candidate launch tuning over n_steps from the current state (restored after
-        each) and keep the fastest: {"prefetch_ctas": chosen, "candidates": [(value, ms/step)]}."""
+        each) and keep the fastest: {"prefetch_ctas", "persistent": chosen, "candidates":
+        [(prefetch, persistent, ms/step)]}."""
         vals = np.zeros(capi.OAL_TUNE_CANDIDATES, np.int64)
+        pers = np.zeros(capi.OAL_TUNE_CANDIDATES, np.int32)
         ms = np.zeros(capi.OAL_TUNE_CANDIDATES)
-        check(lib().oal_level_autotune(self.handle, C.byref(params), int(n_steps), vals.ctypes.data, ms.ctypes.data))
-        return {"prefetch_ctas": self.prefetch_ctas, "candidates": [(int(v), float(t)) for v, t in zip(vals, ms)]}
+        check(lib().oal_level_autotune(self.handle, C.byref(params), int(n_steps), vals.ctypes.data, pers.ctypes.data,
+                                       ms.ctypes.data))
+        return {"prefetch_ctas": self.prefetch_ctas, "persistent": self.persistent,
+                "candidates": [(int(v), int(q), float(t)) for v, q, t in zip(vals, pers, ms)]}
 
     def pi_neq(self) -> np.ndarray:
         """Non-equilibrium stress of the current state (compute_pi_neq_kernel!,
@@ -478,12 +492,24 @@ class Batch:
     def prefetch_ctas(self, value: int) -> None:
         check(lib().oal_batch_set_tuning(self.handle, capi.OAL_TUNE_PREFETCH_CTAS, int(value)))
 
+    @property
+    def persistent(self) -> bool:
+        v = C.c_int64()
+        check(lib().oal_batch_get_tuning(self.handle, capi.OAL_TUNE_PERSISTENT, C.byref(v)))
+        return bool(v.value)
+
+    @persistent.setter
+    def persistent(self, value: bool) -> None:
+        check(lib().oal_batch_set_tuning(self.handle, capi.OAL_TUNE_PERSISTENT, int(bool(value))))
+
     def autotune(self, n_steps: int = 20) -> dict:
         """The pool's autotuner (oal_batch_autotune): the members' state is restored afterwards."""
         vals = np.zeros(capi.OAL_TUNE_CANDIDATES, np.int64)
+        pers = np.zeros(capi.OAL_TUNE_CANDIDATES, np.int32)
         ms = np.zeros(capi.OAL_TUNE_CANDIDATES)
-        check(lib().oal_batch_autotune(self.handle, int(n_steps), vals.ctypes.data, ms.ctypes.data))
-        return {"prefetch_ctas": self.prefetch_ctas, "candidates": [(int(v), float(t)) for v, t in zip(vals, ms)]}
+        check(lib().oal_batch_autotune(self.handle, int(n_steps), vals.ctypes.data, pers.ctypes.data, ms.ctypes.data))
+        return {"prefetch_ctas": self.prefetch_ctas, "persistent": self.persistent,
+                "candidates": [(int(v), int(q), float(t)) for v, q, t in zip(vals, pers, ms)]}
 
     def state(self, member: int):
         nb = self._geoms[member].dom.n_blocks

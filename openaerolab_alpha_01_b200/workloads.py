@@ -75,10 +75,10 @@ def run_batched(cases, steps: int, storage: str = "f16", chunk: int = 100):
     return e0.elapsed_time(e1) / 1e3, B, ids, geoms
 
 
-def run_plain_loop(cases, steps: int, storage: str = "f16", prefetch_ctas: int = 0):
+def run_plain_loop(cases, steps: int, storage: str = "f16", prefetch_ctas: int = 0, persistent: bool = False):
     """The cases one after another, one step call per step; returns (seconds, final states).
-    `prefetch_ctas`: the launch tuning every level uses (the batch's choice, for a like-for-like
-    comparison)."""
+    `prefetch_ctas`, `persistent`: the launch tuning every level uses (the batch's choice, for a
+    like-for-like comparison)."""
     import torch
     s = torch.cuda.Stream()
     levels = []
@@ -86,6 +86,7 @@ def run_plain_loop(cases, steps: int, storage: str = "f16", prefetch_ctas: int =
         g = Geometry(c.dom)
         L = Level(g, storage=storage)
         L.prefetch_ctas = prefetch_ctas
+        L.persistent = persistent
         L.init_equilibrium(c.rho, c.vel)
         L.perform_timestep(c.params, s)  # warm-up of the code path
         L.init_equilibrium(c.rho, c.vel)
@@ -105,7 +106,7 @@ def config4(steps: int = 2000, n_cases: int = 64, seed: int = 4, storage: str = 
     cases = config4_cases(n_cases, seed)
     cells = sum(c.dom.n_blocks * 512 for c in cases)
     tb, B, ids, geoms = run_batched(cases, steps, storage)
-    tp, levels = run_plain_loop(cases, steps, storage, B.tuning["prefetch_ctas"])
+    tp, levels = run_plain_loop(cases, steps, storage, B.tuning["prefetch_ctas"], B.tuning["persistent"])
     # batch invariance on the first members: bit-identical to the plain loop's result
     same = 0
     for i in range(min(check_members, len(cases))):

@@ -1,6 +1,7 @@
-"""Launch tuning and the autotuner (oal_level_autotune, oal_batch_autotune): the L2 prefetch
-distance of the x-pair kernel changes no result bit, the autotuner times every candidate, keeps
-the fastest and leaves the level or the pool in the state it found."""
+"""Launch tuning and the autotuner (oal_level_autotune, oal_batch_autotune): neither the L2
+prefetch distance nor the persistent launch of the x-pair kernel changes a result bit; the
+autotuner times every candidate, keeps the fastest and leaves the level or the pool in the state
+it found."""
 import numpy as np
 import pytest
 
@@ -12,14 +13,15 @@ from openaerolab_alpha_01_b200.solver import Batch, Geometry, Level
 
 
 @pytest.mark.parametrize("storage", ["f16", "bf16", "f32"])
-def test_prefetch_distance_changes_no_bit(oal, storage):
+def test_launch_tuning_changes_no_bit(oal, storage):
     case = sphere_channel_case(64, 32, 32, diameter=8.0, centre_x=16.0, u_inlet=0.05, re=200.0)
     g = Geometry(case.dom)
     out = []
-    for pf in (0, 148 * 4, 148 * 16):
+    for pf, pers in ((0, False), (148 * 4, False), (148 * 16, False), (0, True), (148 * 4, True)):
         L = Level(g, storage=storage)
         L.prefetch_ctas = pf
-        assert L.prefetch_ctas == pf
+        L.persistent = pers
+        assert L.prefetch_ctas == pf and L.persistent == pers
         L.init_equilibrium(case.rho, case.vel)
         for _ in range(3):
             L.perform_timestep(case.params)
@@ -42,11 +44,12 @@ def test_level_autotune_keeps_the_state(oal):
     after = L.state()
     for a, b in zip(before, after):
         assert np.array_equal(a, b)
-    vals = [v for v, _ in r["candidates"]]
-    assert len(vals) == capi.OAL_TUNE_CANDIDATES and vals[0] == 0 and r["prefetch_ctas"] in vals
-    assert all(t > 0 for _, t in r["candidates"])
-    best = min(r["candidates"], key=lambda c: c[1])
-    assert r["prefetch_ctas"] == best[0]
+    cands = [(v, q) for v, q, _ in r["candidates"]]
+    assert len(cands) == capi.OAL_TUNE_CANDIDATES and cands[0] == (0, 0) and (r["prefetch_ctas"], int(r["persistent"])) in cands
+    assert {q for _, q in cands} == {0, 1}
+    assert all(t > 0 for _, _, t in r["candidates"])
+    best = min(r["candidates"], key=lambda c: c[2])
+    assert (r["prefetch_ctas"], int(r["persistent"])) == best[:2]
     # stepping on after tuning equals stepping a level that was never tuned
     M = Level(g, storage="f16")
     M.init_equilibrium(case.rho, case.vel)
@@ -64,10 +67,11 @@ def test_batch_autotune_keeps_the_members(oal):
     B.advance(4)
     before = [B.state(m)[0] for m in ids]
     r = B.autotune(10)
-    assert r["prefetch_ctas"] in [v for v, _ in r["candidates"]]
+    assert (r["prefetch_ctas"], int(r["persistent"])) in [(v, q) for v, q, _ in r["candidates"]]
     for m, f in zip(ids, before):
         assert np.array_equal(B.state(m)[0], f)
     B.prefetch_ctas = 0
+    B.persistent = False
     B.advance(6)
     ref = [B.state(m)[0] for m in ids]
     B.close()
@@ -75,6 +79,7 @@ def test_batch_autotune_keeps_the_members(oal):
     C_ = Batch(storage="f16", max_real_blocks=1024, max_ghost_blocks=1024, max_mask_blocks=16, max_members=4)
     ids2 = [C_.add(g, c.params, c.rho, c.vel) for g, c in zip(geoms, cases)]
     C_.prefetch_ctas = 148 * 8
+    C_.persistent = True
     C_.advance(10)
     for m, f in zip(ids2, ref):
         assert np.array_equal(C_.state(m)[0], f)
