@@ -164,6 +164,15 @@ typedef struct oal_step_params {
   int32_t variable_nu_sgs;
   float c_pi;                    /* VARIABLE_NU_SGS_C_PI (default 0.2) */
   float nu_sgs_floor;            /* VARIABLE_NU_SGS_FLOOR (default 0.002) */
+  /* Spectral vanishing viscosity (kernel_svv_yz_d3q39.jl): the strength of the 5-point bi-Laplacian
+   * filter along x and along y and z on this level, 0 = off (the default). The reference applies
+   * SVV_X_EPSILON on levels <= SVV_X_MAX_LEVEL and SVV_YZ_EPSILON on levels >= SVV_YZ_MIN_LEVEL
+   * (1-based, timestep.jl:1577-1578); the caller passes the level's values. D3Q27: a post-pass after
+   * the step kernels, before the outlet and the wall corrections (timestep.jl:1576-1611); D3Q39:
+   * inside the step, after the post-collision guard (kernel_entropic_d3q39.jl:3256-3310).
+   * Library-owned levels (single, hierarchy and D3Q39) only. */
+  float svv_x_epsilon;
+  float svv_yz_epsilon;
 } oal_step_params;
 
 /* ---- library ---------------------------------------------------------------------------- */

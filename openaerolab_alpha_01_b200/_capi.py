@@ -99,6 +99,8 @@ class StepParams(C.Structure):
         ("variable_nu_sgs", C.c_int32),
         ("c_pi", C.c_float),
         ("nu_sgs_floor", C.c_float),
+        ("svv_x_epsilon", C.c_float),
+        ("svv_yz_epsilon", C.c_float),
     ]
 
 

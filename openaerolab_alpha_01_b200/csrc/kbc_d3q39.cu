@@ -155,6 +155,7 @@ struct KbcArgs {
   const float* sponge;      // [nb*512] or null: the sponge blend toward the inlet state
   const float* wdist;       // [nb*512] or null: wall distance, NaN where there is none
   int32_t sponge_blend;     // sponge_blend_distributions
+  float svv_x, svv_yz;      // spectral vanishing viscosity strengths (0 = off)
 };
 
 // the face fill of one step: every ghost slot a real cell pulls receives its face value
@@ -604,13 +605,83 @@ __global__ void __launch_bounds__(256) k_kbc_fill(const KbcFillArgs a) {
   a.f[((int64_t)g * Q + k) * 512 + ((sx & 7) | ((sy & 7) << 3) | ((sz & 7) << 6))] = v;
 }
 
+// Spectral vanishing viscosity inside the step (apply_svv_yz_d3q39_inline! and
+// apply_svv_x_d3q39_inline!, kernel_svv_yz_d3q39.jl:142-213 and :252-298, frame shift 0): the
+// post-collision f_k less eps times the 5-point bi-Laplacian of the step's INPUT populations along
+// y and z (YZ) or along x, centred on f_k itself; a tap past a missing or ghost block or in a solid
+// cell reads the cell's own input population (get_pop_neighbor_yz / _x, :78-116, 225-250). The
+// 4-moment correction f_k -= w_k (drho + c_k . dj / cs2) then restores the cell's mass and momentum.
+// the input populations and solid masks the taps read (passed by value: a reference to the
+// kernel's argument block would copy the whole block to local memory)
+struct SvvView {
+  const float* fin;
+  const int32_t* mslot;
+  const uint32_t* cmask;
+  int32_t nb;
+};
+
+__device__ __forceinline__ float svv_tap(const SvvView& v, const int32_t* s_nbr, int b, int x, int y, int z, int dx,
+                                         int dy, int dz, int k, float own) {
+  const int nx = x + dx, ny = y + dy, nz = z + dz;
+  const int ox = nx < 0 ? -1 : (nx > 7 ? 1 : 0), oy = ny < 0 ? -1 : (ny > 7 ? 1 : 0), oz = nz < 0 ? -1 : (nz > 7 ? 1 : 0);
+  const int bo = (ox | oy | oz) == 0 ? b : s_nbr[(ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)];
+  if (bo < 0 || bo >= v.nb) return own;
+  const int c = (nx & 7) | ((ny & 7) << 3) | ((nz & 7) << 6);
+  if (v.cmask) {
+    const int32_t sl = v.mslot[bo];
+    if (sl >= 0 && ((v.cmask[(int64_t)sl * 512 + c] >> 13) & 1u)) return own;
+  }
+  return v.fin[((int64_t)bo * Q + k) * 512 + c];
+}
+
+template <bool YZ>
+__device__ __forceinline__ void svv_axis(const SvvView a, const Tables& T, const int32_t* s_nbr, int b, int cell,
+                                      float eps, float* sf) {
+  const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
+  float d_rho = 0.0f, d_jx = 0.0f, d_jy = 0.0f, d_jz = 0.0f;
+#pragma unroll 1
+  for (int k = 0; k < Q; ++k) {
+    const float own = a.fin[((int64_t)b * Q + k) * 512 + cell];
+    const float fc = sf[k * kThreads];
+    float ff;
+    if (YZ) {
+      const float by = svv_tap(a, s_nbr, b, x, y, z, 0, -2, 0, k, own) - 4.0f * svv_tap(a, s_nbr, b, x, y, z, 0, -1, 0, k, own) +
+                       6.0f * fc - 4.0f * svv_tap(a, s_nbr, b, x, y, z, 0, 1, 0, k, own) +
+                       svv_tap(a, s_nbr, b, x, y, z, 0, 2, 0, k, own);
+      const float bz = svv_tap(a, s_nbr, b, x, y, z, 0, 0, -2, k, own) - 4.0f * svv_tap(a, s_nbr, b, x, y, z, 0, 0, -1, k, own) +
+                       6.0f * fc - 4.0f * svv_tap(a, s_nbr, b, x, y, z, 0, 0, 1, k, own) +
+                       svv_tap(a, s_nbr, b, x, y, z, 0, 0, 2, k, own);
+      ff = fc - eps * (by + bz);
+    } else {
+      const float bx = svv_tap(a, s_nbr, b, x, y, z, -2, 0, 0, k, own) - 4.0f * svv_tap(a, s_nbr, b, x, y, z, -1, 0, 0, k, own) +
+                       6.0f * fc - 4.0f * svv_tap(a, s_nbr, b, x, y, z, 1, 0, 0, k, own) +
+                       svv_tap(a, s_nbr, b, x, y, z, 2, 0, 0, k, own);
+      ff = fc - eps * bx;
+    }
+    const float diff = ff - fc;
+    d_rho += diff;
+    d_jx += diff * (float(kcx(k)) - 0.0f);
+    d_jy += diff * (float(kcy(k)) - 0.0f);
+    d_jz += diff * (float(kcz(k)) - 0.0f);
+    sf[k * kThreads] = ff;
+  }
+  const float inv_cs2 = 1.0f / CS2;
+#pragma unroll 1
+  for (int k = 0; k < Q; ++k) {
+    const float cx = float(kcx(k)) - 0.0f, cy = float(kcy(k)) - 0.0f, cz = float(kcz(k)) - 0.0f;
+    const float cu = cx * d_jx + cy * d_jy + cz * d_jz;
+    sf[k * kThreads] -= T.b[k][3].x * (d_rho + inv_cs2 * cu);
+  }
+}
+
 // One cell per thread (kernel_entropic_d3q39.jl:859-3368 on such a level). The thread's populations
 // live in its shared-memory column (the pulled f, then a_k, then the post-collision values) and the
 // per-direction loops run rolled over the CTA's tables, which keeps the step's code small enough to
 // stay in the instruction cache. f_eq is recomputed from its multipliers where a pass needs it.
 // EDGES: the level has domain faces or solid cells (the pin, bounce-back and gradient fall-backs
 // are compiled in); periodic boxes without obstacles run the instance without them.
-template <bool EDGES, bool FAST>
+// SVV: the spectral vanishing viscosity is compiled in (a.svv_x or a.svv_yz > 0).
+template <bool EDGES, bool FAST, bool SVV = false>
 __global__ void __launch_bounds__(kThreads, FAST ? KBC_FAST_MIN_BLOCKS : KBC_MIN_BLOCKS) k_kbc_step(const KbcArgs a) {
   __shared__ Tables T;
   __shared__ int32_t s_nbr[27];
@@ -1011,6 +1082,33 @@ __global__ void __launch_bounds__(kThreads, FAST ? KBC_FAST_MIN_BLOCKS : KBC_MIN
       }
     }
   }
+  if constexpr (SVV) {
+    // the filter after the post-collision guard, y-z first, then x; then the positivity
+    // re-enforcement of an add-on (kernel_entropic_d3q39.jl:3256-3318)
+    const SvvView v{a.fin, a.mslot, a.cmask, a.nb};
+    if (a.svv_yz > 0.0f) svv_axis<true>(v, T, s_nbr, b, cell, a.svv_yz, sf);
+    if (a.svv_x > 0.0f) svv_axis<false>(v, T, s_nbr, b, cell, a.svv_x, sf);
+    if (a.svv_yz > 0.0f || a.svv_x > 0.0f) {
+      float fmin_post = sf[0];
+#pragma unroll 1
+      for (int k = 1; k < Q; ++k) fmin_post = jmin(fmin_post, sf[k * kThreads]);
+      if (fmin_post < 0.0f) {
+        float blend = 1.0f;
+#pragma unroll 1
+        for (int k = 0; k < Q; ++k) {
+          const float fe = eq(T, k);
+          const float fneq = sf[k * kThreads] - fe;
+          if (fneq < 0.0f && fe > F_FLOOR) blend = jmin(blend, fe / (fe - fneq + F_FLOOR));
+        }
+        blend = jmax(blend, 0.0f);
+#pragma unroll 1
+        for (int k = 0; k < Q; ++k) {
+          const float fe = eq(T, k);
+          sf[k * kThreads] = fe + blend * (sf[k * kThreads] - fe);
+        }
+      }
+    }
+  }
   float* fo = a.fout + (int64_t)b * Q * 512 + cell;
 #pragma unroll 13
   for (int k = 0; k < Q; ++k) {
@@ -1206,6 +1304,10 @@ oal_status resolve(const oal_step_params* p, KbcArgs* a) {
   a->u_inlet = p->u_inlet; a->sigma0 = p->lambda_param; a->hrr_sigma = p->hrr_sigma;
   a->sponge_blend = p->sponge_blend_distributions == 1 ? 1 : 0;
   a->nu_floor = p->nu_sgs_lattice_floor; a->shock_nu_max = p->shock_nu_max;
+  if (!(p->svv_x_epsilon >= 0.0f) || !std::isfinite(p->svv_x_epsilon) || !(p->svv_yz_epsilon >= 0.0f) ||
+      !std::isfinite(p->svv_yz_epsilon))
+    return fail(OAL_E_INVALID_ARG, "svv_x_epsilon and svv_yz_epsilon must be finite and >= 0");
+  a->svv_x = p->svv_x_epsilon; a->svv_yz = p->svv_yz_epsilon;
   inlet_equilibrium(p->u_inlet, a->feq_inlet);
   for (int k = 0; k < Q; ++k) {
     const float fe = a->feq_inlet[k];
@@ -1239,7 +1341,11 @@ oal_status enqueue(KbcLevel* L, const KbcArgs& base, const oal_step_params* p_in
   }
   const unsigned grid = (unsigned)L->nb * 4;
   a.warm_gate = KBC_FAST_WARM_GATE;
-  if (L->exact_math) {
+  if (a.svv_x > 0.0f || a.svv_yz > 0.0f) {
+    // the filter's instances carry the domain-face and solid logic (a no-op on periodic boxes)
+    if (L->exact_math) k_kbc_step<true, false, true><<<grid, kThreads, 0, st>>>(a);
+    else k_kbc_step<true, true, true><<<grid, kThreads, 0, st>>>(a);
+  } else if (L->exact_math) {
     if (a.faces || a.cmask) k_kbc_step<true, false><<<grid, kThreads, 0, st>>>(a);
     else k_kbc_step<false, false><<<grid, kThreads, 0, st>>>(a);
   } else {

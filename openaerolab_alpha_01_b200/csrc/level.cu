@@ -14,6 +14,7 @@
 #include "cumulant_math.cuh"
 #include "../../include/oal.h"
 #include "bouzidi_d3q27.h"
+#include "svv_d3q27.h"
 #include "kbc_d3q39.h"
 #include "surface_d3q27.h"
 
@@ -482,6 +483,8 @@ struct oal_level {
   bool comp = false;        // the last step's compressible equilibrium (oal_level_pi_neq)
   int32_t prefetch_ctas = 0;  // launch tuning (OAL_TUNE_PREFETCH_CTAS)
   int32_t persistent = 0;     // launch tuning (OAL_TUNE_PERSISTENT)
+  // spectral vanishing viscosity of the step being enqueued (oal_step_params svv_*_epsilon)
+  float svv_x = 0.0f, svv_yz = 0.0f;
   // characteristic outlet (oal_level_set_nscbc): settings and the listed blocks
   oal_nscbc_params nscbc{};
   int32_t* d_nscbc_blocks = nullptr;
@@ -505,6 +508,9 @@ static oal_status resolve_params(const oal_step_params* p, const oal_geometry* g
     return set_error(OAL_E_INVALID_ARG, "solid_bc %d", p->solid_bc);
   if (p->variable_nu_sgs < 0 || p->variable_nu_sgs > 2)
     return set_error(OAL_E_INVALID_ARG, "variable_nu_sgs %d (0 off, 1 Pi_neq, 2 dynamic)", p->variable_nu_sgs);
+  if (!(p->svv_x_epsilon >= 0.0f) || !std::isfinite(p->svv_x_epsilon) || !(p->svv_yz_epsilon >= 0.0f) ||
+      !std::isfinite(p->svv_yz_epsilon))
+    return set_error(OAL_E_INVALID_ARG, "svv_x_epsilon and svv_yz_epsilon must be finite and >= 0");
   if (p->solid_bc == OAL_SOLID_BOUZIDI && p->collect_forces)
     return set_error(OAL_E_UNSUPPORTED, "collect_forces with OAL_SOLID_BOUZIDI: the momentum exchange would be the full-way "
                                         "wall's, computed before the Bouzidi correction; use the surface-stress forces");
@@ -1324,6 +1330,8 @@ oal_status oal_stream_collide(const oal_geometry* g, const oal_level_fields* fl,
   if (s != OAL_OK) return s;
   if (cp.flags & (CF_SGS_PI | CF_SGS_DYNAMIC))
     return set_error(OAL_E_UNSUPPORTED, "variable_nu_sgs: the Pi_neq field and the test filter belong to plain levels, not to caller-owned arrays (oal_stream_collide)");
+  if (p->svv_x_epsilon > 0.0f || p->svv_yz_epsilon > 0.0f)
+    return set_error(OAL_E_UNSUPPORTED, "the SVV filter is a post-pass of library-owned levels, not of caller-owned arrays (oal_stream_collide)");
   if (!fl->f_in || !fl->f_out || !fl->rho_out || !fl->vel_out || !fl->vel_in)
     return set_error(OAL_E_INVALID_ARG, "f_in, f_out, rho_out, vel_out and vel_in are required");
   if (fl->f_in == fl->f_out) return set_error(OAL_E_INVALID_ARG, "f_in and f_out must differ (pull scheme)");
@@ -1619,6 +1627,17 @@ oal_status oal_level_get_state(oal_level* L, double* f, double* rho, double* vel
   return check_level_error(L);
 }
 
+static_assert(sizeof(oal_step_params) == 160, "oal_step_params: 40 four-byte scalars");
+
+// The filter strengths of the steps about to be enqueued on L, with the filter kernel allowed its
+// shared memory (outside stream capture).
+static oal_status set_svv(oal_level* L, const oal_step_params* p) {
+  L->svv_x = p->svv_x_epsilon;
+  L->svv_yz = p->svv_yz_epsilon;
+  if (L->svv_x > 0.0f || L->svv_yz > 0.0f) OAL_CUDA_TRY(svv_prepare(L->storage));
+  return OAL_OK;
+}
+
 // Enqueue one step of L on st (no host synchronisation).
 static oal_status enqueue_step(oal_level* L, const CaseParams& cp, cudaStream_t st) {
   const oal_geometry* g = L->g;
@@ -1659,6 +1678,12 @@ static oal_status enqueue_step(oal_level* L, const CaseParams& cp, cudaStream_t 
   } else {
     OAL_CUDA_TRY(launch_by_storage(L->storage, g, a, PATH_GHOSTED, st, &L->ov));
   }
+  const bool svv = L->svv_x > 0.0f || L->svv_yz > 0.0f;
+  if (svv) {
+    // spectral vanishing viscosity right after the step kernels (timestep.jl:1576-1611)
+    OAL_CUDA_TRY(svv_enqueue(L->storage, a.f_in, a.f_out, pop_index(L), g->nb, g->d_nbr, g->nb, g->d_mslot,
+                             g->d_cmask, L->svv_x, L->svv_yz, st));
+  }
   if (L->nscbc.enabled && L->n_nscbc > 0) {
     // characteristic outlet after the step, before the wall corrections (timestep.jl:1617-1664)
     cudaError_t e = cudaErrorInvalidValue;
@@ -1672,9 +1697,9 @@ static oal_status enqueue_step(oal_level* L, const CaseParams& cp, cudaStream_t 
   }
   if ((cp.flags & CF_BOUZIDI) && L->bz.n > 0)
     OAL_CUDA_TRY(bouzidi_enqueue(L->bz, L->storage, a.f_out, pop_index(L), g->d_nbr, g->d_mslot, g->d_cmask, st));
-  if ((cp.flags & CF_SGS_PI) && (((cp.flags & CF_BOUZIDI) && L->bz.n > 0) || (L->nscbc.enabled && L->n_nscbc > 0))) {
-    // the Bouzidi correction or the outlet rewrote populations after the fused refresh: refresh
-    // Pi_neq again from the corrected state (timestep.jl:1818-1834)
+  if ((cp.flags & CF_SGS_PI) && (((cp.flags & CF_BOUZIDI) && L->bz.n > 0) || (L->nscbc.enabled && L->n_nscbc > 0) || svv)) {
+    // the filter, the Bouzidi correction or the outlet rewrote populations after the fused
+    // refresh: refresh Pi_neq again from the corrected state (timestep.jl:1818-1834)
     cudaError_t e = cudaErrorInvalidValue;
     switch (L->storage) {
       case OAL_STORE_F32: e = pi_neq_t<float, float, float>(L, p ^ 1, static_cast<float*>(L->pi_neq), st); break;
@@ -1711,6 +1736,7 @@ oal_status oal_level_step(oal_level* L, const oal_step_params* p, void* stream) 
   OAL_CUDA_TRY(cudaSetDevice(L->g->device));
   if ((s = prepare_fill(L, cp, static_cast<cudaStream_t>(stream))) != OAL_OK) return s;
   if ((s = prepare_sgs(L, cp, static_cast<cudaStream_t>(stream))) != OAL_OK) return s;
+  if ((s = set_svv(L, p)) != OAL_OK) return s;
   L->comp = (cp.flags & CF_COMPRESSIBLE) != 0;
   return enqueue_step(L, cp, static_cast<cudaStream_t>(stream));
 }
@@ -1727,6 +1753,7 @@ oal_status oal_level_advance(oal_level* L, const oal_step_params* p, int32_t n, 
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if ((s = prepare_fill(L, cp, st)) != OAL_OK) return s;
   if ((s = prepare_sgs(L, cp, st)) != OAL_OK) return s;
+  if ((s = set_svv(L, p)) != OAL_OK) return s;
   L->comp = (cp.flags & CF_COMPRESSIBLE) != 0;
   oal_step_params key = *p;
   if (!(cp.flags & CF_INLET_NOISE)) key.time_step_seed = 0;  // the seed only matters with inlet noise
@@ -2519,6 +2546,10 @@ oal_status oal_amr_advance(oal_amr* A, const oal_step_params* params, int32_t n,
       return set_error(OAL_E_UNSUPPORTED, "variable_nu_sgs: plain levels only, not the levels of a block-AMR hierarchy");
   }
   OAL_CUDA_TRY(cudaSetDevice(A->device));
+  for (int l = 0; l < nl; ++l) {
+    oal_status s = set_svv(A->lv[(size_t)l].L, &params[l]);
+    if (s != OAL_OK) return s;
+  }
   const int start = A->lv[0].L->parity;
   bool hit = A->exec && A->g_n == n && A->g_parity == start && (int)A->g_p.size() == nl;
   for (int l = 0; hit && l < nl; ++l) {
@@ -2977,6 +3008,8 @@ oal_status oal_batch_add(oal_batch* B, const oal_geometry* g, const oal_step_par
   if (s != OAL_OK) return s;
   if (cp.flags & (CF_SGS_PI | CF_SGS_DYNAMIC))
     return set_error(OAL_E_UNSUPPORTED, "variable_nu_sgs: plain levels only, not batched cases (oal_batch_*)");
+  if (p->svv_x_epsilon > 0.0f || p->svv_yz_epsilon > 0.0f)
+    return set_error(OAL_E_UNSUPPORTED, "the SVV filter: plain levels and hierarchies only, not batched cases (oal_batch_*)");
   if (cp.flags & CF_STORE_POST) return set_error(OAL_E_UNSUPPORTED, "store_post_collision needs caller-owned arrays");
   int32_t m = -1;
   for (int32_t i = 0; i < B->max_members; ++i)
@@ -3088,6 +3121,8 @@ oal_status oal_batch_set_params(oal_batch* B, int32_t m, const oal_step_params* 
   if (s != OAL_OK) return s;
   if (cp.flags & (CF_SGS_PI | CF_SGS_DYNAMIC))
     return set_error(OAL_E_UNSUPPORTED, "variable_nu_sgs: plain levels only, not batched cases (oal_batch_*)");
+  if (p->svv_x_epsilon > 0.0f || p->svv_yz_epsilon > 0.0f)
+    return set_error(OAL_E_UNSUPPORTED, "the SVV filter: plain levels and hierarchies only, not batched cases (oal_batch_*)");
   B->mem[(size_t)m].p = *p; B->mem[(size_t)m].cp = cp;
   B->dirty = true;
   return OAL_OK;

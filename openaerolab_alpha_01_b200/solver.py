@@ -95,6 +95,20 @@ def default_entropic_params(**overrides) -> capi.StepParams:
     return p
 
 
+def svv_epsilons(level_id: int, yz_enabled: bool = False, yz_epsilon: float = 0.002, yz_min_level: int = 4,
+                 x_enabled: bool = False, x_epsilon: float = 0.002, x_max_level: int = 1) -> dict:
+    """The spectral vanishing viscosity strengths of level ``level_id`` (1 = the coarsest), gated as
+    timestep.jl:1577-1578 gates them: y-z on levels >= ``yz_min_level``, x on levels <= ``x_max_level``
+    (config advanced.numerics.svv_yz / svv_x, config_loader.jl:2317-2332, whose defaults these are).
+    Returns the ``svv_x_epsilon`` / ``svv_yz_epsilon`` overrides of the level's step parameters."""
+    if yz_min_level < 1:
+        raise ValueError("svv_yz.min_level must be >= 1")
+    if yz_epsilon < 0 or x_epsilon < 0:
+        raise ValueError("SVV epsilons must be >= 0")
+    return dict(svv_yz_epsilon=float(yz_epsilon) if yz_enabled and level_id >= yz_min_level else 0.0,
+                svv_x_epsilon=float(x_epsilon) if x_enabled and level_id <= x_max_level else 0.0)
+
+
 @dataclass
 class BlockDomain:
     """Block topology and cell fields of one level (host arrays, reference semantics)."""

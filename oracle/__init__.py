@@ -52,6 +52,8 @@ def lib() -> C.CDLL:
             getattr(L, n).argtypes = [i32, i32, i32, i32] + [vp] * 14
             getattr(L, n).restype = C.c_int
         L.ora_pi_neq_f64.argtypes = [i32, vp, vp, vp, vp, i32, vp]
+        for n in ("ora_svv_d3q27_f64", "ora_svv_d3q27_f32"):
+            getattr(L, n).argtypes = [i32, vp, vp, C.c_float, C.c_float, vp, vp, vp]
         for n in ("ora_nscbc_outlet_f64", "ora_nscbc_outlet_f32"):
             getattr(L, n).argtypes = [i32, i32, i32, i32, vp, vp, i32, C.c_float, C.c_float, C.c_float, vp, vp, vp]
         L.ora_q19_tables.argtypes = [vp] * 6
@@ -192,6 +194,18 @@ def init_feq(rho, vel, compressible=0):
     return f
 
 
+def svv_d3q27(nb, nbr, obstacle, eps_x, eps_yz, f_in, f_out, f_post2=None):
+    """The spectral vanishing viscosity post-pass (apply_svv_d3q19_postcollision!,
+    kernel_svv_yz_d3q39.jl:426-458) on reference-layout arrays (27, nb, 512): f_out filtered in
+    place from f_in; f_post2 (or None) receives the same values."""
+    fn = lib().ora_svv_d3q27_f64 if f_out.dtype == np.float64 else lib().ora_svv_d3q27_f32
+    fn(int(nb), _p(nbr), _p(obstacle), float(eps_x), float(eps_yz), _p(f_in), _p(f_out), _p(f_post2))
+
+
+def _svv_on(params):
+    return params.svv_x_epsilon > 0 or params.svv_yz_epsilon > 0
+
+
 class OracleLevel:
     """Reference-layout state stepped by the CPU restatement (double or float)."""
 
@@ -233,10 +247,16 @@ class OracleLevel:
                     _p(self.wall_dist), C.addressof(params), _p(self.f), _p(self.g), None, _p(self.rho),
                     _p(self.vel_new), _p(self.vel), _p(force))
         assert rc == 0
+        if _svv_on(params):
+            # the filter after the step kernels (timestep.jl:1576-1611)
+            svv_d3q27(self.nb, self.nbr, self.obstacle, params.svv_x_epsilon, params.svv_yz_epsilon, self.f, self.g)
         self.f, self.g = self.g, self.f
         self.vel, self.vel_new = self.vel_new, self.vel
         if params.collect_forces:
             self.force = force
+        if _svv_on(params) and params.variable_nu_sgs == 1:
+            # the filter rewrote the populations after the refresh: Pi_neq of the filtered state
+            self.pi_neq[...] = self.state_pi_neq(params.compressible_corr)
         return self
 
     def step_bouzidi(self, params, bz):
@@ -258,6 +278,8 @@ class OracleLevel:
                     _p(self.wall_dist), C.addressof(p), _p(self.f), _p(self.g), _p(post), _p(self.rho),
                     _p(self.vel_new), _p(self.vel), _p(force))
         assert rc == 0
+        if _svv_on(p):
+            svv_d3q27(self.nb, self.nbr, self.obstacle, p.svv_x_epsilon, p.svv_yz_epsilon, self.f, self.g, post)
         cells = np.ascontiguousarray(bz["cells"], np.int32)
         q = np.ascontiguousarray(np.asarray(bz["q"], np.float16).astype(np.float32))
         fb = lib().ora_bouzidi_linear_f64 if self.dtype == np.float64 else lib().ora_bouzidi_linear_f32
@@ -367,6 +389,8 @@ class OracleAMR:
                     _p(Pa["rho_old"]), _p(Pa["vel_old"]), float(params[l - 1].tau), float(tw), 1)
         P.time_step_seed = seed
         assert rc == 0
+        if _svv_on(P):
+            svv_d3q27(L["nb"], L["nbr"], L["obstacle"], P.svv_x_epsilon, P.svv_yz_epsilon, f_in, f_out)
         bz = L["bz"]
         if bz is not None and P.solid_bc == 3:
             post = f_out.copy()  # the step stores the post-collision populations as its output

@@ -1217,6 +1217,73 @@ void nscbc_outlet(const Level& L, int all_blocks, float p_target, float sigma, f
   }
 }
 
+// Spectral vanishing viscosity post-pass (apply_svv_d3q19_postcollision!, kernel_svv_yz_d3q39.jl:
+// 426-458, with apply_svv_d3q19_inline!, :301-375, and the tap helpers get_pop_neighbor_x/_yz,
+// :225-250 and :78-116): for every fluid cell, each post-collision population f_k is filtered by
+// the 5-point bi-Laplacian of the step's INPUT populations along x (eps_x) and along y and z
+// (eps_yz), the centre tap being f_k itself; a tap in a solid cell or past a missing neighbour
+// block reads the cell's own input population. The 4-moment correction
+// f_k -= w_k (drho + c_k . dj / cs2) restores the cell's mass and momentum, then every population
+// is floored at 1e-12. f_out is filtered in place; f_post2, when given, receives the same values
+// (the reference's write of f_post_collision on a level with boundary cells).
+template <class T>
+void svv_post(const Level& L, float eps_x, float eps_yz, const T* f_in, T* f_out, T* f_post2) {
+  if (eps_x == 0.0f && eps_yz == 0.0f) return;
+  Arr<T> A{L.nb};
+  const T ex = T(eps_x), eyz = T(eps_yz);
+  const T inv_cs2 = T(1) / T(1.0 / 3.0);  // CS2_LATTICE
+  auto solid = [&](int x, int y, int z, int b) { return L.obstacle && L.obstacle[A.s(x, y, z, b)]; };
+  // the input population k at (x, y, z) + d (one axis), with the fall-backs of the tap helpers
+  auto tap = [&](int x, int y, int z, int b, int dx, int dy, int dz, int k) -> T {
+    const int nx = x + dx, ny = y + dy, nz = z + dz;
+    const int ox = nx < 0 ? -1 : (nx >= BS ? 1 : 0), oy = ny < 0 ? -1 : (ny >= BS ? 1 : 0),
+              oz = nz < 0 ? -1 : (nz >= BS ? 1 : 0);
+    if (ox == 0 && oy == 0 && oz == 0)
+      return solid(nx, ny, nz, b) ? f_in[A.f(x, y, z, b, k)] : f_in[A.f(nx, ny, nz, b, k)];
+    const int nbb = L.nbr[b + (int64_t)L.nb * ((ox + 1) + 3 * (oy + 1) + 9 * (oz + 1))];
+    if (nbb == 0) return f_in[A.f(x, y, z, b, k)];
+    const int lx = nx - BS * ox, ly = ny - BS * oy, lz = nz - BS * oz;
+    if (solid(lx, ly, lz, nbb - 1)) return f_in[A.f(x, y, z, b, k)];
+    return f_in[A.f(lx, ly, lz, nbb - 1, k)];
+  };
+#pragma omp parallel for schedule(static)
+  for (int b = 0; b < L.nb; ++b)
+    for (int z = 0; z < BS; ++z)
+      for (int y = 0; y < BS; ++y)
+        for (int x = 0; x < BS; ++x) {
+          if (solid(x, y, z, b)) continue;
+          T fl[Q];
+          T d_rho = T(0), d_jx = T(0), d_jy = T(0), d_jz = T(0);
+          for (int k = 0; k < Q; ++k) {
+            const T fc = f_out[A.f(x, y, z, b, k)];
+            T bilap = T(0);
+            if (eps_x > 0.0f)
+              bilap += ex * (tap(x, y, z, b, -2, 0, 0, k) - T(4) * tap(x, y, z, b, -1, 0, 0, k) + T(6) * fc -
+                             T(4) * tap(x, y, z, b, 1, 0, 0, k) + tap(x, y, z, b, 2, 0, 0, k));
+            if (eps_yz > 0.0f) {
+              bilap += eyz * (tap(x, y, z, b, 0, -2, 0, k) - T(4) * tap(x, y, z, b, 0, -1, 0, k) + T(6) * fc -
+                              T(4) * tap(x, y, z, b, 0, 1, 0, k) + tap(x, y, z, b, 0, 2, 0, k));
+              bilap += eyz * (tap(x, y, z, b, 0, 0, -2, k) - T(4) * tap(x, y, z, b, 0, 0, -1, k) + T(6) * fc -
+                              T(4) * tap(x, y, z, b, 0, 0, 1, k) + tap(x, y, z, b, 0, 0, 2, k));
+            }
+            const T ff = fc - bilap;
+            const T diff = ff - fc;
+            d_rho += diff;
+            d_jx += diff * T(TB.cx[k]);
+            d_jy += diff * T(TB.cy[k]);
+            d_jz += diff * T(TB.cz[k]);
+            fl[k] = ff;
+          }
+          for (int k = 0; k < Q; ++k) {
+            const T cu = T(TB.cx[k]) * d_jx + T(TB.cy[k]) * d_jy + T(TB.cz[k]) * d_jz;
+            fl[k] -= T(TB.w[k]) * (d_rho + inv_cs2 * cu);
+            const T fc = fl[k] < T(1e-12f) ? T(1e-12f) : fl[k];
+            f_out[A.f(x, y, z, b, k)] = fc;
+            if (f_post2) f_post2[A.f(x, y, z, b, k)] = fc;
+          }
+        }
+}
+
 }  // namespace
 
 // ---- linear Bouzidi wall (geometry/bouzidi_kernel.jl:150-380, default D3Q27 options) ---------
@@ -1444,6 +1511,20 @@ void ora_nscbc_outlet_f32(int32_t nb, int32_t nx, int32_t ny, int32_t nz, const 
                           int32_t all_blocks, float p_target, float sigma, float blend, float* f, float* rho, float* vel) {
   Level L = make_level(nb, nx, ny, nz, coords, nullptr, obstacle, nullptr, nullptr);
   nscbc_outlet<float>(L, all_blocks, p_target, sigma, blend, f, rho, vel);
+}
+
+// The spectral vanishing viscosity post-pass on a stepped level: f_in the step's input, f_out its
+// output (filtered in place), f_post2 null or a second array to receive the filtered values.
+void ora_svv_d3q27_f64(int32_t nb, const int32_t* nbr, const uint8_t* obstacle, float eps_x, float eps_yz,
+                       const double* f_in, double* f_out, double* f_post2) {
+  Level L = make_level(nb, 0, 0, 0, nullptr, nbr, obstacle, nullptr, nullptr);
+  svv_post<double>(L, eps_x, eps_yz, f_in, f_out, f_post2);
+}
+
+void ora_svv_d3q27_f32(int32_t nb, const int32_t* nbr, const uint8_t* obstacle, float eps_x, float eps_yz,
+                       const float* f_in, float* f_out, float* f_post2) {
+  Level L = make_level(nb, 0, 0, 0, nullptr, nbr, obstacle, nullptr, nullptr);
+  svv_post<float>(L, eps_x, eps_yz, f_in, f_out, f_post2);
 }
 
 // Pi_neq of a stored state (compute_pi_neq_kernel!, kernel_pi_neq.jl:39-180, D3Q27): out

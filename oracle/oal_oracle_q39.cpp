@@ -27,9 +27,13 @@
 //   alpha solvers (bisection, Newton, approximate,
 //   Taylor) and the entropy ....................... kernel_entropic_d3q39.jl:47-528, 3109-3150
 //   KBC update, post blend, post guard, output .... kernel_entropic_d3q39.jl:3153-3368
+//   sponge toward the inlet state, near-wall clamp  kernel_entropic_d3q39.jl:1662, 1787-1841, 2149-2168
+//   spectral vanishing viscosity (y-z, then x) and
+//   the positivity re-enforcement after it ....... kernel_entropic_d3q39.jl:3256-3310,
+//                                                   kernel_svv_yz_d3q39.jl:78-213, 225-298
 // Terms that vanish on such a level are written out where they change rounding (0 force, 0 frame
 // shift); switches that are off there are left out: shock sensor, Knudsen-adaptive tau, variable
-// nu_sgs / sigma, dynamic SGS, feathering, RR-LBM, SVV, Gendre correction, sponge, wall model.
+// nu_sgs / sigma, dynamic SGS, feathering, RR-LBM, Gendre correction, wall model.
 // min/max propagate NaN as Julia's do. exp and log are kbc::exp / kbc::log (Cody-Waite reduction
 // and series), shared with the CUDA kernel so the two agree bit for bit; the reference calls the
 // Float32 exp / log of its backend.
@@ -360,11 +364,66 @@ struct CellOut {
   float rho, u[3];
 };
 
+// The step's input populations around one cell, for the SVV taps: fin (8,8,8,nb,39), nbr (nb,27)
+// 1-based with 0 for a missing block, obstacle (8,8,8,nb) or null.
+struct SvvTaps {
+  const float* fin;
+  int64_t N;
+  const int32_t* nbr;
+  const uint8_t* obst;
+  int nb, b, x, y, z;
+  float eps_x, eps_yz;
+  // population k of (x, y, z) + d (one axis); the cell's own input population past a missing block
+  // or in a solid cell (get_pop_neighbor_yz / _x, kernel_svv_yz_d3q39.jl:78-116, 225-250)
+  float tap(int dx, int dy, int dz, int k) const {
+    const int64_t own = x + 8 * y + 64 * z + 512 * (int64_t)b;
+    const int nx = x + dx, ny = y + dy, nz = z + dz;
+    const int ox = nx < 0 ? -1 : (nx > 7 ? 1 : 0), oy = ny < 0 ? -1 : (ny > 7 ? 1 : 0), oz = nz < 0 ? -1 : (nz > 7 ? 1 : 0);
+    const int bo = (ox | oy | oz) == 0 ? b : nbr[b + (int64_t)nb * ((ox + 1) + 3 * (oy + 1) + 9 * (oz + 1))] - 1;
+    if (bo < 0) return fin[own + N * k];
+    const int64_t c = (nx - 8 * ox) + 8 * (ny - 8 * oy) + 64 * (nz - 8 * oz) + 512 * (int64_t)bo;
+    if (obst && obst[c]) return fin[own + N * k];
+    return fin[c + N * k];
+  }
+};
+
+// apply_svv_yz_d3q39_inline! (axis 1) and apply_svv_x_d3q39_inline! (axis 0), frame shift 0:
+// the bi-Laplacian of the input populations about the post-collision f_k, then the 4-moment
+// correction that restores the cell's mass and momentum.
+void svv_axis(const SvvTaps& t, int yz, float eps, float* fp) {
+  float d_rho = 0.0f, d_jx = 0.0f, d_jy = 0.0f, d_jz = 0.0f;
+  for (int k = 0; k < Q; ++k) {
+    const float fc = fp[k];
+    float ff;
+    if (yz) {
+      const float by = t.tap(0, -2, 0, k) - 4.0f * t.tap(0, -1, 0, k) + 6.0f * fc - 4.0f * t.tap(0, 1, 0, k) + t.tap(0, 2, 0, k);
+      const float bz = t.tap(0, 0, -2, k) - 4.0f * t.tap(0, 0, -1, k) + 6.0f * fc - 4.0f * t.tap(0, 0, 1, k) + t.tap(0, 0, 2, k);
+      ff = fc - eps * (by + bz);
+    } else {
+      const float bx = t.tap(-2, 0, 0, k) - 4.0f * t.tap(-1, 0, 0, k) + 6.0f * fc - 4.0f * t.tap(1, 0, 0, k) + t.tap(2, 0, 0, k);
+      ff = fc - eps * bx;
+    }
+    const float diff = ff - fc;
+    d_rho += diff;
+    d_jx += diff * (float(CX[k]) - 0.0f);
+    d_jy += diff * (float(CY[k]) - 0.0f);
+    d_jz += diff * (float(CZ[k]) - 0.0f);
+    fp[k] = ff;
+  }
+  const float inv_cs2 = 1.0f / CS2;
+  for (int k = 0; k < Q; ++k) {
+    const float cx = float(CX[k]) - 0.0f, cy = float(CY[k]) - 0.0f, cz = float(CZ[k]) - 0.0f;
+    const float cu = cx * d_jx + cy * d_jy + cz * d_jz;
+    fp[k] -= WT[k] * (d_rho + inv_cs2 * cu);
+  }
+}
+
 // One cell of the step after the pull: f (39, pulled), g (d u_a / d x_b, 9, previous velocity),
 // lam (13, warm start in, solution out), f_eq_inlet (39) -> fout (39), rho and u for the level's
 // macro arrays.
 void collide_cell(float* f, const float* g, const oal_step_params& P, const float* f_eq_inlet, float* lam,
-                  float* fout, CellOut& out, float sp = 0.0f, float wd = std::numeric_limits<float>::quiet_NaN()) {
+                  float* fout, CellOut& out, float sp = 0.0f, float wd = std::numeric_limits<float>::quiet_NaN(),
+                  const SvvTaps* svv = nullptr) {
   // moments of the pulled populations (kernel_entropic_d3q39.jl:1281-1287)
   float rho = 0.0f, jx = 0.0f, jy = 0.0f, jz = 0.0f;
   for (int k = 0; k < Q; ++k) {
@@ -647,6 +706,22 @@ void collide_cell(float* f, const float* g, const oal_step_params& P, const floa
       }
     }
   }
+  if (svv && (svv->eps_yz > 0.0f || svv->eps_x > 0.0f)) {
+    if (svv->eps_yz > 0.0f) svv_axis(*svv, 1, svv->eps_yz, fp);
+    if (svv->eps_x > 0.0f) svv_axis(*svv, 0, svv->eps_x, fp);
+    // positivity re-enforcement after the add-on (:3296-3318)
+    float fmin_post = fp[0];
+    for (int k = 1; k < Q; ++k) fmin_post = minf(fmin_post, fp[k]);
+    if (fmin_post < 0.0f) {
+      float blend = 1.0f;
+      for (int k = 0; k < Q; ++k) {
+        const float fneq = fp[k] - feq[k];
+        if (fneq < 0.0f && feq[k] > F_FLOOR) blend = minf(blend, feq[k] / (feq[k] - fneq + F_FLOOR));
+      }
+      blend = maxf(blend, 0.0f);
+      for (int k = 0; k < Q; ++k) fp[k] = feq[k] + blend * (fp[k] - feq[k]);
+    }
+  }
   for (int k = 0; k < Q; ++k) {
     float fc = fp[k];
     if (!(fc == fc) || fc > 1e3f) fc = feq[k];
@@ -767,7 +842,8 @@ void ora_q39_step(int32_t nb, const int32_t* nbr, const oal_step_params* P, cons
       for (int m = 0; m < 13; ++m) la[m] = lam[ci + N * m];
       float fo[Q];
       CellOut o;
-      collide_cell(f, g, *P, f_eq_inlet, la, fo, o);
+      const SvvTaps taps{fin, N, nbr, nullptr, nb, b, x, y, z, P->svv_x_epsilon, P->svv_yz_epsilon};
+      collide_cell(f, g, *P, f_eq_inlet, la, fo, o, 0.0f, std::numeric_limits<float>::quiet_NaN(), &taps);
       for (int m = 0; m < 13; ++m) lam[ci + N * m] = la[m];
       for (int k = 0; k < Q; ++k) fout[ci + N * k] = fo[k];
       rho_out[ci] = o.rho;
@@ -830,8 +906,9 @@ void ora_q39_step_ex(int32_t nb, const int32_t* nbr, const int32_t* coords, int3
       for (int m = 0; m < 13; ++m) la[m] = lam[ci + N * m];
       float fo[Q];
       CellOut o;
+      const SvvTaps taps{fin, N, nbr, obstacle, nb, b, x, y, z, P->svv_x_epsilon, P->svv_yz_epsilon};
       collide_cell(f, g, *P, f_eq_inlet, la, fo, o, sponge ? sponge[ci] : 0.0f,
-                   wall_dist ? wall_dist[ci] : std::numeric_limits<float>::quiet_NaN());
+                   wall_dist ? wall_dist[ci] : std::numeric_limits<float>::quiet_NaN(), &taps);
       for (int m = 0; m < 13; ++m) lam[ci + N * m] = la[m];
       for (int k = 0; k < Q; ++k) fout[ci + N * k] = fo[k];
       rho_out[ci] = o.rho;

@@ -55,7 +55,8 @@ def test_default_params_follow_config_loader(oal):
     assert p.adaptive_omega4 == 1 and abs(p.lambda_param - 1 / 6) < 1e-7
     assert p.limiter_type == capi.OAL_LIMITER_FACTORED and p.compressible_corr == 0
     assert p.wall_model_active == 0 and p.wall_model_max_distance == 10.0
-    assert C.sizeof(capi.StepParams) == 34 * 4 + 4 * 4  # 34 scalars + 4 reserved words
+    assert C.sizeof(capi.StepParams) == 4 * len(capi.StepParams._fields_) == 160  # 40 four-byte scalars
+    assert p.svv_x_epsilon == 0.0 and p.svv_yz_epsilon == 0.0  # SVV off (config_loader.jl:660-669)
 
 
 @pytest.mark.parametrize("dims,mask", [((2, 2, 2), 7), ((4, 2, 3), 0), ((3, 1, 2), 2), ((1, 1, 1), 7), ((5, 3, 2), 5)])

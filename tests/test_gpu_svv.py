@@ -1,0 +1,230 @@
+"""Spectral vanishing viscosity on the GPU against the oracle (kernel_svv_yz_d3q39.jl).
+
+D3Q27 (the post-pass after the step kernels, timestep.jl:1576-1611): the filtered step against the
+oracle's at the plain step's tolerances (FP64 1e-11, FP32 2e-5, FP16 deviation storage 2e-3), on
+a periodic Taylor-Green box and on the sphere channel (domain edges and solid taps); the pass in
+isolation — the oracle's filter applied to the GPU's own unfiltered step — bit for bit in F32 and
+F64 storage and within one storage step in FP16/BF16; with variable nu_sgs the Pi_neq field of the
+filtered state; graph replay; hierarchy levels; the refusals.
+D3Q39 (inside the KBC step): bit for bit against the oracle with exact math, on a periodic box
+and on the sphere channel, and the fast path within the D3Q39 tolerance.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+from openaerolab_alpha_01_b200 import _capi as capi
+from openaerolab_alpha_01_b200.cases import sphere_channel_case, taylor_green_case
+from openaerolab_alpha_01_b200.solver import Batch, Geometry, Level, default_entropic_params
+
+
+def rel(a, b):
+    return float(np.max(np.abs(np.asarray(a, np.float64) - np.asarray(b, np.float64))) / np.max(np.abs(b)))
+
+
+def with_svv(params, eps_x=0.002, eps_yz=0.004, **kw):
+    p = capi.StepParams.from_buffer_copy(params)
+    p.svv_x_epsilon = eps_x
+    p.svv_yz_epsilon = eps_yz
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+@pytest.fixture(scope="module")
+def tgv():
+    return taylor_green_case(16, u0=0.08, re=200.0, c_wale=0.2)
+
+
+@pytest.fixture(scope="module")
+def channel():
+    return sphere_channel_case(32, 16, 16, diameter=6.0, centre_x=10.0, u_inlet=0.05, re=100.0)
+
+
+def run_pair(oracle, case, p, storage, dtype, steps, layout="block"):
+    g = Geometry(case.dom)
+    L = Level(g, storage=storage, layout=layout)
+    L.init_equilibrium(case.rho, case.vel)
+    d = case.dom
+    O = oracle.OracleLevel(d.coords, d.neighbor_table, d.shape, obstacle=d.obstacle, sponge=d.sponge,
+                           wall_dist=d.wall_dist, dtype=dtype)
+    O.init_equilibrium(case.rho, case.vel)
+    for i in range(steps):
+        p.time_step_seed = i
+        L.perform_timestep(p)
+        O.step(p)
+    f, rho, vel = L.state()
+    out = dict(f=f, rho=rho, vel=vel, pi=L.pi_neq() if p.variable_nu_sgs == 1 else None)
+    L.close(); g.close()
+    return out, O
+
+
+@pytest.mark.parametrize("storage,dtype,tol,layout", [("f64", np.float64, 1e-11, "block"),
+                                                      ("f32", np.float32, 2e-5, "block"),
+                                                      ("f32", np.float32, 2e-5, "dense"),
+                                                      ("f16", np.float64, 2e-3, "block")])
+def test_taylor_green(oal, oracle_lib, tgv, storage, dtype, tol, layout):
+    p = with_svv(tgv.params)
+    g, O = run_pair(oracle_lib, tgv, p, storage, dtype, 12, layout)
+    assert rel(g["f"], O.f) < tol
+    assert rel(g["vel"], O.vel) < tol * 50
+
+
+@pytest.mark.parametrize("storage,dtype,tol", [("f64", np.float64, 1e-11), ("f32", np.float32, 2e-5)])
+def test_sphere_channel(oal, oracle_lib, channel, storage, dtype, tol):
+    p = with_svv(channel.params, eps_x=0.003, eps_yz=0.005)
+    g, O = run_pair(oracle_lib, channel, p, storage, dtype, 10)
+    assert rel(g["f"], O.f) < tol
+
+
+@pytest.mark.parametrize("storage,atol_w", [("f64", 0.0), ("f32", 0.0), ("f16", 2.0 ** -11), ("bf16", 2.0 ** -7)])
+def test_pass_in_isolation(oal, oracle_lib, channel, storage, atol_w):
+    """Two levels step alike; the last step of one is filtered. The oracle's filter applied to
+    (state before, unfiltered state after) gives the filtered state: bit for bit where the storage
+    holds the compute type; within one storage step of the deviation f/w - 1 in FP16/BF16 (the GPU
+    rounds the filtered value once, the decoded inputs of the oracle are already rounded)."""
+    d = channel.dom
+    g = Geometry(d)
+    A, B = Level(g, storage=storage), Level(g, storage=storage)
+    for L in (A, B):
+        L.init_equilibrium(channel.rho, channel.vel)
+        L.execute_timestep_batch(channel.params, 6)
+    s0 = A.state()[0]
+    assert np.array_equal(s0, B.state()[0])
+    p = with_svv(channel.params, eps_x=0.003, eps_yz=0.005)
+    p.time_step_seed = 6
+    q = capi.StepParams.from_buffer_copy(channel.params)
+    q.time_step_seed = 6
+    A.perform_timestep(q)
+    B.perform_timestep(p)
+    s1, s2 = A.state()[0], B.state()[0]
+    A.close(); B.close(); g.close()
+    dt = np.float64 if storage == "f64" else np.float32
+    fin = np.ascontiguousarray(s0.astype(dt))
+    fout = np.ascontiguousarray(s1.astype(dt))
+    oracle_lib.svv_d3q27(d.n_blocks, np.ascontiguousarray(d.neighbor_table, np.int32),
+                         np.ascontiguousarray(d.obstacle, np.uint8), 0.003, 0.005, fin, fout)
+    assert not np.array_equal(s1, s2)
+    if atol_w == 0.0:
+        assert np.array_equal(fout.astype(np.float64), s2)
+    else:
+        w = oracle_lib.d3q27_tables()["w"][:, None, None]
+        assert np.max(np.abs(fout - s2) / w) <= atol_w * 1.01
+
+
+def test_variable_nu_sgs_refreshes_after_the_filter(oal, oracle_lib, tgv):
+    p = with_svv(tgv.params, variable_nu_sgs=1, nu_sgs_floor=0.0, c_pi=0.2)
+    g, O = run_pair(oracle_lib, tgv, p, "f64", np.float64, 8)
+    assert rel(g["f"], O.f) < 1e-11
+    assert np.max(np.abs(g["pi"] - O.pi_neq)) < 1e-11 * np.max(np.abs(O.pi_neq)) + 1e-15
+
+
+def test_graph_replay_equals_steps(oal, channel):
+    g = Geometry(channel.dom)
+    p = with_svv(channel.params)
+    A, B = Level(g, storage="f32"), Level(g, storage="f32")
+    for L in (A, B):
+        L.init_equilibrium(channel.rho, channel.vel)
+    for i in range(8):
+        p.time_step_seed = i
+        A.perform_timestep(p)
+    p.time_step_seed = 0
+    B.execute_timestep_batch(p, 8)
+    assert np.array_equal(A.state()[0], B.state()[0])
+    A.close(); B.close(); g.close()
+
+
+def test_refusals(oal, channel, tgv):
+    g = Geometry(channel.dom)
+    L = Level(g, storage="f32")
+    L.init_equilibrium(channel.rho, channel.vel)
+    with pytest.raises(capi.OALError):
+        L.perform_timestep(with_svv(channel.params, eps_x=-1e-3))
+    with pytest.raises(capi.OALError):
+        L.perform_timestep(with_svv(channel.params, eps_yz=float("nan")))
+    L.close()
+    B = Batch(storage="f32", max_real_blocks=64, max_ghost_blocks=64, max_mask_blocks=16, max_members=2)
+    with pytest.raises(capi.OALError):
+        B.add(g, with_svv(channel.params), channel.rho, channel.vel)
+    B.close(); g.close()
+
+
+def test_hierarchy_levels(oal, oracle_lib):
+    """A 3-level periodic hierarchy with the reference's gating at min_level 2 / max_level 1: the
+    y-z filter on the two finer levels, the x filter on the coarsest; FP64 against the oracle's
+    recursion at the hierarchy tolerance (1e-10 of max |f|)."""
+    from openaerolab_alpha_01_b200 import amr
+    from openaerolab_alpha_01_b200.solver import svv_epsilons
+    from .test_gpu_amr import compare, fields, run_pair as amr_pair
+    from .test_oracle_amr import hierarchy, params
+    doms = hierarchy(oracle_lib, 3)
+    P = params(amr.level_taus(0.52, 3), c_wale=0.2)
+    for l, p in enumerate(P):
+        for k, v in svv_epsilons(l + 1, yz_enabled=True, yz_epsilon=0.004, yz_min_level=2, x_enabled=True,
+                                 x_epsilon=0.003, x_max_level=1).items():
+            setattr(p, k, v)
+    assert P[0].svv_x_epsilon > 0 and P[0].svv_yz_epsilon == 0 and P[2].svv_yz_epsilon > 0
+    rho_fn, vel_fn = fields()
+    H, ora = amr_pair((oracle_lib, amr, None), doms, P, "f64", 3, rho_fn, vel_fn)
+    compare(H, ora, 3, 1e-10)
+    H.close()
+
+
+# ---- D3Q39 ------------------------------------------------------------------------------------
+
+def same_bits(a, b):
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    return a.shape == b.shape and np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def q39_channel(oracle, math):
+    case = sphere_channel_case(32, 16, 16, diameter=6.0, centre_x=12.0, u_inlet=0.05, re=200.0)
+    d = case.dom
+    g = Geometry(d)
+    lvl = Level(g, "entropic", math=math)
+    rng = np.random.default_rng(5)
+    vel = case.vel + 0.005 * rng.standard_normal(case.vel.shape) * (d.obstacle == 0)
+    lvl.init_equilibrium(case.rho, vel)
+    ora = oracle.OracleQ39Level(d.neighbor_table, d.coords, d.shape, d.obstacle).init_equilibrium(case.rho, vel)
+    return g, lvl, ora
+
+
+@pytest.mark.parametrize("eps_x,eps_yz", [(0.0, 0.004), (0.003, 0.0), (0.003, 0.004)])
+def test_q39_channel_bitwise(oal, oracle_lib, eps_x, eps_yz):
+    g, lvl, ora = q39_channel(oracle_lib, "exact")
+    p = default_entropic_params(tau=0.56, c_wale=0.2, u_inlet=0.05, svv_x_epsilon=eps_x, svv_yz_epsilon=eps_yz)
+    for i in range(4):
+        p.time_step_seed = 3 + i
+        lvl.step(p)
+        ora.step(p)
+    f, rho, vel = lvl.state()
+    assert same_bits(f, ora.f), np.abs(f - ora.f).max()
+    assert same_bits(vel, ora.vel) and same_bits(rho, ora.rho)
+    lvl.close(); g.close()
+
+
+def test_q39_periodic_bitwise_and_fast(oal, oracle_lib):
+    from openaerolab_alpha_01_b200 import solver
+    dom = solver.build_box(2, 2, 2, periodic=(True, True, True))
+    gx, gy, gz = dom.cell_positions()
+    vel = np.zeros((3, dom.n_blocks, 512))
+    vel[0] = 0.06 * np.sin(2 * np.pi * (gy - 0.5) / 16) + 0.01 * np.where(gz % 2 == 0, 1.0, -1.0)
+    vel[1] = 0.04 * np.cos(2 * np.pi * (gx - 0.5) / 16)
+    rho = np.ones((dom.n_blocks, 512))
+    p = default_entropic_params(tau=0.53, c_wale=0.1, svv_x_epsilon=0.002, svv_yz_epsilon=0.006)
+    g = Geometry(dom)
+    ex = Level(g, "entropic", math="exact")
+    fa = Level(g, "entropic")
+    for L in (ex, fa):
+        L.init_equilibrium(rho, vel)
+    ora = oracle_lib.OracleQ39Level(dom.neighbor_table).init_equilibrium(rho, vel)
+    for i in range(5):
+        ex.step(p)
+        fa.step(p)
+        ora.step(p)
+    f = ex.state()[0]
+    assert same_bits(f, ora.f), np.abs(f - ora.f).max()
+    assert rel(fa.state()[0], ora.f) < 2e-3   # the fast path's bound (CUDA's expf / logf)
+    ex.close(); fa.close(); g.close()
