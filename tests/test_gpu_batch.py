@@ -123,7 +123,7 @@ def test_large_channel_member_matches_alone(oal):
     steps = 6
     f, rho, vel, force, mm = alone(big, "f16", steps)
     geoms = [Geometry(c.dom) for c in (small, big)]
-    B = Batch(storage="f16", max_real_blocks=1024, max_ghost_blocks=1024, max_mask_blocks=256, max_members=2)
+    B = Batch(storage="f16", max_real_blocks=1100, max_ghost_blocks=1100, max_mask_blocks=256, max_members=2)
     ids = [B.add(g, c.params, c.rho, c.vel) for g, c in zip(geoms, (small, big))]
     B.advance(steps)
     assert np.array_equal(B.state(ids[1])[0], f)
