@@ -1629,12 +1629,10 @@ oal_status oal_level_get_state(oal_level* L, double* f, double* rho, double* vel
 
 static_assert(sizeof(oal_step_params) == 160, "oal_step_params: 40 four-byte scalars");
 
-// The filter strengths of the steps about to be enqueued on L, with the filter kernel allowed its
-// shared memory (outside stream capture).
+// The filter strengths of the steps about to be enqueued on L.
 static oal_status set_svv(oal_level* L, const oal_step_params* p) {
   L->svv_x = p->svv_x_epsilon;
   L->svv_yz = p->svv_yz_epsilon;
-  if (L->svv_x > 0.0f || L->svv_yz > 0.0f) OAL_CUDA_TRY(svv_prepare(L->storage));
   return OAL_OK;
 }
 
@@ -1681,7 +1679,8 @@ static oal_status enqueue_step(oal_level* L, const CaseParams& cp, cudaStream_t 
   const bool svv = L->svv_x > 0.0f || L->svv_yz > 0.0f;
   if (svv) {
     // spectral vanishing viscosity right after the step kernels (timestep.jl:1576-1611)
-    OAL_CUDA_TRY(svv_enqueue(L->storage, a.f_in, a.f_out, pop_index(L), g->nb, g->d_nbr, g->nb, g->d_mslot,
+    const int64_t n_el = L->dense ? 27 * kst : (int64_t)(g->nb + g->n_ghost) * 27 * 512;
+    OAL_CUDA_TRY(svv_enqueue(L->storage, a.f_in, a.f_out, pop_index(L), g->nb, n_el, g->d_nbr, g->nb, g->d_mslot,
                              g->d_cmask, L->svv_x, L->svv_yz, st));
   }
   if (L->nscbc.enabled && L->n_nscbc > 0) {

@@ -811,6 +811,10 @@ struct oal_q19_level {
   int32_t n_plain = 0, n_walls = 0, ncut = 0, nlinks = 0, ntri = 0;
   int faces[6] = {0, 0, 0, 0, 0, 0};
   bool forces_valid = false;
+  // the wall octs step on a side stream beside the plain octs (both read the current buffer and
+  // write disjoint octs of the other): a fork and a join event around the two launches
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
 };
 
 namespace {
@@ -904,7 +908,14 @@ template <class T>
 cudaError_t step_level_t(oal_q19_level* L, const oal_q19_params* p, bool collect, cudaStream_t st) {
   const bool forced = !(T(p->body_force[0]) == T(0) && T(p->body_force[1]) == T(0) && T(p->body_force[2]) == T(0));
   const LevelArgs<T> a = level_args<T>(L, p);
-  cudaError_t e = launch_step<T>(a, p->sgs, forced, st);
+  // with a side stream the wall octs run beside the plain ones (fork before, join after)
+  const bool fork = L->walls && L->side != nullptr;
+  cudaError_t e = cudaSuccess;
+  if (fork) {
+    e = cudaEventRecord(L->fork, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(L->side, L->fork, 0);
+  }
+  if (e == cudaSuccess) e = launch_step<T>(a, p->sgs, forced, st);
   if (e == cudaSuccess && L->walls) {
     LevelArgs<T> b = a;
     b.work = L->work_walls;
@@ -924,7 +935,9 @@ cudaError_t step_level_t(oal_q19_level* L, const oal_q19_params* p, bool collect
     w.uin0 = T(p->u_inlet[0]);
     w.uin1 = T(p->u_inlet[1]);
     w.uin2 = T(p->u_inlet[2]);
-    e = launch_walls<T>(b, w, p->sgs, forced, st);
+    e = launch_walls<T>(b, w, p->sgs, forced, fork ? L->side : st);
+    if (fork && e == cudaSuccess) e = cudaEventRecord(L->join, L->side);
+    if (fork && e == cudaSuccess) e = cudaStreamWaitEvent(st, L->join, 0);
   }
   L->cur = 1 - L->cur;
   ++L->steps;
@@ -1236,6 +1249,11 @@ static oal_status create_desc_impl(int32_t device, int32_t precision, const oal_
     if (e == cudaSuccess) e = cudaMemset(L->tri_force, 0, sizeof(double) * (3 * (size_t)L->ntri + 3));
     if (e == cudaSuccess) e = upload(&L->work_plain, plain.data(), plain.size());
     if (e == cudaSuccess) e = upload(&L->work_walls, walls.data(), walls.size());
+    if (e == cudaSuccess && L->n_plain > 0 && L->n_walls > 0) {
+      e = cudaStreamCreateWithFlags(&L->side, cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&L->fork, cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&L->join, cudaEventDisableTiming);
+    }
     if (e != cudaSuccess) {
       cudaGetLastError();
       s = fail(e == cudaErrorMemoryAllocation ? OAL_E_OUT_OF_MEMORY : OAL_E_CUDA, "level tables: %s", cudaGetErrorString(e));
@@ -1265,6 +1283,9 @@ oal_status oal_q19_level_destroy(oal_q19_level* L) {
     void* tabs[] = {L->kind, L->face, L->special, L->cutidx, L->qdir, L->okdir, L->cut_off, L->cut_dir, L->mom,
                     L->tri_off, L->tri_links, L->tri_force, L->work_plain, L->work_walls};
     for (void* t : tabs) cudaFree(t);
+    if (L->fork) cudaEventDestroy(L->fork);
+    if (L->join) cudaEventDestroy(L->join);
+    if (L->side) cudaStreamDestroy(L->side);
   }
   delete L;
   return OAL_OK;
