@@ -11,7 +11,7 @@
 // (a zero-flux wall for the operator). The 4-moment correction f_k' -= w_k (drho + c_k.dj / cs2)
 // then restores the cell's mass and momentum, and every population is floored at 1e-12.
 //
-// One thread per cell, 256 per CTA (half a block). A population's address is linear in its
+// One thread per cell, 256 per CTA (half a block; 128 in FP64). A population's address is linear in its
 // direction in both layouts (block-major: b 27*512 + k 512 + cell; dense: cell + k PX PY PZ), so a
 // thread resolves its twelve taps once — the neighbour block, the solid masks and the fall-back
 // to its own slot — into twelve direction-0 offsets, and each direction then costs one load per
@@ -24,7 +24,9 @@ namespace oal {
 
 namespace {
 
-constexpr int kSvvThreads = 256;  // one thread per cell, two CTAs per block
+// one thread per cell: 256 per CTA (two per block), 128 for FP64 (the filtered populations of a
+// CTA in shared memory stay within the 48 KB of static shared memory)
+template <class R> constexpr int svv_threads() { return sizeof(R) == 8 ? 128 : 256; }
 
 struct SvvArgs {
   PopIndex pi;
@@ -59,9 +61,10 @@ __device__ __forceinline__ IDX svv_tap_offset(const SvvArgs& a, int b, int x, in
 }
 
 template <class S, class R, class IDX>
-__global__ void __launch_bounds__(kSvvThreads, 3) k_svv(const SvvArgs a, const S* __restrict__ fin, S* __restrict__ fout) {
-  const int b = blockIdx.x >> 1;
-  const int cell = ((blockIdx.x & 1) << 8) | threadIdx.x;
+__global__ void __launch_bounds__(svv_threads<R>(), 3) k_svv(const SvvArgs a, const S* __restrict__ fin, S* __restrict__ fout) {
+  constexpr int kT = svv_threads<R>(), kPer = kCells / kT;
+  const int b = blockIdx.x / kPer;
+  const int cell = (blockIdx.x % kPer) * kT + threadIdx.x;
   if (svv_solid(a, b, cell)) return;
   const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
   const IDX own = (IDX)a.pi(b, cell, 0);
@@ -77,7 +80,7 @@ __global__ void __launch_bounds__(kSvvThreads, 3) k_svv(const SvvArgs a, const S
                 : own;
   }
   const R ex = R(a.eps_x), eyz = R(a.eps_yz);
-  __shared__ R s_fl[kQ27][kSvvThreads];  // the filtered populations until the correction
+  __shared__ R s_fl[kQ27][kT];  // the filtered populations until the correction
   R d_rho = R(0), d_jx = R(0), d_jy = R(0), d_jz = R(0);
 #pragma unroll 3
   for (int k = 0; k < kQ27; ++k) {
@@ -112,11 +115,12 @@ __global__ void __launch_bounds__(kSvvThreads, 3) k_svv(const SvvArgs a, const S
 
 template <class S, class R>
 cudaError_t enqueue_t(const SvvArgs& a, const void* fin, void* fout, int32_t nb, int64_t n_elements, cudaStream_t st) {
-  const unsigned grid = (unsigned)nb * 2u;
+  constexpr int kT = svv_threads<R>();
+  const unsigned grid = (unsigned)nb * (unsigned)(kCells / kT);
   if (n_elements < (int64_t(1) << 32))
-    k_svv<S, R, uint32_t><<<grid, kSvvThreads, 0, st>>>(a, static_cast<const S*>(fin), static_cast<S*>(fout));
+    k_svv<S, R, uint32_t><<<grid, kT, 0, st>>>(a, static_cast<const S*>(fin), static_cast<S*>(fout));
   else
-    k_svv<S, R, int64_t><<<grid, kSvvThreads, 0, st>>>(a, static_cast<const S*>(fin), static_cast<S*>(fout));
+    k_svv<S, R, int64_t><<<grid, kT, 0, st>>>(a, static_cast<const S*>(fin), static_cast<S*>(fout));
   return cudaGetLastError();
 }
 
