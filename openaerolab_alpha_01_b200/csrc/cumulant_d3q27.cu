@@ -1505,8 +1505,9 @@ __global__ void __launch_bounds__(128) k_cumulant_gen(const StepArgs a, const in
 // 0xC0000000 | k the weight of direction k.
 // ------------------------------------------------------------------------------------------------
 // Four entries per thread (a stride of the grid apart, so that a warp's accesses stay
-// contiguous), their loads issued before any store.
-template <class S, class R>
+// contiguous), their loads issued before any store. RAW: every code is a source element (the
+// copies of a block pool, whose element indices use all 32 bits).
+template <class S, class R, bool RAW>
 __global__ void __launch_bounds__(256) k_fill_copy(const StepArgs a, const uint2* __restrict__ entries, int64_t n) {
   constexpr int E = 4;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -1521,11 +1522,11 @@ __global__ void __launch_bounds__(256) k_fill_copy(const StepArgs a, const uint2
   }
 #pragma unroll
   for (int j = 0; j < E; ++j)
-    if (en[j].x != 0xFFFFFFFFu && !(en[j].y & 0x80000000u)) v[j] = f[en[j].y];
+    if (en[j].x != 0xFFFFFFFFu && (RAW || !(en[j].y & 0x80000000u))) v[j] = f[en[j].y];
 #pragma unroll
   for (int j = 0; j < E; ++j) {
     if (en[j].x == 0xFFFFFFFFu) continue;
-    if (en[j].y & 0x80000000u) {
+    if (!RAW && (en[j].y & 0x80000000u)) {
       const int k = (int)(en[j].y & 31u);
       const R w = R(q27_w(k));
       R val = w;
@@ -1559,9 +1560,10 @@ cudaError_t build_fast_records(const int32_t* work, int n, const int32_t* nbr, c
 }
 
 template <class S, class R>
-cudaError_t launch_fill_copy(const StepArgs& a, const uint2* entries, int64_t n, cudaStream_t st) {
+cudaError_t launch_fill_copy(const StepArgs& a, const uint2* entries, int64_t n, cudaStream_t st, bool raw) {
   if (n <= 0) return cudaSuccess;
-  k_fill_copy<S, R><<<(unsigned)((n + 1023) / 1024), 256, 0, st>>>(a, entries, n);
+  if (raw) k_fill_copy<S, R, true><<<(unsigned)((n + 1023) / 1024), 256, 0, st>>>(a, entries, n);
+  else k_fill_copy<S, R, false><<<(unsigned)((n + 1023) / 1024), 256, 0, st>>>(a, entries, n);
   return cudaGetLastError();
 }
 
@@ -1795,7 +1797,7 @@ cudaError_t launch_general(const StepArgs& a, const int32_t* work, int n_work, c
 
 #define OAL_INST(S, R)                                                                               \
   template cudaError_t launch_fill_ghosts<S, R>(const StepArgs&, const uint2*, int64_t, cudaStream_t); \
-  template cudaError_t launch_fill_copy<S, R>(const StepArgs&, const uint2*, int64_t, cudaStream_t);   \
+  template cudaError_t launch_fill_copy<S, R>(const StepArgs&, const uint2*, int64_t, cudaStream_t, bool); \
   template cudaError_t launch_restrict<S, R>(const RestrictArgs&, cudaStream_t);                       \
   template cudaError_t launch_parent_nodes<S, R>(const ParentView&, const int32_t*, int32_t, void*, int32_t,  \
                                                  cudaStream_t);                                            \

@@ -22,7 +22,7 @@ namespace oal {
 template <class S, class R>
 cudaError_t launch_fill_ghosts(const StepArgs& a, const uint2* entries, int64_t n, cudaStream_t st);
 template <class S, class R>
-cudaError_t launch_fill_copy(const StepArgs& a, const uint2* entries, int64_t n, cudaStream_t st);
+cudaError_t launch_fill_copy(const StepArgs& a, const uint2* entries, int64_t n, cudaStream_t st, bool raw = false);
 cudaError_t build_fast_records(const int32_t* work, int n, const int32_t* nbr, const int4* binfo, int32_t* rec,
                                cudaStream_t st);
 template <class S, class R>
@@ -2756,7 +2756,7 @@ static oal_status batch_rebuild(oal_batch* B) {
       // the member's raw ghost copies, rebased into the pool (as a single level of the same
       // geometry copies them); its other fill entries stay with the general fill
       const oal_geometry::FillLists* fl = nullptr;
-      if (build_fill_lists(const_cast<oal_geometry*>(g), M.cp.flags) == OAL_OK && pool_elems < (1ll << 31))
+      if (build_fill_lists(const_cast<oal_geometry*>(g), M.cp.flags) == OAL_OK && pool_elems < (1ll << 32))
         for (const auto& c : g->fills)
           if (c.key == fill_key_of(M.cp.flags)) fl = &c;
       if (fl) {
@@ -2818,7 +2818,7 @@ static cudaError_t batch_step_t(oal_batch* B, const StepArgs& a, cudaStream_t st
   if (fork) {
     if ((e = cudaEventRecord(B->ov.fork, st)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(B->ov.side, B->ov.fork, 0)) != cudaSuccess) return e;
-    if ((e = launch_fill_copy<S, R>(a, B->d_fcopy, B->n_fcopy, B->ov.side)) != cudaSuccess) return e;
+    if ((e = launch_fill_copy<S, R>(a, B->d_fcopy, B->n_fcopy, B->ov.side, true)) != cudaSuccess) return e;
     if ((e = launch_fill_ghosts<S, R>(a, B->d_gentries, B->n_gentries, B->ov.side)) != cudaSuccess) return e;
     if ((e = launch_general<S, R>(a, B->d_general, (int)B->n_general, B->ov.side)) != cudaSuccess) return e;
     if ((e = launch_fast_range<S, R>(a, B->d_fast, n_in, n_bd, B->ov.side)) != cudaSuccess) return e;
@@ -2826,7 +2826,7 @@ static cudaError_t batch_step_t(oal_batch* B, const StepArgs& a, cudaStream_t st
     if ((e = launch_fast_range<S, R>(a, B->d_fast, 0, n_in, st)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(st, B->ov.join, 0)) != cudaSuccess) return e;
   } else {
-    if ((e = launch_fill_copy<S, R>(a, B->d_fcopy, B->n_fcopy, st)) != cudaSuccess) return e;
+    if ((e = launch_fill_copy<S, R>(a, B->d_fcopy, B->n_fcopy, st, true)) != cudaSuccess) return e;
     if ((e = launch_fill_ghosts<S, R>(a, B->d_gentries, B->n_gentries, st)) != cudaSuccess) return e;
     if ((e = launch_fast<S, R>(a, B->d_fast, (int)B->n_fast, st)) != cudaSuccess) return e;
     if ((e = launch_general<S, R>(a, B->d_general, (int)B->n_general, st)) != cudaSuccess) return e;

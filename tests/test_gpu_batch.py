@@ -132,3 +132,19 @@ def test_large_channel_member_matches_alone(oal):
     B.close()
     for g in geoms:
         g.close()
+
+
+def test_member_of_a_pool_past_2_31_elements_matches_alone(oal):
+    """A pool whose population buffer holds more than 2^31 elements (160,000 blocks, the size class
+    of the serving pool): the members' raw ghost copies are still a copy list (their element
+    indices use all 32 bits), so a channel member stores the bits it stores alone."""
+    case = sphere_channel_case(64, 32, 32, diameter=8.0, centre_x=16.0, u_inlet=0.05, re=300.0)
+    steps = 120
+    f, rho, vel, force, mm = alone(case, "f16", steps)
+    g = Geometry(case.dom)
+    B = Batch(storage="f16", max_real_blocks=150_000, max_ghost_blocks=10_000, max_mask_blocks=64, max_members=2)
+    m = B.add(g, case.params, case.rho, case.vel)
+    B.advance(steps)
+    assert np.array_equal(B.state(m)[0], f)
+    assert np.array_equal(B.forces(m), force) and np.array_equal(B.mass_momentum(m), mm)
+    B.close(); g.close()
