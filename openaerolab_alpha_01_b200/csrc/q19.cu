@@ -31,7 +31,6 @@
 #include <unordered_map>
 
 #include "../../include/oal.h"
-#include "pdl.cuh"
 
 oal_status oal_internal_set_error(oal_status s, const char* msg);
 
@@ -402,8 +401,6 @@ __device__ __forceinline__ void store_cell(const LevelArgs<T>& a, int64_t o, int
 // SGS: 0 none, 1 WALE, 2 Smagorinsky, 3 Vreman; GRAD: the velocity gradient is needed (SGS or HRR)
 template <class T, int SGS, bool GRAD, bool FORCED>
 __global__ void __launch_bounds__(kThreads) k_q19_step(const LevelArgs<T> a) {
-  oal::pdl_wait();
-  oal::pdl_release();
   __shared__ int32_t s_nb[kOctsPerCta * 27];
   __shared__ int64_t s_o[kOctsPerCta];
   const int n_here = stage_octs<T>(a, s_nb, s_o);
@@ -486,8 +483,6 @@ __device__ __forceinline__ T face_population(const WallArgs<T>& w, uint32_t mask
 // Bouzidi rule on cut links and the momentum exchange (stream.jl:205-257)
 template <class T, int SGS, bool GRAD, bool FORCED>
 __global__ void __launch_bounds__(kThreads) k_q19_walls(const LevelArgs<T> a, const WallArgs<T> w) {
-  oal::pdl_wait();
-  oal::pdl_release();
   __shared__ int32_t s_nb[kOctsPerCta * 27];
   __shared__ int64_t s_o[kOctsPerCta];
   const int n_here = stage_octs<T>(a, s_nb, s_o);
@@ -869,8 +864,8 @@ cudaError_t launch3(const LevelArgs<T>& a, const WallArgs<T>* w, bool forced, cu
   const int64_t n = a.n_work;
   if (n > 0) {
     const unsigned grid = (unsigned)((n + kOctsPerCta - 1) / kOctsPerCta);
-    if (forced) return oal::launch_pdl(k_q19_step<T, SGS, GRAD, true>, grid, kThreads, 0, st, a);
-    return oal::launch_pdl(k_q19_step<T, SGS, GRAD, false>, grid, kThreads, 0, st, a);
+    if (forced) k_q19_step<T, SGS, GRAD, true><<<grid, kThreads, 0, st>>>(a);
+    else k_q19_step<T, SGS, GRAD, false><<<grid, kThreads, 0, st>>>(a);
   }
   (void)w;
   return cudaGetLastError();
@@ -880,8 +875,9 @@ template <class T, int SGS, bool GRAD>
 cudaError_t launch_walls3(const LevelArgs<T>& a, const WallArgs<T>& w, bool forced, cudaStream_t st) {
   if (a.n_work <= 0) return cudaSuccess;
   const unsigned grid = (unsigned)((a.n_work + kOctsPerCta - 1) / kOctsPerCta);
-  if (forced) return oal::launch_pdl(k_q19_walls<T, SGS, GRAD, true>, grid, kThreads, 0, st, a, w);
-  return oal::launch_pdl(k_q19_walls<T, SGS, GRAD, false>, grid, kThreads, 0, st, a, w);
+  if (forced) k_q19_walls<T, SGS, GRAD, true><<<grid, kThreads, 0, st>>>(a, w);
+  else k_q19_walls<T, SGS, GRAD, false><<<grid, kThreads, 0, st>>>(a, w);
+  return cudaGetLastError();
 }
 
 template <class T>
@@ -1488,8 +1484,6 @@ template <class T>
 __global__ void k_q19_donor_moments(int32_t n, const int32_t* __restrict__ cells, const T* __restrict__ fnew,
                                     const T* __restrict__ fold, int mode, T w0, T w1, const uint8_t* __restrict__ cov,
                                     T* __restrict__ out) {
-  oal::pdl_wait();
-  oal::pdl_release();
   const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
   T m[10];
@@ -1536,8 +1530,6 @@ template <class T>
 __global__ void __launch_bounds__(256) k_q19_fill(int32_t ng, const int32_t* __restrict__ ghost_slot,
                                                   const int32_t* __restrict__ dix, const float* __restrict__ gw,
                                                   const T* __restrict__ dm, T scale, T omega, T* f, T* u, T* rho) {
-  oal::pdl_wait();
-  oal::pdl_release();
   const int lane = threadIdx.x & 31, q = lane & 15;
   const int64_t g = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
   if (g >= ng) return;  // both lanes groups of a warp test their own g; a group leaves as a whole
@@ -1563,8 +1555,6 @@ __global__ void __launch_bounds__(256) k_q19_fill(int32_t ng, const int32_t* __r
 template <class T>
 __global__ void k_q19_source_moments(int32_t n, const int32_t* __restrict__ cells, const T* __restrict__ f,
                                      T* __restrict__ out) {
-  oal::pdl_wait();
-  oal::pdl_release();
   const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
   T m[10];
@@ -1584,8 +1574,6 @@ template <class T>
 __global__ void __launch_bounds__(256) k_q19_restrict(int32_t nr, const int32_t* __restrict__ rslot,
                                                       const int32_t* __restrict__ six, const uint8_t* __restrict__ cubic,
                                                       const T* __restrict__ rm, T scale, T omega, T* f, T* u, T* rho) {
-  oal::pdl_wait();
-  oal::pdl_release();
   const int lane = threadIdx.x & 31, q = lane & 15;
   const int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 4;
   if (r >= nr) return;
@@ -1622,8 +1610,6 @@ __global__ void __launch_bounds__(256) k_q19_restrict(int32_t nr, const int32_t*
 template <class T>
 __global__ void k_q19_copy_slots(int32_t n, const int32_t* __restrict__ slots, const T* __restrict__ fs, T* fd,
                                  const T* __restrict__ us, T* ud, const T* __restrict__ rs, T* rd) {
-  oal::pdl_wait();
-  oal::pdl_release();
   const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
   const int64_t s = slots[c], o = s >> 3;
@@ -1727,13 +1713,11 @@ cudaError_t fill_ghosts_t(oal_q19_octree* tr, const oal_q19_params* p, int l, T 
   const T scale = tau_f / (T(2) * tau_c) * pre_collision_factor_h<T>(omega_c);
   const T w1 = weight, w0 = T(1) - weight;
   const int mode = w1 == T(0) ? 0 : (w0 == T(0) ? 1 : 2);
-  cudaError_t e = oal::launch_pdl(k_q19_donor_moments<T>, (unsigned)((t.nd + 127) / 128), 128, 0, st, t.nd,
-                                  (const int32_t*)t.dcells, (const T*)Lc->f[Lc->cur], (const T*)Lc->f[1 - Lc->cur],
-                                  mode, w0, w1, (const uint8_t*)t.dcov, (T*)t.dm);
-  if (e != cudaSuccess) return e;
-  return oal::launch_pdl(k_q19_fill<T>, (unsigned)((16 * (int64_t)t.ng + 255) / 256), 256, 0, st, t.ng,
-                         (const int32_t*)t.ghost_slot, (const int32_t*)t.dix, (const float*)t.gw, (const T*)t.dm, scale,
-                         omega_f, (T*)Lf->f[Lf->cur], (T*)Lf->u[Lf->cur], (T*)Lf->rho[Lf->cur]);
+  k_q19_donor_moments<T><<<(t.nd + 127) / 128, 128, 0, st>>>(t.nd, t.dcells, (const T*)Lc->f[Lc->cur],
+                                                             (const T*)Lc->f[1 - Lc->cur], mode, w0, w1, t.dcov, (T*)t.dm);
+  k_q19_fill<T><<<(unsigned)((16 * (int64_t)t.ng + 255) / 256), 256, 0, st>>>(t.ng, t.ghost_slot, t.dix, t.gw, (const T*)t.dm, scale, omega_f,
+                                                    (T*)Lf->f[Lf->cur], (T*)Lf->u[Lf->cur], (T*)Lf->rho[Lf->cur]);
+  return cudaGetLastError();
 }
 
 template <class T>
@@ -1745,12 +1729,10 @@ cudaError_t restrict_t(oal_q19_octree* tr, const oal_q19_params* p, int l, cudaS
   const T omega_c = omega_of_h<T>(p[l - 1].nu), omega_f = omega_of_h<T>(p[l].nu);
   const T tau_c = T(1) / omega_c, tau_f = T(1) / omega_f;
   const T scale = T(2) * tau_c / tau_f * pre_collision_factor_h<T>(omega_f);
-  cudaError_t e = oal::launch_pdl(k_q19_source_moments<T>, (unsigned)((t.ns + 127) / 128), 128, 0, st, t.ns,
-                                  (const int32_t*)t.scells, (const T*)Lf->f[Lf->cur], (T*)t.rm);
-  if (e != cudaSuccess) return e;
-  return oal::launch_pdl(k_q19_restrict<T>, (unsigned)((16 * (int64_t)t.nr + 255) / 256), 256, 0, st, t.nr,
-                         (const int32_t*)t.rslot, (const int32_t*)t.six, (const uint8_t*)t.rcubic, (const T*)t.rm, scale,
-                         omega_c, (T*)Lc->f[Lc->cur], (T*)Lc->u[Lc->cur], (T*)Lc->rho[Lc->cur]);
+  k_q19_source_moments<T><<<(t.ns + 127) / 128, 128, 0, st>>>(t.ns, t.scells, (const T*)Lf->f[Lf->cur], (T*)t.rm);
+  k_q19_restrict<T><<<(unsigned)((16 * (int64_t)t.nr + 255) / 256), 256, 0, st>>>(t.nr, t.rslot, t.six, t.rcubic, (const T*)t.rm, scale, omega_c,
+                                                        (T*)Lc->f[Lc->cur], (T*)Lc->u[Lc->cur], (T*)Lc->rho[Lc->cur]);
+  return cudaGetLastError();
 }
 
 template <class T>
@@ -1759,9 +1741,9 @@ cudaError_t copy_ghosts_t(oal_q19_octree* tr, int l, cudaStream_t st) {
   if (l == tr->L || t.ng == 0) return cudaSuccess;
   oal_q19_level* S = tr->lv[l - 1];
   const int c = S->cur, o = 1 - S->cur;
-  return oal::launch_pdl(k_q19_copy_slots<T>, (unsigned)((t.ng + 127) / 128), 128, 0, st, t.ng,
-                         (const int32_t*)t.ghost_slot, (const T*)S->f[o], (T*)S->f[c], (const T*)S->u[o], (T*)S->u[c],
-                         (const T*)S->rho[o], (T*)S->rho[c]);
+  k_q19_copy_slots<T><<<(t.ng + 127) / 128, 128, 0, st>>>(t.ng, t.ghost_slot, (const T*)S->f[o], (T*)S->f[c],
+                                                          (const T*)S->u[o], (T*)S->u[c], (const T*)S->rho[o], (T*)S->rho[c]);
+  return cudaGetLastError();
 }
 
 // step_recursive! (coupling.jl:240-254)
