@@ -163,6 +163,54 @@ __device__ __forceinline__ IDX svv_pair_offset(const SvvArgs& a, int b, int x, i
   return (IDX)a.pi(bb, c, 0);
 }
 
+// the filter of the 27 directions of a pair of cells: the filtered values into s_fl, the changes
+// of mass and momentum of each lane into acc; PICK: some tap of the pair falls back
+template <class S, class IDX, bool PICK>
+__device__ __forceinline__ void svv_pairs_filter(const SvvArgs& a, const S* __restrict__ fin, const S* __restrict__ fout,
+                                                 IDX own, IDX kst, const IDX (&t)[10], uint32_t fb, bool fx, bool fyz,
+                                                 float (*s_fl)[256], int l0, float (&acc)[8]) {
+  const float ex = a.eps_x, eyz = a.eps_yz;
+  float r0 = 0.0f, x0 = 0.0f, y0 = 0.0f, z0 = 0.0f, r1 = 0.0f, x1 = 0.0f, y1 = 0.0f, z1 = 0.0f;
+#pragma unroll 3
+  for (int k = 0; k < kQ27; ++k) {
+    const float w = float(q27_w(k)), inv_w = float(1.0 / q27_w(k));
+    const S* fk = fin + (IDX)k * kst;
+    const float2 o = PairIO<S>::load(fk + own, w, inv_w);  // the pair's own input populations
+    const float2 fc = PairIO<S>::load(fout + own + (IDX)k * kst, w, inv_w);
+    auto pick = [&](int bit, float v, float mine) {
+      if constexpr (PICK) return ((fb >> bit) & 1u) ? mine : v;
+      else return v;
+    };
+    float bl0 = 0.0f, bl1 = 0.0f;
+    if (fx) {
+      const float2 m = PairIO<S>::load(fk + t[0], w, inv_w), p = PairIO<S>::load(fk + t[1], w, inv_w);
+      bl0 += ex * ((((pick(0, m.x, o.x) - 4.0f * pick(2, m.y, o.x)) + 6.0f * fc.x) - 4.0f * pick(4, o.y, o.x)) +
+                   pick(6, p.x, o.x));
+      bl1 += ex * ((((pick(1, m.y, o.y) - 4.0f * pick(3, o.x, o.y)) + 6.0f * fc.y) - 4.0f * pick(5, p.x, o.y)) +
+                   pick(7, p.y, o.y));
+    }
+    if (fyz) {
+#pragma unroll
+      for (int a2 = 0; a2 < 2; ++a2) {
+        const int j0 = 2 + 4 * a2, bit = 8 + 8 * a2;
+        const float2 v0 = PairIO<S>::load(fk + t[j0], w, inv_w), v1 = PairIO<S>::load(fk + t[j0 + 1], w, inv_w);
+        const float2 v2 = PairIO<S>::load(fk + t[j0 + 2], w, inv_w), v3 = PairIO<S>::load(fk + t[j0 + 3], w, inv_w);
+        bl0 += eyz * ((((pick(bit, v0.x, o.x) - 4.0f * pick(bit + 2, v1.x, o.x)) + 6.0f * fc.x) -
+                       4.0f * pick(bit + 4, v2.x, o.x)) + pick(bit + 6, v3.x, o.x));
+        bl1 += eyz * ((((pick(bit + 1, v0.y, o.y) - 4.0f * pick(bit + 3, v1.y, o.y)) + 6.0f * fc.y) -
+                       4.0f * pick(bit + 5, v2.y, o.y)) + pick(bit + 7, v3.y, o.y));
+      }
+    }
+    const float f0 = fc.x - bl0, f1 = fc.y - bl1;
+    const float e0 = f0 - fc.x, e1 = f1 - fc.y;
+    r0 += e0; x0 += e0 * float(q27_cx(k)); y0 += e0 * float(q27_cy(k)); z0 += e0 * float(q27_cz(k));
+    r1 += e1; x1 += e1 * float(q27_cx(k)); y1 += e1 * float(q27_cy(k)); z1 += e1 * float(q27_cz(k));
+    s_fl[k][l0] = f0;
+    s_fl[k][l0 + 1] = f1;
+  }
+  acc[0] = r0; acc[1] = x0; acc[2] = y0; acc[3] = z0; acc[4] = r1; acc[5] = x1; acc[6] = y1; acc[7] = z1;
+}
+
 template <class S, class IDX>
 __global__ void __launch_bounds__(128, 6) k_svv_pairs(const SvvArgs a, const S* __restrict__ fin, S* __restrict__ fout) {
   const int b = blockIdx.x >> 1;
@@ -194,43 +242,13 @@ __global__ void __launch_bounds__(128, 6) k_svv_pairs(const SvvArgs a, const S* 
     t[2 + j] = fyz ? svv_pair_offset<IDX>(a, b, x, y, z, 0, j < 4 ? s : 0, j < 4 ? 0 : s, own, q0, q1) : own;
     fb |= (uint32_t)q0 << (8 + 2 * j) | (uint32_t)q1 << (9 + 2 * j);
   }
-  const float ex = a.eps_x, eyz = a.eps_yz;
   __shared__ float s_fl[kQ27][256];
-  float r0 = 0.0f, x0 = 0.0f, y0 = 0.0f, z0 = 0.0f, r1 = 0.0f, x1 = 0.0f, y1 = 0.0f, z1 = 0.0f;
-#pragma unroll 3
-  for (int k = 0; k < kQ27; ++k) {
-    const float w = float(q27_w(k)), inv_w = float(1.0 / q27_w(k));
-    const S* fk = fin + (IDX)k * kst;
-    const float2 o = PairIO<S>::load(fk + own, w, inv_w);  // the pair's own input populations
-    const float2 fc = PairIO<S>::load(fout + own + (IDX)k * kst, w, inv_w);
-    auto pick = [&](int bit, float v, float mine) { return ((fb >> bit) & 1u) ? mine : v; };
-    float bl0 = 0.0f, bl1 = 0.0f;
-    if (fx) {
-      const float2 m = PairIO<S>::load(fk + t[0], w, inv_w), p = PairIO<S>::load(fk + t[1], w, inv_w);
-      bl0 += ex * ((((pick(0, m.x, o.x) - 4.0f * pick(2, m.y, o.x)) + 6.0f * fc.x) - 4.0f * pick(4, o.y, o.x)) +
-                   pick(6, p.x, o.x));
-      bl1 += ex * ((((pick(1, m.y, o.y) - 4.0f * pick(3, o.x, o.y)) + 6.0f * fc.y) - 4.0f * pick(5, p.x, o.y)) +
-                   pick(7, p.y, o.y));
-    }
-    if (fyz) {
-#pragma unroll
-      for (int a2 = 0; a2 < 2; ++a2) {
-        const int j0 = 2 + 4 * a2, bit = 8 + 8 * a2;
-        const float2 v0 = PairIO<S>::load(fk + t[j0], w, inv_w), v1 = PairIO<S>::load(fk + t[j0 + 1], w, inv_w);
-        const float2 v2 = PairIO<S>::load(fk + t[j0 + 2], w, inv_w), v3 = PairIO<S>::load(fk + t[j0 + 3], w, inv_w);
-        bl0 += eyz * ((((pick(bit, v0.x, o.x) - 4.0f * pick(bit + 2, v1.x, o.x)) + 6.0f * fc.x) -
-                       4.0f * pick(bit + 4, v2.x, o.x)) + pick(bit + 6, v3.x, o.x));
-        bl1 += eyz * ((((pick(bit + 1, v0.y, o.y) - 4.0f * pick(bit + 3, v1.y, o.y)) + 6.0f * fc.y) -
-                       4.0f * pick(bit + 5, v2.y, o.y)) + pick(bit + 7, v3.y, o.y));
-      }
-    }
-    const float f0 = fc.x - bl0, f1 = fc.y - bl1;
-    const float e0 = f0 - fc.x, e1 = f1 - fc.y;
-    r0 += e0; x0 += e0 * float(q27_cx(k)); y0 += e0 * float(q27_cy(k)); z0 += e0 * float(q27_cz(k));
-    r1 += e1; x1 += e1 * float(q27_cx(k)); y1 += e1 * float(q27_cy(k)); z1 += e1 * float(q27_cz(k));
-    s_fl[k][l0] = f0;
-    s_fl[k][l0 + 1] = f1;
-  }
+  float acc[8];
+  // the fall-back selects only where a tap of the pair falls back (cells next to a solid or a
+  // missing block); elsewhere the loads are used as they are
+  if (fb == 0) svv_pairs_filter<S, IDX, false>(a, fin, fout, own, kst, t, fb, fx, fyz, s_fl, l0, acc);
+  else svv_pairs_filter<S, IDX, true>(a, fin, fout, own, kst, t, fb, fx, fyz, s_fl, l0, acc);
+  const float r0 = acc[0], x0 = acc[1], y0 = acc[2], z0 = acc[3], r1 = acc[4], x1 = acc[5], y1 = acc[6], z1 = acc[7];
   const float inv_cs2 = 1.0f / float(1.0 / 3.0);  // CS2_LATTICE
 #pragma unroll 3
   for (int k = 0; k < kQ27; ++k) {
