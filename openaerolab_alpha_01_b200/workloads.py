@@ -18,7 +18,8 @@ import time
 
 import numpy as np
 
-from .cases import entropic_taylor_green_case, taylor_green_case
+from . import _capi as capi
+from .cases import entropic_taylor_green_case, sphere_channel_case, taylor_green_case
 from .solver import Batch, Geometry, Level
 
 SIZES = (32, 48, 64, 96, 128)
@@ -231,6 +232,41 @@ def benchmark_amr(steps: int = 50, warmup: int = 5, storage: str = "f16", nx: in
             "gpu_launches_per_coarse_step": "level 0: ghost fill, fast, general; level 1 (x2): parent nodes, interpolation positions, ghost fill, fast, general; restriction; 3 snapshot copies"}
 
 
+def benchmark_svv(steps: int = 100, warmup: int = 20, storage: str = "f16", eps_yz: float = 0.004,
+                  eps_x: float = 0.0) -> dict:
+    """Time the config-2 channel (256 x 128 x 128, sphere D 24) with and without the spectral
+    vanishing viscosity filter (one CUDA graph of `steps` steps each, CUDA events)."""
+    import torch
+    case = sphere_channel_case(256, 128, 128, diameter=24.0, centre_x=64.0, u_inlet=0.05, re=1000.0)
+    geom = Geometry(case.dom)
+    lvl = Level(geom, storage=storage)
+    lvl.init_equilibrium(case.rho, case.vel)
+    cells = case.dom.n_blocks * 512
+    out = {"workload": f"svv_sphere_channel_256x128x128_{storage}_eps_yz{eps_yz:g}_eps_x{eps_x:g}", "cells": cells,
+           "steps": steps}
+    for name, (ex, eyz) in (("off", (0.0, 0.0)), ("svv", (eps_x, eps_yz))):
+        p = capi.StepParams.from_buffer_copy(case.params)
+        p.svv_x_epsilon = ex
+        p.svv_yz_epsilon = eyz
+        lvl.execute_timestep_batch(p, warmup)
+        lvl.execute_timestep_batch(p, steps)  # the timed graph, captured outside the timed region
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        lvl.execute_timestep_batch(p, steps)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        out[name] = {"ms_per_step": round(ms, 4), "mlups": round(cells / ms / 1e3, 1)}
+    filt = out["svv"]["ms_per_step"] - out["off"]["ms_per_step"]
+    bytes_per_cell = 3 * 27 * {"f16": 2, "bf16": 2, "f32": 4, "f64": 8}[storage]
+    out["filter_ms"] = round(filt, 4)
+    out["filter_gbs"] = round(cells * bytes_per_cell / (filt * 1e-3) / 1e9, 1) if filt > 0 else None
+    lvl.close()
+    geom.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--steps", type=int, default=2000)
@@ -242,8 +278,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=5, help="untimed steps before the D3Q39 measurement")
     ap.add_argument("--kbc-math", default="fast", choices=("fast", "exact"),
                     help="D3Q39: CUDA's expf / logf (fast) or the software exp / log shared with the oracle")
+    ap.add_argument("--svv", action="store_true",
+                    help="instead: time the config-2 channel with and without the SVV filter (y-z, eps 0.004)")
     args = ap.parse_args()
     t0 = time.time()
+    if args.svv:
+        print(json.dumps(benchmark_svv(steps=args.steps, warmup=args.warmup, storage=args.storage)))
+        return
     if args.kbc > 0:
         print(json.dumps(benchmark_entropic(args.kbc, steps=args.steps, warmup=args.warmup, math=args.kbc_math)))
         return
