@@ -221,6 +221,16 @@ __device__ __forceinline__ R lagrange3(int i, R w) {
        : i == 1  ? (-w * (w + R(1)) * (w - R(2)) / R(2))
                  : (w * (w + R(1)) * (w - R(1)) / R(6));
 }
+// the four cubic weights of one axis, lagrange3(-1 .. 2, w): evaluated once per stencil, so that a
+// node's weight is two products ((lx ly) lz, the order of the direct product of three calls)
+template <class R>
+struct Lagrange4 {
+  R v[4];
+  __device__ __forceinline__ explicit Lagrange4(R w) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) v[i] = lagrange3<R>(i - 1, w);
+  }
+};
 
 // sample_parent_macro_for_fine_cell (physics_interpolation.jl:188-346)
 template <class R>
@@ -303,11 +313,12 @@ __device__ void pos_macros(const ParentView& P, int32_t pos, int fgx, int fgy, i
   R rho_i, ux_i, uy_i, uz_i;
   if (all_valid) {
     rho_i = ux_i = uy_i = uz_i = R(0);
+    const Lagrange4<R> lx(wx), ly(wy), lz(wz);
 #pragma unroll 4
     for (int i = 0; i < 64; ++i) {
-      const int a = (i >> 4) - 1, bb = ((i >> 2) & 3) - 1, c = (i & 3) - 1;
+      const int a = i >> 4, bb = (i >> 2) & 3, c = i & 3;
       const R* v = static_cast<const R*>(P.node_vals) + (int64_t)nodes[i] * 32;
-      const R w3 = lagrange3<R>(a, wx) * lagrange3<R>(bb, wy) * lagrange3<R>(c, wz);
+      const R w3 = lx.v[a] * ly.v[bb] * lz.v[c];
       rho_i += w3 * v[0];
       ux_i += w3 * v[1];
       uy_i += w3 * v[2];
@@ -425,12 +436,13 @@ __device__ OAL_POS_LINKAGE R pos_population(const ParentView& P, int32_t pos, in
   const R anchor_neq = corner[anchor] >= 0 ? vals[(int64_t)corner[anchor] * 32 + 4 + k] : R(0);
   R f_neq = R(0);
   if (use_cubic) {
+    const Lagrange4<R> lx(wx), ly(wy), lz(wz);
 #pragma unroll 4
     for (int i = 0; i < 64; ++i) {
-      const int a = (i >> 4) - 1, bb = ((i >> 2) & 3) - 1, c = (i & 3) - 1;
+      const int a = i >> 4, bb = (i >> 2) & 3, c = i & 3;
       const int32_t ni = nodes[i];
       const R nv = ni >= 0 ? vals[(int64_t)ni * 32 + 4 + k] : anchor_neq;
-      f_neq += lagrange3<R>(a, wx) * lagrange3<R>(bb, wy) * lagrange3<R>(c, wz) * nv;
+      f_neq += lx.v[a] * ly.v[bb] * lz.v[c] * nv;
     }
   } else {
     R v[8];
@@ -498,11 +510,12 @@ __device__ __noinline__ R parent_population(const ParentView& P, int fgx, int fg
   R rho_i, ux_i, uy_i, uz_i;
   if (cubic_all_valid) {
     rho_i = ux_i = uy_i = uz_i = R(0);
+    const Lagrange4<R> lx(wx), ly(wy), lz(wz);
 #pragma unroll 1
     for (int i = 0; i < 64; ++i) {
       const int a = (i >> 4) - 1, bb = ((i >> 2) & 3) - 1, c = (i & 3) - 1;
       const PNode<R> m = parent_macro<R>(P, px0 + a, py0 + bb, pz0 + c);
-      const R w3 = lagrange3<R>(a, wx) * lagrange3<R>(bb, wy) * lagrange3<R>(c, wz);
+      const R w3 = lx.v[a + 1] * ly.v[bb + 1] * lz.v[c + 1];
       rho_i += w3 * m.rho;
       ux_i += w3 * m.ux;
       uy_i += w3 * m.uy;
@@ -516,11 +529,12 @@ __device__ __noinline__ R parent_population(const ParentView& P, int fgx, int fg
   R f_neq = R(0);
   if (use_cubic) {
     const R anchor_neq = d[anchor].fneq;
+    const Lagrange4<R> lx(wx), ly(wy), lz(wz);
 #pragma unroll 1
     for (int i = 0; i < 64; ++i) {
       const int a = (i >> 4) - 1, bb = ((i >> 2) & 3) - 1, c = (i & 3) - 1;
       const PNode<R> nd = parent_blended<S, R>(P, px0 + a, py0 + bb, pz0 + c, k, wk, cx, cy, cz, comp);
-      f_neq += lagrange3<R>(a, wx) * lagrange3<R>(bb, wy) * lagrange3<R>(c, wz) * (nd.ok ? nd.fneq : anchor_neq);
+      f_neq += lx.v[a + 1] * ly.v[bb + 1] * lz.v[c + 1] * (nd.ok ? nd.fneq : anchor_neq);
     }
   } else {
     f_neq = trilin(&PNode<R>::fneq);
