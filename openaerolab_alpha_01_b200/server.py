@@ -3,7 +3,8 @@
 Requests arrive (Poisson, rate lambda); each asks for `steps` steps of a cubic domain, either D3Q27
 cumulant — a sphere-in-channel (sphere diameter 0.2 N, inlet u = 0.05, half-way walls with the
 FP64 drag) or a periodic Taylor-Green box — or D3Q39 entropic KBC on the same two kinds of domain
-(the KBC channel has no momentum-exchange drag). The server keeps every
+(the KBC channel's drag comes from the surface-stress mapping on the sphere's triangles, the
+reference's force method for that path). The server keeps every
 admitted D3Q27 solve resident in one `Batch`, advanced together in ticks of `tick_steps` steps
 (one CUDA graph per tick, one launch per kernel per step for the whole mix), and every admitted
 KBC solve resident as its own level on its own stream, advanced in the same ticks so that its
@@ -30,7 +31,8 @@ import numpy as np
 
 from . import _capi as capi
 from .cases import entropic_taylor_green_case, sphere_channel_case, taylor_green_case
-from .solver import Batch, Geometry, Level, default_entropic_params
+from .solver import Batch, Geometry, Level, default_entropic_params, default_surface_params
+from .surface import sphere_mesh
 
 # device bytes of one block in a pool (populations x2, rho, velocity x2)
 _POP_BYTES = {"f16": 2, "bf16": 2, "f32": 4, "f64": 8}
@@ -103,6 +105,18 @@ def build_case(req: Request):
     return taylor_green_case(req.n, u0=req.u0, re=req.re, c_wale=0.2)
 
 
+def kbc_drag(req: Request, case, L: Level) -> np.ndarray:
+    """The force on a D3Q39 channel's sphere by the surface-stress mapping, the reference's force
+    method for the entropic path (compute_aerodynamics!, src/forces/surface.jl:1577-1660): the
+    sphere's triangles attached to the level and its stresses integrated in FP64 (lattice units).
+    Periodic boxes have no body: zeros."""
+    if req.kind != "channel":
+        return np.zeros(3)
+    m = case.meta
+    L.set_surface(sphere_mesh(m["centre"], m["diameter"] / 2.0))
+    return L.surface_forces(default_surface_params(tau=float(case.params.tau), c_wale=float(case.params.c_wale)))["total"]
+
+
 def _finish(req: Request, totals: np.ndarray, drag: np.ndarray, t: float):
     """A solve's result: its FP64 drag and FP64 mass/momentum totals (computed on the GPU)."""
     req.done = t
@@ -159,7 +173,7 @@ def serve(requests: list[Request], budget_bytes: float = 150e9, storage: str = "
             g = Geometry(case.dom)
             L = Level(g, "entropic")
             L.init_equilibrium(case.rho, case.vel)
-            kbc[req.rid] = [req, g, L, case.params, torch.cuda.Stream(), 0]
+            kbc[req.rid] = [req, g, L, case.params, torch.cuda.Stream(), 0, case]
             kbc_bytes += need
             return "ok"
         if active and sum(r.n ** 3 for r, _, _ in active.values()) + req.n ** 3 > max_active_cells:
@@ -232,7 +246,7 @@ def serve(requests: list[Request], budget_bytes: float = 150e9, storage: str = "
             e[5] += n
             if e[5] >= e[0].steps:
                 req, g, L = e[0], e[1], e[2]
-                _finish(req, L.mass_momentum(), np.zeros(3), now())
+                _finish(req, L.mass_momentum(), kbc_drag(req, e[6], L), now())
                 if keep_states:
                     states[req.rid] = L.state()[0]
                 L.close()
@@ -265,7 +279,7 @@ def serve_sequential(requests: list[Request], storage: str = "f16", keep_states:
             n = min(1000, left)
             L.execute_timestep_batch(case.params, n)
             left -= n
-        _finish(req, L.mass_momentum(), np.zeros(3) if req.operator == "entropic" else L.forces(), now())
+        _finish(req, L.mass_momentum(), kbc_drag(req, case, L) if req.operator == "entropic" else L.forces(), now())
         if keep_states:
             states[req.rid] = L.state()[0]
         L.close()

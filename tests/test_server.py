@@ -67,8 +67,12 @@ def test_served_mix_with_kbc_equals_solving_alone(oal):
     assert served["completed"] == 10 and served["completed_d3q39"] == sum(r.operator == "entropic" for r in reqs)
     reqs2 = server.make_requests(10, **kw)
     seq, alone = server.serve_sequential(reqs2, storage="f32", keep_states=True)
+    seq_cs = {r.rid: r.checksum for r in reqs2}
     for r in reqs:
         assert np.array_equal(states[r.rid], alone[r.rid]), (r.rid, r.operator)
-        assert all(np.isfinite(r.checksum))
+        assert all(np.isfinite(r.checksum)) and r.checksum == seq_cs[r.rid]
+        if r.operator == "entropic" and r.kind == "channel":
+            # the surface-stress drag on the sphere: in the stream direction
+            assert r.drag > 0, r.checksum
     kbc = [r for r in reqs if r.operator == "entropic"]
     assert len(kbc) < 2 or any(r.admitted - r.arrival > 1e-3 for r in kbc)
