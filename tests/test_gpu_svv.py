@@ -121,6 +121,30 @@ def test_variable_nu_sgs_refreshes_after_the_filter(oal, oracle_lib, tgv):
     assert np.max(np.abs(g["pi"] - O.pi_neq)) < 4e-7 + 1e-11 * np.max(np.abs(O.pi_neq))
 
 
+@pytest.mark.parametrize("storage,dtype,tol", [("f64", np.float64, 1e-11), ("f32", np.float32, 2e-5)])
+def test_bouzidi_after_the_filter(oal, oracle_lib, channel, storage, dtype, tol):
+    """The filter before the linear Bouzidi wall (timestep.jl:1576-1611, then :1752-1768): the
+    correction reads the filtered post-collision populations, as the reference's filter writes
+    f_post_collision on a level with boundary cells."""
+    from openaerolab_alpha_01_b200.bouzidi import sphere_qmap
+    d = channel.dom
+    cells, q = sphere_qmap(d, (10.0, 8.0, 8.0), 3.0)
+    p = with_svv(channel.params, eps_x=0.002, eps_yz=0.004, solid_bc=capi.OAL_SOLID_BOUZIDI, collect_forces=0)
+    g = Geometry(d)
+    L = Level(g, storage=storage)
+    L.init_equilibrium(channel.rho, channel.vel)
+    L.set_bouzidi(cells, q)
+    O = oracle_lib.OracleLevel(d.coords, d.neighbor_table, d.shape, obstacle=d.obstacle, dtype=dtype)
+    O.init_equilibrium(channel.rho, channel.vel)
+    for i in range(10):
+        p.time_step_seed = i
+        L.perform_timestep(p)
+        O.step_bouzidi(p, dict(cells=cells, q=q))
+    f = L.state()[0]
+    L.close(); g.close()
+    assert rel(f, O.f) < tol
+
+
 def test_graph_replay_equals_steps(oal, channel):
     g = Geometry(channel.dom)
     p = with_svv(channel.params)
