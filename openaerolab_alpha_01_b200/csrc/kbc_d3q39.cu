@@ -620,8 +620,9 @@ struct SvvView {
   int32_t nb;
 };
 
-__device__ __forceinline__ float svv_tap(const SvvView& v, const int32_t* s_nbr, int b, int x, int y, int z, int dx,
-                                         int dy, int dz, int k, float own) {
+// the direction-0 element of the input population at (x, y, z) + d (one axis), or `own`
+__device__ __forceinline__ int64_t svv_tap_offset(const SvvView& v, const int32_t* s_nbr, int b, int x, int y, int z,
+                                                  int dx, int dy, int dz, int64_t own) {
   const int nx = x + dx, ny = y + dy, nz = z + dz;
   const int ox = nx < 0 ? -1 : (nx > 7 ? 1 : 0), oy = ny < 0 ? -1 : (ny > 7 ? 1 : 0), oz = nz < 0 ? -1 : (nz > 7 ? 1 : 0);
   const int bo = (ox | oy | oz) == 0 ? b : s_nbr[(ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)];
@@ -631,31 +632,36 @@ __device__ __forceinline__ float svv_tap(const SvvView& v, const int32_t* s_nbr,
     const int32_t sl = v.mslot[bo];
     if (sl >= 0 && ((v.cmask[(int64_t)sl * 512 + c] >> 13) & 1u)) return own;
   }
-  return v.fin[((int64_t)bo * Q + k) * 512 + c];
+  return (int64_t)bo * Q * 512 + c;
 }
 
+// the taps are resolved once per cell (neighbour block, solid masks, fall-back to the cell's own
+// input population); each direction then reads them at + k 512
 template <bool YZ>
 __device__ __forceinline__ void svv_axis(const SvvView a, const Tables& T, const int32_t* s_nbr, int b, int cell,
-                                      float eps, float* sf) {
+                                         float eps, float* sf) {
   const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
+  const int64_t own = (int64_t)b * Q * 512 + cell;
+  constexpr int NT = YZ ? 8 : 4;
+  int64_t off[NT];
+#pragma unroll
+  for (int j = 0; j < NT; ++j) {
+    const int s = (j & 3) < 2 ? (j & 3) - 2 : (j & 3) - 1;  // -2, -1, +1, +2
+    off[j] = YZ ? (j < 4 ? svv_tap_offset(a, s_nbr, b, x, y, z, 0, s, 0, own) : svv_tap_offset(a, s_nbr, b, x, y, z, 0, 0, s, own))
+                : svv_tap_offset(a, s_nbr, b, x, y, z, s, 0, 0, own);
+  }
   float d_rho = 0.0f, d_jx = 0.0f, d_jy = 0.0f, d_jz = 0.0f;
 #pragma unroll 1
   for (int k = 0; k < Q; ++k) {
-    const float own = a.fin[((int64_t)b * Q + k) * 512 + cell];
+    const float* fk = a.fin + (int64_t)k * 512;
     const float fc = sf[k * kThreads];
     float ff;
     if (YZ) {
-      const float by = svv_tap(a, s_nbr, b, x, y, z, 0, -2, 0, k, own) - 4.0f * svv_tap(a, s_nbr, b, x, y, z, 0, -1, 0, k, own) +
-                       6.0f * fc - 4.0f * svv_tap(a, s_nbr, b, x, y, z, 0, 1, 0, k, own) +
-                       svv_tap(a, s_nbr, b, x, y, z, 0, 2, 0, k, own);
-      const float bz = svv_tap(a, s_nbr, b, x, y, z, 0, 0, -2, k, own) - 4.0f * svv_tap(a, s_nbr, b, x, y, z, 0, 0, -1, k, own) +
-                       6.0f * fc - 4.0f * svv_tap(a, s_nbr, b, x, y, z, 0, 0, 1, k, own) +
-                       svv_tap(a, s_nbr, b, x, y, z, 0, 0, 2, k, own);
+      const float by = fk[off[0]] - 4.0f * fk[off[1]] + 6.0f * fc - 4.0f * fk[off[2]] + fk[off[3]];
+      const float bz = fk[off[4]] - 4.0f * fk[off[5]] + 6.0f * fc - 4.0f * fk[off[6]] + fk[off[7]];
       ff = fc - eps * (by + bz);
     } else {
-      const float bx = svv_tap(a, s_nbr, b, x, y, z, -2, 0, 0, k, own) - 4.0f * svv_tap(a, s_nbr, b, x, y, z, -1, 0, 0, k, own) +
-                       6.0f * fc - 4.0f * svv_tap(a, s_nbr, b, x, y, z, 1, 0, 0, k, own) +
-                       svv_tap(a, s_nbr, b, x, y, z, 2, 0, 0, k, own);
+      const float bx = fk[off[0]] - 4.0f * fk[off[1]] + 6.0f * fc - 4.0f * fk[off[2]] + fk[off[3]];
       ff = fc - eps * bx;
     }
     const float diff = ff - fc;
@@ -674,12 +680,6 @@ __device__ __forceinline__ void svv_axis(const SvvView a, const Tables& T, const
   }
 }
 
-// One cell per thread (kernel_entropic_d3q39.jl:859-3368 on such a level). The thread's populations
-// live in its shared-memory column (the pulled f, then a_k, then the post-collision values) and the
-// per-direction loops run rolled over the CTA's tables, which keeps the step's code small enough to
-// stay in the instruction cache. f_eq is recomputed from its multipliers where a pass needs it.
-// EDGES: the level has domain faces or solid cells (the pin, bounce-back and gradient fall-backs
-// are compiled in); periodic boxes without obstacles run the instance without them.
 // SVV: the spectral vanishing viscosity is compiled in (a.svv_x or a.svv_yz > 0).
 template <bool EDGES, bool FAST, bool SVV = false>
 __global__ void __launch_bounds__(kThreads, FAST ? KBC_FAST_MIN_BLOCKS : KBC_MIN_BLOCKS) k_kbc_step(const KbcArgs a) {
