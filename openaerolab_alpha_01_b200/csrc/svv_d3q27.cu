@@ -19,7 +19,6 @@
 // shared memory (the thread's own column) for the correction. HBM traffic per fluid cell: the
 // 27 input populations once, the 27 output populations read and written.
 #include "svv_d3q27.h"
-#include "vmath.cuh"
 
 namespace oal {
 
@@ -122,19 +121,11 @@ __global__ void __launch_bounds__(svv_threads<R>(), 3) k_svv(const SvvArgs a, co
 template <class S> struct PairIO;
 template <> struct PairIO<float> {
   static __device__ __forceinline__ float2 load(const float* p, float, float) { return *reinterpret_cast<const float2*>(p); }
-  static __device__ __forceinline__ F2 load2(const float* p, F2) {
-    const float2 v = *reinterpret_cast<const float2*>(p);
-    return f2(v.x, v.y);
-  }
   static __device__ __forceinline__ void store(float* p, float a, float b, float, float) {
     *reinterpret_cast<float2*>(p) = make_float2(a, b);
   }
 };
 template <> struct PairIO<__half> {
-  static __device__ __forceinline__ F2 load2(const __half* p, F2 w) {
-    const float2 h = __half22float2(*reinterpret_cast<const __half2*>(p));
-    return vfma(w, f2(h.x, h.y), w);
-  }
   static __device__ __forceinline__ float2 load(const __half* p, float w, float) {
     const float2 h = __half22float2(*reinterpret_cast<const __half2*>(p));
     return make_float2(fmaf(w, h.x, w), fmaf(w, h.y, w));
@@ -144,10 +135,6 @@ template <> struct PairIO<__half> {
   }
 };
 template <> struct PairIO<__nv_bfloat16> {
-  static __device__ __forceinline__ F2 load2(const __nv_bfloat16* p, F2 w) {
-    const float2 h = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
-    return vfma(w, f2(h.x, h.y), w);
-  }
   static __device__ __forceinline__ float2 load(const __nv_bfloat16* p, float w, float) {
     const float2 h = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
     return make_float2(fmaf(w, h.x, w), fmaf(w, h.y, w));
@@ -174,48 +161,6 @@ __device__ __forceinline__ IDX svv_pair_offset(const SvvArgs& a, int b, int x, i
   s0 = svv_solid(a, bb, c);
   s1 = svv_solid(a, bb, c + 1);
   return (IDX)a.pi(bb, c, 0);
-}
-
-// The same filter for a pair none of whose taps falls back, on packed f32x2 arithmetic: each
-// instruction performs the scalar form's operation on both lanes, rounded alike (no contraction).
-template <class S, class IDX>
-__device__ __forceinline__ void svv_pairs_filter_packed(const SvvArgs& a, const S* __restrict__ fin,
-                                                        const S* __restrict__ fout, IDX own, IDX kst, const IDX (&t)[10],
-                                                        bool fx, bool fyz, float (*s_fl)[256], int l0, float (&acc)[8]) {
-  const F2 ex = splat<F2>(a.eps_x), eyz = splat<F2>(a.eps_yz), c4 = splat<F2>(4.0f), c6 = splat<F2>(6.0f);
-  F2 r = splat<F2>(0.0f), jx = r, jy = r, jz = r;
-#pragma unroll 3
-  for (int k = 0; k < kQ27; ++k) {
-    const F2 w = splat<F2>(float(q27_w(k)));
-    const S* fk = fin + (IDX)k * kst;
-    const F2 fc = PairIO<S>::load2(fout + own + (IDX)k * kst, w);
-    F2 bl = splat<F2>(0.0f);
-    if (fx) {
-      // lane 0 (x): x-2, x-1, x+1, x+2; lane 1 (x+1): x-1, x, x+2, x+3
-      const F2 o = PairIO<S>::load2(fk + own, w), m = PairIO<S>::load2(fk + t[0], w), p = PairIO<S>::load2(fk + t[1], w);
-      float ol, oh, ml, mh, pl, ph;
-      f2split(o, ol, oh); f2split(m, ml, mh); f2split(p, pl, ph);
-      const F2 t0 = m, t1 = f2(mh, ol), t2 = f2(oh, pl), t3 = p;
-      bl = bl + ex * ((((t0 - c4 * t1) + c6 * fc) - c4 * t2) + t3);
-    }
-    if (fyz) {
-#pragma unroll
-      for (int a2 = 0; a2 < 2; ++a2) {
-        const int j0 = 2 + 4 * a2;
-        const F2 v0 = PairIO<S>::load2(fk + t[j0], w), v1 = PairIO<S>::load2(fk + t[j0 + 1], w);
-        const F2 v2 = PairIO<S>::load2(fk + t[j0 + 2], w), v3 = PairIO<S>::load2(fk + t[j0 + 3], w);
-        bl = bl + eyz * ((((v0 - c4 * v1) + c6 * fc) - c4 * v2) + v3);
-      }
-    }
-    const F2 f = fc - bl;
-    const F2 e = f - fc;
-    r = r + e;
-    jx = jx + e * splat<F2>(float(q27_cx(k)));
-    jy = jy + e * splat<F2>(float(q27_cy(k)));
-    jz = jz + e * splat<F2>(float(q27_cz(k)));
-    f2split(f, s_fl[k][l0], s_fl[k][l0 + 1]);
-  }
-  f2split(r, acc[0], acc[4]); f2split(jx, acc[1], acc[5]); f2split(jy, acc[2], acc[6]); f2split(jz, acc[3], acc[7]);
 }
 
 // the filter of the 27 directions of a pair of cells: the filtered values into s_fl, the changes
@@ -301,7 +246,7 @@ __global__ void __launch_bounds__(128, 6) k_svv_pairs(const SvvArgs a, const S* 
   float acc[8];
   // the fall-back selects only where a tap of the pair falls back (cells next to a solid or a
   // missing block); elsewhere the loads are used as they are
-  if (fb == 0) svv_pairs_filter_packed<S, IDX>(a, fin, fout, own, kst, t, fx, fyz, s_fl, l0, acc);
+  if (fb == 0) svv_pairs_filter<S, IDX, false>(a, fin, fout, own, kst, t, fb, fx, fyz, s_fl, l0, acc);
   else svv_pairs_filter<S, IDX, true>(a, fin, fout, own, kst, t, fb, fx, fyz, s_fl, l0, acc);
   const float r0 = acc[0], x0 = acc[1], y0 = acc[2], z0 = acc[3], r1 = acc[4], x1 = acc[5], y1 = acc[6], z1 = acc[7];
   const float inv_cs2 = 1.0f / float(1.0 / 3.0);  // CS2_LATTICE
