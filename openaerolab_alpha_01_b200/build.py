@@ -18,8 +18,8 @@ INCLUDE = PKG.parent / "include"
 LIB = PKG / "liboal.so"
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
-# -fmad=false: every fused multiply-add in the kernels is written explicitly, so the one-cell and
-# two-cell (packed f32x2) forms of the collision round identically.
+# -fmad=false: the scalar arithmetic of the kernels fuses only the multiply-adds written explicitly
+# (the bit-exact D3Q39, octree and SVV paths rely on it); packed f32x2 code agrees to rounding.
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
               "--expt-relaxed-constexpr", "-fmad=false", "-Xptxas", "-warn-spills"]
 

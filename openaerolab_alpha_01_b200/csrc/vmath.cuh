@@ -1,8 +1,10 @@
 // vmath.cuh — one arithmetic vocabulary for three lane types: float, double and F2 (two float
 // lanes in a 64-bit register, operated on with sm_100a's packed f32x2 instructions). Collision
 // code written once against these helpers runs one cell per thread (float, double) or two cells
-// per thread (F2) with the same operation sequence per lane, so both float forms round alike.
-// The library is compiled with -fmad=false: every fused multiply-add is written explicitly.
+// per thread (F2) with the same operation sequence per lane. The library is compiled with
+// -fmad=false, so the scalar forms fuse only the multiply-adds written explicitly; ptxas may still
+// contract a packed multiply and the packed add that consumes it into one packed FMA, so the F2
+// form agrees with the scalar forms to rounding, not bit for bit.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
