@@ -169,8 +169,9 @@ typedef struct oal_step_params {
    * SVV_X_EPSILON on levels <= SVV_X_MAX_LEVEL and SVV_YZ_EPSILON on levels >= SVV_YZ_MIN_LEVEL
    * (1-based, timestep.jl:1577-1578); the caller passes the level's values. D3Q27: a post-pass after
    * the step kernels, before the outlet and the wall corrections (timestep.jl:1576-1611); D3Q39:
-   * inside the step, after the post-collision guard (kernel_entropic_d3q39.jl:3256-3310).
-   * Library-owned levels (single, hierarchy and D3Q39) only. */
+   * inside the step, after the post-collision guard (kernel_entropic_d3q39.jl:3256-3310). On
+   * caller-owned arrays (oal_stream_collide) the filter also writes f_post_collision when given;
+   * batched cases refuse a non-zero strength. */
   float svv_x_epsilon;
   float svv_yz_epsilon;
 } oal_step_params;

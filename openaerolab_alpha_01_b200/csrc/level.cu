@@ -1330,8 +1330,6 @@ oal_status oal_stream_collide(const oal_geometry* g, const oal_level_fields* fl,
   if (s != OAL_OK) return s;
   if (cp.flags & (CF_SGS_PI | CF_SGS_DYNAMIC))
     return set_error(OAL_E_UNSUPPORTED, "variable_nu_sgs: the Pi_neq field and the test filter belong to plain levels, not to caller-owned arrays (oal_stream_collide)");
-  if (p->svv_x_epsilon > 0.0f || p->svv_yz_epsilon > 0.0f)
-    return set_error(OAL_E_UNSUPPORTED, "the SVV filter is a post-pass of library-owned levels, not of caller-owned arrays (oal_stream_collide)");
   if (!fl->f_in || !fl->f_out || !fl->rho_out || !fl->vel_out || !fl->vel_in)
     return set_error(OAL_E_INVALID_ARG, "f_in, f_out, rho_out, vel_out and vel_in are required");
   if (fl->f_in == fl->f_out) return set_error(OAL_E_INVALID_ARG, "f_in and f_out must differ (pull scheme)");
@@ -1349,6 +1347,17 @@ oal_status oal_stream_collide(const oal_geometry* g, const oal_level_fields* fl,
   a.flags_any = cp.flags;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   OAL_CUDA_TRY(launch_by_storage(fl->storage, g, a, PATH_PLAIN, st));
+  if (p->svv_x_epsilon > 0.0f || p->svv_yz_epsilon > 0.0f) {
+    // the filter on the caller's output, and on its f_post_collision when given (the reference's
+    // filter writes both on a level with boundary cells, timestep.jl:1584-1594)
+    PopIndex pi{};
+    pi.binfo = g->d_binfo;
+    pi.bst = fl->f_block_stride;
+    pi.kst = fl->f_dir_stride;
+    const int64_t n_el = (int64_t)(g->nb - 1) * pi.bst + 26 * pi.kst + 512;
+    OAL_CUDA_TRY(svv_enqueue(fl->storage, fl->f_in, fl->f_out, pi, g->nb, n_el, g->d_nbr, g->nb, g->d_mslot, g->d_cmask,
+                             p->svv_x_epsilon, p->svv_yz_epsilon, st, fl->f_post_collision));
+  }
   if ((cp.flags & CF_COLLECT) && fl->force_out) {
     k_reduce3<<<1, 256, 0, st>>>(g->d_force_part, (int64_t)g->nb * 4, fl->force_out);
     OAL_CUDA_TRY(cudaGetLastError());

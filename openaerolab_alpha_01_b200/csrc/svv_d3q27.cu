@@ -61,7 +61,8 @@ __device__ __forceinline__ IDX svv_tap_offset(const SvvArgs& a, int b, int x, in
 }
 
 template <class S, class R, class IDX>
-__global__ void __launch_bounds__(svv_threads<R>(), 3) k_svv(const SvvArgs a, const S* __restrict__ fin, S* __restrict__ fout) {
+__global__ void __launch_bounds__(svv_threads<R>(), 3) k_svv(const SvvArgs a, const S* __restrict__ fin, S* __restrict__ fout,
+                                                             S* __restrict__ fpost2) {
   constexpr int kT = svv_threads<R>(), kPer = kCells / kT;
   const int b = blockIdx.x / kPer;
   const int cell = (blockIdx.x % kPer) * kT + threadIdx.x;
@@ -109,7 +110,9 @@ __global__ void __launch_bounds__(svv_threads<R>(), 3) k_svv(const SvvArgs a, co
     const R cu = R(q27_cx(k)) * d_jx + R(q27_cy(k)) * d_jy + R(q27_cz(k)) * d_jz;
     R v = s_fl[k][threadIdx.x] - w * (d_rho + inv_cs2 * cu);
     v = v < R(1e-12f) ? R(1e-12f) : v;  // NaN passes
-    fout[own + (IDX)k * kst] = Codec<S>::enc(v, w, inv_w);
+    const S word = Codec<S>::enc(v, w, inv_w);
+    fout[own + (IDX)k * kst] = word;
+    if (fpost2) fpost2[own + (IDX)k * kst] = word;
   }
 }
 
@@ -212,7 +215,8 @@ __device__ __forceinline__ void svv_pairs_filter(const SvvArgs& a, const S* __re
 }
 
 template <class S, class IDX>
-__global__ void __launch_bounds__(128, 6) k_svv_pairs(const SvvArgs a, const S* __restrict__ fin, S* __restrict__ fout) {
+__global__ void __launch_bounds__(128, 6) k_svv_pairs(const SvvArgs a, const S* __restrict__ fin, S* __restrict__ fout,
+                                                      S* __restrict__ fpost2) {
   const int b = blockIdx.x >> 1;
   const int base = (blockIdx.x & 1) << 8;
   const int l0 = threadIdx.x << 1;  // the pair's first cell within the CTA's half block
@@ -261,31 +265,40 @@ __global__ void __launch_bounds__(128, 6) k_svv_pairs(const SvvArgs a, const S* 
     // a solid cell of the pair keeps its stored word
     if (d0 || d1) {
       S* q = fout + own + (IDX)k * kst;
-      if (!d0) q[0] = Codec<S>::enc(v0, w, inv_w);
-      if (!d1) q[1] = Codec<S>::enc(v1, w, inv_w);
+      S* q2 = fpost2 ? fpost2 + own + (IDX)k * kst : nullptr;
+      if (!d0) { q[0] = Codec<S>::enc(v0, w, inv_w); if (q2) q2[0] = q[0]; }
+      if (!d1) { q[1] = Codec<S>::enc(v1, w, inv_w); if (q2) q2[1] = q[1]; }
     } else {
       PairIO<S>::store(fout + own + (IDX)k * kst, v0, v1, w, inv_w);
+      if (fpost2) PairIO<S>::store(fpost2 + own + (IDX)k * kst, v0, v1, w, inv_w);
     }
   }
 }
 
 template <class S, class R>
-cudaError_t enqueue_t(const SvvArgs& a, const void* fin, void* fout, int32_t nb, int64_t n_elements, cudaStream_t st) {
+cudaError_t enqueue_t(const SvvArgs& a, const void* fin, void* fout, void* fpost2, int32_t nb, int64_t n_elements,
+                      cudaStream_t st) {
   constexpr int kT = svv_threads<R>();
   const unsigned grid = (unsigned)nb * (unsigned)(kCells / kT);
+  const S* in = static_cast<const S*>(fin);
+  S* out = static_cast<S*>(fout);
+  S* post = static_cast<S*>(fpost2);
   if constexpr (sizeof(R) == 4) {
-    if (!a.pi.dense) {  // block layout: pairs are aligned words
+    // pairs of x-adjacent cells are aligned words where the strides are even and the arrays start
+    // on a word (every block layout this library allocates; a caller's arrays are checked)
+    auto aligned = [](const void* p) { return p == nullptr || ((uintptr_t)p % (2 * sizeof(S))) == 0; };
+    if (!a.pi.dense && a.pi.bst % 2 == 0 && a.pi.kst % 2 == 0 && aligned(fin) && aligned(fout) && aligned(fpost2)) {
       if (n_elements < (int64_t(1) << 32))
-        k_svv_pairs<S, uint32_t><<<(unsigned)nb * 2u, 128, 0, st>>>(a, static_cast<const S*>(fin), static_cast<S*>(fout));
+        k_svv_pairs<S, uint32_t><<<(unsigned)nb * 2u, 128, 0, st>>>(a, in, out, post);
       else
-        k_svv_pairs<S, int64_t><<<(unsigned)nb * 2u, 128, 0, st>>>(a, static_cast<const S*>(fin), static_cast<S*>(fout));
+        k_svv_pairs<S, int64_t><<<(unsigned)nb * 2u, 128, 0, st>>>(a, in, out, post);
       return cudaGetLastError();
     }
   }
   if (n_elements < (int64_t(1) << 32))
-    k_svv<S, R, uint32_t><<<grid, kT, 0, st>>>(a, static_cast<const S*>(fin), static_cast<S*>(fout));
+    k_svv<S, R, uint32_t><<<grid, kT, 0, st>>>(a, in, out, post);
   else
-    k_svv<S, R, int64_t><<<grid, kT, 0, st>>>(a, static_cast<const S*>(fin), static_cast<S*>(fout));
+    k_svv<S, R, int64_t><<<grid, kT, 0, st>>>(a, in, out, post);
   return cudaGetLastError();
 }
 
@@ -293,16 +306,16 @@ cudaError_t enqueue_t(const SvvArgs& a, const void* fin, void* fout, int32_t nb,
 
 cudaError_t svv_enqueue(int32_t storage, const void* f_in, void* f_out, const PopIndex& pi, int32_t nb,
                         int64_t n_elements, const int32_t* nbr, int32_t n_real, const int32_t* mslot,
-                        const uint32_t* cmask, float eps_x, float eps_yz, cudaStream_t st) {
+                        const uint32_t* cmask, float eps_x, float eps_yz, cudaStream_t st, void* f_post2) {
   if ((eps_x == 0.0f && eps_yz == 0.0f) || nb <= 0) return cudaSuccess;
   SvvArgs a;
   a.pi = pi; a.nbr = nbr; a.n_real = n_real; a.mslot = cmask ? mslot : nullptr; a.cmask = cmask;
   a.eps_x = eps_x; a.eps_yz = eps_yz;
   switch (storage) {
-    case 0: return enqueue_t<float, float>(a, f_in, f_out, nb, n_elements, st);
-    case 1: return enqueue_t<__half, float>(a, f_in, f_out, nb, n_elements, st);
-    case 2: return enqueue_t<__nv_bfloat16, float>(a, f_in, f_out, nb, n_elements, st);
-    case 3: return enqueue_t<double, double>(a, f_in, f_out, nb, n_elements, st);
+    case 0: return enqueue_t<float, float>(a, f_in, f_out, f_post2, nb, n_elements, st);
+    case 1: return enqueue_t<__half, float>(a, f_in, f_out, f_post2, nb, n_elements, st);
+    case 2: return enqueue_t<__nv_bfloat16, float>(a, f_in, f_out, f_post2, nb, n_elements, st);
+    case 3: return enqueue_t<double, double>(a, f_in, f_out, f_post2, nb, n_elements, st);
   }
   return cudaErrorInvalidValue;
 }

@@ -145,6 +145,43 @@ def test_bouzidi_after_the_filter(oal, oracle_lib, channel, storage, dtype, tol)
     assert rel(f, O.f) < tol
 
 
+@pytest.mark.parametrize("storage,dtype,tol,ct", [("f64", np.float64, 1e-11, "float64"), ("f32", np.float32, 2e-5, "float32")])
+def test_caller_owned_arrays_with_post(oal, oracle_lib, channel, storage, dtype, tol, ct):
+    """oal_stream_collide on arrays in the reference's (8,8,8,nb,27) layout with the filter on and
+    f_post_collision given: the filter writes the output and f_post_collision alike."""
+    import ctypes as C
+    import torch
+    d = channel.dom
+    g = Geometry(d)
+    nb = d.n_blocks
+    tdt = getattr(torch, ct)
+    fa = torch.tensor(oracle_lib.init_feq(channel.rho, channel.vel), dtype=tdt, device="cuda").contiguous()
+    fb = torch.empty_like(fa)
+    post = torch.full_like(fa, float("nan"))
+    va = torch.tensor(channel.vel, dtype=tdt, device="cuda").contiguous()
+    vb = torch.empty_like(va)
+    rho = torch.empty((nb, 512), dtype=tdt, device="cuda")
+    p = with_svv(channel.params, eps_x=0.003, eps_yz=0.005, store_post_collision=1, collect_forces=0)
+    st = capi.OAL_STORE_F64 if storage == "f64" else capi.OAL_STORE_F32
+    O = oracle_lib.OracleLevel(d.coords, d.neighbor_table, d.shape, obstacle=d.obstacle, dtype=dtype)
+    O.init_equilibrium(channel.rho, channel.vel)
+    if dtype == np.float32:
+        O.f[...] = fa.cpu().numpy()
+    for i in range(6):
+        p.time_step_seed = i
+        fl = capi.LevelFields(fa.data_ptr(), fb.data_ptr(), post.data_ptr(), rho.data_ptr(), vb.data_ptr(),
+                              va.data_ptr(), st, 0, 512, 512 * nb, 512 * nb, None)
+        capi.check(capi.lib().oal_stream_collide(g.handle, C.byref(fl), C.byref(p), None))
+        O.step(p)
+        fa, fb = fb, fa
+        va, vb = vb, va
+    torch.cuda.synchronize()
+    g.close()
+    got_f, got_post = fa.cpu().numpy(), post.cpu().numpy()
+    assert np.array_equal(got_post, got_f)
+    assert rel(got_f, O.f) < tol
+
+
 def test_graph_replay_equals_steps(oal, channel):
     g = Geometry(channel.dom)
     p = with_svv(channel.params)
