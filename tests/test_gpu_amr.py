@@ -148,17 +148,27 @@ def test_uniform_flow_fp32(env):
 
 
 @pytest.mark.parametrize("storage,tol", [("f64", 1e-10), ("f32", 5e-5)])
-def test_channel_bouzidi_on_the_fine_level(env, storage, tol):
+@pytest.mark.parametrize("sphere", [(48.0, 5.0), (35.5, 3.2)], ids=["inside", "at_the_interface"])
+def test_channel_bouzidi_on_the_fine_level(env, storage, tol, sphere):
     """The linear Bouzidi wall on the sphere of the refined level (the reference applies it on the
     finest level, bouzidi_levels = 1): the correction follows each fine step, before the
-    restriction, in the captured hierarchy graph; a second advance reuses the graph."""
+    restriction, in the captured hierarchy graph; a second advance reuses the graph. With the
+    sphere against the coarse/fine interface (fine x = 32) the cell behind some q < 1/2 links lies
+    in the level's ghost region, outside the level's own blocks: as in the reference, whose
+    neighbour table has no entry there, the link takes the ff_fallback rule."""
     oracle, amr, solver = env
     from openaerolab_alpha_01_b200 import _capi as capi
     from openaerolab_alpha_01_b200.bouzidi import sphere_qmap
     coarse = solver.build_box(6, 2, 2)
     fine = amr.refine(coarse, amr.blocks_in_box(coarse, (16, 0, 0), (32, 16, 16)))
-    solver.apply_analytic_sphere_obstacle(fine, (48.0, 16.0, 16.0), 5.0)
-    cells, q = sphere_qmap(fine, (48.0, 16.0, 16.0), 5.0)
+    cx, r = sphere
+    solver.apply_analytic_sphere_obstacle(fine, (cx, 16.0, 16.0), r)
+    cells, q = sphere_qmap(fine, (cx, 16.0, 16.0), r)
+    if cx < 40.0:
+        # some boundary cell sits in the fine level's first plane, so a link's behind cell is a ghost
+        gx = fine.cell_positions()[0]
+        b, c = cells[:, 0] - 1, (cells[:, 1] - 1) + 8 * (cells[:, 2] - 1) + 64 * (cells[:, 3] - 1)
+        assert (gx[b, c] <= 33.0).any()
     doms = [coarse, fine]
     u = 0.05
     rho_fn = lambda X, Y, Z: np.ones_like(X)
