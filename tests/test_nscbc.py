@@ -136,6 +136,21 @@ def test_gpu_outlet_with_pi_neq_sgs(oal, oracle_lib):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("storage,dtype,tol", [("f64", np.float64, 1e-11), ("f32", np.float32, 2e-5)])
+def test_gpu_outlet_after_the_svv_filter(oal, oracle_lib, storage, dtype, tol):
+    """The filter, then the outlet (timestep.jl:1576-1611 before :1617-1664): the outlet rebuilds
+    its face plane from the filtered state."""
+    from openaerolab_alpha_01_b200 import _capi as capi
+    case = sphere_channel_case(32, 16, 16, diameter=6.0, centre_x=10.0, u_inlet=0.05, re=100.0)
+    p = capi.StepParams.from_buffer_copy(case.params)
+    p.svv_x_epsilon = 0.003
+    p.svv_yz_epsilon = 0.005
+    f, rho, vel, _, O = _level_vs_oracle(oal, oracle_lib, case, storage, dtype, 8, False, p)
+    assert rel(f, O.f) < tol
+    assert rel(rho, O.rho) < tol and rel(vel, O.vel) < tol * 50
+
+
+@pytest.mark.gpu
 def test_gpu_outlet_graph_replay(oal):
     from openaerolab_alpha_01_b200.solver import Geometry, Level
     case = sphere_channel_case(32, 16, 16, diameter=6.0, centre_x=10.0, u_inlet=0.05, re=100.0)
