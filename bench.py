@@ -22,6 +22,7 @@ from __future__ import annotations
 import argparse
 import ctypes as C
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -316,8 +317,12 @@ def main():
     force = level.forces()
 
     # ---- end-to-end through the public API: per step the step parameters go from pinned host
-    # memory into the launch and the FP64 drag comes back to pinned host memory ----
-    pinned_force = torch.zeros(3, dtype=torch.float64).pin_memory()
+    # memory into the launch and the FP64 drag comes back to pinned host memory, where the host
+    # reads it; double-buffered, as a monitoring loop would run: step i + 1 is enqueued before the
+    # host waits for step i's drag ----
+    pinned_force = [torch.zeros(3, dtype=torch.float64).pin_memory() for _ in range(2)]
+    landed = [torch.cuda.Event() for _ in range(2)]
+    drag_seen = []
     e2e_steps = args.steps
     barrier()
     torch.cuda.synchronize()
@@ -326,10 +331,16 @@ def main():
         for i in range(e2e_steps):
             p.time_step_seed = args.warmup + args.steps + n_steady + i
             level.perform_timestep(p, sh)
-            level.forces_async(pinned_force.data_ptr(), sh)
-            stream.synchronize()
+            level.forces_async(pinned_force[i % 2].data_ptr(), sh)
+            landed[i % 2].record(stream)
+            if i > 0:
+                landed[(i - 1) % 2].synchronize()
+                drag_seen.append(float(pinned_force[(i - 1) % 2][0]))
+        landed[(e2e_steps - 1) % 2].synchronize()
+        drag_seen.append(float(pinned_force[(e2e_steps - 1) % 2][0]))
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
+    assert len(drag_seen) == e2e_steps and all(math.isfinite(v) for v in drag_seen)
     te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
