@@ -63,7 +63,9 @@ def run_pair(oracle, case, p, storage, dtype, steps, layout="block"):
 @pytest.mark.parametrize("storage,dtype,tol,layout", [("f64", np.float64, 1e-11, "block"),
                                                       ("f32", np.float32, 2e-5, "block"),
                                                       ("f32", np.float32, 2e-5, "dense"),
-                                                      ("f16", np.float64, 2e-3, "block")])
+                                                      ("f16", np.float64, 2e-3, "block"),
+                                                      ("f16", np.float64, 2e-3, "dense"),
+                                                      ("bf16", np.float64, 2e-2, "block")])
 def test_taylor_green(oal, oracle_lib, tgv, storage, dtype, tol, layout):
     p = with_svv(tgv.params)
     g, O = run_pair(oracle_lib, tgv, p, storage, dtype, 12, layout)
@@ -212,10 +214,11 @@ def test_refusals(oal, channel, tgv):
     B.close(); g.close()
 
 
-def test_hierarchy_levels(oal, oracle_lib):
+@pytest.mark.parametrize("storage,tol", [("f64", 1e-10), ("f32", 5e-5)])
+def test_hierarchy_levels(oal, oracle_lib, storage, tol):
     """A 3-level periodic hierarchy with the reference's gating at min_level 2 / max_level 1: the
-    y-z filter on the two finer levels, the x filter on the coarsest; FP64 against the oracle's
-    recursion at the hierarchy tolerance (1e-10 of max |f|)."""
+    y-z filter on the two finer levels, the x filter on the coarsest; against the oracle's
+    recursion at the hierarchy tolerances (FP64 1e-10, FP32 5e-5 of max |f|)."""
     from openaerolab_alpha_01_b200 import amr
     from openaerolab_alpha_01_b200.solver import svv_epsilons
     from .test_gpu_amr import compare, fields, run_pair as amr_pair
@@ -228,8 +231,8 @@ def test_hierarchy_levels(oal, oracle_lib):
             setattr(p, k, v)
     assert P[0].svv_x_epsilon > 0 and P[0].svv_yz_epsilon == 0 and P[2].svv_yz_epsilon > 0
     rho_fn, vel_fn = fields()
-    H, ora = amr_pair((oracle_lib, amr, None), doms, P, "f64", 3, rho_fn, vel_fn)
-    compare(H, ora, 3, 1e-10)
+    H, ora = amr_pair((oracle_lib, amr, None), doms, P, storage, 3, rho_fn, vel_fn)
+    compare(H, ora, 3, tol)
     H.close()
 
 
@@ -264,6 +267,33 @@ def test_q39_channel_bitwise(oal, oracle_lib, eps_x, eps_yz):
     f, rho, vel = lvl.state()
     assert same_bits(f, ora.f), np.abs(f - ora.f).max()
     assert same_bits(vel, ora.vel) and same_bits(rho, ora.rho)
+    lvl.close(); g.close()
+
+
+def test_q39_channel_sponge_and_svv_bitwise(oal, oracle_lib):
+    """The filter with the sponge toward the inlet state and the near-wall clamp bounds (wall
+    distance given): the oracle's bits after 4 steps."""
+    case = sphere_channel_case(32, 16, 16, diameter=6.0, centre_x=12.0, u_inlet=0.05, re=200.0)
+    d = case.dom
+    gx, gy, gz = d.cell_positions()
+    d.sponge = (np.clip((gx - 24.0) / 8.0, 0.0, 1.0) * 0.6).astype(np.float32)
+    r = np.sqrt((gx - 0.5 - 12.0) ** 2 + (gy - 0.5 - 8.0) ** 2 + (gz - 0.5 - 8.0) ** 2) - 3.0
+    d.wall_dist = np.where(d.obstacle != 0, 0.0, np.maximum(r, 0.0)).astype(np.float32)
+    g = Geometry(d)
+    lvl = Level(g, "entropic", math="exact")
+    rng = np.random.default_rng(9)
+    vel = case.vel + 0.005 * rng.standard_normal(case.vel.shape) * (d.obstacle == 0)
+    lvl.init_equilibrium(case.rho, vel)
+    ora = oracle_lib.OracleQ39Level(d.neighbor_table, d.coords, d.shape, d.obstacle, sponge=d.sponge,
+                                    wall_dist=d.wall_dist).init_equilibrium(case.rho, vel)
+    p = default_entropic_params(tau=0.56, c_wale=0.2, u_inlet=0.05, sponge_blend_distributions=1,
+                                svv_x_epsilon=0.002, svv_yz_epsilon=0.004)
+    for i in range(4):
+        p.time_step_seed = 5 + i
+        lvl.step(p)
+        ora.step(p)
+    f = lvl.state()[0]
+    assert same_bits(f, ora.f), np.abs(f - ora.f).max()
     lvl.close(); g.close()
 
 
